@@ -1,0 +1,423 @@
+"""femorax_b200: a B200-native matrix-free hex8 hot path with the reference's element, operator and
+solver interface (amnp95/FemoraX: exec::InternalForce, exec::MatrixFreeOperator,
+solvers::LinearSolver, solvers::VectorOps), implemented in C++/CUDA behind the C ABI of
+include/femorax_b200.h and driven from here through ctypes.
+
+Device vectors are torch tensors (float64, or float32 for the *_f32 forms) on the handle's device;
+torch is used for memory and streams only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import FxError, check, lib
+from .meshes import ModelSpec
+
+__all__ = ["Model", "Compiled", "MeshArrays", "InternalForce", "OperatorCoefficients", "MatrixFreeOperator",
+           "SolveOptions", "SolveResult", "LinearSolver", "ConjugateGradient", "Gmres", "KrylovSolver",
+           "MixedPrecisionSolver", "VectorOps", "FxError", "ModelSpec"]
+
+
+def _i32(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(L.p_i32)
+
+
+def _f64(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(L.p_f64)
+
+
+def _ptr(t):
+    """Device pointer of a torch tensor (or an int address)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_contiguous():
+        raise ValueError("tensors must be contiguous")
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ------------------------------------------------------------------ model and compile step
+class Model:
+    """io::Model for this path, built in memory from a ModelSpec (meshes.py)."""
+
+    def __init__(self, spec: ModelSpec):
+        self.spec = spec
+        h = C.c_void_p()
+        tags, pt = _i32(spec.tags)
+        coords, pc = _f64(spec.coords)
+        check(lib().fx_model_create(len(tags), pt, pc, C.byref(h)))
+        self._h = h
+        for g in spec.groups:
+            mat = L.fx_material(kind=g.kind, E=g.E, nu=g.nu, rho=g.rho, sigma_y=g.sigma_y, H=g.H, hk=g.hk)
+            b, pb = _f64(np.array(g.b, dtype=np.float64))
+            et, pet = _i32(g.etags)
+            cn, pcn = _i32(np.asarray(g.conn).reshape(-1))
+            check(lib().fx_model_add_group(h, C.byref(mat), pb, int(g.lumped), len(et), pet, pcn))
+        if len(spec.fix_node):
+            a, pa = _i32(spec.fix_node)
+            d, pd = _i32(spec.fix_dof)
+            check(lib().fx_model_add_fix(h, len(a), pa, pd))
+        if len(spec.eqd_retained):
+            r, pr = _i32(spec.eqd_retained)
+            c, pc2 = _i32(spec.eqd_constrained)
+            d, pd = _i32(spec.eqd_dof)
+            check(lib().fx_model_add_equal_dof(h, len(r), pr, pc2, pd))
+        for r in spec.rayleigh:
+            et, pet = _i32(r.etags)
+            check(lib().fx_model_add_rayleigh(h, r.alphaM, r.betaK, r.betaKinit, r.betaKcomm, len(et), pet))
+        if len(spec.mass_node):
+            n, pn = _i32(spec.mass_node)
+            d, pd = _i32(spec.mass_dof)
+            v, pv = _f64(spec.mass_value)
+            check(lib().fx_model_add_mass(h, len(n), pn, pd, pv))
+
+    def compile(self, renumbering="rcm", simd_width=32, coloring=False) -> "Compiled":
+        """compile::compile_model (src/compile/batches.cpp:54-393)."""
+        r = L.FX_RENUMBER_RCM if renumbering == "rcm" else L.FX_RENUMBER_OFF
+        h = C.c_void_p()
+        check(lib().fx_compile(self._h, r, simd_width, int(coloring), C.byref(h)))
+        return Compiled(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().fx_model_destroy(h)
+            self._h = None
+
+
+class Compiled:
+    """The compile step's arrays (compile::Compiled, batches.hpp:80-116)."""
+
+    I32 = ("node_tag", "node_order", "element_order", "eq", "dof_offset", "node_model_index", "b_node", "b_eq",
+           "b_param", "b_tag", "color_start", "color_elements", "eq_dof")
+    F64 = ("coords", "lumped_mass", "lumped_alpha_mass", "nodal_mass", "nodal_alpha_mass")
+
+    def __init__(self, h):
+        self._h = h
+        s = (C.c_int64 * 8)()
+        check(lib().fx_compiled_sizes(h, s))
+        (self.num_nodes, self.num_equations, self.num_slots, self.num_batches, self.count, self.padded,
+         self.num_params, self.num_colors) = [int(v) for v in s]
+
+    def array(self, name):
+        if name in self.I32:
+            n = lib().fx_compiled_array_i32(self._h, name.encode(), None)
+            out = np.zeros(max(n, 0), np.int32)
+            if n > 0:
+                lib().fx_compiled_array_i32(self._h, name.encode(), out.ctypes.data_as(L.p_i32))
+            return out
+        if name in self.F64:
+            n = lib().fx_compiled_array_f64(self._h, name.encode(), None)
+            out = np.zeros(max(n, 0), np.float64)
+            if n > 0:
+                lib().fx_compiled_array_f64(self._h, name.encode(), out.ctypes.data_as(L.p_f64))
+            return out
+        raise KeyError(name)
+
+    def params(self):
+        arr = (L.fx_param_set * max(self.num_params, 1))()
+        m = L.fx_mesh()
+        check(lib().fx_compiled_mesh(self._h, arr, C.byref(m)))
+        return [arr[i] for i in range(self.num_params)]
+
+    def mesh(self) -> "MeshArrays":
+        ps = self.params()
+        return MeshArrays(num_nodes=self.num_nodes, num_equations=self.num_equations,
+                          coords=self.array("coords"), count=self.count, padded=self.padded,
+                          node=self.array("b_node"), eq=self.array("b_eq"), param=self.array("b_param"),
+                          params=params_table(ps), lumped_mass=self.array("lumped_mass"),
+                          nodal_mass=self.array("nodal_mass"), nodal_alpha_mass=self.array("nodal_alpha_mass"))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().fx_compiled_destroy(h)
+            self._h = None
+
+
+PARAM_FIELDS = ("kind", "mass_type", "E", "nu", "rho", "b0", "b1", "b2", "alphaM", "betaK", "betaKinit",
+                "betaKcomm", "sigma_y", "H", "hk")
+
+
+def params_table(ps) -> np.ndarray:
+    """Parameter sets as a float64 table [P, 15] in PARAM_FIELDS order."""
+    out = np.zeros((len(ps), len(PARAM_FIELDS)))
+    for i, p in enumerate(ps):
+        out[i] = [p.kind, p.mass_type, p.E, p.nu, p.rho, p.b[0], p.b[1], p.b[2], p.alphaM, p.betaK, p.betaKinit,
+                  p.betaKcomm, p.sigma_y, p.H, p.hk]
+    return out
+
+
+@dataclasses.dataclass
+class MeshArrays:
+    """What the device path consumes (fx_mesh): the compile step's arrays, from this library's
+    compile step or from the reference's own compile_model."""
+    num_nodes: int
+    num_equations: int
+    coords: np.ndarray  # [3N] SoA
+    count: int
+    padded: int
+    node: np.ndarray  # [8 P]
+    eq: np.ndarray  # [24 P]
+    param: np.ndarray  # [P]
+    params: np.ndarray  # [nparams, 15] (PARAM_FIELDS)
+    lumped_mass: np.ndarray = None
+    nodal_mass: np.ndarray = None
+    nodal_alpha_mass: np.ndarray = None
+
+    def to_c(self):
+        """(fx_mesh, keep-alive list)."""
+        keep = []
+        m = L.fx_mesh()
+        m.num_nodes = self.num_nodes
+        m.num_equations = self.num_equations
+        a, m.coords = _f64(self.coords)
+        keep.append(a)
+        m.count = self.count
+        m.padded = self.padded
+        for name in ("node", "eq", "param"):
+            a, p = _i32(getattr(self, name))
+            keep.append(a)
+            setattr(m, name, p)
+        P = (L.fx_param_set * max(len(self.params), 1))()
+        for i, row in enumerate(self.params):
+            q = P[i]
+            q.kind, q.mass_type = int(row[0]), int(row[1])
+            q.E, q.nu, q.rho = row[2], row[3], row[4]
+            q.b[0], q.b[1], q.b[2] = row[5], row[6], row[7]
+            q.alphaM, q.betaK, q.betaKinit, q.betaKcomm = row[8], row[9], row[10], row[11]
+            q.sigma_y, q.H, q.hk = row[12], row[13], row[14]
+        keep.append(P)
+        m.num_params = len(self.params)
+        m.params = C.cast(P, C.POINTER(L.fx_param_set))
+        for name in ("lumped_mass", "nodal_mass", "nodal_alpha_mass"):
+            v = getattr(self, name)
+            if v is not None and len(v):
+                a, p = _f64(v)
+                keep.append(a)
+                setattr(m, name, p)
+        return m, keep
+
+
+# ------------------------------------------------------------------ operator and force
+@dataclasses.dataclass
+class OperatorCoefficients:
+    """K_eff = stiffness K_t + damping C + mass M (element_operator.hpp:33-40)."""
+    stiffness: float = 1.0
+    damping: float = 0.0
+    mass: float = 0.0
+    initial: bool = False
+
+    def c(self):
+        return L.fx_coeffs(self.stiffness, self.damping, self.mass, int(self.initial), 0)
+
+
+class InternalForce:
+    """exec::InternalForce (src/exec/internal_force.hpp:80-213) on one B200."""
+
+    PATHS = {"auto": L.FX_PATH_AUTO, "general": L.FX_PATH_GENERAL, "box": L.FX_PATH_BOX}
+
+    def __init__(self, mesh: MeshArrays, device: int = 0):
+        m, keep = mesh.to_c()
+        h = C.c_void_p()
+        check(lib().fx_force_create(C.byref(m), device, C.byref(h)))
+        self._h = h
+        self.mesh = mesh
+        self.device = device
+        self.num_equations = mesh.num_equations
+
+    def set_path(self, path: str):
+        check(lib().fx_force_set_path(self._h, self.PATHS[path]))
+
+    def info(self) -> dict:
+        s = (C.c_int64 * 8)()
+        check(lib().fx_force_info(self._h, s))
+        keys = ("num_equations", "num_elements", "path", "box_qualifies", "nx", "ny", "nz", "device_bytes")
+        d = dict(zip(keys, [int(v) for v in s]))
+        d["path"] = {1: "general", 2: "box"}[d["path"]]
+        return d
+
+    def apply_operator(self, k: OperatorCoefficients, x, y, stream=None):
+        f = lib().fx_apply_operator_f32 if x.dtype.itemsize == 4 else lib().fx_apply_operator
+        check(f(self._h, k.c(), _ptr(x), _ptr(y), _stream(stream)))
+
+    def apply_operator_host(self, k: OperatorCoefficients, x: np.ndarray, y: np.ndarray, stream=None):
+        """The same apply from host buffers (copies inside)."""
+        check(lib().fx_apply_operator_host(self._h, k.c(), x.ctypes.data, y.ctypes.data, _stream(stream)))
+
+    def operator_diagonal(self, k: OperatorCoefficients, d, stream=None):
+        check(lib().fx_operator_diagonal(self._h, k.c(), _ptr(d), _stream(stream)))
+
+    def compute(self, u, v, f, stream=None):
+        fn = lib().fx_force_compute_f32 if u.dtype.itemsize == 4 else lib().fx_force_compute
+        check(fn(self._h, _ptr(u), _ptr(v), _ptr(f), _stream(stream)))
+
+    def mass_times_ground(self, direction: int, y, stream=None):
+        check(lib().fx_mass_times_ground(self._h, direction, _ptr(y), _stream(stream)))
+
+    def min_critical_dt(self, scheme: str = "ExplicitDifference") -> float:
+        dt = C.c_double()
+        check(lib().fx_min_critical_dt(self._h, 1 if scheme == "ExplicitDifference" else 0, C.byref(dt)))
+        return dt.value
+
+    def explicit_run(self, mass, u, vh, a, v, dt, steps, ag=None, direction=0, record_eq=None, stream=None):
+        """`steps` ExplicitDifference steps (explicit_analysis.cpp:62-84, 687-705) with ground
+        acceleration ag[step] (host array) in `direction`; returns the recorded acceleration
+        history of equation record_eq (host) when asked."""
+        agp = None
+        if ag is not None:
+            ag = np.ascontiguousarray(ag, np.float64)
+            agp = ag.ctypes.data_as(L.p_f64)
+        check(lib().fx_explicit_record(self._h, -1 if record_eq is None else int(record_eq), None))
+        fn = lib().fx_explicit_run_f32 if u.dtype.itemsize == 4 else lib().fx_explicit_run
+        check(fn(self._h, _ptr(mass), direction, agp, steps, dt, _ptr(u), _ptr(vh), _ptr(a), _ptr(v),
+                 _stream(stream)))
+        if record_eq is not None:
+            import torch
+            hist = torch.zeros(steps + 1, dtype=torch.float64, device=u.device)
+            torch.cuda.synchronize(u.device)
+            check(lib().fx_explicit_record(self._h, int(record_eq), _ptr(hist)))
+            return hist[:steps].cpu().numpy()
+        return None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().fx_force_destroy(h)
+            self._h = None
+
+
+class MatrixFreeOperator:
+    """exec::MatrixFreeOperator (src/exec/matrix_free_operator.hpp:16-36)."""
+
+    def __init__(self, force: InternalForce, k: OperatorCoefficients = None):
+        self.force = force
+        self.k = k or OperatorCoefficients()
+
+    def set_coefficients(self, k):
+        self.k = k
+
+    @property
+    def rows(self):
+        return self.force.num_equations
+
+    def apply(self, x, y, stream=None):
+        self.force.apply_operator(self.k, x, y, stream)
+
+    def diagonal(self, d, stream=None):
+        self.force.operator_diagonal(self.k, d, stream)
+
+
+# ------------------------------------------------------------------ solvers
+@dataclasses.dataclass
+class SolveOptions:
+    relative_tolerance: float = 1e-10
+    absolute_tolerance: float = 0.0
+    max_iterations: int = 10000
+    lanes: int = 32
+    restart: int = 30
+
+
+@dataclasses.dataclass
+class SolveResult:
+    converged: bool
+    iterations: int
+    rhs_norm: float
+    initial_residual: float
+    final_residual: float
+    indefinite: bool
+    refinements: int = 0
+
+
+class LinearSolver:
+    """solvers::LinearSolver with the Jacobi preconditioner (linear_solver.hpp:96-105)."""
+    METHOD = L.FX_SOLVER_CG
+
+    def __init__(self, options: SolveOptions = None):
+        self.options = options or SolveOptions()
+        self._h = None
+        self.op = None
+
+    def setup(self, op: MatrixFreeOperator, stream=None):
+        o = self.options
+        if self._h is None or self.op is None or self.op.force is not op.force:
+            if self._h is not None:
+                lib().fx_solver_destroy(self._h)
+            h = C.c_void_p()
+            opts = L.fx_solve_opts(o.relative_tolerance, o.absolute_tolerance, o.max_iterations, o.lanes, o.restart, 0)
+            check(lib().fx_solver_create(op.force._h, self.METHOD, opts, C.byref(h)))
+            self._h = h
+        self.op = op
+        check(lib().fx_solver_setup(self._h, op.k.c(), _stream(stream)))
+
+    def solve(self, b, x, stream=None) -> SolveResult:
+        r = L.fx_solve_result()
+        check(lib().fx_solver_solve(self._h, _ptr(b), _ptr(x), C.byref(r), _stream(stream)))
+        return SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual, r.final_residual,
+                           bool(r.indefinite), r.refinements)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().fx_solver_destroy(h)
+            self._h = None
+
+
+class ConjugateGradient(LinearSolver):
+    METHOD = L.FX_SOLVER_CG
+
+
+class Gmres(LinearSolver):
+    METHOD = L.FX_SOLVER_GMRES
+
+
+class KrylovSolver(LinearSolver):
+    METHOD = L.FX_SOLVER_KRYLOV
+
+
+class MixedPrecisionSolver(LinearSolver):
+    """FP32 PCG inside FP64 iterative refinement (box meshes)."""
+    METHOD = L.FX_SOLVER_IR
+
+    def __init__(self, options: SolveOptions = None, inner_tolerance: float = 1e-4):
+        super().__init__(options)
+        self.inner_tolerance = inner_tolerance
+
+    def setup(self, op, stream=None):
+        super().setup(op, stream)
+        check(lib().fx_solver_set_inner_tolerance(self._h, self.inner_tolerance))
+
+
+class VectorOps:
+    """solvers::VectorOps(n, lanes): deterministic dot in the documented order."""
+
+    def __init__(self, n: int, lanes: int = 32, device: int = 0):
+        h = C.c_void_p()
+        check(lib().fx_vops_create(n, lanes, device, C.byref(h)))
+        self._h = h
+
+    def dot(self, x, y, stream=None) -> float:
+        r = C.c_double()
+        check(lib().fx_vops_dot(self._h, _ptr(x), _ptr(y), x.numel(), None, C.byref(r), _stream(stream)))
+        return r.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().fx_vops_destroy(h)
+            self._h = None

@@ -1,0 +1,153 @@
+"""ctypes binding of the C ABI in include/femorax_b200.h (the library built in this folder).
+
+Loading fails loudly when the library is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfemorax_b200.so")
+
+FX_OK = 0
+FX_E_INVALID = 1
+FX_E_UNSUPPORTED = 2
+FX_E_NOMEM = 3
+FX_E_NOT_SPD = 4
+FX_E_DIVERGED = 5
+FX_E_TIMEOUT = 6
+FX_E_CUDA = 7
+
+FX_MAT_ELASTIC = 0
+FX_MAT_J2 = 1
+FX_RENUMBER_OFF = 0
+FX_RENUMBER_RCM = 1
+FX_PATH_AUTO = 0
+FX_PATH_GENERAL = 1
+FX_PATH_BOX = 2
+FX_SOLVER_CG = 0
+FX_SOLVER_GMRES = 1
+FX_SOLVER_KRYLOV = 2
+FX_SOLVER_IR = 3
+
+p_i32 = C.POINTER(C.c_int32)
+p_i64 = C.POINTER(C.c_int64)
+p_f64 = C.POINTER(C.c_double)
+p_i8 = C.POINTER(C.c_int8)
+vp = C.c_void_p
+
+
+class fx_material(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("pad_", C.c_int32), ("E", C.c_double), ("nu", C.c_double),
+                ("rho", C.c_double), ("sigma_y", C.c_double), ("H", C.c_double), ("hk", C.c_double)]
+
+
+class fx_param_set(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("mass_type", C.c_int32), ("E", C.c_double), ("nu", C.c_double),
+                ("rho", C.c_double), ("b", C.c_double * 3), ("alphaM", C.c_double), ("betaK", C.c_double),
+                ("betaKinit", C.c_double), ("betaKcomm", C.c_double), ("sigma_y", C.c_double), ("H", C.c_double),
+                ("hk", C.c_double)]
+
+
+class fx_mesh(C.Structure):
+    _fields_ = [("num_nodes", C.c_int32), ("num_equations", C.c_int32), ("coords", p_f64), ("count", C.c_int32),
+                ("padded", C.c_int32), ("node", p_i32), ("eq", p_i32), ("param", p_i32), ("num_params", C.c_int32),
+                ("pad_", C.c_int32), ("params", C.POINTER(fx_param_set)), ("lumped_mass", p_f64),
+                ("nodal_mass", p_f64), ("nodal_alpha_mass", p_f64), ("eq_dof", p_i8)]
+
+
+class fx_coeffs(C.Structure):
+    _fields_ = [("stiffness", C.c_double), ("damping", C.c_double), ("mass", C.c_double), ("initial", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
+class fx_solve_opts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_iterations", C.c_int32), ("lanes", C.c_int32),
+                ("restart", C.c_int32), ("pad_", C.c_int32)]
+
+
+class fx_solve_result(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("rhs_norm", C.c_double),
+                ("initial_residual", C.c_double), ("final_residual", C.c_double), ("indefinite", C.c_int32),
+                ("status", C.c_int32), ("refinements", C.c_int32), ("pad_", C.c_int32)]
+
+
+# name: (restype, argtypes)
+PROTOTYPES = {
+    "fx_last_error": (C.c_char_p, []),
+    "fx_version": (C.c_char_p, []),
+    "fx_model_create": (C.c_int, [C.c_int32, p_i32, p_f64, C.POINTER(vp)]),
+    "fx_model_destroy": (None, [vp]),
+    "fx_model_add_group": (C.c_int, [vp, C.POINTER(fx_material), p_f64, C.c_int32, C.c_int32, p_i32, p_i32]),
+    "fx_model_add_fix": (C.c_int, [vp, C.c_int32, p_i32, p_i32]),
+    "fx_model_add_equal_dof": (C.c_int, [vp, C.c_int32, p_i32, p_i32, p_i32]),
+    "fx_model_add_rayleigh": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, p_i32]),
+    "fx_model_add_mass": (C.c_int, [vp, C.c_int32, p_i32, p_i32, p_f64]),
+    "fx_compile": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(vp)]),
+    "fx_compiled_destroy": (None, [vp]),
+    "fx_compiled_sizes": (C.c_int, [vp, p_i64]),
+    "fx_compiled_array_i32": (C.c_int64, [vp, C.c_char_p, p_i32]),
+    "fx_compiled_array_f64": (C.c_int64, [vp, C.c_char_p, p_f64]),
+    "fx_compiled_mesh": (C.c_int, [vp, C.POINTER(fx_param_set), C.POINTER(fx_mesh)]),
+    "fx_force_create": (C.c_int, [C.POINTER(fx_mesh), C.c_int32, C.POINTER(vp)]),
+    "fx_force_destroy": (None, [vp]),
+    "fx_force_set_path": (C.c_int, [vp, C.c_int32]),
+    "fx_force_info": (C.c_int, [vp, p_i64]),
+    "fx_apply_operator": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
+    "fx_apply_operator_f32": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
+    "fx_apply_operator_host": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
+    "fx_operator_diagonal": (C.c_int, [vp, fx_coeffs, vp, vp]),
+    "fx_force_compute": (C.c_int, [vp, vp, vp, vp, vp]),
+    "fx_force_compute_f32": (C.c_int, [vp, vp, vp, vp, vp]),
+    "fx_mass_times_ground": (C.c_int, [vp, C.c_int32, vp, vp]),
+    "fx_min_critical_dt": (C.c_int, [vp, C.c_int32, p_f64]),
+    "fx_force_commit": (C.c_int, [vp, vp]),
+    "fx_force_plastic_points": (C.c_int, [vp, p_i64]),
+    "fx_vops_create": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]),
+    "fx_vops_destroy": (None, [vp]),
+    "fx_vops_dot": (C.c_int, [vp, vp, vp, C.c_int64, vp, p_f64, vp]),
+    "fx_axpy": (C.c_int, [C.c_double, vp, vp, C.c_int64, vp]),
+    "fx_xpay": (C.c_int, [vp, C.c_double, vp, C.c_int64, vp]),
+    "fx_multiply": (C.c_int, [vp, vp, vp, C.c_int64, vp]),
+    "fx_solver_create": (C.c_int, [vp, C.c_int32, fx_solve_opts, C.POINTER(vp)]),
+    "fx_solver_destroy": (None, [vp]),
+    "fx_solver_setup": (C.c_int, [vp, fx_coeffs, vp]),
+    "fx_solver_set_inner_tolerance": (C.c_int, [vp, C.c_double]),
+    "fx_solver_solve": (C.c_int, [vp, vp, vp, C.POINTER(fx_solve_result), vp]),
+    "fx_explicit_run": (C.c_int, [vp, vp, C.c_int32, p_f64, C.c_int32, C.c_double, vp, vp, vp, vp, vp]),
+    "fx_explicit_run_f32": (C.c_int, [vp, vp, C.c_int32, p_f64, C.c_int32, C.c_double, vp, vp, vp, vp, vp]),
+    "fx_explicit_record": (C.c_int, [vp, C.c_int32, vp]),
+    "fx_newmark_predict": (C.c_int, [C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, vp]),
+    "fx_newmark_update": (C.c_int, [C.c_int64, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+}
+
+_lib = None
+
+
+class FxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """The loaded library (raises if it is not built: there is no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"femorax_b200: {LIB_PATH} is not built (run `python -m femorax_b200.build`); "
+                               "there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in PROTOTYPES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code != FX_OK:
+        raise FxError(code, lib().fx_last_error().decode())

@@ -1,0 +1,120 @@
+// The device-resident force/operator object behind fx_force (exec::InternalForce's role,
+// src/exec/internal_force.hpp:80-213): every device buffer of one mesh, the execution plans
+// and the work vectors, allocated at creation; applies and solves allocate nothing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "brick_gp.cuh"
+#include "common.cuh"
+
+namespace fx {
+
+// Coefficients of the exact modal element operator of one parameter set on the box grid, for
+// the current operator coefficients (box.cu builds them). Scaled by 1/64 where the two
+// Walsh-Hadamard transforms (unnormalised) would otherwise multiply the result by 64.
+struct BoxCoef {
+  double dkm[3][8];  // modal diagonal: stiffness + consistent mass, per component and mode
+  double kap[12];    // couplings: per axis pair (xy, yz, zx) and r in {0,1}: lambda part, mu part
+  double dm[8];      // force mode, consistent mass: alphaM mass diagonal per mode (on v)
+  double mL;         // lumped-mass factor per corner (nodal space)
+  double beta;       // force mode: stiffness-proportional damping factor (u + beta v)
+  double body[3];    // force mode: body force per corner
+  double pad_;
+};
+static_assert(sizeof(BoxCoef) == 50 * 8, "BoxCoef layout");
+
+struct BoxCoef32 {  // the same in FP32 for the mixed-precision operator
+  float dkm[3][8];
+  float kap[12];
+  float dm[8];
+  float mL, beta, body[3], pad_;
+};
+
+// A structured grid of axis-aligned boxes with equal spacing: (nx, ny, nz) elements.
+struct BoxPlan {
+  bool qualifies = false;
+  std::string why_not;
+  int nx = 0, ny = 0, nz = 0;
+  double h[3] = {0, 0, 0};
+  bool consistent = false;  // every parameter set has the consistent mass (else all lumped)
+  DeviceArray<int32_t> node_eq;     // [(nz+1)(ny+1)(nx+1)]: first free equation | free-DOF mask << 29
+  DeviceArray<int32_t> elem_param;  // [nz ny nx]: parameter set of each element
+  DeviceArray<int32_t> node_of;     // host-side check only: grid node -> internal node
+  std::vector<int32_t> grid_node_h; // grid node -> internal node
+  // Launch shape chosen by the autotuner: block (bx, by) element columns, kz node planes.
+  int variant = 0, kz = 16;
+  bool tuned = false;
+  // coefficient tables for the last operator coefficients
+  DeviceArray<BoxCoef> coef;
+  DeviceArray<BoxCoef32> coef32;
+  double last_k[4] = {-1, -1, -1, -1};
+  int last_mode = -1;
+};
+
+// Buffers of the explicit step loop (ground motion, step counter, force, recorded history),
+// grown on the first run that needs them.
+struct ExplicitWork {
+  DeviceArray<double> ag;
+  DeviceArray<int> step;
+  DeviceArray<double> f64;
+  DeviceArray<float> f32;
+  DeviceArray<double> hist;
+  int32_t record_eq = -1;
+};
+
+struct ForceState {
+  int device = 0;
+  int32_t N = 0, neq = 0, count = 0, P = 0, nparams = 0;
+  std::vector<ParamGP> params_h;
+  std::vector<int32_t> node_h, eq_h, param_h;
+  std::vector<double> coords_h, lumped_h, nodal_mass_h, nodal_alpha_h;
+  std::vector<int8_t> eq_dof_h;
+  DeviceArray<double> coords;
+  DeviceArray<int32_t> node, eq, param;
+  DeviceArray<ParamGP> params;
+  DeviceArray<int32_t> gstart, glist;  // per-equation slot lists in (element, DOF) order
+  DeviceArray<double> slots;           // [24 * P]
+  DeviceArray<double> nodal_mass, nodal_alpha_mass, lumped_mass;
+  DeviceArray<int8_t> eq_dof;
+  bool has_nodal_mass = false, has_nodal_alpha = false;
+  int path = FX_PATH_AUTO;  // requested
+  BoxPlan box;
+  // work vectors (host-buffer apply, solvers)
+  DeviceArray<double> wx, wy;
+  DeviceArray<double> scratch;  // reduction partials and solver scalars
+  int64_t plastic_points = 0;
+  ExplicitWork xw;
+  bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
+  int64_t device_bytes() const;
+};
+
+// general.cu (Gauss-point path, built without fused multiply-adds)
+void general_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st,
+                   const int* skip = nullptr);
+void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st);
+void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
+void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
+
+// box.cu (modal node-owner path)
+void box_build_plan(ForceState& s);
+void box_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st,
+               const int* skip = nullptr);
+void box_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st,
+                   const int* skip = nullptr);
+// Build the box coefficient tables for operator coefficients k now (outside any graph capture).
+void box_prepare(ForceState& s, const double k[3]);
+void box_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
+void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cudaStream_t st);
+int box_num_variants();
+void box_set_launch(ForceState& s, int variant, int kz);
+void box_autotune(ForceState& s, cudaStream_t st);
+
+}  // namespace fx
+
+struct fx_force {
+  fx::ForceState s;
+};

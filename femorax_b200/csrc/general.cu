@@ -1,0 +1,162 @@
+// General execution path: any stdBrick mesh. One thread per element evaluates the element with
+// the Gauss-point physics of brick_gp.cuh and writes its 24 values to its own slots
+// (slots[k * padded + e], coalesced across the warp); a second kernel gives every equation the
+// sum of its slots in (element, DOF) order and adds the nodal-mass terms.
+//
+// This is the reference's deterministic gather scatter (src/exec/assembly.hpp:25-55,
+// assembly.cpp:28-38, pair order internal_force.cpp:121-134). Built with --fmad=false, its sums
+// are the reference host build's sums bit for bit.
+#include "force.hpp"
+
+namespace fx {
+namespace {
+
+constexpr int kBlock = 128;
+
+__device__ __forceinline__ void load_coords(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                            int32_t N, int32_t P, int32_t e, double xl[3][8]) {
+  for (int a = 0; a < 8; ++a) {
+    const int32_t n = node[static_cast<int64_t>(a) * P + e];
+    for (int d = 0; d < 3; ++d) xl[d][a] = coords[static_cast<int64_t>(d) * N + n];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                           const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
+                                                           const ParamGP* __restrict__ params, int32_t N, int32_t P,
+                                                           int32_t count, double ks, double kd, double km, int unit_dir,
+                                                           const double* __restrict__ x, double* __restrict__ slots,
+                                                           const int* skip) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count || (skip && *skip)) return;
+  const ParamGP p = params[param[e]];
+  double xl[3][8], xe[24], ye[24];
+  load_coords(coords, node, N, P, e, xl);
+  for (int a = 0; a < 24; ++a) {
+    const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+    if (unit_dir >= 0) xe[a] = (a % 3) == unit_dir ? 1.0 : 0.0;
+    else xe[a] = q >= 0 ? x[q] : 0.0;
+  }
+  const OpFactors f = op_factors(p, ks, kd, km);
+  element_apply(p, f, xl, xe, ye);
+  for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
+}
+
+__global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                          const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
+                                                          const ParamGP* __restrict__ params, int32_t N, int32_t P,
+                                                          int32_t count, double ks, double kd, double km,
+                                                          double* __restrict__ slots) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const ParamGP p = params[param[e]];
+  double xl[3][8], de[24];
+  int eqe[24];
+  load_coords(coords, node, N, P, e, xl);
+  for (int a = 0; a < 24; ++a) eqe[a] = eq[static_cast<int64_t>(a) * P + e];
+  const OpFactors f = op_factors(p, ks, kd, km);
+  element_diagonal(p, f, xl, eqe, de);
+  for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = de[a];
+}
+
+__global__ void __launch_bounds__(kBlock) k_element_force(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                           const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
+                                                           const ParamGP* __restrict__ params, int32_t N, int32_t P,
+                                                           int32_t count, const double* __restrict__ u,
+                                                           const double* __restrict__ v, double* __restrict__ slots) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const ParamGP p = params[param[e]];
+  double xl[3][8], ue[24], ve[24], fe[24];
+  load_coords(coords, node, N, P, e, xl);
+  for (int a = 0; a < 24; ++a) {
+    const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+    ue[a] = q >= 0 ? u[q] : 0.0;
+    ve[a] = q >= 0 ? v[q] : 0.0;
+  }
+  element_force(p, xl, ue, ve, fe);
+  for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = fe[a];
+}
+
+// y[q] = sum of q's slots in list order, then + c1 m1[q] x1[q] + c2 m2[q] x2[q] (the nodal-mass
+// kernels of internal_force.cpp:368-375, 442-448, same expression, same order).
+__global__ void __launch_bounds__(256) k_gather(const int32_t* __restrict__ start, const int32_t* __restrict__ list,
+                                                 const double* __restrict__ slots, int32_t neq, double c1,
+                                                 const double* __restrict__ m1, const double* __restrict__ x1, double c2,
+                                                 const double* __restrict__ m2, const double* __restrict__ x2,
+                                                 double* __restrict__ y, const int* skip) {
+  const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= neq || (skip && *skip)) return;
+  double sum = 0.0;
+  for (int32_t j = start[q]; j < start[q + 1]; ++j) sum += slots[list[j]];
+  if (m1) sum += c1 * m1[q] * (x1 ? x1[q] : 1.0);
+  if (m2) sum += c2 * m2[q] * (x2 ? x2[q] : 1.0);
+  y[q] = sum;
+}
+
+}  // namespace
+
+void general_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
+  if (s.count > 0)
+    k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                                   s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
+                                                                   -1, x, s.slots.ptr, skip);
+  FX_LAUNCH_CHECK("element_apply");
+  const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
+  const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
+  if (s.neq > 0)
+    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, k[2], m1, x, k[1], m2,
+                                                   x, y, skip);
+  FX_LAUNCH_CHECK("slot_gather");
+}
+
+void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st) {
+  if (s.count > 0)
+    k_element_diag<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                                  s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
+                                                                  s.slots.ptr);
+  FX_LAUNCH_CHECK("element_diagonal");
+  const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
+  const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
+  if (s.neq > 0)
+    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, k[2], m1, nullptr,
+                                                   k[1], m2, nullptr, d, nullptr);
+  FX_LAUNCH_CHECK("slot_gather");
+}
+
+void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
+  if (s.count > 0)
+    k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                                   s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr);
+  FX_LAUNCH_CHECK("element_force");
+  const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
+  if (s.neq > 0)
+    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
+                                                   nullptr, 1.0, m2, v, f, nullptr);
+  FX_LAUNCH_CHECK("slot_gather");
+}
+
+// M r_dir: the operator with k = (0, 0, 1) on the rigid unit translation at every element DOF,
+// then the free nodal masses in that direction (internal_force.cpp:601-626).
+__global__ void k_ground_nodal(const double* __restrict__ nm, const int8_t* __restrict__ dof, int32_t neq, int dir,
+                               double* __restrict__ y) {
+  const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= neq) return;
+  if (dof[q] == dir) y[q] += nm[q];
+}
+
+void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st) {
+  if (s.count > 0)
+    k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                                   s.params.ptr, s.N, s.P, s.count, 0.0, 0.0, 1.0, dir,
+                                                                   nullptr, s.slots.ptr, nullptr);
+  FX_LAUNCH_CHECK("element_apply_unit");
+  if (s.neq > 0)
+    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
+                                                   nullptr, 0.0, nullptr, nullptr, y, nullptr);
+  if (s.has_nodal_mass && s.neq > 0)
+    k_ground_nodal<<<grid_for(s.neq, 256), 256, 0, st>>>(s.nodal_mass.ptr, s.eq_dof.ptr, s.neq, dir, y);
+  FX_LAUNCH_CHECK("ground_mass");
+}
+
+}  // namespace fx

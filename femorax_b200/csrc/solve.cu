@@ -1,0 +1,639 @@
+// Linear solvers on the matrix-free operator (solvers::LinearSolver and its implementations,
+// src/solvers/linear_solver.hpp:96-105, cg.cpp:24-71, gmres.cpp:32-123, krylov.cpp:25-41,
+// jacobi.cpp:10-26), B200-resident.
+//
+// CG keeps its scalars on the device: one iteration is the operator, the p.Ap reduction, a
+// one-thread kernel for alpha, one fused pass that updates x and r and forms the chunk sums of
+// r.r and r.z (z = D^-1 r, never stored), the reduction levels, a one-thread kernel for the
+// convergence test and beta, and the p update. The iterations run as a CUDA graph; the host
+// reads the `done` flag after each block of iterations. Every kernel returns at once when the
+// solve is done, so the iterate is frozen at the converged one. All reductions use the
+// documented chunk/lane order (fused multiply-adds), so a solve gives the same bits every run.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "force.hpp"
+#include "vector.hpp"
+
+// scalar slots of one solve
+enum : int {
+  S_RZ = 0,
+  S_PAP = 1,
+  S_ALPHA = 2,
+  S_BETA = 3,
+  S_RNORM = 4,
+  S_TOL = 5,
+  S_RHS = 6,
+  S_RR = 7,      // r.r of the update kernel (with S_RZNEW contiguous: two columns)
+  S_RZNEW = 8,
+  S_INIT = 9,
+  S_BB = 10,
+  S_NSCALAR = 16
+};
+enum : int { F_DONE = 0, F_CONV = 1, F_INDEF = 2, F_ITERS = 3, F_NFLAG = 4 };
+
+namespace fx {
+namespace {
+
+constexpr int kWarps = 8;
+
+// documented-order chunk sums of x.y for vectors of type T, accumulated in double
+template <class T>
+__global__ void __launch_bounds__(32 * kWarps) k_dot_chunks(const T* __restrict__ x, const T* __restrict__ y, int64_t n,
+                                                            int lanes, int64_t nchunks, double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int64_t begin = c * kChunk;
+  const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
+  double s = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) s = fma(static_cast<double>(x[begin + k]), static_cast<double>(y[begin + k]), s);
+  double total = 0.0;
+  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, s, j);
+  if (lane == 0) out[c] = total;
+}
+
+// r = b - ap; z = inv r; p = z; chunk sums of r.r and r.z (columns 0 and 1 of out)
+template <class T>
+__global__ void __launch_bounds__(32 * kWarps) k_cg_begin(const T* __restrict__ b, const T* __restrict__ ap,
+                                                          const T* __restrict__ inv, T* __restrict__ r,
+                                                          T* __restrict__ p, int64_t n, int lanes, int64_t nchunks,
+                                                          double* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int64_t begin = c * kChunk;
+  const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      const T ri = fma(T(-1), ap[i], b[i]);
+      const T zi = inv[i] * ri;
+      r[i] = ri;
+      p[i] = zi;
+      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+    }
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    out[c] = trr;
+    out[nchunks + c] = trz;
+  }
+}
+
+// x += alpha p; r -= alpha ap; chunk sums of r.r and r.z
+template <class T>
+__global__ void __launch_bounds__(32 * kWarps) k_cg_update(const double* __restrict__ sc, const int* __restrict__ fl,
+                                                           const T* __restrict__ p, const T* __restrict__ ap,
+                                                           const T* __restrict__ inv, T* __restrict__ x,
+                                                           T* __restrict__ r, int64_t n, int lanes, int64_t nchunks,
+                                                           double* __restrict__ out) {
+  if (fl[F_DONE]) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const T alpha = static_cast<T>(sc[S_ALPHA]);
+  const int64_t begin = c * kChunk;
+  const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      x[i] = fma(alpha, p[i], x[i]);
+      const T ri = fma(-alpha, ap[i], r[i]);
+      r[i] = ri;
+      const T zi = inv[i] * ri;
+      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+    }
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    out[c] = trr;
+    out[nchunks + c] = trz;
+  }
+}
+
+template <class T>
+__global__ void k_cg_p(const double* __restrict__ sc, const int* __restrict__ fl, const T* __restrict__ inv,
+                       const T* __restrict__ r, T* __restrict__ p, int64_t n) {
+  if (fl[F_DONE]) return;
+  const T beta = static_cast<T>(sc[S_BETA]);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    p[i] = fma(beta, p[i], inv[i] * r[i]);
+}
+
+__global__ void k_cg_start(double* sc, int* fl, double rtol, double atol, int max_it) {
+  sc[S_RHS] = sqrt(sc[S_BB]);
+  const double rn = sqrt(sc[S_RR]);
+  sc[S_RNORM] = rn;
+  sc[S_INIT] = rn;
+  sc[S_RZ] = sc[S_RZNEW];
+  const double tol = rtol * sc[S_RHS];
+  sc[S_TOL] = tol > atol ? tol : atol;
+  fl[F_ITERS] = 0;
+  fl[F_INDEF] = 0;
+  fl[F_CONV] = rn <= sc[S_TOL];
+  fl[F_DONE] = fl[F_CONV] || max_it <= 0;
+}
+
+__global__ void k_cg_alpha(double* sc, int* fl) {
+  if (fl[F_DONE]) return;
+  const double pap = sc[S_PAP];
+  if (!(pap > 0.0)) {
+    fl[F_INDEF] = 1;
+    fl[F_DONE] = 1;
+    return;
+  }
+  sc[S_ALPHA] = sc[S_RZ] / pap;
+}
+
+__global__ void k_cg_beta(double* sc, int* fl, int max_it) {
+  if (fl[F_DONE]) return;
+  const double rn = sqrt(sc[S_RR]);
+  sc[S_RNORM] = rn;
+  const int it = ++fl[F_ITERS];
+  if (rn <= sc[S_TOL]) {
+    fl[F_CONV] = 1;
+    fl[F_DONE] = 1;
+    return;
+  }
+  if (it >= max_it) {
+    fl[F_DONE] = 1;
+    return;
+  }
+  sc[S_BETA] = sc[S_RZNEW] / sc[S_RZ];
+  sc[S_RZ] = sc[S_RZNEW];
+}
+
+__global__ void k_count_zero(const double* __restrict__ d, int64_t n, int* count) {
+  int local = 0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    local += d[i] == 0.0;
+  if (local) atomicAdd(count, local);
+}
+
+template <class T>
+__global__ void k_reciprocal_t(const double* __restrict__ d, T* __restrict__ y, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = static_cast<T>(1.0 / d[i]);
+}
+
+// IR helpers: r64 = b - ax (FP64), r32 = (float) r64, x += (double) d32
+__global__ void k_residual64(const double* __restrict__ b, const double* __restrict__ ax, double* __restrict__ r,
+                             int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    r[i] = b[i] - ax[i];
+}
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    b[i] = static_cast<float>(a[i]);
+}
+__global__ void k_add_f32(const float* __restrict__ d, double* __restrict__ x, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] += static_cast<double>(d[i]);
+}
+__global__ void k_zero_f32(float* __restrict__ x, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] = 0.f;
+}
+
+unsigned ew(int64_t n) {
+  const int64_t blocks = (n + 255) / 256;
+  const int64_t cap = static_cast<int64_t>(num_sms()) * 8;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min(blocks, cap)));
+}
+unsigned chunk_grid(int64_t nchunks) { return static_cast<unsigned>((nchunks + kWarps - 1) / kWarps); }
+
+}  // namespace
+
+// ------------------------------------------------------------------ the solver object
+struct Solver {
+  fx_force* f = nullptr;
+  int method = FX_SOLVER_CG;
+  fx_solve_opts o{};
+  double inner_rtol = 1e-4;
+  double k[3] = {1, 0, 0};
+  bool ready = false;
+  int64_t n = 0;
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  ReduceWork w;
+  DeviceArray<double> diag, inv, r, p, ap, x0;
+  DeviceArray<float> inv32, r32, p32, ap32, d32;
+  DeviceArray<double> sc;
+  DeviceArray<int> fl;
+  DeviceArray<int> zero_count;
+  DeviceArray<double> V, Z, wv, hbuf;  // GMRES
+  int* host_flags = nullptr;           // pinned
+  double* host_sc = nullptr;           // pinned
+  ~Solver() {
+    if (cs) cudaStreamDestroy(cs);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (host_flags) cudaFreeHost(host_flags);
+    if (host_sc) cudaFreeHost(host_sc);
+  }
+
+  void apply64(const double* x, double* y, const int* skip) {
+    if (f->s.use_box()) box_apply(f->s, k, x, y, cs, skip);
+    else general_apply(f->s, k, x, y, cs, skip);
+  }
+  void apply32(const float* x, float* y, const int* skip) { box_apply_f32(f->s, k, x, y, cs, skip); }
+
+  void read_state() {
+    FX_CUDA(cudaMemcpyAsync(host_flags, fl.ptr, sizeof(int) * F_NFLAG, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaMemcpyAsync(host_sc, sc.ptr, sizeof(double) * S_NSCALAR, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+  }
+
+  // Jacobi-PCG on vectors of type T (double: the plain solve; float: the inner solve of IR).
+  template <class T>
+  void cg(const T* b, T* x, T* rr, T* pp, T* aa, const T* iv, double rtol, double atol, int max_it, fx_solve_result* res) {
+    const int lanes = o.lanes;
+    const int64_t nc = chunks_of(n);
+    auto apply = [&](const T* xin, T* yout, const int* skip) {
+      if constexpr (sizeof(T) == 8) apply64(xin, yout, skip);
+      else apply32(xin, yout, skip);
+    };
+    // b.b, r = b - A x, r.r, r.z, p = z
+    k_dot_chunks<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(b, b, n, lanes, nc, w.level[0].ptr);
+    FX_LAUNCH_CHECK("cg_bb");
+    reduce_partials(w, nc, 1, sc.ptr + S_BB, cs);
+    apply(x, aa, nullptr);
+    k_cg_begin<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(b, aa, iv, rr, pp, n, lanes, nc, w.level[0].ptr);
+    FX_LAUNCH_CHECK("cg_begin");
+    reduce_partials(w, nc, 2, sc.ptr + S_RR, cs);
+    k_cg_start<<<1, 1, 0, cs>>>(sc.ptr, fl.ptr, rtol, atol, max_it);
+    FX_LAUNCH_CHECK("cg_start");
+    auto iteration = [&] {
+      apply(pp, aa, fl.ptr + F_DONE);
+      k_dot_chunks<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(pp, aa, n, lanes, nc, w.level[0].ptr);
+      reduce_partials(w, nc, 1, sc.ptr + S_PAP, cs);
+      k_cg_alpha<<<1, 1, 0, cs>>>(sc.ptr, fl.ptr);
+      k_cg_update<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, pp, aa, iv, x, rr, n, lanes, nc,
+                                                            w.level[0].ptr);
+      reduce_partials(w, nc, 2, sc.ptr + S_RR, cs);
+      k_cg_beta<<<1, 1, 0, cs>>>(sc.ptr, fl.ptr, max_it);
+      k_cg_p<T><<<ew(n), 256, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, pp, n);
+      FX_LAUNCH_CHECK("cg_iteration");
+    };
+    // the first block without a graph (it also builds any lazy state), then graphs of `block`
+    const int block = 8;
+    for (int i = 0; i < block; ++i) iteration();
+    read_state();
+    cudaGraphExec_t exec = nullptr;
+    while (!host_flags[F_DONE]) {
+      if (!exec) {
+        cudaGraph_t graph = nullptr;
+        FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int i = 0; i < block; ++i) iteration();
+        } catch (...) {
+          cudaStreamEndCapture(cs, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        FX_CUDA(cudaStreamEndCapture(cs, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        FX_CUDA(e);
+      }
+      FX_CUDA(cudaGraphLaunch(exec, cs));
+      read_state();
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    res->converged = host_flags[F_CONV];
+    res->iterations = host_flags[F_ITERS];
+    res->indefinite = host_flags[F_INDEF];
+    res->rhs_norm = host_sc[S_RHS];
+    res->initial_residual = host_sc[S_INIT];
+    res->final_residual = host_sc[S_RNORM];
+  }
+
+  void gmres(const double* b, double* x, fx_solve_result* res);
+  void ir(const double* b, double* x, fx_solve_result* res);
+};
+
+// FGMRES(m) with CGS2, host-side Hessenberg and Givens rotations, as gmres.cpp:32-123.
+void Solver::gmres(const double* b, double* x, fx_solve_result* res) {
+  const int m = std::max(1, std::min(o.restart, 63));
+  const int64_t ld = n;
+  std::vector<double> H(static_cast<size_t>((m + 1) * m)), cs_(m), sn(m), g(m + 1), h(m + 1), h2(m + 1), y(m);
+  auto Hij = [&](int i, int j) -> double& { return H[static_cast<size_t>(j * (m + 1) + i)]; };
+  auto dot_host = [&](const double* a, const double* c) {
+    dot_device(w, a, c, n, sc.ptr + S_PAP, cs);
+    FX_CUDA(cudaMemcpyAsync(host_sc, sc.ptr + S_PAP, sizeof(double), cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+    return host_sc[0];
+  };
+  auto dots_host = [&](int kk, const double* wvec, std::vector<double>& out) {
+    multi_dot_device(w, V.ptr, ld, kk, wvec, n, hbuf.ptr, cs);
+    FX_CUDA(cudaMemcpyAsync(out.data(), hbuf.ptr, sizeof(double) * kk, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+  };
+  auto combine = [&](const double* M, int kk, const std::vector<double>& coef, double a, double* wvec) {
+    for (int c = 0; c < kk; ++c) axpy(a * coef[c], M + static_cast<int64_t>(c) * ld, wvec, n, cs);
+  };
+  res->rhs_norm = std::sqrt(dot_host(b, b));
+  const double tol = std::max(o.rtol * res->rhs_norm, o.atol);
+  bool first = true;
+  int iterations = 0;
+  for (;;) {
+    apply64(x, wv.ptr, nullptr);
+    FX_CUDA(cudaMemcpyAsync(r.ptr, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs));
+    axpy(-1.0, wv.ptr, r.ptr, n, cs);
+    const double beta = std::sqrt(dot_host(r.ptr, r.ptr));
+    if (first) res->initial_residual = beta;
+    first = false;
+    res->final_residual = beta;
+    if (beta <= tol) {
+      res->converged = 1;
+      break;
+    }
+    if (iterations >= o.max_iterations) break;
+    fill(V.ptr, 0.0, n, cs);
+    axpy(1.0 / beta, r.ptr, V.ptr, n, cs);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    for (; j < m && iterations < o.max_iterations; ++j) {
+      double* vj = V.ptr + static_cast<int64_t>(j) * ld;
+      double* zj = Z.ptr + static_cast<int64_t>(j) * ld;
+      multiply(inv.ptr, vj, zj, n, cs);
+      apply64(zj, wv.ptr, nullptr);
+      dots_host(j + 1, wv.ptr, h);
+      combine(V.ptr, j + 1, h, -1.0, wv.ptr);
+      dots_host(j + 1, wv.ptr, h2);
+      combine(V.ptr, j + 1, h2, -1.0, wv.ptr);
+      for (int i = 0; i <= j; ++i) Hij(i, j) = h[i] + h2[i];
+      const double hn = std::sqrt(dot_host(wv.ptr, wv.ptr));
+      Hij(j + 1, j) = hn;
+      if (hn > 0.0) {
+        double* vn = V.ptr + static_cast<int64_t>(j + 1) * ld;
+        fill(vn, 0.0, n, cs);
+        axpy(1.0 / hn, wv.ptr, vn, n, cs);
+      }
+      for (int i = 0; i < j; ++i) {
+        const double a = Hij(i, j), c = Hij(i + 1, j);
+        Hij(i, j) = cs_[i] * a + sn[i] * c;
+        Hij(i + 1, j) = -sn[i] * a + cs_[i] * c;
+      }
+      const double a = Hij(j, j), c = Hij(j + 1, j);
+      const double d = std::hypot(a, c);
+      cs_[j] = d > 0.0 ? a / d : 1.0;
+      sn[j] = d > 0.0 ? c / d : 0.0;
+      Hij(j, j) = d;
+      Hij(j + 1, j) = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs_[j] * g[j];
+      ++iterations;
+      res->final_residual = std::abs(g[j + 1]);
+      if (res->final_residual <= tol || hn == 0.0) {
+        ++j;
+        break;
+      }
+    }
+    for (int i = j - 1; i >= 0; --i) {
+      double s = g[i];
+      for (int kk = i + 1; kk < j; ++kk) s -= Hij(i, kk) * y[kk];
+      y[i] = s / Hij(i, i);
+    }
+    combine(Z.ptr, j, y, 1.0, x);
+    if (res->final_residual <= tol) {
+      apply64(x, wv.ptr, nullptr);
+      FX_CUDA(cudaMemcpyAsync(r.ptr, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs));
+      axpy(-1.0, wv.ptr, r.ptr, n, cs);
+      res->final_residual = std::sqrt(dot_host(r.ptr, r.ptr));
+      if (res->final_residual <= tol) {
+        res->converged = 1;
+        break;
+      }
+    }
+    if (iterations >= o.max_iterations) break;
+  }
+  res->iterations = iterations;
+}
+
+// FP32 PCG inside FP64 iterative refinement.
+void Solver::ir(const double* b, double* x, fx_solve_result* res) {
+  res->rhs_norm = -1.0;
+  int outer = 0, inner_total = 0;
+  double bnorm = 0.0;
+  const int max_outer = 50;
+  for (;;) {
+    apply64(x, ap.ptr, nullptr);
+    k_residual64<<<ew(n), 256, 0, cs>>>(b, ap.ptr, r.ptr, n);
+    FX_LAUNCH_CHECK("ir_residual");
+    if (outer == 0) {
+      dot_device(w, b, b, n, sc.ptr + S_BB, cs);
+    }
+    dot_device(w, r.ptr, r.ptr, n, sc.ptr + S_RR, cs);
+    FX_CUDA(cudaMemcpyAsync(host_sc, sc.ptr, sizeof(double) * S_NSCALAR, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+    if (outer == 0) {
+      bnorm = std::sqrt(host_sc[S_BB]);
+      res->rhs_norm = bnorm;
+    }
+    const double rn = std::sqrt(host_sc[S_RR]);
+    if (outer == 0) res->initial_residual = rn;
+    res->final_residual = rn;
+    if (rn <= std::max(o.rtol * bnorm, o.atol)) {
+      res->converged = 1;
+      break;
+    }
+    if (outer >= max_outer || inner_total >= o.max_iterations) break;
+    // inner: K d = r in FP32 from d = 0
+    k_to_f32<<<ew(n), 256, 0, cs>>>(r.ptr, r32.ptr, n);
+    k_zero_f32<<<ew(n), 256, 0, cs>>>(d32.ptr, n);
+    FX_LAUNCH_CHECK("ir_inner_setup");
+    fx_solve_result ri{};
+    // the FP32 rhs lives in r32; the CG residual vector needs its own buffer: reuse x0 as FP32 storage
+    float* rr32 = reinterpret_cast<float*>(x0.ptr);
+    cg<float>(r32.ptr, d32.ptr, rr32, p32.ptr, ap32.ptr, inv32.ptr, inner_rtol, 0.0, o.max_iterations - inner_total, &ri);
+    inner_total += ri.iterations;
+    k_add_f32<<<ew(n), 256, 0, cs>>>(d32.ptr, x, n);
+    FX_LAUNCH_CHECK("ir_correct");
+    ++outer;
+    if (ri.iterations == 0 && !ri.converged) break;
+  }
+  res->iterations = inner_total;
+  res->refinements = outer;
+}
+
+}  // namespace fx
+
+struct fx_solver {
+  fx::Solver s;
+};
+
+namespace {
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return FX_OK;
+  } catch (const fx::Error& e) {
+    fx::set_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    fx::set_error(e.what());
+    return FX_E_INVALID;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fx_solver_create(fx_force* f, int32_t method, fx_solve_opts o, fx_solver** out) {
+  return guard([&] {
+    if (!f || !out) throw fx::Error(FX_E_INVALID, "fx_solver_create: bad arguments");
+    if (method < FX_SOLVER_CG || method > FX_SOLVER_IR) throw fx::Error(FX_E_INVALID, "fx_solver_create: unknown method");
+    if (method == FX_SOLVER_IR && !f->s.use_box())
+      throw fx::Error(FX_E_UNSUPPORTED, "the FP32 inner solve runs on the box path only: " + f->s.box.why_not);
+    if (o.lanes <= 0) o.lanes = 32;
+    if (o.lanes > 32) throw fx::Error(FX_E_INVALID, "lanes must be in 1..32");
+    if (o.restart <= 0) o.restart = 30;
+    if (o.max_iterations < 0) throw fx::Error(FX_E_INVALID, "max_iterations must be >= 0");
+    FX_CUDA(cudaSetDevice(f->s.device));
+    auto* h = new fx_solver;
+    fx::Solver& s = h->s;
+    try {
+      s.f = f;
+      s.method = method;
+      s.o = o;
+      s.n = f->s.neq;
+      const size_t n = static_cast<size_t>(std::max<int64_t>(s.n, 1));
+      FX_CUDA(cudaStreamCreateWithFlags(&s.cs, cudaStreamNonBlocking));
+      FX_CUDA(cudaEventCreateWithFlags(&s.ev_in, cudaEventDisableTiming));
+      FX_CUDA(cudaEventCreateWithFlags(&s.ev_out, cudaEventDisableTiming));
+      FX_CUDA(cudaMallocHost(&s.host_flags, sizeof(int) * F_NFLAG));
+      FX_CUDA(cudaMallocHost(&s.host_sc, sizeof(double) * S_NSCALAR));
+      s.w.init(std::max<int64_t>(s.n, 1), o.lanes);
+      s.diag.alloc(n);
+      s.inv.alloc(n);
+      s.r.alloc(n);
+      s.p.alloc(n);
+      s.ap.alloc(n);
+      s.x0.alloc(n);
+      s.sc.alloc(S_NSCALAR);
+      s.fl.alloc(F_NFLAG);
+      s.zero_count.alloc(1);
+      s.hbuf.alloc(64);
+      if (method == FX_SOLVER_GMRES || method == FX_SOLVER_KRYLOV) {
+        const int m = std::max(1, std::min(o.restart, 63));
+        s.V.alloc(n * static_cast<size_t>(m + 1));
+        s.Z.alloc(n * static_cast<size_t>(m));
+        s.wv.alloc(n);
+      }
+      if (method == FX_SOLVER_IR) {
+        s.inv32.alloc(n);
+        s.r32.alloc(n);
+        s.p32.alloc(n);
+        s.ap32.alloc(n);
+        s.d32.alloc(n);
+      }
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+void fx_solver_destroy(fx_solver* s) { delete s; }
+
+int fx_solver_set_inner_tolerance(fx_solver* s, double inner_rtol) {
+  return guard([&] {
+    if (!s || !(inner_rtol > 0.0 && inner_rtol < 1.0)) throw fx::Error(FX_E_INVALID, "inner tolerance must be in (0, 1)");
+    s->s.inner_rtol = inner_rtol;
+  });
+}
+
+int fx_solver_setup(fx_solver* h, fx_coeffs k, void* stream) {
+  return guard([&] {
+    if (!h) throw fx::Error(FX_E_INVALID, "fx_solver_setup: null handle");
+    fx::Solver& s = h->s;
+    auto st = static_cast<cudaStream_t>(stream);
+    s.k[0] = k.stiffness;
+    s.k[1] = k.damping;
+    s.k[2] = k.mass;
+    if (s.n > 0) {
+      fx::general_diagonal(s.f->s, s.k, s.diag.ptr, st);
+      FX_CUDA(cudaMemsetAsync(s.zero_count.ptr, 0, sizeof(int), st));
+      fx::k_count_zero<<<fx::ew(s.n), 256, 0, st>>>(s.diag.ptr, s.n, s.zero_count.ptr);
+      int zeros = 0;
+      FX_CUDA(cudaMemcpyAsync(&zeros, s.zero_count.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+      FX_CUDA(cudaStreamSynchronize(st));
+      if (zeros > 0) throw fx::Error(FX_E_INVALID, "Jacobi: " + std::to_string(zeros) + " zero diagonal entries");
+      fx::k_reciprocal_t<double><<<fx::ew(s.n), 256, 0, st>>>(s.diag.ptr, s.inv.ptr, s.n);
+      if (s.method == FX_SOLVER_IR) fx::k_reciprocal_t<float><<<fx::ew(s.n), 256, 0, st>>>(s.diag.ptr, s.inv32.ptr, s.n);
+      FX_LAUNCH_CHECK("jacobi_setup");
+      if (s.f->s.use_box()) fx::box_prepare(s.f->s, s.k);
+      FX_CUDA(cudaStreamSynchronize(st));
+    }
+    s.ready = true;
+  });
+}
+
+int fx_solver_solve(fx_solver* h, const double* b, double* x, fx_solve_result* r, void* stream) {
+  return guard([&] {
+    if (!h || !r || (h->s.n > 0 && (!b || !x))) throw fx::Error(FX_E_INVALID, "fx_solver_solve: bad arguments");
+    fx::Solver& s = h->s;
+    if (!s.ready) throw fx::Error(FX_E_INVALID, "fx_solver_solve: call fx_solver_setup first");
+    *r = fx_solve_result{};
+    if (s.n == 0) {
+      r->converged = 1;
+      return;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    FX_CUDA(cudaEventRecord(s.ev_in, st));
+    FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
+    switch (s.method) {
+      case FX_SOLVER_CG:
+        s.cg<double>(b, x, s.r.ptr, s.p.ptr, s.ap.ptr, s.inv.ptr, s.o.rtol, s.o.atol, s.o.max_iterations, r);
+        break;
+      case FX_SOLVER_GMRES:
+        s.gmres(b, x, r);
+        break;
+      case FX_SOLVER_KRYLOV: {
+        FX_CUDA(cudaMemcpyAsync(s.x0.ptr, x, sizeof(double) * s.n, cudaMemcpyDeviceToDevice, s.cs));
+        s.cg<double>(b, x, s.r.ptr, s.p.ptr, s.ap.ptr, s.inv.ptr, s.o.rtol, s.o.atol, s.o.max_iterations, r);
+        if (r->indefinite) {
+          const int cg_it = r->iterations;
+          FX_CUDA(cudaMemcpyAsync(x, s.x0.ptr, sizeof(double) * s.n, cudaMemcpyDeviceToDevice, s.cs));
+          *r = fx_solve_result{};
+          s.gmres(b, x, r);
+          r->iterations += cg_it;
+          r->indefinite = 1;
+        }
+        break;
+      }
+      case FX_SOLVER_IR:
+        s.ir(b, x, r);
+        break;
+    }
+    FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
+    FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
+    r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);
+  });
+}
+
+}  // extern "C"

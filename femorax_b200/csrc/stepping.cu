@@ -1,0 +1,346 @@
+// Time stepping: the ExplicitDifference step loop and the Newmark form-D kernels
+// (src/exec/explicit_analysis.cpp:62-84, 687-705; src/exec/implicit_stage.cpp:29-68), and the
+// stable time step (StdBrick::critical_dt, std_brick.hpp:629-694; stable_dt,
+// src/physics/explicit_stability.hpp:16-32).
+//
+// One ExplicitDifference step is two launches: the force at (u, vh), then one fused pass that
+// does the correction of this step and the prediction of the next (a = (-f + g)/m,
+// v = vh + dt/8 (3a + a_old), vh += dt a, u += dt vh). The prediction only needs the corrected
+// acceleration, so moving it into the correction pass changes no value. The steps run as a
+// CUDA graph of a block of steps; the ground acceleration of each step is read from a device
+// array indexed by a device step counter, so one captured graph serves every block.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "force.hpp"
+
+namespace fx {
+namespace {
+
+template <class T>
+__global__ void k_ed_predict(T* __restrict__ u, T* __restrict__ vh, const T* __restrict__ a, T dt, int64_t n) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const T v = vh[q] + a[q] * dt;
+    vh[q] = v;
+    u[q] = u[q] + v * dt;
+  }
+}
+
+// correction of step `step` and prediction of step `step + 1`
+template <class T>
+__global__ void k_ed_correct_predict(const T* __restrict__ f, const T* __restrict__ m, const int8_t* __restrict__ dof,
+                                     const double* __restrict__ ag, int* __restrict__ step, int dir, T dt,
+                                     T* __restrict__ u, T* __restrict__ vh, T* __restrict__ a, T* __restrict__ v,
+                                     int64_t n, int32_t record_eq, double* __restrict__ hist, int predict) {
+  const int s = *step;
+  const T g = ag ? static_cast<T>(ag[s]) : T(0);
+  const T halfT = dt * T(0.125);
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const T mq = m[q];
+    T gl = T(0);
+    if (ag && dof[q] == dir) gl = -(mq * g);
+    const T R = -f[q] + gl;
+    const T an = R / mq;
+    const T t = T(3) * an + a[q];
+    const T vhq = vh[q];
+    v[q] = vhq + t * halfT;
+    a[q] = an;
+    if (q == record_eq && hist) hist[s] = static_cast<double>(an);
+    if (predict) {
+      const T vn = vhq + an * dt;
+      vh[q] = vn;
+      u[q] = u[q] + vn * dt;
+    }
+  }
+}
+
+__global__ void k_step_advance(int* step) { ++*step; }
+
+__global__ void k_newmark_predict(double* __restrict__ u, double* __restrict__ v, double* __restrict__ a,
+                                  double* __restrict__ ut, double* __restrict__ vt, double* __restrict__ at, double a1,
+                                  double a2, double a3, double a4, int64_t n) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    ut[q] = u[q];
+    vt[q] = v[q];
+    at[q] = a[q];
+    v[q] = v[q] * a1 + at[q] * a2;
+    a[q] = a[q] * a4 + vt[q] * a3;
+  }
+}
+
+__global__ void k_newmark_update(const double* __restrict__ du, double* __restrict__ u, double* __restrict__ v,
+                                 double* __restrict__ a, double c2, double c3, int64_t n) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    u[q] += du[q];
+    v[q] += du[q] * c2;
+    a[q] += du[q] * c3;
+  }
+}
+
+unsigned ew(int64_t n) {
+  const int64_t blocks = (n + 255) / 256;
+  const int64_t cap = static_cast<int64_t>(num_sms()) * 8;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min(blocks, cap)));
+}
+
+// Cyclic Jacobi largest eigenvalue of a symmetric 24 x 24 matrix (Golub and Van Loan, Algorithm
+// 8.4.1, the rotation the reference's sym_eigen.hpp uses).
+double max_eig24(double A[24][24]) {
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0, dg = 0.0;
+    for (int i = 0; i < 24; ++i) {
+      dg += A[i][i] * A[i][i];
+      for (int j = i + 1; j < 24; ++j) off += A[i][j] * A[i][j];
+    }
+    if (off <= 1e-30 * dg || off == 0.0) break;
+    for (int p = 0; p < 23; ++p)
+      for (int q = p + 1; q < 24; ++q) {
+        const double apq = A[p][q];
+        if (apq == 0.0) continue;
+        const double th = (A[q][q] - A[p][p]) / (2.0 * apq);
+        const double t = (th >= 0.0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 24; ++k) {
+          const double akp = A[k][p], akq = A[k][q];
+          A[k][p] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 24; ++k) {
+          const double apk = A[p][k], aqk = A[q][k];
+          A[p][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+        A[p][q] = A[q][p] = 0.0;
+      }
+  }
+  double l = A[0][0];
+  for (int i = 1; i < 24; ++i) l = std::max(l, A[i][i]);
+  return l;
+}
+
+// omega^2 of one element: K with the elastic tangent, lumped mass (std_brick.hpp:658-688).
+double element_omega_sq(const ParamGP& p, const double xl[3][8]) {
+  double m[8];
+  lumped_mass(p, xl, m);
+  double D[6][6];
+  elastic_D(p, D);
+  double A[24][24];
+  for (int a = 0; a < 24; ++a)
+    for (int c = 0; c < 24; ++c) A[a][c] = 0.0;
+  for (int gp = 0; gp < 8; ++gp) {
+    PointShape s;
+    point_shape(xl, gp, s);
+    for (int j = 0; j < 8; ++j)
+      for (int k = 0; k < 8; ++k) {
+        double blk[3][3];
+        block_tangent(s, D, j, k, blk);
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) A[3 * j + a][3 * k + c] += blk[a][c];
+      }
+  }
+  double ism[8];
+  for (int j = 0; j < 8; ++j) {
+    if (!(m[j] > 0.0)) return 0.0;
+    ism[j] = 1.0 / std::sqrt(m[j]);
+  }
+  for (int a = 0; a < 24; ++a)
+    for (int c = 0; c < 24; ++c) A[a][c] *= ism[a / 3] * ism[c / 3];
+  return max_eig24(A);
+}
+
+double stable_dt(int scheme, const ParamGP& p, double w2) {
+  if (!(w2 > 0.0)) return INFINITY;
+  const double w = std::sqrt(w2);
+  if (scheme == 0) return 2.0 / w;
+  const double beta = p.betaK + p.betaKinit + p.betaKcomm;
+  const double c = p.alphaM + beta * w2;
+  return 4.0 / (std::sqrt(c * c + 4.0 * w2) + c);
+}
+
+}  // namespace
+
+}  // namespace fx
+
+namespace {
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return FX_OK;
+  } catch (const fx::Error& e) {
+    fx::set_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    fx::set_error(e.what());
+    return FX_E_INVALID;
+  }
+}
+
+fx::ExplicitWork& work_of(fx_force* f) { return f->s.xw; }
+
+template <class T>
+void explicit_run(fx_force* f, const T* mass, int32_t dir, const double* ag_host, int32_t steps, double dt, T* u,
+                  T* vh, T* a, T* v, cudaStream_t st) {
+  using namespace fx;
+  ForceState& s = f->s;
+  if (steps < 0 || !(dt > 0.0)) throw Error(FX_E_INVALID, "fx_explicit_run: steps >= 0 and dt > 0 required");
+  if (ag_host && (dir < 0 || dir > 2)) throw Error(FX_E_INVALID, "fx_explicit_run: dir must be 0, 1 or 2");
+  if (sizeof(T) == 4 && !s.use_box()) throw Error(FX_E_UNSUPPORTED, "the FP32 explicit step runs on the box path only");
+  ExplicitWork& w = work_of(f);
+  const int64_t n = s.neq;
+  if (w.step.n == 0) w.step.alloc(1);
+  if (ag_host) {
+    if (w.ag.n < static_cast<size_t>(steps) + 1) w.ag.alloc(static_cast<size_t>(steps) + 1);
+    FX_CUDA(cudaMemcpyAsync(w.ag.ptr, ag_host, sizeof(double) * steps, cudaMemcpyHostToDevice, st));
+  }
+  if (w.record_eq >= 0 && w.hist.n < static_cast<size_t>(steps) + 1) w.hist.alloc(static_cast<size_t>(steps) + 1);
+  T* fbuf;
+  if constexpr (sizeof(T) == 8) {
+    if (w.f64.n < static_cast<size_t>(n)) w.f64.alloc(static_cast<size_t>(std::max<int64_t>(n, 1)));
+    fbuf = w.f64.ptr;
+  } else {
+    if (w.f32.n < static_cast<size_t>(n)) w.f32.alloc(static_cast<size_t>(std::max<int64_t>(n, 1)));
+    fbuf = w.f32.ptr;
+  }
+  FX_CUDA(cudaMemsetAsync(w.step.ptr, 0, sizeof(int), st));
+  if (steps == 0) return;
+  const T tdt = static_cast<T>(dt);
+  k_ed_predict<T><<<ew(n), 256, 0, st>>>(u, vh, a, tdt, n);
+  FX_LAUNCH_CHECK("ed_predict");
+  const double* agp = ag_host ? w.ag.ptr : nullptr;
+  auto one_step = [&](int predict) {
+    if constexpr (sizeof(T) == 8) {
+      if (s.use_box()) box_force(s, u, vh, fbuf, st);
+      else general_force(s, u, vh, fbuf, st);
+    } else {
+      box_force_f32(s, u, vh, fbuf, st);
+    }
+    k_ed_correct_predict<T><<<ew(n), 256, 0, st>>>(fbuf, mass, s.eq_dof.ptr, agp, w.step.ptr, dir, tdt, u, vh, a, v, n,
+                                                   w.record_eq, w.hist.ptr, predict);
+    k_step_advance<<<1, 1, 0, st>>>(w.step.ptr);
+    FX_LAUNCH_CHECK("ed_step");
+  };
+  // first step eagerly (coefficient tables, attributes), then graphs of `block` steps
+  const int block = 16;
+  int done = 0;
+  one_step(steps > 1);
+  ++done;
+  cudaStream_t cs = st;
+  bool own_stream = false;
+  if (cs == nullptr) {  // the legacy stream cannot be captured: run the graph on a private stream
+    FX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    own_stream = true;
+    cudaEvent_t e;
+    FX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    FX_CUDA(cudaEventRecord(e, st));
+    FX_CUDA(cudaStreamWaitEvent(cs, e, 0));
+    cudaEventDestroy(e);
+  }
+  st = cs;
+  cudaGraphExec_t exec = nullptr;
+  while (done < steps) {
+    const int left = steps - done;
+    if (left > block) {
+      if (!exec) {
+        cudaGraph_t g = nullptr;
+        FX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < block; ++i) one_step(1);
+        FX_CUDA(cudaStreamEndCapture(st, &g));
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        FX_CUDA(e);
+      }
+      FX_CUDA(cudaGraphLaunch(exec, st));
+      done += block;
+    } else {
+      one_step(left > 1);
+      ++done;
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (own_stream) {
+    FX_CUDA(cudaStreamSynchronize(cs));
+    cudaStreamDestroy(cs);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fx_explicit_run(fx_force* f, const double* mass, int32_t dir, const double* ag_host, int32_t steps, double dt,
+                    double* u, double* vh, double* a, double* v, void* stream) {
+  return guard([&] {
+    if (!f || (f->s.neq > 0 && (!mass || !u || !vh || !a || !v))) throw fx::Error(FX_E_INVALID, "fx_explicit_run: bad arguments");
+    explicit_run<double>(f, mass, dir, ag_host, steps, dt, u, vh, a, v, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fx_explicit_run_f32(fx_force* f, const float* mass, int32_t dir, const double* ag_host, int32_t steps, double dt,
+                        float* u, float* vh, float* a, float* v, void* stream) {
+  return guard([&] {
+    if (!f || (f->s.neq > 0 && (!mass || !u || !vh || !a || !v)))
+      throw fx::Error(FX_E_INVALID, "fx_explicit_run_f32: bad arguments");
+    explicit_run<float>(f, mass, dir, ag_host, steps, dt, u, vh, a, v, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev) {
+  return guard([&] {
+    if (!f || eq >= f->s.neq) throw fx::Error(FX_E_INVALID, "fx_explicit_record: bad arguments");
+    fx::ExplicitWork& w = work_of(f);
+    if (hist_dev == nullptr) {
+      w.record_eq = eq;
+      return;
+    }
+    if (w.hist.n == 0) throw fx::Error(FX_E_INVALID, "fx_explicit_record: nothing recorded");
+    FX_CUDA(cudaMemcpy(hist_dev, w.hist.ptr, w.hist.bytes(), cudaMemcpyDeviceToDevice));
+  });
+}
+
+int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
+                       double a2, double a3, double a4, void* stream) {
+  return guard([&] {
+    if (n <= 0) return;
+    fx::k_newmark_predict<<<fx::ew(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(u, v, a, ut, vt, at, a1, a2, a3, a4, n);
+    FX_LAUNCH_CHECK("newmark_predict");
+  });
+}
+
+int fx_newmark_update(int64_t n, const double* du, double* u, double* v, double* a, double c2, double c3,
+                      void* stream) {
+  return guard([&] {
+    if (n <= 0) return;
+    fx::k_newmark_update<<<fx::ew(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(du, u, v, a, c2, c3, n);
+    FX_LAUNCH_CHECK("newmark_update");
+  });
+}
+
+int fx_min_critical_dt(fx_force* f, int32_t scheme, double* dt) {
+  return guard([&] {
+    if (!f || !dt || (scheme != 0 && scheme != 1)) throw fx::Error(FX_E_INVALID, "fx_min_critical_dt: bad arguments");
+    const fx::ForceState& s = f->s;
+    double best = 1e300;
+    // elements of one parameter set on a box grid are congruent: one eigenproblem per set
+    std::vector<char> seen(static_cast<size_t>(s.nparams), 0);
+    for (int32_t e = 0; e < s.count; ++e) {
+      const int32_t pi = s.param_h[e];
+      if (s.box.qualifies && seen[pi]) continue;
+      seen[pi] = 1;
+      double xl[3][8];
+      for (int a = 0; a < 8; ++a) {
+        const int32_t nd = s.node_h[static_cast<size_t>(a) * s.P + e];
+        for (int d = 0; d < 3; ++d) xl[d][a] = s.coords_h[static_cast<size_t>(d) * s.N + nd];
+      }
+      const fx::ParamGP& p = s.params_h[pi];
+      best = std::min(best, fx::stable_dt(scheme, p, fx::element_omega_sq(p, xl)));
+    }
+    *dt = best;
+  });
+}
+
+}  // extern "C"

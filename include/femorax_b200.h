@@ -1,0 +1,269 @@
+/* femorax_b200: B200-native matrix-free hex8 (stdBrick, 2x2x2 Gauss) hot path behind a C ABI.
+ *
+ * Plain C types only: pointers, sizes, status codes. Device vectors are FP64 (or FP32 for the
+ * *_f32 twins), in the compile step's equation numbering, resident in the memory of the device
+ * the handle was created on. Calls on one handle are stream-ordered on the stream the caller
+ * passes (cudaStream_t as void*; NULL is the legacy default stream). Nothing here allocates
+ * device memory after the create calls, except where a function says so.
+ *
+ * Each entry point names the reference interface it replaces (amnp95/FemoraX, paths relative to
+ * its repository root).
+ */
+#ifndef FEMORAX_B200_H
+#define FEMORAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes
+ * Replace the reference's exceptions (io::ModelError, io::UnsupportedComponent,
+ * std::runtime_error from solvers/jacobi.cpp:22) and Kokkos::abort calls
+ * (src/exec/internal_force.cpp:359,541,562): no exception crosses this ABI. */
+#define FX_OK 0
+#define FX_E_INVALID 1     /* bad argument or model (io::ModelError) */
+#define FX_E_UNSUPPORTED 2 /* valid but not supported here (io::UnsupportedComponent) */
+#define FX_E_NOMEM 3       /* device or host allocation failed */
+#define FX_E_NOT_SPD 4     /* CG met p.Ap <= 0 (SolveResult::indefinite) */
+#define FX_E_DIVERGED 5    /* non-finite values or no convergence */
+#define FX_E_TIMEOUT 6     /* a bounded device wait gave up */
+#define FX_E_CUDA 7        /* a CUDA runtime error (message in fx_last_error) */
+
+/* Message of the last failed call on this host thread. */
+const char* fx_last_error(void);
+/* Library version string. */
+const char* fx_version(void);
+
+/* ------------------------------------------------------------------ model description
+ * The fields of io::Model the hot path reads (src/io/model.hpp:34-172), as flat arrays.
+ * Replaces the HDF5 model file for this path: the host side builds the model in memory. */
+typedef struct fx_model fx_model;
+
+/* Material kinds of a parameter set. */
+#define FX_MAT_ELASTIC 0 /* ElasticIsotropic (src/physics/materials/elastic_isotropic.hpp) */
+#define FX_MAT_J2 1      /* J2 plasticity, linear hardening (no counterpart in the reference) */
+
+/* One material: kind and its constants. J2 uses E, nu, rho, sigma_y, H (hardening modulus) and
+ * hk (kinematic share of H, 0 = isotropic, 1 = kinematic). */
+typedef struct fx_material {
+  int32_t kind;
+  int32_t pad_;
+  double E, nu, rho;
+  double sigma_y, H, hk;
+} fx_material;
+
+/* N nodes: tags and coordinates (row-major, 3 per node); 3 DOFs per node. */
+int fx_model_create(int32_t num_nodes, const int32_t* tags, const double* coords, fx_model** out);
+void fx_model_destroy(fx_model* m);
+/* One stdBrick element group (io::ElementGroup, model.hpp:100-126) with its own material:
+ * body force b[3], -lumped flag, element tags, 8 node tags per element in stdBrick order. */
+int fx_model_add_group(fx_model* m, const fx_material* mat, const double* b, int32_t lumped, int32_t count,
+                       const int32_t* element_tags, const int32_t* connectivity);
+/* fix rows (node tag, 1-based DOF), model.hpp:134-137. */
+int fx_model_add_fix(fx_model* m, int32_t n, const int32_t* node, const int32_t* dof);
+/* equalDOF rows (retained, constrained, 1-based DOF), model.hpp:157-162. */
+int fx_model_add_equal_dof(fx_model* m, int32_t n, const int32_t* retained, const int32_t* constrained,
+                           const int32_t* dof);
+/* A Rayleigh region (model.hpp:164-170); the last region naming an element wins. */
+int fx_model_add_rayleigh(fx_model* m, double alphaM, double betaK, double betaKinit, double betaKcomm, int32_t n,
+                          const int32_t* element_tags);
+/* Nodal masses (node tag, 1-based DOF, value), model.hpp:129-132. */
+int fx_model_add_mass(fx_model* m, int32_t n, const int32_t* node, const int32_t* dof, const double* value);
+
+/* ------------------------------------------------------------------ compile step
+ * compile::compile_model (src/compile/batches.cpp:54-393) for stdBrick groups: RCM node order
+ * (src/compile/renumber.cpp:98-183), element order, DOF numbering with equalDOF groups and
+ * fixes (src/compile/dof_numbering.cpp:269-485), one batch padded to simd_width, parameter
+ * sets per (group, Rayleigh region), lumped masses, optional greedy coloring (:23-50). The
+ * arrays are bit-identical to the reference's. */
+typedef struct fx_compiled fx_compiled;
+#define FX_RENUMBER_OFF 0
+#define FX_RENUMBER_RCM 1
+int fx_compile(const fx_model* m, int32_t renumbering, int32_t simd_width, int32_t coloring, fx_compiled** out);
+void fx_compiled_destroy(fx_compiled* c);
+/* sizes[8] = num_nodes, num_equations, num_slots, num_batches, count, padded, num_params,
+ * num_colors (batch 0). */
+int fx_compiled_sizes(const fx_compiled* c, int64_t* sizes);
+/* Named arrays, as the reference's Compiled holds them (batches.hpp:80-116); returns the
+ * length, or -1 for an unknown name; out may be NULL to ask the length. int32 names:
+ * node_tag, node_order, element_order, eq, dof_offset, node_model_index, b_node, b_eq,
+ * b_param, b_tag, color_start, color_elements, eq_dof. double names: coords, lumped_mass,
+ * lumped_alpha_mass, nodal_mass, nodal_alpha_mass. */
+int64_t fx_compiled_array_i32(const fx_compiled* c, const char* name, int32_t* out);
+int64_t fx_compiled_array_f64(const fx_compiled* c, const char* name, double* out);
+
+/* ------------------------------------------------------------------ mesh arrays
+ * What the device path consumes: the compile step's arrays as plain host pointers
+ * (compile::Compiled, batches.hpp:80-116, one stdBrick batch), from fx_compile or from the
+ * reference's own compile_model. */
+typedef struct fx_param_set {
+  int32_t kind;      /* FX_MAT_* */
+  int32_t mass_type; /* 0 consistent, 1 lumped (StdBrick::Params::massType) */
+  double E, nu, rho;
+  double b[3];                                /* body force per unit volume */
+  double alphaM, betaK, betaKinit, betaKcomm; /* Rayleigh (physics/contracts.hpp:69-75) */
+  double sigma_y, H, hk;                      /* J2 only */
+} fx_param_set;
+
+typedef struct fx_mesh {
+  int32_t num_nodes, num_equations;
+  const double* coords; /* [3 * num_nodes] structure of arrays x[N] y[N] z[N] */
+  int32_t count, padded;
+  const int32_t* node;  /* [8 * padded]: internal node of corner a of element e at a*padded+e */
+  const int32_t* eq;    /* [24 * padded]: equation of local DOF k at k*padded+e, -1 fixed */
+  const int32_t* param; /* [padded] */
+  int32_t num_params;
+  int32_t pad_;
+  const fx_param_set* params;      /* [num_params] */
+  const double* lumped_mass;       /* [num_equations] or NULL */
+  const double* nodal_mass;        /* [num_equations] or NULL */
+  const double* nodal_alpha_mass;  /* [num_equations] or NULL */
+  const int8_t* eq_dof;            /* [num_equations] or NULL: the nodal DOF of each equation */
+} fx_mesh;
+
+/* Fills *mesh with pointers into c (valid while c lives); params[] must hold num_params. */
+int fx_compiled_mesh(const fx_compiled* c, fx_param_set* params, fx_mesh* mesh);
+
+/* ------------------------------------------------------------------ internal force / operator
+ * exec::InternalForce (src/exec/internal_force.hpp:80-213): owns every device buffer of one
+ * mesh (maps, parameters, state, plans, work vectors); compute/apply allocate nothing. */
+typedef struct fx_force fx_force;
+
+/* Execution paths (set by fx_force_set_path; default FX_PATH_AUTO).
+ *   FX_PATH_GENERAL     Gauss-point element kernel in the reference's arithmetic order, element
+ *                       values into slots, per-equation slot gather in (element, DOF) order:
+ *                       any hexahedra.
+ *   FX_PATH_BOX         node-owner kernel over structured grids of axis-aligned boxes, exact
+ *                       modal (Walsh-Hadamard) form of the 2x2x2-Gauss element operator.
+ *   FX_PATH_AUTO        BOX when the mesh qualifies, else GENERAL. */
+#define FX_PATH_AUTO 0
+#define FX_PATH_GENERAL 1
+#define FX_PATH_BOX 2
+
+int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out);
+void fx_force_destroy(fx_force* f);
+int fx_force_set_path(fx_force* f, int32_t path);
+/* info[8] = num_equations, num_elements, path in use, box qualifies (0/1), grid nx, ny, nz,
+ * device bytes held. */
+int fx_force_info(const fx_force* f, int64_t* info);
+
+/* Operator coefficients K_eff = stiffness K_t + damping C + mass M (OperatorCoefficients,
+ * src/physics/operators/element_operator.hpp:33-40). */
+typedef struct fx_coeffs {
+  double stiffness, damping, mass;
+  int32_t initial; /* K_0 in the stiffness term (ModifiedNewton -initial) */
+  int32_t pad_;
+} fx_coeffs;
+
+/* y = K_eff x (InternalForce::apply_operator, internal_force.cpp:545-573; x, y device FP64,
+ * never aliasing). */
+int fx_apply_operator(fx_force* f, fx_coeffs k, const double* x, double* y, void* stream);
+/* FP32 twin: x, y device FP32, parameters rounded to FP32 (the mixed-precision inner operator). */
+int fx_apply_operator_f32(fx_force* f, fx_coeffs k, const float* x, float* y, void* stream);
+/* The same apply from HOST vectors (pinned or pageable): copies in, applies, copies out. */
+int fx_apply_operator_host(fx_force* f, fx_coeffs k, const double* x_host, double* y_host, void* stream);
+/* d = diag(K_eff) (InternalForce::operator_diagonal, internal_force.cpp:575-599). */
+int fx_operator_diagonal(fx_force* f, fx_coeffs k, double* d, void* stream);
+/* f = f_int(u) + Rayleigh damping forces at v + nodal alphaM M v (InternalForce::compute,
+ * internal_force.cpp:354-377). u, v, f device FP64. */
+int fx_force_compute(fx_force* f, const double* u, const double* v, double* out, void* stream);
+int fx_force_compute_f32(fx_force* f, const float* u, const float* v, float* out, void* stream);
+/* y = M r_dir, the UniformExcitation load shape (InternalForce::mass_times_ground,
+ * internal_force.cpp:601-626). */
+int fx_mass_times_ground(fx_force* f, int32_t dir, double* y, void* stream);
+/* Smallest stable step of the elements (InternalForce::min_critical_dt,
+ * internal_force.hpp:201): scheme 0 CentralDifference, 1 ExplicitDifference. Host result. */
+int fx_min_critical_dt(fx_force* f, int32_t scheme, double* dt);
+/* Material state: commit the trial state (InternalForce::commit_state, internal_force.cpp:507). */
+int fx_force_commit(fx_force* f, void* stream);
+/* Number of Gauss points that were plastic at the last force evaluation (J2). */
+int fx_force_plastic_points(fx_force* f, int64_t* count);
+
+/* ------------------------------------------------------------------ vector kernels
+ * solvers::VectorOps (src/solvers/vector_ops.hpp:17-57): deterministic reductions in the
+ * documented order (chunks of 2048 entries; lane l of `lanes` sums entries l, l+lanes, ... of a
+ * chunk; the lane sums are added in lane order; levels of chunk sums until one value is left).
+ * lanes = 32 is the order of the reference's CUDA build, lanes = 1 that of its host build.
+ * Products are fused multiply-adds. Like VectorOps(n, lanes), the handle owns the partial sums
+ * for vectors of up to `capacity` entries, allocated at creation. */
+typedef struct fx_vops fx_vops;
+int fx_vops_create(int64_t capacity, int32_t lanes, int32_t device, fx_vops** out);
+void fx_vops_destroy(fx_vops* v);
+/* x.y of n entries (VectorOps::dot, vector_ops.cpp:54-73): written to *result_dev (device) when
+ * given, and to *result_host (after a stream synchronisation) when given. */
+int fx_vops_dot(fx_vops* v, const double* x, const double* y, int64_t n, double* result_dev, double* result_host,
+                void* stream);
+/* Element-wise kernels (vector_ops.cpp:77-103): y += a x; y = x + a y; y = d .* x. */
+int fx_axpy(double a, const double* x, double* y, int64_t n, void* stream);
+int fx_xpay(const double* x, double a, double* y, int64_t n, void* stream);
+int fx_multiply(const double* d, const double* x, double* y, int64_t n, void* stream);
+
+/* ------------------------------------------------------------------ solvers
+ * solvers::SolveOptions / SolveResult (src/solvers/linear_solver.hpp:79-94). */
+typedef struct fx_solve_opts {
+  double rtol, atol;
+  int32_t max_iterations;
+  int32_t lanes;   /* dot order; 32 = the reference's CUDA order */
+  int32_t restart; /* GMRES */
+  int32_t pad_;
+} fx_solve_opts;
+typedef struct fx_solve_result {
+  int32_t converged, iterations;
+  double rhs_norm, initial_residual, final_residual;
+  int32_t indefinite, status;
+  int32_t refinements; /* fx_ir_solve: outer FP64 corrections */
+  int32_t pad_;
+} fx_solve_result;
+
+/* A linear solver on the matrix-free operator K_eff of one fx_force (solvers::LinearSolver,
+ * src/solvers/linear_solver.hpp:96-105, with the Jacobi preconditioner of jacobi.cpp:10-26).
+ * fx_solver_create allocates the work vectors (LinearSolver::setup's allocation);
+ * fx_solver_setup takes the operator coefficients and builds the Jacobi diagonal (call it when
+ * the coefficients change); fx_solver_solve solves K_eff x = b with x holding the initial guess.
+ * Methods:
+ *   FX_SOLVER_CG      Jacobi-PCG (ConjugateGradient::solve, src/solvers/cg.cpp:24-71),
+ *                     device-resident: scalars stay on the device, iterations run as a CUDA
+ *                     graph, the host reads a convergence flag every few iterations.
+ *   FX_SOLVER_GMRES   FGMRES(restart) with CGS2 (Gmres::solve, src/solvers/gmres.cpp:32-123).
+ *   FX_SOLVER_KRYLOV  CG, then GMRES from the initial guess if CG meets p.Ap <= 0
+ *                     (KrylovSolver::solve, src/solvers/krylov.cpp:25-41).
+ *   FX_SOLVER_IR      CG in FP32 (FP32 operator and vectors) inside FP64 iterative refinement:
+ *                     r = b - K x in FP64, K d = r by FP32 PCG to inner_rtol, x += d in FP64,
+ *                     until ||b - K x|| <= rtol ||b|| in FP64. Box path only. */
+#define FX_SOLVER_CG 0
+#define FX_SOLVER_GMRES 1
+#define FX_SOLVER_KRYLOV 2
+#define FX_SOLVER_IR 3
+typedef struct fx_solver fx_solver;
+int fx_solver_create(fx_force* f, int32_t method, fx_solve_opts o, fx_solver** out);
+void fx_solver_destroy(fx_solver* s);
+int fx_solver_setup(fx_solver* s, fx_coeffs k, void* stream);
+/* FX_SOLVER_IR: the relative tolerance of each inner FP32 solve (default 1e-4). */
+int fx_solver_set_inner_tolerance(fx_solver* s, double inner_rtol);
+int fx_solver_solve(fx_solver* s, const double* b, double* x, fx_solve_result* r, void* stream);
+
+/* ------------------------------------------------------------------ time stepping
+ * ExplicitDifference steps (src/exec/explicit_analysis.cpp:62-84, 687-705): per step
+ * predict (vh += dt a; u += dt vh), force at (u, vh), correct (a = (-f - m ag)/m,
+ * v = vh + dt/8 (3a + a_old)). ag(t) of the UniformExcitation in direction dir is given per
+ * step in ag_host[steps] (NULL: none). State vectors u, vh, a, v device FP64 (FP32 for _f32). */
+int fx_explicit_run(fx_force* f, const double* mass, int32_t dir, const double* ag_host, int32_t steps, double dt,
+                    double* u, double* vh, double* a, double* v, void* stream);
+int fx_explicit_run_f32(fx_force* f, const float* mass, int32_t dir, const double* ag_host, int32_t steps, double dt,
+                        float* u, float* vh, float* a, float* v, void* stream);
+/* Record one equation's acceleration history: after fx_explicit_run, hist_dev[step] = a[eq]. */
+int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev);
+
+/* Newmark form D kernels (src/exec/implicit_stage.cpp:29-68). */
+int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
+                       double a2, double a3, double a4, void* stream);
+int fx_newmark_update(int64_t n, const double* du, double* u, double* v, double* a, double c2, double c3,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,390 @@
+// Test infrastructure only: a C-ABI driver around the reference's own C++ code, compiled from
+// the reference's sources (src/physics, src/compile, src/exec, src/solvers) together with the
+// Kokkos-subset shim in this folder. It is the "reference run here" that pins the oracle and
+// the CUDA path: the reference's compile step (index maps), its InternalForce operator and
+// force evaluation (gather scatter, geometry cache), its CG/GMRES/Jacobi solvers and its
+// per-element stdBrick physics, all on the host.
+//
+// Only tests/, the smoke check and bench.py's CPU-baseline leg load the library built from this
+// file (oracle/_ref/libfxref.so). The product library never links it.
+
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "compile/batches.hpp"
+#include "exec/internal_force.hpp"
+#include "exec/matrix_free_operator.hpp"
+#include "physics/elements/std_brick.hpp"
+#include "physics/materials/elastic_isotropic.hpp"
+#include "physics/operators/element_operator.hpp"
+#include "solvers/cg.hpp"
+#include "solvers/gmres.hpp"
+#include "solvers/jacobi.hpp"
+#include "solvers/vector_ops.hpp"
+
+using namespace femorax;
+
+namespace {
+thread_local std::string g_error;
+int fail(const std::exception& e) {
+  g_error = e.what();
+  return -1;
+}
+using Brick = StdBrick<ElasticIsotropic>;
+}  // namespace
+
+extern "C" {
+
+const char* fxref_last_error() { return g_error.c_str(); }
+
+// ------------------------------------------------------------------------------ model
+// A model is described by flat arrays (the fields of io::Model the hot path reads):
+//   nodes: tags[N], coords[3N] row-major, ndf 3 for every node;
+//   element groups g: material (E, nu, rho), body force b[3], lumped flag, element tags and
+//   connectivity (8 node tags per element), group_start[G+1] offsets into the element arrays;
+//   fix rows (node tag, dof 1..3); equalDOF rows (retained, constrained, dof);
+//   Rayleigh regions r: alphaM, betaK, betaKinit, betaKcomm and element tags
+//   (region_start[R+1] offsets); nodal masses (node tag, dof, value).
+struct fxref_model {
+  io::Model m;
+};
+
+fxref_model* fxref_model_create(int32_t N, const int32_t* tags, const double* coords) {
+  auto* h = new fxref_model;
+  h->m.ndm = 3;
+  h->m.nodes.tags.assign(tags, tags + N);
+  h->m.nodes.coords.assign(coords, coords + 3 * static_cast<std::size_t>(N));
+  h->m.nodes.ndf.assign(static_cast<std::size_t>(N), 3);
+  return h;
+}
+
+void fxref_model_destroy(fxref_model* h) { delete h; }
+
+// Adds one material (tag = index + 1) and one stdBrick element group that uses it.
+int fxref_model_add_group(fxref_model* h, double E, double nu, double rho, const double* b, int lumped,
+                          int32_t count, const int32_t* etags, const int32_t* conn) {
+  io::NDMaterial mat;
+  mat.tag = static_cast<std::int32_t>(h->m.materials.size()) + 1;
+  mat.data = io::ElasticIsotropicData{E, nu, rho};
+  h->m.materials.push_back(mat);
+  io::ElementGroup g;
+  g.id = std::to_string(h->m.elements.size());
+  g.type = io::ElementType::StdBrick;
+  g.material = mat.tag;
+  g.body_force = {b[0], b[1], b[2]};
+  g.lumped = lumped != 0;
+  g.tags.assign(etags, etags + count);
+  g.connectivity.assign(conn, conn + 8 * static_cast<std::size_t>(count));
+  h->m.elements.push_back(std::move(g));
+  return 0;
+}
+
+void fxref_model_add_fix(fxref_model* h, int32_t n, const int32_t* node, const int32_t* dof) {
+  h->m.fix.node.insert(h->m.fix.node.end(), node, node + n);
+  h->m.fix.dof.insert(h->m.fix.dof.end(), dof, dof + n);
+}
+
+void fxref_model_add_equal_dof(fxref_model* h, int32_t n, const int32_t* retained, const int32_t* constrained,
+                               const int32_t* dof) {
+  h->m.equal_dof.retained.insert(h->m.equal_dof.retained.end(), retained, retained + n);
+  h->m.equal_dof.constrained.insert(h->m.equal_dof.constrained.end(), constrained, constrained + n);
+  h->m.equal_dof.dof.insert(h->m.equal_dof.dof.end(), dof, dof + n);
+}
+
+void fxref_model_add_rayleigh(fxref_model* h, double alphaM, double betaK, double betaKinit, double betaKcomm,
+                              int32_t n, const int32_t* etags) {
+  io::RayleighRegion r;
+  r.id = std::to_string(h->m.rayleigh.size());
+  r.alphaM = alphaM;
+  r.betaK = betaK;
+  r.betaKinit = betaKinit;
+  r.betaKcomm = betaKcomm;
+  r.elements.assign(etags, etags + n);
+  h->m.rayleigh.push_back(std::move(r));
+}
+
+void fxref_model_add_mass(fxref_model* h, int32_t n, const int32_t* node, const int32_t* dof, const double* value) {
+  h->m.mass.node.insert(h->m.mass.node.end(), node, node + n);
+  h->m.mass.dof.insert(h->m.mass.dof.end(), dof, dof + n);
+  h->m.mass.value.insert(h->m.mass.value.end(), value, value + n);
+}
+
+// ------------------------------------------------------------------------------ compile
+struct fxref_compiled {
+  compile::Compiled c;
+};
+
+// renumbering: 0 off (file order), 1 RCM. simd_width: the batch padding.
+fxref_compiled* fxref_compile(const fxref_model* h, int renumbering, int simd_width, int coloring) {
+  try {
+    compile::CompileOptions o;
+    o.renumbering = renumbering ? compile::Renumbering::RCM : compile::Renumbering::Off;
+    o.simd_width = simd_width;
+    o.build_coloring = coloring != 0;
+    auto* c = new fxref_compiled;
+    c->c = compile::compile_model(h->m, o);
+    return c;
+  } catch (const std::exception& e) {
+    fail(e);
+    return nullptr;
+  }
+}
+void fxref_compiled_destroy(fxref_compiled* c) { delete c; }
+
+// Sizes: [num_nodes, num_equations, num_slots, num_batches, batch0 count, batch0 padded,
+//         batch0 num params, batch0 num colors]
+void fxref_compiled_sizes(const fxref_compiled* h, int64_t* out) {
+  const auto& c = h->c;
+  out[0] = c.dofs.num_nodes();
+  out[1] = c.dofs.num_equations;
+  out[2] = c.dofs.num_slots;
+  out[3] = static_cast<int64_t>(c.batches.size());
+  out[4] = c.batches.empty() ? 0 : c.batches[0].count;
+  out[5] = c.batches.empty() ? 0 : c.batches[0].padded;
+  out[6] = c.batches.empty() ? 0 : static_cast<int64_t>(c.batches[0].params.size());
+  out[7] = c.batches.empty() ? 0 : c.batches[0].num_colors();
+}
+
+// Copies a named array of the compiled model (batch 0 for the per-element ones) into out; returns
+// its length (call with out = NULL to ask). Names: coords, node_tag, node_order, eq (the DOF
+// numbering's eq[ndof]), dof_offset, b_node, b_eq, b_param, b_tag, color_start, color_elements,
+// lumped_mass, lumped_alpha_mass, nodal_mass, nodal_alpha_mass, eq_dof.
+int64_t fxref_compiled_array_i32(const fxref_compiled* h, const char* name, int32_t* out) {
+  const auto& c = h->c;
+  const std::vector<std::int32_t>* v = nullptr;
+  std::vector<std::int32_t> tmp;
+  const std::string n(name);
+  if (n == "node_tag") v = &c.dofs.node_tag;
+  else if (n == "node_order") v = &c.ordering.node_order;
+  else if (n == "element_order") v = &c.ordering.element_order;
+  else if (n == "eq") v = &c.dofs.eq;
+  else if (n == "dof_offset") v = &c.dofs.dof_offset;
+  else if (n == "node_model_index") v = &c.dofs.node_model_index;
+  else if (!c.batches.empty() && n == "b_node") v = &c.batches[0].node;
+  else if (!c.batches.empty() && n == "b_eq") v = &c.batches[0].eq;
+  else if (!c.batches.empty() && n == "b_param") v = &c.batches[0].param;
+  else if (!c.batches.empty() && n == "b_tag") v = &c.batches[0].tag;
+  else if (!c.batches.empty() && n == "color_start") v = &c.batches[0].color_start;
+  else if (!c.batches.empty() && n == "color_elements") v = &c.batches[0].color_elements;
+  else if (n == "eq_dof") {
+    tmp.assign(c.eq_dof.begin(), c.eq_dof.end());
+    v = &tmp;
+  } else {
+    return -1;
+  }
+  if (out) std::memcpy(out, v->data(), v->size() * sizeof(std::int32_t));
+  return static_cast<int64_t>(v->size());
+}
+
+int64_t fxref_compiled_array_f64(const fxref_compiled* h, const char* name, double* out) {
+  const auto& c = h->c;
+  const std::vector<double>* v = nullptr;
+  const std::string n(name);
+  if (n == "coords") v = &c.coords;
+  else if (n == "lumped_mass") v = &c.lumped_mass;
+  else if (n == "lumped_alpha_mass") v = &c.lumped_alpha_mass;
+  else if (n == "nodal_mass") v = &c.nodal_mass;
+  else if (n == "nodal_alpha_mass") v = &c.nodal_alpha_mass;
+  else return -1;
+  if (out) std::memcpy(out, v->data(), v->size() * sizeof(double));
+  return static_cast<int64_t>(v->size());
+}
+
+// Parameter set p of batch 0: [E, nu, rho, b0, b1, b2, massType, alphaM, betaK, betaKinit, betaKcomm,
+// group, material, region].
+int fxref_compiled_param(const fxref_compiled* h, int32_t p, double* out) {
+  const auto& b = h->c.batches.at(0);
+  const auto& ps = b.params.at(static_cast<std::size_t>(p));
+  const auto bp = ps.params<Brick>();
+  const double v[14] = {bp.mat.E,           bp.mat.v,          bp.mat.rho,
+                        bp.b[0],            bp.b[1],           bp.b[2],
+                        double(bp.massType), ps.damping.alphaM, ps.damping.betaK,
+                        ps.damping.betaKinit, ps.damping.betaKcomm, double(ps.group),
+                        double(ps.material), double(ps.region)};
+  std::memcpy(out, v, sizeof(v));
+  return 0;
+}
+
+// ------------------------------------------------------------------------------ exec
+struct fxref_force {
+  std::unique_ptr<exec::InternalForce> f;
+  int32_t neq = 0;
+};
+
+// cache: 0 Off, 1 On (the geometry cache).
+fxref_force* fxref_force_create(const fxref_compiled* c, int cache) {
+  try {
+    auto* h = new fxref_force;
+    h->f = std::make_unique<exec::InternalForce>(c->c, cache ? exec::GeometryCache::On : exec::GeometryCache::Off);
+    h->neq = h->f->num_equations();
+    return h;
+  } catch (const std::exception& e) {
+    fail(e);
+    return nullptr;
+  }
+}
+void fxref_force_destroy(fxref_force* h) { delete h; }
+
+namespace {
+exec::OperatorSettings op_settings(int scatter, int geometry) {
+  exec::OperatorSettings s;
+  s.scatter = scatter == 0 ? exec::Scatter::Gather : scatter == 1 ? exec::Scatter::Atomic : exec::Scatter::Colored;
+  s.geometry = geometry ? exec::Geometry::Cached : exec::Geometry::Recompute;
+  s.tangent = exec::TangentSource::Auto;
+  return s;
+}
+exec::Vec wrap(const double* p, int64_t n) { return exec::Vec(const_cast<double*>(p), static_cast<std::size_t>(n)); }
+}  // namespace
+
+// y = (cK K + cC C + cM M) x through InternalForce::apply_operator (u = 0: elastic tangents).
+int fxref_apply_operator(fxref_force* h, double cK, double cC, double cM, int scatter, int geometry, const double* x,
+                         double* y) {
+  try {
+    exec::Vec u("u0", static_cast<std::size_t>(h->neq));
+    h->f->apply_operator(OperatorCoefficients{cK, cC, cM, false}, op_settings(scatter, geometry), u, wrap(x, h->neq),
+                         wrap(y, h->neq));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+int fxref_operator_diagonal(fxref_force* h, double cK, double cC, double cM, int geometry, double* d) {
+  try {
+    exec::Vec u("u0", static_cast<std::size_t>(h->neq));
+    h->f->operator_diagonal(OperatorCoefficients{cK, cC, cM, false}, op_settings(0, geometry), u, wrap(d, h->neq));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// y = M r_dir (UniformExcitation load shape), through InternalForce::mass_times_ground.
+int fxref_mass_times_ground(fxref_force* h, int dir, double* y) {
+  try {
+    exec::Vec u("u0", static_cast<std::size_t>(h->neq));
+    h->f->mass_times_ground(dir, op_settings(0, 1), u, wrap(y, h->neq));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// f = f_int(u) + Rayleigh damping forces at v (flat layout, gather scatter).
+int fxref_force_compute(fxref_force* h, const double* u, const double* v, int geometry, double* f) {
+  try {
+    auto& F = *h->f;
+    for (int32_t q = 0; q < h->neq; ++q) {
+      F.u(q) = u[q];
+      F.v(q) = v[q];
+    }
+    exec::ForceSettings s;
+    s.layout = exec::Layout::Flat;
+    s.scatter = exec::Scatter::Gather;
+    s.geometry = geometry ? exec::Geometry::Cached : exec::Geometry::Recompute;
+    F.compute(s);
+    for (int32_t q = 0; q < h->neq; ++q) f[q] = F.f(q);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// scheme: 0 CentralDifference, 1 ExplicitDifference.
+double fxref_min_critical_dt(fxref_force* h, int scheme) {
+  return h->f->min_critical_dt(scheme ? ExplicitScheme::ExplicitDifference : ExplicitScheme::CentralDifference);
+}
+
+// ------------------------------------------------------------------------------ solvers
+// result: [converged, iterations, rhs_norm, initial_residual, final_residual, indefinite]
+int fxref_solve(fxref_force* h, int method, double cK, double cC, double cM, double rtol, double atol, int max_it,
+                int lanes, int restart, const double* b, double* x, double* result) {
+  try {
+    exec::Vec u("u0", static_cast<std::size_t>(h->neq));
+    exec::MatrixFreeOperator op(*h->f, u, OperatorCoefficients{cK, cC, cM, false});
+    solvers::Jacobi jac;
+    jac.setup(op);
+    solvers::SolveOptions so;
+    so.relative_tolerance = rtol;
+    so.absolute_tolerance = atol;
+    so.max_iterations = max_it;
+    solvers::SolveResult r;
+    exec::Vec xv = wrap(x, h->neq);
+    if (method == 0) {
+      solvers::ConjugateGradient cg(so, lanes);
+      cg.setup(op, &jac);
+      r = cg.solve(wrap(b, h->neq), xv);
+    } else {
+      solvers::Gmres gm(so, lanes, restart);
+      gm.setup(op, &jac);
+      r = gm.solve(wrap(b, h->neq), xv);
+    }
+    result[0] = r.converged;
+    result[1] = r.iterations;
+    result[2] = r.rhs_norm;
+    result[3] = r.initial_residual;
+    result[4] = r.final_residual;
+    result[5] = r.indefinite;
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+double fxref_host_dot(const double* x, const double* y, int64_t n, int lanes) {
+  std::vector<double> a(x, x + n), b(y, y + n);
+  return solvers::VectorOps::host_dot(a, b, lanes);
+}
+
+// ------------------------------------------------------------------------------ element level
+// p = [E, nu, rho, b0, b1, b2, massType]; damp = [alphaM, betaK, betaKinit, betaKcomm];
+// xe[8][3]. Outputs fe[24] and, if Ke != NULL, Ke[24][24] row-major.
+int fxref_brick_compute(const double* p, const double* damp, const double* xe, const double* u, const double* v,
+                        double* fe, double* Ke) {
+  Brick::Params bp{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}, static_cast<int>(p[6])};
+  Rayleigh d{damp[0], damp[1], damp[2], damp[3], {}};
+  const auto* x = reinterpret_cast<const double(*)[3]>(xe);
+  if (Ke) {
+    Brick::compute<true>(bp, d, x, u, v, {}, {}, fe, reinterpret_cast<double(*)[24]>(Ke));
+  } else {
+    Brick::compute<false>(bp, d, x, u, v, {}, {}, fe, nullptr);
+  }
+  return 0;
+}
+
+int fxref_brick_mass(const double* p, const double* xe, double* Me, double* lumped) {
+  Brick::Params bp{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}, static_cast<int>(p[6])};
+  const auto* x = reinterpret_cast<const double(*)[3]>(xe);
+  if (Me) Brick::mass(bp, x, Me);
+  if (lumped) Brick::lumped_mass(bp, x, lumped);
+  return 0;
+}
+
+// y_e = K_eff,e v_e by element_operator_apply with recomputed geometry and the constant tangent.
+int fxref_brick_operator(const double* p, const double* damp, const double* k, const double* xe, const double* ve,
+                         double* ye, int diagonal, const int32_t* eq) {
+  Brick::Params bp{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}, static_cast<int>(p[6])};
+  Rayleigh d{damp[0], damp[1], damp[2], damp[3], {}};
+  OperatorCoefficients kc{k[0], k[1], k[2], false};
+  double xl[3][8];
+  Brick::local_coords(reinterpret_cast<const double(*)[3]>(xe), xl);
+  const auto geo = Brick::recomputed_geometry(xl, bp);
+  auto tangent_at = [&](int, const Brick::PointShape&, double (*D)[6]) { ElasticIsotropic::initial_tangent(bp.mat, D); };
+  auto committed_at = [&](int, double (*D)[6]) { ElasticIsotropic::initial_tangent(bp.mat, D); };
+  if (diagonal) element_operator_diagonal<Brick>(bp, d, kc, geo, tangent_at, committed_at, eq, ye);
+  else element_operator_apply<Brick>(bp, d, kc, geo, tangent_at, committed_at, ve, ye);
+  return 0;
+}
+
+double fxref_brick_critical_dt(const double* p, const double* damp, int scheme, const double* xe) {
+  Brick::Params bp{{p[0], p[1], p[2]}, {p[3], p[4], p[5]}, static_cast<int>(p[6])};
+  Rayleigh d{damp[0], damp[1], damp[2], damp[3], {}};
+  return Brick::critical_dt(bp, d, scheme ? ExplicitScheme::ExplicitDifference : ExplicitScheme::CentralDifference,
+                            reinterpret_cast<const double(*)[3]>(xe), {});
+}
+
+}  // extern "C"
