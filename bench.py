@@ -1,0 +1,291 @@
+"""Benchmark: the plain FP64 matrix-free apply y = K x on the layered soil box (128 x 128 x 64
+stdBrick, 8 layers, ~3.2 M equations), in GDoF/s (equations / apply time).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: one process per GPU (torchrun for N > 1), each GPU applies the operator of its own copy
+of the mesh (independent replicas: no data-path collective; weak scaling); the timed region is K
+applies with x resident in HBM, L2 flushed (a 256 MB write) between applies, each apply timed by
+CUDA events on its stream; value = all ranks' equations x K / the slowest rank's summed time.
+`e2e` is the same metric through the public host-buffer call (fx_apply_operator_host: pinned host
+x in, y out, copies inside the timed region). `roofline` relates the kernel to the measured HBM
+copy bandwidth with the algorithmic bytes of one apply: 8 neq (x) + 8 neq (y) + 32 n_el (8 node
+ids) + 12 N (node -> equations) + 4 n_el (parameter index). `cpu_baseline` times the reference's
+own InternalForce::apply_operator (built here from its sources, oracle/_ref) on a bounded sample.
+
+The reference arm (--impl reference) times that reference CPU path alone, on every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+WORKLOAD = dict(workload="layered soil box 128x128x64 stdBrick (8 layers, seed 0), plain FP64 y = K x",
+                nx=128, ny=128, nz=64, layers=8, seed=0)
+METRIC = "K*x GDoF/s (plain FP64 matrix-free apply, layered box 128x128x64)"
+
+
+def algorithmic_bytes(neq, n_el, n_nodes):
+    return 8 * neq + 8 * neq + 32 * n_el + 12 * n_nodes + 4 * n_el
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per apply from the committed ncu summary of this kernel and workload."""
+    p = os.path.join(ROOT, "profiles", "box_apply_layered128.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                           "-i", self.gpu, "-lms", "200"], stdout=subprocess.PIPE,
+                                          stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self._proc = None
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def stop(self):
+        if self._proc:
+            time.sleep(0.25)
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=2)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 4 + i and s[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_mesh():
+    import femorax_b200 as fx
+    from femorax_b200 import meshes
+    spec, _ = meshes.layered_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], WORKLOAD["layers"], seed=WORKLOAD["seed"])
+    return spec, fx.Model(spec).compile(renumbering="rcm", simd_width=32)
+
+
+def cpu_reference_apply(spec, max_seconds=20.0, max_reps=5):
+    """The reference's InternalForce::apply_operator (gather scatter, cached geometry, constant
+    tangent) on the host, OpenMP over every host thread: GDoF/s over a bounded number of applies."""
+    import oracle as O
+    if not O.have_ref():
+        return None
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    c = O.RefModel(spec).compile(renumbering="rcm", simd_width=32)
+    rf = O.RefForce(c, cache=True)
+    x = np.random.default_rng(0).standard_normal(c.num_equations)
+    rf.apply_operator((1.0, 0.0, 0.0), x)  # warm-up (first touch of the cache and slots)
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_reps and (time.perf_counter() - t_start) < max_seconds:
+        t0 = time.perf_counter()
+        rf.apply_operator((1.0, 0.0, 0.0), x)
+        times.append(time.perf_counter() - t0)
+    best = min(times)
+    return dict(value=c.num_equations / best / 1e9, unit="GDoF/s", cores=int(os.environ.get("OMP_NUM_THREADS", threads)),
+                kind="reference",
+                sample=f"{len(times)} applies of the full 128x128x64 layered box (min time {best * 1e3:.1f} ms) through "
+                       "the reference's own InternalForce::apply_operator (gather scatter, geometry cache, constant "
+                       "tangent), built from its sources with a serial/OpenMP Kokkos-subset shim")
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    spec, _ = build_mesh()
+    import oracle as O
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfxref.so (the reference built from "
+                                                               "its sources) is missing"}))
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    c = O.RefModel(spec).compile(renumbering="rcm", simd_width=32)
+    rf = O.RefForce(c, cache=True)
+    x = np.random.default_rng(0).standard_normal(c.num_equations)
+    for _ in range(args.warmup):
+        rf.apply_operator((1.0, 0.0, 0.0), x)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rf.apply_operator((1.0, 0.0, 0.0), x)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = c.num_equations * args.steps / total / 1e9
+    cores = int(os.environ.get("OMP_NUM_THREADS", threads))
+    line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, neq=c.num_equations, elements=c.count, parallelism="host OpenMP"),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "GDoF/s", "cores": cores, "kind": "reference",
+                             "sample": f"{args.steps} applies of the full workload, each one step"},
+            "e2e": {"value": value, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import femorax_b200 as fx
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    spec, comp = build_mesh()
+    mesh = comp.mesh()
+    force = fx.InternalForce(mesh, device=local)
+    info = force.info()
+    neq, n_el, n_nodes = mesh.num_equations, mesh.count, mesh.num_nodes
+    dev = torch.device("cuda", local)
+    k = fx.OperatorCoefficients(1.0, 0.0, 0.0)
+    x = torch.as_tensor(np.random.default_rng(rank).standard_normal(neq), device=dev)
+    y = torch.zeros(neq, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(max(args.warmup, 3)):
+        force.apply_operator(k, x, y, stream)
+    torch.cuda.synchronize(dev)
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    for i in range(args.steps):
+        flush.fill_(float(i))  # 256 MB write: L2 (126 MB) holds nothing of the last apply
+        starts[i].record(stream)
+        force.apply_operator(k, x, y, stream)
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.stop()
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * neq * args.steps / (total_ms * 1e-3) / 1e9
+
+    # e2e: the public host-buffer call, copies included
+    xh = torch.empty(neq, dtype=torch.float64, pin_memory=True)
+    xh.copy_(x.cpu())
+    yh = torch.empty(neq, dtype=torch.float64, pin_memory=True)
+    xn, yn = xh.numpy(), yh.numpy()
+    force.apply_operator_host(k, xn, yn, stream)
+    e_ms = []
+    for i in range(args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        force.apply_operator_host(k, xn, yn, stream)
+        e_ms.append((time.perf_counter() - t0) * 1e3)
+    te = torch.tensor([sum(e_ms)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = world * neq * args.steps / (float(te.item()) * 1e-3) / 1e9
+
+    peak, peak_kind = load_peaks()
+    alg = algorithmic_bytes(neq, n_el, n_nodes)
+    achieved = alg / (total_ms / args.steps * 1e-3) / 1e9
+    traffic = load_traffic()
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
+    line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded layer properties)",
+            "config": dict(WORKLOAD, neq=neq, elements=n_el, nodes=n_nodes, path=info["path"],
+                           parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                           l2="flushed (256 MB write) between timed applies"),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * neq, "d2h_bytes_per_step": 8 * neq},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary()}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

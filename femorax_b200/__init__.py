@@ -283,7 +283,7 @@ class InternalForce:
         if ag is not None:
             ag = np.ascontiguousarray(ag, np.float64)
             agp = ag.ctypes.data_as(L.p_f64)
-        check(lib().fx_explicit_record(self._h, -1 if record_eq is None else int(record_eq), None))
+        check(lib().fx_explicit_record(self._h, -1 if record_eq is None else int(record_eq), None, 0))
         fn = lib().fx_explicit_run_f32 if u.dtype.itemsize == 4 else lib().fx_explicit_run
         check(fn(self._h, _ptr(mass), direction, agp, steps, dt, _ptr(u), _ptr(vh), _ptr(a), _ptr(v),
                  _stream(stream)))
@@ -291,7 +291,7 @@ class InternalForce:
             import torch
             hist = torch.zeros(steps + 1, dtype=torch.float64, device=u.device)
             torch.cuda.synchronize(u.device)
-            check(lib().fx_explicit_record(self._h, int(record_eq), _ptr(hist)))
+            check(lib().fx_explicit_record(self._h, int(record_eq), _ptr(hist), steps))
             return hist[:steps].cpu().numpy()
         return None
 

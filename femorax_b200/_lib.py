@@ -94,6 +94,9 @@ PROTOTYPES = {
     "fx_force_destroy": (None, [vp]),
     "fx_force_set_path": (C.c_int, [vp, C.c_int32]),
     "fx_force_info": (C.c_int, [vp, p_i64]),
+    "fx_force_set_launch": (C.c_int, [vp, C.c_int32, C.c_int32]),
+    "fx_force_get_launch": (C.c_int, [vp, p_i32]),
+    "fx_force_tune": (C.c_int, [vp, vp]),
     "fx_apply_operator": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_apply_operator_f32": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_apply_operator_host": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
@@ -117,7 +120,7 @@ PROTOTYPES = {
     "fx_solver_solve": (C.c_int, [vp, vp, vp, C.POINTER(fx_solve_result), vp]),
     "fx_explicit_run": (C.c_int, [vp, vp, C.c_int32, p_f64, C.c_int32, C.c_double, vp, vp, vp, vp, vp]),
     "fx_explicit_run_f32": (C.c_int, [vp, vp, C.c_int32, p_f64, C.c_int32, C.c_double, vp, vp, vp, vp, vp]),
-    "fx_explicit_record": (C.c_int, [vp, C.c_int32, vp]),
+    "fx_explicit_record": (C.c_int, [vp, C.c_int32, vp, C.c_int32]),
     "fx_newmark_predict": (C.c_int, [C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, vp]),
     "fx_newmark_update": (C.c_int, [C.c_int64, vp, vp, vp, vp, C.c_double, C.c_double, vp]),

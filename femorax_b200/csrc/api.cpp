@@ -349,6 +349,29 @@ int fx_force_info(const fx_force* f, int64_t* info) {
   });
 }
 
+int fx_force_set_launch(fx_force* f, int32_t variant, int32_t kz) {
+  return guarded([&] {
+    FX_REQUIRE(f, "fx_force_set_launch: null handle");
+    if (!f->s.box.qualifies) throw fx::Error(FX_E_UNSUPPORTED, "no box plan: " + f->s.box.why_not);
+    fx::box_set_launch(f->s, variant, kz);
+  });
+}
+
+int fx_force_get_launch(const fx_force* f, int32_t* launch) {
+  return guarded([&] {
+    FX_REQUIRE(f && launch, "fx_force_get_launch: bad arguments");
+    launch[0] = f->s.box.variant;
+    launch[1] = f->s.box.kz;
+  });
+}
+
+int fx_force_tune(fx_force* f, void* stream) {
+  return guarded([&] {
+    FX_REQUIRE(f, "fx_force_tune: null handle");
+    if (f->s.box.qualifies) fx::box_autotune(f->s, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int fx_apply_operator(fx_force* f, fx_coeffs k, const double* x, double* y, void* stream) {
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || (x && y)), "fx_apply_operator: bad arguments");

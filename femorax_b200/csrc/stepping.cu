@@ -289,16 +289,17 @@ int fx_explicit_run_f32(fx_force* f, const float* mass, int32_t dir, const doubl
   });
 }
 
-int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev) {
+int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev, int32_t count) {
   return guard([&] {
-    if (!f || eq >= f->s.neq) throw fx::Error(FX_E_INVALID, "fx_explicit_record: bad arguments");
+    if (!f || eq >= f->s.neq || count < 0) throw fx::Error(FX_E_INVALID, "fx_explicit_record: bad arguments");
     fx::ExplicitWork& w = work_of(f);
     if (hist_dev == nullptr) {
-      w.record_eq = eq;
+      w.record_eq = eq < 0 ? -1 : eq;
       return;
     }
     if (w.hist.n == 0) throw fx::Error(FX_E_INVALID, "fx_explicit_record: nothing recorded");
-    FX_CUDA(cudaMemcpy(hist_dev, w.hist.ptr, w.hist.bytes(), cudaMemcpyDeviceToDevice));
+    const size_t n = std::min(static_cast<size_t>(count), w.hist.n);
+    FX_CUDA(cudaMemcpy(hist_dev, w.hist.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice));
   });
 }
 

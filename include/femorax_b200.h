@@ -149,6 +149,13 @@ int fx_force_set_path(fx_force* f, int32_t path);
 /* info[8] = num_equations, num_elements, path in use, box qualifies (0/1), grid nx, ny, nz,
  * device bytes held. */
 int fx_force_info(const fx_force* f, int64_t* info);
+/* Box path launch shape: variant (block of element columns) and kz (node planes per CTA);
+ * fx_force_tune times the candidates on the device and keeps the fastest (the autotuner
+ * fx_force_create runs; exec::choose_force_settings' role, src/exec/force_settings.cpp:71-205).
+ * launch[2] of fx_force_get_launch receives (variant, kz). */
+int fx_force_set_launch(fx_force* f, int32_t variant, int32_t kz);
+int fx_force_get_launch(const fx_force* f, int32_t* launch);
+int fx_force_tune(fx_force* f, void* stream);
 
 /* Operator coefficients K_eff = stiffness K_t + damping C + mass M (OperatorCoefficients,
  * src/physics/operators/element_operator.hpp:33-40). */
@@ -254,8 +261,10 @@ int fx_explicit_run(fx_force* f, const double* mass, int32_t dir, const double* 
                     double* u, double* vh, double* a, double* v, void* stream);
 int fx_explicit_run_f32(fx_force* f, const float* mass, int32_t dir, const double* ag_host, int32_t steps, double dt,
                         float* u, float* vh, float* a, float* v, void* stream);
-/* Record one equation's acceleration history: after fx_explicit_run, hist_dev[step] = a[eq]. */
-int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev);
+/* Acceleration history of one equation. With hist_dev NULL: record equation eq (-1: none) in the
+ * following fx_explicit_run calls. Otherwise copy the last run's first `count` recorded values
+ * (hist_dev[step] = a[eq] after step `step`) to hist_dev (device, at least `count` doubles). */
+int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev, int32_t count);
 
 /* Newmark form D kernels (src/exec/implicit_stage.cpp:29-68). */
 int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,

@@ -560,6 +560,20 @@ void fxo_mass_times_ground(const fxo_mesh* m, int dir, double* y) {
       if (q >= 0) y[q] += ye[a];
     }
   }
+  if (m->nodal_mass) {
+    /* the free nodal masses in direction dir (ground_nodal_mass, internal_force.cpp:621-625);
+     * an equation's DOF is its local DOF index mod 3 in any element that has it */
+    int8_t* dof = (int8_t*)malloc((size_t)(m->num_equations > 0 ? m->num_equations : 1));
+    for (int32_t q = 0; q < m->num_equations; ++q) dof[q] = -1;
+    for (int32_t e = 0; e < m->count; ++e)
+      for (int a = 0; a < NDOF; ++a) {
+        const int32_t q = m->eq[(int64_t)a * m->padded + e];
+        if (q >= 0) dof[q] = (int8_t)(a % 3);
+      }
+    for (int32_t q = 0; q < m->num_equations; ++q)
+      if (dof[q] == dir) y[q] += m->nodal_mass[q];
+    free(dof);
+  }
 }
 
 /* ---------------------------------------------------------------- vector kernels */

@@ -1,0 +1,56 @@
+"""Small models the tests share: the reference's synthetic soil column shape (two materials,
+laminar equalDOF ties at every elevation, two Rayleigh regions, body force, lumped mass) and a
+block with two overlapping Rayleigh regions and nodal masses."""
+import numpy as np
+
+from femorax_b200 import meshes
+
+
+def soil_column(nx=3, ny=2, nz=8, lumped=True):
+    """The layered column the reference's tests build in memory (tests/common/synthetic_models.hpp
+    shape): stdBrick, lower and upper material, fixed base, side nodes at each elevation tied to
+    the first side node in DOFs 1 2 3, a Rayleigh region over everything and one over the top
+    layer."""
+    NX, NY, NZ = nx + 1, ny + 1, nz + 1
+    tags, coords = meshes.block_nodes(nx, ny, nz, 1.0, 1.0, 0.5, origin=(0.0, 0.0, -nz * 0.5))
+    groups = []
+    for layer in range(2):
+        k0, k1 = (0, nz // 2) if layer == 0 else (nz // 2, nz)
+        et, cn = meshes.block_connectivity(nx, ny, nz, k0, k1)
+        groups.append(meshes.Group(377000.0 if layer == 0 else 109200.0, 0.3, 2.0285 if layer == 0 else 2.0183, et, cn,
+                                   b=(0.0, 0.0, -19.9 if layer == 0 else -19.8), lumped=lumped))
+    spec = meshes.ModelSpec(tags=tags, coords=coords, groups=groups)
+    spec.fix_node, spec.fix_dof = meshes.fix_base(nx, ny)
+    ret, con, dof = [], [], []
+    for k in range(1, NZ):
+        master = -1
+        for j in range(NY):
+            for i in range(NX):
+                if not (i == 0 or i == nx or j == 0 or j == ny):
+                    continue
+                t = meshes.node_tag(i, j, k, nx, ny)
+                if master < 0:
+                    master = t
+                    continue
+                for d in (1, 2, 3):
+                    ret.append(master)
+                    con.append(t)
+                    dof.append(d)
+    spec.eqd_retained, spec.eqd_constrained, spec.eqd_dof = [np.array(a, np.int32) for a in (ret, con, dof)]
+    all_e = np.concatenate([g.etags for g in groups])
+    spec.rayleigh = [meshes.Rayleigh(0.6, 5.8e-4, 0.0, 0.0, all_e),
+                     meshes.Rayleigh(0.9, 3e-4, 1e-4, 0.0, groups[1].etags[-nx * ny:])]
+    return spec
+
+
+def two_region_block(nx=4, ny=3, nz=5, lumped=False):
+    """A consistent-mass block with two overlapping Rayleigh regions (all four factors used)
+    and nodal masses on a few nodes."""
+    spec = meshes.box_model(nx, ny, nz, (2.0, 1.5, 2.5), E=2.0e5, nu=0.25, rho=1.9, lumped=lumped, b=(0.1, -0.2, -9.8))
+    et = spec.groups[0].etags
+    spec.rayleigh = [meshes.Rayleigh(0.3, 1e-3, 0.0, 0.0, et), meshes.Rayleigh(0.5, 2e-3, 5e-4, 1e-4, et[::3])]
+    top = [meshes.node_tag(i, j, nz, nx, ny) for i in (0, nx) for j in (0, ny)]
+    spec.mass_node = np.repeat(np.array(top, np.int32), 3)
+    spec.mass_dof = np.tile(np.array([1, 2, 3], np.int32), len(top))
+    spec.mass_value = np.linspace(0.5, 2.0, len(spec.mass_node))
+    return spec
