@@ -245,9 +245,9 @@ class InternalForce:
         check(lib().fx_force_set_path(self._h, self.PATHS[path]))
 
     def info(self) -> dict:
-        s = (C.c_int64 * 8)()
+        s = (C.c_int64 * 9)()
         check(lib().fx_force_info(self._h, s))
-        keys = ("num_equations", "num_elements", "path", "box_qualifies", "nx", "ny", "nz", "device_bytes")
+        keys = ("num_equations", "num_elements", "path", "box_qualifies", "nx", "ny", "nz", "device_bytes", "box_force")
         d = dict(zip(keys, [int(v) for v in s]))
         d["path"] = {1: "general", 2: "box"}[d["path"]]
         return d

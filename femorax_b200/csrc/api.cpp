@@ -346,6 +346,7 @@ int fx_force_info(const fx_force* f, int64_t* info) {
     info[5] = s.box.ny;
     info[6] = s.box.nz;
     info[7] = s.device_bytes();
+    info[8] = s.use_box_force();
   });
 }
 
@@ -420,7 +421,7 @@ int fx_force_compute(fx_force* f, const double* u, const double* v, double* out,
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || (u && v && out)), "fx_force_compute: bad arguments");
     auto st = static_cast<cudaStream_t>(stream);
-    if (f->s.use_box()) fx::box_force(f->s, u, v, out, st);
+    if (f->s.use_box_force()) fx::box_force(f->s, u, v, out, st);
     else fx::general_force(f->s, u, v, out, st);
   });
 }
@@ -428,7 +429,7 @@ int fx_force_compute(fx_force* f, const double* u, const double* v, double* out,
 int fx_force_compute_f32(fx_force* f, const float* u, const float* v, float* out, void* stream) {
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || (u && v && out)), "fx_force_compute_f32: bad arguments");
-    if (!f->s.use_box())
+    if (!f->s.use_box_force())
       throw fx::Error(FX_E_UNSUPPORTED, "the FP32 force runs on the box path only: " + f->s.box.why_not);
     fx::box_force_f32(f->s, u, v, out, static_cast<cudaStream_t>(stream));
   });

@@ -4,20 +4,27 @@
 // Element operator. On an axis-aligned box the Jacobian is constant and diagonal, and 2x2x2 Gauss
 // integrates the trilinear element's stiffness and consistent mass exactly, so the element
 // operator of the reference's Gauss-point form equals, up to rounding, the exact bilinear form
-// written in the Walsh-Hadamard (modal) basis of the 8 corner values: 1, xi, eta, zeta, xi eta,
-// ... In that basis the mass is diagonal and the stiffness is diagonal plus 24 couplings, so one
-// element costs 3 x 24 butterflies forward, 24 products, 24 fused couplings and 3 x 24
-// butterflies back: about 190 FP64 operations instead of several thousand.
+// written in the Walsh-Hadamard (modal) basis of the 8 corner values (1, xi, eta, zeta, xi eta,
+// ...). In that basis the mass (consistent, or lumped since H^T H = 8 I) is diagonal and the
+// stiffness is diagonal plus 24 couplings.
 //
-// Scatter. Each CTA owns a (BX-1) x (BY-1) column of grid nodes over kz node planes and sweeps up
-// the planes: it stages a plane of x (with a one-node halo) in shared memory, evaluates the
-// BX x BY element columns around its nodes (the halo elements are evaluated by both neighbours:
-// no atomics, no cross-CTA exchange), keeps the element values in shared memory and gives each
-// owned node the sum of its eight element values in a fixed order. Every equation is written
-// once, by its owner, in a fixed order: deterministic, and y needs no zeroing.
+// The transform is split by axis. An element column sweeps up the grid, so the 2D transform of
+// the face it shares with the element above is computed once and kept in registers; the two faces'
+// transforms give the element's modes with 24 butterflies; the modal operator is 24 products and
+// 24 fused couplings; the result is split back into a bottom and a top face; the bottom face is
+// added (in modal form) to the top face left by the element below, and one 2D inverse transform
+// gives the four corner values of the face. About 160 FP64 operations per element.
+//
+// Scatter. Each CTA owns a (BX-1) x (BY-1) column of grid nodes over kz node planes. Per plane it
+// stages the node values of the plane above (one-node halo) in shared memory, evaluates the BX x BY
+// element columns around its nodes (halo columns are evaluated by both neighbouring CTAs: no
+// atomics, no cross-CTA exchange), and gives each owned node the sum of the face corner values of
+// its four columns in a fixed order. Every equation is written once, by its owner, in a fixed
+// order: deterministic for any launch shape, and y needs no zeroing. The plane values are read into
+// registers one plane (equations: two planes) ahead, so global latency overlaps the element work;
+// two barriers per plane.
 #include <algorithm>
 #include <cmath>
-#include <map>
 
 #include "force.hpp"
 
@@ -25,23 +32,22 @@ namespace fx {
 
 namespace {
 
-// corner c = i + 2j + 4k (lexicographic) -> stdBrick local node
-__host__ __device__ constexpr int lex_to_local(int c) {
-  return c == 0 ? 0 : c == 1 ? 1 : c == 2 ? 3 : c == 3 ? 2 : c == 4 ? 4 : c == 5 ? 5 : c == 6 ? 7 : 6;
-}
+constexpr int kParamsInShared = 16;  // coefficient tables of up to this many parameter sets in shared memory
 
 template <class T>
 struct BoxArgs {
   int nx, ny, nz, kz;
+  int nparams;
   const int32_t* __restrict__ node_eq;
   const int32_t* __restrict__ elem_param;
   const void* __restrict__ coef;  // BoxCoef or BoxCoef32
   const T* __restrict__ x;        // apply: x; force: u
   const T* __restrict__ v;        // force: v
   T* __restrict__ y;
-  const double* __restrict__ nm1;  // nodal mass (apply: k.mass) or NULL
-  const double* __restrict__ nm2;  // nodal alpha mass (apply: k.damping; force: 1) or NULL
+  const double* __restrict__ nm1;  // apply: nodal mass (with c1 = k.mass) or NULL
+  const double* __restrict__ nm2;  // apply: nodal alpha mass (c2 = k.damping); force: lumped alphaM masses
   double c1, c2;
+  T beta;           // force: u + beta v
   const int* skip;  // when set and nonzero on the device, the launch does nothing (a finished solve)
 };
 
@@ -56,54 +62,29 @@ struct Coef<float> {
   using type = BoxCoef32;
 };
 
-// Unnormalised Walsh-Hadamard transform of 8 corner values (lexicographic), in place:
-// for each axis bit b: (v_i, v_{i+b}) -> (v_i + v_{i+b}, v_{i+b} - v_i).
-template <class T>
-__device__ __forceinline__ void wht_fwd(T v[8]) {
-#pragma unroll
-  for (int b = 1; b < 8; b <<= 1)
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-      if (!(i & b)) {
-        const T a = v[i], c = v[i + b];
-        v[i] = a + c;
-        v[i + b] = c - a;
-      }
-}
-// Its transpose: (g_i, g_{i+b}) -> (g_i - g_{i+b}, g_i + g_{i+b}).
-template <class T>
-__device__ __forceinline__ void wht_bwd(T v[8]) {
-#pragma unroll
-  for (int b = 4; b >= 1; b >>= 1)
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-      if (!(i & b)) {
-        const T a = v[i], c = v[i + b];
-        v[i] = a - c;
-        v[i + b] = a + c;
-      }
-}
-
-// The modal element operator: t[c][m] (transformed corner values of component c) -> g[c][m].
-// Axis pairs (c, d, e): (0,1,2), (1,2,0), (2,0,1); for r in {0,1}: modes a = bit c + r bit e,
-// b = bit d + r bit e; lambda couples (c,a)<->(d,b), mu couples (c,b)<->(d,a).
+// Row block `d` of the modal operator: g[m] (output component d) from the modes t of all three
+// components. Axis pairs (c0, c1, e): (0,1,2), (1,2,0), (2,0,1); for r in {0,1}: modes
+// a = bit c0 + r bit e, b = bit c1 + r bit e; lambda couples (c0,a)<->(c1,b), mu couples
+// (c0,b)<->(c1,a). d is a compile-time constant after unrolling, so the branches vanish.
 template <class T, class C>
-__device__ __forceinline__ void modal_apply(const C& k, const T t[3][8], T g[3][8]) {
+__device__ __forceinline__ void modal_row(const C& k, const T t[3][8], int d, T g[8]) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int m = 0; m < 8; ++m) g[c][m] = T(k.dkm[c][m]) * t[c][m];
+  for (int m = 0; m < 8; ++m) g[m] = T(k.dkm[d][m]) * t[d][m];
 #pragma unroll
   for (int pr = 0; pr < 3; ++pr) {
-    const int c = pr, d = (pr + 1) % 3, e = (pr + 2) % 3;
+    const int c0 = pr, c1 = (pr + 1) % 3, e = (pr + 2) % 3;
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      const int ma = (1 << c) | (r << e), mb = (1 << d) | (r << e);
+      const int ma = (1 << c0) | (r << e), mb = (1 << c1) | (r << e);
       const T kl = T(k.kap[pr * 4 + r * 2 + 0]), km = T(k.kap[pr * 4 + r * 2 + 1]);
-      g[d][mb] = fma(kl, t[c][ma], g[d][mb]);
-      g[c][ma] = fma(kl, t[d][mb], g[c][ma]);
-      g[d][ma] = fma(km, t[c][mb], g[d][ma]);
-      g[c][mb] = fma(km, t[d][ma], g[c][mb]);
+      if (d == c1) {
+        g[mb] = fma(kl, t[c0][ma], g[mb]);
+        g[ma] = fma(km, t[c0][mb], g[ma]);
+      }
+      if (d == c0) {
+        g[ma] = fma(kl, t[c1][mb], g[ma]);
+        g[mb] = fma(km, t[c1][ma], g[mb]);
+      }
     }
   }
 }
@@ -119,22 +100,36 @@ __device__ __forceinline__ T load_dof(const T* __restrict__ x, int32_t packed, i
 template <int BX, int BY, class T, int MODE>
 struct Smem {
   static constexpr int NT = BX * BY, SX = BX + 1, SY = BY + 1, NS = SX * SY;
-  static constexpr int NV = MODE == 1 ? 2 : 1;  // staged vectors: x (apply) or u, v (force)
-  static constexpr size_t bytes = sizeof(T) * (24 * NT + 2 * 3 * NS * NV) + sizeof(int32_t) * 2 * NS;
+  // MODE 0 stages planes asynchronously into a ring of three; MODE 1 through registers into two
+  static constexpr int NB = MODE == 0 ? 3 : 2;
+  static constexpr size_t coef_bytes = sizeof(typename Coef<T>::type) * kParamsInShared;
+  static constexpr size_t bytes = coef_bytes + sizeof(T) * (12 * NT + NB * 3 * NS) + sizeof(int32_t) * NB * NS;
 };
 
-// MODE 0: y = K_eff x (+ nodal masses). MODE 1: f = K (u + beta v) + alphaM M v - body
-// (+ nodal alphaM masses times v). CONSISTENT: the modal mass term (else lumped, nodal space).
-template <int BX, int BY, class T, int MODE, bool CONSISTENT>
-__global__ void __launch_bounds__(BX* BY) k_box(BoxArgs<T> a) {
+__device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, int bytes, bool valid) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int src = valid ? bytes : 0;  // 0: the destination is filled with zeros, nothing is read
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// MODE 0: y = K_eff x (+ k.mass nodal masses x + k.damping nodal alphaM masses x).
+// MODE 1: f = K (u + beta v) - body + la v (la: lumped alphaM masses, element and nodal).
+// MINB: CTAs per SM the register budget is sized for.
+template <int BX, int BY, class T, int MODE, int MINB>
+__global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   using S = Smem<BX, BY, T, MODE>;
   using CT = typename Coef<T>::type;
-  constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NV = S::NV;
+  constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* ys = reinterpret_cast<T*>(smem_raw);  // [24][NT]: element values, (corner, component) major
-  T* xs = ys + 24 * NT;                    // [2 planes][NV][3][NS]
-  int32_t* es = reinterpret_cast<int32_t*>(xs + 2 * 3 * NS * NV);  // [2][NS]
-  const CT* __restrict__ coef = reinterpret_cast<const CT*>(a.coef);
+  CT* cs = reinterpret_cast<CT*>(smem_raw);
+  T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [4 corners][3][NT]: face corner values
+  T* xs = ys + 12 * NT;                                     // [NB planes][3][NS]: staged node values
+  int32_t* es = reinterpret_cast<int32_t*>(xs + NB * 3 * NS);  // [NB][NS]: staged equations
   if (a.skip && *a.skip) return;
 
   const int t = threadIdx.x;
@@ -145,174 +140,270 @@ __global__ void __launch_bounds__(BX* BY) k_box(BoxArgs<T> a) {
   const int NXn = a.nx + 1, NYn = a.ny + 1;
   const int ei = i0 - 1 + ci, ej = j0 - 1 + cj;
   const bool col_ok = ei >= 0 && ei < a.nx && ej >= 0 && ej < a.ny;
-  const int gi = i0 + ci, gj = j0 + cj;
-  const bool own = ci < BX - 1 && cj < BY - 1 && gi < NXn && gj < NYn;
+  const bool own = ci < BX - 1 && cj < BY - 1 && i0 + ci < NXn && j0 + cj < NYn;
+  const int s00 = ci + cj * SX;  // staging slot of the column's corner (0, 0)
 
-  auto stage = [&](int k, int b) {
-    for (int s = t; s < NS; s += NT) {
-      const int si = s % SX, sj = s / SX;
-      const int ni = i0 - 1 + si, nj = j0 - 1 + sj;
+  // coefficient tables in shared memory (few parameter sets) or read through L1
+  const bool shared_coef = a.nparams <= kParamsInShared;
+  if (shared_coef) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(a.coef);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(cs);
+    const int words = a.nparams * static_cast<int>(sizeof(CT) / 4);
+    for (int w = t; w < words; w += NT) dst[w] = __ldg(&src[w]);
+  }
+  const CT* coef = shared_coef ? cs : reinterpret_cast<const CT*>(a.coef);
+
+  // ---- staging: equations two planes ahead in registers; values one plane ahead
+  constexpr int SPT = (NS + NT - 1) / NT;
+  int32_t pk_next[SPT], pk_cur[SPT];
+  T px[MODE == 1 ? SPT : 1][3];
+  auto load_packed = [&](int k, int32_t (&out)[SPT]) {
+#pragma unroll
+    for (int j = 0; j < SPT; ++j) {
+      const int s = t + j * NT;
+      const int ni = i0 - 1 + s % SX, nj = j0 - 1 + s / SX;
       int32_t packed = 0;
-      if (k >= 0 && k <= a.nz && ni >= 0 && ni < NXn && nj >= 0 && nj < NYn)
-        packed = a.node_eq[(static_cast<int64_t>(k) * NYn + nj) * NXn + ni];
+      if (s < NS && k >= 0 && k <= a.nz && ni >= 0 && ni < NXn && nj >= 0 && nj < NYn)
+        packed = __ldg(&a.node_eq[(static_cast<int64_t>(k) * NYn + nj) * NXn + ni]);
+      out[j] = packed;
+    }
+  };
+  // MODE 0: copies into buffer b go out now and land by the next cp_async_wait_all
+  auto issue = [&](int b, const int32_t (&pk)[SPT]) {
+#pragma unroll
+    for (int j = 0; j < SPT; ++j) {
+      const int s = t + j * NT;
+      if (s >= NS) continue;
+      const int32_t packed = pk[j];
       es[b * NS + s] = packed;
+      const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
+      const int32_t base = packed & 0x1FFFFFFF;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) xs[((b * NV + 0) * 3 + d) * NS + s] = load_dof(a.x, packed, d);
-      if (MODE == 1) {
+      for (int d = 0; d < 3; ++d) {
+        const bool free_dof = (mask >> d) & 1u;
+        const T* src = free_dof ? a.x + base + __popc(mask & ((1u << d) - 1u)) : a.x;
+        cp_async_zfill(&xs[(b * 3 + d) * NS + s], src, sizeof(T), free_dof);
+      }
+    }
+    cp_async_commit();
+  };
+  // MODE 1: u + beta v into registers, then into buffer b once it is free
+  auto load_values = [&](const int32_t (&pk)[SPT]) {
+    if constexpr (MODE == 1) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) xs[((b * NV + 1) * 3 + d) * NS + s] = load_dof(a.v, packed, d);
+      for (int j = 0; j < SPT; ++j)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) px[j][d] = fma(a.beta, load_dof(a.v, pk[j], d), load_dof(a.x, pk[j], d));
+    }
+  };
+  auto commit = [&](int b, const int32_t (&pk)[SPT]) {
+    if constexpr (MODE == 1) {
+#pragma unroll
+      for (int j = 0; j < SPT; ++j) {
+        const int s = t + j * NT;
+        if (s >= NS) continue;
+        es[b * NS + s] = pk[j];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xs[(b * 3 + d) * NS + s] = px[j][d];
       }
     }
   };
-
-  T acc[3] = {T(0), T(0), T(0)};
-  int buf = 0;
-  stage(k0 - 1, 0);
-  for (int ek = k0 - 1; ek < k1; ++ek) {
-    stage(ek + 1, buf ^ 1);
-    __syncthreads();
-    // ---- element (ei, ej, ek)
-    T out[8][3];
-    if (col_ok && ek >= 0 && ek < a.nz) {
-      const CT& k = coef[a.elem_param[(static_cast<int64_t>(ek) * a.ny + ej) * a.nx + ei]];
-      T tv[3][8];
-      T vv[3][8];
+  auto param_of = [&](int ek) {
+    return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.elem_param[(static_cast<int64_t>(ek) * a.ny + ej) * a.nx + ei])
+                                            : -1;
+  };
+  // 2D transform of the column's face in staging buffer b: f = p + 2q (p: x mode, q: y mode)
+  // (written to f[d * stride + 0..3])
+  auto face = [&](int b, T* f, const int stride) {
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int pb = (c & 4) ? (buf ^ 1) : buf;
-        const int s = (ci + (c & 1)) + (cj + ((c >> 1) & 1)) * SX;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const T xv = xs[((pb * NV + 0) * 3 + d) * NS + s];
-          if (MODE == 1) {
-            const T vd = xs[((pb * NV + 1) * 3 + d) * NS + s];
-            vv[d][c] = vd;
-            tv[d][c] = fma(T(k.beta), vd, xv);
-          } else {
-            tv[d][c] = xv;
-            vv[d][c] = xv;
-          }
-        }
-      }
-      T g[3][8];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) wht_fwd(tv[d]);
-      modal_apply(k, tv, g);
-      if (MODE == 1 && CONSISTENT) {  // alphaM times the consistent mass, on v
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          T mv[8];
-#pragma unroll
-          for (int c = 0; c < 8; ++c) mv[c] = vv[d][c];
-          wht_fwd(mv);
-#pragma unroll
-          for (int m = 0; m < 8; ++m) g[d][m] = fma(T(k.dm[m]), mv[m], g[d][m]);
-        }
-      }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) wht_bwd(g[d]);
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          T val = g[d][c];
-          if (!CONSISTENT) val = fma(T(k.mL), vv[d][c], val);  // lumped mass (apply: x; force: v)
-          if (MODE == 1) val -= T(k.body[d]);
-          out[c][d] = val;
-        }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) out[c][d] = T(0);
+    for (int d = 0; d < 3; ++d) {
+      const T* p = xs + (b * 3 + d) * NS + s00;
+      const T a00 = p[0], a10 = p[1], a01 = p[SX], a11 = p[SX + 1];
+      const T s0 = a00 + a10, d0 = a10 - a00, s1 = a01 + a11, d1 = a11 - a01;
+      f[d * stride + 0] = s0 + s1;
+      f[d * stride + 1] = d0 + d1;
+      f[d * stride + 2] = s1 - s0;
+      f[d * stride + 3] = d1 - d0;
     }
+  };
+
+  // prologue: planes k0 - 1 (bottom of the first element plane) and k0 staged; equations of
+  // k0 + 1 in registers
+  if constexpr (MODE == 0) {
+    load_packed(k0 - 1, pk_cur);
+    issue(0, pk_cur);
+    load_packed(k0, pk_cur);
+    issue(1, pk_cur);
+    cp_async_wait_all();
+  } else {
+    load_packed(k0 - 1, pk_cur);
+    load_values(pk_cur);
+    commit(0, pk_cur);
+    load_packed(k0, pk_cur);
+    load_values(pk_cur);
+    commit(1, pk_cur);
+  }
+  load_packed(k0 + 1, pk_next);
+  int p_cur = param_of(k0 - 1), p_nxt = param_of(k0);
+  __syncthreads();
+  T fb[3][4], facc[3][4];
+  face(0, &fb[0][0], 4);
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
+  for (int d = 0; d < 3; ++d)
 #pragma unroll
-      for (int d = 0; d < 3; ++d) ys[(c * 3 + d) * NT + t] = out[c][d];
-    __syncthreads();
-    // ---- owned node (gi, gj): element columns (ci,cj) (node is its corner i=1,j=1),
-    // (ci+1,cj) (i=0,j=1), (ci,cj+1) (i=1,j=0), (ci+1,cj+1) (i=0,j=0)
-    if (own) {
-      const int tA = ci + cj * BX, tB = tA + 1, tC = tA + BX, tD = tA + BX + 1;
-      if (ek >= k0) {
-        const int s = (ci + 1) + (cj + 1) * SX;
-        const int32_t packed = es[buf * NS + s];
-        const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
-        const int32_t base = packed & 0x1FFFFFFF;
+    for (int f = 0; f < 4; ++f) facc[d][f] = T(0);
+  // buffers: plane ek in bb, plane ek + 1 in tb, plane ek + 2 goes to nb
+  int bb = 0, tb = 1, nb = 2 % NB;
+
+  for (int ek = k0 - 1; ek < k1; ++ek) {
+    // issue the values of plane ek + 2, the equations of plane ek + 3, the parameters of ek + 2
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          T val = acc[d];
-          val += ys[(3 * 3 + d) * NT + tA];
-          val += ys[(2 * 3 + d) * NT + tB];
-          val += ys[(1 * 3 + d) * NT + tC];
-          val += ys[(0 * 3 + d) * NT + tD];
-          if ((mask >> d) & 1u) {
-            const int32_t q = base + __popc(mask & ((1u << d) - 1u));
-            if (a.nm1) val += T(a.c1 * a.nm1[q]) * xs[((buf * NV + 0) * 3 + d) * NS + s];
-            if (a.nm2) val += T(a.c2 * a.nm2[q]) * xs[((buf * NV + (MODE == 1 ? 1 : 0)) * 3 + d) * NS + s];
-            a.y[q] = val;
-          }
-        }
+    for (int j = 0; j < SPT; ++j) pk_cur[j] = pk_next[j];
+    if constexpr (MODE == 0) issue(nb, pk_cur);
+    else load_values(pk_cur);
+    load_packed(ek + 3, pk_next);
+    const int p_here = p_cur;
+    p_cur = p_nxt;
+    p_nxt = param_of(ek + 2);
+    // what the node phase of plane ek reads from plane ek's staging (MODE 1 replaces it below)
+    const bool out_plane = own && ek >= k0;
+    int32_t own_packed = 0;
+    T own_x[3] = {T(0), T(0), T(0)};
+    if (out_plane) {
+      const int s = s00 + SX + 1;
+      own_packed = es[bb * NS + s];
+      if (MODE == 0 && (a.nm1 || a.nm2)) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) own_x[d] = xs[(bb * 3 + d) * NS + s];
       }
+    }
+    // ---- element (ei, ej, ek): modes from the top face (transformed here) and the bottom face
+    // (kept from the plane below); fb takes the top face in place
+    T tv[3][8];
+    face(tb, &tv[0][0], 8);  // top face into tv[.][0..3]
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const T top = tv[d][f], bot = fb[d][f];
+        tv[d][f] = top + bot;
+        tv[d][f + 4] = top - bot;
+        fb[d][f] = top;
+      }
+    if (p_here >= 0) {
+      const CT& k = coef[p_here];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        T val = ys[(7 * 3 + d) * NT + tA];
-        val += ys[(6 * 3 + d) * NT + tB];
-        val += ys[(5 * 3 + d) * NT + tC];
-        val += ys[(4 * 3 + d) * NT + tD];
-        acc[d] = val;
+        T g[8];
+        modal_row(k, tv, d, g);
+        if (MODE == 1) g[0] -= T(k.body[d]);
+        T h[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          h[f] = facc[d][f] + (g[f] - g[f + 4]);  // bottom face, plus the element below's top face
+          facc[d][f] = g[f] + g[f + 4];            // top face, for the plane above
+        }
+        // inverse 2D transform of the face: corners c = i + 2j
+        const T u0 = h[0] - h[2], u2 = h[0] + h[2], u1 = h[1] - h[3], u3 = h[1] + h[3];
+        ys[(0 * 3 + d) * NT + t] = u0 - u1;
+        ys[(1 * 3 + d) * NT + t] = u0 + u1;
+        ys[(2 * 3 + d) * NT + t] = u2 - u3;
+        ys[(3 * 3 + d) * NT + t] = u2 + u3;
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const T u0 = facc[d][0] - facc[d][2], u2 = facc[d][0] + facc[d][2];
+        const T u1 = facc[d][1] - facc[d][3], u3 = facc[d][1] + facc[d][3];
+        ys[(0 * 3 + d) * NT + t] = u0 - u1;
+        ys[(1 * 3 + d) * NT + t] = u0 + u1;
+        ys[(2 * 3 + d) * NT + t] = u2 - u3;
+        ys[(3 * 3 + d) * NT + t] = u2 + u3;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) facc[d][f] = T(0);
       }
     }
     __syncthreads();
-    buf ^= 1;
+    // ---- owned node (i0 + ci, j0 + cj) of plane ek: corner (1,1) of column (ci,cj), (0,1) of
+    // (ci+1,cj), (1,0) of (ci,cj+1), (0,0) of (ci+1,cj+1)
+    if (out_plane) {
+      const int tA = t, tB = t + 1, tC = t + BX, tD = t + BX + 1;
+      const uint32_t mask = static_cast<uint32_t>(own_packed) >> 29;
+      const int32_t base = own_packed & 0x1FFFFFFF;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (!((mask >> d) & 1u)) continue;
+        T val = ys[(3 * 3 + d) * NT + tA];
+        val += ys[(2 * 3 + d) * NT + tB];
+        val += ys[(1 * 3 + d) * NT + tC];
+        val += ys[(0 * 3 + d) * NT + tD];
+        const int32_t q = base + __popc(mask & ((1u << d) - 1u));
+        if (MODE == 0) {
+          if (a.nm1) val += T(a.c1 * a.nm1[q]) * own_x[d];
+          if (a.nm2) val += T(a.c2 * a.nm2[q]) * own_x[d];
+        } else if (a.nm2) {
+          val += T(a.nm2[q]) * a.v[q];
+        }
+        a.y[q] = val;
+      }
+    }
+    if constexpr (MODE == 0) {
+      cp_async_wait_all();  // plane ek + 2 has landed (this thread's copies; the barrier: all)
+      bb = tb;
+      tb = nb;
+      nb = (nb + 1) % 3;
+    } else {
+      commit(bb, pk_cur);  // plane ek + 2 replaces plane ek
+      const int x = bb;
+      bb = tb;
+      tb = x;
+    }
+    __syncthreads();
   }
 }
 
 // ------------------------------------------------------------------ launch variants
-struct Variant {
-  int bx, by;
-};
-constexpr Variant kVariants[] = {{32, 8}, {16, 16}, {32, 4}, {64, 4}, {16, 8}, {32, 16}};
-constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+// (BX, BY, CTAs per SM for the register budget)
+constexpr int kNumVariants = 8;  // (32,8,2) (16,16,2) (32,4,2) (64,4,2) (16,8,2) (32,16,1) (32,8,1) (16,16,1)
 
-template <int BX, int BY, class T, int MODE, bool CONS>
+template <int BX, int BY, int MINB, class T, int MODE>
 void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   using S = Smem<BX, BY, T, MODE>;
   static bool configured = false;
   if (!configured) {
-    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, CONS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(S::bytes)));
     configured = true;
   }
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
-  k_box<BX, BY, T, MODE, CONS><<<grid, BX * BY, S::bytes, st>>>(a);
+  k_box<BX, BY, T, MODE, MINB><<<grid, BX * BY, S::bytes, st>>>(a);
   FX_LAUNCH_CHECK("box_operator");
-}
-
-template <class T, int MODE, bool CONS>
-void launch_variant(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
-  switch (p.variant) {
-    case 0: return launch_one<32, 8, T, MODE, CONS>(p, a, st);
-    case 1: return launch_one<16, 16, T, MODE, CONS>(p, a, st);
-    case 2: return launch_one<32, 4, T, MODE, CONS>(p, a, st);
-    case 3: return launch_one<64, 4, T, MODE, CONS>(p, a, st);
-    case 4: return launch_one<16, 8, T, MODE, CONS>(p, a, st);
-    default: return launch_one<32, 16, T, MODE, CONS>(p, a, st);
-  }
 }
 
 template <class T, int MODE>
 void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
-  if (p.consistent) launch_variant<T, MODE, true>(p, a, st);
-  else launch_variant<T, MODE, false>(p, a, st);
+  switch (p.variant) {
+    case 0: return launch_one<32, 8, 2, T, MODE>(p, a, st);
+    case 1: return launch_one<16, 16, 2, T, MODE>(p, a, st);
+    case 2: return launch_one<32, 4, 2, T, MODE>(p, a, st);
+    case 3: return launch_one<64, 4, 2, T, MODE>(p, a, st);
+    case 4: return launch_one<16, 8, 2, T, MODE>(p, a, st);
+    case 5: return launch_one<32, 16, 1, T, MODE>(p, a, st);
+    case 6: return launch_one<32, 8, 1, T, MODE>(p, a, st);
+    default: return launch_one<16, 16, 1, T, MODE>(p, a, st);
+  }
 }
 
 // ------------------------------------------------------------------ coefficients
-// Exact element operator on a box with sides h (see the file comment). J = hx hy hz / 8,
-// rho_d = 2 / h_d, w(0) = 2, w(1) = 2/3 (integrals of 1 and xi^2 over [-1, 1]).
-// mode 0 (apply): stiffness factor sk = cK + c0 + cc, mass factor sm = cM'.
-// mode 1 (force): stiffness factor 1 on u + beta v, mass factor alphaM on v, body force.
+// Exact element operator on a box with sides h. With J = hx hy hz / 8, rho_d = 2 / h_d, and
+// w(0) = 2, w(1) = 2/3 (integrals of 1 and xi^2 over [-1, 1]), for mode m of component c:
+//   diag = 2 J [ (lambda + mu) [m_c] rho_c^2 prod_{e != c} w(m_e)
+//                + mu sum_{d: m_d} rho_d^2 prod_{e != d} w(m_e) ] (stiffness)
+//          + rho J prod_e w(m_e) (consistent mass) or 8 rho J (lumped mass, H^T H = 8 I),
+// couplings 4 J rho_c0 rho_c1 w(r) lambda (resp. mu); all scaled by 1/64 for the two
+// unnormalised transforms. Apply: stiffness factor cK + c0 + cc (the elastic tangents are one
+// matrix), mass factor cM'. Force: stiffness factor 1 (on u + beta v), no mass (the lumped
+// alphaM masses act in nodal space), body force b J on mode 0.
 void build_coef(ForceState& s, int mode, const double k[3]) {
   BoxPlan& p = s.box;
   const double J = p.h[0] * p.h[1] * p.h[2] / 8.0;
@@ -324,21 +415,18 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
     const ParamGP& q = s.params_h[i];
     double l2m, lam, mu;
     lame(q, l2m, lam, mu);
-    double sk, sm;
+    double sk = 1.0, sm = 0.0;
     if (mode == 0) {
       const OpFactors f = op_factors(q, k[0], k[1], k[2]);
       sk = f.cK + f.c0 + f.cc;
       sm = f.cM;
-    } else {
-      sk = 1.0;
-      sm = q.alphaM;
     }
     const bool cons = q.mass_type == 0;
     BoxCoef c{};
     for (int comp = 0; comp < 3; ++comp)
       for (int m = 0; m < 8; ++m) {
-        double dk = 0.0;
         auto bit = [&](int d) { return (m >> d) & 1; };
+        double dk = 0.0;
         if (bit(comp)) {
           double pw = 1.0;
           for (int e = 0; e < 3; ++e)
@@ -353,34 +441,23 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
           dk += mu * rd[d] * rd[d] * pw;
         }
         dk *= 2.0 * J * sk;
-        double dm = 0.0;
-        if (cons) dm = sm * q.rho * J * w(bit(0)) * w(bit(1)) * w(bit(2));
-        if (mode == 0) {
-          c.dkm[comp][m] = (dk + dm) / 64.0;
-        } else {
-          c.dkm[comp][m] = dk / 64.0;
-          if (comp == 0) c.dm[m] = dm / 64.0;
-        }
+        const double dm = cons ? sm * q.rho * J * w(bit(0)) * w(bit(1)) * w(bit(2)) : 8.0 * sm * q.rho * J;
+        c.dkm[comp][m] = (dk + dm) / 64.0;
       }
     for (int pr = 0; pr < 3; ++pr) {
-      const int cc = pr, d = (pr + 1) % 3;
+      const int c0 = pr, c1 = (pr + 1) % 3;
       for (int r = 0; r < 2; ++r) {
-        const double base = 4.0 * J * rd[cc] * rd[d] * w(r) * sk / 64.0;
+        const double base = 4.0 * J * rd[c0] * rd[c1] * w(r) * sk / 64.0;
         c.kap[pr * 4 + r * 2 + 0] = base * lam;
         c.kap[pr * 4 + r * 2 + 1] = base * mu;
       }
     }
-    c.mL = cons ? 0.0 : sm * q.rho * J;
-    c.beta = mode == 1 ? q.betaK + q.betaKinit + q.betaKcomm : 0.0;
     for (int d = 0; d < 3; ++d) c.body[d] = mode == 1 ? q.b[d] * J : 0.0;
     h[i] = c;
     BoxCoef32& f = h32[i];
     for (int comp = 0; comp < 3; ++comp)
       for (int m = 0; m < 8; ++m) f.dkm[comp][m] = static_cast<float>(c.dkm[comp][m]);
     for (int j = 0; j < 12; ++j) f.kap[j] = static_cast<float>(c.kap[j]);
-    for (int j = 0; j < 8; ++j) f.dm[j] = static_cast<float>(c.dm[j]);
-    f.mL = static_cast<float>(c.mL);
-    f.beta = static_cast<float>(c.beta);
     for (int d = 0; d < 3; ++d) f.body[d] = static_cast<float>(c.body[d]);
     f.pad_ = 0.f;
   }
@@ -418,17 +495,13 @@ void box_build_plan(ForceState& s) {
   p.qualifies = false;
   auto no = [&](const std::string& why) { p.why_not = why; };
   if (s.count == 0) return no("no elements");
-  bool all_cons = true, all_lumped = true;
+  bool all_lumped = true;
   for (const auto& q : s.params_h) {
     if (q.kind != 0) return no("a parameter set is not elastic");
     if (q.mass_type == 0) all_lumped = false;
-    else all_cons = false;
   }
-  if (!all_cons && !all_lumped) return no("mixed consistent and lumped masses");
-  p.consistent = all_cons;
   const int32_t N = s.N, P = s.P;
   auto X = [&](int32_t n, int d) { return s.coords_h[static_cast<size_t>(d) * N + n]; };
-  // spacing from element 0
   double h[3];
   {
     const int32_t n0 = s.node_h[0], n1 = s.node_h[static_cast<size_t>(1) * P], n3 = s.node_h[static_cast<size_t>(3) * P],
@@ -517,6 +590,27 @@ void box_build_plan(ForceState& s) {
   }
   std::vector<int32_t> eparam(static_cast<size_t>(s.count));
   for (size_t c = 0; c < cell.size(); ++c) eparam[c] = s.param_h[cell[c]];
+  // force form: lumped masses and one beta
+  const double beta0 = s.params_h[0].betaK + s.params_h[0].betaKinit + s.params_h[0].betaKcomm;
+  bool one_beta = true;
+  for (const auto& q : s.params_h) one_beta = one_beta && (q.betaK + q.betaKinit + q.betaKcomm) == beta0;
+  p.force_ok = all_lumped && one_beta;
+  p.beta = beta0;
+  if (p.force_ok) {
+    // lumped alphaM masses per equation: alphaM_e rho_e J per element corner, then the nodal ones
+    const double J = h[0] * h[1] * h[2] / 8.0;
+    std::vector<double> la(static_cast<size_t>(s.neq), 0.0);
+    for (int32_t e = 0; e < s.count; ++e) {
+      const ParamGP& q = s.params_h[s.param_h[e]];
+      const double m = q.alphaM * q.rho * J;
+      for (int k = 0; k < 24; ++k) {
+        const int32_t eq = s.eq_h[static_cast<size_t>(k) * P + e];
+        if (eq >= 0) la[eq] += m;
+      }
+    }
+    for (size_t i = 0; i < s.nodal_alpha_h.size(); ++i) la[i] += s.nodal_alpha_h[i];
+    p.la.upload(la);
+  }
   p.nx = nx;
   p.ny = ny;
   p.nz = nz;
@@ -537,6 +631,7 @@ static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const 
   a.ny = s.box.ny;
   a.nz = s.box.nz;
   a.kz = s.box.kz;
+  a.nparams = s.nparams;
   a.node_eq = s.box.node_eq.ptr;
   a.elem_param = s.box.elem_param.ptr;
   a.coef = coef;
@@ -546,60 +641,49 @@ static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const 
   return a;
 }
 
+template <class T>
+static void apply_t(ForceState& s, const double k[3], const T* x, T* y, cudaStream_t st, const int* skip) {
+  ensure_coef(s, 0, k);
+  BoxArgs<T> a = args<T>(s, sizeof(T) == 8 ? static_cast<const void*>(s.box.coef.ptr) : s.box.coef32.ptr, x, nullptr, y);
+  a.skip = skip;
+  if (k[2] != 0.0 && s.has_nodal_mass) {
+    a.nm1 = s.nodal_mass.ptr;
+    a.c1 = k[2];
+  }
+  if (k[1] != 0.0 && s.has_nodal_alpha) {
+    a.nm2 = s.nodal_alpha_mass.ptr;
+    a.c2 = k[1];
+  }
+  launch<T, 0>(s.box, a, st);
+}
+
+template <class T>
+static void force_t(ForceState& s, const T* u, const T* v, T* f, cudaStream_t st) {
+  const double k1[3] = {1.0, 0.0, 0.0};
+  ensure_coef(s, 1, k1);
+  BoxArgs<T> a = args<T>(s, sizeof(T) == 8 ? static_cast<const void*>(s.box.coef.ptr) : s.box.coef32.ptr, u, v, f);
+  a.beta = static_cast<T>(s.box.beta);
+  a.nm2 = s.box.la.ptr;
+  launch<T, 1>(s.box, a, st);
+}
+
 void box_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
-  ensure_coef(s, 0, k);
-  BoxArgs<double> a = args<double>(s, s.box.coef.ptr, x, nullptr, y);
-  a.skip = skip;
-  if (k[2] != 0.0 && s.has_nodal_mass) {
-    a.nm1 = s.nodal_mass.ptr;
-    a.c1 = k[2];
-  }
-  if (k[1] != 0.0 && s.has_nodal_alpha) {
-    a.nm2 = s.nodal_alpha_mass.ptr;
-    a.c2 = k[1];
-  }
-  launch<double, 0>(s.box, a, st);
+  apply_t<double>(s, k, x, y, st, skip);
 }
-
 void box_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st, const int* skip) {
-  ensure_coef(s, 0, k);
-  BoxArgs<float> a = args<float>(s, s.box.coef32.ptr, x, nullptr, y);
-  a.skip = skip;
-  if (k[2] != 0.0 && s.has_nodal_mass) {
-    a.nm1 = s.nodal_mass.ptr;
-    a.c1 = k[2];
-  }
-  if (k[1] != 0.0 && s.has_nodal_alpha) {
-    a.nm2 = s.nodal_alpha_mass.ptr;
-    a.c2 = k[1];
-  }
-  launch<float, 0>(s.box, a, st);
+  apply_t<float>(s, k, x, y, st, skip);
 }
-
 void box_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
-  const double k1[3] = {1.0, 0.0, 0.0};
-  ensure_coef(s, 1, k1);
-  BoxArgs<double> a = args<double>(s, s.box.coef.ptr, u, v, f);
-  if (s.has_nodal_alpha) {
-    a.nm2 = s.nodal_alpha_mass.ptr;
-    a.c2 = 1.0;
-  }
-  launch<double, 1>(s.box, a, st);
+  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs lumped masses and one beta");
+  force_t<double>(s, u, v, f, st);
 }
-
 void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cudaStream_t st) {
-  const double k1[3] = {1.0, 0.0, 0.0};
-  ensure_coef(s, 1, k1);
-  BoxArgs<float> a = args<float>(s, s.box.coef32.ptr, u, v, f);
-  if (s.has_nodal_alpha) {
-    a.nm2 = s.nodal_alpha_mass.ptr;
-    a.c2 = 1.0;
-  }
-  launch<float, 1>(s.box, a, st);
+  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs lumped masses and one beta");
+  force_t<float>(s, u, v, f, st);
 }
 
-// Times every launch variant and a few plane counts on the operator (FP64, coefficients of a
-// unit stiffness) and keeps the fastest: CUDA events on the stream, median of 5 after 2 warm-ups.
+// Times every launch variant and plane count on the operator (FP64, unit stiffness) and keeps the
+// fastest: CUDA events on the stream, median of 5 after 2 warm-ups.
 void box_autotune(ForceState& s, cudaStream_t st) {
   if (!s.box.qualifies) return;
   DeviceArray<double> x, y;
@@ -612,16 +696,16 @@ void box_autotune(ForceState& s, cudaStream_t st) {
   FX_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int bv = 0, bk = 16;
-  const int kzs[] = {4, 8, 16, 32, 64};
+  const int kzs[] = {8, 16, 32, 64};
   for (int v = 0; v < kNumVariants; ++v)
     for (int kz : kzs) {
-      if (kz > s.box.nz + 1 && kz != 4) continue;
+      if (kz > 8 && kz >= 2 * (s.box.nz + 1)) continue;
       s.box.variant = v;
       s.box.kz = kz;
       std::vector<float> times;
       for (int r = 0; r < 7; ++r) {
         FX_CUDA(cudaEventRecord(e0, st));
-        box_apply(s, k, x.ptr, y.ptr, st);
+        box_apply(s, k, x.ptr, y.ptr, st, nullptr);
         FX_CUDA(cudaEventRecord(e1, st));
         FX_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;

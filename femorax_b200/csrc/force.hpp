@@ -17,21 +17,18 @@ namespace fx {
 // the current operator coefficients (box.cu builds them). Scaled by 1/64 where the two
 // Walsh-Hadamard transforms (unnormalised) would otherwise multiply the result by 64.
 struct BoxCoef {
-  double dkm[3][8];  // modal diagonal: stiffness + consistent mass, per component and mode
+  double dkm[3][8];  // modal diagonal: stiffness + mass (consistent, or lumped: H^T H = 8 I)
   double kap[12];    // couplings: per axis pair (xy, yz, zx) and r in {0,1}: lambda part, mu part
-  double dm[8];      // force mode, consistent mass: alphaM mass diagonal per mode (on v)
-  double mL;         // lumped-mass factor per corner (nodal space)
-  double beta;       // force mode: stiffness-proportional damping factor (u + beta v)
-  double body[3];    // force mode: body force per corner
+  double body[3];    // force mode: body force per corner (b J), on mode 0
   double pad_;
 };
-static_assert(sizeof(BoxCoef) == 50 * 8, "BoxCoef layout");
+static_assert(sizeof(BoxCoef) == 40 * 8, "BoxCoef layout");
 
 struct BoxCoef32 {  // the same in FP32 for the mixed-precision operator
   float dkm[3][8];
   float kap[12];
-  float dm[8];
-  float mL, beta, body[3], pad_;
+  float body[3];
+  float pad_;
 };
 
 // A structured grid of axis-aligned boxes with equal spacing: (nx, ny, nz) elements.
@@ -40,7 +37,12 @@ struct BoxPlan {
   std::string why_not;
   int nx = 0, ny = 0, nz = 0;
   double h[3] = {0, 0, 0};
-  bool consistent = false;  // every parameter set has the consistent mass (else all lumped)
+  // The force (explicit) form runs here when every parameter set has the lumped mass and one
+  // stiffness-proportional damping factor beta (then f = K (u + beta v) - body + la v, la the
+  // lumped alphaM masses); otherwise the general path evaluates the force.
+  bool force_ok = false;
+  double beta = 0.0;
+  DeviceArray<double> la;  // [neq] lumped alphaM masses (element and nodal), force form
   DeviceArray<int32_t> node_eq;     // [(nz+1)(ny+1)(nx+1)]: first free equation | free-DOF mask << 29
   DeviceArray<int32_t> elem_param;  // [nz ny nx]: parameter set of each element
   DeviceArray<int32_t> node_of;     // host-side check only: grid node -> internal node
@@ -89,6 +91,7 @@ struct ForceState {
   int64_t plastic_points = 0;
   ExplicitWork xw;
   bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
+  bool use_box_force() const { return use_box() && box.force_ok; }
   int64_t device_bytes() const;
 };
 

@@ -190,7 +190,7 @@ void explicit_run(fx_force* f, const T* mass, int32_t dir, const double* ag_host
   ForceState& s = f->s;
   if (steps < 0 || !(dt > 0.0)) throw Error(FX_E_INVALID, "fx_explicit_run: steps >= 0 and dt > 0 required");
   if (ag_host && (dir < 0 || dir > 2)) throw Error(FX_E_INVALID, "fx_explicit_run: dir must be 0, 1 or 2");
-  if (sizeof(T) == 4 && !s.use_box()) throw Error(FX_E_UNSUPPORTED, "the FP32 explicit step runs on the box path only");
+  if (sizeof(T) == 4 && !s.use_box_force()) throw Error(FX_E_UNSUPPORTED, "the FP32 explicit step runs on the box path only");
   ExplicitWork& w = work_of(f);
   const int64_t n = s.neq;
   if (w.step.n == 0) w.step.alloc(1);
@@ -215,7 +215,7 @@ void explicit_run(fx_force* f, const T* mass, int32_t dir, const double* ag_host
   const double* agp = ag_host ? w.ag.ptr : nullptr;
   auto one_step = [&](int predict) {
     if constexpr (sizeof(T) == 8) {
-      if (s.use_box()) box_force(s, u, vh, fbuf, st);
+      if (s.use_box_force()) box_force(s, u, vh, fbuf, st);
       else general_force(s, u, vh, fbuf, st);
     } else {
       box_force_f32(s, u, vh, fbuf, st);

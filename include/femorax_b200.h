@@ -146,8 +146,8 @@ typedef struct fx_force fx_force;
 int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out);
 void fx_force_destroy(fx_force* f);
 int fx_force_set_path(fx_force* f, int32_t path);
-/* info[8] = num_equations, num_elements, path in use, box qualifies (0/1), grid nx, ny, nz,
- * device bytes held. */
+/* info[9] = num_equations, num_elements, path of the operator, box qualifies (0/1), grid nx, ny,
+ * nz, device bytes held, force form on the box path (0/1: lumped masses and one beta). */
 int fx_force_info(const fx_force* f, int64_t* info);
 /* Box path launch shape: variant (block of element columns) and kz (node planes per CTA);
  * fx_force_tune times the candidates on the device and keeps the fastest (the autotuner

@@ -132,6 +132,10 @@ def test_box_path_fp32(case):
     y = torch.zeros(mesh.num_equations, dtype=torch.float32, device=DEV)
     force.apply_operator(fx.OperatorCoefficients(*k), t(x, torch.float32), y)
     assert rel_err(y.cpu().numpy().astype(np.float64), port.apply_operator(k, x)) <= TOL_F32
+    if not force.info()["box_force"]:
+        with pytest.raises(fx.FxError):
+            force.compute(t(x, torch.float32), t(x, torch.float32), y)
+        return
     u = np.random.default_rng(12).standard_normal(mesh.num_equations) * 1e-3
     v = np.random.default_rng(13).standard_normal(mesh.num_equations) * 1e-2
     f = torch.zeros(mesh.num_equations, dtype=torch.float32, device=DEV)
@@ -169,7 +173,7 @@ def test_launch_variants_agree(oracle_mod):
     from femorax_b200 import _lib as L
     import ctypes as C
     lib = L.lib()
-    for variant in range(6):
+    for variant in range(8):
         for kz in (1, 3, 8, 64):
             lib_rc = lib.fx_force_set_launch(force._h, variant, kz) if hasattr(lib, "fx_force_set_launch") else None
             if lib_rc is None:
