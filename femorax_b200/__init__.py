@@ -96,7 +96,10 @@ class Model:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().fx_model_destroy(h)
+            try:
+                lib().fx_model_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
             self._h = None
 
 
@@ -146,7 +149,10 @@ class Compiled:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().fx_compiled_destroy(h)
+            try:
+                lib().fx_compiled_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
             self._h = None
 
 
@@ -298,7 +304,10 @@ class InternalForce:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().fx_force_destroy(h)
+            try:
+                lib().fx_force_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
             self._h = None
 
 
@@ -374,7 +383,10 @@ class LinearSolver:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().fx_solver_destroy(h)
+            try:
+                lib().fx_solver_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
             self._h = None
 
 
@@ -419,5 +431,8 @@ class VectorOps:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().fx_vops_destroy(h)
+            try:
+                lib().fx_vops_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
             self._h = None

@@ -100,10 +100,12 @@ __device__ __forceinline__ T load_dof(const T* __restrict__ x, int32_t packed, i
 template <int BX, int BY, class T, int MODE>
 struct Smem {
   static constexpr int NT = BX * BY, SX = BX + 1, SY = BY + 1, NS = SX * SY;
-  // MODE 0 stages planes asynchronously into a ring of three; MODE 1 through registers into two
-  static constexpr int NB = MODE == 0 ? 3 : 2;
+  // Planes are gathered D planes ahead; their equations D + 2 planes ahead; the ring holds D + 3.
+  static constexpr int D = 4, NB = D + 3;
+  static constexpr int NV = MODE == 1 ? 2 : 1;  // staged vectors: x, or u and v
   static constexpr size_t coef_bytes = sizeof(typename Coef<T>::type) * kParamsInShared;
-  static constexpr size_t bytes = coef_bytes + sizeof(T) * (12 * NT + NB * 3 * NS) + sizeof(int32_t) * NB * NS;
+  static constexpr size_t bytes =
+      coef_bytes + sizeof(T) * (12 * NT + NB * NV * 3 * NS) + sizeof(int32_t) * NB * NS;
 };
 
 __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, int bytes, bool valid) {
@@ -115,21 +117,64 @@ __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, int
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// n values from 16-byte aligned coefficient storage, two (double) or four (float) per load
+template <int N>
+__device__ __forceinline__ void load_coef(const double* __restrict__ src, double* dst) {
+#pragma unroll
+  for (int i = 0; i < N / 2; ++i) {
+    const double2 v = reinterpret_cast<const double2*>(src)[i];
+    dst[2 * i] = v.x;
+    dst[2 * i + 1] = v.y;
+  }
+}
+template <int N>
+__device__ __forceinline__ void load_coef(const float* __restrict__ src, float* dst) {
+#pragma unroll
+  for (int i = 0; i < N / 4; ++i) {
+    const float4 v = reinterpret_cast<const float4*>(src)[i];
+    dst[4 * i] = v.x;
+    dst[4 * i + 1] = v.y;
+    dst[4 * i + 2] = v.z;
+    dst[4 * i + 3] = v.w;
+  }
+}
+__device__ __forceinline__ void load_pair(const double* __restrict__ src, double& a, double& b) {
+  const double2 v = *reinterpret_cast<const double2*>(src);
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void load_pair(const float* __restrict__ src, float& a, float& b) {
+  const float2 v = *reinterpret_cast<const float2*>(src);
+  a = v.x;
+  b = v.y;
+}
 
 // MODE 0: y = K_eff x (+ k.mass nodal masses x + k.damping nodal alphaM masses x).
 // MODE 1: f = K (u + beta v) - body + la v (la: lumped alphaM masses, element and nodal).
-// MINB: CTAs per SM the register budget is sized for.
-template <int BX, int BY, class T, int MODE, int MINB>
+// MINB: CTAs per SM the register budget is sized for. CACHE: keep the bottom face's transform
+// in registers from the plane below (fewer operations, more registers) or transform it again
+// from the staged plane (fewer registers, more resident warps).
+//
+// Staging ring (all copies asynchronous, each thread owns fixed slots of a plane): in the
+// iteration of element plane ek a thread copies the equations of its slots of plane ek + D + 2
+// and, from the equations it copied two iterations before, the node values of plane ek + D;
+// one commit group per iteration; waiting for all but the newest group at the end of the
+// iteration leaves planes up to ek + D + 1 (equations) and ek + D - 1 (values) landed.
+template <int BX, int BY, class T, int MODE, int MINB, bool CACHE>
 __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   using S = Smem<BX, BY, T, MODE>;
   using CT = typename Coef<T>::type;
-  constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB;
+  constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB, NV = S::NV, D = S::D;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* cs = reinterpret_cast<CT*>(smem_raw);
   T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [4 corners][3][NT]: face corner values
-  T* xs = ys + 12 * NT;                                     // [NB planes][3][NS]: staged node values
-  int32_t* es = reinterpret_cast<int32_t*>(xs + NB * 3 * NS);  // [NB][NS]: staged equations
+  T* xs = ys + 12 * NT;                                     // [NB planes][NV][3][NS]: node values
+  int32_t* es = reinterpret_cast<int32_t*>(xs + NB * NV * 3 * NS);  // [NB][NS]: equations
   if (a.skip && *a.skip) return;
 
   const int t = threadIdx.x;
@@ -138,6 +183,7 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   const int k0 = blockIdx.z * a.kz;
   const int k1 = min(k0 + a.kz, a.nz + 1);
   const int NXn = a.nx + 1, NYn = a.ny + 1;
+  const int64_t plane_stride = static_cast<int64_t>(NXn) * NYn;
   const int ei = i0 - 1 + ci, ej = j0 - 1 + cj;
   const bool col_ok = ei >= 0 && ei < a.nx && ej >= 0 && ej < a.ny;
   const bool own = ci < BX - 1 && cj < BY - 1 && i0 + ci < NXn && j0 + cj < NYn;
@@ -153,72 +199,64 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   }
   const CT* coef = shared_coef ? cs : reinterpret_cast<const CT*>(a.coef);
 
-  // ---- staging: equations two planes ahead in registers; values one plane ahead
+  // ---- staging slots of this thread (fixed for the whole sweep)
   constexpr int SPT = (NS + NT - 1) / NT;
-  int32_t pk_next[SPT], pk_cur[SPT];
-  T px[MODE == 1 ? SPT : 1][3];
-  auto load_packed = [&](int k, int32_t (&out)[SPT]) {
+  int slot_off[SPT];  // node offset within a plane; -1: outside the grid; -2: past the slots
+#pragma unroll
+  for (int j = 0; j < SPT; ++j) {
+    const int s = t + j * NT;
+    const int ni = i0 - 1 + s % SX, nj = j0 - 1 + s / SX;
+    slot_off[j] = s >= NS ? -2 : (ni >= 0 && ni < NXn && nj >= 0 && nj < NYn) ? nj * NXn + ni : -1;
+  }
+  // (planes above k1 are never read: nothing is copied for them)
+  auto copy_equations = [&](int k) {  // plane k's equations into its ring buffer
+    if (k > k1) return;
+    const int b = (k - k0 + 1) % NB;
 #pragma unroll
     for (int j = 0; j < SPT; ++j) {
-      const int s = t + j * NT;
-      const int ni = i0 - 1 + s % SX, nj = j0 - 1 + s / SX;
-      int32_t packed = 0;
-      if (s < NS && k >= 0 && k <= a.nz && ni >= 0 && ni < NXn && nj >= 0 && nj < NYn)
-        packed = __ldg(&a.node_eq[(static_cast<int64_t>(k) * NYn + nj) * NXn + ni]);
-      out[j] = packed;
+      if (slot_off[j] == -2) continue;
+      const bool valid = slot_off[j] >= 0 && k >= 0 && k <= a.nz;
+      cp_async_zfill(&es[b * NS + t + j * NT], valid ? a.node_eq + k * plane_stride + slot_off[j] : a.node_eq, 4, valid);
     }
   };
-  // MODE 0: copies into buffer b go out now and land by the next cp_async_wait_all
-  auto issue = [&](int b, const int32_t (&pk)[SPT]) {
+  auto copy_values = [&](int k) {  // plane k's node values, from its landed equations
+    if (k > k1) return;
+    const int b = (k - k0 + 1) % NB;
 #pragma unroll
     for (int j = 0; j < SPT; ++j) {
+      if (slot_off[j] == -2) continue;
       const int s = t + j * NT;
-      if (s >= NS) continue;
-      const int32_t packed = pk[j];
-      es[b * NS + s] = packed;
+      const int32_t packed = es[b * NS + s];
       const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
       const int32_t base = packed & 0x1FFFFFFF;
+      int off = 0;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const bool free_dof = (mask >> d) & 1u;
-        const T* src = free_dof ? a.x + base + __popc(mask & ((1u << d) - 1u)) : a.x;
-        cp_async_zfill(&xs[(b * 3 + d) * NS + s], src, sizeof(T), free_dof);
-      }
-    }
-    cp_async_commit();
-  };
-  // MODE 1: u + beta v into registers, then into buffer b once it is free
-  auto load_values = [&](const int32_t (&pk)[SPT]) {
-    if constexpr (MODE == 1) {
-#pragma unroll
-      for (int j = 0; j < SPT; ++j)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) px[j][d] = fma(a.beta, load_dof(a.v, pk[j], d), load_dof(a.x, pk[j], d));
-    }
-  };
-  auto commit = [&](int b, const int32_t (&pk)[SPT]) {
-    if constexpr (MODE == 1) {
-#pragma unroll
-      for (int j = 0; j < SPT; ++j) {
-        const int s = t + j * NT;
-        if (s >= NS) continue;
-        es[b * NS + s] = pk[j];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) xs[(b * 3 + d) * NS + s] = px[j][d];
+        cp_async_zfill(&xs[((b * NV + 0) * 3 + d) * NS + s], free_dof ? a.x + base + off : a.x, sizeof(T), free_dof);
+        if (MODE == 1)
+          cp_async_zfill(&xs[((b * NV + 1) * 3 + d) * NS + s], free_dof ? a.v + base + off : a.v, sizeof(T), free_dof);
+        off += free_dof;
       }
     }
   };
-  auto param_of = [&](int ek) {
-    return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.elem_param[(static_cast<int64_t>(ek) * a.ny + ej) * a.nx + ei])
-                                            : -1;
-  };
-  // 2D transform of the column's face in staging buffer b: f = p + 2q (p: x mode, q: y mode)
-  // (written to f[d * stride + 0..3])
+  const int64_t col_off = static_cast<int64_t>(ej) * a.nx + ei;
+  const int64_t layer = static_cast<int64_t>(a.nx) * a.ny;
+  auto param_of = [&](int ek) { return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.elem_param[ek * layer + col_off]) : -1; };
+  // 2D transform of the column's face of plane buffer b (MODE 1: of u + beta v): f = p + 2q
+  // (p: x mode, q: y mode), written to f[d * stride + 0..3]
   auto face = [&](int b, T* f, const int stride) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const T* p = xs + (b * 3 + d) * NS + s00;
-      const T a00 = p[0], a10 = p[1], a01 = p[SX], a11 = p[SX + 1];
+      const T* p = xs + ((b * NV + 0) * 3 + d) * NS + s00;
+      T a00 = p[0], a10 = p[1], a01 = p[SX], a11 = p[SX + 1];
+      if (MODE == 1) {
+        const T* q = xs + ((b * NV + 1) * 3 + d) * NS + s00;
+        a00 = fma(a.beta, q[0], a00);
+        a10 = fma(a.beta, q[1], a10);
+        a01 = fma(a.beta, q[SX], a01);
+        a11 = fma(a.beta, q[SX + 1], a11);
+      }
       const T s0 = a00 + a10, d0 = a10 - a00, s1 = a01 + a11, d1 = a11 - a01;
       f[d * stride + 0] = s0 + s1;
       f[d * stride + 1] = d0 + d1;
@@ -227,45 +265,33 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
     }
   };
 
-  // prologue: planes k0 - 1 (bottom of the first element plane) and k0 staged; equations of
-  // k0 + 1 in registers
-  if constexpr (MODE == 0) {
-    load_packed(k0 - 1, pk_cur);
-    issue(0, pk_cur);
-    load_packed(k0, pk_cur);
-    issue(1, pk_cur);
-    cp_async_wait_all();
-  } else {
-    load_packed(k0 - 1, pk_cur);
-    load_values(pk_cur);
-    commit(0, pk_cur);
-    load_packed(k0, pk_cur);
-    load_values(pk_cur);
-    commit(1, pk_cur);
-  }
-  load_packed(k0 + 1, pk_next);
+  // prologue: equations of planes k0 - 1 .. k0 + D, then values of k0 - 1 .. k0 + D - 2 (the loop's
+  // first iteration continues with k0 + D + 1 and k0 + D - 1)
+  for (int k = k0 - 1; k <= k0 + D; ++k) copy_equations(k);
+  cp_async_commit();
+  cp_async_wait<0>();
+  for (int k = k0 - 1; k <= k0 + D - 2; ++k) copy_values(k);
+  cp_async_commit();
+  cp_async_wait<0>();
   int p_cur = param_of(k0 - 1), p_nxt = param_of(k0);
   __syncthreads();
   T fb[3][4], facc[3][4];
-  face(0, &fb[0][0], 4);
+  if constexpr (CACHE) face(0, &fb[0][0], 4);
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
     for (int f = 0; f < 4; ++f) facc[d][f] = T(0);
-  // buffers: plane ek in bb, plane ek + 1 in tb, plane ek + 2 goes to nb
-  int bb = 0, tb = 1, nb = 2 % NB;
+  int bb = 0;  // buffer of plane ek; plane ek + i is in (bb + i) % NB
 
   for (int ek = k0 - 1; ek < k1; ++ek) {
-    // issue the values of plane ek + 2, the equations of plane ek + 3, the parameters of ek + 2
-#pragma unroll
-    for (int j = 0; j < SPT; ++j) pk_cur[j] = pk_next[j];
-    if constexpr (MODE == 0) issue(nb, pk_cur);
-    else load_values(pk_cur);
-    load_packed(ek + 3, pk_next);
+    const int tb = bb + 1 == NB ? 0 : bb + 1;
+    copy_equations(ek + D + 2);
+    copy_values(ek + D);
+    cp_async_commit();
     const int p_here = p_cur;
     p_cur = p_nxt;
     p_nxt = param_of(ek + 2);
-    // what the node phase of plane ek reads from plane ek's staging (MODE 1 replaces it below)
+    // what the node phase of plane ek reads from plane ek's staging
     const bool out_plane = own && ek >= k0;
     int32_t own_packed = 0;
     T own_x[3] = {T(0), T(0), T(0)};
@@ -274,13 +300,13 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
       own_packed = es[bb * NS + s];
       if (MODE == 0 && (a.nm1 || a.nm2)) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) own_x[d] = xs[(bb * 3 + d) * NS + s];
+        for (int d = 0; d < 3; ++d) own_x[d] = xs[((bb * NV + 0) * 3 + d) * NS + s];
       }
     }
     // ---- element (ei, ej, ek): modes from the top face (transformed here) and the bottom face
-    // (kept from the plane below); fb takes the top face in place
     T tv[3][8];
     face(tb, &tv[0][0], 8);  // top face into tv[.][0..3]
+    if constexpr (!CACHE) face(bb, &fb[0][0], 4);
 #pragma unroll
     for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -288,14 +314,38 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
         const T top = tv[d][f], bot = fb[d][f];
         tv[d][f] = top + bot;
         tv[d][f + 4] = top - bot;
-        fb[d][f] = top;
+        if constexpr (CACHE) fb[d][f] = top;
       }
     if (p_here >= 0) {
       const CT& k = coef[p_here];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
+        T dk[8];
+        load_coef<8>(k.dkm[d], dk);
         T g[8];
-        modal_row(k, tv, d, g);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) g[m] = dk[m] * tv[d][m];
+        // couplings: axis pairs (c0, c1, e), r in {0,1}; modes a = bit c0 + r bit e,
+        // b = bit c1 + r bit e; lambda couples (c0,a)<->(c1,b), mu couples (c0,b)<->(c1,a)
+#pragma unroll
+        for (int pr = 0; pr < 3; ++pr) {
+          const int c0 = pr, c1 = (pr + 1) % 3, e = (pr + 2) % 3;
+          if (d != c0 && d != c1) continue;
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            const int ma = (1 << c0) | (r << e), mb = (1 << c1) | (r << e);
+            T kl, km;
+            load_pair(k.kap + pr * 4 + r * 2, kl, km);
+            if (d == c1) {
+              g[mb] = fma(kl, tv[c0][ma], g[mb]);
+              g[ma] = fma(km, tv[c0][mb], g[ma]);
+            }
+            if (d == c0) {
+              g[ma] = fma(kl, tv[c1][mb], g[ma]);
+              g[mb] = fma(km, tv[c1][ma], g[mb]);
+            }
+          }
+        }
         if (MODE == 1) g[0] -= T(k.body[d]);
         T h[4];
 #pragma unroll
@@ -330,6 +380,7 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
       const int tA = t, tB = t + 1, tC = t + BX, tD = t + BX + 1;
       const uint32_t mask = static_cast<uint32_t>(own_packed) >> 29;
       const int32_t base = own_packed & 0x1FFFFFFF;
+      int off = 0;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         if (!((mask >> d) & 1u)) continue;
@@ -337,7 +388,8 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
         val += ys[(2 * 3 + d) * NT + tB];
         val += ys[(1 * 3 + d) * NT + tC];
         val += ys[(0 * 3 + d) * NT + tD];
-        const int32_t q = base + __popc(mask & ((1u << d) - 1u));
+        const int32_t q = base + off;
+        ++off;
         if (MODE == 0) {
           if (a.nm1) val += T(a.c1 * a.nm1[q]) * own_x[d];
           if (a.nm2) val += T(a.c2 * a.nm2[q]) * own_x[d];
@@ -347,50 +399,43 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
         a.y[q] = val;
       }
     }
-    if constexpr (MODE == 0) {
-      cp_async_wait_all();  // plane ek + 2 has landed (this thread's copies; the barrier: all)
-      bb = tb;
-      tb = nb;
-      nb = (nb + 1) % 3;
-    } else {
-      commit(bb, pk_cur);  // plane ek + 2 replaces plane ek
-      const int x = bb;
-      bb = tb;
-      tb = x;
-    }
+    cp_async_wait<1>();
     __syncthreads();
+    bb = tb;
   }
+  cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------------ launch variants
-// (BX, BY, CTAs per SM for the register budget)
-constexpr int kNumVariants = 8;  // (32,8,2) (16,16,2) (32,4,2) (64,4,2) (16,8,2) (32,16,1) (32,8,1) (16,16,1)
+// (BX, BY, CTAs per SM for the register budget, face caching)
+constexpr int kNumVariants = 9;  // see launch()
 
-template <int BX, int BY, int MINB, class T, int MODE>
+template <int BX, int BY, int MINB, bool CACHE, class T, int MODE>
 void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   using S = Smem<BX, BY, T, MODE>;
   static bool configured = false;
   if (!configured) {
-    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, MINB, CACHE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(S::bytes)));
     configured = true;
   }
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
-  k_box<BX, BY, T, MODE, MINB><<<grid, BX * BY, S::bytes, st>>>(a);
+  k_box<BX, BY, T, MODE, MINB, CACHE><<<grid, BX * BY, S::bytes, st>>>(a);
   FX_LAUNCH_CHECK("box_operator");
 }
 
 template <class T, int MODE>
 void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   switch (p.variant) {
-    case 0: return launch_one<32, 8, 2, T, MODE>(p, a, st);
-    case 1: return launch_one<16, 16, 2, T, MODE>(p, a, st);
-    case 2: return launch_one<32, 4, 2, T, MODE>(p, a, st);
-    case 3: return launch_one<64, 4, 2, T, MODE>(p, a, st);
-    case 4: return launch_one<16, 8, 2, T, MODE>(p, a, st);
-    case 5: return launch_one<32, 16, 1, T, MODE>(p, a, st);
-    case 6: return launch_one<32, 8, 1, T, MODE>(p, a, st);
-    default: return launch_one<16, 16, 1, T, MODE>(p, a, st);
+    case 0: return launch_one<32, 8, 2, false, T, MODE>(p, a, st);
+    case 1: return launch_one<16, 16, 2, false, T, MODE>(p, a, st);
+    case 2: return launch_one<16, 8, 4, false, T, MODE>(p, a, st);
+    case 3: return launch_one<32, 16, 1, false, T, MODE>(p, a, st);
+    case 4: return launch_one<16, 8, 2, true, T, MODE>(p, a, st);
+    case 5: return launch_one<32, 8, 1, true, T, MODE>(p, a, st);
+    case 6: return launch_one<16, 16, 1, true, T, MODE>(p, a, st);
+    case 7: return launch_one<32, 4, 4, false, T, MODE>(p, a, st);
+    default: return launch_one<64, 4, 2, false, T, MODE>(p, a, st);
   }
 }
 
@@ -696,7 +741,7 @@ void box_autotune(ForceState& s, cudaStream_t st) {
   FX_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int bv = 0, bk = 16;
-  const int kzs[] = {8, 16, 32, 64};
+  const int kzs[] = {8, 16, 32, 64};  // (kz = 4 adds a quarter of redundant planes)
   for (int v = 0; v < kNumVariants; ++v)
     for (int kz : kzs) {
       if (kz > 8 && kz >= 2 * (s.box.nz + 1)) continue;

@@ -173,7 +173,7 @@ def test_launch_variants_agree(oracle_mod):
     from femorax_b200 import _lib as L
     import ctypes as C
     lib = L.lib()
-    for variant in range(8):
+    for variant in range(9):
         for kz in (1, 3, 8, 64):
             lib_rc = lib.fx_force_set_launch(force._h, variant, kz) if hasattr(lib, "fx_force_set_launch") else None
             if lib_rc is None:
