@@ -110,6 +110,7 @@ PROTOTYPES = {
     "fx_vops_create": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]),
     "fx_vops_destroy": (None, [vp]),
     "fx_vops_dot": (C.c_int, [vp, vp, vp, C.c_int64, vp, p_f64, vp]),
+    "fx_dot_noalloc": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, p_f64, vp]),
     "fx_axpy": (C.c_int, [C.c_double, vp, vp, C.c_int64, vp]),
     "fx_xpay": (C.c_int, [vp, C.c_double, vp, C.c_int64, vp]),
     "fx_multiply": (C.c_int, [vp, vp, vp, C.c_int64, vp]),

@@ -5,6 +5,9 @@
 // of the chunk in index order (fused multiply-add for products), then lane 0 adds the lane sums
 // in lane order. Levels of chunk sums repeat this until one value is left. The order depends
 // only on n and lanes, so the bits are the same run after run and for any launch shape.
+#include <mutex>
+#include <string>
+
 #include "vector.hpp"
 
 namespace fx {
@@ -175,6 +178,74 @@ void fill(double* y, double a, int64_t n, cudaStream_t st) {
   FX_LAUNCH_CHECK("fill");
 }
 
+// ------------------------------------------------------------------ dot without allocation
+// The same reduction as dot_device, with its partial sums in one file-scope device array
+// instead of memory allocated by a handle. The array is shared by every call in the process:
+// each level writes every partial it later reads, so nothing has to start at zero, and it keeps
+// the last call's partials afterwards. Calls whose kernels overlap on the GPU race on it.
+namespace {
+constexpr int64_t kNoAllocMaxN = int64_t(1) << 27;                     // entries per vector
+constexpr int64_t kNoAllocL0 = (kNoAllocMaxN + kChunk - 1) / kChunk;  // 65536 chunk sums
+constexpr int64_t kNoAllocL1 = (kNoAllocL0 + kChunk - 1) / kChunk;    // 32 sums of those
+constexpr int kNoAllocDevices = 64;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocL0 + kNoAllocL1 + 1];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocDevices] = {};
+
+// The scratch array's address on the current device, looked up on the first call there.
+double* noalloc_scratch() {
+  int dev = 0;
+  FX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocDevices) throw Error(FX_E_UNSUPPORTED, "fx_dot_noalloc: device index above 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      throw Error(FX_E_CUDA, std::string("fx_dot_noalloc: cudaGetSymbolAddress of the scratch array failed: ") +
+                                 cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+void dot_noalloc(const double* x, const double* y, int64_t n, int lanes, double* result, double* result_host,
+                 cudaStream_t st) {
+  check_lanes(lanes);
+  if (n < 0 || (n > 0 && (!x || !y))) throw Error(FX_E_INVALID, "fx_dot_noalloc: bad arguments");
+  if (n > kNoAllocMaxN)
+    throw Error(FX_E_INVALID, "fx_dot_noalloc: n = " + std::to_string(n) + " exceeds the scratch limit of " +
+                                  std::to_string(kNoAllocMaxN) + " entries");
+  if (!result && !result_host) throw Error(FX_E_INVALID, "fx_dot_noalloc: no result pointer given");
+  double* scratch = noalloc_scratch();
+  double* level[2] = {scratch, scratch + kNoAllocL0};
+  double* r = result ? result : scratch + kNoAllocL0 + kNoAllocL1;
+  if (n == 0) {
+    FX_CUDA(cudaMemsetAsync(r, 0, sizeof(double), st));
+  } else {
+    int64_t nc = chunks_of(n);
+    dim3 grid(static_cast<unsigned>((nc + kWarpsPerBlock - 1) / kWarpsPerBlock), 1);
+    k_reduce_chunks<<<grid, 32 * kWarpsPerBlock, 0, st>>>(x, 0, y, n, lanes, nc, nc == 1 ? r : level[0]);
+    FX_LAUNCH_CHECK("dot_noalloc");
+    int cur = 0;
+    while (nc > 1) {
+      const int64_t m = chunks_of(nc);
+      dim3 g(static_cast<unsigned>((m + kWarpsPerBlock - 1) / kWarpsPerBlock), 1);
+      k_reduce_chunks<<<g, 32 * kWarpsPerBlock, 0, st>>>(level[cur], 0, nullptr, nc, lanes, m,
+                                                         m == 1 ? r : level[cur ^ 1]);
+      FX_LAUNCH_CHECK("dot_noalloc levels");
+      nc = m;
+      cur ^= 1;
+    }
+  }
+  if (result_host) {
+    FX_CUDA(cudaMemcpyAsync(result_host, r, sizeof(double), cudaMemcpyDeviceToHost, st));
+    FX_CUDA(cudaStreamSynchronize(st));
+  }
+}
+
 }  // namespace fx
 
 // ------------------------------------------------------------------ C ABI
@@ -227,6 +298,11 @@ int fx_vops_dot(fx_vops* v, const double* x, const double* y, int64_t n, double*
       FX_CUDA(cudaStreamSynchronize(st));
     }
   });
+}
+
+int fx_dot_noalloc(const double* x, const double* y, int64_t n, int32_t lanes, double* result_dev,
+                   double* result_host, void* stream) {
+  return guard([&] { fx::dot_noalloc(x, y, n, lanes, result_dev, result_host, static_cast<cudaStream_t>(stream)); });
 }
 
 int fx_axpy(double a, const double* x, double* y, int64_t n, void* stream) {

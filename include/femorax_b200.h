@@ -203,6 +203,22 @@ void fx_vops_destroy(fx_vops* v);
  * given, and to *result_host (after a stream synchronisation) when given. */
 int fx_vops_dot(fx_vops* v, const double* x, const double* y, int64_t n, double* result_dev, double* result_host,
                 void* stream);
+/* x.y of n entries on the current device, in the same order and with the same bits as
+ * fx_vops_dot with the same lanes, but allocating nothing: no cudaMalloc, no cudaFree and no
+ * allocating library routine. It has no counterpart in the reference. It is for callers that
+ * must not allocate device memory: an application that hands all of the GPU's memory to its own
+ * pool at start-up and forbids other allocations, or a latency-bound loop that cannot afford
+ * cudaMalloc's implicit device synchronisation. The partial sums live in one fixed device array
+ * of this library, so n is limited to 2^27 (134,217,728) entries; larger n is rejected with
+ * FX_E_INVALID. The first call on a device looks up that array's address there (once per
+ * device), so make the first call on each device before any stream capture. Every call in the
+ * process shares the array and it keeps the last call's partials (each call writes every partial
+ * it reads, so none has to start at zero); calls whose kernels overlap on the GPU, from two
+ * streams or two host threads, race on it and must be ordered by the caller. The result goes to
+ * *result_dev (device) and/or *result_host (after a stream synchronisation); at least one must be
+ * given. lanes is 1..32 as in fx_vops_create. */
+int fx_dot_noalloc(const double* x, const double* y, int64_t n, int32_t lanes, double* result_dev,
+                   double* result_host, void* stream);
 /* Element-wise kernels (vector_ops.cpp:77-103): y += a x; y = x + a y; y = d .* x. */
 int fx_axpy(double a, const double* x, double* y, int64_t n, void* stream);
 int fx_xpay(const double* x, double a, double* y, int64_t n, void* stream);
