@@ -62,33 +62,6 @@ struct Coef<float> {
   using type = BoxCoef32;
 };
 
-// Row block `d` of the modal operator: g[m] (output component d) from the modes t of all three
-// components. Axis pairs (c0, c1, e): (0,1,2), (1,2,0), (2,0,1); for r in {0,1}: modes
-// a = bit c0 + r bit e, b = bit c1 + r bit e; lambda couples (c0,a)<->(c1,b), mu couples
-// (c0,b)<->(c1,a). d is a compile-time constant after unrolling, so the branches vanish.
-template <class T, class C>
-__device__ __forceinline__ void modal_row(const C& k, const T t[3][8], int d, T g[8]) {
-#pragma unroll
-  for (int m = 0; m < 8; ++m) g[m] = T(k.dkm[d][m]) * t[d][m];
-#pragma unroll
-  for (int pr = 0; pr < 3; ++pr) {
-    const int c0 = pr, c1 = (pr + 1) % 3, e = (pr + 2) % 3;
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int ma = (1 << c0) | (r << e), mb = (1 << c1) | (r << e);
-      const T kl = T(k.kap[pr * 4 + r * 2 + 0]), km = T(k.kap[pr * 4 + r * 2 + 1]);
-      if (d == c1) {
-        g[mb] = fma(kl, t[c0][ma], g[mb]);
-        g[ma] = fma(km, t[c0][mb], g[ma]);
-      }
-      if (d == c0) {
-        g[ma] = fma(kl, t[c1][mb], g[ma]);
-        g[mb] = fma(km, t[c1][ma], g[mb]);
-      }
-    }
-  }
-}
-
 template <class T>
 __device__ __forceinline__ T load_dof(const T* __restrict__ x, int32_t packed, int d) {
   const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
@@ -100,12 +73,13 @@ __device__ __forceinline__ T load_dof(const T* __restrict__ x, int32_t packed, i
 template <int BX, int BY, class T, int MODE>
 struct Smem {
   static constexpr int NT = BX * BY, SX = BX + 1, SY = BY + 1, NS = SX * SY;
+  static constexpr int NO = (BX - 1) * (BY - 1);  // owned nodes per plane
   // Planes are gathered D planes ahead; their equations D + 2 planes ahead; the ring holds D + 3.
   static constexpr int D = 4, NB = D + 3;
   static constexpr int NV = MODE == 1 ? 2 : 1;  // staged vectors: x, or u and v
   static constexpr size_t coef_bytes = sizeof(typename Coef<T>::type) * kParamsInShared;
   static constexpr size_t bytes =
-      coef_bytes + sizeof(T) * (12 * NT + NB * NV * 3 * NS) + sizeof(int32_t) * NB * NS;
+      coef_bytes + sizeof(T) * (12 * NT + NB * NV * 3 * NS + 3 * NO) + sizeof(int32_t) * (NB * NS + NO);
 };
 
 __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, int bytes, bool valid) {
@@ -154,27 +128,89 @@ __device__ __forceinline__ void load_pair(const float* __restrict__ src, float& 
   b = v.y;
 }
 
+// The modal operator, in place on the modes t[c][m] of the three components. Unknown (c, m)
+// belongs to group s = m ^ 2^c and only unknowns of one group are coupled, so each group is a
+// 3 x 3 block: its diagonal, then its couplings in the order of their axis pairs (pair 0 couples
+// components 0 and 1, pair 1 components 1 and 2, pair 2 components 2 and 0). Groups 1..6 hold one
+// coupling: lambda between the pair's components for s = 2^e (e the pair's third axis: 4, 1, 2),
+// mu for s = 2^c0 + 2^c1 (3, 6, 5); group 0 holds the three lambda couplings of r = 0, group 7
+// the three mu couplings of r = 1.
+// VEC: the table is in shared or global memory (16-byte loads); otherwise it is a kernel
+// parameter, read value by value.
+template <bool VEC, class T, class CT>
+__device__ __forceinline__ void modal_apply(const CT& k, T t[3][8]) {
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    T c[4];
+    if constexpr (VEC) {
+      load_coef<4>(k.grp[s], c);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) c[j] = k.grp[s][j];
+    }
+    const T u0 = t[0][s ^ 1], u1 = t[1][s ^ 2], u2 = t[2][s ^ 4];
+    T o0 = c[0] * u0, o1 = c[1] * u1, o2 = c[2] * u2;
+    if (s == 0 || s == 7) {
+      T k1, k2;
+      if constexpr (VEC) {
+        load_pair(k.more + (s == 7 ? 2 : 0), k1, k2);
+      } else {
+        k1 = k.more[s == 7 ? 2 : 0];
+        k2 = k.more[s == 7 ? 3 : 1];
+      }
+      o1 = fma(c[3], u0, o1);  // pair 0
+      o0 = fma(c[3], u1, o0);
+      o2 = fma(k1, u1, o2);  // pair 1
+      o1 = fma(k1, u2, o1);
+      o0 = fma(k2, u2, o0);  // pair 2
+      o2 = fma(k2, u0, o2);
+    } else if (s == 4 || s == 3) {
+      o1 = fma(c[3], u0, o1);
+      o0 = fma(c[3], u1, o0);
+    } else if (s == 1 || s == 6) {
+      o2 = fma(c[3], u1, o2);
+      o1 = fma(c[3], u2, o1);
+    } else {
+      o0 = fma(c[3], u2, o0);
+      o2 = fma(c[3], u0, o2);
+    }
+    t[0][s ^ 1] = o0;
+    t[1][s ^ 2] = o1;
+    t[2][s ^ 4] = o2;
+  }
+}
+
 // MODE 0: y = K_eff x (+ k.mass nodal masses x + k.damping nodal alphaM masses x).
 // MODE 1: f = K (u + beta v) - body + la v (la: lumped alphaM masses, element and nodal).
 // MINB: CTAs per SM the register budget is sized for. CACHE: keep the bottom face's transform
 // in registers from the plane below (fewer operations, more registers) or transform it again
 // from the staged plane (fewer registers, more resident warps).
 //
-// Staging ring (all copies asynchronous, each thread owns fixed slots of a plane): in the
-// iteration of element plane ek a thread copies the equations of its slots of plane ek + D + 2
-// and, from the equations it copied two iterations before, the node values of plane ek + D;
-// one commit group per iteration; waiting for all but the newest group at the end of the
-// iteration leaves planes up to ek + D + 1 (equations) and ek + D - 1 (values) landed.
-template <int BX, int BY, class T, int MODE, int MINB, bool CACHE>
-__global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
+// Staging ring (all copies asynchronous): in the iteration of element plane ek the CTA copies
+// the equations of plane ek + D + 2 (one node per thread slot) and, from the equations it copied
+// two iterations before, the node values of plane ek + D; one commit group per iteration; waiting
+// for all but the newest group at the end of the iteration leaves planes up to ek + D + 1
+// (equations) and ek + D - 1 (values) landed.
+//
+// Node values are gathered, and results stored, by (node, component) items: consecutive lanes
+// take the three components of one node, so one warp instruction touches about one cache line
+// per node whatever the equation numbering (the reference's RCM numbering puts neighbouring
+// grid nodes hundreds of equations apart). The owners of a plane's nodes leave their sums and
+// equations in shared memory; the stores run in the next iteration, after the barrier.
+// LAYERED: the coefficient tables come from `tab` (layered grids), else from a.coef.
+template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, bool LAYERED>
+__global__ void __launch_bounds__(BX* BY, MINB)
+    k_box(BoxArgs<T> a, const __grid_constant__ BoxTable<typename Coef<T>::type> tab) {
   using S = Smem<BX, BY, T, MODE>;
   using CT = typename Coef<T>::type;
-  constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB, NV = S::NV, D = S::D;
+  constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB, NV = S::NV, D = S::D, NO = S::NO;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* cs = reinterpret_cast<CT*>(smem_raw);
   T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [4 corners][3][NT]: face corner values
   T* xs = ys + 12 * NT;                                     // [NB planes][NV][3][NS]: node values
-  int32_t* es = reinterpret_cast<int32_t*>(xs + NB * NV * 3 * NS);  // [NB][NS]: equations
+  T* yo = xs + NB * NV * 3 * NS;                            // [3][NO]: owned nodes' sums, last plane
+  int32_t* es = reinterpret_cast<int32_t*>(yo + 3 * NO);   // [NB][NS]: equations
+  int32_t* yq = es + NB * NS;                               // [NO]: owned nodes' equations (0: none)
   if (a.skip && *a.skip) return;
 
   const int t = threadIdx.x;
@@ -186,11 +222,13 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   const int64_t plane_stride = static_cast<int64_t>(NXn) * NYn;
   const int ei = i0 - 1 + ci, ej = j0 - 1 + cj;
   const bool col_ok = ei >= 0 && ei < a.nx && ej >= 0 && ej < a.ny;
-  const bool own = ci < BX - 1 && cj < BY - 1 && i0 + ci < NXn && j0 + cj < NYn;
-  const int s00 = ci + cj * SX;  // staging slot of the column's corner (0, 0)
+  const bool owner_slot = ci < BX - 1 && cj < BY - 1;
+  const bool own = owner_slot && i0 + ci < NXn && j0 + cj < NYn;
+  const int o_idx = ci + cj * (BX - 1);  // owned node index (owner_slot)
+  const int s00 = ci + cj * SX;          // staging slot of the column's corner (0, 0)
 
   // coefficient tables in shared memory (few parameter sets) or read through L1
-  const bool shared_coef = a.nparams <= kParamsInShared;
+  const bool shared_coef = !LAYERED && a.nparams <= kParamsInShared;
   if (shared_coef) {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(a.coef);
     uint32_t* dst = reinterpret_cast<uint32_t*>(cs);
@@ -199,14 +237,27 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   }
   const CT* coef = shared_coef ? cs : reinterpret_cast<const CT*>(a.coef);
 
-  // ---- staging slots of this thread (fixed for the whole sweep)
-  constexpr int SPT = (NS + NT - 1) / NT;
+  // ---- this thread's fixed work items
+  constexpr int SPT = (NS + NT - 1) / NT;             // node slots (equation copies)
+  constexpr int IPT = (3 * NS + NT - 1) / NT;         // (slot, component) gathers
+  constexpr int OPT = (3 * NO + NT - 1) / NT;         // (owned node, component) stores
   int slot_off[SPT];  // node offset within a plane; -1: outside the grid; -2: past the slots
 #pragma unroll
   for (int j = 0; j < SPT; ++j) {
     const int s = t + j * NT;
     const int ni = i0 - 1 + s % SX, nj = j0 - 1 + s / SX;
     slot_off[j] = s >= NS ? -2 : (ni >= 0 && ni < NXn && nj >= 0 && nj < NYn) ? nj * NXn + ni : -1;
+  }
+  int gitem[IPT], oitem[OPT];  // item i = t + j NT: (i / 3) << 2 | i % 3, or -1 past the items
+#pragma unroll
+  for (int j = 0; j < IPT; ++j) {
+    const int i = t + j * NT;
+    gitem[j] = i < 3 * NS ? ((i / 3) << 2) | (i % 3) : -1;
+  }
+#pragma unroll
+  for (int j = 0; j < OPT; ++j) {
+    const int i = t + j * NT;
+    oitem[j] = i < 3 * NO ? ((i / 3) << 2) | (i % 3) : -1;
   }
   // (planes above k1 are never read: nothing is copied for them)
   auto copy_equations = [&](int k) {  // plane k's equations into its ring buffer
@@ -223,26 +274,43 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
     if (k > k1) return;
     const int b = (k - k0 + 1) % NB;
 #pragma unroll
-    for (int j = 0; j < SPT; ++j) {
-      if (slot_off[j] == -2) continue;
-      const int s = t + j * NT;
+    for (int j = 0; j < IPT; ++j) {
+      if (gitem[j] < 0) continue;
+      const int s = gitem[j] >> 2, d = gitem[j] & 3;
       const int32_t packed = es[b * NS + s];
       const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
-      const int32_t base = packed & 0x1FFFFFFF;
-      int off = 0;
+      const int32_t q = (packed & 0x1FFFFFFF) + __popc(mask & ((1u << d) - 1u));
+      const bool free_dof = (mask >> d) & 1u;
+      cp_async_zfill(&xs[((b * NV + 0) * 3 + d) * NS + s], free_dof ? a.x + q : a.x, sizeof(T), free_dof);
+      if (MODE == 1)
+        cp_async_zfill(&xs[((b * NV + 1) * 3 + d) * NS + s], free_dof ? a.v + q : a.v, sizeof(T), free_dof);
+    }
+  };
+  auto store_plane = [&]() {  // the owned nodes' sums of the last plane, with the nodal terms
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const bool free_dof = (mask >> d) & 1u;
-        cp_async_zfill(&xs[((b * NV + 0) * 3 + d) * NS + s], free_dof ? a.x + base + off : a.x, sizeof(T), free_dof);
-        if (MODE == 1)
-          cp_async_zfill(&xs[((b * NV + 1) * 3 + d) * NS + s], free_dof ? a.v + base + off : a.v, sizeof(T), free_dof);
-        off += free_dof;
+    for (int j = 0; j < OPT; ++j) {
+      if (oitem[j] < 0) continue;
+      const int o = oitem[j] >> 2, d = oitem[j] & 3;
+      const int32_t packed = yq[o];
+      const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
+      if (!((mask >> d) & 1u)) continue;
+      const int32_t q = (packed & 0x1FFFFFFF) + __popc(mask & ((1u << d) - 1u));
+      T val = yo[d * NO + o];
+      if (MODE == 0) {
+        if (a.nm1) val += T(a.c1 * a.nm1[q]) * a.x[q];
+        if (a.nm2) val += T(a.c2 * a.nm2[q]) * a.x[q];
+      } else if (a.nm2) {
+        val += T(a.nm2[q]) * a.v[q];
       }
+      a.y[q] = val;
     }
   };
   const int64_t col_off = static_cast<int64_t>(ej) * a.nx + ei;
   const int64_t layer = static_cast<int64_t>(a.nx) * a.ny;
-  auto param_of = [&](int ek) { return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.elem_param[ek * layer + col_off]) : -1; };
+  auto param_of = [&](int ek) {
+    if constexpr (LAYERED) return (ek >= 0 && ek < a.nz) ? static_cast<int>(tab.layer[ek]) : -1;  // same for all threads
+    return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.elem_param[ek * layer + col_off]) : -1;
+  };
   // 2D transform of the column's face of plane buffer b (MODE 1: of u + beta v): f = p + 2q
   // (p: x mode, q: y mode), written to f[d * stride + 0..3]
   auto face = [&](int b, T* f, const int stride) {
@@ -270,6 +338,7 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
   for (int k = k0 - 1; k <= k0 + D; ++k) copy_equations(k);
   cp_async_commit();
   cp_async_wait<0>();
+  __syncthreads();  // the values' copies read other threads' equations
   for (int k = k0 - 1; k <= k0 + D - 2; ++k) copy_values(k);
   cp_async_commit();
   cp_async_wait<0>();
@@ -285,24 +354,15 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
 
   for (int ek = k0 - 1; ek < k1; ++ek) {
     const int tb = bb + 1 == NB ? 0 : bb + 1;
+    if (ek - 1 >= k0) store_plane();  // plane ek - 1 (left by the last iteration, before its barrier)
     copy_equations(ek + D + 2);
     copy_values(ek + D);
     cp_async_commit();
     const int p_here = p_cur;
     p_cur = p_nxt;
     p_nxt = param_of(ek + 2);
-    // what the node phase of plane ek reads from plane ek's staging
     const bool out_plane = own && ek >= k0;
-    int32_t own_packed = 0;
-    T own_x[3] = {T(0), T(0), T(0)};
-    if (out_plane) {
-      const int s = s00 + SX + 1;
-      own_packed = es[bb * NS + s];
-      if (MODE == 0 && (a.nm1 || a.nm2)) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) own_x[d] = xs[((bb * NV + 0) * 3 + d) * NS + s];
-      }
-    }
+    const int32_t own_packed = out_plane ? es[bb * NS + s00 + SX + 1] : 0;
     // ---- element (ei, ej, ek): modes from the top face (transformed here) and the bottom face
     T tv[3][8];
     face(tb, &tv[0][0], 8);  // top face into tv[.][0..3]
@@ -316,37 +376,22 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
         tv[d][f + 4] = top - bot;
         if constexpr (CACHE) fb[d][f] = top;
       }
-    if (p_here >= 0) {
-      const CT& k = coef[p_here];
+    if (p_here >= 0 && (!LAYERED || col_ok)) {
+      T body[3] = {T(0), T(0), T(0)};
+      if constexpr (LAYERED) {
+        modal_apply<false>(tab.c[p_here], tv);
+        if (MODE == 1)
+          for (int d = 0; d < 3; ++d) body[d] = T(tab.c[p_here].body[d]);
+      } else {
+        const CT& k = coef[p_here];
+        modal_apply<true>(k, tv);
+        if (MODE == 1)
+          for (int d = 0; d < 3; ++d) body[d] = T(k.body[d]);
+      }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        T dk[8];
-        load_coef<8>(k.dkm[d], dk);
-        T g[8];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) g[m] = dk[m] * tv[d][m];
-        // couplings: axis pairs (c0, c1, e), r in {0,1}; modes a = bit c0 + r bit e,
-        // b = bit c1 + r bit e; lambda couples (c0,a)<->(c1,b), mu couples (c0,b)<->(c1,a)
-#pragma unroll
-        for (int pr = 0; pr < 3; ++pr) {
-          const int c0 = pr, c1 = (pr + 1) % 3, e = (pr + 2) % 3;
-          if (d != c0 && d != c1) continue;
-#pragma unroll
-          for (int r = 0; r < 2; ++r) {
-            const int ma = (1 << c0) | (r << e), mb = (1 << c1) | (r << e);
-            T kl, km;
-            load_pair(k.kap + pr * 4 + r * 2, kl, km);
-            if (d == c1) {
-              g[mb] = fma(kl, tv[c0][ma], g[mb]);
-              g[ma] = fma(km, tv[c0][mb], g[ma]);
-            }
-            if (d == c0) {
-              g[ma] = fma(kl, tv[c1][mb], g[ma]);
-              g[mb] = fma(km, tv[c1][ma], g[mb]);
-            }
-          }
-        }
-        if (MODE == 1) g[0] -= T(k.body[d]);
+        T* g = tv[d];
+        if (MODE == 1) g[0] -= body[d];
         T h[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
@@ -375,53 +420,62 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_box(BoxArgs<T> a) {
     }
     __syncthreads();
     // ---- owned node (i0 + ci, j0 + cj) of plane ek: corner (1,1) of column (ci,cj), (0,1) of
-    // (ci+1,cj), (1,0) of (ci,cj+1), (0,0) of (ci+1,cj+1)
-    if (out_plane) {
-      const int tA = t, tB = t + 1, tC = t + BX, tD = t + BX + 1;
-      const uint32_t mask = static_cast<uint32_t>(own_packed) >> 29;
-      const int32_t base = own_packed & 0x1FFFFFFF;
-      int off = 0;
+    // (ci+1,cj), (1,0) of (ci,cj+1), (0,0) of (ci+1,cj+1), summed in that order
+    if (owner_slot) {
+      if (out_plane) {
+        const int tA = t, tB = t + 1, tC = t + BX, tD = t + BX + 1;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        if (!((mask >> d) & 1u)) continue;
-        T val = ys[(3 * 3 + d) * NT + tA];
-        val += ys[(2 * 3 + d) * NT + tB];
-        val += ys[(1 * 3 + d) * NT + tC];
-        val += ys[(0 * 3 + d) * NT + tD];
-        const int32_t q = base + off;
-        ++off;
-        if (MODE == 0) {
-          if (a.nm1) val += T(a.c1 * a.nm1[q]) * own_x[d];
-          if (a.nm2) val += T(a.c2 * a.nm2[q]) * own_x[d];
-        } else if (a.nm2) {
-          val += T(a.nm2[q]) * a.v[q];
+        for (int d = 0; d < 3; ++d) {
+          T val = ys[(3 * 3 + d) * NT + tA];
+          val += ys[(2 * 3 + d) * NT + tB];
+          val += ys[(1 * 3 + d) * NT + tC];
+          val += ys[(0 * 3 + d) * NT + tD];
+          yo[d * NO + o_idx] = val;
         }
-        a.y[q] = val;
       }
+      yq[o_idx] = own_packed;
     }
     cp_async_wait<1>();
     __syncthreads();
     bb = tb;
   }
   cp_async_wait<0>();
+  if (k1 - 1 >= k0) store_plane();
 }
 
 // ------------------------------------------------------------------ launch variants
 // (BX, BY, CTAs per SM for the register budget, face caching)
 constexpr int kNumVariants = 9;  // see launch()
 
-template <int BX, int BY, int MINB, bool CACHE, class T, int MODE>
-void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
+template <class T>
+const BoxTable<typename Coef<T>::type>& table_of(const BoxPlan& p);
+template <>
+const BoxTable<BoxCoef>& table_of<double>(const BoxPlan& p) {
+  return p.tab;
+}
+template <>
+const BoxTable<BoxCoef32>& table_of<float>(const BoxPlan& p) {
+  return p.tab32;
+}
+
+template <int BX, int BY, int MINB, bool CACHE, bool LAYERED, class T, int MODE>
+void launch_shape(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   using S = Smem<BX, BY, T, MODE>;
   static bool configured = false;
   if (!configured) {
-    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, MINB, CACHE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(S::bytes)));
+    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, MINB, CACHE, LAYERED>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
     configured = true;
   }
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
-  k_box<BX, BY, T, MODE, MINB, CACHE><<<grid, BX * BY, S::bytes, st>>>(a);
+  k_box<BX, BY, T, MODE, MINB, CACHE, LAYERED><<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p));
   FX_LAUNCH_CHECK("box_operator");
+}
+
+template <int BX, int BY, int MINB, bool CACHE, class T, int MODE>
+void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
+  if (p.layered) return launch_shape<BX, BY, MINB, CACHE, true, T, MODE>(p, a, st);
+  return launch_shape<BX, BY, MINB, CACHE, false, T, MODE>(p, a, st);
 }
 
 template <class T, int MODE>
@@ -487,25 +541,36 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
         }
         dk *= 2.0 * J * sk;
         const double dm = cons ? sm * q.rho * J * w(bit(0)) * w(bit(1)) * w(bit(2)) : 8.0 * sm * q.rho * J;
-        c.dkm[comp][m] = (dk + dm) / 64.0;
+        c.grp[m ^ (1 << comp)][comp] = (dk + dm) / 64.0;
       }
+    // couplings of axis pair pr (components pr, pr + 1 mod 3; third axis e): lambda part for
+    // r = 0 in group 0 and for r = 1 in group 2^e; mu part for r = 0 in group 2^c0 + 2^c1 and
+    // for r = 1 in group 7
     for (int pr = 0; pr < 3; ++pr) {
-      const int c0 = pr, c1 = (pr + 1) % 3;
-      for (int r = 0; r < 2; ++r) {
-        const double base = 4.0 * J * rd[c0] * rd[c1] * w(r) * sk / 64.0;
-        c.kap[pr * 4 + r * 2 + 0] = base * lam;
-        c.kap[pr * 4 + r * 2 + 1] = base * mu;
-      }
+      const int c0 = pr, c1 = (pr + 1) % 3, e = (pr + 2) % 3;
+      const double base0 = 4.0 * J * rd[c0] * rd[c1] * w(0) * sk / 64.0;
+      const double base1 = 4.0 * J * rd[c0] * rd[c1] * w(1) * sk / 64.0;
+      if (pr == 0) c.grp[0][3] = base0 * lam;
+      else c.more[pr - 1] = base0 * lam;
+      c.grp[1 << e][3] = base1 * lam;
+      c.grp[(1 << c0) | (1 << c1)][3] = base0 * mu;
+      if (pr == 0) c.grp[7][3] = base1 * mu;
+      else c.more[2 + pr - 1] = base1 * mu;
     }
     for (int d = 0; d < 3; ++d) c.body[d] = mode == 1 ? q.b[d] * J : 0.0;
     h[i] = c;
     BoxCoef32& f = h32[i];
-    for (int comp = 0; comp < 3; ++comp)
-      for (int m = 0; m < 8; ++m) f.dkm[comp][m] = static_cast<float>(c.dkm[comp][m]);
-    for (int j = 0; j < 12; ++j) f.kap[j] = static_cast<float>(c.kap[j]);
+    for (int g = 0; g < 8; ++g)
+      for (int j = 0; j < 4; ++j) f.grp[g][j] = static_cast<float>(c.grp[g][j]);
+    for (int j = 0; j < 4; ++j) f.more[j] = static_cast<float>(c.more[j]);
     for (int d = 0; d < 3; ++d) f.body[d] = static_cast<float>(c.body[d]);
     f.pad_ = 0.f;
   }
+  if (p.layered)
+    for (int32_t i = 0; i < s.nparams; ++i) {
+      p.tab.c[i] = h[i];
+      p.tab32.c[i] = h32[i];
+    }
   if (p.coef.n != h.size()) p.coef.alloc(h.size());
   if (p.coef32.n != h32.size()) p.coef32.alloc(h32.size());
   FX_CUDA(cudaMemcpy(p.coef.ptr, h.data(), h.size() * sizeof(BoxCoef), cudaMemcpyHostToDevice));
@@ -635,6 +700,17 @@ void box_build_plan(ForceState& s) {
   }
   std::vector<int32_t> eparam(static_cast<size_t>(s.count));
   for (size_t c = 0; c < cell.size(); ++c) eparam[c] = s.param_h[cell[c]];
+  // layered: one parameter set per element plane, few sets and planes (kernel-parameter tables)
+  p.layered = s.nparams <= kTableParams && nz <= kTableLayers;
+  for (int k = 0; k < nz && p.layered; ++k) {
+    const int32_t first = eparam[static_cast<size_t>(k) * nx * ny];
+    for (int64_t c = 0; c < static_cast<int64_t>(nx) * ny; ++c)
+      if (eparam[static_cast<size_t>(k) * nx * ny + c] != first) {
+        p.layered = false;
+        break;
+      }
+    p.tab.layer[k] = p.tab32.layer[k] = static_cast<uint8_t>(first);
+  }
   // force form: lumped masses and one beta
   const double beta0 = s.params_h[0].betaK + s.params_h[0].betaKinit + s.params_h[0].betaKcomm;
   bool one_beta = true;

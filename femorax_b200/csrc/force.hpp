@@ -16,19 +16,36 @@ namespace fx {
 // Coefficients of the exact modal element operator of one parameter set on the box grid, for
 // the current operator coefficients (box.cu builds them). Scaled by 1/64 where the two
 // Walsh-Hadamard transforms (unnormalised) would otherwise multiply the result by 64.
+//
+// The 24 modal unknowns (component c, mode m) fall into 8 groups by s = m ^ 2^c, and the
+// operator couples unknowns of one group only: groups 1..6 hold one coupling (between two
+// components), groups 0 and 7 three. So the table is group-major: grp[s][c] is the diagonal of
+// (c, s ^ 2^c) (stiffness + mass, consistent or lumped: H^T H = 8 I), grp[s][3] the group's first
+// coupling, more[0..1] the second and third couplings of group 0 and more[2..3] those of group 7.
 struct BoxCoef {
-  double dkm[3][8];  // modal diagonal: stiffness + mass (consistent, or lumped: H^T H = 8 I)
-  double kap[12];    // couplings: per axis pair (xy, yz, zx) and r in {0,1}: lambda part, mu part
-  double body[3];    // force mode: body force per corner (b J), on mode 0
+  double grp[8][4];
+  double more[4];
+  double body[3];  // force mode: body force per corner (b J), on mode 0
   double pad_;
 };
 static_assert(sizeof(BoxCoef) == 40 * 8, "BoxCoef layout");
 
 struct BoxCoef32 {  // the same in FP32 for the mixed-precision operator
-  float dkm[3][8];
-  float kap[12];
+  float grp[8][4];
+  float more[4];
   float body[3];
   float pad_;
+};
+
+// The coefficient tables of a layered grid (one parameter set per element plane, at most
+// kTableParams sets and kTableLayers planes), passed to the box kernel as a kernel parameter: the
+// set of a plane is then the same for every thread, and its coefficients are read through the
+// constant cache instead of the shared-memory pipe that the node values already load.
+constexpr int kTableParams = 16, kTableLayers = 1024;
+template <class CT>
+struct BoxTable {
+  CT c[kTableParams];
+  uint8_t layer[kTableLayers];  // parameter set of element plane k
 };
 
 // A structured grid of axis-aligned boxes with equal spacing: (nx, ny, nz) elements.
@@ -53,6 +70,9 @@ struct BoxPlan {
   // coefficient tables for the last operator coefficients
   DeviceArray<BoxCoef> coef;
   DeviceArray<BoxCoef32> coef32;
+  bool layered = false;  // one parameter set per element plane (kernel-parameter tables)
+  BoxTable<BoxCoef> tab{};
+  BoxTable<BoxCoef32> tab32{};
   double last_k[4] = {-1, -1, -1, -1};
   int last_mode = -1;
 };
