@@ -79,7 +79,7 @@ struct Smem {
   static constexpr int NV = MODE == 1 ? 2 : 1;  // staged vectors: x, or u and v
   static constexpr size_t coef_bytes = sizeof(typename Coef<T>::type) * kParamsInShared;
   static constexpr size_t bytes =
-      coef_bytes + sizeof(T) * (12 * NT + NB * NV * 3 * NS + 3 * NO) + sizeof(int32_t) * (NB * NS + NO);
+      coef_bytes + sizeof(T) * (3 * NT + NB * NV * 3 * NS + 3 * NO) + sizeof(int32_t) * (NB * NS + NO);
 };
 
 __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, int bytes, bool valid) {
@@ -204,10 +204,11 @@ __global__ void __launch_bounds__(BX* BY, MINB)
   using S = Smem<BX, BY, T, MODE>;
   using CT = typename Coef<T>::type;
   constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB, NV = S::NV, D = S::D, NO = S::NO;
+  static_assert(BX == 16 || BX == 32, "a row of element columns must lie within one warp");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* cs = reinterpret_cast<CT*>(smem_raw);
-  T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [4 corners][3][NT]: face corner values
-  T* xs = ys + 12 * NT;                                     // [NB planes][NV][3][NS]: node values
+  T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [3][NT]: row sums for the row below
+  T* xs = ys + 3 * NT;                                      // [NB planes][NV][3][NS]: node values
   T* yo = xs + NB * NV * 3 * NS;                            // [3][NO]: owned nodes' sums, last plane
   int32_t* es = reinterpret_cast<int32_t*>(yo + 3 * NO);   // [NB][NS]: equations
   int32_t* yq = es + NB * NS;                               // [NO]: owned nodes' equations (0: none)
@@ -376,6 +377,7 @@ __global__ void __launch_bounds__(BX* BY, MINB)
         tv[d][f + 4] = top - bot;
         if constexpr (CACHE) fb[d][f] = top;
       }
+    T cor[3][4];  // face corner values c = i + 2j of the three components
     if (p_here >= 0 && (!LAYERED || col_ok)) {
       T body[3] = {T(0), T(0), T(0)};
       if constexpr (LAYERED) {
@@ -398,40 +400,44 @@ __global__ void __launch_bounds__(BX* BY, MINB)
           h[f] = facc[d][f] + (g[f] - g[f + 4]);  // bottom face, plus the element below's top face
           facc[d][f] = g[f] + g[f + 4];            // top face, for the plane above
         }
-        // inverse 2D transform of the face: corners c = i + 2j
+        // inverse 2D transform of the face
         const T u0 = h[0] - h[2], u2 = h[0] + h[2], u1 = h[1] - h[3], u3 = h[1] + h[3];
-        ys[(0 * 3 + d) * NT + t] = u0 - u1;
-        ys[(1 * 3 + d) * NT + t] = u0 + u1;
-        ys[(2 * 3 + d) * NT + t] = u2 - u3;
-        ys[(3 * 3 + d) * NT + t] = u2 + u3;
+        cor[d][0] = u0 - u1;
+        cor[d][1] = u0 + u1;
+        cor[d][2] = u2 - u3;
+        cor[d][3] = u2 + u3;
       }
     } else {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const T u0 = facc[d][0] - facc[d][2], u2 = facc[d][0] + facc[d][2];
         const T u1 = facc[d][1] - facc[d][3], u3 = facc[d][1] + facc[d][3];
-        ys[(0 * 3 + d) * NT + t] = u0 - u1;
-        ys[(1 * 3 + d) * NT + t] = u0 + u1;
-        ys[(2 * 3 + d) * NT + t] = u2 - u3;
-        ys[(3 * 3 + d) * NT + t] = u2 + u3;
+        cor[d][0] = u0 - u1;
+        cor[d][1] = u0 + u1;
+        cor[d][2] = u2 - u3;
+        cor[d][3] = u2 + u3;
 #pragma unroll
         for (int f = 0; f < 4; ++f) facc[d][f] = T(0);
       }
     }
+    // The owned node (ci, cj) of plane ek is corner (1,1) of column (ci, cj), corner (0,1) of
+    // (ci+1, cj), corner (1,0) of (ci, cj+1) and corner (0,0) of (ci+1, cj+1); its value is the
+    // sum of its row's pair plus the pair of the row above, in that order. Column ci+1 of the same
+    // row is the next lane (a row of columns lies within one warp), so its corners come by
+    // shuffle; the pair sums for the row below go through shared memory.
+    T phi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T c01n = __shfl_down_sync(0xffffffffu, cor[d][2], 1);
+      const T c00n = __shfl_down_sync(0xffffffffu, cor[d][0], 1);
+      phi[d] = cor[d][3] + c01n;
+      ys[d * NT + t] = cor[d][1] + c00n;
+    }
     __syncthreads();
-    // ---- owned node (i0 + ci, j0 + cj) of plane ek: corner (1,1) of column (ci,cj), (0,1) of
-    // (ci+1,cj), (1,0) of (ci,cj+1), (0,0) of (ci+1,cj+1), summed in that order
     if (owner_slot) {
       if (out_plane) {
-        const int tA = t, tB = t + 1, tC = t + BX, tD = t + BX + 1;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          T val = ys[(3 * 3 + d) * NT + tA];
-          val += ys[(2 * 3 + d) * NT + tB];
-          val += ys[(1 * 3 + d) * NT + tC];
-          val += ys[(0 * 3 + d) * NT + tD];
-          yo[d * NO + o_idx] = val;
-        }
+        for (int d = 0; d < 3; ++d) yo[d * NO + o_idx] = phi[d] + ys[d * NT + t + BX];
       }
       yq[o_idx] = own_packed;
     }
@@ -489,7 +495,7 @@ void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     case 5: return launch_one<32, 8, 1, true, T, MODE>(p, a, st);
     case 6: return launch_one<16, 16, 1, true, T, MODE>(p, a, st);
     case 7: return launch_one<32, 4, 4, false, T, MODE>(p, a, st);
-    default: return launch_one<64, 4, 2, false, T, MODE>(p, a, st);
+    default: return launch_one<16, 32, 1, false, T, MODE>(p, a, st);
   }
 }
 
