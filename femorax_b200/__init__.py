@@ -19,7 +19,7 @@ from .meshes import ModelSpec
 
 __all__ = ["Model", "Compiled", "MeshArrays", "InternalForce", "OperatorCoefficients", "MatrixFreeOperator",
            "SolveOptions", "SolveResult", "LinearSolver", "ConjugateGradient", "Gmres", "KrylovSolver",
-           "MixedPrecisionSolver", "VectorOps", "FxError", "ModelSpec"]
+           "MixedPrecisionSolver", "BatchEngine", "VectorOps", "FxError", "ModelSpec"]
 
 
 def _i32(a):
@@ -413,6 +413,81 @@ class MixedPrecisionSolver(LinearSolver):
     def setup(self, op, stream=None):
         super().setup(op, stream)
         check(lib().fx_solver_set_inner_tolerance(self._h, self.inner_tolerance))
+
+
+class BatchEngine:
+    """Many box meshes resident on one device and solved together (fx_engine_*): per slot FP32
+    Jacobi-PCG inside FP64 iterative refinement, the same bits as MixedPrecisionSolver on that mesh
+    alone; one launch per operator apply over every running slot's element tiles.
+
+    admit() takes an InternalForce (kept alive here until its slot is retired) and a host
+    right-hand side; round() advances every running slot by one refinement round; finished() and
+    retire() hand results back. try_admit() returns None instead of raising when the engine is full.
+    """
+
+    def __init__(self, capacity: int, max_slots: int, k: OperatorCoefficients = None, options: SolveOptions = None,
+                 inner_tolerance: float = 1e-4, device: int = 0):
+        o = options or SolveOptions(relative_tolerance=1e-8)
+        k = k or OperatorCoefficients()
+        opts = L.fx_solve_opts(o.relative_tolerance, o.absolute_tolerance, o.max_iterations, o.lanes, o.restart, 0)
+        h = C.c_void_p()
+        check(lib().fx_engine_create(device, capacity, max_slots, k.c(), opts, inner_tolerance, C.byref(h)))
+        self._h = h
+        self.device = device
+        self._forces = {}
+
+    def admit(self, force: InternalForce, b: np.ndarray) -> int:
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        slot = C.c_int32()
+        check(lib().fx_engine_admit(self._h, force._h, b.ctypes.data_as(L.p_f64), C.byref(slot)))
+        self._forces[slot.value] = force
+        return slot.value
+
+    def try_admit(self, force: InternalForce, b: np.ndarray):
+        try:
+            return self.admit(force, b)
+        except FxError as e:
+            if e.code == L.FX_E_NOMEM:
+                return None
+            raise
+
+    def round(self) -> int:
+        running = C.c_int32()
+        check(lib().fx_engine_round(self._h, C.byref(running)))
+        return running.value
+
+    def finished(self, slot: int) -> bool:
+        f = C.c_int32()
+        check(lib().fx_engine_finished(self._h, slot, C.byref(f)))
+        return bool(f.value)
+
+    def retire(self, slot: int, n: int = None):
+        force = self._forces[slot]
+        n = force.info()["num_equations"] if n is None else n
+        x = np.empty(n)
+        r = L.fx_solve_result()
+        check(lib().fx_engine_retire(self._h, slot, x.ctypes.data_as(L.p_f64), C.byref(r)))
+        del self._forces[slot]
+        return x, SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual, r.final_residual,
+                              bool(r.indefinite), r.refinements)
+
+    def slots(self):
+        return list(self._forces)
+
+    def info(self) -> dict:
+        a = (C.c_int64 * 6)()
+        check(lib().fx_engine_info(self._h, a))
+        keys = ["capacity", "in_use", "max_slots", "slots_in_use", "rounds", "vector_bytes"]
+        return dict(zip(keys, list(a)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().fx_engine_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
+            self._h = None
 
 
 class VectorOps:

@@ -125,6 +125,14 @@ PROTOTYPES = {
     "fx_newmark_predict": (C.c_int, [C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, vp]),
     "fx_newmark_update": (C.c_int, [C.c_int64, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+    "fx_engine_create": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, fx_coeffs, fx_solve_opts, C.c_double,
+                                   C.POINTER(vp)]),
+    "fx_engine_destroy": (None, [vp]),
+    "fx_engine_admit": (C.c_int, [vp, vp, p_f64, C.POINTER(C.c_int32)]),
+    "fx_engine_round": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+    "fx_engine_finished": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_int32)]),
+    "fx_engine_retire": (C.c_int, [vp, C.c_int32, p_f64, C.POINTER(fx_solve_result)]),
+    "fx_engine_info": (C.c_int, [vp, C.POINTER(C.c_int64)]),
 }
 
 _lib = None

@@ -37,6 +37,7 @@ CUDA_SOURCES = [
     ("vector.cu", []),
     ("solve.cu", []),
     ("stepping.cu", []),
+    ("batch.cu", []),
 ]
 CXX_SOURCES = ["api.cpp", "compile.cpp"]
 

@@ -1,0 +1,772 @@
+// Batched and served solves: many independent box-grid meshes resident on one GPU ("slots"),
+// solved together. Each slot is one fx_force with its own right-hand side and solution; the
+// engine solves K_eff x = b for every running slot by FP32 Jacobi-PCG inside FP64 iterative
+// refinement (the FX_SOLVER_IR method of solve.cu, step for step), with
+//   - one launch per operator apply for all slots: the box kernel over a work list of every
+//     running slot's element tiles (k_box_batch), each slot with its own maps, coefficient
+//     tables, vectors and skip flag;
+//   - per-slot CG scalars and stopping flags on the device (a slot that has converged is
+//     skipped by every kernel while the others continue);
+//   - the inner iterations as CUDA graphs of 8 iterations over the whole batch.
+//
+// The vectors of all slots live in one set of engine vectors; slot s owns the entries
+// [off_s, off_s + n_s), off_s a multiple of the 2048-entry reduction chunk, so a slot's chunks
+// hold its own entries only. Its reductions are the documented chunk/lane order over its own
+// range (the second level a warp per slot over its chunk sums), exactly as a single solve of
+// the same mesh: a slot's result is bit for bit the same alone and in any mix.
+//
+// Serving (the host loop above) works in rounds: fx_engine_round runs one refinement round
+// (FP64 residual, FP32 inner solve, FP64 correction) of every running slot; between rounds the
+// host admits new requests into free slots and chunk ranges and retires finished ones.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "force.hpp"
+#include "vector.hpp"
+
+namespace fx {
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int64_t kMaxSlotChunks = 2048;  // one level of chunk sums: n <= 2048 * 2048 per slot
+
+// per-slot scalars
+enum : int {
+  S_RZ = 0, S_PAP, S_ALPHA, S_BETA, S_RNORM, S_TOL, S_RHS, S_RR, S_RZNEW, S_INIT,  // inner CG
+  O_RR, O_BB, O_BNORM, O_RNORM, O_INIT,                                             // outer
+  NSC = 16
+};
+// per-slot flags
+enum : int {
+  F_DONE = 0,  // inner solve finished (the FP32 apply's skip flag)
+  F_CONV, F_INDEF, F_ITERS, F_MAXIT,
+  G_SKIP,      // not in this round's outer step (the FP64 apply's skip flag)
+  G_FIN,       // finished (converged or given up)
+  G_CONV,      // converged to the FP64 tolerance
+  G_OUTER, G_INNER, G_INNER_RAN,
+  NFL = 12
+};
+
+struct SlotDev {
+  int64_t off, n;  // entries
+  int64_t c0, nc;  // chunks
+};
+
+__device__ __forceinline__ int slot_of_chunk(const int* chunk_slot, int64_t c) { return chunk_slot[c]; }
+
+// chunk sums of x.y (T accumulated in double, fused multiply-adds, lane order) of the chunks of
+// slots whose flag `gate` is 0; column `col` of part
+template <class T>
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_dot(const T* __restrict__ x, const T* __restrict__ y, int64_t nchunks, const int* __restrict__ chunk_slot,
+            const SlotDev* __restrict__ sd, const int* __restrict__ fl, int gate, int lanes, double* __restrict__ part) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + gate]) return;
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  double acc = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes)
+      acc = fma(static_cast<double>(x[begin + k]), static_cast<double>(y[begin + k]), acc);
+  double total = 0.0;
+  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  if (lane == 0) part[c] = total;
+}
+
+// second level: slot s's `ncol` columns of chunk sums (column j at part + j * nchunks) into
+// sc[s * NSC + dst + j], one warp per (slot, column), for slots whose flag `gate` is 0
+__global__ void k_b_level(const double* __restrict__ part, int64_t nchunks, int ncol, const SlotDev* __restrict__ sd,
+                          const int* __restrict__ fl, int gate, int nslots, int lanes, const int* __restrict__ used,
+                          double* __restrict__ sc, int dst) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= nslots * ncol) return;
+  const int s = w / ncol, j = w % ncol;
+  if (!used[s] || fl[s * NFL + gate]) return;
+  const double* p = part + static_cast<int64_t>(j) * nchunks + sd[s].c0;
+  const int64_t nc = sd[s].nc;
+  double acc = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < nc; k += lanes) acc += p[k];
+  double total = 0.0;
+  for (int l = 0; l < lanes; ++l) total += __shfl_sync(0xffffffffu, acc, l);
+  if (lane == 0) sc[s * NSC + dst + j] = total;
+}
+
+// outer step: r = b - ap (FP64); chunk sums of r.r (column 0) and b.b (column 1, at part + ld)
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_residual(const double* __restrict__ b, const double* __restrict__ ap, double* __restrict__ r, int64_t nchunks,
+                 const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, const int* __restrict__ fl,
+                 int lanes, double* __restrict__ part, int64_t ld) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + G_SKIP]) return;
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  for (int64_t k = lane; k < len; k += 32) r[begin + k] = b[begin + k] - ap[begin + k];
+  __syncwarp();
+  double srr = 0.0, sbb = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      srr = fma(r[begin + k], r[begin + k], srr);
+      sbb = fma(b[begin + k], b[begin + k], sbb);
+    }
+  double trr = 0.0, tbb = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    tbb += __shfl_sync(0xffffffffu, sbb, j);
+  }
+  if (lane == 0) {
+    part[c] = trr;
+    part[ld + c] = tbb;
+  }
+}
+
+// per slot: the outer test (ir: ||b - K x|| <= max(rtol ||b||, atol)), then the inner solve's
+// limits, or the end of the slot's solve
+__global__ void k_b_outer(double* sc, int* fl, const int* used, int nslots, double rtol, double atol, int max_outer,
+                          int max_it) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !used[s]) return;
+  int* f = fl + s * NFL;
+  double* c = sc + s * NSC;
+  if (f[G_SKIP]) return;
+  if (f[G_OUTER] == 0) {
+    c[O_BNORM] = sqrt(c[O_BB]);
+    c[O_INIT] = sqrt(c[O_RR]);
+  }
+  const double rn = sqrt(c[O_RR]);
+  c[O_RNORM] = rn;
+  const double tol = rtol * c[O_BNORM];
+  if (rn <= (tol > atol ? tol : atol)) {
+    f[G_CONV] = 1;
+    f[G_FIN] = 1;
+  } else if (f[G_OUTER] >= max_outer || f[G_INNER] >= max_it) {
+    f[G_FIN] = 1;
+  }
+  if (f[G_FIN]) {
+    f[F_DONE] = 1;
+    f[G_INNER_RAN] = 0;
+    return;
+  }
+  f[F_DONE] = 0;
+  f[F_MAXIT] = max_it - f[G_INNER];
+  f[G_INNER_RAN] = 1;
+}
+
+// inner setup: r32 = (float) r, d = 0; CG begin from d = 0 (K d = 0): rr = r32, z = inv r32,
+// p = z; chunk sums of rr.rr (column 0) and rr.z (column 1, at part + ld)
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_inner_begin(const double* __restrict__ r, float* __restrict__ r32, float* __restrict__ d,
+                    float* __restrict__ rr, float* __restrict__ p, const float* __restrict__ inv, int64_t nchunks,
+                    const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, const int* __restrict__ fl,
+                    int lanes, double* __restrict__ part, int64_t ld) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + F_DONE]) return;
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  for (int64_t k = lane; k < len; k += 32) {
+    const int64_t i = begin + k;
+    r32[i] = static_cast<float>(r[i]);
+    d[i] = 0.f;
+  }
+  __syncwarp();
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      const float ri = fmaf(-1.f, 0.f, r32[i]);
+      const float zi = inv[i] * ri;
+      rr[i] = ri;
+      p[i] = zi;
+      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+    }
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    part[c] = trr;
+    part[ld + c] = trz;
+  }
+}
+
+__global__ void k_b_inner_start(double* sc, int* fl, const int* used, int nslots, double rtol) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !used[s]) return;
+  int* f = fl + s * NFL;
+  double* c = sc + s * NSC;
+  if (f[F_DONE]) return;
+  c[S_RHS] = sqrt(c[S_RR]);  // b.b of the inner system: the same sum as r.r at d = 0
+  const double rn = sqrt(c[S_RR]);
+  c[S_RNORM] = rn;
+  c[S_INIT] = rn;
+  c[S_RZ] = c[S_RZNEW];
+  const double tol = rtol * c[S_RHS];
+  c[S_TOL] = tol > 0.0 ? tol : 0.0;
+  f[F_ITERS] = 0;
+  f[F_INDEF] = 0;
+  f[F_CONV] = rn <= c[S_TOL];
+  f[F_DONE] = f[F_CONV] || f[F_MAXIT] <= 0;
+}
+
+__global__ void k_b_alpha(double* sc, int* fl, const int* used, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !used[s]) return;
+  int* f = fl + s * NFL;
+  double* c = sc + s * NSC;
+  if (f[F_DONE]) return;
+  const double pap = c[S_PAP];
+  if (!(pap > 0.0)) {
+    f[F_INDEF] = 1;
+    f[F_DONE] = 1;
+    return;
+  }
+  c[S_ALPHA] = c[S_RZ] / pap;
+}
+
+// d += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (column 1 at part + ld)
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_update(const double* __restrict__ sc, const int* __restrict__ fl, const float* __restrict__ p,
+               const float* __restrict__ ap, const float* __restrict__ inv, float* __restrict__ d,
+               float* __restrict__ rr, int64_t nchunks, const int* __restrict__ chunk_slot,
+               const SlotDev* __restrict__ sd, int lanes, double* __restrict__ part, int64_t ld) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + F_DONE]) return;
+  const float alpha = static_cast<float>(sc[s * NSC + S_ALPHA]);
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      d[i] = fmaf(alpha, p[i], d[i]);
+      const float ri = fmaf(-alpha, ap[i], rr[i]);
+      rr[i] = ri;
+      const float zi = inv[i] * ri;
+      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+    }
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    part[c] = trr;
+    part[ld + c] = trz;
+  }
+}
+
+__global__ void k_b_beta(double* sc, int* fl, const int* used, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !used[s]) return;
+  int* f = fl + s * NFL;
+  double* c = sc + s * NSC;
+  if (f[F_DONE]) return;
+  const double rn = sqrt(c[S_RR]);
+  c[S_RNORM] = rn;
+  const int it = ++f[F_ITERS];
+  if (rn <= c[S_TOL]) {
+    f[F_CONV] = 1;
+    f[F_DONE] = 1;
+    return;
+  }
+  if (it >= f[F_MAXIT]) {
+    f[F_DONE] = 1;
+    return;
+  }
+  c[S_BETA] = c[S_RZNEW] / c[S_RZ];
+  c[S_RZ] = c[S_RZNEW];
+}
+
+// p = inv rr + beta p (the beta of a slot that finished this iteration is stale: its p is
+// never read again)
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_p(const double* __restrict__ sc, const int* __restrict__ fl, const float* __restrict__ inv,
+          const float* __restrict__ rr, float* __restrict__ p, int64_t nchunks, const int* __restrict__ chunk_slot,
+          const SlotDev* __restrict__ sd) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + F_DONE]) return;
+  const float beta = static_cast<float>(sc[s * NSC + S_BETA]);
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  for (int64_t k = lane; k < len; k += 32) {
+    const int64_t i = begin + k;
+    p[i] = fmaf(beta, p[i], inv[i] * rr[i]);
+  }
+}
+
+// x += (double) d for slots that ran an inner solve this round; the round's counters
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_correct(const float* __restrict__ d, double* __restrict__ x, int64_t nchunks,
+                const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, const int* __restrict__ fl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + G_SKIP] || !fl[s * NFL + G_INNER_RAN]) return;
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  for (int64_t k = lane; k < len; k += 32) x[begin + k] += static_cast<double>(d[begin + k]);
+}
+
+__global__ void k_b_round_end(int* fl, const int* used, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !used[s]) return;
+  int* f = fl + s * NFL;
+  if (f[G_SKIP] || !f[G_INNER_RAN]) return;
+  f[G_INNER] += f[F_ITERS];
+  f[G_OUTER] += 1;
+  if (f[F_ITERS] == 0 && !f[F_CONV]) f[G_FIN] = 1;  // the inner solve made no progress
+  f[G_INNER_RAN] = 0;
+}
+
+// slot set-up: inverse diagonal (FP64 and FP32), zero x
+__global__ void k_b_setup(const double* __restrict__ diag, double* __restrict__ inv, float* __restrict__ inv32,
+                          double* __restrict__ x, int64_t n, int* zeros) {
+  int local = 0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    local += diag[i] == 0.0;
+    inv[i] = 1.0 / diag[i];
+    inv32[i] = static_cast<float>(1.0 / diag[i]);
+    x[i] = 0.0;
+  }
+  if (local) atomicAdd(zeros, local);
+}
+
+unsigned chunk_grid(int64_t nchunks) { return static_cast<unsigned>(std::max<int64_t>(1, (nchunks + kWarps - 1) / kWarps)); }
+
+}  // namespace
+
+struct Engine {
+  int device = 0;
+  cudaStream_t cs = nullptr;
+  int max_slots = 0;
+  int64_t nchunks = 0;  // capacity in chunks
+  double k[3] = {1, 0, 0};
+  fx_solve_opts o{};
+  double inner_rtol = 1e-4;
+  int max_outer = 50;
+  // vectors over the capacity
+  DeviceArray<double> b, x, r, ap, inv;
+  DeviceArray<float> r32, d32, rr32, p32, ap32, inv32;
+  DeviceArray<int> chunk_slot;
+  DeviceArray<double> part;  // [2][nchunks]
+  DeviceArray<double> sc;
+  DeviceArray<int> fl, used_dev, zeros;
+  DeviceArray<SlotDev> sd_dev;
+  DeviceArray<unsigned char> inst64, inst32;  // descriptors per slot
+  DeviceArray<int4> work;
+  int nwork = 0;
+  // host state
+  struct Slot {
+    bool used = false;
+    fx_force* f = nullptr;
+    int64_t c0 = 0, nc = 0, n = 0;
+  };
+  std::vector<Slot> slots;
+  std::vector<int> chunk_slot_h;
+  std::vector<int> used_h;
+  int* fl_h = nullptr;      // pinned [max_slots * NFL]
+  double* sc_h = nullptr;   // pinned [max_slots * NSC]
+  size_t a64 = 0, a32 = 0;  // descriptor sizes
+  int64_t high = 0;         // chunks in use up to here
+  bool dirty = true;        // the work list / slot tables changed
+  cudaGraphExec_t graph = nullptr;
+  int64_t rounds = 0;
+
+  ~Engine() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (fl_h) cudaFreeHost(fl_h);
+    if (sc_h) cudaFreeHost(sc_h);
+    if (cs) cudaStreamDestroy(cs);
+  }
+
+  int64_t find_range(int64_t need) const {
+    int64_t run = 0;
+    for (int64_t c = 0; c < nchunks; ++c) {
+      run = chunk_slot_h[c] < 0 ? run + 1 : 0;
+      if (run == need) return c - need + 1;
+    }
+    return -1;
+  }
+
+  void read_flags() {
+    FX_CUDA(cudaMemcpyAsync(fl_h, fl.ptr, sizeof(int) * NFL * max_slots, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaMemcpyAsync(sc_h, sc.ptr, sizeof(double) * NSC * max_slots, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+  }
+
+  void upload_tables() {
+    if (!dirty) return;
+    // chunk owners, slot table, used flags, work list of every slot that is not finished
+    std::vector<SlotDev> sdh(static_cast<size_t>(max_slots), SlotDev{0, 0, 0, 0});
+    high = 0;
+    for (int s = 0; s < max_slots; ++s)
+      if (slots[s].used) {
+        sdh[s] = SlotDev{slots[s].c0 * kChunk, slots[s].n, slots[s].c0, slots[s].nc};
+        high = std::max(high, slots[s].c0 + slots[s].nc);
+      }
+    std::vector<int4> wl;
+    for (int s = 0; s < max_slots; ++s) {
+      if (!slots[s].used || fl_h[s * NFL + G_FIN]) continue;
+      int gx, gy, gz;
+      box_batch_tiles(slots[s].f->s, gx, gy, gz);
+      for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < gy; ++y)
+          for (int xx = 0; xx < gx; ++xx) wl.push_back(make_int4(s, xx, y, z));
+    }
+    nwork = static_cast<int>(wl.size());
+    if (work.n < wl.size()) work.alloc(std::max<size_t>(wl.size(), 1024));
+    FX_CUDA(cudaMemcpyAsync(sd_dev.ptr, sdh.data(), sizeof(SlotDev) * max_slots, cudaMemcpyHostToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(chunk_slot.ptr, chunk_slot_h.data(), sizeof(int) * nchunks, cudaMemcpyHostToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(used_dev.ptr, used_h.data(), sizeof(int) * max_slots, cudaMemcpyHostToDevice, cs));
+    if (nwork)
+      FX_CUDA(cudaMemcpyAsync(work.ptr, wl.data(), sizeof(int4) * wl.size(), cudaMemcpyHostToDevice, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));  // the host vectors above go out of scope
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    dirty = false;
+  }
+
+  void level(int ncol, int gate, int dst) {
+    const int warps = max_slots * ncol;
+    k_b_level<<<(warps + 7) / 8, 256, 0, cs>>>(part.ptr, nchunks, ncol, sd_dev.ptr, fl.ptr, gate, max_slots, o.lanes,
+                                               used_dev.ptr, sc.ptr, dst);
+    FX_LAUNCH_CHECK("batch_level");
+  }
+  unsigned slot_grid() const { return static_cast<unsigned>((max_slots + 127) / 128); }
+
+  void inner_iteration() {
+    const unsigned g = chunk_grid(high);
+    box_batch_apply(true, inst32.ptr, work.ptr, nwork, cs);
+    k_b_dot<float><<<g, 32 * kWarps, 0, cs>>>(p32.ptr, ap32.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, F_DONE,
+                                              o.lanes, part.ptr);
+    level(1, F_DONE, S_PAP);
+    k_b_alpha<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots);
+    k_b_update<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr, high,
+                                          chunk_slot.ptr, sd_dev.ptr, o.lanes, part.ptr, nchunks);
+    level(2, F_DONE, S_RR);
+    k_b_beta<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots);
+    k_b_p<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv32.ptr, rr32.ptr, p32.ptr, high, chunk_slot.ptr, sd_dev.ptr);
+    FX_LAUNCH_CHECK("batch_inner");
+  }
+
+  bool any_inner_running() const {
+    for (int s = 0; s < max_slots; ++s)
+      if (slots[s].used && !fl_h[s * NFL + F_DONE]) return true;
+    return false;
+  }
+
+  // one refinement round of every running slot; returns the number of running slots it saw
+  int round() {
+    read_flags();
+    int running = 0;
+    for (int s = 0; s < max_slots; ++s) {
+      if (!slots[s].used) continue;
+      const bool run = !fl_h[s * NFL + G_FIN];
+      running += run;
+      if (fl_h[s * NFL + G_SKIP] != !run) {
+        fl_h[s * NFL + G_SKIP] = !run;
+        FX_CUDA(cudaMemcpyAsync(fl.ptr + s * NFL + G_SKIP, fl_h + s * NFL + G_SKIP, sizeof(int),
+                                cudaMemcpyHostToDevice, cs));
+      }
+    }
+    if (!running) return 0;
+    upload_tables();
+    const unsigned g = chunk_grid(high);
+    // outer: r = b - K x (FP64), norms, test
+    box_batch_apply(false, inst64.ptr, work.ptr, nwork, cs);
+    k_b_residual<<<g, 32 * kWarps, 0, cs>>>(b.ptr, ap.ptr, r.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
+                                            part.ptr, nchunks);
+    level(2, G_SKIP, O_RR);
+    k_b_outer<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, o.rtol, o.atol, max_outer,
+                                           o.max_iterations);
+    // inner: FP32 PCG from d = 0
+    k_b_inner_begin<<<g, 32 * kWarps, 0, cs>>>(r.ptr, r32.ptr, d32.ptr, rr32.ptr, p32.ptr, inv32.ptr, high,
+                                               chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
+    level(2, F_DONE, S_RR);
+    k_b_inner_start<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, inner_rtol);
+    FX_LAUNCH_CHECK("batch_outer");
+    // the first block of iterations directly, then graphs of 8
+    const int block = 8;
+    for (int i = 0; i < block; ++i) inner_iteration();
+    read_flags();
+    while (any_inner_running()) {
+      if (!graph) {
+        cudaGraph_t gr = nullptr;
+        FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int i = 0; i < block; ++i) inner_iteration();
+        } catch (...) {
+          cudaStreamEndCapture(cs, &gr);
+          if (gr) cudaGraphDestroy(gr);
+          throw;
+        }
+        FX_CUDA(cudaStreamEndCapture(cs, &gr));
+        const cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
+        cudaGraphDestroy(gr);
+        FX_CUDA(e);
+      }
+      FX_CUDA(cudaGraphLaunch(graph, cs));
+      read_flags();
+    }
+    k_b_correct<<<g, 32 * kWarps, 0, cs>>>(d32.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
+    k_b_round_end<<<slot_grid(), 128, 0, cs>>>(fl.ptr, used_dev.ptr, max_slots);
+    FX_LAUNCH_CHECK("batch_correct");
+    read_flags();
+    // slots that finished leave the work list
+    for (int s = 0; s < max_slots; ++s)
+      if (slots[s].used && fl_h[s * NFL + G_FIN]) dirty = true;
+    ++rounds;
+    return running;
+  }
+
+  void admit(fx_force* f, const double* b_host, int* slot_out) {
+    ForceState& s = f->s;
+    if (s.device != device) throw Error(FX_E_INVALID, "fx_engine_admit: the mesh lives on another device");
+    if (!s.use_box()) throw Error(FX_E_UNSUPPORTED, "fx_engine_admit: the batched operator needs a box grid: " + s.box.why_not);
+    const int64_t n = s.neq;
+    if (n <= 0) throw Error(FX_E_INVALID, "fx_engine_admit: no equations");
+    const int64_t nc = chunks_of(n);
+    if (nc > kMaxSlotChunks) throw Error(FX_E_UNSUPPORTED, "fx_engine_admit: more than 2048 * 2048 equations");
+    int slot = -1;
+    for (int i = 0; i < max_slots; ++i)
+      if (!slots[i].used) {
+        slot = i;
+        break;
+      }
+    if (slot < 0) throw Error(FX_E_NOMEM, "fx_engine_admit: no free slot");
+    const int64_t c0 = find_range(nc);
+    if (c0 < 0) throw Error(FX_E_NOMEM, "fx_engine_admit: no free range of " + std::to_string(nc) + " chunks");
+    const int64_t off = c0 * kChunk, span = nc * kChunk;
+    // zero the slot's range of every vector, then b, the inverse diagonals and x
+    FX_CUDA(cudaMemsetAsync(b.ptr + off, 0, sizeof(double) * span, cs));
+    FX_CUDA(cudaMemsetAsync(x.ptr + off, 0, sizeof(double) * span, cs));
+    FX_CUDA(cudaMemsetAsync(r.ptr + off, 0, sizeof(double) * span, cs));
+    FX_CUDA(cudaMemsetAsync(ap.ptr + off, 0, sizeof(double) * span, cs));
+    FX_CUDA(cudaMemsetAsync(inv.ptr + off, 0, sizeof(double) * span, cs));
+    for (float* v : {r32.ptr, d32.ptr, rr32.ptr, p32.ptr, ap32.ptr, inv32.ptr})
+      FX_CUDA(cudaMemsetAsync(v + off, 0, sizeof(float) * span, cs));
+    FX_CUDA(cudaMemcpyAsync(b.ptr + off, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+    general_diagonal(s, k, r.ptr + off, cs);  // the diagonal, in r for now
+    FX_CUDA(cudaMemsetAsync(zeros.ptr, 0, sizeof(int), cs));
+    k_b_setup<<<static_cast<unsigned>(std::min<int64_t>((n + 255) / 256, 4096)), 256, 0, cs>>>(
+        r.ptr + off, inv.ptr + off, inv32.ptr + off, x.ptr + off, n, zeros.ptr);
+    FX_LAUNCH_CHECK("batch_setup");
+    int nz = 0;
+    FX_CUDA(cudaMemcpyAsync(&nz, zeros.ptr, sizeof(int), cudaMemcpyDeviceToHost, cs));
+    // descriptors: FP64 operator x -> ap (skipped while the slot is not in the outer step),
+    // FP32 operator p32 -> ap32 (skipped once its inner solve is done)
+    std::vector<unsigned char> d64(a64), d32h(a32);
+    box_fill_args(s, k, false, x.ptr + off, ap.ptr + off, fl.ptr + slot * NFL + G_SKIP, d64.data());
+    box_fill_args(s, k, true, p32.ptr + off, ap32.ptr + off, fl.ptr + slot * NFL + F_DONE, d32h.data());
+    FX_CUDA(cudaMemcpyAsync(inst64.ptr + static_cast<size_t>(slot) * a64, d64.data(), a64, cudaMemcpyHostToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(inst32.ptr + static_cast<size_t>(slot) * a32, d32h.data(), a32, cudaMemcpyHostToDevice, cs));
+    std::vector<int> f0(NFL, 0);
+    f0[F_DONE] = 1;
+    std::vector<double> s0(NSC, 0.0);
+    FX_CUDA(cudaMemcpyAsync(fl.ptr + slot * NFL, f0.data(), sizeof(int) * NFL, cudaMemcpyHostToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(sc.ptr + slot * NSC, s0.data(), sizeof(double) * NSC, cudaMemcpyHostToDevice, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+    if (nz > 0) {
+      // leave the range free again: nothing points at it
+      throw Error(FX_E_INVALID, "Jacobi: " + std::to_string(nz) + " zero diagonal entries");
+    }
+    std::memcpy(fl_h + slot * NFL, f0.data(), sizeof(int) * NFL);
+    slots[slot] = Slot{true, f, c0, nc, n};
+    for (int64_t c = c0; c < c0 + nc; ++c) chunk_slot_h[c] = slot;
+    used_h[slot] = 1;
+    dirty = true;
+    *slot_out = slot;
+  }
+
+  void retire(int slot, double* x_host, fx_solve_result* res) {
+    if (slot < 0 || slot >= max_slots || !slots[slot].used) throw Error(FX_E_INVALID, "fx_engine_retire: no such slot");
+    read_flags();
+    const int* f = fl_h + slot * NFL;
+    const double* c = sc_h + slot * NSC;
+    const Slot& sl = slots[slot];
+    if (x_host)
+      FX_CUDA(cudaMemcpyAsync(x_host, x.ptr + sl.c0 * kChunk, sizeof(double) * sl.n, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+    if (res) {
+      *res = fx_solve_result{};
+      res->converged = f[G_CONV];
+      res->iterations = f[G_INNER];
+      res->refinements = f[G_OUTER];
+      res->rhs_norm = c[O_BNORM];
+      res->initial_residual = c[O_INIT];
+      res->final_residual = c[O_RNORM];
+      res->status = f[G_CONV] ? FX_OK : FX_E_DIVERGED;
+    }
+    for (int64_t cc = sl.c0; cc < sl.c0 + sl.nc; ++cc) chunk_slot_h[cc] = -1;
+    slots[slot] = Slot{};
+    used_h[slot] = 0;
+    dirty = true;
+  }
+};
+
+}  // namespace fx
+
+struct fx_engine {
+  fx::Engine e;
+};
+
+namespace {
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return FX_OK;
+  } catch (const fx::Error& e) {
+    fx::set_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    fx::set_error(e.what());
+    return FX_E_INVALID;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fx_engine_create(int32_t device, int64_t capacity, int32_t max_slots, fx_coeffs k, fx_solve_opts o,
+                     double inner_rtol, fx_engine** out) {
+  return guard([&] {
+    if (!out || capacity <= 0 || max_slots <= 0) throw fx::Error(FX_E_INVALID, "fx_engine_create: bad arguments");
+    if (!(inner_rtol > 0.0 && inner_rtol < 1.0)) throw fx::Error(FX_E_INVALID, "inner tolerance must be in (0, 1)");
+    if (o.lanes <= 0) o.lanes = 32;
+    if (o.lanes > 32) throw fx::Error(FX_E_INVALID, "lanes must be in 1..32");
+    if (o.max_iterations < 0) throw fx::Error(FX_E_INVALID, "max_iterations must be >= 0");
+    FX_CUDA(cudaSetDevice(device));
+    auto* h = new fx_engine;
+    fx::Engine& e = h->e;
+    try {
+      e.device = device;
+      e.max_slots = max_slots;
+      e.k[0] = k.stiffness;
+      e.k[1] = k.damping;
+      e.k[2] = k.mass;
+      e.o = o;
+      e.inner_rtol = inner_rtol;
+      e.nchunks = fx::chunks_of(capacity);
+      const size_t n = static_cast<size_t>(e.nchunks * fx::kChunk);
+      FX_CUDA(cudaStreamCreateWithFlags(&e.cs, cudaStreamNonBlocking));
+      for (auto* v : {&e.b, &e.x, &e.r, &e.ap, &e.inv}) v->alloc(n);
+      for (auto* v : {&e.r32, &e.d32, &e.rr32, &e.p32, &e.ap32, &e.inv32}) v->alloc(n);
+      e.chunk_slot.alloc(static_cast<size_t>(e.nchunks));
+      e.part.alloc(static_cast<size_t>(e.nchunks) * 2);
+      e.sc.alloc(static_cast<size_t>(max_slots) * fx::NSC);
+      e.fl.alloc(static_cast<size_t>(max_slots) * fx::NFL);
+      e.used_dev.alloc(static_cast<size_t>(max_slots));
+      e.zeros.alloc(1);
+      e.sd_dev.alloc(static_cast<size_t>(max_slots));
+      e.a64 = fx::box_args_bytes(false);
+      e.a32 = fx::box_args_bytes(true);
+      e.inst64.alloc(e.a64 * max_slots);
+      e.inst32.alloc(e.a32 * max_slots);
+      e.work.alloc(1024);
+      e.slots.assign(static_cast<size_t>(max_slots), fx::Engine::Slot{});
+      e.chunk_slot_h.assign(static_cast<size_t>(e.nchunks), -1);
+      e.used_h.assign(static_cast<size_t>(max_slots), 0);
+      FX_CUDA(cudaMallocHost(&e.fl_h, sizeof(int) * fx::NFL * max_slots));
+      FX_CUDA(cudaMallocHost(&e.sc_h, sizeof(double) * fx::NSC * max_slots));
+      std::vector<int> f0(static_cast<size_t>(max_slots) * fx::NFL, 0);
+      for (int s = 0; s < max_slots; ++s) f0[s * fx::NFL + fx::F_DONE] = 1;
+      std::memcpy(e.fl_h, f0.data(), sizeof(int) * f0.size());
+      FX_CUDA(cudaMemcpy(e.fl.ptr, f0.data(), sizeof(int) * f0.size(), cudaMemcpyHostToDevice));
+      FX_CUDA(cudaMemset(e.sc.ptr, 0, sizeof(double) * fx::NSC * max_slots));
+      FX_CUDA(cudaMemset(e.used_dev.ptr, 0, sizeof(int) * max_slots));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+void fx_engine_destroy(fx_engine* e) { delete e; }
+
+int fx_engine_admit(fx_engine* e, fx_force* f, const double* b_host, int32_t* slot) {
+  return guard([&] {
+    if (!e || !f || !b_host || !slot) throw fx::Error(FX_E_INVALID, "fx_engine_admit: bad arguments");
+    FX_CUDA(cudaSetDevice(e->e.device));
+    int s = -1;
+    e->e.admit(f, b_host, &s);
+    *slot = s;
+  });
+}
+
+int fx_engine_round(fx_engine* e, int32_t* running) {
+  return guard([&] {
+    if (!e) throw fx::Error(FX_E_INVALID, "fx_engine_round: null engine");
+    FX_CUDA(cudaSetDevice(e->e.device));
+    const int r = e->e.round();
+    if (running) *running = r;
+  });
+}
+
+int fx_engine_finished(fx_engine* e, int32_t slot, int32_t* finished) {
+  return guard([&] {
+    if (!e || !finished || slot < 0 || slot >= e->e.max_slots) throw fx::Error(FX_E_INVALID, "fx_engine_finished: bad arguments");
+    *finished = e->e.slots[slot].used && e->e.fl_h[slot * fx::NFL + fx::G_FIN];
+  });
+}
+
+int fx_engine_retire(fx_engine* e, int32_t slot, double* x_host, fx_solve_result* r) {
+  return guard([&] {
+    if (!e) throw fx::Error(FX_E_INVALID, "fx_engine_retire: null engine");
+    FX_CUDA(cudaSetDevice(e->e.device));
+    e->e.retire(slot, x_host, r);
+  });
+}
+
+int fx_engine_info(const fx_engine* e, int64_t* info) {
+  return guard([&] {
+    if (!e || !info) throw fx::Error(FX_E_INVALID, "fx_engine_info: bad arguments");
+    const fx::Engine& g = e->e;
+    int64_t used_chunks = 0, used_slots = 0;
+    for (const auto& s : g.slots)
+      if (s.used) {
+        used_chunks += s.nc;
+        ++used_slots;
+      }
+    info[0] = g.nchunks * fx::kChunk;
+    info[1] = used_chunks * fx::kChunk;
+    info[2] = g.max_slots;
+    info[3] = used_slots;
+    info[4] = g.rounds;
+    info[5] = static_cast<int64_t>(g.nchunks * fx::kChunk) * (5 * 8 + 6 * 4);  // vector bytes
+  });
+}
+
+}  // extern "C"

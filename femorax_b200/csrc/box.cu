@@ -24,6 +24,7 @@
 // registers one plane (equations: two planes) ahead, so global latency overlaps the element work;
 // two barriers per plane.
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 
 #include "force.hpp"
@@ -197,10 +198,11 @@ __device__ __forceinline__ void modal_apply(const CT& k, T t[3][8]) {
 // per node whatever the equation numbering (the reference's RCM numbering puts neighbouring
 // grid nodes hundreds of equations apart). The owners of a plane's nodes leave their sums and
 // equations in shared memory; the stores run in the next iteration, after the barrier.
-// LAYERED: the coefficient tables come from `tab` (layered grids), else from a.coef.
-template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, bool LAYERED>
-__global__ void __launch_bounds__(BX* BY, MINB)
-    k_box(BoxArgs<T> a, const __grid_constant__ BoxTable<typename Coef<T>::type> tab) {
+// One CTA's tile (bx, by, bz) of grid a. LAYERED: the coefficient tables come from *tab (layered
+// grids), else from a.coef.
+template <int BX, int BY, class T, int MODE, bool CACHE, bool LAYERED>
+__device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typename Coef<T>::type>* tab, int bx,
+                                         int by, int bz) {
   using S = Smem<BX, BY, T, MODE>;
   using CT = typename Coef<T>::type;
   constexpr int NT = S::NT, SX = S::SX, NS = S::NS, NB = S::NB, NV = S::NV, D = S::D, NO = S::NO;
@@ -216,8 +218,8 @@ __global__ void __launch_bounds__(BX* BY, MINB)
 
   const int t = threadIdx.x;
   const int ci = t % BX, cj = t / BX;
-  const int i0 = blockIdx.x * (BX - 1), j0 = blockIdx.y * (BY - 1);
-  const int k0 = blockIdx.z * a.kz;
+  const int i0 = bx * (BX - 1), j0 = by * (BY - 1);
+  const int k0 = bz * a.kz;
   const int k1 = min(k0 + a.kz, a.nz + 1);
   const int NXn = a.nx + 1, NYn = a.ny + 1;
   const int64_t plane_stride = static_cast<int64_t>(NXn) * NYn;
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(BX* BY, MINB)
   const int64_t col_off = static_cast<int64_t>(ej) * a.nx + ei;
   const int64_t layer = static_cast<int64_t>(a.nx) * a.ny;
   auto param_of = [&](int ek) {
-    if constexpr (LAYERED) return (ek >= 0 && ek < a.nz) ? static_cast<int>(tab.layer[ek]) : -1;  // same for all threads
+    if constexpr (LAYERED) return (ek >= 0 && ek < a.nz) ? static_cast<int>(tab->layer[ek]) : -1;  // same for all threads
     return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.elem_param[ek * layer + col_off]) : -1;
   };
   // 2D transform of the column's face of plane buffer b (MODE 1: of u + beta v): f = p + 2q
@@ -381,9 +383,9 @@ __global__ void __launch_bounds__(BX* BY, MINB)
     if (p_here >= 0 && (!LAYERED || col_ok)) {
       T body[3] = {T(0), T(0), T(0)};
       if constexpr (LAYERED) {
-        modal_apply<false>(tab.c[p_here], tv);
+        modal_apply<false>(tab->c[p_here], tv);
         if (MODE == 1)
-          for (int d = 0; d < 3; ++d) body[d] = T(tab.c[p_here].body[d]);
+          for (int d = 0; d < 3; ++d) body[d] = T(tab->c[p_here].body[d]);
       } else {
         const CT& k = coef[p_here];
         modal_apply<true>(k, tv);
@@ -447,6 +449,22 @@ __global__ void __launch_bounds__(BX* BY, MINB)
   }
   cp_async_wait<0>();
   if (k1 - 1 >= k0) store_plane();
+}
+
+template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, bool LAYERED>
+__global__ void __launch_bounds__(BX* BY, MINB)
+    k_box(BoxArgs<T> a, const __grid_constant__ BoxTable<typename Coef<T>::type> tab) {
+  box_tile<BX, BY, T, MODE, CACHE, LAYERED>(a, &tab, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Many grids in one launch: CTA b takes work item work[b] = (grid, tile x, tile y, tile z) of the
+// grids inst[] describes (each with its own maps, tables, vectors and skip flag).
+template <int BX, int BY, class T, int MODE, int MINB>
+__global__ void __launch_bounds__(BX* BY, MINB)
+    k_box_batch(const BoxArgs<T>* __restrict__ inst, const int4* __restrict__ work) {
+  const int4 w = work[blockIdx.x];
+  const BoxArgs<T> a = inst[w.x];
+  box_tile<BX, BY, T, MODE, false, false>(a, nullptr, w.y, w.z, w.w);
 }
 
 // ------------------------------------------------------------------ launch variants
@@ -809,10 +827,20 @@ void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cuda
   force_t<float>(s, u, v, f, st);
 }
 
+// Meshes below this many elements take the launch shape that is fastest on large grids (16 x 8
+// columns, 8 planes) without timing.
+constexpr int32_t kTuneMinElements = 262144;
+
 // Times every launch variant and plane count on the operator (FP64, unit stiffness) and keeps the
 // fastest: CUDA events on the stream, median of 5 after 2 warm-ups.
 void box_autotune(ForceState& s, cudaStream_t st) {
   if (!s.box.qualifies) return;
+  if (s.count < kTuneMinElements) {  // launch-bound: timing costs more than it can save
+    s.box.variant = 2;
+    s.box.kz = 8;
+    s.box.tuned = true;
+    return;
+  }
   DeviceArray<double> x, y;
   x.alloc(static_cast<size_t>(std::max(s.neq, 1)));
   y.alloc(static_cast<size_t>(std::max(s.neq, 1)));
@@ -852,6 +880,65 @@ void box_autotune(ForceState& s, cudaStream_t st) {
   s.box.variant = bv;
   s.box.kz = bk;
   s.box.tuned = true;
+}
+
+
+// ------------------------------------------------------------------ batches of grids
+// One launch shape for batches: 16 x 8 element columns, 4 CTAs per SM, kBatchKz node planes per tile.
+namespace {
+constexpr int kBatchBX = 16, kBatchBY = 8, kBatchMinB = 4, kBatchKz = 8;
+
+template <class T>
+void batch_launch(const void* inst, const int4* work, int nwork, cudaStream_t st) {
+  using S = Smem<kBatchBX, kBatchBY, T, 0>;
+  static bool configured = false;
+  if (!configured) {
+    FX_CUDA(cudaFuncSetAttribute(k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
+    configured = true;
+  }
+  k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB>
+      <<<nwork, kBatchBX * kBatchBY, S::bytes, st>>>(static_cast<const BoxArgs<T>*>(inst), work);
+  FX_LAUNCH_CHECK("box_batch");
+}
+
+template <class T>
+void fill_args(ForceState& s, const double k[3], const void* x, void* y, const int* skip, void* dst) {
+  ensure_coef(s, 0, k);
+  BoxArgs<T> a = args<T>(s, sizeof(T) == 8 ? static_cast<const void*>(s.box.coef.ptr) : s.box.coef32.ptr,
+                         static_cast<const T*>(x), nullptr, static_cast<T*>(y));
+  a.kz = kBatchKz;
+  a.skip = skip;
+  if (k[2] != 0.0 && s.has_nodal_mass) {
+    a.nm1 = s.nodal_mass.ptr;
+    a.c1 = k[2];
+  }
+  if (k[1] != 0.0 && s.has_nodal_alpha) {
+    a.nm2 = s.nodal_alpha_mass.ptr;
+    a.c2 = k[1];
+  }
+  std::memcpy(dst, &a, sizeof(a));
+}
+}  // namespace
+
+size_t box_args_bytes(bool f32) { return f32 ? sizeof(BoxArgs<float>) : sizeof(BoxArgs<double>); }
+
+void box_fill_args(ForceState& s, const double k[3], bool f32, const void* x, void* y, const int* skip, void* dst) {
+  if (!s.box.qualifies) throw Error(FX_E_UNSUPPORTED, "batched operator: not a box grid: " + s.box.why_not);
+  if (f32) fill_args<float>(s, k, x, y, skip, dst);
+  else fill_args<double>(s, k, x, y, skip, dst);
+}
+
+void box_batch_tiles(const ForceState& s, int& gx, int& gy, int& gz) {
+  gx = (s.box.nx + 1 + kBatchBX - 2) / (kBatchBX - 1);
+  gy = (s.box.ny + 1 + kBatchBY - 2) / (kBatchBY - 1);
+  gz = (s.box.nz + 1 + kBatchKz - 1) / kBatchKz;
+}
+
+void box_batch_apply(bool f32, const void* inst, const int4* work, int nwork, cudaStream_t st) {
+  if (nwork <= 0) return;
+  if (f32) batch_launch<float>(inst, work, nwork, st);
+  else batch_launch<double>(inst, work, nwork, st);
 }
 
 }  // namespace fx

@@ -135,6 +135,14 @@ void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cuda
 int box_num_variants();
 void box_set_launch(ForceState& s, int variant, int kz);
 void box_autotune(ForceState& s, cudaStream_t st);
+// Batches of box grids in one launch: the per-grid descriptor (box_args_bytes bytes, written by
+// box_fill_args for y = K_eff x with operator coefficients k, FP64 or FP32 vectors x, y and a
+// skip flag), the grid's tile counts, and the launch over a work list of
+// (grid, tile x, tile y, tile z) items.
+size_t box_args_bytes(bool f32);
+void box_fill_args(ForceState& s, const double k[3], bool f32, const void* x, void* y, const int* skip, void* dst);
+void box_batch_tiles(const ForceState& s, int& gx, int& gy, int& gz);
+void box_batch_apply(bool f32, const void* inst, const int4* work, int nwork, cudaStream_t st);
 
 }  // namespace fx
 

@@ -288,6 +288,38 @@ int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, d
 int fx_newmark_update(int64_t n, const double* du, double* u, double* v, double* a, double c2, double c3,
                       void* stream);
 
+/* ------------------------------------------------------------------ batched and served solves
+ * An engine holds many independent meshes ("slots", each one fx_force on the box path, a
+ * structured grid of equal boxes) resident on one device and solves K_eff x = b for all of them
+ * together by FP32 Jacobi-PCG inside FP64 iterative refinement, per slot exactly as
+ * FX_SOLVER_IR (the same bits): one launch per operator apply over the element tiles of every
+ * running slot, per-slot CG scalars and stopping on the device, inner iterations as CUDA graphs.
+ * No counterpart in the reference, which solves one mesh per process
+ * (ConjugateGradient::solve, src/solvers/cg.cpp:24-71, is the per-slot algorithm).
+ *   fx_engine_create   vectors for `capacity` equations in all (rounded to 2048-entry chunks,
+ *                      each slot a whole number of chunks) and `max_slots` slots; operator
+ *                      coefficients k; rtol / atol / max_iterations / lanes as fx_solve_opts;
+ *                      inner_rtol the inner FP32 solve's relative tolerance.
+ *   fx_engine_admit    takes a mesh (the engine uses f until the slot is retired) and its
+ *                      right-hand side (host, num_equations doubles) into a free slot: copies
+ *                      b, builds the Jacobi diagonal, x = 0. FX_E_NOMEM when no slot or no
+ *                      contiguous range of chunks is free (admit again after a retire).
+ *   fx_engine_round    one refinement round of every running slot (FP64 residual and test,
+ *                      FP32 inner solve, FP64 correction); *running = the slots it advanced.
+ *   fx_engine_finished whether a slot's solve has ended (converged or given up).
+ *   fx_engine_retire   copies x (host, may be NULL) and the result out and frees the slot.
+ *   fx_engine_info     info[6] = capacity (equations), equations in use, max slots, slots in
+ *                      use, rounds run, device bytes of the engine's vectors. */
+typedef struct fx_engine fx_engine;
+int fx_engine_create(int32_t device, int64_t capacity, int32_t max_slots, fx_coeffs k, fx_solve_opts o,
+                     double inner_rtol, fx_engine** out);
+void fx_engine_destroy(fx_engine* e);
+int fx_engine_admit(fx_engine* e, fx_force* f, const double* b_host, int32_t* slot);
+int fx_engine_round(fx_engine* e, int32_t* running);
+int fx_engine_finished(fx_engine* e, int32_t slot, int32_t* finished);
+int fx_engine_retire(fx_engine* e, int32_t slot, double* x_host, fx_solve_result* r);
+int fx_engine_info(const fx_engine* e, int64_t* info);
+
 #ifdef __cplusplus
 }
 #endif
