@@ -64,16 +64,33 @@ class Served:
 
 
 def equation_map(compiled):
-    """(node tag, dof 0..2) -> equation (-1 fixed), from the compile step's arrays."""
+    """eq[tag, dof]: the equation of (node tag, dof 0..2), -1 fixed, as an array indexed by tag,
+    from the compile step's arrays."""
     tags = compiled.array("node_tag")
     off = compiled.array("dof_offset")
     eq = compiled.array("eq")
-    where = {int(t): i for i, t in enumerate(tags)}
+    out = np.full((int(tags.max()) + 1, 3), -1, dtype=np.int64)
+    for d in range(3):
+        out[tags, d] = eq[off[:-1] + d]
+    return out
 
-    def eq_of(tag, dof):
-        return int(eq[off[where[int(tag)]] + dof])
 
-    return eq_of
+def top_load(req: Request, eqmap) -> np.ndarray:
+    """Equation-space load of the uniform vertical traction q on the top face: each top quad gives
+    q h^2 / 4 to each of its 4 nodes (a top node carries the shares of the 1, 2 or 4 quads around it)."""
+    share = req.q * req.h * req.h / 4.0
+    ci = np.full(req.nx + 1, 2.0)
+    cj = np.full(req.ny + 1, 2.0)
+    ci[[0, -1]] = 1.0
+    cj[[0, -1]] = 1.0
+    i, j = np.meshgrid(np.arange(req.nx + 1), np.arange(req.ny + 1), indexing="ij")
+    tags = 1 + i + (req.nx + 1) * (j + (req.ny + 1) * req.nz)
+    q = eqmap[tags.ravel(), 2]
+    f = (share * np.outer(ci, cj)).ravel()
+    b = np.zeros(int(eqmap.max()) + 1)
+    keep = q >= 0
+    np.add.at(b, q[keep], f[keep])
+    return b
 
 
 def prepare(req: Request, device: int = 0):
@@ -81,12 +98,7 @@ def prepare(req: Request, device: int = 0):
     spec = meshes.box_model(req.nx, req.ny, req.nz, (req.nx * req.h, req.ny * req.h, req.nz * req.h), E=req.E,
                             nu=req.nu)
     comp = Model(spec).compile()
-    eq_of = equation_map(comp)
-    b = np.zeros(comp.num_equations)
-    for tag, f in meshes.top_traction_rhs(spec, eq_of, req.q).items():
-        q = eq_of(tag, 2)
-        if q >= 0:
-            b[q] += f
+    b = top_load(req, equation_map(comp))
     force = InternalForce(comp.mesh(), device=device)
     return force, b, comp.num_equations
 
