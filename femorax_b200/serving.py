@@ -187,8 +187,24 @@ class Server:
         return served, time.perf_counter() - t0
 
 
-def serve_one_at_a_time(requests, rtol: float = 1e-8, realtime: bool = True, device: int = 0):
-    """The same stream, first come first served, each solved alone by plain FP64 Jacobi-PCG."""
+def resident(requests, device: int = 0, rtol: float = 1e-8):
+    """Prepare every request's mesh up front (the resident state a serving process keeps):
+    {id: (force, b, n)}, and for the one-at-a-time arm a plain FP64 CG per mesh, already created
+    (its work vectors allocated): {id: solver}."""
+    prepared = {r.id: prepare(r, device) for r in requests}
+    solvers = {}
+    for rid, (force, b, n) in prepared.items():
+        cg = ConjugateGradient(SolveOptions(relative_tolerance=rtol))
+        cg.setup(MatrixFreeOperator(force, OperatorCoefficients()))
+        solvers[rid] = cg
+    return prepared, solvers
+
+
+def serve_one_at_a_time(requests, rtol: float = 1e-8, realtime: bool = True, device: int = 0, prepared=None,
+                        solvers=None):
+    """The same stream, first come first served, each solved alone by plain FP64 Jacobi-PCG. With
+    `prepared` / `solvers` (from resident()) the meshes and solvers are resident; otherwise each
+    request is prepared when its turn comes."""
     import torch
     reqs = sorted(requests, key=lambda r: r.arrival)
     dev = torch.device("cuda", device)
@@ -200,10 +216,10 @@ def serve_one_at_a_time(requests, rtol: float = 1e-8, realtime: bool = True, dev
             if wait > 0:
                 time.sleep(wait)
         adm = time.perf_counter() - t0
-        force, b, n = prepare(req, device)
+        force, b, n = prepared[req.id] if prepared else prepare(req, device)
         op = MatrixFreeOperator(force, OperatorCoefficients())
-        cg = ConjugateGradient(SolveOptions(relative_tolerance=rtol))
-        cg.setup(op)
+        cg = solvers[req.id] if solvers else ConjugateGradient(SolveOptions(relative_tolerance=rtol))
+        cg.setup(op)  # the Jacobi diagonal, as the engine builds it at admission
         bt = torch.as_tensor(b, device=dev)
         x = torch.zeros(n, dtype=torch.float64, device=dev)
         res = cg.solve(bt, x)
