@@ -276,6 +276,31 @@ class InternalForce:
     def mass_times_ground(self, direction: int, y, stream=None):
         check(lib().fx_mass_times_ground(self._h, direction, _ptr(y), _stream(stream)))
 
+    def commit_state(self, stream=None):
+        """InternalForce::commit_state (internal_force.cpp:507-509): the trial J2 state becomes
+        the committed one."""
+        check(lib().fx_force_commit(self._h, _stream(stream)))
+
+    def plastic_points(self) -> int:
+        n = C.c_int64()
+        check(lib().fx_force_plastic_points(self._h, C.byref(n)))
+        return n.value
+
+    J2_STATE = {"committed": (0, 13), "trial": (1, 13), "tangent": (2, 8)}
+
+    def j2_state(self, which: str = "committed") -> np.ndarray:
+        """The J2 state of the Gauss points, component c of point gp of element e at
+        [(c * 8 + gp) * padded + e]."""
+        w, comps = self.J2_STATE[which]
+        out = np.empty(comps * 8 * self.mesh.padded)
+        check(lib().fx_force_state(self._h, w, out.ctypes.data_as(L.p_f64), out.size))
+        return out
+
+    def set_j2_state(self, values: np.ndarray, which: str = "committed"):
+        w, _ = self.J2_STATE[which]
+        values = np.ascontiguousarray(values, np.float64)
+        check(lib().fx_force_set_state(self._h, w, values.ctypes.data_as(L.p_f64), values.size))
+
     def min_critical_dt(self, scheme: str = "ExplicitDifference") -> float:
         dt = C.c_double()
         check(lib().fx_min_critical_dt(self._h, 1 if scheme == "ExplicitDifference" else 0, C.byref(dt)))

@@ -125,6 +125,8 @@ PROTOTYPES = {
     "fx_newmark_predict": (C.c_int, [C.c_int64, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, vp]),
     "fx_newmark_update": (C.c_int, [C.c_int64, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+    "fx_force_state": (C.c_int, [vp, C.c_int32, p_f64, C.c_int64]),
+    "fx_force_set_state": (C.c_int, [vp, C.c_int32, p_f64, C.c_int64]),
     "fx_engine_create": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, fx_coeffs, fx_solve_opts, C.c_double,
                                    C.POINTER(vp)]),
     "fx_engine_destroy": (None, [vp]),

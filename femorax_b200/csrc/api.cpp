@@ -41,6 +41,7 @@ int64_t ForceState::device_bytes() const {
               glist.bytes() + slots.bytes() + nodal_mass.bytes() + nodal_alpha_mass.bytes() + lumped_mass.bytes() +
               eq_dof.bytes() + wx.bytes() + wy.bytes() + scratch.bytes();
   b += box.node_eq.bytes() + box.elem_param.bytes() + box.coef.bytes() + box.coef32.bytes();
+  b += j2_committed.bytes() + j2_trial.bytes() + j2_tan.bytes() + plastic_dev.bytes();
   return b;
 }
 
@@ -279,6 +280,25 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
       s.gstart.upload(start);
       s.glist.upload(list);
       s.slots.alloc(24 * P);
+      // J2 sets: state and tangent per Gauss point (virgin state, elastic tangent)
+      for (const auto& q : s.params_h)
+        if (q.kind == FX_MAT_J2) {
+          s.has_j2 = true;
+          if (q.betaK != 0.0 || q.betaKinit != 0.0 || q.betaKcomm != 0.0)
+            throw fx::Error(FX_E_UNSUPPORTED, "stiffness-proportional Rayleigh damping on a J2 set");
+          if (!(q.sigma_y > 0.0) || q.H < 0.0 || q.hk < 0.0 || q.hk > 1.0)
+            throw fx::Error(FX_E_INVALID, "J2 set: sigma_y > 0, H >= 0 and 0 <= hk <= 1 required");
+        }
+      if (s.has_j2) {
+        const size_t pts = static_cast<size_t>(8) * P;
+        s.j2_committed.upload(std::vector<double>(pts * fx::kJ2State, 0.0));
+        s.j2_trial.upload(std::vector<double>(pts * fx::kJ2State, 0.0));
+        std::vector<double> tan(pts * fx::kJ2Tan, 0.0);
+        std::fill(tan.begin(), tan.begin() + static_cast<std::ptrdiff_t>(pts), 1.0);  // theta = 1
+        s.j2_tan.upload(tan);
+        s.plastic_dev.alloc(1);
+        FX_CUDA(cudaMemset(s.plastic_dev.ptr, 0, sizeof(int)));
+      }
       auto nonzero = [&](const double* p) {
         if (!p) return false;
         for (int32_t q = 0; q < s.neq; ++q)
@@ -377,8 +397,9 @@ int fx_apply_operator(fx_force* f, fx_coeffs k, const double* x, double* y, void
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || (x && y)), "fx_apply_operator: bad arguments");
     FX_REQUIRE(x != y, "fx_apply_operator: x and y must not alias");
-    const double kk[3] = {k.initial ? k.stiffness : k.stiffness, k.damping, k.mass};
+    const double kk[3] = {k.stiffness, k.damping, k.mass};
     auto st = static_cast<cudaStream_t>(stream);
+    f->s.initial = k.initial != 0;
     if (f->s.use_box()) fx::box_apply(f->s, kk, x, y, st);
     else fx::general_apply(f->s, kk, x, y, st);
   });
@@ -402,6 +423,7 @@ int fx_apply_operator_host(fx_force* f, fx_coeffs k, const double* xh, double* y
     const size_t bytes = sizeof(double) * static_cast<size_t>(f->s.neq);
     FX_CUDA(cudaMemcpyAsync(f->s.wx.ptr, xh, bytes, cudaMemcpyHostToDevice, st));
     const double kk[3] = {k.stiffness, k.damping, k.mass};
+    f->s.initial = k.initial != 0;
     if (f->s.use_box()) fx::box_apply(f->s, kk, f->s.wx.ptr, f->s.wy.ptr, st);
     else fx::general_apply(f->s, kk, f->s.wx.ptr, f->s.wy.ptr, st);
     FX_CUDA(cudaMemcpyAsync(yh, f->s.wy.ptr, bytes, cudaMemcpyDeviceToHost, st));
@@ -413,6 +435,7 @@ int fx_operator_diagonal(fx_force* f, fx_coeffs k, double* d, void* stream) {
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || d), "fx_operator_diagonal: bad arguments");
     const double kk[3] = {k.stiffness, k.damping, k.mass};
+    f->s.initial = k.initial != 0;
     fx::general_diagonal(f->s, kk, d, static_cast<cudaStream_t>(stream));
   });
 }
@@ -442,14 +465,57 @@ int fx_mass_times_ground(fx_force* f, int32_t dir, double* y, void* stream) {
   });
 }
 
-int fx_force_commit(fx_force* f, void*) {
-  return guarded([&] { FX_REQUIRE(f, "fx_force_commit: null handle"); });
+int fx_force_commit(fx_force* f, void* stream) {
+  return guarded([&] {
+    FX_REQUIRE(f, "fx_force_commit: null handle");
+    fx::ForceState& s = f->s;
+    if (s.has_j2)
+      FX_CUDA(cudaMemcpyAsync(s.j2_committed.ptr, s.j2_trial.ptr, s.j2_committed.bytes(), cudaMemcpyDeviceToDevice,
+                              static_cast<cudaStream_t>(stream)));
+  });
+}
+
+static fx::DeviceArray<double>& j2_array(fx::ForceState& s, int32_t which, int& comps) {
+  if (!s.has_j2) throw fx::Error(FX_E_UNSUPPORTED, "the mesh has no J2 parameter set");
+  if (which == 0 || which == 1) {
+    comps = fx::kJ2State;
+    return which == 0 ? s.j2_committed : s.j2_trial;
+  }
+  if (which == 2) {
+    comps = fx::kJ2Tan;
+    return s.j2_tan;
+  }
+  throw fx::Error(FX_E_INVALID, "J2 state: which must be 0 (committed), 1 (trial) or 2 (tangent)");
+}
+
+int fx_force_state(fx_force* f, int32_t which, double* host, int64_t count) {
+  return guarded([&] {
+    FX_REQUIRE(f && host, "fx_force_state: bad arguments");
+    int comps = 0;
+    fx::DeviceArray<double>& a = j2_array(f->s, which, comps);
+    FX_REQUIRE(count >= static_cast<int64_t>(a.n), "fx_force_state: host buffer too small");
+    FX_CUDA(cudaMemcpy(host, a.ptr, a.bytes(), cudaMemcpyDeviceToHost));
+  });
+}
+
+int fx_force_set_state(fx_force* f, int32_t which, const double* host, int64_t count) {
+  return guarded([&] {
+    FX_REQUIRE(f && host, "fx_force_set_state: bad arguments");
+    FX_REQUIRE(which == 0 || which == 1, "fx_force_set_state: which must be 0 (committed) or 1 (trial)");
+    int comps = 0;
+    fx::DeviceArray<double>& a = j2_array(f->s, which, comps);
+    FX_REQUIRE(count == static_cast<int64_t>(a.n), "fx_force_set_state: count must be 13 * 8 * padded");
+    FX_CUDA(cudaMemcpy(a.ptr, host, a.bytes(), cudaMemcpyHostToDevice));
+  });
 }
 
 int fx_force_plastic_points(fx_force* f, int64_t* count) {
   return guarded([&] {
     FX_REQUIRE(f && count, "fx_force_plastic_points: bad arguments");
-    *count = f->s.plastic_points;
+    int n = 0;
+    if (f->s.has_j2) FX_CUDA(cudaMemcpy(&n, f->s.plastic_dev.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    f->s.plastic_points = n;
+    *count = n;
   });
 }
 

@@ -194,6 +194,79 @@ FX_HD void elastic_stress(const ParamGP& p, const double e[6], double sg[6]) {
   sg[5] = mu * e[5];
 }
 
+// ---------------------------------------------------------------- J2 plasticity
+// No counterpart in the reference (which has no J2 material): the von Mises radial return with
+// linear hardening H split into isotropic (1 - hk) H and kinematic hk H parts (Simo and Hughes,
+// Computational Inelasticity, 1998, box 3.2), on engineering strains in the OpenSees order
+// (11 22 33 12 23 31). State per Gauss point (kJ2State values): plastic strain (engineering
+// shear) [6], equivalent plastic strain, back stress [6]. Consistent tangent per point, compact
+// (kJ2Tan values): theta, thetab, n[6], with
+//   D_t = K 1 (x) 1 + 2 G theta I_dev - 2 G thetab n (x) n
+// (theta = 1, thetab = 0, n = 0 at an elastic point gives the elastic matrix exactly).
+constexpr int kJ2State = 13;
+constexpr int kJ2Tan = 8;
+
+FX_HD void j2_moduli(const ParamGP& p, double& K, double& G) {
+  K = p.E / (3.0 * (1.0 - 2.0 * p.nu));
+  G = p.E / (2.0 * (1.0 + p.nu));
+}
+
+// Trial state and stress at total strain eps from the committed state; returns true if plastic.
+FX_HD bool j2_update(const ParamGP& p, const double* committed, double* trial, const double eps[6], double sigma[6],
+                     double tan[kJ2Tan]) {
+  double K, G;
+  j2_moduli(p, K, G);
+  const double Hkin = p.hk * p.H, Hiso = (1.0 - p.hk) * p.H;
+  double ee[6];
+  for (int i = 0; i < 6; ++i) ee[i] = (i < 3 ? 1.0 : 0.5) * (eps[i] - committed[i]);
+  const double alpha = committed[6];
+  const double* back = committed + 7;
+  const double tr = ee[0] + ee[1] + ee[2];
+  double s_tr[6], xi[6];
+  for (int i = 0; i < 6; ++i) s_tr[i] = 2.0 * G * (i < 3 ? ee[i] - tr / 3.0 : ee[i]);
+  for (int i = 0; i < 6; ++i) xi[i] = s_tr[i] - back[i];
+  const double nxi = sqrt(xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2] +
+                          2.0 * (xi[3] * xi[3] + xi[4] * xi[4] + xi[5] * xi[5]));
+  const double r23 = sqrt(2.0 / 3.0);
+  const double f = nxi - r23 * (p.sigma_y + Hiso * alpha);
+  for (int i = 0; i < kJ2State; ++i) trial[i] = committed[i];
+  const double pr = K * tr;
+  tan[0] = 1.0;
+  for (int i = 1; i < kJ2Tan; ++i) tan[i] = 0.0;
+  if (f <= 0.0 || nxi == 0.0) {
+    for (int i = 0; i < 6; ++i) sigma[i] = s_tr[i] + (i < 3 ? pr : 0.0);
+    return false;
+  }
+  const double dg = f / (2.0 * G + (2.0 / 3.0) * p.H);
+  double n[6];
+  for (int i = 0; i < 6; ++i) n[i] = xi[i] / nxi;
+  for (int i = 0; i < 6; ++i) sigma[i] = s_tr[i] - 2.0 * G * dg * n[i] + (i < 3 ? pr : 0.0);
+  for (int i = 0; i < 6; ++i) trial[i] = committed[i] + (i < 3 ? 1.0 : 2.0) * dg * n[i];
+  trial[6] = alpha + r23 * dg;
+  for (int i = 0; i < 6; ++i) trial[7 + i] = back[i] + (2.0 / 3.0) * Hkin * dg * n[i];
+  const double theta = 1.0 - 2.0 * G * dg / nxi;
+  tan[0] = theta;
+  tan[1] = 1.0 / (1.0 + p.H / (3.0 * G)) - (1.0 - theta);
+  for (int i = 0; i < 6; ++i) tan[2 + i] = n[i];
+  return true;
+}
+
+// The 6 x 6 consistent tangent of a point from its compact form.
+FX_HD void j2_D(const ParamGP& p, const double tan[kJ2Tan], double D[6][6]) {
+  double K, G;
+  j2_moduli(p, K, G);
+  const double theta = tan[0], thetab = tan[1];
+  const double* n = tan + 2;
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double idev;
+      if (i < 3 && j < 3) idev = (i == j ? 1.0 : 0.0) - 1.0 / 3.0;
+      else idev = (i == j) ? 0.5 : 0.0;
+      const double vol = (i < 3 && j < 3) ? K : 0.0;
+      D[i][j] = vol + 2.0 * G * theta * idev - 2.0 * G * thetab * n[i] * n[j];
+    }
+}
+
 // Operator factors (element_operator.hpp:45-56; stdBrick's initial stiffness is not its
 // tangent): k = {stiffness, damping, mass}.
 struct OpFactors {
@@ -221,14 +294,43 @@ FX_HD void effective_D(const OpFactors& f, const ParamGP& p, double De[6][6]) {
     }
 }
 
-// y_e = K_eff,e x_e point by point.
-FX_HD void element_apply(const ParamGP& p, const OpFactors& f, const double xl[3][8], const double* xe, double* ye) {
-  for (int a = 0; a < 24; ++a) ye[a] = 0.0;
+// Sources of the effective material matrix at a point: the constant elastic one, or a J2
+// element's consistent tangent per point (component c of point gp at tan[(c * 8 + gp) * stride]),
+// scaled by the stiffness factor (J2 sets carry no stiffness-proportional damping); `initial`
+// takes the elastic matrix (ModifiedNewton -initial).
+struct ConstD {
   double De[6][6];
-  effective_D(f, p, De);
+  FX_HD void operator()(int, double D[6][6]) const {
+    for (int a = 0; a < 6; ++a)
+      for (int c = 0; c < 6; ++c) D[a][c] = De[a][c];
+  }
+};
+struct J2PointD {
+  const ParamGP* p;
+  const double* tan;
+  int64_t stride;
+  double cK;
+  bool initial;
+  FX_HD void operator()(int gp, double De[6][6]) const {
+    double t[kJ2Tan];
+    for (int c = 0; c < kJ2Tan; ++c) t[c] = initial ? (c == 0 ? 1.0 : 0.0) : tan[(c * 8 + gp) * stride];
+    double D[6][6];
+    j2_D(*p, t, D);
+    for (int a = 0; a < 6; ++a)
+      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[a][c];
+  }
+};
+
+// y_e = K_eff,e x_e point by point, the material matrix of point gp from dsrc.
+template <class DSrc>
+FX_HD void element_apply_d(const ParamGP& p, const OpFactors& f, const double xl[3][8], const double* xe, double* ye,
+                           const DSrc& dsrc) {
+  for (int a = 0; a < 24; ++a) ye[a] = 0.0;
   for (int gp = 0; gp < 8; ++gp) {
     PointShape s;
     point_shape(xl, gp, s);
+    double De[6][6];
+    dsrc(gp, De);
     double e[6], sg[6];
     strain_of(s, xe, e);
     for (int a = 0; a < 6; ++a) {
@@ -257,6 +359,12 @@ FX_HD void element_apply(const ParamGP& p, const OpFactors& f, const double xl[3
       }
     }
   }
+}
+
+FX_HD void element_apply(const ParamGP& p, const OpFactors& f, const double xl[3][8], const double* xe, double* ye) {
+  ConstD c;
+  effective_D(f, p, c.De);
+  element_apply_d(p, f, xl, xe, ye, c);
 }
 
 // 3x3 block (J, K) of B^T D B dvol at one point, in the reference's two-stage form.
@@ -303,8 +411,11 @@ FX_HD double mass_entry(const ParamGP& p, const PointShape& s, int j, int k) {
 }
 
 // Diagonal of K_eff,e by local DOF, with the terms of local DOFs merged into one equation
-// (element_operator.hpp:138-209). eq: the element's 24 equations.
-FX_HD void element_diagonal(const ParamGP& p, const OpFactors& f, const double xl[3][8], const int* eq, double* de) {
+// (element_operator.hpp:138-209). eq: the element's 24 equations; the material matrix of point gp
+// from dsrc.
+template <class DSrc>
+FX_HD void element_diagonal_d(const ParamGP& p, const OpFactors& f, const double xl[3][8], const int* eq, double* de,
+                              const DSrc& dsrc) {
   for (int a = 0; a < 24; ++a) de[a] = 0.0;
   int first[24];
   bool merged = false;
@@ -318,11 +429,11 @@ FX_HD void element_diagonal(const ParamGP& p, const OpFactors& f, const double x
         break;
       }
   }
-  double De[6][6];
-  effective_D(f, p, De);
   for (int gp = 0; gp < 8; ++gp) {
     PointShape s;
     point_shape(xl, gp, s);
+    double De[6][6];
+    dsrc(gp, De);
     for (int j = 0; j < 8; ++j) {
       double blk[3][3];
       block_tangent(s, De, j, j, blk);
@@ -350,6 +461,12 @@ FX_HD void element_diagonal(const ParamGP& p, const OpFactors& f, const double x
           }
       }
   }
+}
+
+FX_HD void element_diagonal(const ParamGP& p, const OpFactors& f, const double xl[3][8], const int* eq, double* de) {
+  ConstD c;
+  effective_D(f, p, c.De);
+  element_diagonal_d(p, f, xl, eq, de, c);
 }
 
 // Internal force with body force plus the four Rayleigh damping forces (elastic material).
@@ -405,6 +522,52 @@ FX_HD void element_force(const ParamGP& p, const double xl[3][8], const double* 
     }
   }
   for (int a = 0; a < 24; ++a) fe[a] = resid[a] + fdamp[a];
+}
+
+// Internal force of a J2 element at displacement ue: the stress of every point by the return map
+// from its committed state (component c of point gp at committed[(c * 8 + gp) * stride]), which
+// also writes the point's trial state and compact tangent (same layout); minus the body force;
+// plus the mass-proportional Rayleigh force at ve (J2 sets carry no stiffness-proportional
+// damping). The sums run in element_force's order. Returns the number of plastic points.
+FX_HD int element_force_j2(const ParamGP& p, const double xl[3][8], const double* ue, const double* ve,
+                           const double* committed, double* trial, double* tan, int64_t stride, double* fe) {
+  double resid[24], fdamp[24];
+  for (int a = 0; a < 24; ++a) resid[a] = fdamp[a] = 0.0;
+  int plastic = 0;
+  for (int gp = 0; gp < 8; gp++) {
+    PointShape s;
+    point_shape(xl, gp, s);
+    double e[6], sg[6], vg[3], cst[kJ2State], tst[kJ2State], tn[kJ2Tan];
+    strain_of(s, ue, e);
+    for (int c = 0; c < kJ2State; ++c) cst[c] = committed[(c * 8 + gp) * stride];
+    plastic += j2_update(p, cst, tst, e, sg, tn) ? 1 : 0;
+    for (int c = 0; c < kJ2State; ++c) trial[(c * 8 + gp) * stride] = tst[c];
+    for (int c = 0; c < kJ2Tan; ++c) tan[(c * 8 + gp) * stride] = tn[c];
+    vg[0] = vg[1] = vg[2] = 0.0;
+    if (p.alphaM != 0.0 && p.mass_type == 0)
+      for (int j = 0; j < 8; j++)
+        for (int q = 0; q < 3; q++) vg[q] += s.N[j] * ve[3 * j + q];
+    for (int j = 0; j < 8; j++) {
+      double r[3], body[3], dj[3];
+      node_force(s, sg, j, r);
+      for (int q = 0; q < 3; q++) body[q] = s.dvol * p.b[q] * s.N[j];
+      dj[0] = dj[1] = dj[2] = 0.0;
+      if (p.alphaM != 0.0) {
+        const double t = s.N[j] * s.dvol * p.rho;
+        for (int q = 0; q < 3; q++) {
+          const double vq = p.mass_type == 0 ? vg[q] : ve[3 * j + q];
+          dj[q] += p.alphaM * t * vq;
+        }
+      }
+      for (int q = 0; q < 3; q++) {
+        resid[3 * j + q] += r[q];
+        resid[3 * j + q] -= body[q];
+        fdamp[3 * j + q] += dj[q];
+      }
+    }
+  }
+  for (int a = 0; a < 24; ++a) fe[a] = resid[a] + fdamp[a];
+  return plastic;
 }
 
 // Row-sum lumped mass per corner.

@@ -109,6 +109,13 @@ struct ForceState {
   DeviceArray<double> wx, wy;
   DeviceArray<double> scratch;  // reduction partials and solver scalars
   int64_t plastic_points = 0;
+  // J2 sets (general path): per element and Gauss point, component c of point gp of element e at
+  // [(c * 8 + gp) * P + e]: committed state, trial state of the last force evaluation, and that
+  // evaluation's compact consistent tangent (elastic until the first force evaluation)
+  bool has_j2 = false;
+  bool initial = false;  // the operator's stiffness term takes the initial (elastic) matrix
+  DeviceArray<double> j2_committed, j2_trial, j2_tan;
+  DeviceArray<int> plastic_dev;  // plastic points of the last force evaluation
   ExplicitWork xw;
   bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
   bool use_box_force() const { return use_box() && box.force_ok; }

@@ -1,4 +1,5 @@
-// General execution path: any stdBrick mesh. One thread per element evaluates the element with
+// General execution path: any stdBrick mesh (and the only path for J2 sets, whose material
+// matrix differs from point to point). One thread per element evaluates the element with
 // the Gauss-point physics of brick_gp.cuh and writes its 24 values to its own slots
 // (slots[k * padded + e], coalesced across the warp); a second kernel gives every equation the
 // sum of its slots in (element, DOF) order and adds the nodal-mass terms.
@@ -26,7 +27,8 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
                                                            const ParamGP* __restrict__ params, int32_t N, int32_t P,
                                                            int32_t count, double ks, double kd, double km, int unit_dir,
                                                            const double* __restrict__ x, double* __restrict__ slots,
-                                                           const int* skip) {
+                                                           const int* skip, const double* __restrict__ j2tan,
+                                                           int initial) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count || (skip && *skip)) return;
   const ParamGP p = params[param[e]];
@@ -38,7 +40,8 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
     else xe[a] = q >= 0 ? x[q] : 0.0;
   }
   const OpFactors f = op_factors(p, ks, kd, km);
-  element_apply(p, f, xl, xe, ye);
+  if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
+  else element_apply(p, f, xl, xe, ye);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
 }
 
@@ -46,7 +49,8 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
                                                           const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
                                                           const ParamGP* __restrict__ params, int32_t N, int32_t P,
                                                           int32_t count, double ks, double kd, double km,
-                                                          double* __restrict__ slots) {
+                                                          double* __restrict__ slots, const double* __restrict__ j2tan,
+                                                          int initial) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -55,7 +59,8 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
   load_coords(coords, node, N, P, e, xl);
   for (int a = 0; a < 24; ++a) eqe[a] = eq[static_cast<int64_t>(a) * P + e];
   const OpFactors f = op_factors(p, ks, kd, km);
-  element_diagonal(p, f, xl, eqe, de);
+  if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
+  else element_diagonal(p, f, xl, eqe, de);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = de[a];
 }
 
@@ -63,7 +68,9 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
                                                            const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
                                                            const ParamGP* __restrict__ params, int32_t N, int32_t P,
                                                            int32_t count, const double* __restrict__ u,
-                                                           const double* __restrict__ v, double* __restrict__ slots) {
+                                                           const double* __restrict__ v, double* __restrict__ slots,
+                                                           const double* __restrict__ j2c, double* __restrict__ j2t,
+                                                           double* __restrict__ j2tan, int* __restrict__ plastic) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -74,7 +81,12 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
     ue[a] = q >= 0 ? u[q] : 0.0;
     ve[a] = q >= 0 ? v[q] : 0.0;
   }
-  element_force(p, xl, ue, ve, fe);
+  if (p.kind == 1) {
+    const int np = element_force_j2(p, xl, ue, ve, j2c + e, j2t + e, j2tan + e, P, fe);
+    if (np) atomicAdd(plastic, np);
+  } else {
+    element_force(p, xl, ue, ve, fe);
+  }
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = fe[a];
 }
 
@@ -100,7 +112,7 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
   if (s.count > 0)
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
-                                                                   -1, x, s.slots.ptr, skip);
+                                                                   -1, x, s.slots.ptr, skip, s.j2_tan.ptr, s.initial);
   FX_LAUNCH_CHECK("element_apply");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -114,7 +126,7 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
   if (s.count > 0)
     k_element_diag<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                   s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
-                                                                  s.slots.ptr);
+                                                                  s.slots.ptr, s.j2_tan.ptr, s.initial);
   FX_LAUNCH_CHECK("element_diagonal");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -125,9 +137,12 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
 }
 
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
+  if (s.has_j2) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
   if (s.count > 0)
     k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
-                                                                   s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr);
+                                                                   s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr,
+                                                                   s.j2_committed.ptr, s.j2_trial.ptr, s.j2_tan.ptr,
+                                                                   s.plastic_dev.ptr);
   FX_LAUNCH_CHECK("element_force");
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
@@ -149,7 +164,7 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
   if (s.count > 0)
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, 0.0, 0.0, 1.0, dir,
-                                                                   nullptr, s.slots.ptr, nullptr);
+                                                                   nullptr, s.slots.ptr, nullptr, s.j2_tan.ptr, 0);
   FX_LAUNCH_CHECK("element_apply_unit");
   if (s.neq > 0)
     k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,

@@ -575,6 +575,7 @@ int fx_solver_setup(fx_solver* h, fx_coeffs k, void* stream) {
     s.k[0] = k.stiffness;
     s.k[1] = k.damping;
     s.k[2] = k.mass;
+    s.f->s.initial = k.initial != 0;
     if (s.n > 0) {
       fx::general_diagonal(s.f->s, s.k, s.diag.ptr, st);
       FX_CUDA(cudaMemsetAsync(s.zero_count.ptr, 0, sizeof(int), st));

@@ -188,6 +188,15 @@ int fx_min_critical_dt(fx_force* f, int32_t scheme, double* dt);
 int fx_force_commit(fx_force* f, void* stream);
 /* Number of Gauss points that were plastic at the last force evaluation (J2). */
 int fx_force_plastic_points(fx_force* f, int64_t* count);
+/* The J2 material state of the Gauss points (the state InternalForce keeps per point and swaps
+ * in commit_state, internal_force.cpp:507-509; for checkpoints and tests). which = 0 committed
+ * and 1 trial state (13 components per point: plastic strain with engineering shear [6],
+ * equivalent plastic strain, back stress [6]), 2 the compact consistent tangent of the last force
+ * evaluation (8: theta, thetab, n[6]); component c of point gp of element e at
+ * [(c * 8 + gp) * padded + e]. `count` is the host buffer's length in doubles (get: at least the
+ * array's; set: exactly it; set takes which 0 or 1). FX_E_UNSUPPORTED without J2 sets. */
+int fx_force_state(fx_force* f, int32_t which, double* host, int64_t count);
+int fx_force_set_state(fx_force* f, int32_t which, const double* host, int64_t count);
 
 /* ------------------------------------------------------------------ vector kernels
  * solvers::VectorOps (src/solvers/vector_ops.hpp:17-57): deterministic reductions in the

@@ -276,6 +276,9 @@ def port():
         L.fxo_apply_operator.argtypes = [M, p_f64, p_f64, p_f64]
         L.fxo_operator_diagonal.argtypes = [M, p_f64, p_f64]
         L.fxo_force.argtypes = [M, p_f64, p_f64, p_f64]
+        L.fxo_force_j2.argtypes = [M, p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, C.POINTER(C.c_int)]
+        L.fxo_apply_j2.argtypes = [M, p_f64, p_f64, p_f64, C.c_int, p_f64, p_f64]
+        L.fxo_diagonal_j2.argtypes = [M, p_f64, p_f64, p_f64, C.c_int, p_f64]
         L.fxo_mass_times_ground.argtypes = [M, C.c_int, p_f64]
         L.fxo_dot.restype = C.c_double
         L.fxo_dot.argtypes = [p_f64, p_f64, C.c_int64, C.c_int, C.c_int]
@@ -328,6 +331,44 @@ class PortMesh:
                 setattr(s, name, p)
         self.s = s
         self.n = m.num_equations
+        # J2 table: kind, sigma_y, H, hk per parameter set; per-point arrays [(c * 8 + gp) * padded + e]
+        self.j2 = np.ascontiguousarray(np.array([[r[0], r[12], r[13], r[14]] for r in m.params],
+                                                np.float64).reshape(-1))
+        self.points = 8 * m.padded
+
+    def j2_state(self):
+        """A virgin J2 state (13 components per point)."""
+        return np.zeros(13 * self.points)
+
+    def force_j2(self, committed, u, v):
+        """(f, trial state, point tangents (36 per point), plastic points) at u, v."""
+        committed, pc = _f(committed)
+        u, pu = _f(u)
+        v, pv = _f(v)
+        trial = np.zeros(13 * self.points)
+        D = np.zeros(36 * self.points)
+        f = np.zeros(self.n)
+        npl = C.c_int()
+        port().fxo_force_j2(C.byref(self.s), self.j2.ctypes.data_as(p_f64), pc, trial.ctypes.data_as(p_f64),
+                            D.ctypes.data_as(p_f64), pu, pv, f.ctypes.data_as(p_f64), C.byref(npl))
+        return f, trial, D, npl.value
+
+    def apply_j2(self, D, k, x, initial=False):
+        D, pD = _f(D)
+        k, pk = _f(np.array(k, np.float64))
+        x, px = _f(x)
+        y = np.zeros(self.n)
+        port().fxo_apply_j2(C.byref(self.s), self.j2.ctypes.data_as(p_f64), pD, pk, int(initial), px,
+                            y.ctypes.data_as(p_f64))
+        return y
+
+    def diagonal_j2(self, D, k, initial=False):
+        D, pD = _f(D)
+        k, pk = _f(np.array(k, np.float64))
+        d = np.zeros(self.n)
+        port().fxo_diagonal_j2(C.byref(self.s), self.j2.ctypes.data_as(p_f64), pD, pk, int(initial),
+                               d.ctypes.data_as(p_f64))
+        return d
 
     def apply_operator(self, k, x):
         k, pk = _f(np.array(k, np.float64))

@@ -332,13 +332,13 @@ static void effective_tangent(const factors* f, const fxo_param* p, double Deff[
 
 /* element_operator_apply, element_operator.hpp:82-130, with point_mass_apply
  * (std_brick.hpp:361-374). */
-void fxo_brick_operator(const fxo_param* p, const double* k, const double* xe, const double* ve, double* ye) {
-  const factors f = make_factors(p, k);
+/* Dp[gp]: the effective material matrix of point gp. */
+static void brick_operator_pts(const fxo_param* p, const factors* fp, const double* xe, const double* ve,
+                               double Dp[NGP][NS][NS], double* ye) {
+  const factors f = *fp;
   double xl[3][8];
   local_coords(xe, xl);
   for (int a = 0; a < NDOF; ++a) ye[a] = 0.0;
-  double Deff[NS][NS];
-  effective_tangent(&f, p, Deff);
   for (int gp = 0; gp < NGP; ++gp) {
     point_shape s;
     point_geometry(xl, gp, &s);
@@ -346,7 +346,7 @@ void fxo_brick_operator(const fxo_param* p, const double* k, const double* xe, c
     point_strain(&s, ve, eps);
     for (int a = 0; a < NS; ++a) {
       double sum = 0.0;
-      for (int c = 0; c < NS; ++c) sum += Deff[a][c] * eps[c];
+      for (int c = 0; c < NS; ++c) sum += Dp[gp][a][c] * eps[c];
       sig[a] = sum;
     }
     for (int j = 0; j < NNODE; ++j) {
@@ -372,6 +372,14 @@ void fxo_brick_operator(const fxo_param* p, const double* k, const double* xe, c
   }
 }
 
+void fxo_brick_operator(const fxo_param* p, const double* k, const double* xe, const double* ve, double* ye) {
+  const factors f = make_factors(p, k);
+  double Dp[NGP][NS][NS];
+  effective_tangent(&f, p, Dp[0]);
+  for (int gp = 1; gp < NGP; ++gp) memcpy(Dp[gp], Dp[0], sizeof(Dp[0]));
+  brick_operator_pts(p, &f, xe, ve, Dp, ye);
+}
+
 /* point_mass_entry, std_brick.hpp:379-383. */
 static double mass_entry(const fxo_param* p, const point_shape* s, int j, int k) {
   const double temp = s->shp[3][j] * s->dvol * p->rho;
@@ -380,8 +388,9 @@ static double mass_entry(const fxo_param* p, const point_shape* s, int j, int k)
 }
 
 /* element_operator_diagonal, element_operator.hpp:138-209 (with the merged-equation terms). */
-void fxo_brick_diagonal(const fxo_param* p, const double* k, const double* xe, const int32_t* eq, double* de) {
-  const factors f = make_factors(p, k);
+static void brick_diagonal_pts(const fxo_param* p, const factors* fp, const double* xe, const int32_t* eq,
+                               double Dp[NGP][NS][NS], double* de) {
+  const factors f = *fp;
   double xl[3][8];
   local_coords(xe, xl);
   for (int a = 0; a < NDOF; ++a) de[a] = 0.0;
@@ -397,11 +406,10 @@ void fxo_brick_diagonal(const fxo_param* p, const double* k, const double* xe, c
         break;
       }
   }
-  double Deff[NS][NS];
-  effective_tangent(&f, p, Deff);
   for (int gp = 0; gp < NGP; ++gp) {
     point_shape s;
     point_geometry(xl, gp, &s);
+    double (*Deff)[NS] = Dp[gp];
     for (int j = 0; j < NNODE; ++j) {
       double blk[3][3];
       block_tangent(&s, Deff, j, j, blk);
@@ -429,6 +437,14 @@ void fxo_brick_diagonal(const fxo_param* p, const double* k, const double* xe, c
           }
       }
   }
+}
+
+void fxo_brick_diagonal(const fxo_param* p, const double* k, const double* xe, const int32_t* eq, double* de) {
+  const factors f = make_factors(p, k);
+  double Dp[NGP][NS][NS];
+  effective_tangent(&f, p, Dp[0]);
+  for (int gp = 1; gp < NGP; ++gp) memcpy(Dp[gp], Dp[0], sizeof(Dp[0]));
+  brick_diagonal_pts(p, &f, xe, eq, Dp, de);
 }
 
 /* StdBrick::mass and lumped_mass, std_brick.hpp:582-623 (row-major 24x24). */
@@ -900,4 +916,157 @@ int fxo_j2_update(double E, double nu, double sigma_y, double H, double hk, cons
       D[i * 6 + j] = vol + 2.0 * G * theta * idev - 2.0 * G * thetab * n[i] * n[j];
     }
   return 1;
+}
+
+/* ---------------------------------------------------------------- J2 system level
+ * No counterpart in the reference. j2[4 * s] = {kind (0 elastic, 1 J2), sigma_y, H, hk} of
+ * parameter set s. Per element and Gauss point, component c of point gp of element e is at
+ * [(c * 8 + gp) * padded + e]: the committed and trial states (13 components) and the point's
+ * consistent tangent of the last force evaluation (36 components, row-major). Elastic sets use the
+ * elastic element routines above. */
+static int is_j2(const double* j2, int32_t s) { return j2[4 * s] == 1.0; }
+
+/* The J2 element force: fxo_brick_compute's sums with the return-mapped stress (no stiffness-
+ * proportional damping on J2 sets). */
+static int brick_force_j2(const fxo_param* p, const double* j2p, const double* xe, const double* ue,
+                          const double* ve, const double* committed, double* trial, double* Dpts, int64_t stride,
+                          double* fe) {
+  double xl[3][8];
+  local_coords(xe, xl);
+  double resid[NDOF], fdamp[NDOF];
+  for (int a = 0; a < NDOF; ++a) resid[a] = fdamp[a] = 0.0;
+  int plastic = 0;
+  for (int i = 0; i < NGP; i++) {
+    point_shape s;
+    point_geometry(xl, i, &s);
+    double strain[NS], stress[NS], D[NS * NS], cst[13], tst[13], v_gp[3];
+    point_strain(&s, ue, strain);
+    for (int c = 0; c < 13; ++c) cst[c] = committed[(c * 8 + i) * stride];
+    plastic += fxo_j2_update(p->E, p->nu, j2p[1], j2p[2], j2p[3], cst, tst, strain, stress, D);
+    for (int c = 0; c < 13; ++c) trial[(c * 8 + i) * stride] = tst[c];
+    for (int c = 0; c < 36; ++c) Dpts[(c * 8 + i) * stride] = D[c];
+    v_gp[0] = v_gp[1] = v_gp[2] = 0.0;
+    if (p->alphaM != 0.0 && p->mass_type == 0)
+      for (int j = 0; j < NNODE; j++)
+        for (int q = 0; q < 3; q++) v_gp[q] += s.shp[3][j] * ve[3 * j + q];
+    for (int j = 0; j < NNODE; j++) {
+      double residJ[3], body[3], dampJ[3];
+      point_node_force(&s, stress, j, residJ);
+      for (int q = 0; q < 3; q++) body[q] = s.dvol * p->b[q] * s.shp[3][j];
+      dampJ[0] = dampJ[1] = dampJ[2] = 0.0;
+      if (p->alphaM != 0.0) {
+        const double temp = s.shp[3][j] * s.dvol * p->rho;
+        for (int q = 0; q < 3; q++) {
+          const double vq = p->mass_type == 0 ? v_gp[q] : ve[3 * j + q];
+          dampJ[q] += p->alphaM * temp * vq;
+        }
+      }
+      for (int q = 0; q < 3; q++) {
+        resid[3 * j + q] += residJ[q];
+        resid[3 * j + q] -= body[q];
+        fdamp[3 * j + q] += dampJ[q];
+      }
+    }
+  }
+  for (int a = 0; a < NDOF; ++a) fe[a] = resid[a] + fdamp[a];
+  return plastic;
+}
+
+void fxo_force_j2(const fxo_mesh* m, const double* j2, const double* committed, double* trial, double* Dpts,
+                  const double* u, const double* v, double* f, int* plastic) {
+  int np = 0;
+  for (int32_t q = 0; q < m->num_equations; ++q) f[q] = 0.0;
+  for (int32_t e = 0; e < m->count; ++e) {
+    double xe[24], ue[24], ve[24], fe[24];
+    element_coords(m, e, xe);
+    for (int a = 0; a < NDOF; ++a) {
+      const int32_t q = m->eq[(int64_t)a * m->padded + e];
+      ue[a] = q >= 0 ? u[q] : 0.0;
+      ve[a] = q >= 0 ? v[q] : 0.0;
+    }
+    const int32_t ps = m->param[e];
+    if (is_j2(j2, ps))
+      np += brick_force_j2(&m->params[ps], j2 + 4 * ps, xe, ue, ve, committed + e, trial + e, Dpts + e, m->padded, fe);
+    else
+      fxo_brick_compute(&m->params[ps], xe, ue, ve, fe, NULL);
+    for (int a = 0; a < NDOF; ++a) {
+      const int32_t q = m->eq[(int64_t)a * m->padded + e];
+      if (q >= 0) f[q] += fe[a];
+    }
+  }
+  if (m->nodal_alpha_mass)
+    for (int32_t q = 0; q < m->num_equations; ++q) f[q] += m->nodal_alpha_mass[q] * v[q];
+  *plastic = np;
+}
+
+/* Effective matrices of a J2 element's points: cK D_t (or cK D_elastic with `initial`). */
+static void j2_point_matrices(const fxo_param* p, const double* j2p, const factors* f, const double* Dpts,
+                              int64_t stride, int initial, double Dp[NGP][NS][NS]) {
+  double De[NS * NS], sig[NS], cst[13] = {0}, tst[13];
+  const double zero[NS] = {0, 0, 0, 0, 0, 0};
+  if (initial) fxo_j2_update(p->E, p->nu, j2p[1], j2p[2], j2p[3], cst, tst, zero, sig, De);
+  for (int gp = 0; gp < NGP; ++gp)
+    for (int a = 0; a < NS; ++a)
+      for (int c = 0; c < NS; ++c) {
+        const double D = initial ? De[a * NS + c] : Dpts[((a * NS + c) * 8 + gp) * stride];
+        Dp[gp][a][c] = f->cK * D;
+      }
+}
+
+void fxo_apply_j2(const fxo_mesh* m, const double* j2, const double* Dpts, const double* k, int initial,
+                  const double* x, double* y) {
+  for (int32_t q = 0; q < m->num_equations; ++q) y[q] = 0.0;
+  for (int32_t e = 0; e < m->count; ++e) {
+    double xe[24], ve[24], ye[24];
+    element_coords(m, e, xe);
+    for (int a = 0; a < NDOF; ++a) {
+      const int32_t q = m->eq[(int64_t)a * m->padded + e];
+      ve[a] = q >= 0 ? x[q] : 0.0;
+    }
+    const int32_t ps = m->param[e];
+    const fxo_param* p = &m->params[ps];
+    if (is_j2(j2, ps)) {
+      const factors f = make_factors(p, k);
+      double Dp[NGP][NS][NS];
+      j2_point_matrices(p, j2 + 4 * ps, &f, Dpts + e, m->padded, initial, Dp);
+      brick_operator_pts(p, &f, xe, ve, Dp, ye);
+    } else {
+      fxo_brick_operator(p, k, xe, ve, ye);
+    }
+    for (int a = 0; a < NDOF; ++a) {
+      const int32_t q = m->eq[(int64_t)a * m->padded + e];
+      if (q >= 0) y[q] += ye[a];
+    }
+  }
+  if (k[2] != 0.0 && m->nodal_mass)
+    for (int32_t q = 0; q < m->num_equations; ++q) y[q] += k[2] * m->nodal_mass[q] * x[q];
+  if (k[1] != 0.0 && m->nodal_alpha_mass)
+    for (int32_t q = 0; q < m->num_equations; ++q) y[q] += k[1] * m->nodal_alpha_mass[q] * x[q];
+}
+
+void fxo_diagonal_j2(const fxo_mesh* m, const double* j2, const double* Dpts, const double* k, int initial,
+                     double* d) {
+  for (int32_t q = 0; q < m->num_equations; ++q) d[q] = 0.0;
+  for (int32_t e = 0; e < m->count; ++e) {
+    double xe[24], de[24];
+    int32_t eqe[24];
+    element_coords(m, e, xe);
+    for (int a = 0; a < NDOF; ++a) eqe[a] = m->eq[(int64_t)a * m->padded + e];
+    const int32_t ps = m->param[e];
+    const fxo_param* p = &m->params[ps];
+    if (is_j2(j2, ps)) {
+      const factors f = make_factors(p, k);
+      double Dp[NGP][NS][NS];
+      j2_point_matrices(p, j2 + 4 * ps, &f, Dpts + e, m->padded, initial, Dp);
+      brick_diagonal_pts(p, &f, xe, eqe, Dp, de);
+    } else {
+      fxo_brick_diagonal(p, k, xe, eqe, de);
+    }
+    for (int a = 0; a < NDOF; ++a)
+      if (eqe[a] >= 0) d[eqe[a]] += de[a];
+  }
+  if (k[2] != 0.0 && m->nodal_mass)
+    for (int32_t q = 0; q < m->num_equations; ++q) d[q] += k[2] * m->nodal_mass[q] * 1.0;
+  if (k[1] != 0.0 && m->nodal_alpha_mass)
+    for (int32_t q = 0; q < m->num_equations; ++q) d[q] += k[1] * m->nodal_alpha_mass[q] * 1.0;
 }

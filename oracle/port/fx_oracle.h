@@ -85,6 +85,19 @@ void fxo_newmark_update(int64_t n, const double* du, double* u, double* v, doubl
 int fxo_j2_update(double E, double nu, double sigma_y, double H, double hk, const double* committed,
                   double* trial, const double* eps, double* sigma, double* D);
 
+/* J2 system level (no counterpart in the reference): j2[4 * s] = {kind (0 elastic, 1 J2),
+ * sigma_y, H, hk} per parameter set; per element and Gauss point, component c of point gp of
+ * element e at [(c * 8 + gp) * padded + e]: state (13), consistent tangent (36, row-major).
+ * fxo_force_j2: internal force at u, v from the committed state; writes the trial state, the
+ * points' tangents and the number of plastic points. fxo_apply_j2 / fxo_diagonal_j2: the
+ * operator and its diagonal with those tangents (initial: the elastic matrix instead). */
+void fxo_force_j2(const fxo_mesh* m, const double* j2, const double* committed, double* trial, double* Dpts,
+                  const double* u, const double* v, double* f, int* plastic);
+void fxo_apply_j2(const fxo_mesh* m, const double* j2, const double* Dpts, const double* k, int initial,
+                  const double* x, double* y);
+void fxo_diagonal_j2(const fxo_mesh* m, const double* j2, const double* Dpts, const double* k, int initial,
+                     double* d);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,3 +54,24 @@ def two_region_block(nx=4, ny=3, nz=5, lumped=False):
     spec.mass_dof = np.tile(np.array([1, 2, 3], np.int32), len(top))
     spec.mass_value = np.linspace(0.5, 2.0, len(spec.mass_node))
     return spec
+
+
+def j2_column(nx=2, ny=3, nz=6, lumped=False, hk=0.5, h=0.5):
+    """A column with an elastic lower half and a J2 upper half (sigma_y 60 kPa, H = 0.05 E, kinematic
+    share hk), base fixed, mass-proportional Rayleigh damping on the J2 half."""
+    tags, coords = meshes.block_nodes(nx, ny, nz, h, h, h)
+    groups = []
+    for layer in range(2):
+        k0, k1 = (0, nz // 2) if layer == 0 else (nz // 2, nz)
+        et, cn = meshes.block_connectivity(nx, ny, nz, k0, k1)
+        if layer == 0:
+            groups.append(meshes.Group(80e6, 0.3, 2000.0, et, cn, b=(0.0, 0.0, -19.6e3), lumped=lumped))
+        else:
+            groups.append(meshes.Group(40e6, 0.33, 1900.0, et, cn, b=(0.0, 0.0, -18.6e3), lumped=lumped, kind=1,
+                                       sigma_y=60e3, H=0.05 * 40e6, hk=hk))
+    spec = meshes.ModelSpec(tags=tags, coords=coords, groups=groups)
+    spec.fix_node, spec.fix_dof = meshes.fix_base(nx, ny)
+    spec.rayleigh = [meshes.Rayleigh(0.4, 0.0, 0.0, 0.0, groups[1].etags)]
+    spec.grid = (nx, ny, nz, h, h, h)
+    return spec
+
