@@ -405,6 +405,18 @@ class LinearSolver:
         return SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual, r.final_residual,
                            bool(r.indefinite), r.refinements)
 
+    def newton(self, fext, u, tol: float = 1e-6, test: str = "NormUnbalance", max_newton: int = 25, stream=None):
+        """Newton iterations of one quasi-static load step (fx_solver_newton) with the stage's
+        absolute convergence test (NormUnbalance or NormDispIncr); u is updated in place; returns
+        (Newton iterations, SolveResult of the Newton test). CG solvers only."""
+        r = L.fx_solve_result()
+        it = C.c_int32()
+        t = L.FX_TEST_NORM_UNBALANCE if test == "NormUnbalance" else L.FX_TEST_NORM_DISP_INCR
+        check(lib().fx_solver_newton(self._h, _ptr(fext), _ptr(u), t, tol, max_newton, C.byref(it), C.byref(r),
+                                     _stream(stream)))
+        return it.value, SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual,
+                                     r.final_residual, bool(r.indefinite), r.refinements)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

@@ -199,6 +199,17 @@ __global__ void k_residual64(const double* __restrict__ b, const double* __restr
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     r[i] = b[i] - ax[i];
 }
+// y = b - y
+__global__ void k_sub_from(const double* __restrict__ b, double* __restrict__ y, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = b[i] - y[i];
+}
+__global__ void k_add64(const double* __restrict__ d, double* __restrict__ x, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] += d[i];
+}
 __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -242,6 +253,7 @@ struct Solver {
   DeviceArray<int> fl;
   DeviceArray<int> zero_count;
   DeviceArray<double> V, Z, wv, hbuf;  // GMRES
+  DeviceArray<double> nres, ndu;       // Newton: residual and increment
   int* host_flags = nullptr;           // pinned
   double* host_sc = nullptr;           // pinned
   ~Solver() {
@@ -330,6 +342,7 @@ struct Solver {
 
   void gmres(const double* b, double* x, fx_solve_result* res);
   void ir(const double* b, double* x, fx_solve_result* res);
+  int newton(const double* fext, double* u, int test, double tol, int max_newton, fx_solve_result* res);
 };
 
 // FGMRES(m) with CGS2, host-side Hessenberg and Givens rotations, as gmres.cpp:32-123.
@@ -478,6 +491,63 @@ void Solver::ir(const double* b, double* x, fx_solve_result* res) {
   res->refinements = outer;
 }
 
+// Newton iterations of one quasi-static load step (ImplicitStage's Newton loop without inertia,
+// src/exec/implicit_stage.cpp:118-437): r = f_ext - f_int(u) with the material update of every
+// point (which also stores the points' consistent tangents), the Jacobi diagonal of that
+// tangent, K_t du = r by CG from du = 0, u += du; the convergence test is the stage's
+// (implicit_stage.cpp:199, 241-242, 342): NormUnbalance ||r|| <= tol or NormDispIncr
+// ||du|| <= tol, absolute. After a NormDispIncr convergence the force is evaluated once more at
+// the final u, so that the trial material state is u's. The trial state is left for the caller
+// to commit. Returns the Newton iterations (solves); res: converged, CG iterations in all,
+// ||f_ext||, the first and last ||r||.
+int Solver::newton(const double* fext, double* u, int test, double tol, int max_newton, fx_solve_result* res) {
+  ForceState& fs = f->s;
+  FX_CUDA(cudaMemsetAsync(x0.ptr, 0, sizeof(double) * n, cs));  // velocity 0 (quasi-static)
+  auto norm = [&](const double* v) {
+    dot_device(w, v, v, n, sc.ptr + S_RR, cs);
+    FX_CUDA(cudaMemcpyAsync(host_sc, sc.ptr, sizeof(double) * S_NSCALAR, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+    return std::sqrt(host_sc[S_RR]);
+  };
+  auto residual = [&]() {  // nres = f_ext - f_int(u)
+    if (fs.use_box_force()) box_force(fs, u, x0.ptr, nres.ptr, cs);
+    else general_force(fs, u, x0.ptr, nres.ptr, cs);
+    k_sub_from<<<ew(n), 256, 0, cs>>>(fext, nres.ptr, n);
+    FX_LAUNCH_CHECK("newton_residual");
+    return norm(nres.ptr);
+  };
+  res->rhs_norm = norm(fext);
+  int it = 0;
+  double rn = residual();
+  res->initial_residual = rn;
+  for (;;) {
+    res->final_residual = rn;
+    if (test == FX_TEST_NORM_UNBALANCE && rn <= tol) {
+      res->converged = 1;
+      break;
+    }
+    if (it >= max_newton) break;
+    general_diagonal(fs, k, diag.ptr, cs);
+    k_reciprocal_t<double><<<ew(n), 256, 0, cs>>>(diag.ptr, inv.ptr, n);
+    FX_CUDA(cudaMemsetAsync(ndu.ptr, 0, sizeof(double) * n, cs));
+    fx_solve_result lin{};
+    cg<double>(nres.ptr, ndu.ptr, r.ptr, p.ptr, ap.ptr, inv.ptr, o.rtol, o.atol, o.max_iterations, &lin);
+    k_add64<<<ew(n), 256, 0, cs>>>(ndu.ptr, u, n);
+    FX_LAUNCH_CHECK("newton_update");
+    res->iterations += lin.iterations;
+    res->indefinite |= lin.indefinite;
+    ++it;
+    const double dn = test == FX_TEST_NORM_DISP_INCR ? norm(ndu.ptr) : 0.0;
+    rn = residual();
+    if (test == FX_TEST_NORM_DISP_INCR && dn <= tol) {
+      res->final_residual = rn;
+      res->converged = 1;
+      break;
+    }
+  }
+  return it;
+}
+
 }  // namespace fx
 
 struct fx_solver {
@@ -537,6 +607,8 @@ int fx_solver_create(fx_force* f, int32_t method, fx_solve_opts o, fx_solver** o
       s.fl.alloc(F_NFLAG);
       s.zero_count.alloc(1);
       s.hbuf.alloc(64);
+      s.nres.alloc(n);
+      s.ndu.alloc(n);
       if (method == FX_SOLVER_GMRES || method == FX_SOLVER_KRYLOV) {
         const int m = std::max(1, std::min(o.restart, 63));
         s.V.alloc(n * static_cast<size_t>(m + 1));
@@ -631,6 +703,32 @@ int fx_solver_solve(fx_solver* h, const double* b, double* x, fx_solve_result* r
         s.ir(b, x, r);
         break;
     }
+    FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
+    FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
+    r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);
+  });
+}
+
+int fx_solver_newton(fx_solver* h, const double* fext, double* u, int32_t test, double tol, int32_t max_newton,
+                     int32_t* newton_iterations, fx_solve_result* r, void* stream) {
+  return guard([&] {
+    if (!h || !r || !newton_iterations || (h->s.n > 0 && (!fext || !u)) || max_newton < 0 || !(tol >= 0.0))
+      throw fx::Error(FX_E_INVALID, "fx_solver_newton: bad arguments");
+    if (test != FX_TEST_NORM_UNBALANCE && test != FX_TEST_NORM_DISP_INCR)
+      throw fx::Error(FX_E_INVALID, "fx_solver_newton: unknown convergence test");
+    fx::Solver& s = h->s;
+    if (!s.ready) throw fx::Error(FX_E_INVALID, "fx_solver_newton: call fx_solver_setup first");
+    if (s.method != FX_SOLVER_CG) throw fx::Error(FX_E_UNSUPPORTED, "fx_solver_newton: CG solvers only");
+    *r = fx_solve_result{};
+    *newton_iterations = 0;
+    if (s.n == 0) {
+      r->converged = 1;
+      return;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    FX_CUDA(cudaEventRecord(s.ev_in, st));
+    FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
+    *newton_iterations = s.newton(fext, u, test, tol, max_newton, r);
     FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
     FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
     r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);

@@ -276,6 +276,20 @@ int fx_solver_setup(fx_solver* s, fx_coeffs k, void* stream);
 /* FX_SOLVER_IR: the relative tolerance of each inner FP32 solve (default 1e-4). */
 int fx_solver_set_inner_tolerance(fx_solver* s, double inner_rtol);
 int fx_solver_solve(fx_solver* s, const double* b, double* x, fx_solve_result* r, void* stream);
+/* Newton iterations of one quasi-static load step (ImplicitStage's Newton loop without inertia,
+ * src/exec/implicit_stage.cpp:118-437): r = f_ext - f_int(u) with every point's material update
+ * (J2: the return map, which also stores the points' consistent tangents), the Jacobi diagonal
+ * of that tangent, K_t du = r by this CG solver from du = 0, u += du; until the stage's test
+ * (implicit_stage.cpp:199, 241-242, 342) holds, absolute: FX_TEST_NORM_UNBALANCE ||r|| <= tol,
+ * FX_TEST_NORM_DISP_INCR ||du|| <= tol (then the force is evaluated once more at the final u);
+ * or max_newton solves. u (device) holds the start and receives the result; the trial material
+ * state is u's, left for fx_force_commit. r: converged, iterations (CG iterations in all),
+ * rhs_norm = ||f_ext||, initial/final_residual = ||r|| at the first and last evaluation. CG
+ * solvers only (set up with the stiffness coefficient 1). */
+#define FX_TEST_NORM_UNBALANCE 0
+#define FX_TEST_NORM_DISP_INCR 1
+int fx_solver_newton(fx_solver* s, const double* fext, double* u, int32_t test, double tol, int32_t max_newton,
+                     int32_t* newton_iterations, fx_solve_result* r, void* stream);
 
 /* ------------------------------------------------------------------ time stepping
  * ExplicitDifference steps (src/exec/explicit_analysis.cpp:62-84, 687-705): per step
