@@ -140,6 +140,39 @@ def cpu_reference_apply(spec, max_seconds=20.0, max_reps=5):
                        "tangent), built from its sources with a serial/OpenMP Kokkos-subset shim")
 
 
+def explicit_comparison(force, mesh, comp, device, steps=4000):
+    """The explicit wave configuration's time stepping on the bench mesh: ExplicitDifference steps
+    (force + update, CUDA graphs of 16 steps) at dt = 0.5 dt_crit under a 5 Hz Ricker base
+    acceleration, FP64 and FP32; steps/s by CUDA events around each run, and the FP32 surface-centre
+    acceleration history against the FP64 one (max abs difference over the FP64 peak)."""
+    import torch
+    from femorax_b200 import meshes, serving
+    nx, ny, nz = WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"]
+    eqmap = serving.equation_map(comp)
+    rec = int(eqmap[1 + nx // 2 + (nx + 1) * (ny // 2 + (ny + 1) * nz), 0])
+    dt = 0.5 * force.min_critical_dt("ExplicitDifference")
+    ag = meshes.ricker(np.arange(steps) * dt + dt, f0=5.0, amplitude=1.0)
+    dev = torch.device("cuda", device)
+    out = {"steps": steps, "dt_s": dt, "record": "surface-centre x acceleration"}
+    hist = {}
+    for name, dt_ in (("f64", torch.float64), ("f32", torch.float32)):
+        n = mesh.num_equations
+        mass = torch.as_tensor(mesh.lumped_mass, device=dev).to(dt_)
+        u, vh, a, v = (torch.zeros(n, dtype=dt_, device=dev) for _ in range(4))
+        force.explicit_run(mass, u, vh, a, v, dt, 32, ag=ag[:32], direction=0)  # warm-up (graphs, modules)
+        u.zero_(), vh.zero_(), a.zero_(), v.zero_()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        hist[name] = force.explicit_run(mass, u, vh, a, v, dt, steps, ag=ag, direction=0, record_eq=rec)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        out[f"steps_per_s_{name}"] = steps / (e0.elapsed_time(e1) * 1e-3)
+    peak = float(np.max(np.abs(hist["f64"])))
+    out["f32_history_max_abs_diff_over_peak"] = float(np.max(np.abs(hist["f32"] - hist["f64"]))) / peak
+    return out
+
+
 def serve_comparison(device, count=32, seed=1):
     """Solves/s and p50/p99 latency at a 1e-8 relative FP64 residual on a stream of static solves
     on resident meshes (structured blocks, log-uniform 1e4 - 5e5 equations, all arriving at once;
@@ -298,6 +331,7 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    explicit = explicit_comparison(force, mesh, comp, local) if world == 1 and not args.no_serve else None
     served = serve_comparison(local) if world == 1 and not args.no_serve else None
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
@@ -315,6 +349,7 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * neq, "d2h_bytes_per_step": 8 * neq},
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
+            "explicit": explicit,
             "served": served}
     print(json.dumps(line))
     return 0
@@ -327,7 +362,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--no-serve", action="store_true", help="skip the served-versus-plain solve comparison")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the explicit-stepping and served-versus-plain solve comparisons")
     ap.add_argument("--launch", default="", help="pin the box launch shape 'variant,kz' (profiling)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -417,6 +417,18 @@ class LinearSolver:
         return it.value, SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual,
                                      r.final_residual, bool(r.indefinite), r.refinements)
 
+    def newmark_step(self, fext, u, v, a, dt: float, beta: float = 0.25, gamma: float = 0.5, tol: float = 1e-6,
+                     test: str = "NormUnbalance", max_newton: int = 25, stream=None):
+        """One Newmark time step (fx_solver_newmark); u, v, a updated in place. The solver must be
+        set up with OperatorCoefficients(1, gamma / (beta dt), 1 / (beta dt^2))."""
+        r = L.fx_solve_result()
+        it = C.c_int32()
+        t = L.FX_TEST_NORM_UNBALANCE if test == "NormUnbalance" else L.FX_TEST_NORM_DISP_INCR
+        check(lib().fx_solver_newmark(self._h, _ptr(fext), _ptr(u), _ptr(v), _ptr(a), dt, beta, gamma, t, tol,
+                                      max_newton, C.byref(it), C.byref(r), _stream(stream)))
+        return it.value, SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual,
+                                     r.final_residual, bool(r.indefinite), r.refinements)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

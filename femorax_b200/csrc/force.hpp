@@ -129,6 +129,12 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
 
+// stepping.cu: the Newmark form-D kernels (implicit_stage.cpp:29-68)
+void newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
+                     double a2, double a3, double a4, cudaStream_t st);
+void newmark_update(int64_t n, const double* du, double* u, double* v, double* a, double c2, double c3,
+                    cudaStream_t st);
+
 // box.cu (modal node-owner path)
 void box_build_plan(ForceState& s);
 void box_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st,

@@ -199,6 +199,18 @@ __global__ void k_residual64(const double* __restrict__ b, const double* __restr
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     r[i] = b[i] - ax[i];
 }
+// r = b - f - ma
+__global__ void k_dyn_residual(const double* __restrict__ b, const double* __restrict__ ma, double* __restrict__ r,
+                               int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    r[i] = b[i] - r[i] - ma[i];
+}
+__global__ void k_mul(const double* __restrict__ d, const double* __restrict__ x, double* __restrict__ y, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = d[i] * x[i];
+}
 // y = b - y
 __global__ void k_sub_from(const double* __restrict__ b, double* __restrict__ y, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -254,6 +266,7 @@ struct Solver {
   DeviceArray<int> zero_count;
   DeviceArray<double> V, Z, wv, hbuf;  // GMRES
   DeviceArray<double> nres, ndu;       // Newton: residual and increment
+  DeviceArray<double> nut, nvt, nat;   // Newmark: the last step's u, v, a
   int* host_flags = nullptr;           // pinned
   double* host_sc = nullptr;           // pinned
   ~Solver() {
@@ -343,6 +356,8 @@ struct Solver {
   void gmres(const double* b, double* x, fx_solve_result* res);
   void ir(const double* b, double* x, fx_solve_result* res);
   int newton(const double* fext, double* u, int test, double tol, int max_newton, fx_solve_result* res);
+  int newmark(const double* fext, double* u, double* v, double* a, double h, double beta, double gamma, int test,
+              double tol, int max_newton, fx_solve_result* res);
 };
 
 // FGMRES(m) with CGS2, host-side Hessenberg and Givens rotations, as gmres.cpp:32-123.
@@ -548,6 +563,76 @@ int Solver::newton(const double* fext, double* u, int test, double tol, int max_
   return it;
 }
 
+// One Newmark time step (Newmark::newStep with displ == 1 and ImplicitStage's Newton loop with
+// inertia, src/exec/implicit_stage.cpp:29-68, 118-437): predict (v = a1 v + a2 a, a = a4 a + a3 v
+// of the last step; u kept), then Newton: r = f_ext - f_int(u, v) - M a, K_eff du = r by the
+// solver's method (plain FP64 CG, or FP32 CG inside FP64 refinement), u += du, v += c2 du,
+// a += c3 du, with K_eff = K + c2 C + c3 M, c2 = gamma / (beta h), c3 = 1 / (beta h^2): the
+// coefficients the solver must be set up with. M a is the lumped masses times a when every set
+// is lumped, else the mass operator of the general path. Tests as newton().
+int Solver::newmark(const double* fext, double* u, double* v, double* a, double h, double beta, double gamma,
+                    int test, double tol, int max_newton, fx_solve_result* res) {
+  ForceState& fs = f->s;
+  const double c2 = gamma / (beta * h), c3 = 1.0 / (beta * h * h);
+  if (k[0] != 1.0 || k[1] != c2 || k[2] != c3)
+    throw Error(FX_E_INVALID, "newmark: set the solver up with the coefficients (1, gamma/(beta h), 1/(beta h^2))");
+  const double a1 = 1.0 - gamma / beta, a2 = h * (1.0 - 0.5 * gamma / beta), a3 = -1.0 / (beta * h),
+               a4 = 1.0 - 0.5 / beta;
+  newmark_predict(n, u, v, a, nut.ptr, nvt.ptr, nat.ptr, a1, a2, a3, a4, cs);
+  bool all_lumped = fs.lumped_mass.n > 0;
+  for (const auto& q : fs.params_h) all_lumped = all_lumped && q.mass_type == 1;
+  auto norm = [&](const double* x) {
+    dot_device(w, x, x, n, sc.ptr + S_RR, cs);
+    FX_CUDA(cudaMemcpyAsync(host_sc, sc.ptr, sizeof(double) * S_NSCALAR, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+    return std::sqrt(host_sc[S_RR]);
+  };
+  auto residual = [&]() {  // nres = f_ext - f_int(u, v) - M a
+    if (fs.use_box_force()) box_force(fs, u, v, nres.ptr, cs);
+    else general_force(fs, u, v, nres.ptr, cs);
+    if (all_lumped) {
+      k_mul<<<ew(n), 256, 0, cs>>>(fs.lumped_mass.ptr, a, nut.ptr, n);  // nut is free after the predict
+    } else {
+      const double km[3] = {0.0, 0.0, 1.0};
+      const bool init = fs.initial;
+      general_apply(fs, km, a, nut.ptr, cs);
+      fs.initial = init;
+    }
+    k_dyn_residual<<<ew(n), 256, 0, cs>>>(fext, nut.ptr, nres.ptr, n);
+    FX_LAUNCH_CHECK("newmark_residual");
+    return norm(nres.ptr);
+  };
+  res->rhs_norm = norm(fext);
+  int it = 0;
+  double rn = residual();
+  res->initial_residual = rn;
+  for (;;) {
+    res->final_residual = rn;
+    if (test == FX_TEST_NORM_UNBALANCE && rn <= tol) {
+      res->converged = 1;
+      break;
+    }
+    if (it >= max_newton) break;
+    FX_CUDA(cudaMemsetAsync(ndu.ptr, 0, sizeof(double) * n, cs));
+    fx_solve_result lin{};
+    if (method == FX_SOLVER_IR) ir(nres.ptr, ndu.ptr, &lin);
+    else cg<double>(nres.ptr, ndu.ptr, r.ptr, p.ptr, ap.ptr, inv.ptr, o.rtol, o.atol, o.max_iterations, &lin);
+    newmark_update(n, ndu.ptr, u, v, a, c2, c3, cs);
+    res->iterations += lin.iterations;
+    res->refinements += lin.refinements;
+    res->indefinite |= lin.indefinite;
+    ++it;
+    const double dn = test == FX_TEST_NORM_DISP_INCR ? norm(ndu.ptr) : 0.0;
+    rn = residual();
+    if (test == FX_TEST_NORM_DISP_INCR && dn <= tol) {
+      res->final_residual = rn;
+      res->converged = 1;
+      break;
+    }
+  }
+  return it;
+}
+
 }  // namespace fx
 
 struct fx_solver {
@@ -609,6 +694,9 @@ int fx_solver_create(fx_force* f, int32_t method, fx_solve_opts o, fx_solver** o
       s.hbuf.alloc(64);
       s.nres.alloc(n);
       s.ndu.alloc(n);
+      s.nut.alloc(n);
+      s.nvt.alloc(n);
+      s.nat.alloc(n);
       if (method == FX_SOLVER_GMRES || method == FX_SOLVER_KRYLOV) {
         const int m = std::max(1, std::min(o.restart, 63));
         s.V.alloc(n * static_cast<size_t>(m + 1));
@@ -729,6 +817,35 @@ int fx_solver_newton(fx_solver* h, const double* fext, double* u, int32_t test, 
     FX_CUDA(cudaEventRecord(s.ev_in, st));
     FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
     *newton_iterations = s.newton(fext, u, test, tol, max_newton, r);
+    FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
+    FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
+    r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);
+  });
+}
+
+int fx_solver_newmark(fx_solver* h, const double* fext, double* u, double* v, double* a, double dt, double beta,
+                      double gamma, int32_t test, double tol, int32_t max_newton, int32_t* newton_iterations,
+                      fx_solve_result* r, void* stream) {
+  return guard([&] {
+    if (!h || !r || !newton_iterations || (h->s.n > 0 && (!fext || !u || !v || !a)) || max_newton < 0 ||
+        !(tol >= 0.0) || !(dt > 0.0) || !(beta > 0.0) || !(gamma > 0.0))
+      throw fx::Error(FX_E_INVALID, "fx_solver_newmark: bad arguments");
+    if (test != FX_TEST_NORM_UNBALANCE && test != FX_TEST_NORM_DISP_INCR)
+      throw fx::Error(FX_E_INVALID, "fx_solver_newmark: unknown convergence test");
+    fx::Solver& s = h->s;
+    if (!s.ready) throw fx::Error(FX_E_INVALID, "fx_solver_newmark: call fx_solver_setup first");
+    if (s.method != FX_SOLVER_CG && s.method != FX_SOLVER_IR)
+      throw fx::Error(FX_E_UNSUPPORTED, "fx_solver_newmark: CG or IR solvers only");
+    *r = fx_solve_result{};
+    *newton_iterations = 0;
+    if (s.n == 0) {
+      r->converged = 1;
+      return;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    FX_CUDA(cudaEventRecord(s.ev_in, st));
+    FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
+    *newton_iterations = s.newmark(fext, u, v, a, dt, beta, gamma, test, tol, max_newton, r);
     FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
     FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
     r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);

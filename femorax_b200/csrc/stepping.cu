@@ -164,6 +164,19 @@ double stable_dt(int scheme, const ParamGP& p, double w2) {
 
 }  // namespace
 
+void newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
+                     double a2, double a3, double a4, cudaStream_t st) {
+  if (n <= 0) return;
+  k_newmark_predict<<<ew(n), 256, 0, st>>>(u, v, a, ut, vt, at, a1, a2, a3, a4, n);
+  FX_LAUNCH_CHECK("newmark_predict");
+}
+void newmark_update(int64_t n, const double* du, double* u, double* v, double* a, double c2, double c3,
+                    cudaStream_t st) {
+  if (n <= 0) return;
+  k_newmark_update<<<ew(n), 256, 0, st>>>(du, u, v, a, c2, c3, n);
+  FX_LAUNCH_CHECK("newmark_update");
+}
+
 }  // namespace fx
 
 namespace {

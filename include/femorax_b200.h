@@ -290,6 +290,16 @@ int fx_solver_solve(fx_solver* s, const double* b, double* x, fx_solve_result* r
 #define FX_TEST_NORM_DISP_INCR 1
 int fx_solver_newton(fx_solver* s, const double* fext, double* u, int32_t test, double tol, int32_t max_newton,
                      int32_t* newton_iterations, fx_solve_result* r, void* stream);
+/* One Newmark time step of size dt (Newmark::newStep with displ == 1 and ImplicitStage's Newton
+ * loop with inertia, src/exec/implicit_stage.cpp:29-68, 118-437): predict v and a from the last
+ * step (u kept), then Newton iterations r = f_ext - f_int(u, v) - M a, K_eff du = r by this
+ * solver (FX_SOLVER_CG: plain FP64; FX_SOLVER_IR: FP32 CG inside FP64 refinement), u += du,
+ * v += c2 du, a += c3 du, with the test of fx_solver_newton. The solver must be set up with the
+ * coefficients (1, c2 = gamma/(beta dt), c3 = 1/(beta dt^2)). u, v, a (device) hold the last
+ * step's state and receive the new one; the trial material state is left for fx_force_commit. */
+int fx_solver_newmark(fx_solver* s, const double* fext, double* u, double* v, double* a, double dt, double beta,
+                      double gamma, int32_t test, double tol, int32_t max_newton, int32_t* newton_iterations,
+                      fx_solve_result* r, void* stream);
 
 /* ------------------------------------------------------------------ time stepping
  * ExplicitDifference steps (src/exec/explicit_analysis.cpp:62-84, 687-705): per step

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import femorax_b200 as fx
-from femorax_b200 import quasistatic, serving
+from femorax_b200 import serving, stages
 from tests.j2_newton_ref import dense_newton_path, top_shear_load
 from tests.models_for_tests import j2_column
 
@@ -26,10 +26,10 @@ def test_cyclic_path_matches_dense_newton(oracle_mod, total, hk):
     comp = fx.Model(spec).compile()
     mesh = comp.mesh()
     F, mon = top_shear_load(spec, serving.equation_map(comp), total)
-    factors = quasistatic.cyclic_factors(1, 8)
+    factors = stages.cyclic_factors(1, 8)
     want, plastic = dense_newton_path(oracle_mod.PortMesh(mesh), F, factors, mon, tol=1e-6)
     force = fx.InternalForce(mesh)
-    got = quasistatic.load_path(force, torch.as_tensor(F, device=DEV), factors, mon, tol=1e-6)
+    got = stages.load_path(force, torch.as_tensor(F, device=DEV), factors, mon, tol=1e-6)
     assert got.converged
     assert np.max(np.abs(got.monitor - want)) <= 1e-7 * np.max(np.abs(want))
     assert np.array_equal(got.plastic, plastic)
@@ -43,7 +43,7 @@ def test_disp_incr_test_and_elastic_box(oracle_mod):
     force = fx.InternalForce(comp.mesh())
     assert force.info()["box_force"] == 1
     F, mon = top_shear_load(spec, serving.equation_map(comp), 1e5)
-    got = quasistatic.load_path(force, torch.as_tensor(F, device=DEV), [1.0], mon, tol=1e-9, test="NormDispIncr")
+    got = stages.load_path(force, torch.as_tensor(F, device=DEV), [1.0], mon, tol=1e-9, test="NormDispIncr")
     assert got.converged and got.newton[0] <= 2
     x = torch.zeros(comp.num_equations, dtype=torch.float64, device=DEV)
     cg = fx.ConjugateGradient(fx.SolveOptions(relative_tolerance=1e-12))
