@@ -50,6 +50,8 @@ struct BoxArgs {
   double c1, c2;
   T beta;           // force: u + beta v
   const int* skip;  // when set and nonzero on the device, the launch does nothing (a finished solve)
+  int* queue;       // persistent launch: [next tile, CTAs done]; NULL: one CTA per tile (the grid)
+  int gx, gy, gz;   // tiles per axis (persistent launch)
 };
 
 template <class T>
@@ -454,7 +456,28 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
 template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, bool LAYERED>
 __global__ void __launch_bounds__(BX* BY, MINB)
     k_box(BoxArgs<T> a, const __grid_constant__ BoxTable<typename Coef<T>::type> tab) {
-  box_tile<BX, BY, T, MODE, CACHE, LAYERED>(a, &tab, blockIdx.x, blockIdx.y, blockIdx.z);
+  if (!a.queue) {
+    box_tile<BX, BY, T, MODE, CACHE, LAYERED>(a, &tab, blockIdx.x, blockIdx.y, blockIdx.z);
+    return;
+  }
+  // Persistent launch (one wave of CTAs): each CTA takes the next tile (x fastest) from the queue
+  // until none is left, so the last wave of a one-CTA-per-tile grid leaves no SM idle. The last
+  // CTA to finish resets the queue for the next launch (every CTA has stopped taking tiles then).
+  __shared__ int s_tile;
+  const int ntiles = a.gx * a.gy * a.gz;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&a.queue[0], 1);
+    __syncthreads();
+    const int tile = s_tile;
+    __syncthreads();
+    if (tile >= ntiles) break;
+    box_tile<BX, BY, T, MODE, CACHE, LAYERED>(a, &tab, tile % a.gx, (tile / a.gx) % a.gy, tile / (a.gx * a.gy));
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && atomicAdd(&a.queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
+    a.queue[0] = 0;
+    a.queue[1] = 0;
+  }
 }
 
 // Many grids in one launch: CTA b takes work item work[b] = (grid, tile x, tile y, tile z) of the
@@ -485,14 +508,26 @@ const BoxTable<BoxCoef32>& table_of<float>(const BoxPlan& p) {
 template <int BX, int BY, int MINB, bool CACHE, bool LAYERED, class T, int MODE>
 void launch_shape(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   using S = Smem<BX, BY, T, MODE>;
-  static bool configured = false;
-  if (!configured) {
-    FX_CUDA(cudaFuncSetAttribute(k_box<BX, BY, T, MODE, MINB, CACHE, LAYERED>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
-    configured = true;
+  auto kern = k_box<BX, BY, T, MODE, MINB, CACHE, LAYERED>;
+  static int resident = 0;  // CTAs per SM at this shape's registers and shared memory
+  if (!resident) {
+    FX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
+    FX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, BX * BY, S::bytes));
+    resident = std::max(resident, 1);
   }
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
-  k_box<BX, BY, T, MODE, MINB, CACHE, LAYERED><<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p));
+  if (p.shape[sizeof(T) == 4 ? 1 : 0].persistent) {
+    BoxArgs<T> b = a;
+    b.queue = p.queue.ptr;
+    b.gx = static_cast<int>(grid.x);
+    b.gy = static_cast<int>(grid.y);
+    b.gz = static_cast<int>(grid.z);
+    const int ntiles = b.gx * b.gy * b.gz;
+    const int ctas = std::min(ntiles, resident * num_sms());
+    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p));
+  } else {
+    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p));
+  }
   FX_LAUNCH_CHECK("box_operator");
 }
 
@@ -504,14 +539,14 @@ void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
 
 template <class T, int MODE>
 void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
-  switch (p.variant) {
+  switch (p.shape[sizeof(T) == 4 ? 1 : 0].variant) {
     case 0: return launch_one<32, 8, 2, false, T, MODE>(p, a, st);
     case 1: return launch_one<16, 16, 2, false, T, MODE>(p, a, st);
     case 2: return launch_one<16, 8, 4, false, T, MODE>(p, a, st);
     case 3: return launch_one<32, 16, 1, false, T, MODE>(p, a, st);
     case 4: return launch_one<16, 8, 2, true, T, MODE>(p, a, st);
-    case 5: return launch_one<32, 8, 1, true, T, MODE>(p, a, st);
-    case 6: return launch_one<16, 16, 1, true, T, MODE>(p, a, st);
+    case 5: return launch_one<16, 8, 5, false, T, MODE>(p, a, st);
+    case 6: return launch_one<16, 8, 6, false, T, MODE>(p, a, st);
     case 7: return launch_one<32, 4, 4, false, T, MODE>(p, a, st);
     default: return launch_one<16, 32, 1, false, T, MODE>(p, a, st);
   }
@@ -617,9 +652,12 @@ void box_prepare(ForceState& s, const double k[3]) { ensure_coef(s, 0, k); }
 
 void box_set_launch(ForceState& s, int variant, int kz) {
   if (variant < 0 || variant >= kNumVariants) throw Error(FX_E_INVALID, "box launch variant out of range");
-  if (kz < 1) throw Error(FX_E_INVALID, "kz must be positive");
-  s.box.variant = variant;
-  s.box.kz = kz;
+  if (kz == 0) throw Error(FX_E_INVALID, "kz must not be 0");
+  for (auto& sh : s.box.shape) {
+    sh.variant = variant;
+    sh.kz = kz > 0 ? kz : -kz;
+    sh.persistent = kz < 0;
+  }
   s.box.tuned = true;
 }
 
@@ -761,6 +799,7 @@ void box_build_plan(ForceState& s) {
   p.nz = nz;
   for (int d = 0; d < 3; ++d) p.h[d] = h[d];
   p.node_eq.upload(packed);
+  p.queue.upload(std::vector<int>(2, 0));
   p.elem_param.upload(eparam);
   p.grid_node_h = std::move(gnode);
   p.qualifies = true;
@@ -775,7 +814,7 @@ static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const 
   a.nx = s.box.nx;
   a.ny = s.box.ny;
   a.nz = s.box.nz;
-  a.kz = s.box.kz;
+  a.kz = s.box.shape[sizeof(T) == 4 ? 1 : 0].kz;
   a.nparams = s.nparams;
   a.node_eq = s.box.node_eq.ptr;
   a.elem_param = s.box.elem_param.ptr;
@@ -831,73 +870,87 @@ void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cuda
 // columns, 8 planes) without timing.
 constexpr int32_t kTuneMinElements = 262144;
 
-// Times every launch variant and plane count on the operator (FP64, unit stiffness) and keeps the
-// fastest: CUDA events on the stream, median of 5 after 2 warm-ups.
+// Times every launch variant and plane count, as a grid and as a persistent launch, on the operator
+// (unit stiffness) in FP64 and in FP32 and keeps the fastest of each: CUDA events on the stream,
+// L2 flushed before each apply, median of 5 after 2 warm-ups.
 void box_autotune(ForceState& s, cudaStream_t st) {
   if (!s.box.qualifies) return;
   if (s.count < kTuneMinElements) {  // launch-bound: timing costs more than it can save
-    s.box.variant = 2;
-    s.box.kz = 8;
+    for (auto& sh : s.box.shape) sh = BoxPlan::Shape{};
     s.box.tuned = true;
     return;
   }
+  const size_t n = static_cast<size_t>(std::max(s.neq, 1));
   DeviceArray<double> x, y;
-  x.alloc(static_cast<size_t>(std::max(s.neq, 1)));
-  y.alloc(static_cast<size_t>(std::max(s.neq, 1)));
+  DeviceArray<float> x32, y32;
+  x.alloc(n);
+  y.alloc(n);
+  x32.alloc(n);
+  y32.alloc(n);
   x.zero(st);
+  FX_CUDA(cudaMemsetAsync(x32.ptr, 0, sizeof(float) * n, st));
+  // an apply inside a solve finds little of its operand in L2 (the solver's vectors are larger):
+  // a write larger than L2 between the timed applies keeps the timing in that regime
+  DeviceArray<unsigned char> flush;
+  flush.alloc(static_cast<size_t>(256) << 20);
   const double k[3] = {1.0, 0.0, 0.0};
   cudaEvent_t e0, e1;
   FX_CUDA(cudaEventCreate(&e0));
   FX_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int bv = 0, bk = 16;
   const int kzs[] = {8, 16, 32, 64};  // (kz = 4 adds a quarter of redundant planes)
-  for (int v = 0; v < kNumVariants; ++v)
-    for (int kz : kzs) {
-      if (kz > 8 && kz >= 2 * (s.box.nz + 1)) continue;
-      s.box.variant = v;
-      s.box.kz = kz;
-      std::vector<float> times;
-      for (int r = 0; r < 7; ++r) {
-        FX_CUDA(cudaEventRecord(e0, st));
-        box_apply(s, k, x.ptr, y.ptr, st, nullptr);
-        FX_CUDA(cudaEventRecord(e1, st));
-        FX_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        FX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (r >= 2) times.push_back(ms);
-      }
-      std::sort(times.begin(), times.end());
-      const float med = times[times.size() / 2];
-      if (med < best) {
-        best = med;
-        bv = v;
-        bk = kz;
-      }
-    }
+  for (int prec = 0; prec < 2; ++prec) {
+    BoxPlan::Shape& sh = s.box.shape[prec];
+    BoxPlan::Shape best_shape;
+    float best = 1e30f;
+    for (int v = 0; v < kNumVariants; ++v)
+      for (int kz : kzs)
+        for (int pers = 0; pers < 2; ++pers) {
+          if (kz > 8 && kz >= 2 * (s.box.nz + 1)) continue;
+          sh = BoxPlan::Shape{v, kz, pers != 0};
+          std::vector<float> times;
+          for (int r = 0; r < 7; ++r) {
+            FX_CUDA(cudaMemsetAsync(flush.ptr, r, flush.n, st));
+            FX_CUDA(cudaEventRecord(e0, st));
+            if (prec == 0) box_apply(s, k, x.ptr, y.ptr, st, nullptr);
+            else box_apply_f32(s, k, x32.ptr, y32.ptr, st, nullptr);
+            FX_CUDA(cudaEventRecord(e1, st));
+            FX_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            FX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (r >= 2) times.push_back(ms);
+          }
+          std::sort(times.begin(), times.end());
+          const float med = times[times.size() / 2];
+          if (med < best) {
+            best = med;
+            best_shape = sh;
+          }
+        }
+    sh = best_shape;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  s.box.variant = bv;
-  s.box.kz = bk;
   s.box.tuned = true;
 }
 
-
 // ------------------------------------------------------------------ batches of grids
-// One launch shape for batches: 16 x 8 element columns, 4 CTAs per SM, kBatchKz node planes per tile.
+// One launch shape for batches: 16 x 8 element columns, 4 CTAs per SM (FP64) or 6 (FP32), kBatchKz
+// node planes per tile.
 namespace {
-constexpr int kBatchBX = 16, kBatchBY = 8, kBatchMinB = 4, kBatchKz = 8;
+constexpr int kBatchBX = 16, kBatchBY = 8, kBatchKz = 8;
+template <class T>
+constexpr int kBatchMinB = sizeof(T) == 4 ? 6 : 4;  // FP32 fits 6 CTAs per SM without spills
 
 template <class T>
 void batch_launch(const void* inst, const int4* work, int nwork, cudaStream_t st) {
   using S = Smem<kBatchBX, kBatchBY, T, 0>;
   static bool configured = false;
   if (!configured) {
-    FX_CUDA(cudaFuncSetAttribute(k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB>,
+    FX_CUDA(cudaFuncSetAttribute(k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB<T>>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
     configured = true;
   }
-  k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB>
+  k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB<T>>
       <<<nwork, kBatchBX * kBatchBY, S::bytes, st>>>(static_cast<const BoxArgs<T>*>(inst), work);
   FX_LAUNCH_CHECK("box_batch");
 }

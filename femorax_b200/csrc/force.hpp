@@ -64,8 +64,14 @@ struct BoxPlan {
   DeviceArray<int32_t> elem_param;  // [nz ny nx]: parameter set of each element
   DeviceArray<int32_t> node_of;     // host-side check only: grid node -> internal node
   std::vector<int32_t> grid_node_h; // grid node -> internal node
-  // Launch shape chosen by the autotuner: block (bx, by) element columns, kz node planes.
-  int variant = 0, kz = 16;
+  // Launch shape per precision (0: FP64, 1: FP32), chosen by the autotuner: variant (block of
+  // element columns, CTAs per SM), kz node planes per tile, and the persistent form (one wave of
+  // CTAs taking tiles from `queue`) or one CTA per tile.
+  struct Shape {
+    int variant = 2, kz = 8;
+    bool persistent = false;
+  } shape[2];
+  DeviceArray<int> queue;    // [next tile, CTAs done], zero between launches
   bool tuned = false;
   // coefficient tables for the last operator coefficients
   DeviceArray<BoxCoef> coef;

@@ -165,7 +165,8 @@ def test_box_rejected_for_ties():
 
 
 def test_launch_variants_agree(oracle_mod):
-    """Every launch shape and plane count gives the same bits (the owner sums in a fixed order)."""
+    """Every launch shape and plane count, as a grid or persistent (negative kz), gives the same bits
+    (the owner sums in a fixed order)."""
     mesh, force, _ = build(meshes.layered_box(33, 17, 21, layers=3, seed=1)[0])
     k = fx.OperatorCoefficients(1.0, 0.1, 2.0)
     x = t(np.random.default_rng(15).standard_normal(mesh.num_equations))
@@ -174,7 +175,7 @@ def test_launch_variants_agree(oracle_mod):
     import ctypes as C
     lib = L.lib()
     for variant in range(9):
-        for kz in (1, 3, 8, 64):
+        for kz in (1, 3, 8, 64, -3, -8):
             lib_rc = lib.fx_force_set_launch(force._h, variant, kz) if hasattr(lib, "fx_force_set_launch") else None
             if lib_rc is None:
                 pytest.skip("no launch override")
