@@ -19,7 +19,7 @@ from .meshes import ModelSpec
 
 __all__ = ["Model", "Compiled", "MeshArrays", "InternalForce", "OperatorCoefficients", "MatrixFreeOperator",
            "SolveOptions", "SolveResult", "LinearSolver", "ConjugateGradient", "Gmres", "KrylovSolver",
-           "MixedPrecisionSolver", "BatchEngine", "VectorOps", "FxError", "ModelSpec"]
+           "MixedPrecisionSolver", "BatchEngine", "BatchedNewton", "VectorOps", "FxError", "ModelSpec"]
 
 
 def _i32(a):
@@ -534,6 +534,73 @@ class BatchEngine:
         if h:
             try:
                 lib().fx_engine_destroy(h)
+            except Exception:  # interpreter shutdown: the library may be gone already
+                pass
+            self._h = None
+
+
+class BatchedNewton:
+    """Quasi-static load steps of many independent meshes at once (fx_nbatch_*): one combined
+    mesh (instance i's equations at offsets[i] .. offsets[i] + equations[i]), one launch per element
+    kernel for all instances, per-instance Newton test and Jacobi-PCG on the device; per instance
+    bit for bit LinearSolver.newton (NormUnbalance) on that mesh alone."""
+
+    def __init__(self, meshes, options: SolveOptions = None, device: int = 0):
+        o = options or SolveOptions(relative_tolerance=1e-12, max_iterations=20000)
+        arr = (L.fx_mesh * len(meshes))()
+        keep = []
+        for i, m in enumerate(meshes):
+            cm, k = m.to_c()
+            arr[i] = cm
+            keep.append(k)
+        opts = L.fx_solve_opts(o.relative_tolerance, o.absolute_tolerance, o.max_iterations, o.lanes, o.restart, 0)
+        h = C.c_void_p()
+        check(lib().fx_nbatch_create(arr, len(meshes), device, opts, C.byref(h)))
+        self._h = h
+        self.count = len(meshes)
+        self.device = device
+        off = (C.c_int64 * (self.count + 1))()
+        neq = (C.c_int64 * self.count)()
+        check(lib().fx_nbatch_layout(h, off, neq))
+        self.offsets = np.array(off[:])
+        self.equations = np.array(neq[:])
+        self.total = int(self.offsets[-1])
+        self._force = lib().fx_nbatch_force(h)
+
+    def combine(self, per_instance) -> np.ndarray:
+        """Host vectors of the instances -> one vector in the combined layout."""
+        out = np.zeros(self.total)
+        for i, v in enumerate(per_instance):
+            out[self.offsets[i]:self.offsets[i] + self.equations[i]] = v
+        return out
+
+    def split(self, combined):
+        """One vector in the combined layout -> the instances' host vectors."""
+        c = np.asarray(combined)
+        return [c[self.offsets[i]:self.offsets[i] + self.equations[i]] for i in range(self.count)]
+
+    def step(self, fext, u, tol: float = 1e-6, max_newton: int = 25, stream=None):
+        """One load step of every instance (u updated in place): (Newton solves, SolveResults)."""
+        it = (C.c_int32 * self.count)()
+        res = (L.fx_solve_result * self.count)()
+        check(lib().fx_nbatch_step(self._h, _ptr(fext), _ptr(u), tol, max_newton, it, res, _stream(stream)))
+        out = [SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual, r.final_residual,
+                           bool(r.indefinite), r.refinements) for r in res]
+        return np.array(it[:]), out
+
+    def commit_state(self, stream=None):
+        check(lib().fx_force_commit(self._force, _stream(stream)))
+
+    def plastic_points(self) -> int:
+        n = C.c_int64()
+        check(lib().fx_force_plastic_points(self._force, C.byref(n)))
+        return n.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().fx_nbatch_destroy(h)
             except Exception:  # interpreter shutdown: the library may be gone already
                 pass
             self._h = None

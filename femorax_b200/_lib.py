@@ -134,6 +134,12 @@ PROTOTYPES = {
     "fx_newmark_update": (C.c_int, [C.c_int64, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
     "fx_force_state": (C.c_int, [vp, C.c_int32, p_f64, C.c_int64]),
     "fx_force_set_state": (C.c_int, [vp, C.c_int32, p_f64, C.c_int64]),
+    "fx_nbatch_create": (C.c_int, [C.POINTER(fx_mesh), C.c_int32, C.c_int32, fx_solve_opts, C.POINTER(vp)]),
+    "fx_nbatch_destroy": (None, [vp]),
+    "fx_nbatch_layout": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "fx_nbatch_force": (vp, [vp]),
+    "fx_nbatch_step": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32), C.POINTER(fx_solve_result),
+                                 vp]),
     "fx_engine_create": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, fx_coeffs, fx_solve_opts, C.c_double,
                                    C.POINTER(vp)]),
     "fx_engine_destroy": (None, [vp]),

@@ -38,6 +38,7 @@ CUDA_SOURCES = [
     ("solve.cu", []),
     ("stepping.cu", []),
     ("batch.cu", []),
+    ("nbatch.cu", []),
 ]
 CXX_SOURCES = ["api.cpp", "compile.cpp"]
 

@@ -1,0 +1,587 @@
+// Batched quasi-static Newton on many independent meshes (the batched J2 configuration): the
+// meshes are concatenated into one mesh whose element kernels and gather run every instance in
+// one launch each, and each instance keeps its own Newton test and its own Jacobi-PCG recurrence
+// on the device (scalars and stopping flags per instance; CG iterations as CUDA graphs).
+//
+// Instance s owns the equations [off_s, off_s + n_s) of the combined numbering, off_s a multiple
+// of the 2048-entry reduction chunk; its elements keep their order, so every equation's gather
+// sums the same (element, DOF) values in the same order as the instance alone, and the chunk
+// reductions over its range are the documented order of a vector of n_s entries. An instance's
+// Newton iterates, CG iterates and material states are therefore bit for bit those of
+// fx_solver_newton (NormUnbalance) on the instance alone.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "force.hpp"
+#include "vector.hpp"
+
+namespace fx {
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int64_t kMaxInstanceChunks = 2048;  // one level of chunk sums per instance
+
+// per-instance scalars and flags
+enum : int { N_RN = 0, N_BB, N_RZ, N_PAP, N_ALPHA, N_BETA, N_RR, N_RZNEW, N_TOL, N_RNORM, NNS = 12 };
+enum : int {
+  G_NEWTON_DONE = 0,  // the Newton test has passed or the iteration limit is reached
+  G_CONV,             // the Newton test passed
+  G_ITERS,            // Newton solves
+  G_CG_DONE,          // this CG solve is finished (the apply's and the vector kernels' gate)
+  G_CG_ITERS, G_CG_TOTAL, G_CG_CONV, G_INDEF,
+  NNF = 8
+};
+
+struct Range {
+  int64_t off, n, c0, nc;
+};
+
+__device__ __forceinline__ int64_t chunk_len(const Range& r, int64_t begin) {
+  const int64_t end = r.off + r.n;
+  return (end - begin < kChunk) ? end - begin : kChunk;
+}
+
+// chunk sums of x.y over the chunks of instances whose flag `gate` is 0 (column 0 of part)
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_dot(const double* __restrict__ x, const double* __restrict__ y, int64_t nchunks,
+             const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl, int gate,
+             int lanes, double* __restrict__ part) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + gate]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  double acc = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) acc = fma(x[begin + k], y[begin + k], acc);
+  double total = 0.0;
+  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  if (lane == 0) part[c] = total;
+}
+
+// second level: instance s's `ncol` columns of chunk sums (column j at part + j * ld) into
+// sc[s * NNS + dst + j], a warp per (instance, column), for instances whose flag `gate` is 0
+__global__ void k_nb_level(const double* __restrict__ part, int64_t ld, int ncol, const Range* __restrict__ rg,
+                           const int* __restrict__ fl, int gate, int count, int lanes, double* __restrict__ sc,
+                           int dst) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= count * ncol) return;
+  const int s = w / ncol, j = w % ncol;
+  if (fl[s * NNF + gate]) return;
+  const double* p = part + static_cast<int64_t>(j) * ld + rg[s].c0;
+  double acc = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < rg[s].nc; k += lanes) acc += p[k];
+  double total = 0.0;
+  for (int l = 0; l < lanes; ++l) total += __shfl_sync(0xffffffffu, acc, l);
+  if (lane == 0) sc[s * NNS + dst + j] = total;
+}
+
+// r = f_ext - f_int for instances still iterating
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_residual(const double* __restrict__ fext, double* __restrict__ r, int64_t nchunks,
+                  const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_NEWTON_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  for (int64_t k = lane; k < len; k += 32) r[begin + k] = fext[begin + k] - r[begin + k];
+}
+
+// the Newton test per instance (NormUnbalance, absolute); instances that continue start a CG
+// solve: G_CG_DONE = 0
+__global__ void k_nb_test(double* sc, int* fl, int count, double tol, int max_newton) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  double* c = sc + s * NNS;
+  if (f[G_NEWTON_DONE]) return;
+  const double rn = sqrt(c[N_RN]);
+  c[N_RNORM] = rn;
+  if (rn <= tol) {
+    f[G_CONV] = 1;
+    f[G_NEWTON_DONE] = 1;
+  } else if (f[G_ITERS] >= max_newton) {
+    f[G_NEWTON_DONE] = 1;
+  }
+  f[G_CG_DONE] = f[G_NEWTON_DONE];
+}
+
+// inverse of the tangent's diagonal (0 at equations of no instance)
+__global__ void k_nb_inverse(const double* __restrict__ d, double* __restrict__ inv, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    inv[i] = d[i] != 0.0 ? 1.0 / d[i] : 0.0;
+}
+
+// CG from du = 0 (K 0 = 0): du = 0, rr = r, z = inv rr, p = z; chunk sums of rr.rr and rr.z
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_cg_begin(const double* __restrict__ r, double* __restrict__ du, double* __restrict__ rr,
+                  double* __restrict__ p, const double* __restrict__ inv, int64_t nchunks,
+                  const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl, int lanes,
+                  double* __restrict__ part, int64_t ld) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  for (int64_t k = lane; k < len; k += 32) du[begin + k] = 0.0;
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      const double ri = fma(-1.0, 0.0, r[i]);
+      const double zi = inv[i] * ri;
+      rr[i] = ri;
+      p[i] = zi;
+      srr = fma(ri, ri, srr);
+      srz = fma(ri, zi, srz);
+    }
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    part[c] = trr;
+    part[ld + c] = trz;
+  }
+}
+
+// per instance: the CG start (ConjugateGradient's tolerance max(rtol ||b||, atol), b = r)
+__global__ void k_nb_cg_start(double* sc, int* fl, int count, double rtol, double atol, int max_it) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  double* c = sc + s * NNS;
+  if (f[G_CG_DONE]) return;
+  const double rhs = sqrt(c[N_RR]);  // b.b: the same sum as rr.rr at du = 0
+  const double rn = sqrt(c[N_RR]);
+  c[N_RZ] = c[N_RZNEW];
+  const double tol = rtol * rhs;
+  c[N_TOL] = tol > atol ? tol : atol;
+  f[G_CG_ITERS] = 0;
+  f[G_CG_CONV] = rn <= c[N_TOL];
+  f[G_CG_DONE] = f[G_CG_CONV] || max_it <= 0;
+}
+
+__global__ void k_nb_alpha(double* sc, int* fl, int count) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  double* c = sc + s * NNS;
+  if (f[G_CG_DONE]) return;
+  const double pap = c[N_PAP];
+  if (!(pap > 0.0)) {
+    f[G_INDEF] = 1;
+    f[G_CG_DONE] = 1;
+    return;
+  }
+  c[N_ALPHA] = c[N_RZ] / pap;
+}
+
+// du += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_update(const double* __restrict__ sc, const int* __restrict__ fl, const double* __restrict__ p,
+                const double* __restrict__ ap, const double* __restrict__ inv, double* __restrict__ du,
+                double* __restrict__ rr, int64_t nchunks, const int* __restrict__ owner, const Range* __restrict__ rg,
+                int lanes, double* __restrict__ part, int64_t ld) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+  const double alpha = sc[s * NNS + N_ALPHA];
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      du[i] = fma(alpha, p[i], du[i]);
+      const double ri = fma(-alpha, ap[i], rr[i]);
+      rr[i] = ri;
+      const double zi = inv[i] * ri;
+      srr = fma(ri, ri, srr);
+      srz = fma(ri, zi, srz);
+    }
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    part[c] = trr;
+    part[ld + c] = trz;
+  }
+}
+
+__global__ void k_nb_beta(double* sc, int* fl, int count, int max_it) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  double* c = sc + s * NNS;
+  if (f[G_CG_DONE]) return;
+  const double rn = sqrt(c[N_RR]);
+  const int it = ++f[G_CG_ITERS];
+  if (rn <= c[N_TOL]) {
+    f[G_CG_CONV] = 1;
+    f[G_CG_DONE] = 1;
+    return;
+  }
+  if (it >= max_it) {
+    f[G_CG_DONE] = 1;
+    return;
+  }
+  c[N_BETA] = c[N_RZNEW] / c[N_RZ];
+  c[N_RZ] = c[N_RZNEW];
+}
+
+// p = inv rr + beta p
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_p(const double* __restrict__ sc, const int* __restrict__ fl, const double* __restrict__ inv,
+           const double* __restrict__ rr, double* __restrict__ p, int64_t nchunks, const int* __restrict__ owner,
+           const Range* __restrict__ rg) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+  const double beta = sc[s * NNS + N_BETA];
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  for (int64_t k = lane; k < len; k += 32) {
+    const int64_t i = begin + k;
+    p[i] = fma(beta, p[i], inv[i] * rr[i]);
+  }
+}
+
+// u += du for instances that solved this iteration; their counters
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_correct(const double* __restrict__ du, double* __restrict__ u, int64_t nchunks,
+                 const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_NEWTON_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  for (int64_t k = lane; k < len; k += 32) u[begin + k] += du[begin + k];
+}
+
+__global__ void k_nb_iteration_end(int* fl, int count) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  if (f[G_NEWTON_DONE]) return;
+  f[G_CG_TOTAL] += f[G_CG_ITERS];
+  f[G_ITERS] += 1;
+}
+
+unsigned chunk_grid(int64_t nchunks) { return static_cast<unsigned>(std::max<int64_t>(1, (nchunks + kWarps - 1) / kWarps)); }
+unsigned ew(int64_t n) {
+  const int64_t blocks = (n + 255) / 256;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, static_cast<int64_t>(num_sms()) * 8)));
+}
+
+}  // namespace
+
+struct NBatch {
+  int device = 0;
+  int count = 0;
+  int64_t total = 0, nchunks = 0;
+  fx_force* force = nullptr;
+  fx_solve_opts o{};
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::vector<Range> rg_h;
+  DeviceArray<Range> rg;
+  DeviceArray<int> owner;
+  DeviceArray<double> r, du, rr, p, ap, d, inv, zero, part, sc;
+  DeviceArray<int> fl;
+  int* fl_h = nullptr;
+  double* sc_h = nullptr;
+  cudaGraphExec_t graph = nullptr;
+
+  ~NBatch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (fl_h) cudaFreeHost(fl_h);
+    if (sc_h) cudaFreeHost(sc_h);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (cs) cudaStreamDestroy(cs);
+    if (force) fx_force_destroy(force);
+  }
+
+  void read_flags() {
+    FX_CUDA(cudaMemcpyAsync(fl_h, fl.ptr, sizeof(int) * NNF * count, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaMemcpyAsync(sc_h, sc.ptr, sizeof(double) * NNS * count, cudaMemcpyDeviceToHost, cs));
+    FX_CUDA(cudaStreamSynchronize(cs));
+  }
+  unsigned inst_grid() const { return static_cast<unsigned>((count + 127) / 128); }
+  void level(int ncol, int gate, int dst) {
+    const int warps = count * ncol;
+    k_nb_level<<<(warps + 7) / 8, 256, 0, cs>>>(part.ptr, nchunks, ncol, rg.ptr, fl.ptr, gate, count, o.lanes,
+                                                sc.ptr, dst);
+    FX_LAUNCH_CHECK("nbatch_level");
+  }
+
+  void cg_iteration() {
+    const double k[3] = {1.0, 0.0, 0.0};
+    const unsigned g = chunk_grid(nchunks);
+    general_apply(force->s, k, p.ptr, ap.ptr, cs);
+    k_nb_dot<<<g, 32 * kWarps, 0, cs>>>(p.ptr, ap.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_CG_DONE, o.lanes,
+                                        part.ptr);
+    level(1, G_CG_DONE, N_PAP);
+    k_nb_alpha<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+    k_nb_update<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p.ptr, ap.ptr, inv.ptr, du.ptr, rr.ptr, nchunks, owner.ptr,
+                                           rg.ptr, o.lanes, part.ptr, nchunks);
+    level(2, G_CG_DONE, N_RR);
+    k_nb_beta<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, o.max_iterations);
+    k_nb_p<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv.ptr, rr.ptr, p.ptr, nchunks, owner.ptr, rg.ptr);
+    FX_LAUNCH_CHECK("nbatch_cg");
+  }
+
+  bool any(int flag, int value) const {
+    for (int s = 0; s < count; ++s)
+      if (fl_h[s * NNF + flag] == value) return true;
+    return false;
+  }
+
+  // one load step of every instance (NormUnbalance, absolute tol)
+  void step(const double* fext, double* u, double tol, int max_newton) {
+    const double k[3] = {1.0, 0.0, 0.0};
+    const unsigned g = chunk_grid(nchunks);
+    FX_CUDA(cudaMemsetAsync(fl.ptr, 0, sizeof(int) * NNF * count, cs));
+    for (;;) {
+      general_force(force->s, u, zero.ptr, r.ptr, cs);
+      k_nb_residual<<<g, 32 * kWarps, 0, cs>>>(fext, r.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr);
+      k_nb_dot<<<g, 32 * kWarps, 0, cs>>>(r.ptr, r.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_NEWTON_DONE, o.lanes,
+                                          part.ptr);
+      level(1, G_NEWTON_DONE, N_RN);
+      k_nb_test<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, tol, max_newton);
+      FX_LAUNCH_CHECK("nbatch_test");
+      read_flags();
+      if (!any(G_NEWTON_DONE, 0)) break;
+      general_diagonal(force->s, k, d.ptr, cs);
+      k_nb_inverse<<<ew(total), 256, 0, cs>>>(d.ptr, inv.ptr, total);
+      k_nb_cg_begin<<<g, 32 * kWarps, 0, cs>>>(r.ptr, du.ptr, rr.ptr, p.ptr, inv.ptr, nchunks, owner.ptr, rg.ptr,
+                                               fl.ptr, o.lanes, part.ptr, nchunks);
+      level(2, G_CG_DONE, N_RR);
+      k_nb_cg_start<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, o.rtol, o.atol, o.max_iterations);
+      FX_LAUNCH_CHECK("nbatch_cg_begin");
+      const int block = 8;
+      for (int i = 0; i < block; ++i) cg_iteration();
+      read_flags();
+      while (any(G_CG_DONE, 0)) {
+        if (!graph) {
+          cudaGraph_t gr = nullptr;
+          FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+          try {
+            for (int i = 0; i < block; ++i) cg_iteration();
+          } catch (...) {
+            cudaStreamEndCapture(cs, &gr);
+            if (gr) cudaGraphDestroy(gr);
+            throw;
+          }
+          FX_CUDA(cudaStreamEndCapture(cs, &gr));
+          const cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
+          cudaGraphDestroy(gr);
+          FX_CUDA(e);
+        }
+        FX_CUDA(cudaGraphLaunch(graph, cs));
+        read_flags();
+      }
+      k_nb_correct<<<g, 32 * kWarps, 0, cs>>>(du.ptr, u, nchunks, owner.ptr, rg.ptr, fl.ptr);
+      k_nb_iteration_end<<<inst_grid(), 128, 0, cs>>>(fl.ptr, count);
+      FX_LAUNCH_CHECK("nbatch_correct");
+    }
+  }
+};
+
+}  // namespace fx
+
+struct fx_nbatch {
+  fx::NBatch b;
+};
+
+namespace {
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return FX_OK;
+  } catch (const fx::Error& e) {
+    fx::set_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    fx::set_error(e.what());
+    return FX_E_INVALID;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int fx_nbatch_create(const fx_mesh* meshes, int32_t count, int32_t device, fx_solve_opts o, fx_nbatch** out) {
+  return guard([&] {
+    if (!meshes || count <= 0 || !out) throw fx::Error(FX_E_INVALID, "fx_nbatch_create: bad arguments");
+    if (o.lanes <= 0) o.lanes = 32;
+    if (o.lanes > 32 || o.max_iterations < 0) throw fx::Error(FX_E_INVALID, "fx_nbatch_create: bad solver options");
+    // offsets of every instance in the combined mesh
+    int64_t N = 0, E = 0, Pn = 0, Q = 0;
+    std::vector<int64_t> no(count), eo(count), po(count), qo(count);
+    for (int i = 0; i < count; ++i) {
+      const fx_mesh& m = meshes[i];
+      if (m.num_equations <= 0) throw fx::Error(FX_E_INVALID, "fx_nbatch_create: an instance has no equations");
+      if (fx::chunks_of(m.num_equations) > fx::kMaxInstanceChunks)
+        throw fx::Error(FX_E_UNSUPPORTED, "fx_nbatch_create: an instance has more than 2048 * 2048 equations");
+      no[i] = N, eo[i] = E, po[i] = Pn, qo[i] = Q;
+      N += m.num_nodes;
+      E += m.count;
+      Pn += m.num_params;
+      Q += fx::chunks_of(m.num_equations) * fx::kChunk;
+    }
+    if (N > INT32_MAX || E > INT32_MAX || Q > INT32_MAX) throw fx::Error(FX_E_UNSUPPORTED, "fx_nbatch_create: too large");
+    const int64_t P = (E + 31) / 32 * 32;
+    std::vector<double> coords(static_cast<size_t>(3 * N));
+    std::vector<int32_t> node(static_cast<size_t>(8 * P), 0), eq(static_cast<size_t>(24 * P), -1),
+        param(static_cast<size_t>(P), 0);
+    std::vector<fx_param_set> params(static_cast<size_t>(Pn));
+    std::vector<double> lumped(static_cast<size_t>(Q), 0.0), nmass(static_cast<size_t>(Q), 0.0),
+        namass(static_cast<size_t>(Q), 0.0);
+    std::vector<int8_t> eqdof(static_cast<size_t>(Q), 0);
+    bool any_lumped = false, any_nmass = false, any_namass = false;
+    for (int i = 0; i < count; ++i) {
+      const fx_mesh& m = meshes[i];
+      for (int d = 0; d < 3; ++d)
+        std::copy(m.coords + static_cast<int64_t>(d) * m.num_nodes, m.coords + static_cast<int64_t>(d + 1) * m.num_nodes,
+                  coords.begin() + d * N + no[i]);
+      for (int32_t e = 0; e < m.count; ++e) {
+        const int64_t ce = eo[i] + e;
+        for (int a = 0; a < 8; ++a)
+          node[a * P + ce] = static_cast<int32_t>(m.node[static_cast<int64_t>(a) * m.padded + e] + no[i]);
+        for (int k = 0; k < 24; ++k) {
+          const int32_t q = m.eq[static_cast<int64_t>(k) * m.padded + e];
+          eq[k * P + ce] = q >= 0 ? static_cast<int32_t>(q + qo[i]) : -1;
+        }
+        param[ce] = static_cast<int32_t>(m.param[e] + po[i]);
+      }
+      std::copy(m.params, m.params + m.num_params, params.begin() + po[i]);
+      auto put = [&](const double* src, std::vector<double>& dst, bool& any) {
+        if (!src) return;
+        any = true;
+        std::copy(src, src + m.num_equations, dst.begin() + qo[i]);
+      };
+      put(m.lumped_mass, lumped, any_lumped);
+      put(m.nodal_mass, nmass, any_nmass);
+      put(m.nodal_alpha_mass, namass, any_namass);
+      if (m.eq_dof) std::copy(m.eq_dof, m.eq_dof + m.num_equations, eqdof.begin() + qo[i]);
+    }
+    fx_mesh cm{};
+    cm.num_nodes = static_cast<int32_t>(N);
+    cm.num_equations = static_cast<int32_t>(Q);
+    cm.coords = coords.data();
+    cm.count = static_cast<int32_t>(E);
+    cm.padded = static_cast<int32_t>(P);
+    cm.node = node.data();
+    cm.eq = eq.data();
+    cm.param = param.data();
+    cm.num_params = static_cast<int32_t>(Pn);
+    cm.params = params.data();
+    cm.lumped_mass = any_lumped ? lumped.data() : nullptr;
+    cm.nodal_mass = any_nmass ? nmass.data() : nullptr;
+    cm.nodal_alpha_mass = any_namass ? namass.data() : nullptr;
+    cm.eq_dof = eqdof.data();
+    auto* h = new fx_nbatch;
+    fx::NBatch& b = h->b;
+    try {
+      const int rc = fx_force_create(&cm, device, &b.force);
+      if (rc != FX_OK) throw fx::Error(rc, fx_last_error());
+      b.device = device;
+      b.count = count;
+      b.total = Q;
+      b.nchunks = fx::chunks_of(Q);
+      b.o = o;
+      b.rg_h.resize(static_cast<size_t>(count));
+      std::vector<int> owner(static_cast<size_t>(b.nchunks), -1);
+      for (int i = 0; i < count; ++i) {
+        const int64_t nc = fx::chunks_of(meshes[i].num_equations);
+        b.rg_h[i] = fx::Range{qo[i], meshes[i].num_equations, qo[i] / fx::kChunk, nc};
+        for (int64_t c = 0; c < nc; ++c) owner[qo[i] / fx::kChunk + c] = i;
+      }
+      FX_CUDA(cudaSetDevice(device));
+      FX_CUDA(cudaStreamCreateWithFlags(&b.cs, cudaStreamNonBlocking));
+      FX_CUDA(cudaEventCreateWithFlags(&b.ev_in, cudaEventDisableTiming));
+      FX_CUDA(cudaEventCreateWithFlags(&b.ev_out, cudaEventDisableTiming));
+      b.rg.upload(b.rg_h);
+      b.owner.upload(owner);
+      for (auto* v : {&b.r, &b.du, &b.rr, &b.p, &b.ap, &b.d, &b.inv, &b.zero}) {
+        v->alloc(static_cast<size_t>(Q));
+        v->zero(nullptr);
+      }
+      b.part.alloc(static_cast<size_t>(b.nchunks) * 2);
+      b.sc.alloc(static_cast<size_t>(count) * fx::NNS);
+      b.fl.alloc(static_cast<size_t>(count) * fx::NNF);
+      FX_CUDA(cudaMallocHost(&b.fl_h, sizeof(int) * fx::NNF * count));
+      FX_CUDA(cudaMallocHost(&b.sc_h, sizeof(double) * fx::NNS * count));
+      FX_CUDA(cudaDeviceSynchronize());
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+void fx_nbatch_destroy(fx_nbatch* b) { delete b; }
+
+int fx_nbatch_layout(const fx_nbatch* h, int64_t* offsets, int64_t* equations) {
+  return guard([&] {
+    if (!h || !offsets) throw fx::Error(FX_E_INVALID, "fx_nbatch_layout: bad arguments");
+    for (int i = 0; i < h->b.count; ++i) {
+      offsets[i] = h->b.rg_h[i].off;
+      if (equations) equations[i] = h->b.rg_h[i].n;
+    }
+    offsets[h->b.count] = h->b.total;
+  });
+}
+
+fx_force* fx_nbatch_force(fx_nbatch* h) { return h ? h->b.force : nullptr; }
+
+int fx_nbatch_step(fx_nbatch* h, const double* fext, double* u, double tol, int32_t max_newton,
+                   int32_t* newton_iterations, fx_solve_result* results, void* stream) {
+  return guard([&] {
+    if (!h || !fext || !u || !(tol >= 0.0) || max_newton < 0)
+      throw fx::Error(FX_E_INVALID, "fx_nbatch_step: bad arguments");
+    fx::NBatch& b = h->b;
+    FX_CUDA(cudaSetDevice(b.device));
+    auto st = static_cast<cudaStream_t>(stream);
+    FX_CUDA(cudaEventRecord(b.ev_in, st));
+    FX_CUDA(cudaStreamWaitEvent(b.cs, b.ev_in, 0));
+    b.step(fext, u, tol, max_newton);
+    FX_CUDA(cudaEventRecord(b.ev_out, b.cs));
+    FX_CUDA(cudaStreamWaitEvent(st, b.ev_out, 0));
+    for (int i = 0; i < b.count; ++i) {
+      const int* f = b.fl_h + i * fx::NNF;
+      const double* c = b.sc_h + i * fx::NNS;
+      if (newton_iterations) newton_iterations[i] = f[fx::G_ITERS];
+      if (results) {
+        fx_solve_result r{};
+        r.converged = f[fx::G_CONV];
+        r.iterations = f[fx::G_CG_TOTAL];
+        r.final_residual = c[fx::N_RNORM];
+        r.indefinite = f[fx::G_INDEF];
+        r.status = r.converged ? FX_OK : (r.indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);
+        results[i] = r;
+      }
+    }
+  });
+}
+
+}  // extern "C"

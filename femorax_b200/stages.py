@@ -13,7 +13,8 @@ import dataclasses
 
 import numpy as np
 
-from . import ConjugateGradient, MatrixFreeOperator, MixedPrecisionSolver, OperatorCoefficients, SolveOptions
+from . import (BatchedNewton, ConjugateGradient, MatrixFreeOperator, MixedPrecisionSolver, OperatorCoefficients,
+               SolveOptions)
 
 
 def cyclic_factors(cycles: int, steps_per_cycle: int) -> np.ndarray:
@@ -97,3 +98,39 @@ def newmark_run(force, load, steps: int, dt: float, monitor_eq: int, mixed: bool
     torch.cuda.synchronize(dev)
     secs = time.perf_counter() - t0
     return NewmarkResult(torch.stack(mon).cpu().numpy(), np.array(nit), np.array(inner), np.array(refs), ok, secs)
+
+
+@dataclasses.dataclass
+class BatchedPathResult:
+    monitor: np.ndarray          # [steps, instances]: each instance's monitored displacement
+    newton: np.ndarray           # [steps, instances]: Newton solves
+    converged: bool
+    seconds: float               # wall time of the steps
+
+
+def batched_load_path(meshes, fext_units, factors, monitor_eqs, tol: float = 1e-6, cg_rtol: float = 1e-12,
+                      max_newton: int = 25, device: int = 0) -> BatchedPathResult:
+    """`load_path` for many meshes at once (BatchedNewton): instance i under factor *
+    fext_units[i] (host), monitoring its equation monitor_eqs[i]; per instance the same bits as
+    load_path on that mesh alone."""
+    import time
+
+    import torch
+    b = BatchedNewton(meshes, SolveOptions(relative_tolerance=cg_rtol, max_iterations=20000), device)
+    dev = torch.device("cuda", device)
+    F = torch.as_tensor(b.combine(fext_units), device=dev)
+    u = torch.zeros(b.total, dtype=torch.float64, device=dev)
+    idx = torch.as_tensor(np.asarray(b.offsets[:-1]) + np.asarray(monitor_eqs), device=dev)
+    mon, nit = [], []
+    ok = True
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for lam in factors:
+        it, res = b.step(F * float(lam), u, tol=tol, max_newton=max_newton)
+        ok = ok and all(r.converged for r in res)
+        b.commit_state()
+        mon.append(u[idx].clone())
+        nit.append(it)
+    torch.cuda.synchronize(dev)
+    secs = time.perf_counter() - t0
+    return BatchedPathResult(torch.stack(mon).cpu().numpy(), np.array(nit), ok, secs)

@@ -324,6 +324,33 @@ int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, d
 int fx_newmark_update(int64_t n, const double* du, double* u, double* v, double* a, double c2, double c3,
                       void* stream);
 
+/* ------------------------------------------------------------------ batched Newton
+ * Quasi-static load steps of many independent meshes at once (the batched J2 configuration): the
+ * instances are concatenated into one mesh (instance s's equations at [offset_s, offset_s + n_s),
+ * offsets multiples of 2048, the gaps unused), whose element kernels and gather run every
+ * instance in one launch each, while each instance keeps its own Newton test and its own
+ * Jacobi-PCG recurrence on the device (per-instance scalars and stopping flags, CG iterations as
+ * CUDA graphs). Per instance the iterates and material states are bit for bit those of
+ * fx_solver_newton with FX_TEST_NORM_UNBALANCE on that mesh alone. No counterpart in the
+ * reference (one mesh per process; per instance its ImplicitStage Newton loop,
+ * src/exec/implicit_stage.cpp:118-437, with ConjugateGradient, cg.cpp:24-71).
+ *   fx_nbatch_create   the instances' mesh arrays (as fx_compiled_mesh gives them), CG options
+ *   fx_nbatch_layout   offsets[count + 1] (offsets[count] = combined length) and the instances'
+ *                      equation counts (may be NULL)
+ *   fx_nbatch_step     one load step of every instance: f_ext and u (device, combined layout; u
+ *                      holds the start and receives the result), NormUnbalance ||r|| <= tol,
+ *                      at most max_newton solves; per instance the Newton solves and a result
+ *                      (converged, CG iterations in all, final ||r||)
+ *   fx_nbatch_force    the combined fx_force (owned by the batch): fx_force_commit commits every
+ *                      instance's material state, fx_force_state reads it */
+typedef struct fx_nbatch fx_nbatch;
+int fx_nbatch_create(const fx_mesh* meshes, int32_t count, int32_t device, fx_solve_opts o, fx_nbatch** out);
+void fx_nbatch_destroy(fx_nbatch* b);
+int fx_nbatch_layout(const fx_nbatch* b, int64_t* offsets, int64_t* equations);
+fx_force* fx_nbatch_force(fx_nbatch* b);
+int fx_nbatch_step(fx_nbatch* b, const double* fext, double* u, double tol, int32_t max_newton,
+                   int32_t* newton_iterations, fx_solve_result* results, void* stream);
+
 /* ------------------------------------------------------------------ batched and served solves
  * An engine holds many independent meshes ("slots", each one fx_force on the box path, a
  * structured grid of equal boxes) resident on one device and solves K_eff x = b for all of them

@@ -1,0 +1,55 @@
+"""Batched quasi-static Newton (fx_nbatch_*) on a B200: several J2 columns of different sizes,
+hardening and loads on one cyclic load path in one batch. Each instance's displacement history
+and Newton solve counts must be bit for bit those of the single-instance path (fx_solver_newton
+with the same options) on that mesh alone: the combined mesh keeps every instance's gather order,
+and every instance's reductions run over its own range in the documented order.
+"""
+import numpy as np
+import pytest
+
+import femorax_b200 as fx
+from femorax_b200 import serving, stages
+from tests.j2_newton_ref import top_shear_load
+from tests.models_for_tests import j2_column
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+DEV = torch.device("cuda:0")
+CASES = [(1, 1, 4, 0.5, 8e3), (2, 2, 4, 0.0, 30e3), (3, 2, 6, 1.0, 40e3), (2, 3, 8, 0.5, 20e3),
+         (1, 2, 2, 0.5, 6e3), (3, 3, 4, 0.25, 45e3)]
+
+
+def instances():
+    out = []
+    for nx, ny, nz, hk, total in CASES:
+        spec = j2_column(nx=nx, ny=ny, nz=nz, hk=hk)
+        comp = fx.Model(spec).compile()
+        F, mon = top_shear_load(spec, serving.equation_map(comp), total)
+        out.append((comp.mesh(), F, mon))
+    return out
+
+
+def test_batched_newton_equals_single_paths():
+    inst = instances()
+    factors = stages.cyclic_factors(1, 8)
+    batched = stages.batched_load_path([m for m, _, _ in inst], [F for _, F, _ in inst], factors,
+                                       [mon for _, _, mon in inst], tol=1e-6)
+    assert batched.converged
+    for i, (mesh, F, mon) in enumerate(inst):
+        single = stages.load_path(fx.InternalForce(mesh), torch.as_tensor(F, device=DEV), factors, mon, tol=1e-6)
+        assert single.converged
+        assert np.array_equal(batched.monitor[:, i], single.monitor), i
+        assert np.array_equal(batched.newton[:, i], single.newton), i
+
+
+def test_layout():
+    inst = instances()
+    b = fx.BatchedNewton([m for m, _, _ in inst])
+    assert np.all(b.offsets[:-1] % 2048 == 0)
+    assert list(b.equations) == [m.num_equations for m, _, _ in inst]
+    v = [np.arange(n, dtype=float) + i for i, n in enumerate(b.equations)]
+    back = b.split(b.combine(v))
+    assert all(np.array_equal(a, c) for a, c in zip(back, v))
