@@ -94,13 +94,14 @@ def fix_base(nx, ny):
 
 
 def box_model(nx, ny, nz, size=(1.0, 1.0, 1.0), E=50e6, nu=0.3, rho=2000.0, lumped=False, b=(0.0, 0.0, 0.0),
-              fixed_base=True):
-    """One material over an nx x ny x nz block of size `size` (metres), base z = 0 fixed."""
+              fixed_base=True, kind=0, sigma_y=0.0, H=0.0, hk=0.0):
+    """One material over an nx x ny x nz block of size `size` (metres), base z = 0 fixed; kind 1
+    makes it J2 with yield stress sigma_y, hardening H and kinematic share hk."""
     hx, hy, hz = size[0] / nx, size[1] / ny, size[2] / nz
     tags, coords = block_nodes(nx, ny, nz, hx, hy, hz)
     etags, conn = block_connectivity(nx, ny, nz)
-    spec = ModelSpec(tags=tags, coords=coords, groups=[Group(E, nu, rho, etags, conn, b=b, lumped=lumped)],
-                     grid=(nx, ny, nz, hx, hy, hz))
+    group = Group(E, nu, rho, etags, conn, b=b, lumped=lumped, kind=kind, sigma_y=sigma_y, H=H, hk=hk)
+    spec = ModelSpec(tags=tags, coords=coords, groups=[group], grid=(nx, ny, nz, hx, hy, hz))
     if fixed_base:
         spec.fix_node, spec.fix_dof = fix_base(nx, ny)
     return spec

@@ -134,3 +134,42 @@ def batched_load_path(meshes, fext_units, factors, monitor_eqs, tol: float = 1e-
     torch.cuda.synchronize(dev)
     secs = time.perf_counter() - t0
     return BatchedPathResult(torch.stack(mon).cpu().numpy(), np.array(nit), ok, secs)
+
+
+def j2_instances(count: int, seed: int = 0, sizes=(1, 2, 4, 8, 16, 24), nz_range=(20, 400), h: float = 0.5,
+                 load_ratio: float = 1.2):
+    """The batched J2 configuration's instances, seeded: soil columns and blocks of nx = ny drawn
+    from `sizes` and nz uniform in nz_range, boxes of h metres, J2 with sigma_y ~ U[50, 200] kPa,
+    E ~ U[40, 120] MPa, nu 0.3, H = 0.05 E, hk 0.5, base fixed; each with a uniform horizontal
+    shear traction on its top face totalling load_ratio times the force that first yields the
+    base in elastic bending, sigma_y b^3 / (6 L) (b the width, L the height).
+    Returns [(spec, total top force)]."""
+    from . import meshes
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(sizes))
+        nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
+        sy = rng.uniform(50e3, 200e3)
+        E = rng.uniform(40e6, 120e6)
+        spec = meshes.box_model(n, n, nz, (n * h, n * h, nz * h), E=E, nu=0.3, kind=1, sigma_y=sy, H=0.05 * E,
+                                hk=0.5)
+        b, L = n * h, nz * h
+        out.append((spec, load_ratio * sy * b ** 3 / (6.0 * L)))
+    return out
+
+
+def top_shear(spec, eqmap, total):
+    """x-direction nodal loads of a uniform shear traction on the top face summing to `total`, and
+    the equation of the top corner node's x displacement (eqmap: serving.equation_map)."""
+    nx, ny, nz, _, _, _ = spec.grid
+    ci = np.full(nx + 1, 2.0)
+    cj = np.full(ny + 1, 2.0)
+    ci[[0, -1]] = 1.0
+    cj[[0, -1]] = 1.0
+    i, j = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), indexing="ij")
+    tags = 1 + i + (nx + 1) * (j + (ny + 1) * nz)
+    q = eqmap[tags.ravel(), 0]
+    f = np.zeros(int(eqmap.max()) + 1)
+    np.add.at(f, q[q >= 0], (total / (4.0 * nx * ny) * np.outer(ci, cj)).ravel()[q >= 0])
+    return f, int(eqmap[tags[-1, -1], 0])
