@@ -13,16 +13,16 @@
 // transforms give the element's modes with 24 butterflies; the modal operator is 24 products and
 // 24 fused couplings; the result is split back into a bottom and a top face; the bottom face is
 // added (in modal form) to the top face left by the element below, and one 2D inverse transform
-// gives the four corner values of the face. About 160 FP64 operations per element.
+// gives the four corner values of the face. About 165 FP64 operations per element.
 //
 // Scatter. Each CTA owns a (BX-1) x (BY-1) column of grid nodes over kz node planes. Per plane it
 // stages the node values of the plane above (one-node halo) in shared memory, evaluates the BX x BY
 // element columns around its nodes (halo columns are evaluated by both neighbouring CTAs: no
 // atomics, no cross-CTA exchange), and gives each owned node the sum of the face corner values of
 // its four columns in a fixed order. Every equation is written once, by its owner, in a fixed
-// order: deterministic for any launch shape, and y needs no zeroing. The plane values are read into
-// registers one plane (equations: two planes) ahead, so global latency overlaps the element work;
-// two barriers per plane.
+// order: deterministic for any launch shape, and y needs no zeroing. Equations and values are
+// copied into a shared-memory ring several planes ahead (cp.async), so global latency overlaps the
+// element work; one barrier per plane.
 #include <algorithm>
 #include <cstring>
 #include <cmath>
@@ -82,7 +82,7 @@ struct Smem {
   static constexpr int NV = MODE == 1 ? 2 : 1;  // staged vectors: x, or u and v
   static constexpr size_t coef_bytes = sizeof(typename Coef<T>::type) * kParamsInShared;
   static constexpr size_t bytes =
-      coef_bytes + sizeof(T) * (3 * NT + NB * NV * 3 * NS + 3 * NO) + sizeof(int32_t) * (NB * NS + NO);
+      coef_bytes + sizeof(T) * (6 * NT + NB * NV * 3 * NS + 6 * NO) + sizeof(int32_t) * (NB * NS + 2 * NO);
 };
 
 __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, int bytes, bool valid) {
@@ -211,11 +211,12 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
   static_assert(BX == 16 || BX == 32, "a row of element columns must lie within one warp");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* cs = reinterpret_cast<CT*>(smem_raw);
-  T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [3][NT]: row sums for the row below
-  T* xs = ys + 3 * NT;                                      // [NB planes][NV][3][NS]: node values
-  T* yo = xs + NB * NV * 3 * NS;                            // [3][NO]: owned nodes' sums, last plane
-  int32_t* es = reinterpret_cast<int32_t*>(yo + 3 * NO);   // [NB][NS]: equations
-  int32_t* yq = es + NB * NS;                               // [NO]: owned nodes' equations (0: none)
+  // ys, yo and yq have two buffers, by the parity of the plane: one barrier per plane suffices
+  T* ys = reinterpret_cast<T*>(smem_raw + S::coef_bytes);  // [2][3][NT]: row sums for the row below
+  T* xs = ys + 6 * NT;                                      // [NB planes][NV][3][NS]: node values
+  T* yo = xs + NB * NV * 3 * NS;                            // [2][3][NO]: owned nodes' sums
+  int32_t* es = reinterpret_cast<int32_t*>(yo + 6 * NO);   // [NB][NS]: equations
+  int32_t* yq = es + NB * NS;                               // [2][NO]: owned nodes' equations (0: none)
   if (a.skip && *a.skip) return;
 
   const int t = threadIdx.x;
@@ -291,16 +292,18 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
         cp_async_zfill(&xs[((b * NV + 1) * 3 + d) * NS + s], free_dof ? a.v + q : a.v, sizeof(T), free_dof);
     }
   };
-  auto store_plane = [&]() {  // the owned nodes' sums of the last plane, with the nodal terms
+  auto store_plane = [&](int par) {  // the owned nodes' sums of a plane, with the nodal terms
+    const T* yop = yo + par * 3 * NO;
+    const int32_t* yqp = yq + par * NO;
 #pragma unroll
     for (int j = 0; j < OPT; ++j) {
       if (oitem[j] < 0) continue;
       const int o = oitem[j] >> 2, d = oitem[j] & 3;
-      const int32_t packed = yq[o];
+      const int32_t packed = yqp[o];
       const uint32_t mask = static_cast<uint32_t>(packed) >> 29;
       if (!((mask >> d) & 1u)) continue;
       const int32_t q = (packed & 0x1FFFFFFF) + __popc(mask & ((1u << d) - 1u));
-      T val = yo[d * NO + o];
+      T val = yop[d * NO + o];
       if (MODE == 0) {
         if (a.nm1) val += T(a.c1 * a.nm1[q]) * a.x[q];
         if (a.nm2) val += T(a.c2 * a.nm2[q]) * a.x[q];
@@ -357,9 +360,9 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
     for (int f = 0; f < 4; ++f) facc[d][f] = T(0);
   int bb = 0;  // buffer of plane ek; plane ek + i is in (bb + i) % NB
 
-  for (int ek = k0 - 1; ek < k1; ++ek) {
+  int par = 0;  // buffer of ys, yo, yq for plane ek
+  for (int ek = k0 - 1; ek < k1; ++ek, par ^= 1) {
     const int tb = bb + 1 == NB ? 0 : bb + 1;
-    if (ek - 1 >= k0) store_plane();  // plane ek - 1 (left by the last iteration, before its barrier)
     copy_equations(ek + D + 2);
     copy_values(ek + D);
     cp_async_commit();
@@ -430,27 +433,31 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
     // row is the next lane (a row of columns lies within one warp), so its corners come by
     // shuffle; the pair sums for the row below go through shared memory.
     T phi[3];
+    T* ysp = ys + par * 3 * NT;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const T c01n = __shfl_down_sync(0xffffffffu, cor[d][2], 1);
       const T c00n = __shfl_down_sync(0xffffffffu, cor[d][0], 1);
       phi[d] = cor[d][3] + c01n;
-      ys[d * NT + t] = cor[d][1] + c00n;
+      ysp[d * NT + t] = cor[d][1] + c00n;
     }
+    // The one barrier of the plane: this plane's pair sums, the last plane's owned sums and the
+    // staging ring's copies up to the planes the next iteration reads are all in place after it.
+    cp_async_wait<1>();
     __syncthreads();
+    if (ek - 1 >= k0) store_plane(par ^ 1);  // plane ek - 1
     if (owner_slot) {
       if (out_plane) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) yo[d * NO + o_idx] = phi[d] + ys[d * NT + t + BX];
+        for (int d = 0; d < 3; ++d) yo[(par * 3 + d) * NO + o_idx] = phi[d] + ysp[d * NT + t + BX];
       }
-      yq[o_idx] = own_packed;
+      yq[par * NO + o_idx] = own_packed;
     }
-    cp_async_wait<1>();
-    __syncthreads();
     bb = tb;
   }
   cp_async_wait<0>();
-  if (k1 - 1 >= k0) store_plane();
+  __syncthreads();
+  if (k1 - 1 >= k0) store_plane(par ^ 1);  // the last plane (par has advanced past it)
 }
 
 template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, bool LAYERED>
