@@ -50,6 +50,7 @@ struct BoxArgs {
   double c1, c2;
   T beta;           // force: u + beta v
   const int* skip;  // when set and nonzero on the device, the launch does nothing (a finished solve)
+  const T* __restrict__ escale;  // per-element E scale (sets that differ only in E), or NULL
   int* queue;       // persistent launch: [next tile, CTAs done]; NULL: one CTA per tile (the grid)
   int gx, gy, gz;   // tiles per axis (persistent launch)
 };
@@ -59,10 +60,12 @@ struct Coef;
 template <>
 struct Coef<double> {
   using type = BoxCoef;
+  using scaled = BoxScaled;
 };
 template <>
 struct Coef<float> {
   using type = BoxCoef32;
+  using scaled = BoxScaled32;
 };
 
 template <class T>
@@ -140,8 +143,10 @@ __device__ __forceinline__ void load_pair(const float* __restrict__ src, float& 
 // the three mu couplings of r = 1.
 // VEC: the table is in shared or global memory (16-byte loads); otherwise it is a kernel
 // parameter, read value by value.
-template <bool VEC, class T, class CT>
-__device__ __forceinline__ void modal_apply(const CT& k, T t[3][8]) {
+// SCALED: k is a BoxScaled table; each group's result is sc times its stiffness part plus the
+// mass diagonal dmm of its modes.
+template <bool VEC, bool SCALED = false, class T, class CT>
+__device__ __forceinline__ void modal_apply(const CT& k, T t[3][8], T sc = T(1)) {
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     T c[4];
@@ -177,6 +182,11 @@ __device__ __forceinline__ void modal_apply(const CT& k, T t[3][8]) {
       o0 = fma(c[3], u2, o0);
       o2 = fma(c[3], u0, o2);
     }
+    if constexpr (SCALED) {
+      o0 = fma(sc, o0, T(k.dmm[s ^ 1]) * u0);
+      o1 = fma(sc, o1, T(k.dmm[s ^ 2]) * u1);
+      o2 = fma(sc, o2, T(k.dmm[s ^ 4]) * u2);
+    }
     t[0][s ^ 1] = o0;
     t[1][s ^ 2] = o1;
     t[2][s ^ 4] = o2;
@@ -200,9 +210,13 @@ __device__ __forceinline__ void modal_apply(const CT& k, T t[3][8]) {
 // per node whatever the equation numbering (the reference's RCM numbering puts neighbouring
 // grid nodes hundreds of equations apart). The owners of a plane's nodes leave their sums and
 // equations in shared memory; the stores run in the next iteration, after the barrier.
-// One CTA's tile (bx, by, bz) of grid a. LAYERED: the coefficient tables come from *tab (layered
-// grids), else from a.coef.
-template <int BX, int BY, class T, int MODE, bool CACHE, bool LAYERED>
+// Where the element coefficients come from: a table per parameter set in a.coef (shared memory
+// for few sets), the layered tables *tab (a kernel parameter), or one table in a.coef scaled per
+// element by a.escale (sets that differ only in E).
+enum CoefMode : int { kPerSet = 0, kLayered = 1, kScaled = 2 };
+
+// One CTA's tile (bx, by, bz) of grid a, the coefficients by CM.
+template <int BX, int BY, class T, int MODE, bool CACHE, int CM>
 __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typename Coef<T>::type>* tab, int bx,
                                          int by, int bz) {
   using S = Smem<BX, BY, T, MODE>;
@@ -234,14 +248,18 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
   const int s00 = ci + cj * SX;          // staging slot of the column's corner (0, 0)
 
   // coefficient tables in shared memory (few parameter sets) or read through L1
-  const bool shared_coef = !LAYERED && a.nparams <= kParamsInShared;
+  using ST = typename Coef<T>::scaled;
+  constexpr bool LAYERED = CM == kLayered;
+  constexpr bool scaled = CM == kScaled;
+  const bool shared_coef = !LAYERED && (scaled || a.nparams <= kParamsInShared);
   if (shared_coef) {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(a.coef);
     uint32_t* dst = reinterpret_cast<uint32_t*>(cs);
-    const int words = a.nparams * static_cast<int>(sizeof(CT) / 4);
+    const int words = scaled ? static_cast<int>(sizeof(ST) / 4) : a.nparams * static_cast<int>(sizeof(CT) / 4);
     for (int w = t; w < words; w += NT) dst[w] = __ldg(&src[w]);
   }
   const CT* coef = shared_coef ? cs : reinterpret_cast<const CT*>(a.coef);
+  const ST& stab = *reinterpret_cast<const ST*>(cs);
 
   // ---- this thread's fixed work items
   constexpr int SPT = (NS + NT - 1) / NT;             // node slots (equation copies)
@@ -350,7 +368,12 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
   for (int k = k0 - 1; k <= k0 + D - 2; ++k) copy_values(k);
   cp_async_commit();
   cp_async_wait<0>();
+  auto scale_of = [&](int ek) {
+    if constexpr (scaled) return (col_ok && ek >= 0 && ek < a.nz) ? __ldg(&a.escale[ek * layer + col_off]) : T(0);
+    return T(0);
+  };
   int p_cur = param_of(k0 - 1), p_nxt = param_of(k0);
+  T s_cur = scale_of(k0 - 1), s_nxt = scale_of(k0);
   __syncthreads();
   T fb[3][4], facc[3][4];
   if constexpr (CACHE) face(0, &fb[0][0], 4);
@@ -369,6 +392,9 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
     const int p_here = p_cur;
     p_cur = p_nxt;
     p_nxt = param_of(ek + 2);
+    const T s_here = s_cur;
+    s_cur = s_nxt;
+    s_nxt = scale_of(ek + 2);
     const bool out_plane = own && ek >= k0;
     const int32_t own_packed = out_plane ? es[bb * NS + s00 + SX + 1] : 0;
     // ---- element (ei, ej, ek): modes from the top face (transformed here) and the bottom face
@@ -391,6 +417,10 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
         modal_apply<false>(tab->c[p_here], tv);
         if (MODE == 1)
           for (int d = 0; d < 3; ++d) body[d] = T(tab->c[p_here].body[d]);
+      } else if constexpr (scaled) {
+        modal_apply<true, true>(stab, tv, s_here);
+        if (MODE == 1)
+          for (int d = 0; d < 3; ++d) body[d] = T(stab.body[d]);
       } else {
         const CT& k = coef[p_here];
         modal_apply<true>(k, tv);
@@ -460,11 +490,11 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
   if (k1 - 1 >= k0) store_plane(par ^ 1);  // the last plane (par has advanced past it)
 }
 
-template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, bool LAYERED>
+template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, int CM>
 __global__ void __launch_bounds__(BX* BY, MINB)
     k_box(BoxArgs<T> a, const __grid_constant__ BoxTable<typename Coef<T>::type> tab) {
   if (!a.queue) {
-    box_tile<BX, BY, T, MODE, CACHE, LAYERED>(a, &tab, blockIdx.x, blockIdx.y, blockIdx.z);
+    box_tile<BX, BY, T, MODE, CACHE, CM>(a, &tab, blockIdx.x, blockIdx.y, blockIdx.z);
     return;
   }
   // Persistent launch (one wave of CTAs): each CTA takes the next tile (x fastest) from the queue
@@ -478,7 +508,7 @@ __global__ void __launch_bounds__(BX* BY, MINB)
     const int tile = s_tile;
     __syncthreads();
     if (tile >= ntiles) break;
-    box_tile<BX, BY, T, MODE, CACHE, LAYERED>(a, &tab, tile % a.gx, (tile / a.gx) % a.gy, tile / (a.gx * a.gy));
+    box_tile<BX, BY, T, MODE, CACHE, CM>(a, &tab, tile % a.gx, (tile / a.gx) % a.gy, tile / (a.gx * a.gy));
     __syncthreads();
   }
   if (threadIdx.x == 0 && atomicAdd(&a.queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
@@ -494,7 +524,7 @@ __global__ void __launch_bounds__(BX* BY, MINB)
     k_box_batch(const BoxArgs<T>* __restrict__ inst, const int4* __restrict__ work) {
   const int4 w = work[blockIdx.x];
   const BoxArgs<T> a = inst[w.x];
-  box_tile<BX, BY, T, MODE, false, false>(a, nullptr, w.y, w.z, w.w);
+  box_tile<BX, BY, T, MODE, false, kPerSet>(a, nullptr, w.y, w.z, w.w);
 }
 
 // ------------------------------------------------------------------ launch variants
@@ -512,10 +542,10 @@ const BoxTable<BoxCoef32>& table_of<float>(const BoxPlan& p) {
   return p.tab32;
 }
 
-template <int BX, int BY, int MINB, bool CACHE, bool LAYERED, class T, int MODE>
+template <int BX, int BY, int MINB, bool CACHE, int CM, class T, int MODE>
 void launch_shape(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   using S = Smem<BX, BY, T, MODE>;
-  auto kern = k_box<BX, BY, T, MODE, MINB, CACHE, LAYERED>;
+  auto kern = k_box<BX, BY, T, MODE, MINB, CACHE, CM>;
   static int resident = 0;  // CTAs per SM at this shape's registers and shared memory
   if (!resident) {
     FX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
@@ -540,8 +570,9 @@ void launch_shape(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
 
 template <int BX, int BY, int MINB, bool CACHE, class T, int MODE>
 void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
-  if (p.layered) return launch_shape<BX, BY, MINB, CACHE, true, T, MODE>(p, a, st);
-  return launch_shape<BX, BY, MINB, CACHE, false, T, MODE>(p, a, st);
+  if (p.layered) return launch_shape<BX, BY, MINB, CACHE, kLayered, T, MODE>(p, a, st);
+  if (p.scaled) return launch_shape<BX, BY, MINB, CACHE, kScaled, T, MODE>(p, a, st);
+  return launch_shape<BX, BY, MINB, CACHE, kPerSet, T, MODE>(p, a, st);
 }
 
 template <class T, int MODE>
@@ -576,6 +607,7 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
   auto w = [](int bit) { return bit ? 2.0 / 3.0 : 2.0; };
   std::vector<BoxCoef> h(static_cast<size_t>(s.nparams));
   std::vector<BoxCoef32> h32(static_cast<size_t>(s.nparams));
+  BoxScaled sc0{};  // scaled grids: set 0's stiffness (per element times E_e / E_0) and its mass
   for (int32_t i = 0; i < s.nparams; ++i) {
     const ParamGP& q = s.params_h[i];
     double l2m, lam, mu;
@@ -608,6 +640,10 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
         dk *= 2.0 * J * sk;
         const double dm = cons ? sm * q.rho * J * w(bit(0)) * w(bit(1)) * w(bit(2)) : 8.0 * sm * q.rho * J;
         c.grp[m ^ (1 << comp)][comp] = (dk + dm) / 64.0;
+        if (i == 0) {
+          sc0.grp[m ^ (1 << comp)][comp] = dk / 64.0;
+          sc0.dmm[m] = dm / 64.0;
+        }
       }
     // couplings of axis pair pr (components pr, pr + 1 mod 3; third axis e): lambda part for
     // r = 0 in group 0 and for r = 1 in group 2^e; mu part for r = 0 in group 2^c0 + 2^c1 and
@@ -637,10 +673,27 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
       p.tab.c[i] = h[i];
       p.tab32.c[i] = h32[i];
     }
-  if (p.coef.n != h.size()) p.coef.alloc(h.size());
-  if (p.coef32.n != h32.size()) p.coef32.alloc(h32.size());
-  FX_CUDA(cudaMemcpy(p.coef.ptr, h.data(), h.size() * sizeof(BoxCoef), cudaMemcpyHostToDevice));
-  FX_CUDA(cudaMemcpy(p.coef32.ptr, h32.data(), h32.size() * sizeof(BoxCoef32), cudaMemcpyHostToDevice));
+  if (p.scaled) {
+    BoxScaled32 c32{};
+    for (int g = 0; g < 8; ++g) sc0.grp[g][3] = h[0].grp[g][3];
+    for (int j = 0; j < 4; ++j) sc0.more[j] = h[0].more[j];
+    for (int d = 0; d < 3; ++d) sc0.body[d] = h[0].body[d];
+    for (int g = 0; g < 8; ++g)
+      for (int j = 0; j < 4; ++j) c32.grp[g][j] = static_cast<float>(sc0.grp[g][j]);
+    for (int j = 0; j < 4; ++j) c32.more[j] = static_cast<float>(sc0.more[j]);
+    for (int m = 0; m < 8; ++m) c32.dmm[m] = static_cast<float>(sc0.dmm[m]);
+    for (int d = 0; d < 3; ++d) c32.body[d] = static_cast<float>(sc0.body[d]);
+    if (p.scoef.n != 1) p.scoef.alloc(1);
+    if (p.scoef32.n != 1) p.scoef32.alloc(1);
+    FX_CUDA(cudaMemcpy(p.scoef.ptr, &sc0, sizeof(sc0), cudaMemcpyHostToDevice));
+    FX_CUDA(cudaMemcpy(p.scoef32.ptr, &c32, sizeof(c32), cudaMemcpyHostToDevice));
+  }
+  if (!p.scaled) {  // (a scaled grid reads its one table only)
+    if (p.coef.n != h.size()) p.coef.alloc(h.size());
+    if (p.coef32.n != h32.size()) p.coef32.alloc(h32.size());
+    FX_CUDA(cudaMemcpy(p.coef.ptr, h.data(), h.size() * sizeof(BoxCoef), cudaMemcpyHostToDevice));
+    FX_CUDA(cudaMemcpy(p.coef32.ptr, h32.data(), h32.size() * sizeof(BoxCoef32), cudaMemcpyHostToDevice));
+  }
   p.last_mode = mode;
   for (int j = 0; j < 3; ++j) p.last_k[j] = k[j];
 }
@@ -780,6 +833,27 @@ void box_build_plan(ForceState& s) {
       }
     p.tab.layer[k] = p.tab32.layer[k] = static_cast<uint8_t>(first);
   }
+  // scaled: many sets that differ only in E (per-element moduli): one table, per-element scales
+  p.scaled = false;
+  if (!p.layered && s.nparams > kParamsInShared) {
+    const ParamGP& q0 = s.params_h[0];
+    bool same = q0.E > 0.0;
+    for (const auto& q : s.params_h)
+      same = same && q.kind == 0 && q.E > 0.0 && q.nu == q0.nu && q.rho == q0.rho && q.b[0] == q0.b[0] &&
+             q.b[1] == q0.b[1] && q.b[2] == q0.b[2] && q.alphaM == q0.alphaM && q.betaK == q0.betaK &&
+             q.betaKinit == q0.betaKinit && q.betaKcomm == q0.betaKcomm && q.mass_type == q0.mass_type;
+    if (same) {
+      std::vector<double> es(eparam.size());
+      std::vector<float> es32(eparam.size());
+      for (size_t c = 0; c < eparam.size(); ++c) {
+        es[c] = s.params_h[eparam[c]].E / q0.E;
+        es32[c] = static_cast<float>(es[c]);
+      }
+      p.escale.upload(es);
+      p.escale32.upload(es32);
+      p.scaled = true;
+    }
+  }
   // force form: lumped masses and one beta
   const double beta0 = s.params_h[0].betaK + s.params_h[0].betaKinit + s.params_h[0].betaKcomm;
   bool one_beta = true;
@@ -826,6 +900,15 @@ static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const 
   a.node_eq = s.box.node_eq.ptr;
   a.elem_param = s.box.elem_param.ptr;
   a.coef = coef;
+  if (s.box.scaled) {
+    if constexpr (sizeof(T) == 8) {
+      a.coef = s.box.scoef.ptr;
+      a.escale = s.box.escale.ptr;
+    } else {
+      a.coef = s.box.scoef32.ptr;
+      a.escale = s.box.escale32.ptr;
+    }
+  }
   a.x = x;
   a.v = v;
   a.y = y;
@@ -985,6 +1068,7 @@ size_t box_args_bytes(bool f32) { return f32 ? sizeof(BoxArgs<float>) : sizeof(B
 
 void box_fill_args(ForceState& s, const double k[3], bool f32, const void* x, void* y, const int* skip, void* dst) {
   if (!s.box.qualifies) throw Error(FX_E_UNSUPPORTED, "batched operator: not a box grid: " + s.box.why_not);
+  if (s.box.scaled) throw Error(FX_E_UNSUPPORTED, "batched operator: per-element moduli are not batched");
   if (f32) fill_args<float>(s, k, x, y, skip, dst);
   else fill_args<double>(s, k, x, y, skip, dst);
 }

@@ -37,6 +37,27 @@ struct BoxCoef32 {  // the same in FP32 for the mixed-precision operator
   float pad_;
 };
 
+// The table of a grid whose parameter sets differ only in E (a per-element modulus, the
+// heterogeneous cube): the element operator is E_e / E_ref times the stiffness of the reference
+// set plus the common mass, so one table serves every element with a per-element scale. grp and
+// more as in BoxCoef for the stiffness alone (E_ref), dmm[m] the mass diagonal of mode m (the same
+// for the three components).
+struct BoxScaled {
+  double grp[8][4];
+  double more[4];
+  double dmm[8];
+  double body[3];
+  double pad_;
+};
+static_assert(sizeof(BoxScaled) == 48 * 8, "BoxScaled layout");
+struct BoxScaled32 {
+  float grp[8][4];
+  float more[4];
+  float dmm[8];
+  float body[3];
+  float pad_;
+};
+
 // The coefficient tables of a layered grid (one parameter set per element plane, at most
 // kTableParams sets and kTableLayers planes), passed to the box kernel as a kernel parameter: the
 // set of a plane is then the same for every thread, and its coefficients are read through the
@@ -77,6 +98,11 @@ struct BoxPlan {
   DeviceArray<BoxCoef> coef;
   DeviceArray<BoxCoef32> coef32;
   bool layered = false;  // one parameter set per element plane (kernel-parameter tables)
+  bool scaled = false;   // the sets differ only in E: one table and a per-element scale
+  DeviceArray<double> escale;   // [nz ny nx]: E_e / E_ref
+  DeviceArray<float> escale32;
+  DeviceArray<BoxScaled> scoef;
+  DeviceArray<BoxScaled32> scoef32;
   BoxTable<BoxCoef> tab{};
   BoxTable<BoxCoef32> tab32{};
   double last_k[4] = {-1, -1, -1, -1};
