@@ -40,7 +40,8 @@ int64_t ForceState::device_bytes() const {
   int64_t b = coords.bytes() + node.bytes() + eq.bytes() + param.bytes() + params.bytes() + gstart.bytes() +
               glist.bytes() + slots.bytes() + nodal_mass.bytes() + nodal_alpha_mass.bytes() + lumped_mass.bytes() +
               eq_dof.bytes() + wx.bytes() + wy.bytes() + scratch.bytes();
-  b += box.node_eq.bytes() + box.elem_param.bytes() + box.coef.bytes() + box.coef32.bytes();
+  b += box.node_eq.bytes() + box.elem_param.bytes() + box.escale.bytes() + box.escale32.bytes() + box.la.bytes();
+  for (const auto& cs : box.cset) b += cs.coef.bytes() + cs.coef32.bytes() + cs.scoef.bytes() + cs.scoef32.bytes();
   b += j2_committed.bytes() + j2_trial.bytes() + j2_tan.bytes() + plastic_dev.bytes();
   return b;
 }

@@ -532,14 +532,14 @@ __global__ void __launch_bounds__(BX* BY, MINB)
 constexpr int kNumVariants = 9;  // see launch()
 
 template <class T>
-const BoxTable<typename Coef<T>::type>& table_of(const BoxPlan& p);
+const BoxTable<typename Coef<T>::type>& table_of(const BoxPlan& p, int mode);
 template <>
-const BoxTable<BoxCoef>& table_of<double>(const BoxPlan& p) {
-  return p.tab;
+const BoxTable<BoxCoef>& table_of<double>(const BoxPlan& p, int mode) {
+  return p.cset[mode].tab;
 }
 template <>
-const BoxTable<BoxCoef32>& table_of<float>(const BoxPlan& p) {
-  return p.tab32;
+const BoxTable<BoxCoef32>& table_of<float>(const BoxPlan& p, int mode) {
+  return p.cset[mode].tab32;
 }
 
 template <int BX, int BY, int MINB, bool CACHE, int CM, class T, int MODE>
@@ -561,9 +561,9 @@ void launch_shape(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     b.gz = static_cast<int>(grid.z);
     const int ntiles = b.gx * b.gy * b.gz;
     const int ctas = std::min(ntiles, resident * num_sms());
-    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p));
+    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p, MODE));
   } else {
-    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p));
+    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p, MODE));
   }
   FX_LAUNCH_CHECK("box_operator");
 }
@@ -608,7 +608,8 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
   std::vector<BoxCoef> h(static_cast<size_t>(s.nparams));
   std::vector<BoxCoef32> h32(static_cast<size_t>(s.nparams));
   BoxScaled sc0{};  // scaled grids: set 0's stiffness (per element times E_e / E_0) and its mass
-  for (int32_t i = 0; i < s.nparams; ++i) {
+  const int32_t nbuild = p.scaled ? 1 : s.nparams;  // a scaled grid needs set 0 only
+  for (int32_t i = 0; i < nbuild; ++i) {
     const ParamGP& q = s.params_h[i];
     double l2m, lam, mu;
     lame(q, l2m, lam, mu);
@@ -668,10 +669,11 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
     for (int d = 0; d < 3; ++d) f.body[d] = static_cast<float>(c.body[d]);
     f.pad_ = 0.f;
   }
+  BoxPlan::CoefSet& cs = p.cset[mode];
   if (p.layered)
     for (int32_t i = 0; i < s.nparams; ++i) {
-      p.tab.c[i] = h[i];
-      p.tab32.c[i] = h32[i];
+      cs.tab.c[i] = h[i];
+      cs.tab32.c[i] = h32[i];
     }
   if (p.scaled) {
     BoxScaled32 c32{};
@@ -683,24 +685,25 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
     for (int j = 0; j < 4; ++j) c32.more[j] = static_cast<float>(sc0.more[j]);
     for (int m = 0; m < 8; ++m) c32.dmm[m] = static_cast<float>(sc0.dmm[m]);
     for (int d = 0; d < 3; ++d) c32.body[d] = static_cast<float>(sc0.body[d]);
-    if (p.scoef.n != 1) p.scoef.alloc(1);
-    if (p.scoef32.n != 1) p.scoef32.alloc(1);
-    FX_CUDA(cudaMemcpy(p.scoef.ptr, &sc0, sizeof(sc0), cudaMemcpyHostToDevice));
-    FX_CUDA(cudaMemcpy(p.scoef32.ptr, &c32, sizeof(c32), cudaMemcpyHostToDevice));
+    if (cs.scoef.n != 1) cs.scoef.alloc(1);
+    if (cs.scoef32.n != 1) cs.scoef32.alloc(1);
+    FX_CUDA(cudaMemcpy(cs.scoef.ptr, &sc0, sizeof(sc0), cudaMemcpyHostToDevice));
+    FX_CUDA(cudaMemcpy(cs.scoef32.ptr, &c32, sizeof(c32), cudaMemcpyHostToDevice));
   }
   if (!p.scaled) {  // (a scaled grid reads its one table only)
-    if (p.coef.n != h.size()) p.coef.alloc(h.size());
-    if (p.coef32.n != h32.size()) p.coef32.alloc(h32.size());
-    FX_CUDA(cudaMemcpy(p.coef.ptr, h.data(), h.size() * sizeof(BoxCoef), cudaMemcpyHostToDevice));
-    FX_CUDA(cudaMemcpy(p.coef32.ptr, h32.data(), h32.size() * sizeof(BoxCoef32), cudaMemcpyHostToDevice));
+    if (cs.coef.n != h.size()) cs.coef.alloc(h.size());
+    if (cs.coef32.n != h32.size()) cs.coef32.alloc(h32.size());
+    FX_CUDA(cudaMemcpy(cs.coef.ptr, h.data(), h.size() * sizeof(BoxCoef), cudaMemcpyHostToDevice));
+    FX_CUDA(cudaMemcpy(cs.coef32.ptr, h32.data(), h32.size() * sizeof(BoxCoef32), cudaMemcpyHostToDevice));
   }
-  p.last_mode = mode;
-  for (int j = 0; j < 3; ++j) p.last_k[j] = k[j];
+  for (int j = 0; j < 3; ++j) cs.k[j] = k[j];
+  cs.built = true;
 }
 
 void ensure_coef(ForceState& s, int mode, const double k[3]) {
   const BoxPlan& p = s.box;
-  if (p.last_mode == mode && p.last_k[0] == k[0] && p.last_k[1] == k[1] && p.last_k[2] == k[2]) return;
+  const BoxPlan::CoefSet& cs = p.cset[mode];
+  if (cs.built && cs.k[0] == k[0] && cs.k[1] == k[1] && cs.k[2] == k[2]) return;
   build_coef(s, mode, k);
 }
 
@@ -831,7 +834,7 @@ void box_build_plan(ForceState& s) {
         p.layered = false;
         break;
       }
-    p.tab.layer[k] = p.tab32.layer[k] = static_cast<uint8_t>(first);
+    for (auto& cs : p.cset) cs.tab.layer[k] = cs.tab32.layer[k] = static_cast<uint8_t>(first);
   }
   // scaled: many sets that differ only in E (per-element moduli): one table, per-element scales
   p.scaled = false;
@@ -854,11 +857,15 @@ void box_build_plan(ForceState& s) {
       p.scaled = true;
     }
   }
-  // force form: lumped masses and one beta
+  // force form: one beta, and lumped masses or no mass-proportional damping (then f_int has no
+  // mass term and the mass type does not matter)
   const double beta0 = s.params_h[0].betaK + s.params_h[0].betaKinit + s.params_h[0].betaKcomm;
   bool one_beta = true;
   for (const auto& q : s.params_h) one_beta = one_beta && (q.betaK + q.betaKinit + q.betaKcomm) == beta0;
-  p.force_ok = all_lumped && one_beta;
+  bool no_alpha = s.nodal_alpha_h.empty() || std::all_of(s.nodal_alpha_h.begin(), s.nodal_alpha_h.end(),
+                                                           [](double m) { return m == 0.0; });
+  for (const auto& q : s.params_h) no_alpha = no_alpha && q.alphaM == 0.0;
+  p.force_ok = one_beta && (all_lumped || no_alpha);
   p.beta = beta0;
   if (p.force_ok) {
     // lumped alphaM masses per equation: alphaM_e rho_e J per element corner, then the nodal ones
@@ -885,12 +892,14 @@ void box_build_plan(ForceState& s) {
   p.grid_node_h = std::move(gnode);
   p.qualifies = true;
   p.why_not.clear();
-  p.last_mode = -1;
+  for (auto& cs : p.cset) cs.built = false;
 }
 
 // ------------------------------------------------------------------ operator entry points
 template <class T>
-static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const T* v, T* y) {
+static BoxArgs<T> args(const ForceState& s, int mode, const T* x, const T* v, T* y) {
+  const BoxPlan::CoefSet& cs = s.box.cset[mode];
+  const void* coef = sizeof(T) == 8 ? static_cast<const void*>(cs.coef.ptr) : static_cast<const void*>(cs.coef32.ptr);
   BoxArgs<T> a{};
   a.nx = s.box.nx;
   a.ny = s.box.ny;
@@ -902,10 +911,10 @@ static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const 
   a.coef = coef;
   if (s.box.scaled) {
     if constexpr (sizeof(T) == 8) {
-      a.coef = s.box.scoef.ptr;
+      a.coef = cs.scoef.ptr;
       a.escale = s.box.escale.ptr;
     } else {
-      a.coef = s.box.scoef32.ptr;
+      a.coef = cs.scoef32.ptr;
       a.escale = s.box.escale32.ptr;
     }
   }
@@ -918,7 +927,7 @@ static BoxArgs<T> args(const ForceState& s, const void* coef, const T* x, const 
 template <class T>
 static void apply_t(ForceState& s, const double k[3], const T* x, T* y, cudaStream_t st, const int* skip) {
   ensure_coef(s, 0, k);
-  BoxArgs<T> a = args<T>(s, sizeof(T) == 8 ? static_cast<const void*>(s.box.coef.ptr) : s.box.coef32.ptr, x, nullptr, y);
+  BoxArgs<T> a = args<T>(s, 0, x, nullptr, y);
   a.skip = skip;
   if (k[2] != 0.0 && s.has_nodal_mass) {
     a.nm1 = s.nodal_mass.ptr;
@@ -935,7 +944,7 @@ template <class T>
 static void force_t(ForceState& s, const T* u, const T* v, T* f, cudaStream_t st) {
   const double k1[3] = {1.0, 0.0, 0.0};
   ensure_coef(s, 1, k1);
-  BoxArgs<T> a = args<T>(s, sizeof(T) == 8 ? static_cast<const void*>(s.box.coef.ptr) : s.box.coef32.ptr, u, v, f);
+  BoxArgs<T> a = args<T>(s, 1, u, v, f);
   a.beta = static_cast<T>(s.box.beta);
   a.nm2 = s.box.la.ptr;
   launch<T, 1>(s.box, a, st);
@@ -948,11 +957,11 @@ void box_apply_f32(ForceState& s, const double k[3], const float* x, float* y, c
   apply_t<float>(s, k, x, y, st, skip);
 }
 void box_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
-  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs lumped masses and one beta");
+  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs one beta, and lumped masses or no mass-proportional damping");
   force_t<double>(s, u, v, f, st);
 }
 void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cudaStream_t st) {
-  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs lumped masses and one beta");
+  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs one beta, and lumped masses or no mass-proportional damping");
   force_t<float>(s, u, v, f, st);
 }
 
@@ -1048,8 +1057,7 @@ void batch_launch(const void* inst, const int4* work, int nwork, cudaStream_t st
 template <class T>
 void fill_args(ForceState& s, const double k[3], const void* x, void* y, const int* skip, void* dst) {
   ensure_coef(s, 0, k);
-  BoxArgs<T> a = args<T>(s, sizeof(T) == 8 ? static_cast<const void*>(s.box.coef.ptr) : s.box.coef32.ptr,
-                         static_cast<const T*>(x), nullptr, static_cast<T*>(y));
+  BoxArgs<T> a = args<T>(s, 0, static_cast<const T*>(x), nullptr, static_cast<T*>(y));
   a.kz = kBatchKz;
   a.skip = skip;
   if (k[2] != 0.0 && s.has_nodal_mass) {

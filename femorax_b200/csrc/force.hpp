@@ -75,9 +75,10 @@ struct BoxPlan {
   std::string why_not;
   int nx = 0, ny = 0, nz = 0;
   double h[3] = {0, 0, 0};
-  // The force (explicit) form runs here when every parameter set has the lumped mass and one
-  // stiffness-proportional damping factor beta (then f = K (u + beta v) - body + la v, la the
-  // lumped alphaM masses); otherwise the general path evaluates the force.
+  // The force (explicit) form runs here when every parameter set has one stiffness-proportional
+  // damping factor beta and either the lumped mass or no mass-proportional damping (then
+  // f = K (u + beta v) - body + la v, la the lumped alphaM masses, zero without alphaM);
+  // otherwise the general path evaluates the force.
   bool force_ok = false;
   double beta = 0.0;
   DeviceArray<double> la;  // [neq] lumped alphaM masses (element and nodal), force form
@@ -94,19 +95,23 @@ struct BoxPlan {
   } shape[2];
   DeviceArray<int> queue;    // [next tile, CTAs done], zero between launches
   bool tuned = false;
-  // coefficient tables for the last operator coefficients
-  DeviceArray<BoxCoef> coef;
-  DeviceArray<BoxCoef32> coef32;
   bool layered = false;  // one parameter set per element plane (kernel-parameter tables)
   bool scaled = false;   // the sets differ only in E: one table and a per-element scale
   DeviceArray<double> escale;   // [nz ny nx]: E_e / E_ref
   DeviceArray<float> escale32;
-  DeviceArray<BoxScaled> scoef;
-  DeviceArray<BoxScaled32> scoef32;
-  BoxTable<BoxCoef> tab{};
-  BoxTable<BoxCoef32> tab32{};
-  double last_k[4] = {-1, -1, -1, -1};
-  int last_mode = -1;
+  // The coefficient tables of one kernel mode (0: the operator for the last operator
+  // coefficients k, 1: the internal force), each kept until its coefficients change, so that a
+  // solve that alternates forces and operator applies builds them once.
+  struct CoefSet {
+    DeviceArray<BoxCoef> coef;  // per parameter set (neither layered nor scaled)
+    DeviceArray<BoxCoef32> coef32;
+    BoxTable<BoxCoef> tab{};    // layered
+    BoxTable<BoxCoef32> tab32{};
+    DeviceArray<BoxScaled> scoef;  // scaled
+    DeviceArray<BoxScaled32> scoef32;
+    double k[3] = {0, 0, 0};
+    bool built = false;
+  } cset[2];
 };
 
 // Buffers of the explicit step loop (ground motion, step counter, force, recorded history),
