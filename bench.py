@@ -14,6 +14,7 @@ ids) + 12 N (node -> equations) + 4 n_el (parameter index). `cpu_baseline` times
 own InternalForce::apply_operator (built here from its sources, oracle/_ref) on a bounded sample.
 
 `explicit` times the explicit wave configuration's stepping (FP64 and FP32, 4000 steps);
+`newmark` compares the Newmark stage with plain FP64 and mixed-precision inner solves;
 `batched_j2` compares the batched J2 Newton with one instance at a time on a bounded sample;
 `served` compares solves/s and p50/p99 latency at a 1e-8 FP64 residual on a stream of static solves:
 the batched mixed-precision engine behind the serving loop versus plain FP64 CG one at a time.
@@ -172,6 +173,41 @@ def explicit_comparison(force, mesh, comp, device, steps=4000):
         out[f"steps_per_s_{name}"] = steps / (e0.elapsed_time(e1) * 1e-3)
     peak = float(np.max(np.abs(hist["f64"])))
     out["f32_history_max_abs_diff_over_peak"] = float(np.max(np.abs(hist["f32"] - hist["f64"]))) / peak
+    return out
+
+
+def newmark_comparison(device, n=48, steps=40, seed=0):
+    """The Newmark configuration on a bounded sample: a heterogeneous cube of n^3 boxes (per-element
+    E log-normal, median 80 MPa, sigma 0.5; nu 0.3; base fixed), a harmonic horizontal surface load,
+    Newmark beta 0.25 gamma 0.5 with one inner solve per step to a 1e-8 relative FP64 residual:
+    plain FP64 CG against FP32 CG inside FP64 refinement. Steps/s by wall clock around each run
+    (after a 2-step warm-up of each); the monitored top displacement histories compared."""
+    import math
+
+    import torch
+    import femorax_b200 as fx
+    from femorax_b200 import meshes, serving, stages
+    spec = meshes.heterogeneous_cube(n, seed=seed, size=0.5 * n)
+    comp = fx.Model(spec).compile()
+    mesh = comp.mesh()
+    force = fx.InternalForce(mesh, device=device)
+    f, mon = stages.top_shear(spec, serving.equation_map(comp), 1e6)
+    ft = torch.as_tensor(f, device=torch.device("cuda", device))
+
+    def load(t):
+        return ft * math.sin(2 * math.pi * 5.0 * t)
+
+    out = {"mesh": f"heterogeneous cube {n}^3, {mesh.num_equations} equations", "steps": steps, "dt_s": 2e-3}
+    runs = {}
+    for mixed in (False, True):
+        stages.newmark_run(force, load, 2, 2e-3, mon, mixed=mixed, rtol=1e-8)
+        runs[mixed] = stages.newmark_run(force, load, steps, 2e-3, mon, mixed=mixed, rtol=1e-8)
+    out["plain_fp64_steps_per_s"] = steps / runs[False].seconds
+    out["mixed_steps_per_s"] = steps / runs[True].seconds
+    out["speedup"] = runs[False].seconds / runs[True].seconds
+    peak = float(np.max(np.abs(runs[False].monitor)))
+    out["mixed_vs_plain_max_abs_diff_over_peak"] = float(np.max(np.abs(runs[True].monitor - runs[False].monitor))) / peak
+    out["converged"] = bool(runs[False].converged and runs[True].converged)
     return out
 
 
@@ -375,6 +411,7 @@ def run_ours(args):
     explicit = explicit_comparison(force, mesh, comp, local) if world == 1 and not args.no_serve else None
     served = serve_comparison(local) if world == 1 and not args.no_serve else None
     batched_j2 = batched_j2_comparison(local) if world == 1 and not args.no_serve else None
+    newmark = newmark_comparison(local) if world == 1 and not args.no_serve else None
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -393,7 +430,8 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "explicit": explicit,
             "served": served,
-            "batched_j2": batched_j2}
+            "batched_j2": batched_j2,
+            "newmark": newmark}
     print(json.dumps(line))
     return 0
 
