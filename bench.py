@@ -43,6 +43,23 @@ WORKLOAD = dict(workload="layered soil box 128x128x64 stdBrick (8 layers, seed 0
 METRIC = "K*x GDoF/s (plain FP64 matrix-free apply, layered box 128x128x64)"
 
 
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Each value's maximum over the ranks of the process group (the slowest rank's time); the
+    values themselves without a group."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_value(world, neq, steps, total_ms):
+    """GDoF/s of `world` independent replicas, each applying its own operator of neq equations
+    `steps` times, the slowest taking total_ms in all."""
+    return world * neq * steps / (total_ms * 1e-3) / 1e9
+
+
 def algorithmic_bytes(neq, n_el, n_nodes):
     return 8 * neq + 8 * neq + 32 * n_el + 12 * n_nodes + 4 * n_el
 
@@ -375,11 +392,8 @@ def run_ours(args):
     clocks.stop()
     ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = sum(ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * neq * args.steps / (total_ms * 1e-3) / 1e9
+    total_ms = max_over_ranks([total_ms], dist, dev)[0]
+    value = replica_value(world, neq, args.steps, total_ms)
 
     # e2e: the public host-buffer call, copies included
     xh = torch.empty(neq, dtype=torch.float64, pin_memory=True)
@@ -393,10 +407,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         force.apply_operator_host(k, xn, yn, stream)
         e_ms.append((time.perf_counter() - t0) * 1e3)
-    te = torch.tensor([sum(e_ms)], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e = world * neq * args.steps / (float(te.item()) * 1e-3) / 1e9
+    e2e = replica_value(world, neq, args.steps, max_over_ranks([sum(e_ms)], dist, dev)[0])
 
     peak, peak_kind = load_peaks()
     alg = algorithmic_bytes(neq, n_el, n_nodes)
