@@ -19,7 +19,7 @@ from .meshes import ModelSpec
 
 __all__ = ["Model", "Compiled", "MeshArrays", "InternalForce", "OperatorCoefficients", "MatrixFreeOperator",
            "SolveOptions", "SolveResult", "LinearSolver", "ConjugateGradient", "Gmres", "KrylovSolver",
-           "MixedPrecisionSolver", "BatchEngine", "BatchedNewton", "VectorOps", "FxError", "ModelSpec"]
+           "MixedPrecisionSolver", "BatchEngine", "BatchedNewton", "VectorOps", "GroundMotions", "FxError", "ModelSpec"]
 
 
 def _i32(a):
@@ -326,12 +326,76 @@ class InternalForce:
             return hist[:steps].cpu().numpy()
         return None
 
+    def explicit_stage(self, scheme, mass, u, v, a, dt, steps, time=0.0, motions=None, alpha_mass=None,
+                       resume=False, record_eq=None, stream=None):
+        """An explicit stage (explicit_analysis.cpp:665-725): `steps` steps of "ExplicitDifference"
+        or "CentralDifference" from `time` with the ground motions of `motions` (a GroundMotions,
+        evaluated on the device each step); u, v, a (device FP64) are the committed state in and
+        the end state out; alpha_mass is Compiled::lumped_alpha_mass (CentralDifference's damping
+        diagonal). resume continues the previous call. Returns (end time, recorded acceleration
+        history of record_eq or None)."""
+        sc = {"ExplicitDifference": 1, "CentralDifference": 0}[scheme]
+        check(lib().fx_explicit_record(self._h, -1 if record_eq is None else int(record_eq), None, 0))
+        t = C.c_double(time)
+        check(lib().fx_explicit_stage(self._h, sc, _ptr(mass), None if alpha_mass is None else _ptr(alpha_mass),
+                                      None if motions is None else motions._h, steps, dt, C.byref(t), _ptr(u), _ptr(v),
+                                      _ptr(a), 1 if resume else 0, _stream(stream)))
+        hist = None
+        if record_eq is not None:
+            import torch
+            h = torch.zeros(steps + 1, dtype=torch.float64, device=u.device)
+            check(lib().fx_explicit_record(self._h, int(record_eq), _ptr(h), steps))
+            hist = h[:steps].cpu().numpy()
+        return t.value, hist
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
             try:
                 lib().fx_force_destroy(h)
             except Exception:  # interpreter shutdown: the library may be gone already
+                pass
+            self._h = None
+
+
+class GroundMotions:
+    """exec::GroundMotions (src/exec/ground_motion.hpp:22-70): UniformExcitation patterns with
+    Path series, evaluated on the device. add(): one pattern in DOF `dof` (0-based) with factor
+    `fact`; its series is `values` with a uniform spacing `dt` (PathSeries) or at `times`
+    (PathTimeSeries), scaled by `factor`."""
+
+    def __init__(self, patterns=()):
+        h = C.c_void_p()
+        check(lib().fx_motions_create(C.byref(h)))
+        self._h = h
+        self.count = 0
+        for p in patterns:
+            self.add(**p)
+
+    def add(self, dof, fact, values, dt=None, times=None, factor=1.0, use_last=False, prepend_zero=False):
+        v = np.ascontiguousarray(values, np.float64)
+        tp = None
+        if times is not None:
+            tm = np.ascontiguousarray(times, np.float64)
+            if tm.size != v.size:
+                raise ValueError("times and values differ in length")
+            tp = tm.ctypes.data_as(L.p_f64)
+        check(lib().fx_motions_add(self._h, int(dof), float(fact), v.ctypes.data_as(L.p_f64), tp, v.size,
+                                   0.0 if dt is None else float(dt), float(factor), int(bool(use_last)),
+                                   int(bool(prepend_zero))))
+        self.count += 1
+
+    def evaluate(self, t):
+        out = np.zeros(max(self.count, 1))
+        check(lib().fx_motions_evaluate(self._h, float(t), out.ctypes.data_as(L.p_f64)))
+        return out[:self.count]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().fx_motions_destroy(h)
+            except Exception:
                 pass
             self._h = None
 

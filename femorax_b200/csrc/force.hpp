@@ -123,6 +123,10 @@ struct ExplicitWork {
   DeviceArray<float> f32;
   DeviceArray<double> hist;
   int32_t record_eq = -1;
+  // explicit stages: the half-step velocity (ExplicitDifference) or the previous displacement
+  // (CentralDifference) carried between calls, the element velocity, the stage time
+  DeviceArray<double> carry, v_elem, time;
+  int carry_scheme = -1;
 };
 
 struct ForceState {

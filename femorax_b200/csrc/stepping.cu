@@ -59,6 +59,161 @@ __global__ void k_ed_correct_predict(const T* __restrict__ f, const T* __restric
 
 __global__ void k_step_advance(int* step) { ++*step; }
 
+// ---- explicit stages with device ground motions
+// Every operation of these kernels is an explicitly rounded IEEE operation (no contraction into
+// fused multiply-adds), in the reference's order, so a stage on the bit-exact general path gives
+// the reference's host bits.
+struct MotionPattern {
+  int32_t dof, uniform, use_last, pad_;
+  int64_t n, off;  // samples, offset into the values (and times) arrays
+  double fact, dt, factor;
+};
+
+// PathSeries::getFactor with a uniform spacing (src/exec/ground_motion.cpp:21-39), start 0
+__device__ double path_uniform(const double* v, int64_t n, double dt, double factor, int use_last, double t) {
+  if (t < 0.0) return 0.0;
+  const double incr = __ddiv_rn(t, dt);
+  // floor(incr) + 1 >= n, tested before the conversion (which could overflow for huge t / dt)
+  if (!(incr < static_cast<double>(n - 1))) return use_last ? __dmul_rn(factor, v[n - 1]) : 0.0;
+  const long long i1 = static_cast<long long>(floor(incr));
+  const double v1 = v[i1], v2 = v[i1 + 1];
+  return __dmul_rn(factor, __dadd_rn(v1, __dmul_rn(__dsub_rn(v2, v1), __dsub_rn(incr, static_cast<double>(i1)))));
+}
+
+// PathTimeSeries::getFactor (ground_motion.cpp:41-77): the interval walk from *loc, kept
+__device__ double path_time(const double* v, const double* tm, int64_t n, double factor, int* loc, double t) {
+  int l = *loc;
+  double t1 = tm[l];
+  if (t < t1 && l == 0) return 0.0;
+  if (t == t1) return __dmul_rn(factor, v[l]);
+  const int last = static_cast<int>(n) - 1;
+  if (t > t1 && l == last) return 0.0;
+  double t2 = tm[l + 1];
+  if (t > t2) {
+    while (t > t2 && l < last - 1) {
+      ++l;
+      t1 = t2;
+      t2 = tm[l + 1];
+    }
+    *loc = l;
+    if (t > t2) return 0.0;
+  } else if (t < t1) {
+    while (t < t1 && l > 0) {
+      --l;
+      t2 = t1;
+      t1 = tm[l];
+    }
+    *loc = l;
+    if (t < t1) return 0.0;
+  }
+  const double v1 = v[l], v2 = v[l + 1];
+  return __dmul_rn(factor, __dadd_rn(v1, __ddiv_rn(__dmul_rn(__dsub_rn(v2, v1), __dsub_rn(t, t1)), __dsub_rn(t2, t1))));
+}
+
+// One thread: the stage's step counter and time, and every pattern's ground acceleration at the
+// step's load time (GroundMotions::evaluate, ground_motion.cpp:150-175). ExplicitDifference
+// evaluates after time += dt, CentralDifference before it (explicit_analysis.cpp:700-721).
+// dt == 0: evaluate at *time only (no step).
+__global__ void k_motions(const MotionPattern* __restrict__ pats, int npat, const double* __restrict__ values,
+                          const double* __restrict__ times, int* __restrict__ loc, double* __restrict__ accel,
+                          double* __restrict__ time, int* __restrict__ step, double dt, int advance_first) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (step) ++*step;
+  if (advance_first) *time = __dadd_rn(*time, dt);
+  const double t = *time;
+  for (int p = 0; p < npat; ++p) {
+    const MotionPattern& m = pats[p];
+    double g = 0.0;  // GroundMotion::getAccel: 0 for t < 0
+    if (t >= 0.0) {
+      if (m.uniform) g = path_uniform(values + m.off, m.n, m.dt, m.factor, m.use_last, t);
+      else g = path_time(values + m.off, times + m.off, m.n, m.factor, &loc[p], t);
+    }
+    accel[p] = __dmul_rn(m.fact, g);  // UniformExcitation: R = fact in its DOF
+  }
+  if (!advance_first && dt != 0.0) *time = __dadd_rn(*time, dt);
+}
+
+// ground_load (explicit_analysis.cpp:51-58)
+__device__ __forceinline__ double ground_load(double mq, int dof_q, const double* accel, const int* gdof, int npat) {
+  double r = 0.0;
+  for (int p = 0; p < npat; ++p)
+    if (gdof[p] == dof_q) r = __dsub_rn(r, __dmul_rn(mq, accel[p]));
+  return r;
+}
+
+// ed_predict (explicit_analysis.cpp:62-69)
+__global__ void k_stage_ed_predict(double* __restrict__ u, double* __restrict__ vh, const double* __restrict__ a,
+                                   double dt, int64_t n) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = __dadd_rn(vh[q], __dmul_rn(a[q], dt));
+    vh[q] = v;
+    u[q] = __dadd_rn(u[q], __dmul_rn(v, dt));
+  }
+}
+
+// ed_correct (explicit_analysis.cpp:71-84), then the next step's ed_predict when `predict`
+__global__ void k_stage_ed_correct(const double* __restrict__ f, const double* __restrict__ m,
+                                   const int8_t* __restrict__ dof, const double* __restrict__ accel,
+                                   const int* __restrict__ gdof, int npat, double dt, double* __restrict__ u,
+                                   double* __restrict__ vh, double* __restrict__ a, double* __restrict__ v,
+                                   int64_t n, const int* __restrict__ step, int32_t record_eq,
+                                   double* __restrict__ hist, int predict) {
+  const double halfT = __dmul_rn(dt, 0.125);
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double mq = m[q];
+    const double R = __dadd_rn(-f[q], ground_load(mq, dof[q], accel, gdof, npat));
+    const double an = __ddiv_rn(R, mq);
+    const double t = __dadd_rn(__dmul_rn(3.0, an), a[q]);
+    const double vhq = vh[q];
+    v[q] = __dadd_rn(vhq, __dmul_rn(t, halfT));
+    a[q] = an;
+    if (q == record_eq && hist) hist[*step] = an;
+    if (predict) {
+      const double vn = __dadd_rn(vhq, __dmul_rn(an, dt));
+      vh[q] = vn;
+      u[q] = __dadd_rn(u[q], __dmul_rn(vn, dt));
+    }
+  }
+}
+
+// cd_garbage_velocity (explicit_analysis.cpp:86-92)
+__global__ void k_stage_cd_garbage(double* __restrict__ ve, const double* __restrict__ um, double c2, int64_t n) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    ve[q] = __dmul_rn(um[q], -c2);
+}
+
+// cd_solve (explicit_analysis.cpp:94-117), then the next step's garbage velocity -c2 um
+__global__ void k_stage_cd_solve(const double* __restrict__ f, const double* __restrict__ m,
+                                 const double* __restrict__ cm, const int8_t* __restrict__ dof,
+                                 const double* __restrict__ accel, const int* __restrict__ gdof, int npat, double c2,
+                                 double c3, double dt, double* __restrict__ u, double* __restrict__ um,
+                                 double* __restrict__ v, double* __restrict__ a, double* __restrict__ ve, int64_t n,
+                                 const int* __restrict__ step, int32_t record_eq, double* __restrict__ hist,
+                                 int next) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double uq = u[q], umq = um[q], mq = m[q];
+    const double ag = __dadd_rn(__dmul_rn(uq, __dmul_rn(-2.0, c3)), __dmul_rn(umq, c3));
+    const double R = __dadd_rn(__dsub_rn(-f[q], __dmul_rn(mq, ag)), ground_load(mq, dof[q], accel, gdof, npat));
+    const double A = __dadd_rn(__dmul_rn(mq, c3), __dmul_rn(cm ? cm[q] : 0.0, c2));
+    const double U = __ddiv_rn(R, A);
+    double Ud = __dmul_rn(U, 3.0);
+    Ud = __dadd_rn(Ud, __dmul_rn(uq, -4.0));
+    Ud = __dadd_rn(Ud, umq);
+    Ud = __dmul_rn(Ud, c2);
+    const double Udd = __ddiv_rn(__dsub_rn(Ud, v[q]), dt);
+    um[q] = uq;
+    u[q] = U;
+    v[q] = Ud;
+    a[q] = Udd;
+    if (q == record_eq && hist) hist[*step] = Udd;
+    if (next) ve[q] = __dmul_rn(uq, -c2);
+  }
+}
+
 __global__ void k_newmark_predict(double* __restrict__ u, double* __restrict__ v, double* __restrict__ a,
                                   double* __restrict__ ut, double* __restrict__ vt, double* __restrict__ at, double a1,
                                   double a2, double a3, double a4, int64_t n) {
@@ -283,7 +438,204 @@ void explicit_run(fx_force* f, const T* mass, int32_t dir, const double* ag_host
 }
 }  // namespace
 
+// UniformExcitation patterns with their series, on the device (exec::GroundMotions).
+struct fx_motions {
+  int device = 0;
+  std::vector<fx::MotionPattern> pats;
+  std::vector<double> values, times;
+  fx::DeviceArray<fx::MotionPattern> d_pats;
+  fx::DeviceArray<double> d_values, d_times, d_accel, d_time;
+  fx::DeviceArray<int> d_dof, d_loc;
+  bool uploaded = false;
+
+  void upload() {
+    if (uploaded) return;
+    d_pats.upload(pats);
+    d_values.upload(values.empty() ? std::vector<double>(1, 0.0) : values);
+    d_times.upload(times.empty() ? std::vector<double>(1, 0.0) : times);
+    std::vector<int> dof;
+    for (const auto& p : pats) dof.push_back(p.dof);
+    d_dof.upload(dof.empty() ? std::vector<int>(1, -1) : dof);
+    d_loc.upload(std::vector<int>(std::max<size_t>(pats.size(), 1), 0));
+    d_accel.upload(std::vector<double>(std::max<size_t>(pats.size(), 1), 0.0));
+    d_time.upload(std::vector<double>(1, 0.0));
+    uploaded = true;
+  }
+};
+
+namespace {
+
+// An explicit stage (src/exec/explicit_analysis.cpp:665-725 without local time stepping, exact
+// constraints, DRM or recorders). Per ExplicitDifference step: [motions: time += dt, ag(time)]
+// [force at (u, vh)] [ed_correct + the next ed_predict] [commit]; per CentralDifference step:
+// [motions: ag(time), time += dt] [force at (u, -c2 um)] [cd_solve + the next garbage velocity]
+// [commit]. The steps after the first run as CUDA graphs of 16.
+void explicit_stage(fx_force* f, int scheme, const double* mass, const double* cm, fx_motions* mo, int32_t steps,
+                    double dt, double* time, double* u, double* v, double* a, int resume, cudaStream_t st) {
+  using namespace fx;
+  ForceState& s = f->s;
+  if (scheme != 0 && scheme != 1) throw Error(FX_E_INVALID, "fx_explicit_stage: scheme must be 0 (CD) or 1 (ED)");
+  if (steps < 0 || !(dt > 0.0) || !time) throw Error(FX_E_INVALID, "fx_explicit_stage: steps >= 0, dt > 0 and time required");
+  ExplicitWork& w = work_of(f);
+  if (resume && w.carry_scheme != scheme) throw Error(FX_E_INVALID, "fx_explicit_stage: nothing to resume for this scheme");
+  const int64_t n = s.neq;
+  const size_t nn = static_cast<size_t>(std::max<int64_t>(n, 1));
+  if (w.carry.n < nn) w.carry.alloc(nn);
+  if (w.v_elem.n < nn) w.v_elem.alloc(nn);
+  if (w.f64.n < nn) w.f64.alloc(nn);
+  if (w.step.n == 0) w.step.alloc(1);
+  if (w.time.n == 0) w.time.alloc(1);
+  if (w.record_eq >= 0 && w.hist.n < static_cast<size_t>(steps) + 1) w.hist.alloc(static_cast<size_t>(steps) + 1);
+  fx_motions none;
+  fx_motions* m = mo ? mo : &none;
+  m->upload();
+  const int npat = static_cast<int>(m->pats.size());
+  const double c2 = 0.5 / dt, c3 = 1.0 / (dt * dt);
+  double* carry = w.carry.ptr;  // ED: the half-step velocity; CD: the previous displacement
+  double* ve = scheme == 1 ? carry : w.v_elem.ptr;
+  FX_CUDA(cudaMemcpyAsync(w.time.ptr, time, sizeof(double), cudaMemcpyHostToDevice, st));
+  const int minus_one = -1;
+  FX_CUDA(cudaMemcpyAsync(w.step.ptr, &minus_one, sizeof(int), cudaMemcpyHostToDevice, st));
+  if (!resume && n > 0) {  // domainChanged: ED starts vh from the committed velocity, CD takes Utm1 = Ut
+    FX_CUDA(cudaMemcpyAsync(carry, scheme == 1 ? v : u, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  }
+  w.carry_scheme = scheme;
+  if (steps == 0) {
+    FX_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  if (n > 0) {
+    if (scheme == 1) k_stage_ed_predict<<<ew(n), 256, 0, st>>>(u, carry, a, dt, n);
+    else k_stage_cd_garbage<<<ew(n), 256, 0, st>>>(ve, carry, c2, n);
+    FX_LAUNCH_CHECK("explicit_stage_begin");
+  }
+  double* fbuf = w.f64.ptr;
+  auto one_step = [&](int more) {
+    k_motions<<<1, 32, 0, st>>>(m->d_pats.ptr, npat, m->d_values.ptr, m->d_times.ptr, m->d_loc.ptr, m->d_accel.ptr,
+                                w.time.ptr, w.step.ptr, dt, scheme == 1);
+    if (n > 0) {
+      if (s.use_box_force()) box_force(s, u, ve, fbuf, st);
+      else general_force(s, u, ve, fbuf, st);
+      if (scheme == 1)
+        k_stage_ed_correct<<<ew(n), 256, 0, st>>>(fbuf, mass, s.eq_dof.ptr, m->d_accel.ptr, m->d_dof.ptr, npat, dt, u,
+                                                  carry, a, v, n, w.step.ptr, w.record_eq, w.hist.ptr, more);
+      else
+        k_stage_cd_solve<<<ew(n), 256, 0, st>>>(fbuf, mass, cm, s.eq_dof.ptr, m->d_accel.ptr, m->d_dof.ptr, npat, c2,
+                                                c3, dt, u, carry, v, a, ve, n, w.step.ptr, w.record_eq, w.hist.ptr,
+                                                more);
+    }
+    FX_LAUNCH_CHECK("explicit_stage_step");
+    if (s.has_j2)  // Domain::commit after every step
+      FX_CUDA(cudaMemcpyAsync(s.j2_committed.ptr, s.j2_trial.ptr, s.j2_committed.bytes(), cudaMemcpyDeviceToDevice, st));
+  };
+  // The last step does no prediction: u, v, a are the stage's end state; a resumed call
+  // starts with the prediction (ED) or the garbage velocity (CD) from the carried vector.
+  const int block = 16;
+  int done = 0;
+  one_step(steps > 1);
+  ++done;
+  cudaStream_t cs = st;
+  bool own_stream = false;
+  if (cs == nullptr) {  // the legacy stream cannot be captured: run the graph on a private stream
+    FX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    own_stream = true;
+    cudaEvent_t e;
+    FX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    FX_CUDA(cudaEventRecord(e, st));
+    FX_CUDA(cudaStreamWaitEvent(cs, e, 0));
+    cudaEventDestroy(e);
+  }
+  st = cs;
+  cudaGraphExec_t exec = nullptr;
+  while (done < steps) {
+    if (steps - done > block) {
+      if (!exec) {
+        cudaGraph_t g = nullptr;
+        FX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < block; ++i) one_step(1);
+        FX_CUDA(cudaStreamEndCapture(st, &g));
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        FX_CUDA(e);
+      }
+      FX_CUDA(cudaGraphLaunch(exec, st));
+      done += block;
+    } else {
+      one_step(steps - done > 1);
+      ++done;
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  FX_CUDA(cudaMemcpyAsync(time, w.time.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+  FX_CUDA(cudaStreamSynchronize(st));
+  if (own_stream) cudaStreamDestroy(cs);
+}
+}  // namespace
+
 extern "C" {
+
+int fx_motions_create(fx_motions** out) {
+  return guard([&] {
+    if (!out) throw fx::Error(FX_E_INVALID, "fx_motions_create: null output");
+    auto m = std::make_unique<fx_motions>();
+    FX_CUDA(cudaGetDevice(&m->device));
+    *out = m.release();
+  });
+}
+
+int fx_motions_destroy(fx_motions* m) {
+  delete m;
+  return FX_OK;
+}
+
+int fx_motions_add(fx_motions* m, int32_t dof, double fact, const double* values, const double* times, int32_t n,
+                   double dt, double factor, int32_t use_last, int32_t prepend_zero) {
+  return guard([&] {
+    if (!m || !values || n < 1 || dof < 0 || dof > 2) throw fx::Error(FX_E_INVALID, "fx_motions_add: bad arguments");
+    if (!times && !(dt > 0.0)) throw fx::Error(FX_E_INVALID, "fx_motions_add: a uniform series needs dt > 0");
+    if (times && n < 2) throw fx::Error(FX_E_INVALID, "fx_motions_add: a time series needs two samples");
+    fx::MotionPattern p{};
+    p.dof = dof;
+    p.uniform = times ? 0 : 1;
+    p.use_last = use_last ? 1 : 0;
+    p.fact = fact;
+    p.dt = dt;
+    p.factor = factor;
+    // values and times run in parallel (a uniform series' times stay 0)
+    p.off = static_cast<int64_t>(m->values.size());
+    // PathSeries' constructor puts a zero first when asked (ground_motion.cpp:88)
+    if (!times && prepend_zero) m->values.push_back(0.0);
+    m->values.insert(m->values.end(), values, values + n);
+    p.n = static_cast<int64_t>(m->values.size()) - p.off;
+    if (times) m->times.insert(m->times.end(), times, times + n);
+    m->times.resize(m->values.size(), 0.0);
+    m->pats.push_back(p);
+    m->uploaded = false;
+  });
+}
+
+int fx_motions_evaluate(fx_motions* m, double t, double* accel) {
+  return guard([&] {
+    if (!m || (!accel && !m->pats.empty())) throw fx::Error(FX_E_INVALID, "fx_motions_evaluate: bad arguments");
+    m->upload();
+    FX_CUDA(cudaMemcpy(m->d_time.ptr, &t, sizeof(double), cudaMemcpyHostToDevice));
+    fx::k_motions<<<1, 32>>>(m->d_pats.ptr, static_cast<int>(m->pats.size()), m->d_values.ptr, m->d_times.ptr,
+                             m->d_loc.ptr, m->d_accel.ptr, m->d_time.ptr, nullptr, 0.0, 0);
+    FX_LAUNCH_CHECK("motions_evaluate");
+    if (!m->pats.empty())
+      FX_CUDA(cudaMemcpy(accel, m->d_accel.ptr, sizeof(double) * m->pats.size(), cudaMemcpyDeviceToHost));
+  });
+}
+
+int fx_explicit_stage(fx_force* f, int32_t scheme, const double* mass, const double* alpha_mass, fx_motions* motions,
+                      int32_t steps, double dt, double* time, double* u, double* v, double* a, int32_t resume,
+                      void* stream) {
+  return guard([&] {
+    if (!f || (f->s.neq > 0 && (!mass || !u || !v || !a))) throw fx::Error(FX_E_INVALID, "fx_explicit_stage: bad arguments");
+    explicit_stage(f, scheme, mass, alpha_mass, motions, steps, dt, time, u, v, a, resume,
+                   static_cast<cudaStream_t>(stream));
+  });
+}
 
 int fx_explicit_run(fx_force* f, const double* mass, int32_t dir, const double* ag_host, int32_t steps, double dt,
                     double* u, double* vh, double* a, double* v, void* stream) {

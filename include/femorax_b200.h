@@ -318,6 +318,36 @@ int fx_explicit_run_f32(fx_force* f, const float* mass, int32_t dir, const doubl
  * (hist_dev[step] = a[eq] after step `step`) to hist_dev (device, at least `count` doubles). */
 int fx_explicit_record(fx_force* f, int32_t eq, double* hist_dev, int32_t count);
 
+/* Ground motions on the device (exec::GroundMotions, src/exec/ground_motion.hpp:22-70,
+ * ground_motion.cpp:64-175): UniformExcitation patterns, each with its own Path series.
+ * fx_motions_add: pattern acting in DOF dof (0-based) with factor fact; the series has n values
+ * and either a uniform spacing dt (times NULL; OpenSees PathSeries, prepend_zero puts a zero
+ * first, use_last holds the last value after the end) or times[n] (PathTimeSeries); factor is
+ * the series' cFactor. fx_motions_evaluate: accel_host[p] = fact_p * series_p(t) for every
+ * pattern, evaluated on the device (a time series keeps its interval between calls, as the
+ * reference's does). */
+typedef struct fx_motions fx_motions;
+int fx_motions_create(fx_motions** out);
+int fx_motions_destroy(fx_motions* m);
+int fx_motions_add(fx_motions* m, int32_t dof, double fact, const double* values, const double* times, int32_t n,
+                   double dt, double factor, int32_t use_last, int32_t prepend_zero);
+int fx_motions_evaluate(fx_motions* m, double t, double* accel_host);
+
+/* An explicit analysis stage (src/exec/explicit_analysis.cpp:665-725; no local time stepping,
+ * exact constraints, DRM or recorders): `steps` steps of dt from *time with scheme 1
+ * ExplicitDifference (ed_predict / ed_correct, :62-84) or 0 CentralDifference
+ * (cd_garbage_velocity / cd_solve, :86-117, alpha_mass = Compiled::lumped_alpha_mass), the
+ * ground accelerations of `motions` (NULL: none) evaluated on the device at each step's load
+ * time, the material state committed after every step. u, v, a (device FP64) hold the
+ * committed displacement, velocity and acceleration and receive the stage's end state; *time
+ * (host) receives the end time. resume = 0 starts a stage (ED: half-step velocity = v; CD:
+ * previous displacement = u); resume = 1 continues the previous call of the same scheme, so that
+ * a stage run in pieces equals one call. fx_explicit_record's equation is recorded (the
+ * acceleration after each step). */
+int fx_explicit_stage(fx_force* f, int32_t scheme, const double* mass, const double* alpha_mass, fx_motions* motions,
+                      int32_t steps, double dt, double* time, double* u, double* v, double* a, int32_t resume,
+                      void* stream);
+
 /* Newmark form D kernels (src/exec/implicit_stage.cpp:29-68). */
 int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
                        double a2, double a3, double a4, void* stream);

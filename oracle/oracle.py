@@ -52,6 +52,11 @@ def ref():
         L.fxref_model_add_equal_dof.argtypes = [vp, C.c_int32, p_i32, p_i32, p_i32]
         L.fxref_model_add_rayleigh.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, p_i32]
         L.fxref_model_add_mass.argtypes = [vp, C.c_int32, p_i32, p_i32, p_f64]
+        L.fxref_motions_create.restype = vp
+        L.fxref_motions_destroy.argtypes = [vp]
+        L.fxref_motions_add.argtypes = [vp, C.c_int32, C.c_double, p_f64, p_f64, C.c_int32, C.c_double, C.c_double,
+                                        C.c_int32, C.c_int32]
+        L.fxref_motions_evaluate.argtypes = [vp, C.c_double, p_f64]
         L.fxref_compile.restype = vp
         L.fxref_compile.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.fxref_compiled_destroy.argtypes = [vp]
@@ -290,6 +295,14 @@ def port():
         L.fxo_newmark_update.argtypes = [C.c_int64, p_f64, p_f64, p_f64, p_f64, C.c_double, C.c_double]
         L.fxo_j2_update.restype = C.c_int
         L.fxo_j2_update.argtypes = [C.c_double] * 5 + [p_f64, p_f64, p_f64, p_f64, p_f64]
+        L.fxo_path_uniform.restype = C.c_double
+        L.fxo_path_uniform.argtypes = [p_f64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double]
+        L.fxo_path_time.restype = C.c_double
+        L.fxo_path_time.argtypes = [p_f64, p_f64, C.c_int64, C.c_double, C.POINTER(C.c_int), C.c_double]
+        L.fxo_ed_stage_step.argtypes = [M, p_f64, p_i8, p_f64, p_i32, C.c_int, C.c_double, p_f64, p_f64, p_f64, p_f64,
+                                        p_f64]
+        L.fxo_cd_stage_step.argtypes = [M, p_f64, p_f64, p_i8, p_f64, p_i32, C.c_int, C.c_double, p_f64, p_f64, p_f64,
+                                        p_f64, p_f64, p_f64]
         _port = L
     return _port
 
@@ -413,6 +426,44 @@ class PortMesh:
         return x, dict(converged=bool(r[0]), iterations=int(r[1]), rhs_norm=r[2], initial_residual=r[3],
                        final_residual=r[4])
 
+    def stage(self, scheme, mass, cm, eq_dof, patterns, dt, steps, time=0.0, u=None, v=None, a=None,
+              record_eq=None):
+        """An explicit stage as ExplicitAnalysis runs it (src/exec/explicit_analysis.cpp:665-725,
+        no LTS, constraints or recorders): ExplicitDifference (scheme 1) starts the half-step
+        velocity from the committed one; CentralDifference (scheme 0) starts Utm1 = Ut. Returns
+        (u, v_rec, a, time, hist)."""
+        n = self.n
+        u = np.zeros(n) if u is None else np.array(u, np.float64)
+        v = np.zeros(n) if v is None else np.array(v, np.float64)
+        a = np.zeros(n) if a is None else np.array(a, np.float64)
+        f = np.zeros(n)
+        m, pm = _f(mass)
+        c, pc = _f(cm)
+        dof = np.ascontiguousarray(eq_dof, np.int8)
+        mot = PortMotions(patterns)
+        gd, pgd = mot.dof, mot.dof.ctypes.data_as(p_i32)
+        P = lambda x: x.ctypes.data_as(p_f64)
+        hist = []
+        if scheme == 1:
+            vh = v.copy()
+        else:
+            um = u.copy()
+            ve = np.zeros(n)
+        for _ in range(steps):
+            if scheme == 1:
+                time += dt
+                g, pg = _f(mot.evaluate(time))
+                port().fxo_ed_stage_step(C.byref(self.s), pm, dof.ctypes.data_as(p_i8), pg, pgd, len(gd), dt, P(u),
+                                         P(vh), P(a), P(v), P(f))
+            else:
+                g, pg = _f(mot.evaluate(time))
+                port().fxo_cd_stage_step(C.byref(self.s), pm, pc, dof.ctypes.data_as(p_i8), pg, pgd, len(gd), dt,
+                                         P(u), P(um), P(ve), P(a), P(v), P(f))
+                time += dt
+            if record_eq is not None:
+                hist.append(a[record_eq])
+        return u, v, a, time, np.array(hist)
+
     def ed_steps(self, mass, eq_dof, dt, steps, ag=None, direction=0, u=None, vh=None, a=None, record_eq=None):
         n = self.n
         u = np.zeros(n) if u is None else u.copy()
@@ -434,6 +485,65 @@ class PortMesh:
             if record_eq is not None:
                 hist.append(a[record_eq])
         return u, vh, a, v, np.array(hist)
+
+
+class PortMotions:
+    """UniformExcitation patterns evaluated by the port's restatement of GroundMotions::evaluate
+    (src/exec/ground_motion.cpp:150-175): accel[p] = fact_p * series_p(t), 0 for t < 0. A pattern
+    is a dict: dof (0-based), fact, values, and dt (PathSeries) or times (PathTimeSeries), factor,
+    use_last, prepend_zero."""
+
+    def __init__(self, patterns):
+        self.patterns = [dict(p) for p in patterns]
+        self.loc = [C.c_int(0) for _ in self.patterns]
+        self.dof = np.array([p["dof"] for p in self.patterns], np.int32)
+
+    def evaluate(self, t):
+        out = np.zeros(len(self.patterns))
+        for i, p in enumerate(self.patterns):
+            a = 0.0
+            if t >= 0.0:
+                vals = np.asarray(p["values"], np.float64)
+                if p.get("times") is None:
+                    if p.get("prepend_zero"):
+                        vals = np.concatenate([[0.0], vals])
+                    v, pv = _f(vals)
+                    a = port().fxo_path_uniform(pv, len(v), p["dt"], p.get("factor", 1.0), 0.0,
+                                                int(bool(p.get("use_last"))), t)
+                else:
+                    v, pv = _f(vals)
+                    tm, pt = _f(p["times"])
+                    a = port().fxo_path_time(pv, pt, len(v), p.get("factor", 1.0), C.byref(self.loc[i]), t)
+            out[i] = p["fact"] * a
+        return out
+
+
+class RefMotions:
+    """The same patterns through the reference's own exec::GroundMotions (oracle/_ref)."""
+
+    def __init__(self, patterns):
+        self.n = len(patterns)
+        self.h = ref().fxref_motions_create()
+        for p in patterns:
+            v, pv = _f(p["values"])
+            if p.get("times") is None:
+                pt, dt = None, p["dt"]
+            else:
+                tm, pt = _f(p["times"])
+                dt = 0.0
+            rc = ref().fxref_motions_add(self.h, p["dof"], p["fact"], pv, pt, len(v), dt, p.get("factor", 1.0),
+                                         int(bool(p.get("use_last"))), int(bool(p.get("prepend_zero"))))
+            assert rc == 0, ref().fxref_last_error()
+
+    def evaluate(self, t):
+        out = np.zeros(self.n)
+        rc = ref().fxref_motions_evaluate(self.h, t, out.ctypes.data_as(p_f64))
+        assert rc == 0, ref().fxref_last_error()
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().fxref_motions_destroy(self.h)
 
 
 def port_dot(x, y, lanes, fused):

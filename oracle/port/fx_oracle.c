@@ -850,6 +850,105 @@ void fxo_ed_step(const fxo_mesh* m, const double* mass, const int8_t* eq_dof, co
   }
 }
 
+/* ---------------------------------------------------------------- ground motions and stages */
+/* PathSeries::getFactor, uniform spacing (src/exec/ground_motion.cpp:21-39): 0 before the start,
+ * linear between samples floor(incr) and floor(incr) + 1, the last value (useLast) or 0 after. */
+double fxo_path_uniform(const double* values, int64_t n, double dt, double factor, double start, int use_last,
+                        double t) {
+  if (t < start) return 0.0;
+  const double incr = (t - start) / dt;
+  const long long i1 = (long long)floor(incr);
+  const long long i2 = i1 + 1;
+  if (i2 >= n) return use_last ? factor * values[n - 1] : 0.0;
+  const double v1 = values[i1], v2 = values[i2];
+  return factor * (v1 + (v2 - v1) * (incr - (double)i1));
+}
+
+/* PathTimeSeries::getFactor (ground_motion.cpp:41-77): the interval walk from *loc, forwards or
+ * backwards, kept for the next call; 0 outside the times. */
+double fxo_path_time(const double* values, const double* times, int64_t n, double factor, int* loc, double t) {
+  int l = *loc;
+  double t1 = times[l];
+  if (t < t1 && l == 0) return 0.0;
+  if (t == t1) return factor * values[l];
+  const int last = (int)n - 1;
+  if (t > t1 && l == last) return 0.0;
+  double t2 = times[l + 1];
+  if (t > t2) {
+    while (t > t2 && l < last - 1) {
+      ++l;
+      t1 = t2;
+      t2 = times[l + 1];
+    }
+    *loc = l;
+    if (t > t2) return 0.0;
+  } else if (t < t1) {
+    while (t < t1 && l > 0) {
+      --l;
+      t2 = t1;
+      t1 = times[l];
+    }
+    *loc = l;
+    if (t < t1) return 0.0;
+  }
+  const double v1 = values[l], v2 = values[l + 1];
+  return factor * (v1 + (v2 - v1) * (t - t1) / (t2 - t1));
+}
+
+/* ground_load (explicit_analysis.cpp:51-58): -m accel(p) for every pattern acting in the DOF */
+static double ground_load(double mq, int dof_q, const double* accel, const int32_t* gdof, int npat) {
+  double r = 0.0;
+  for (int p = 0; p < npat; ++p)
+    if (gdof[p] == dof_q) r -= mq * accel[p];
+  return r;
+}
+
+/* ed_predict, force, ed_correct (explicit_analysis.cpp:62-84 in the order of :700-711) */
+void fxo_ed_stage_step(const fxo_mesh* m, const double* mass, const int8_t* eq_dof, const double* accel,
+                       const int32_t* gdof, int npat, double dt, double* u, double* vh, double* a, double* v_rec,
+                       double* f) {
+  const int32_t n = m->num_equations;
+  for (int32_t q = 0; q < n; ++q) {
+    vh[q] += a[q] * dt;
+    u[q] += vh[q] * dt;
+  }
+  fxo_force(m, u, vh, f);
+  const double halfT = dt * 0.125;
+  for (int32_t q = 0; q < n; ++q) {
+    const double R = -f[q] + ground_load(mass[q], eq_dof[q], accel, gdof, npat);
+    const double a_new = R / mass[q];
+    const double t = 3.0 * a_new + a[q];
+    v_rec[q] = vh[q] + t * halfT;
+    a[q] = a_new;
+  }
+}
+
+/* cd_garbage_velocity, force, cd_solve (explicit_analysis.cpp:86-117 in the order of :712-721),
+ * c2 = 0.5 / dt, c3 = 1 / dt^2 (:673) */
+void fxo_cd_stage_step(const fxo_mesh* m, const double* mass, const double* cm, const int8_t* eq_dof,
+                       const double* accel, const int32_t* gdof, int npat, double dt, double* u, double* um,
+                       double* v_elem, double* a, double* v_rec, double* f) {
+  const int32_t n = m->num_equations;
+  const double c2 = 0.5 / dt, c3 = 1.0 / (dt * dt);
+  for (int32_t q = 0; q < n; ++q) v_elem[q] = um[q] * -c2;
+  fxo_force(m, u, v_elem, f);
+  for (int32_t q = 0; q < n; ++q) {
+    const double ag = u[q] * (-2.0 * c3) + um[q] * c3;
+    const double R = -f[q] - mass[q] * ag + ground_load(mass[q], eq_dof[q], accel, gdof, npat);
+    const double A = mass[q] * c3 + cm[q] * c2;
+    const double U = R / A;
+    double Ud = U * 3.0;
+    Ud += u[q] * -4.0;
+    Ud += um[q];
+    Ud *= c2;
+    const double Udd = (Ud - v_rec[q]) / dt;
+    um[q] = u[q];
+    u[q] = U;
+    v_rec[q] = Ud;
+    a[q] = Udd;
+  }
+}
+
 void fxo_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
                          double a2, double a3, double a4) {
   for (int64_t q = 0; q < n; ++q) {

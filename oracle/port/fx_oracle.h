@@ -72,6 +72,25 @@ void fxo_gmres(const fxo_mesh* m, const double* k, const double* b, double* x, d
 void fxo_ed_step(const fxo_mesh* m, const double* mass, const int8_t* eq_dof, const double* ag, double dt, double* u,
                  double* vh, double* a, double* v_rec, double* f_work);
 
+/* Ground motions (src/exec/ground_motion.cpp:21-77, 150-175): PathSeries::getFactor with a
+ * uniform spacing (values[n], dt, cFactor, startTime, useLast) and PathTimeSeries::getFactor
+ * with a time array (values[n], times[n], cFactor, *loc kept between calls). */
+double fxo_path_uniform(const double* values, int64_t n, double dt, double factor, double start, int use_last,
+                        double t);
+double fxo_path_time(const double* values, const double* times, int64_t n, double factor, int* loc, double t);
+
+/* One explicit step of a stage with npat UniformExcitation patterns whose ground accelerations
+ * at the step's load time are accel[p] acting in DOF gdof[p] (explicit_analysis.cpp:51-58).
+ * ExplicitDifference (:62-84, 700-711): predict, force at (u, vh), correct. CentralDifference
+ * (:86-117, 712-721): v_elem = -c2 um, force at (u, v_elem), the diagonal solve with the lumped
+ * alphaM masses cm; um, u, v_rec, a updated. f_work: neq doubles. */
+void fxo_ed_stage_step(const fxo_mesh* m, const double* mass, const int8_t* eq_dof, const double* accel,
+                       const int32_t* gdof, int npat, double dt, double* u, double* vh, double* a, double* v_rec,
+                       double* f_work);
+void fxo_cd_stage_step(const fxo_mesh* m, const double* mass, const double* cm, const int8_t* eq_dof,
+                       const double* accel, const int32_t* gdof, int npat, double dt, double* u, double* um,
+                       double* v_elem, double* a, double* v_rec, double* f_work);
+
 /* Newmark form-D kernels (src/exec/implicit_stage.cpp:29-68). */
 void fxo_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,
                          double a2, double a3, double a4);

@@ -39,3 +39,12 @@ std::size_t Model::element_count() const {
 }
 
 }  // namespace femorax::io
+
+// GroundMotions (src/exec/ground_motion.cpp) forwards to its H5DRM patterns; none is ever
+// activated here (the DRM reader needs HDF5), so these are never reached.
+#include "exec/drm_load.hpp"
+
+namespace femorax::exec {
+void DrmLoad::apply(double, const Vec&) {}
+void DrmLoad::commit() {}
+}  // namespace femorax::exec

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "compile/batches.hpp"
+#include "exec/ground_motion.hpp"
 #include "exec/internal_force.hpp"
 #include "exec/matrix_free_operator.hpp"
 #include "physics/elements/std_brick.hpp"
@@ -385,6 +386,59 @@ double fxref_brick_critical_dt(const double* p, const double* damp, int scheme, 
   Rayleigh d{damp[0], damp[1], damp[2], damp[3], {}};
   return Brick::critical_dt(bp, d, scheme ? ExplicitScheme::ExplicitDifference : ExplicitScheme::CentralDifference,
                             reinterpret_cast<const double(*)[3]>(xe), {});
+}
+
+// ------------------------------------------------------------------------------ ground motions
+// exec::GroundMotions (src/exec/ground_motion.cpp) over time series and UniformExcitation
+// patterns added one by one (pattern i uses series i); the motions object is built and every
+// pattern activated at the first evaluation.
+struct fxref_motions {
+  io::Model m;
+  std::unique_ptr<exec::GroundMotions> g;
+};
+
+fxref_motions* fxref_motions_create() { return new fxref_motions; }
+void fxref_motions_destroy(fxref_motions* h) { delete h; }
+
+// dof 0-based; times NULL: uniform spacing dt (PathSeries), else PathTimeSeries
+int fxref_motions_add(fxref_motions* h, int32_t dof, double fact, const double* values, const double* times,
+                      int32_t n, double dt, double factor, int32_t use_last, int32_t prepend_zero) {
+  try {
+    io::PathSeries s;
+    s.tag = static_cast<int32_t>(h->m.time_series.size()) + 1;
+    s.factor = factor;
+    if (!times) s.dt = dt;
+    else s.time.assign(times, times + n);
+    s.values.assign(values, values + n);
+    s.use_last = use_last != 0;
+    s.prepend_zero = prepend_zero != 0;
+    h->m.time_series.push_back(s);
+    io::UniformExcitation p;
+    p.tag = s.tag;
+    p.dof = dof + 1;
+    p.accel = s.tag;
+    p.factor = fact;
+    h->m.patterns.push_back(p);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// accel[p] = the active patterns' ground accelerations at time t (GroundMotions::evaluate)
+int fxref_motions_evaluate(fxref_motions* h, double t, double* accel) {
+  try {
+    if (!h->g) {
+      h->g = std::make_unique<exec::GroundMotions>(h->m);
+      for (const auto& p : h->m.patterns) h->g->activate(p.tag);
+    }
+    h->g->evaluate(t);
+    const auto a = h->g->accel();
+    for (int p = 0; p < h->g->num_active(); ++p) accel[p] = a(p);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
 }
 
 }  // extern "C"
