@@ -34,6 +34,10 @@ CXX_COMMON = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" +
 CUDA_SOURCES = [
     ("general.cu", ["--fmad=false"]),
     ("box.cu", []),
+    ("box_f64_apply.cu", []),
+    ("box_f64_force.cu", []),
+    ("box_f32_apply.cu", []),
+    ("box_f32_force.cu", []),
     ("vector.cu", []),
     ("solve.cu", []),
     ("stepping.cu", []),

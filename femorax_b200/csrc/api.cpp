@@ -382,7 +382,7 @@ int fx_force_set_launch(fx_force* f, int32_t variant, int32_t kz) {
 int fx_force_get_launch(const fx_force* f, int32_t* launch) {
   return guarded([&] {
     FX_REQUIRE(f && launch, "fx_force_get_launch: bad arguments");
-    const auto& sh = f->s.box.shape[0];
+    const auto& sh = f->s.box.shape[0][0];
     launch[0] = sh.variant;
     launch[1] = sh.persistent ? -sh.kz : sh.kz;
   });

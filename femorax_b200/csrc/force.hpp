@@ -86,17 +86,19 @@ struct BoxPlan {
   DeviceArray<int32_t> elem_param;  // [nz ny nx]: parameter set of each element
   DeviceArray<int32_t> node_of;     // host-side check only: grid node -> internal node
   std::vector<int32_t> grid_node_h; // grid node -> internal node
-  // Launch shape per precision (0: FP64, 1: FP32), chosen by the autotuner: variant (block of
-  // element columns, CTAs per SM), kz node planes per tile, and the persistent form (one wave of
-  // CTAs taking tiles from `queue`) or one CTA per tile.
+  // Launch shape per precision (0: FP64, 1: FP32) and kernel mode (0: operator apply, 1: internal
+  // force), chosen by the autotuner: variant (block of element columns, CTAs per SM), kz node
+  // planes per tile, and the persistent form (one wave of CTAs taking tiles from `queue`) or one
+  // CTA per tile.
   struct Shape {
     int variant = 2, kz = 8;
     bool persistent = false;
-  } shape[2];
+  } shape[2][2];
   DeviceArray<int> queue;    // [next tile, CTAs done], zero between launches
   bool tuned = false;
   bool layered = false;  // one parameter set per element plane (kernel-parameter tables)
   bool scaled = false;   // the sets differ only in E: one table and a per-element scale
+  bool full = false;     // every grid node has all three DOFs free or none
   DeviceArray<double> escale;   // [nz ny nx]: E_e / E_ref
   DeviceArray<float> escale32;
   // The coefficient tables of one kernel mode (0: the operator for the last operator

@@ -151,11 +151,12 @@ int fx_force_set_path(fx_force* f, int32_t path);
 int fx_force_info(const fx_force* f, int64_t* info);
 /* Box path launch shape: variant (block of element columns, CTAs per SM) and kz (node planes
  * per CTA); fx_force_tune times the candidates on the device, for the FP64 and the FP32 operator
- * separately, and keeps the fastest of each (the autotuner fx_force_create runs on meshes of
- * 262,144 elements or more; exec::choose_force_settings' role, src/exec/force_settings.cpp:71-205).
- * fx_force_set_launch pins both precisions to one shape; launch[2] of fx_force_get_launch
- * receives the FP64 shape (variant, kz). A negative kz selects (or reports) the persistent form
- * of that shape: one wave of CTAs taking tiles of |kz| planes from a queue. */
+ * and internal force separately, and keeps the fastest of each (the autotuner fx_force_create
+ * runs on meshes of 262,144 elements or more; exec::choose_force_settings' role,
+ * src/exec/force_settings.cpp:71-205). fx_force_set_launch pins every precision and kernel to
+ * one shape; launch[2] of fx_force_get_launch receives the FP64 operator's shape (variant, kz).
+ * A negative kz selects (or reports) the persistent form of that shape: one wave of CTAs taking
+ * tiles of |kz| planes from a queue. */
 int fx_force_set_launch(fx_force* f, int32_t variant, int32_t kz);
 int fx_force_get_launch(const fx_force* f, int32_t* launch);
 int fx_force_tune(fx_force* f, void* stream);
