@@ -354,12 +354,17 @@ def run_ours(args):
 
     spec, comp = build_mesh()
     mesh = comp.mesh()
+    if args.launch:  # pinned before the force is created: no tuning launches
+        os.environ["FEMORAX_B200_BOX_LAUNCH"] = args.launch
     force = fx.InternalForce(mesh, device=local)
     if args.launch:
-        v, kz = (int(t) for t in args.launch.split(","))
-        fx_check(fx_lib().fx_force_set_launch(force._h, v, kz))
+        os.environ.pop("FEMORAX_B200_BOX_LAUNCH")
     launch = (fx_ctypes.c_int32 * 2)()
     fx_check(fx_lib().fx_force_get_launch(force._h, launch))
+    shapes = (fx_ctypes.c_int32 * 8)()
+    fx_check(fx_lib().fx_force_get_launches(force._h, shapes))
+    tuned = {name: [int(shapes[2 * i]), int(shapes[2 * i + 1])]
+             for i, name in enumerate(("f64_apply", "f64_force", "f32_apply", "f32_force"))}
     info = force.info()
     neq, n_el, n_nodes = mesh.num_equations, mesh.count, mesh.num_nodes
     dev = torch.device("cuda", local)
@@ -430,7 +435,7 @@ def run_ours(args):
             "config": dict(WORKLOAD, neq=neq, elements=n_el, nodes=n_nodes, path=info["path"],
                            parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                            launch={"variant": int(launch[0]), "kz": int(launch[1]),
-                                   "chosen_by": "option" if args.launch else "autotuner"},
+                                   "chosen_by": "option" if args.launch else "autotuner", "all": tuned},
                            l2="flushed (256 MB write) between timed applies"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",

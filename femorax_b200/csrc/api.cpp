@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -333,7 +335,15 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
       s.wx.alloc(static_cast<size_t>(std::max(s.neq, 1)));
       s.wy.alloc(static_cast<size_t>(std::max(s.neq, 1)));
       fx::box_build_plan(s);
-      if (s.box.qualifies) fx::box_autotune(s, nullptr);
+      if (s.box.qualifies) {
+        // FEMORAX_B200_BOX_LAUNCH="variant,kz" pins the launch shape instead of timing the
+        // candidates, as the reference's FEMORAX_FORCE_SETTINGS overrides its autotuner
+        // (src/exec/force_settings.cpp:186-190)
+        int variant = 0, kz = 0;
+        const char* o = std::getenv("FEMORAX_B200_BOX_LAUNCH");
+        if (o && *o && std::sscanf(o, "%d,%d", &variant, &kz) == 2) fx::box_set_launch(s, variant, kz);
+        else fx::box_autotune(s, nullptr);
+      }
       FX_CUDA(cudaDeviceSynchronize());
     } catch (...) {
       delete h;
@@ -385,6 +395,18 @@ int fx_force_get_launch(const fx_force* f, int32_t* launch) {
     const auto& sh = f->s.box.shape[0][0];
     launch[0] = sh.variant;
     launch[1] = sh.persistent ? -sh.kz : sh.kz;
+  });
+}
+
+int fx_force_get_launches(const fx_force* f, int32_t* launch) {
+  return guarded([&] {
+    FX_REQUIRE(f && launch, "fx_force_get_launches: bad arguments");
+    for (int prec = 0; prec < 2; ++prec)
+      for (int mode = 0; mode < 2; ++mode) {
+        const auto& sh = f->s.box.shape[prec][mode];
+        launch[(prec * 2 + mode) * 2] = sh.variant;
+        launch[(prec * 2 + mode) * 2 + 1] = sh.persistent ? -sh.kz : sh.kz;
+      }
   });
 }
 

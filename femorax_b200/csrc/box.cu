@@ -314,7 +314,7 @@ void box_build_plan(ForceState& s) {
     for (size_t i = 0; i < s.nodal_alpha_h.size(); ++i) la[i] += s.nodal_alpha_h[i];
     p.la.upload(la);
   }
-  p.full = full;
+  p.full = full && s.neq >= 3;  // (the FULL gather addresses equation d < 3 of a fixed node)
   p.nx = nx;
   p.ny = ny;
   p.nz = nz;

@@ -312,9 +312,11 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
         q = (packed & 0x1FFFFFFF) + __popc(mask & ((1u << d) - 1u));
         free_dof = (mask >> d) & 1u;
       }
-      cp_async_zfill(&xs[((b * NV + 0) * 3 + d) * NS + s], free_dof ? a.x + q : a.x, sizeof(T), free_dof);
-      if (MODE == 1)
-        cp_async_zfill(&xs[((b * NV + 1) * 3 + d) * NS + s], free_dof ? a.v + q : a.v, sizeof(T), free_dof);
+      // FULL: a fixed or outside node's word is 0, so q = d < 3 <= neq is in bounds (and nothing
+      // is read: the copy size is 0); otherwise the address of a fixed DOF is replaced by x
+      const int32_t qa = FULL || free_dof ? q : 0;
+      cp_async_zfill(&xs[((b * NV + 0) * 3 + d) * NS + s], a.x + qa, sizeof(T), free_dof);
+      if (MODE == 1) cp_async_zfill(&xs[((b * NV + 1) * 3 + d) * NS + s], a.v + qa, sizeof(T), free_dof);
     }
   };
   auto store_plane = [&](int par) {  // the owned nodes' sums of a plane, with the nodal terms

@@ -156,9 +156,14 @@ int fx_force_info(const fx_force* f, int64_t* info);
  * src/exec/force_settings.cpp:71-205). fx_force_set_launch pins every precision and kernel to
  * one shape; launch[2] of fx_force_get_launch receives the FP64 operator's shape (variant, kz).
  * A negative kz selects (or reports) the persistent form of that shape: one wave of CTAs taking
- * tiles of |kz| planes from a queue. */
+ * tiles of |kz| planes from a queue. The environment variable FEMORAX_B200_BOX_LAUNCH="variant,kz"
+ * makes fx_force_create pin that shape instead of timing the candidates (the role of the
+ * reference's FEMORAX_FORCE_SETTINGS, src/exec/force_settings.cpp:186-190). */
 int fx_force_set_launch(fx_force* f, int32_t variant, int32_t kz);
 int fx_force_get_launch(const fx_force* f, int32_t* launch);
+/* Every tuned shape: launch[8] = (variant, kz) of the FP64 operator, FP64 internal force, FP32
+ * operator, FP32 internal force (no counterpart in the reference). */
+int fx_force_get_launches(const fx_force* f, int32_t* launch);
 int fx_force_tune(fx_force* f, void* stream);
 
 /* Operator coefficients K_eff = stiffness K_t + damping C + mass M (OperatorCoefficients,

@@ -75,3 +75,22 @@ def j2_column(nx=2, ny=3, nz=6, lumped=False, hk=0.5, h=0.5):
     spec.grid = (nx, ny, nz, h, h, h)
     return spec
 
+
+
+def roller_block(nx=5, ny=4, nz=6):
+    """A box-grid block on rollers: base fixed, the x faces fixed in x and the y faces in y, so
+    side nodes keep two free DOFs and corner columns one (nodes neither fully free nor fixed)."""
+    spec = meshes.box_model(nx, ny, nz, (2.0, 1.5, 3.0), E=3.0e5, nu=0.3, rho=1.8, lumped=False)
+    nodes, dofs = [], []
+    for k in range(1, nz + 1):
+        for j in range(ny + 1):
+            for i in (0, nx):
+                nodes.append(meshes.node_tag(i, j, k, nx, ny))
+                dofs.append(1)
+        for i in range(nx + 1):
+            for j in (0, ny):
+                nodes.append(meshes.node_tag(i, j, k, nx, ny))
+                dofs.append(2)
+    spec.fix_node = np.concatenate([spec.fix_node, np.array(nodes, np.int32)])
+    spec.fix_dof = np.concatenate([spec.fix_dof, np.array(dofs, np.int32)])
+    return spec

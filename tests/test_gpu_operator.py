@@ -11,7 +11,7 @@ import pytest
 
 import femorax_b200 as fx
 from femorax_b200 import meshes
-from tests.models_for_tests import soil_column, two_region_block
+from tests.models_for_tests import soil_column, two_region_block, roller_block
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -40,6 +40,7 @@ def models():
         "column_ties": soil_column(),
         "layered": meshes.layered_box(10, 7, 16, layers=4, seed=3)[0],
         "hetero": meshes.heterogeneous_cube(6, seed=4),
+        "rollers": roller_block(),
         "distorted": meshes.distort(meshes.box_model(5, 4, 3), 0.2, seed=5),
     }
     return out
