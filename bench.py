@@ -17,7 +17,9 @@ own InternalForce::apply_operator (built here from its sources, oracle/_ref) on 
 `newmark` compares the Newmark stage with plain FP64 and mixed-precision inner solves;
 `batched_j2` compares the batched J2 Newton with one instance at a time on a bounded sample;
 `served` compares solves/s and p50/p99 latency at a 1e-8 FP64 residual on a stream of static solves:
-the batched mixed-precision engine behind the serving loop versus plain FP64 CG one at a time.
+the batched mixed-precision engine behind the serving loop versus plain FP64 CG one at a time;
+`served_mixed` does the same on a stream of 70 % static solves and 30 % J2 load paths (J2 cohorts
+beside the engine's slots).
 
 The reference arm (--impl reference) times that reference CPU path alone, on every host thread.
 """
@@ -298,6 +300,47 @@ def serve_comparison(device, count=32, seed=1):
             "engine_rounds": eng.info()["rounds"]}
 
 
+def serve_mixed_comparison(device, count=32, seed=2):
+    """The served mixed stream on a bounded sample: `count` requests all arriving at once, 70 % static
+    solves as in serve_comparison and 30 % J2 load paths (the batched J2 sample's instances: nx = ny
+    in {1, 2, 4, 8}, nz in [20, 40], one cyclic top-shear cycle of 8 load steps). The serving loop
+    (BatchEngine slots for the static solves, J2 cohorts of up to 32 beside them) against the same
+    stream solved one at a time by the plain FP64 path. The J2 results of the two arms are compared
+    bit for bit."""
+    import femorax_b200 as fx
+    from femorax_b200 import serving
+    reqs = serving.mixed_stream(count, rate=1e9, j2_share=0.3, min_dof=1e4, max_dof=5e5, seed=seed,
+                                j2_sizes=(1, 2, 4, 8), j2_nz=(20, 40))
+    sy, b, L = 100e3, 0.5, 10.0
+    warm = [serving.Request(10_000, 4, 4, 4), serving.J2Request(10_001, 1, 1, 20, sigma_y=sy,
+                                                               total=1.2 * sy * b ** 3 / (6.0 * L))]
+    prepared, solvers = serving.resident(reqs + warm, device)
+    server_prep = {r.id: serving.prepare_j2(r, device) if isinstance(r, serving.J2Request) else prepared[r.id]
+                   for r in reqs + warm}
+    eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
+
+    def server():
+        return serving.Server(eng, hbm_budget=64 << 30, device=device, prepare_fn=lambda r, d: server_prep[r.id])
+
+    server().run(warm, realtime=False)  # untimed: module loading, first launches, graph set-up
+    serving.serve_one_at_a_time(warm, realtime=False, device=device, prepared=prepared, solvers=solvers)
+    mixed, wall_m = server().run(reqs, realtime=False)
+    plain, wall_p = serving.serve_one_at_a_time(reqs, 1e-8, realtime=False, device=device, prepared=prepared,
+                                                solvers=solvers)
+    m, p = serving.summary(mixed, wall_m), serving.summary(plain, wall_p)
+    j2_ids = [r.id for r in reqs if isinstance(r, serving.J2Request)]
+    pm, pp = {s.id: s for s in mixed}, {s.id: s for s in plain}
+    same = all(np.array_equal(pm[i].x, pp[i].x) and np.array_equal(pm[i].result.monitor, pp[i].result.monitor)
+               for i in j2_ids)
+    return {"stream": f"{count} requests all at t=0 (seed {seed}): {count - len(j2_ids)} static solves on "
+                      f"structured blocks (log-uniform 1e4-5e5 equations, rtol 1e-8 in FP64), {len(j2_ids)} J2 "
+                      f"load paths (nx = ny in {{1, 2, 4, 8}}, nz in [20, 40], one cycle of 8 load steps)",
+            "mixed_batched": {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
+            "plain_fp64_one_at_a_time": {k: p[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
+            "speedup_solves_per_s": m["solves_per_s"] / p["solves_per_s"] if p["solves_per_s"] else None,
+            "j2_bit_identical": bool(same)}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -426,6 +469,7 @@ def run_ours(args):
         return 0
     explicit = explicit_comparison(force, mesh, comp, local) if world == 1 and not args.no_serve else None
     served = serve_comparison(local) if world == 1 and not args.no_serve else None
+    served_mixed = serve_mixed_comparison(local) if world == 1 and not args.no_serve else None
     batched_j2 = batched_j2_comparison(local) if world == 1 and not args.no_serve else None
     newmark = newmark_comparison(local) if world == 1 and not args.no_serve else None
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
@@ -446,6 +490,7 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "explicit": explicit,
             "served": served,
+            "served_mixed": served_mixed,
             "batched_j2": batched_j2,
             "newmark": newmark}
     print(json.dumps(line))

@@ -38,6 +38,8 @@ CUDA_SOURCES = [
     ("box_f64_force.cu", []),
     ("box_f32_apply.cu", []),
     ("box_f32_force.cu", []),
+    ("box_f64_forcew.cu", []),
+    ("box_f32_forcew.cu", []),
     ("vector.cu", []),
     ("solve.cu", []),
     ("stepping.cu", []),

@@ -9,11 +9,13 @@
 
 namespace fx {
 namespace boxk {
-// instantiated in box_f64_apply.cu, box_f64_force.cu, box_f32_apply.cu and box_f32_force.cu
+// instantiated in box_f64_apply.cu, box_f64_force.cu, box_f64_forcew.cu and their FP32 twins
 extern template void launch<double, 0>(const BoxPlan&, const BoxArgs<double>&, cudaStream_t);
 extern template void launch<double, 1>(const BoxPlan&, const BoxArgs<double>&, cudaStream_t);
 extern template void launch<float, 0>(const BoxPlan&, const BoxArgs<float>&, cudaStream_t);
 extern template void launch<float, 1>(const BoxPlan&, const BoxArgs<float>&, cudaStream_t);
+extern template void launch<double, 2>(const BoxPlan&, const BoxArgs<double>&, cudaStream_t);
+extern template void launch<float, 2>(const BoxPlan&, const BoxArgs<float>&, cudaStream_t);
 }  // namespace boxk
 using namespace boxk;
 
@@ -381,6 +383,25 @@ static void force_t(ForceState& s, const T* u, const T* v, T* f, cudaStream_t st
   a.beta = static_cast<T>(s.box.beta);
   a.nm2 = s.box.la.ptr;
   launch<T, 1>(s.box, a, st);
+}
+
+// the force from w = u + beta v, formed by the caller (v: the velocity of the la v term)
+template <class T>
+static void force_w_t(ForceState& s, const T* w, const T* v, T* f, cudaStream_t st) {
+  if (!s.box.force_ok) throw Error(FX_E_UNSUPPORTED, "box force form needs one beta, and lumped masses or no mass-proportional damping");
+  const double k1[3] = {1.0, 0.0, 0.0};
+  ensure_coef(s, 1, k1);
+  BoxArgs<T> a = args<T>(s, 1, w, v, f);
+  a.kz = s.box.shape[sizeof(T) == 4 ? 1 : 0][0].kz;  // one staged vector: the apply's shape
+  a.nm2 = s.box.la.ptr;
+  launch<T, 2>(s.box, a, st);
+}
+
+void box_force_w(ForceState& s, const double* w, const double* v, double* f, cudaStream_t st) {
+  force_w_t<double>(s, w, v, f, st);
+}
+void box_force_w_f32(ForceState& s, const float* w, const float* v, float* f, cudaStream_t st) {
+  force_w_t<float>(s, w, v, f, st);
 }
 
 void box_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {

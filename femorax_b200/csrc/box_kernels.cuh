@@ -198,6 +198,8 @@ __device__ __forceinline__ void modal_apply(const CT& k, T t[3][8], T sc = T(1))
 
 // MODE 0: y = K_eff x (+ k.mass nodal masses x + k.damping nodal alphaM masses x).
 // MODE 1: f = K (u + beta v) - body + la v (la: lumped alphaM masses, element and nodal).
+// MODE 2: MODE 1's force from w = u + beta v formed beforehand (x = w, v read by the owners for
+// la v only): one staged vector, as the apply.
 // MINB: CTAs per SM the register budget is sized for. CACHE: keep the bottom face's transform
 // in registers from the plane below (fewer operations, more registers) or transform it again
 // from the staged plane (fewer registers, more resident warps).
@@ -433,22 +435,22 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
       T body[3] = {T(0), T(0), T(0)};
       if constexpr (LAYERED) {
         modal_apply<false>(tab->c[p_here], tv);
-        if (MODE == 1)
+        if (MODE >= 1)
           for (int d = 0; d < 3; ++d) body[d] = T(tab->c[p_here].body[d]);
       } else if constexpr (scaled) {
         modal_apply<true, true>(stab, tv, s_here);
-        if (MODE == 1)
+        if (MODE >= 1)
           for (int d = 0; d < 3; ++d) body[d] = T(stab.body[d]);
       } else {
         const CT& k = coef[p_here];
         modal_apply<true>(k, tv);
-        if (MODE == 1)
+        if (MODE >= 1)
           for (int d = 0; d < 3; ++d) body[d] = T(k.body[d]);
       }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         T* g = tv[d];
-        if (MODE == 1) g[0] -= body[d];
+        if (MODE >= 1) g[0] -= body[d];
         T h[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
@@ -576,7 +578,7 @@ void launch_kernel(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     resident = std::max(resident, 1);
   }
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
-  if (p.shape[sizeof(T) == 4 ? 1 : 0][MODE].persistent) {
+  if (p.shape[sizeof(T) == 4 ? 1 : 0][MODE == 1 ? 1 : 0].persistent) {
     BoxArgs<T> b = a;
     b.queue = p.queue.ptr;
     b.gx = static_cast<int>(grid.x);
@@ -584,9 +586,9 @@ void launch_kernel(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     b.gz = static_cast<int>(grid.z);
     const int ntiles = b.gx * b.gy * b.gz;
     const int ctas = std::min(ntiles, resident * num_sms());
-    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p, MODE));
+    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p, MODE == 0 ? 0 : 1));
   } else {
-    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p, MODE));
+    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p, MODE == 0 ? 0 : 1));
   }
   FX_LAUNCH_CHECK("box_operator");
 }
@@ -606,7 +608,8 @@ void launch_one(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
 
 template <class T, int MODE>
 void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
-  switch (p.shape[sizeof(T) == 4 ? 1 : 0][MODE].variant) {
+  // (MODE 2 stages one vector, as the apply: the apply's shape)
+  switch (p.shape[sizeof(T) == 4 ? 1 : 0][MODE == 1 ? 1 : 0].variant) {
     case 0: return launch_one<32, 8, 2, false, T, MODE>(p, a, st);
     case 1: return launch_one<16, 16, 2, false, T, MODE>(p, a, st);
     case 2: return launch_one<16, 8, 4, false, T, MODE>(p, a, st);

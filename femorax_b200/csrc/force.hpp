@@ -128,6 +128,8 @@ struct ExplicitWork {
   // explicit stages: the half-step velocity (ExplicitDifference) or the previous displacement
   // (CentralDifference) carried between calls, the element velocity, the stage time
   DeviceArray<double> carry, v_elem, time;
+  DeviceArray<double> w64;  // w = u + beta v of the next force evaluation (box path)
+  DeviceArray<float> w32;
   int carry_scheme = -1;
 };
 
@@ -188,6 +190,10 @@ void box_apply_f32(ForceState& s, const double k[3], const float* x, float* y, c
 void box_prepare(ForceState& s, const double k[3]);
 void box_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cudaStream_t st);
+// the box force from w = u + beta v formed by the caller with fma(beta, v, u), as the force kernel
+// forms it (the same values), v for the lumped alphaM term: one staged vector instead of two
+void box_force_w(ForceState& s, const double* w, const double* v, double* f, cudaStream_t st);
+void box_force_w_f32(ForceState& s, const float* w, const float* v, float* f, cudaStream_t st);
 int box_num_variants();
 void box_set_launch(ForceState& s, int variant, int kz);
 void box_autotune(ForceState& s, cudaStream_t st);

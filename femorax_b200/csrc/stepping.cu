@@ -18,13 +18,18 @@
 namespace fx {
 namespace {
 
+// w (when set): u + beta vh of the force evaluation that follows, fma(beta, vh, u) as the box force
+// kernel forms it
 template <class T>
-__global__ void k_ed_predict(T* __restrict__ u, T* __restrict__ vh, const T* __restrict__ a, T dt, int64_t n) {
+__global__ void k_ed_predict(T* __restrict__ u, T* __restrict__ vh, const T* __restrict__ a, T dt, int64_t n,
+                             T* __restrict__ w, T beta) {
   for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
        q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const T v = vh[q] + a[q] * dt;
     vh[q] = v;
-    u[q] = u[q] + v * dt;
+    const T un = u[q] + v * dt;
+    u[q] = un;
+    if (w) w[q] = fma(beta, v, un);
   }
 }
 
@@ -33,7 +38,8 @@ template <class T>
 __global__ void k_ed_correct_predict(const T* __restrict__ f, const T* __restrict__ m, const int8_t* __restrict__ dof,
                                      const double* __restrict__ ag, int* __restrict__ step, int dir, T dt,
                                      T* __restrict__ u, T* __restrict__ vh, T* __restrict__ a, T* __restrict__ v,
-                                     int64_t n, int32_t record_eq, double* __restrict__ hist, int predict) {
+                                     int64_t n, int32_t record_eq, double* __restrict__ hist, int predict,
+                                     T* __restrict__ w, T beta) {
   const int s = *step;
   const T g = ag ? static_cast<T>(ag[s]) : T(0);
   const T halfT = dt * T(0.125);
@@ -52,7 +58,9 @@ __global__ void k_ed_correct_predict(const T* __restrict__ f, const T* __restric
     if (predict) {
       const T vn = vhq + an * dt;
       vh[q] = vn;
-      u[q] = u[q] + vn * dt;
+      const T un = u[q] + vn * dt;
+      u[q] = un;
+      if (w) w[q] = fma(beta, vn, un);
     }
   }
 }
@@ -141,14 +149,17 @@ __device__ __forceinline__ double ground_load(double mq, int dof_q, const double
   return r;
 }
 
-// ed_predict (explicit_analysis.cpp:62-69)
+// ed_predict (explicit_analysis.cpp:62-69); w (box path): u + beta vh for the force, as the box
+// force kernel forms it
 __global__ void k_stage_ed_predict(double* __restrict__ u, double* __restrict__ vh, const double* __restrict__ a,
-                                   double dt, int64_t n) {
+                                   double dt, int64_t n, double* __restrict__ w, double beta) {
   for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
        q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double v = __dadd_rn(vh[q], __dmul_rn(a[q], dt));
     vh[q] = v;
-    u[q] = __dadd_rn(u[q], __dmul_rn(v, dt));
+    const double un = __dadd_rn(u[q], __dmul_rn(v, dt));
+    u[q] = un;
+    if (w) w[q] = __fma_rn(beta, v, un);
   }
 }
 
@@ -158,7 +169,7 @@ __global__ void k_stage_ed_correct(const double* __restrict__ f, const double* _
                                    const int* __restrict__ gdof, int npat, double dt, double* __restrict__ u,
                                    double* __restrict__ vh, double* __restrict__ a, double* __restrict__ v,
                                    int64_t n, const int* __restrict__ step, int32_t record_eq,
-                                   double* __restrict__ hist, int predict) {
+                                   double* __restrict__ hist, int predict, double* __restrict__ w, double beta) {
   const double halfT = __dmul_rn(dt, 0.125);
   for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
        q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -173,16 +184,22 @@ __global__ void k_stage_ed_correct(const double* __restrict__ f, const double* _
     if (predict) {
       const double vn = __dadd_rn(vhq, __dmul_rn(an, dt));
       vh[q] = vn;
-      u[q] = __dadd_rn(u[q], __dmul_rn(vn, dt));
+      const double un = __dadd_rn(u[q], __dmul_rn(vn, dt));
+      u[q] = un;
+      if (w) w[q] = __fma_rn(beta, vn, un);
     }
   }
 }
 
 // cd_garbage_velocity (explicit_analysis.cpp:86-92)
-__global__ void k_stage_cd_garbage(double* __restrict__ ve, const double* __restrict__ um, double c2, int64_t n) {
+__global__ void k_stage_cd_garbage(double* __restrict__ ve, const double* __restrict__ um, double c2, int64_t n,
+                                   double* __restrict__ w, const double* __restrict__ u, double beta) {
   for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
-       q += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    ve[q] = __dmul_rn(um[q], -c2);
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = __dmul_rn(um[q], -c2);
+    ve[q] = v;
+    if (w) w[q] = __fma_rn(beta, v, u[q]);
+  }
 }
 
 // cd_solve (explicit_analysis.cpp:94-117), then the next step's garbage velocity -c2 um
@@ -192,7 +209,7 @@ __global__ void k_stage_cd_solve(const double* __restrict__ f, const double* __r
                                  double c3, double dt, double* __restrict__ u, double* __restrict__ um,
                                  double* __restrict__ v, double* __restrict__ a, double* __restrict__ ve, int64_t n,
                                  const int* __restrict__ step, int32_t record_eq, double* __restrict__ hist,
-                                 int next) {
+                                 int next, double* __restrict__ w, double beta) {
   for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
        q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const double uq = u[q], umq = um[q], mq = m[q];
@@ -210,7 +227,11 @@ __global__ void k_stage_cd_solve(const double* __restrict__ f, const double* __r
     v[q] = Ud;
     a[q] = Udd;
     if (q == record_eq && hist) hist[*step] = Udd;
-    if (next) ve[q] = __dmul_rn(uq, -c2);
+    if (next) {
+      const double vn = __dmul_rn(uq, -c2);
+      ve[q] = vn;
+      if (w) w[q] = __fma_rn(beta, vn, U);
+    }
   }
 }
 
@@ -375,21 +396,33 @@ void explicit_run(fx_force* f, const T* mass, int32_t dir, const double* ag_host
     if (w.f32.n < static_cast<size_t>(n)) w.f32.alloc(static_cast<size_t>(std::max<int64_t>(n, 1)));
     fbuf = w.f32.ptr;
   }
+  // on the box path the update passes also form w = u + beta vh, so the force stages one vector
+  T* wbuf = nullptr;
+  if (s.use_box_force()) {
+    if constexpr (sizeof(T) == 8) {
+      if (w.w64.n < static_cast<size_t>(n)) w.w64.alloc(static_cast<size_t>(std::max<int64_t>(n, 1)));
+      wbuf = w.w64.ptr;
+    } else {
+      if (w.w32.n < static_cast<size_t>(n)) w.w32.alloc(static_cast<size_t>(std::max<int64_t>(n, 1)));
+      wbuf = w.w32.ptr;
+    }
+  }
+  const T tbeta = static_cast<T>(s.box.beta);
   FX_CUDA(cudaMemsetAsync(w.step.ptr, 0, sizeof(int), st));
   if (steps == 0) return;
   const T tdt = static_cast<T>(dt);
-  k_ed_predict<T><<<ew(n), 256, 0, st>>>(u, vh, a, tdt, n);
+  k_ed_predict<T><<<ew(n), 256, 0, st>>>(u, vh, a, tdt, n, wbuf, tbeta);
   FX_LAUNCH_CHECK("ed_predict");
   const double* agp = ag_host ? w.ag.ptr : nullptr;
   auto one_step = [&](int predict) {
     if constexpr (sizeof(T) == 8) {
-      if (s.use_box_force()) box_force(s, u, vh, fbuf, st);
+      if (wbuf) box_force_w(s, wbuf, vh, fbuf, st);
       else general_force(s, u, vh, fbuf, st);
     } else {
-      box_force_f32(s, u, vh, fbuf, st);
+      box_force_w_f32(s, wbuf, vh, fbuf, st);
     }
     k_ed_correct_predict<T><<<ew(n), 256, 0, st>>>(fbuf, mass, s.eq_dof.ptr, agp, w.step.ptr, dir, tdt, u, vh, a, v, n,
-                                                   w.record_eq, w.hist.ptr, predict);
+                                                   w.record_eq, w.hist.ptr, predict, wbuf, tbeta);
     k_step_advance<<<1, 1, 0, st>>>(w.step.ptr);
     FX_LAUNCH_CHECK("ed_step");
   };
@@ -504,9 +537,16 @@ void explicit_stage(fx_force* f, int scheme, const double* mass, const double* c
     FX_CUDA(cudaStreamSynchronize(st));
     return;
   }
+  // on the box path the update passes also form w = u + beta v_elem: the force stages one vector
+  double* wbuf = nullptr;
+  if (s.use_box_force()) {
+    if (w.w64.n < nn) w.w64.alloc(nn);
+    wbuf = w.w64.ptr;
+  }
+  const double beta = s.box.beta;
   if (n > 0) {
-    if (scheme == 1) k_stage_ed_predict<<<ew(n), 256, 0, st>>>(u, carry, a, dt, n);
-    else k_stage_cd_garbage<<<ew(n), 256, 0, st>>>(ve, carry, c2, n);
+    if (scheme == 1) k_stage_ed_predict<<<ew(n), 256, 0, st>>>(u, carry, a, dt, n, wbuf, beta);
+    else k_stage_cd_garbage<<<ew(n), 256, 0, st>>>(ve, carry, c2, n, wbuf, u, beta);
     FX_LAUNCH_CHECK("explicit_stage_begin");
   }
   double* fbuf = w.f64.ptr;
@@ -514,15 +554,16 @@ void explicit_stage(fx_force* f, int scheme, const double* mass, const double* c
     k_motions<<<1, 32, 0, st>>>(m->d_pats.ptr, npat, m->d_values.ptr, m->d_times.ptr, m->d_loc.ptr, m->d_accel.ptr,
                                 w.time.ptr, w.step.ptr, dt, scheme == 1);
     if (n > 0) {
-      if (s.use_box_force()) box_force(s, u, ve, fbuf, st);
+      if (wbuf) box_force_w(s, wbuf, ve, fbuf, st);
       else general_force(s, u, ve, fbuf, st);
       if (scheme == 1)
         k_stage_ed_correct<<<ew(n), 256, 0, st>>>(fbuf, mass, s.eq_dof.ptr, m->d_accel.ptr, m->d_dof.ptr, npat, dt, u,
-                                                  carry, a, v, n, w.step.ptr, w.record_eq, w.hist.ptr, more);
+                                                  carry, a, v, n, w.step.ptr, w.record_eq, w.hist.ptr, more, wbuf,
+                                                  beta);
       else
         k_stage_cd_solve<<<ew(n), 256, 0, st>>>(fbuf, mass, cm, s.eq_dof.ptr, m->d_accel.ptr, m->d_dof.ptr, npat, c2,
                                                 c3, dt, u, carry, v, a, ve, n, w.step.ptr, w.record_eq, w.hist.ptr,
-                                                more);
+                                                more, wbuf, beta);
     }
     FX_LAUNCH_CHECK("explicit_stage_step");
     if (s.has_j2)  // Domain::commit after every step

@@ -1,6 +1,8 @@
-"""Serving: a request loop over a BatchEngine (continuous batching of static solves).
+"""Serving: a request loop over a BatchEngine (continuous batching of static solves) and a lane of
+batched J2 load paths.
 
-A request is a structured hex8 block (its model) and a load. The loop
+A request is a structured hex8 block (its model) and a load: a static elastic solve (`Request`)
+or a quasi-static J2 load path (`J2Request`). For the static solves the loop
   - prepares each arrived request's resident state (compile step, device maps: an InternalForce;
     this allocates) on a pool of host threads, in arrival order;
   - admits prepared requests, in arrival order, into the engine while their HBM footprint (the
@@ -13,8 +15,14 @@ A request is a structured hex8 block (its model) and a load. The loop
 Each slot's arithmetic does not depend on the others, so a request's solution is bit for bit the
 same alone and in any mix (tests/test_gpu_batch.py checks it).
 
+J2 load paths run in cohorts: when the J2 lane is idle, the prepared J2 requests waiting (in
+arrival order, up to `max_cohort`, the same load path) become one BatchedNewton (one combined
+mesh, per-instance Newton and CG on the device), which advances one load step per pass of the
+loop, between the engine's rounds, and retires all its requests at the end of the path. Each
+instance's arithmetic is that of the load path alone, bit for bit (tests/test_gpu_serving.py).
+
 `serve_one_at_a_time` is the comparison: the same stream, first come first served, each request
-solved alone by the plain FP64 Jacobi-PCG to the same tolerance.
+solved alone by the plain FP64 path (Jacobi-PCG; for J2, Newton with Jacobi-PCG per load step).
 """
 from __future__ import annotations
 
@@ -26,8 +34,8 @@ import time
 
 import numpy as np
 
-from . import (BatchEngine, ConjugateGradient, InternalForce, MatrixFreeOperator, Model, OperatorCoefficients,
-               SolveOptions, SolveResult, meshes)
+from . import (BatchEngine, BatchedNewton, ConjugateGradient, InternalForce, MatrixFreeOperator, Model,
+               OperatorCoefficients, SolveOptions, SolveResult, meshes, stages)
 
 
 @dataclasses.dataclass
@@ -47,6 +55,42 @@ class Request:
     @property
     def equations(self) -> int:
         return 3 * (self.nx + 1) * (self.ny + 1) * self.nz
+
+
+@dataclasses.dataclass
+class J2Request:
+    """A quasi-static J2 load path (the batched J2 configuration): an nx x ny x nz block of
+    h-metre boxes, base fixed, J2 with yield stress sigma_y, hardening H = 0.05 E and kinematic
+    share 0.5, under a horizontal shear traction on its top face totalling `total` newtons, scaled
+    by `cycles` triangular load cycles of `steps_per_cycle` steps."""
+    id: int
+    nx: int
+    ny: int
+    nz: int
+    E: float = 80e6
+    sigma_y: float = 100e3
+    total: float = 1e3
+    h: float = 0.5
+    cycles: int = 1
+    steps_per_cycle: int = 8
+    arrival: float = 0.0
+
+    @property
+    def equations(self) -> int:
+        return 3 * (self.nx + 1) * (self.ny + 1) * self.nz
+
+    @property
+    def path(self):
+        return (self.cycles, self.steps_per_cycle)
+
+
+@dataclasses.dataclass
+class J2Result:
+    """A served J2 load path: the monitored top displacement after each step and the Newton
+    solves per step; converged when every step converged."""
+    monitor: np.ndarray
+    newton: np.ndarray
+    converged: bool
 
 
 @dataclasses.dataclass
@@ -103,6 +147,31 @@ def prepare(req: Request, device: int = 0):
     return force, b, comp.num_equations
 
 
+def j2_spec(req: J2Request):
+    return meshes.box_model(req.nx, req.ny, req.nz, (req.nx * req.h, req.ny * req.h, req.nz * req.h), E=req.E,
+                            nu=0.3, kind=1, sigma_y=req.sigma_y, H=0.05 * req.E, hk=0.5)
+
+
+def prepare_j2(req: J2Request, device: int = 0):
+    """A J2 request's host state: (mesh arrays, unit load, monitored equation, equations). The
+    device state is the cohort's (BatchedNewton) or, alone, an InternalForce."""
+    comp = Model(j2_spec(req)).compile()
+    f, mon = stages.top_shear(j2_spec(req), equation_map(comp), req.total)
+    return comp.mesh(), f, mon, comp.num_equations
+
+
+def prepare_any(req, device: int = 0):
+    return prepare_j2(req, device) if isinstance(req, J2Request) else prepare(req, device)
+
+
+def j2_footprint(mesh) -> int:
+    """Device bytes of one J2 instance in a cohort: element maps and slots (8 nodes, 24 equations,
+    24 slot values), the material state of 8 points (two 13-value states and an 8-value tangent),
+    and about 20 vectors of its equations."""
+    per_element = 4 * (8 + 24 + 1) + 8 * 24 + 8 * 8 * (2 * 13 + 8)
+    return int(mesh.padded * per_element + 8 * 20 * mesh.num_equations)
+
+
 def synthetic_stream(count: int, rate: float, min_dof: float = 1e4, max_dof: float = 2e6, seed: int = 0):
     """Poisson arrivals at `rate` requests/s; sizes log-uniform in [min_dof, max_dof] equations on
     near-cubic blocks; E ~ U[50, 200] MPa, nu ~ U[0.25, 0.40]."""
@@ -118,21 +187,123 @@ def synthetic_stream(count: int, rate: float, min_dof: float = 1e4, max_dof: flo
     return out
 
 
+def mixed_stream(count: int, rate: float, j2_share: float = 0.3, min_dof: float = 1e4, max_dof: float = 2e6,
+                 seed: int = 0, cycles: int = 1, steps_per_cycle: int = 8, j2_sizes=(1, 2, 4, 8, 16, 24),
+                 j2_nz=(20, 400)):
+    """The served mixed stream: Poisson arrivals at `rate`; a share j2_share of the requests are J2
+    load paths (the batched J2 configuration's instances: nx = ny from j2_sizes, nz uniform in
+    j2_nz, sigma_y U[50, 200] kPa), the others static elastic solves as synthetic_stream."""
+    rng = np.random.default_rng(seed)
+    elastic = synthetic_stream(count, rate, min_dof, max_dof, seed)
+    j2 = stages.j2_instances(count, seed=seed + 1, sizes=j2_sizes, nz_range=j2_nz)
+    out = []
+    for i, r in enumerate(elastic):
+        if rng.uniform() < j2_share:
+            spec, total = j2[i]
+            nx, ny, nz, h, _, _ = spec.grid
+            g = spec.groups[0]
+            out.append(J2Request(r.id, nx, ny, nz, E=g.E, sigma_y=g.sigma_y, total=total, h=h, cycles=cycles,
+                                 steps_per_cycle=steps_per_cycle, arrival=r.arrival))
+        else:
+            out.append(r)
+    return out
+
+
+class J2Lane:
+    """A cohort of J2 load paths advancing together, one load step per call of step()."""
+
+    def __init__(self, device: int = 0, tol: float = 1e-6, cg_rtol: float = 1e-12, max_newton: int = 25):
+        self.device = device
+        self.tol = tol
+        self.cg_rtol = cg_rtol
+        self.max_newton = max_newton
+        self.members = []  # [(request, footprint, admitted)]
+        self.batch = None
+
+    @property
+    def idle(self) -> bool:
+        return not self.members
+
+    def start(self, members, prepared):
+        """members: [(request, footprint, admitted)], all with the same load path; prepared: their
+        prepare_j2 results."""
+        import torch
+        self.members = list(members)
+        reqs = [m[0] for m in members]
+        self.factors = stages.cyclic_factors(*reqs[0].path)
+        self.batch = BatchedNewton([p[0] for p in prepared],
+                                   SolveOptions(relative_tolerance=self.cg_rtol, max_iterations=20000), self.device)
+        dev = torch.device("cuda", self.device)
+        self.F = torch.as_tensor(self.batch.combine([p[1] for p in prepared]), device=dev)
+        self.u = torch.zeros(self.batch.total, dtype=torch.float64, device=dev)
+        self.idx = torch.as_tensor(np.asarray(self.batch.offsets[:-1]) + np.asarray([p[2] for p in prepared]),
+                                   device=dev)
+        self.k = 0
+        self.mon, self.nit = [], []
+        self.conv = np.ones(len(members), dtype=bool)
+
+    def step(self):
+        """One load step of every member; at the end of the path returns [(request, footprint,
+        admitted, final displacement, J2Result)] and the lane becomes idle, else []."""
+        it, res = self.batch.step(self.F * float(self.factors[self.k]), self.u, tol=self.tol,
+                                  max_newton=self.max_newton)
+        self.conv &= np.array([r.converged for r in res], dtype=bool)
+        self.batch.commit_state()
+        self.mon.append(self.u[self.idx].clone())
+        self.nit.append(it)
+        self.k += 1
+        if self.k < len(self.factors):
+            return []
+        import torch
+        mon = torch.stack(self.mon).cpu().numpy()
+        nit = np.array(self.nit)
+        us = self.batch.split(self.u.cpu().numpy())
+        out = []
+        for i, (req, foot, adm) in enumerate(self.members):
+            out.append((req, foot, adm, us[i], J2Result(mon[:, i], nit[:, i], bool(self.conv[i]))))
+        self.members, self.batch = [], None
+        return out
+
+
 def percentile(v, p):
     return float(np.percentile(np.asarray(v), p)) if len(v) else float("nan")
 
 
 class Server:
-    """The continuous-batching loop over one BatchEngine."""
+    """The continuous-batching loop over one BatchEngine (static solves) and one J2Lane (J2 load
+    paths, in cohorts of up to max_cohort)."""
 
     def __init__(self, engine: BatchEngine, hbm_budget: int, device: int = 0, prep_threads: int = 4,
-                 prepare_fn=None):
+                 prepare_fn=None, lane=None, max_cohort: int = 32):
         self.engine = engine
         self.budget = int(hbm_budget)
         self.device = device
         self.prep_threads = prep_threads
-        self.prepare = prepare_fn or prepare
+        self.prepare = prepare_fn or prepare_any
+        self.lane = lane if lane is not None else J2Lane(device)
+        self.max_cohort = max_cohort
         self.resident = 0  # footprint of the admitted requests
+
+    def _start_cohort(self, pending_j2, slots, t0):
+        """Moves the prepared J2 requests at the head of pending_j2 (same load path, up to
+        max_cohort, while the footprint fits) into the idle lane."""
+        members, prepared, foot_sum = [], [], 0
+        path = pending_j2[0][0].path
+        while pending_j2 and len(members) < self.max_cohort and pending_j2[0][1].done():
+            req, fut = pending_j2[0]
+            if req.path != path:
+                break
+            prep = fut.result()
+            foot = j2_footprint(prep[0])
+            if (slots or members) and self.resident + foot_sum + foot > self.budget:
+                break
+            pending_j2.popleft()
+            members.append((req, foot, time.perf_counter() - t0))
+            prepared.append(prep)
+            foot_sum += foot
+        if members:
+            self.lane.start(members, prepared)
+            self.resident += foot_sum
 
     def run(self, requests, realtime: bool = True):
         """Serve `requests` (sorted by arrival). With realtime, a request becomes visible at its
@@ -141,23 +312,26 @@ class Server:
         t0 = time.perf_counter()
         now = (lambda: time.perf_counter() - t0) if realtime else (lambda: math.inf)
         pool = cf.ThreadPoolExecutor(max_workers=self.prep_threads)
-        pending = collections.deque()  # (request, future) in arrival order
-        slots = {}                     # slot -> (request, footprint, admitted time)
+        pending = collections.deque()     # static solves: (request, future) in arrival order
+        pending_j2 = collections.deque()  # J2 load paths: (request, future) in arrival order
+        slots = {}                        # slot -> (request, footprint, admitted time)
         served = []
         nxt = 0
         try:
-            while nxt < len(reqs) or pending or slots:
+            while nxt < len(reqs) or pending or pending_j2 or slots or not self.lane.idle:
                 # arrivals
                 t = now()
                 while nxt < len(reqs) and reqs[nxt].arrival <= t:
-                    pending.append((reqs[nxt], pool.submit(self.prepare, reqs[nxt], self.device)))
+                    r = reqs[nxt]
+                    (pending_j2 if isinstance(r, J2Request) else pending).append(
+                        (r, pool.submit(self.prepare, r, self.device)))
                     nxt += 1
                 # admissions in arrival order, while the footprint fits and the engine has room
                 while pending and pending[0][1].done():
                     req, fut = pending[0]
                     force, b, n = fut.result()
                     foot = int(force.info()["device_bytes"])
-                    if slots and self.resident + foot > self.budget:
+                    if (slots or not self.lane.idle) and self.resident + foot > self.budget:
                         break
                     slot = self.engine.try_admit(force, b)
                     if slot is None:
@@ -165,23 +339,33 @@ class Server:
                     pending.popleft()
                     self.resident += foot
                     slots[slot] = (req, foot, time.perf_counter() - t0)
-                if not slots and pending and pending[0][1].done():
+                if not slots and self.lane.idle and pending and pending[0][1].done():
                     raise RuntimeError(f"request {pending[0][0].id} does not fit the engine even alone")
-                if not slots:
+                # a new J2 cohort when the lane is free
+                if self.lane.idle and pending_j2 and pending_j2[0][1].done():
+                    self._start_cohort(pending_j2, slots, t0)
+                if not slots and self.lane.idle:
                     # nothing on the GPU: wait for the next preparation or arrival
-                    if pending:
-                        cf.wait([pending[0][1]], return_when=cf.FIRST_COMPLETED)
+                    heads = [q[0][1] for q in (pending, pending_j2) if q]
+                    if heads:
+                        cf.wait(heads, return_when=cf.FIRST_COMPLETED)
                     elif nxt < len(reqs) and realtime:
                         time.sleep(max(0.0, min(0.01, reqs[nxt].arrival - now())))
                     continue
-                self.engine.round()
-                for slot in list(slots):
-                    if self.engine.finished(slot):
-                        req, foot, adm = slots.pop(slot)
-                        x, res = self.engine.retire(slot)
+                if slots:
+                    self.engine.round()
+                    for slot in list(slots):
+                        if self.engine.finished(slot):
+                            req, foot, adm = slots.pop(slot)
+                            x, res = self.engine.retire(slot)
+                            self.resident -= foot
+                            done = time.perf_counter() - t0
+                            served.append(Served(req.id, x, res, req.arrival if realtime else 0.0, adm, done))
+                if not self.lane.idle:
+                    for req, foot, adm, u, res in self.lane.step():
                         self.resident -= foot
                         done = time.perf_counter() - t0
-                        served.append(Served(req.id, x, res, req.arrival if realtime else 0.0, adm, done))
+                        served.append(Served(req.id, u, res, req.arrival if realtime else 0.0, adm, done))
         finally:
             pool.shutdown(wait=True)
         return served, time.perf_counter() - t0
@@ -189,22 +373,39 @@ class Server:
 
 def resident(requests, device: int = 0, rtol: float = 1e-8):
     """Prepare every request's mesh up front (the resident state a serving process keeps):
-    {id: (force, b, n)}, and for the one-at-a-time arm a plain FP64 CG per mesh, already created
-    (its work vectors allocated): {id: solver}."""
-    prepared = {r.id: prepare(r, device) for r in requests}
-    solvers = {}
-    for rid, (force, b, n) in prepared.items():
-        cg = ConjugateGradient(SolveOptions(relative_tolerance=rtol))
-        cg.setup(MatrixFreeOperator(force, OperatorCoefficients()))
-        solvers[rid] = cg
+    {id: (force, b, n)} for static solves and {id: (force, unit load, monitored equation, n)} for
+    J2 paths, and for the one-at-a-time arm a plain FP64 CG per mesh, already created (its work
+    vectors allocated): {id: solver}."""
+    import torch
+    prepared, solvers = {}, {}
+    for r in requests:
+        if isinstance(r, J2Request):
+            mesh, f, mon, n = prepare_j2(r, device)
+            prepared[r.id] = (InternalForce(mesh, device=device), torch.as_tensor(f, device=torch.device("cuda", device)),
+                              mon, n)
+            solvers[r.id] = ConjugateGradient(SolveOptions(relative_tolerance=1e-12, max_iterations=20000))
+        else:
+            prepared[r.id] = prepare(r, device)
+            cg = ConjugateGradient(SolveOptions(relative_tolerance=rtol))
+            cg.setup(MatrixFreeOperator(prepared[r.id][0], OperatorCoefficients()))
+            solvers[r.id] = cg
     return prepared, solvers
+
+
+def solve_j2_alone(req: J2Request, force, f_unit, monitor_eq, solver=None, tol: float = 1e-6):
+    """A J2 request alone by the plain FP64 path (stages.load_path from the virgin material state):
+    (final displacement, J2Result)."""
+    force.set_j2_state(np.zeros_like(force.j2_state("committed")), "committed")
+    r = stages.load_path(force, f_unit, stages.cyclic_factors(*req.path), monitor_eq, tol=tol, solver=solver)
+    return r.u, J2Result(r.monitor, r.newton, r.converged)
 
 
 def serve_one_at_a_time(requests, rtol: float = 1e-8, realtime: bool = True, device: int = 0, prepared=None,
                         solvers=None):
-    """The same stream, first come first served, each solved alone by plain FP64 Jacobi-PCG. With
-    `prepared` / `solvers` (from resident()) the meshes and solvers are resident; otherwise each
-    request is prepared when its turn comes."""
+    """The same stream, first come first served, each solved alone by the plain FP64 path
+    (Jacobi-PCG; J2: Newton with Jacobi-PCG per load step). With `prepared` / `solvers` (from
+    resident()) the meshes and solvers are resident; otherwise each request is prepared when its
+    turn comes."""
     import torch
     reqs = sorted(requests, key=lambda r: r.arrival)
     dev = torch.device("cuda", device)
@@ -216,14 +417,22 @@ def serve_one_at_a_time(requests, rtol: float = 1e-8, realtime: bool = True, dev
             if wait > 0:
                 time.sleep(wait)
         adm = time.perf_counter() - t0
-        force, b, n = prepared[req.id] if prepared else prepare(req, device)
-        op = MatrixFreeOperator(force, OperatorCoefficients())
-        cg = solvers[req.id] if solvers else ConjugateGradient(SolveOptions(relative_tolerance=rtol))
-        cg.setup(op)  # the Jacobi diagonal, as the engine builds it at admission
-        bt = torch.as_tensor(b, device=dev)
-        x = torch.zeros(n, dtype=torch.float64, device=dev)
-        res = cg.solve(bt, x)
-        xh = x.cpu().numpy()
+        if isinstance(req, J2Request):
+            if prepared:
+                force, f, mon, n = prepared[req.id]
+            else:
+                mesh, fh, mon, n = prepare_j2(req, device)
+                force, f = InternalForce(mesh, device=device), torch.as_tensor(fh, device=dev)
+            xh, res = solve_j2_alone(req, force, f, mon, solvers[req.id] if solvers else None)
+        else:
+            force, b, n = prepared[req.id] if prepared else prepare(req, device)
+            op = MatrixFreeOperator(force, OperatorCoefficients())
+            cg = solvers[req.id] if solvers else ConjugateGradient(SolveOptions(relative_tolerance=rtol))
+            cg.setup(op)  # the Jacobi diagonal, as the engine builds it at admission
+            bt = torch.as_tensor(b, device=dev)
+            x = torch.zeros(n, dtype=torch.float64, device=dev)
+            res = cg.solve(bt, x)
+            xh = x.cpu().numpy()
         done = time.perf_counter() - t0
         served.append(Served(req.id, xh, res, req.arrival if realtime else 0.0, adm, done))
     return served, time.perf_counter() - t0

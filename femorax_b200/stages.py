@@ -32,16 +32,19 @@ class PathResult:
     cg: np.ndarray               # CG iterations per step
     plastic: np.ndarray          # plastic points at each step's last force evaluation
     converged: bool
+    u: np.ndarray = None         # the displacements after the last step (host)
 
 
 def load_path(force, fext_unit, factors, monitor_eq: int, tol: float = 1e-6, test: str = "NormUnbalance",
-              cg_rtol: float = 1e-12, max_newton: int = 25, stream=None) -> PathResult:
+              cg_rtol: float = 1e-12, max_newton: int = 25, stream=None, solver=None) -> PathResult:
     """Run the load path f_ext = factor * fext_unit (device vector) on `force`; displacements start
-    at zero and the material state at its committed state."""
+    at zero and the material state at its committed state. `solver`: a ConjugateGradient made
+    beforehand (its work vectors allocated), or None to make one."""
     import torch
     n = force.num_equations
     dev = fext_unit.device
-    solver = ConjugateGradient(SolveOptions(relative_tolerance=cg_rtol, max_iterations=20000))
+    if solver is None:
+        solver = ConjugateGradient(SolveOptions(relative_tolerance=cg_rtol, max_iterations=20000))
     solver.setup(MatrixFreeOperator(force, OperatorCoefficients(1.0, 0.0, 0.0)), stream)
     u = torch.zeros(n, dtype=torch.float64, device=dev)
     mon, nit, cgit, npl = [], [], [], []
@@ -55,7 +58,8 @@ def load_path(force, fext_unit, factors, monitor_eq: int, tol: float = 1e-6, tes
         mon.append(float(u[monitor_eq].item()))
         nit.append(it)
         cgit.append(res.iterations)
-    return PathResult(np.asarray(factors, float), np.array(mon), np.array(nit), np.array(cgit), np.array(npl), ok)
+    return PathResult(np.asarray(factors, float), np.array(mon), np.array(nit), np.array(cgit), np.array(npl), ok,
+                      u.cpu().numpy())
 
 
 @dataclasses.dataclass

@@ -1,0 +1,64 @@
+"""The serving loop on the device with a mixed stream: static elastic solves (BatchEngine slots)
+and J2 load paths (J2Lane cohorts) at once. Each J2 result is bit for bit the load path alone
+(serving.solve_j2_alone: plain Newton with Jacobi-PCG on an InternalForce of that mesh), and
+each static solution bit for bit the same request served alone."""
+import numpy as np
+import pytest
+import torch
+
+import femorax_b200 as fx
+from femorax_b200 import serving
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+RTOL = 1e-8
+
+
+def engine():
+    return fx.BatchEngine(1 << 22, 8, options=fx.SolveOptions(relative_tolerance=RTOL))
+
+
+STREAM = [serving.Request(0, 6, 5, 9, E=70e6, nu=0.3),
+          serving.J2Request(1, 1, 1, 24, E=60e6, sigma_y=80e3, total=0.0, steps_per_cycle=4),
+          serving.Request(2, 4, 4, 12, E=120e6, nu=0.35),
+          serving.J2Request(3, 2, 2, 30, E=90e6, sigma_y=150e3, total=0.0, steps_per_cycle=4),
+          serving.J2Request(4, 1, 1, 21, E=45e6, sigma_y=60e3, total=0.0, steps_per_cycle=4),
+          serving.Request(5, 7, 3, 5, E=50e6, nu=0.25)]
+
+
+def with_loads(stream):
+    """J2 loads at 1.2 times the force that first yields the base in elastic bending."""
+    out = []
+    for r in stream:
+        if isinstance(r, serving.J2Request):
+            b, L = r.nx * r.h, r.nz * r.h
+            r = serving.J2Request(r.id, r.nx, r.ny, r.nz, r.E, r.sigma_y, 1.2 * r.sigma_y * b ** 3 / (6.0 * L), r.h,
+                                  r.cycles, r.steps_per_cycle, arrival=0.001 * r.id)
+        else:
+            r = serving.Request(r.id, r.nx, r.ny, r.nz, r.E, r.nu, r.q, r.h, arrival=0.001 * r.id)
+        out.append(r)
+    return out
+
+
+def test_mixed_stream_same_alone_and_in_the_mix():
+    stream = with_loads(STREAM)
+    srv = serving.Server(engine(), hbm_budget=1 << 34, max_cohort=2)
+    served, wall = srv.run(stream, realtime=False)
+    assert sorted(s.id for s in served) == [r.id for r in stream]
+    by_id = {s.id: s for s in served}
+    for r in stream:
+        s = by_id[r.id]
+        assert s.result.converged, r.id
+        if isinstance(r, serving.J2Request):
+            mesh, f, mon, n = serving.prepare_j2(r)
+            force = fx.InternalForce(mesh)
+            u, res = serving.solve_j2_alone(r, force, torch.as_tensor(f, device=DEV), mon)
+            assert np.array_equal(s.x, u), r.id
+            assert np.array_equal(s.result.monitor, res.monitor), r.id
+            assert np.array_equal(s.result.newton, res.newton), r.id
+        else:
+            alone, _ = serving.Server(engine(), hbm_budget=1 << 34).run([r], realtime=False)
+            assert np.array_equal(s.x, alone[0].x), r.id
+    assert srv.resident == 0
+    summ = serving.summary(served, wall)
+    assert summ["converged"] == len(stream)
