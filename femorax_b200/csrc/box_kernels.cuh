@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(BX* BY, MINB)
 
 // ------------------------------------------------------------------ launch variants
 // (BX, BY, CTAs per SM for the register budget, face caching)
-constexpr int kNumVariants = 9;  // see launch()
+constexpr int kNumVariants = 10;  // see launch()
 
 template <class T>
 const BoxTable<typename Coef<T>::type>& table_of(const BoxPlan& p, int mode);
@@ -618,7 +618,8 @@ void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     case 5: return launch_one<16, 8, 5, false, T, MODE>(p, a, st);
     case 6: return launch_one<16, 8, 6, false, T, MODE>(p, a, st);
     case 7: return launch_one<32, 4, 4, false, T, MODE>(p, a, st);
-    default: return launch_one<16, 32, 1, false, T, MODE>(p, a, st);
+    case 8: return launch_one<16, 32, 1, false, T, MODE>(p, a, st);
+    default: return launch_one<16, 8, 3, true, T, MODE>(p, a, st);
   }
 }
 

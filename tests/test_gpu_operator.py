@@ -167,22 +167,29 @@ def test_box_rejected_for_ties():
 
 def test_launch_variants_agree(oracle_mod):
     """Every launch shape and plane count, as a grid or persistent (negative kz), gives the same bits
-    (the owner sums in a fixed order)."""
+    (the owner sums in a fixed order): the operator and the internal force."""
     mesh, force, _ = build(meshes.layered_box(33, 17, 21, layers=3, seed=1)[0])
     k = fx.OperatorCoefficients(1.0, 0.1, 2.0)
-    x = t(np.random.default_rng(15).standard_normal(mesh.num_equations))
-    ref = None
+    rng = np.random.default_rng(15)
+    x = t(rng.standard_normal(mesh.num_equations))
+    v = t(rng.standard_normal(mesh.num_equations))
+    ref = fref = None
     from femorax_b200 import _lib as L
-    import ctypes as C
     lib = L.lib()
-    for variant in range(9):
+    for variant in range(10):
         for kz in (1, 3, 8, 64, -3, -8):
-            lib_rc = lib.fx_force_set_launch(force._h, variant, kz) if hasattr(lib, "fx_force_set_launch") else None
-            if lib_rc is None:
-                pytest.skip("no launch override")
-            L.check(lib_rc)
+            L.check(lib.fx_force_set_launch(force._h, variant, kz))
             y = torch.zeros(mesh.num_equations, dtype=torch.float64, device=DEV)
             force.apply_operator(k, x, y)
+            f = torch.zeros_like(y)
+            try:
+                force.compute(x, v, f)
+            except fx.FxError as e:  # u and v staged together exceed a CTA's shared memory
+                assert e.code == 2 and variant in (3, 8), (variant, kz)
+                f = None
             if ref is None:
                 ref = y.clone()
+            if fref is None and f is not None:
+                fref = f.clone()
             assert torch.equal(y, ref), (variant, kz)
+            assert f is None or torch.equal(f, fref), (variant, kz)
