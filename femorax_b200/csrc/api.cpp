@@ -344,7 +344,9 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
         if (o && *o && std::sscanf(o, "%d,%d", &variant, &kz) == 2) fx::box_set_launch(s, variant, kz);
         else fx::box_autotune(s, nullptr);
       }
-      FX_CUDA(cudaDeviceSynchronize());
+      // the creation's work is on the legacy stream; a device-wide synchronization would also wait
+      // for (and break the capture of) another thread's graph capture on its own stream
+      FX_CUDA(cudaStreamSynchronize(nullptr));
     } catch (...) {
       delete h;
       throw;

@@ -72,8 +72,10 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
   double acc = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes)
-      acc = fma(static_cast<double>(x[begin + k]), static_cast<double>(y[begin + k]), acc);
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{x[i], y[i]}}; },
+                 [&](int64_t, const Ops<T, 2>& o) {
+                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
+                 });
   double total = 0.0;
   for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
   if (lane == 0) part[c] = total;
@@ -112,14 +114,16 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  for (int64_t k = lane; k < len; k += 32) r[begin + k] = b[begin + k] - ap[begin + k];
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{b[i], ap[i]}}; },
+               [&](int64_t i, const Ops<double, 2>& o) { r[i] = o.v[0] - o.v[1]; });
   __syncwarp();
   double srr = 0.0, sbb = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      srr = fma(r[begin + k], r[begin + k], srr);
-      sbb = fma(b[begin + k], b[begin + k], sbb);
-    }
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 2>{{r[i], b[i]}}; },
+                 [&](int64_t, const Ops<double, 2>& o) {
+                   srr = fma(o.v[0], o.v[0], srr);
+                   sbb = fma(o.v[1], o.v[1], sbb);
+                 });
   double trr = 0.0, tbb = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
@@ -178,23 +182,23 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  for (int64_t k = lane; k < len; k += 32) {
-    const int64_t i = begin + k;
-    r32[i] = static_cast<float>(r[i]);
-    d[i] = 0.f;
-  }
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 1>{{r[i]}}; },
+               [&](int64_t i, const Ops<double, 1>& o) {
+                 r32[i] = static_cast<float>(o.v[0]);
+                 d[i] = 0.f;
+               });
   __syncwarp();
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      const int64_t i = begin + k;
-      const float ri = fmaf(-1.f, 0.f, r32[i]);
-      const float zi = inv[i] * ri;
-      rr[i] = ri;
-      p[i] = zi;
-      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
-      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
-    }
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<float, 2>{{r32[i], inv[i]}}; },
+                 [&](int64_t i, const Ops<float, 2>& o) {
+                   const float ri = fmaf(-1.f, 0.f, o.v[0]);
+                   const float zi = o.v[1] * ri;
+                   rr[i] = ri;
+                   p[i] = zi;
+                   srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+                   srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+                 });
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
@@ -257,15 +261,15 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      const int64_t i = begin + k;
-      d[i] = fmaf(alpha, p[i], d[i]);
-      const float ri = fmaf(-alpha, ap[i], rr[i]);
-      rr[i] = ri;
-      const float zi = inv[i] * ri;
-      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
-      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
-    }
+    lane_loop<4>(begin, len, lane, lanes, [&](int64_t i) { return Ops<float, 5>{{p[i], ap[i], inv[i], d[i], rr[i]}}; },
+                 [&](int64_t i, const Ops<float, 5>& o) {
+                   d[i] = fmaf(alpha, o.v[0], o.v[3]);
+                   const float ri = fmaf(-alpha, o.v[1], o.v[4]);
+                   rr[i] = ri;
+                   const float zi = o.v[2] * ri;
+                   srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+                   srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+                 });
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
@@ -314,10 +318,8 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  for (int64_t k = lane; k < len; k += 32) {
-    const int64_t i = begin + k;
-    p[i] = fmaf(beta, p[i], inv[i] * rr[i]);
-  }
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<float, 3>{{p[i], inv[i], rr[i]}}; },
+               [&](int64_t i, const Ops<float, 3>& o) { p[i] = fmaf(beta, o.v[0], o.v[1] * o.v[2]); });
 }
 
 // x += (double) d for slots that ran an inner solve this round; the round's counters
@@ -332,7 +334,8 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  for (int64_t k = lane; k < len; k += 32) x[begin + k] += static_cast<double>(d[begin + k]);
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{static_cast<double>(d[i]), x[i]}}; },
+               [&](int64_t i, const Ops<double, 2>& o) { x[i] = o.v[1] + o.v[0]; });
 }
 
 __global__ void k_b_round_end(int* fl, const int* used, int nslots) {

@@ -45,7 +45,7 @@ void build_coef(ForceState& s, int mode, const double k[3]) {
     double l2m, lam, mu;
     lame(q, l2m, lam, mu);
     double sk = 1.0, sm = 0.0;
-    if (mode == 0) {
+    if (mode != 1) {  // the operator (0) or the mass product (2): factors of the coefficients k
       const OpFactors f = op_factors(q, k[0], k[1], k[2]);
       sk = f.cK + f.c0 + f.cc;
       sm = f.cM;
@@ -336,10 +336,11 @@ static BoxArgs<T> args(const ForceState& s, int mode, const T* x, const T* v, T*
   const BoxPlan::CoefSet& cs = s.box.cset[mode];
   const void* coef = sizeof(T) == 8 ? static_cast<const void*>(cs.coef.ptr) : static_cast<const void*>(cs.coef32.ptr);
   BoxArgs<T> a{};
+  a.cset = mode;
   a.nx = s.box.nx;
   a.ny = s.box.ny;
   a.nz = s.box.nz;
-  a.kz = s.box.shape[sizeof(T) == 4 ? 1 : 0][mode].kz;
+  a.kz = s.box.shape[sizeof(T) == 4 ? 1 : 0][mode == 1 ? 1 : 0].kz;
   a.nparams = s.nparams;
   a.node_eq = s.box.node_eq.ptr;
   a.elem_param = s.box.elem_param.ptr;
@@ -395,6 +396,17 @@ static void force_w_t(ForceState& s, const T* w, const T* v, T* f, cudaStream_t 
   a.kz = s.box.shape[sizeof(T) == 4 ? 1 : 0][0].kz;  // one staged vector: the apply's shape
   a.nm2 = s.box.la.ptr;
   launch<T, 2>(s.box, a, st);
+}
+
+void box_mass_apply(ForceState& s, const double* x, double* y, cudaStream_t st) {
+  const double k[3] = {0.0, 0.0, 1.0};
+  ensure_coef(s, 2, k);
+  BoxArgs<double> a = args<double>(s, 2, x, nullptr, y);
+  if (s.has_nodal_mass) {
+    a.nm1 = s.nodal_mass.ptr;
+    a.c1 = 1.0;
+  }
+  launch<double, 0>(s.box, a, st);
 }
 
 void box_force_w(ForceState& s, const double* w, const double* v, double* f, cudaStream_t st) {

@@ -54,6 +54,7 @@ struct BoxArgs {
   const T* __restrict__ escale;  // per-element E scale (sets that differ only in E), or NULL
   int* queue;       // persistent launch: [next tile, CTAs done]; NULL: one CTA per tile (the grid)
   int gx, gy, gz;   // tiles per axis (persistent launch)
+  int cset;         // (host side) the coefficient set whose tables the launch passes
 };
 
 template <class T>
@@ -586,9 +587,9 @@ void launch_kernel(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     b.gz = static_cast<int>(grid.z);
     const int ntiles = b.gx * b.gy * b.gz;
     const int ctas = std::min(ntiles, resident * num_sms());
-    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p, MODE == 0 ? 0 : 1));
+    kern<<<ctas, BX * BY, S::bytes, st>>>(b, table_of<T>(p, a.cset));
   } else {
-    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p, MODE == 0 ? 0 : 1));
+    kern<<<grid, BX * BY, S::bytes, st>>>(a, table_of<T>(p, a.cset));
   }
   FX_LAUNCH_CHECK("box_operator");
 }

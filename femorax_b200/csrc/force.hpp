@@ -101,9 +101,9 @@ struct BoxPlan {
   bool full = false;     // every grid node has all three DOFs free or none
   DeviceArray<double> escale;   // [nz ny nx]: E_e / E_ref
   DeviceArray<float> escale32;
-  // The coefficient tables of one kernel mode (0: the operator for the last operator
-  // coefficients k, 1: the internal force), each kept until its coefficients change, so that a
-  // solve that alternates forces and operator applies builds them once.
+  // The coefficient tables of one use (0: the operator for the last operator coefficients k, 1: the
+  // internal force, 2: the mass product M x), each kept until its coefficients change, so that a
+  // solve that alternates forces, mass products and operator applies builds them once.
   struct CoefSet {
     DeviceArray<BoxCoef> coef;  // per parameter set (neither layered nor scaled)
     DeviceArray<BoxCoef32> coef32;
@@ -113,7 +113,7 @@ struct BoxPlan {
     DeviceArray<BoxScaled32> scoef32;
     double k[3] = {0, 0, 0};
     bool built = false;
-  } cset[2];
+  } cset[3];
 };
 
 // Buffers of the explicit step loop (ground motion, step counter, force, recorded history),
@@ -190,6 +190,8 @@ void box_apply_f32(ForceState& s, const double k[3], const float* x, float* y, c
 void box_prepare(ForceState& s, const double k[3]);
 void box_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void box_force_f32(ForceState& s, const float* u, const float* v, float* f, cudaStream_t st);
+// y = M x (element masses, consistent or lumped, and nodal masses) on the box path
+void box_mass_apply(ForceState& s, const double* x, double* y, cudaStream_t st);
 // the box force from w = u + beta v formed by the caller with fma(beta, v, u), as the force kernel
 // forms it (the same values), v for the lumped alphaM term: one staged vector instead of two
 void box_force_w(ForceState& s, const double* w, const double* v, double* f, cudaStream_t st);

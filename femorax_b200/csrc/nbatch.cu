@@ -56,7 +56,8 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
   double acc = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) acc = fma(x[begin + k], y[begin + k], acc);
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 2>{{x[i], y[i]}}; },
+                 [&](int64_t, const Ops<double, 2>& o) { acc = fma(o.v[0], o.v[1], acc); });
   double total = 0.0;
   for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
   if (lane == 0) part[c] = total;
@@ -91,7 +92,8 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int s = owner[c];
   if (s < 0 || fl[s * NNF + G_NEWTON_DONE]) return;
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  for (int64_t k = lane; k < len; k += 32) r[begin + k] = fext[begin + k] - r[begin + k];
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{fext[i], r[i]}}; },
+               [&](int64_t i, const Ops<double, 2>& o) { r[i] = o.v[0] - o.v[1]; });
 }
 
 // the Newton test per instance (NormUnbalance, absolute); instances that continue start a CG
@@ -135,15 +137,15 @@ __global__ void __launch_bounds__(32 * kWarps)
   for (int64_t k = lane; k < len; k += 32) du[begin + k] = 0.0;
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      const int64_t i = begin + k;
-      const double ri = fma(-1.0, 0.0, r[i]);
-      const double zi = inv[i] * ri;
-      rr[i] = ri;
-      p[i] = zi;
-      srr = fma(ri, ri, srr);
-      srz = fma(ri, zi, srz);
-    }
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 2>{{r[i], inv[i]}}; },
+                 [&](int64_t i, const Ops<double, 2>& o) {
+                   const double ri = fma(-1.0, 0.0, o.v[0]);
+                   const double zi = o.v[1] * ri;
+                   rr[i] = ri;
+                   p[i] = zi;
+                   srr = fma(ri, ri, srr);
+                   srz = fma(ri, zi, srz);
+                 });
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
@@ -202,15 +204,16 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      const int64_t i = begin + k;
-      du[i] = fma(alpha, p[i], du[i]);
-      const double ri = fma(-alpha, ap[i], rr[i]);
-      rr[i] = ri;
-      const double zi = inv[i] * ri;
-      srr = fma(ri, ri, srr);
-      srz = fma(ri, zi, srz);
-    }
+    lane_loop<4>(begin, len, lane, lanes,
+                 [&](int64_t i) { return Ops<double, 5>{{p[i], ap[i], inv[i], du[i], rr[i]}}; },
+                 [&](int64_t i, const Ops<double, 5>& o) {
+                   du[i] = fma(alpha, o.v[0], o.v[3]);
+                   const double ri = fma(-alpha, o.v[1], o.v[4]);
+                   rr[i] = ri;
+                   const double zi = o.v[2] * ri;
+                   srr = fma(ri, ri, srr);
+                   srz = fma(ri, zi, srz);
+                 });
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
@@ -255,10 +258,8 @@ __global__ void __launch_bounds__(32 * kWarps)
   if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
   const double beta = sc[s * NNS + N_BETA];
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  for (int64_t k = lane; k < len; k += 32) {
-    const int64_t i = begin + k;
-    p[i] = fma(beta, p[i], inv[i] * rr[i]);
-  }
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 3>{{p[i], inv[i], rr[i]}}; },
+               [&](int64_t i, const Ops<double, 3>& o) { p[i] = fma(beta, o.v[0], o.v[1] * o.v[2]); });
 }
 
 // u += du for instances that solved this iteration; their counters
@@ -271,7 +272,8 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int s = owner[c];
   if (s < 0 || fl[s * NNF + G_NEWTON_DONE]) return;
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  for (int64_t k = lane; k < len; k += 32) u[begin + k] += du[begin + k];
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{u[i], du[i]}}; },
+               [&](int64_t i, const Ops<double, 2>& o) { u[i] = o.v[0] + o.v[1]; });
 }
 
 __global__ void k_nb_iteration_end(int* fl, int count) {
@@ -530,7 +532,9 @@ int fx_nbatch_create(const fx_mesh* meshes, int32_t count, int32_t device, fx_so
       b.fl.alloc(static_cast<size_t>(count) * fx::NNF);
       FX_CUDA(cudaMallocHost(&b.fl_h, sizeof(int) * fx::NNF * count));
       FX_CUDA(cudaMallocHost(&b.sc_h, sizeof(double) * fx::NNS * count));
-      FX_CUDA(cudaDeviceSynchronize());
+      // the creation's work is on the legacy stream; a device-wide synchronization would also wait
+      // for (and break the capture of) another thread's graph capture on its own stream
+      FX_CUDA(cudaStreamSynchronize(nullptr));
     } catch (...) {
       delete h;
       throw;

@@ -10,6 +10,7 @@
 // solve is done, so the iterate is frozen at the converged one. All reductions use the
 // documented chunk/lane order (fused multiply-adds), so a solve gives the same bits every run.
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <vector>
 
@@ -37,6 +38,15 @@ namespace fx {
 namespace {
 
 constexpr int kWarps = 8;
+// A lane's sum runs over its entries in index order (the documented order), but the operands of
+// kAhead consecutive iterations are fetched before their products are added, so that a warp has
+// that many loads in flight per vector instead of one: the chunks are few per SM, and one load
+// at a time leaves them waiting on memory latency.
+constexpr int kAhead = 8;
+
+// the scalar steps of an iteration (alpha, then the test and beta), defined below
+__device__ void cg_alpha_step(double* sc, int* fl);
+__device__ void cg_beta_step(double* sc, int* fl, int max_it);
 
 // documented-order chunk sums of x.y for vectors of type T, accumulated in double
 template <class T>
@@ -48,11 +58,51 @@ __global__ void __launch_bounds__(32 * kWarps) k_dot_chunks(const T* __restrict_
   const int64_t begin = c * kChunk;
   const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
   double s = 0.0;
-  if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) s = fma(static_cast<double>(x[begin + k]), static_cast<double>(y[begin + k]), s);
+  if (lane < lanes) {
+    int64_t k = lane;
+    for (; k + (kAhead - 1) * lanes < len; k += kAhead * lanes) {
+      T a[kAhead], b[kAhead];
+#pragma unroll
+      for (int u = 0; u < kAhead; ++u) {
+        a[u] = x[begin + k + u * lanes];
+        b[u] = y[begin + k + u * lanes];
+      }
+#pragma unroll
+      for (int u = 0; u < kAhead; ++u) s = fma(static_cast<double>(a[u]), static_cast<double>(b[u]), s);
+    }
+    for (; k < len; k += lanes) s = fma(static_cast<double>(x[begin + k]), static_cast<double>(y[begin + k]), s);
+  }
   double total = 0.0;
   for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, s, j);
   if (lane == 0) out[c] = total;
+}
+
+// chunk sums of p.Ap; then, in the grid's last block, their levels (into S_PAP) and the alpha step
+template <class T>
+__global__ void __launch_bounds__(32 * kWarps) k_cg_pap(const T* __restrict__ p, const T* __restrict__ ap, int64_t n,
+                                                        int lanes, int64_t nchunks, double* __restrict__ out,
+                                                        double* __restrict__ out2, unsigned* __restrict__ counter,
+                                                        double* __restrict__ sc, int* __restrict__ fl) {
+  if (fl[F_DONE]) return;  // (the same for every block: the counter stays untouched)
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  const int64_t begin = c * kChunk;
+  const int64_t len = c >= nchunks ? 0 : ((n - begin < kChunk) ? n - begin : kChunk);
+  double s = 0.0;
+  if (lane < lanes)
+    lane_loop<kAhead>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{p[i], ap[i]}}; },
+                      [&](int64_t, const Ops<T, 2>& o) {
+                        s = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), s);
+                      });
+  double total = 0.0;
+  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, s, j);
+  if (lane == 0 && c < nchunks) out[c] = total;
+  if (!last_block(counter)) return;
+  block_levels(out, out2, nchunks, 1, lanes, sc + S_PAP);
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    cg_alpha_step(sc, fl);
+  }
 }
 
 // r = b - ap; z = inv r; p = z; chunk sums of r.r and r.z (columns 0 and 1 of out)
@@ -67,16 +117,31 @@ __global__ void __launch_bounds__(32 * kWarps) k_cg_begin(const T* __restrict__ 
   const int64_t begin = c * kChunk;
   const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
   double srr = 0.0, srz = 0.0;
-  if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      const int64_t i = begin + k;
-      const T ri = fma(T(-1), ap[i], b[i]);
-      const T zi = inv[i] * ri;
-      r[i] = ri;
-      p[i] = zi;
-      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
-      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+  auto one = [&](int64_t i, T bi, T ai, T vi) {
+    const T ri = fma(T(-1), ai, bi);
+    const T zi = vi * ri;
+    r[i] = ri;
+    p[i] = zi;
+    srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+    srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+  };
+  if (lane < lanes) {
+    constexpr int U = kAhead / 2;
+    int64_t k = lane;
+    for (; k + (U - 1) * lanes < len; k += U * lanes) {
+      T bv[U], av[U], vv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t i = begin + k + u * lanes;
+        bv[u] = b[i];
+        av[u] = ap[i];
+        vv[u] = inv[i];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) one(begin + k + u * lanes, bv[u], av[u], vv[u]);
     }
+    for (; k < len; k += lanes) one(begin + k, b[begin + k], ap[begin + k], inv[begin + k]);
+  }
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
@@ -88,39 +153,66 @@ __global__ void __launch_bounds__(32 * kWarps) k_cg_begin(const T* __restrict__ 
   }
 }
 
-// x += alpha p; r -= alpha ap; chunk sums of r.r and r.z
+// x += alpha p; r -= alpha ap; chunk sums of r.r and r.z; then, in the grid's last block, their
+// levels (into S_RR, S_RZNEW) and the beta step: the convergence test, the iteration count, beta
 template <class T>
-__global__ void __launch_bounds__(32 * kWarps) k_cg_update(const double* __restrict__ sc, const int* __restrict__ fl,
+__global__ void __launch_bounds__(32 * kWarps) k_cg_update(double* __restrict__ sc, int* __restrict__ fl,
                                                            const T* __restrict__ p, const T* __restrict__ ap,
                                                            const T* __restrict__ inv, T* __restrict__ x,
                                                            T* __restrict__ r, int64_t n, int lanes, int64_t nchunks,
-                                                           double* __restrict__ out) {
-  if (fl[F_DONE]) return;
+                                                           double* __restrict__ out, double* __restrict__ out2,
+                                                           unsigned* __restrict__ counter, int max_it) {
+  if (fl[F_DONE]) return;  // (the same for every block: the counter stays untouched)
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
   const T alpha = static_cast<T>(sc[S_ALPHA]);
   const int64_t begin = c * kChunk;
-  const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
+  const int64_t len = c >= nchunks ? 0 : ((n - begin < kChunk) ? n - begin : kChunk);
   double srr = 0.0, srz = 0.0;
-  if (lane < lanes)
-    for (int64_t k = lane; k < len; k += lanes) {
-      const int64_t i = begin + k;
-      x[i] = fma(alpha, p[i], x[i]);
-      const T ri = fma(-alpha, ap[i], r[i]);
-      r[i] = ri;
-      const T zi = inv[i] * ri;
-      srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
-      srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+  auto one = [&](int64_t i, T pi, T ai, T vi, T xi, T ri0) {
+    x[i] = fma(alpha, pi, xi);
+    const T ri = fma(-alpha, ai, ri0);
+    r[i] = ri;
+    const T zi = vi * ri;
+    srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+    srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+  };
+  if (lane < lanes) {
+    constexpr int U = kAhead / 2;
+    int64_t k = lane;
+    for (; k + (U - 1) * lanes < len; k += U * lanes) {
+      T pv[U], av[U], vv[U], xv[U], rv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t i = begin + k + u * lanes;
+        pv[u] = p[i];
+        av[u] = ap[i];
+        vv[u] = inv[i];
+        xv[u] = x[i];
+        rv[u] = r[i];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) one(begin + k + u * lanes, pv[u], av[u], vv[u], xv[u], rv[u]);
     }
+    for (; k < len; k += lanes) {
+      const int64_t i = begin + k;
+      one(i, p[i], ap[i], inv[i], x[i], r[i]);
+    }
+  }
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
     trr += __shfl_sync(0xffffffffu, srr, j);
     trz += __shfl_sync(0xffffffffu, srz, j);
   }
-  if (lane == 0) {
+  if (lane == 0 && c < nchunks) {
     out[c] = trr;
     out[nchunks + c] = trz;
+  }
+  if (!last_block(counter)) return;
+  block_levels(out, out2, nchunks, 2, lanes, sc + S_RR);
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    cg_beta_step(sc, fl, max_it);
   }
 }
 
@@ -148,7 +240,7 @@ __global__ void k_cg_start(double* sc, int* fl, double rtol, double atol, int ma
   fl[F_DONE] = fl[F_CONV] || max_it <= 0;
 }
 
-__global__ void k_cg_alpha(double* sc, int* fl) {
+__device__ void cg_alpha_step(double* sc, int* fl) {
   if (fl[F_DONE]) return;
   const double pap = sc[S_PAP];
   if (!(pap > 0.0)) {
@@ -159,7 +251,7 @@ __global__ void k_cg_alpha(double* sc, int* fl) {
   sc[S_ALPHA] = sc[S_RZ] / pap;
 }
 
-__global__ void k_cg_beta(double* sc, int* fl, int max_it) {
+__device__ void cg_beta_step(double* sc, int* fl, int max_it) {
   if (fl[F_DONE]) return;
   const double rn = sqrt(sc[S_RR]);
   sc[S_RNORM] = rn;
@@ -175,6 +267,13 @@ __global__ void k_cg_beta(double* sc, int* fl, int max_it) {
   }
   sc[S_BETA] = sc[S_RZNEW] / sc[S_RZ];
   sc[S_RZ] = sc[S_RZNEW];
+}
+
+// The condition of the CG loop graph: another iteration while the solve is not done, at most
+// `cap` passes (a bound the solve's own max_it already keeps below).
+__global__ void k_cg_cond(cudaGraphConditionalHandle h, const int* __restrict__ fl, int* __restrict__ passes, int cap) {
+  const int c = ++*passes;
+  cudaGraphSetConditional(h, (!fl[F_DONE] && c < cap) ? 1u : 0u);
 }
 
 __global__ void k_count_zero(const double* __restrict__ d, int64_t n, int* count) {
@@ -264,12 +363,30 @@ struct Solver {
   DeviceArray<double> sc;
   DeviceArray<int> fl;
   DeviceArray<int> zero_count;
+  DeviceArray<int> passes;  // the CG loop graph's pass counter
+  DeviceArray<unsigned> counter;  // the fused kernels' last-block counter (0 between launches)
   DeviceArray<double> V, Z, wv, hbuf;  // GMRES
   DeviceArray<double> nres, ndu;       // Newton: residual and increment
   DeviceArray<double> nut, nvt, nat;   // Newmark: the last step's u, v, a
   int* host_flags = nullptr;           // pinned
   double* host_sc = nullptr;           // pinned
+  // The CG loop graph of the last solve per precision (0: FP64, 1: FP32 inner), kept for the next
+  // solve on the same vectors (the Newton and Newmark loops, refinement rounds): capturing and
+  // instantiating it costs as much as several iterations. Dropped when setup changes the
+  // coefficients (the layered tables are kernel parameters captured with it).
+  struct CgGraph {
+    cudaGraphExec_t exec = nullptr;
+    const void* key[5] = {};
+    int max_it = 0;
+  } cg_graph[2];
+  void drop_graphs() {
+    for (auto& g : cg_graph) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g = CgGraph{};
+    }
+  }
   ~Solver() {
+    drop_graphs();
     if (cs) cudaStreamDestroy(cs);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
@@ -310,41 +427,63 @@ struct Solver {
     FX_LAUNCH_CHECK("cg_start");
     auto iteration = [&] {
       apply(pp, aa, fl.ptr + F_DONE);
-      k_dot_chunks<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(pp, aa, n, lanes, nc, w.level[0].ptr);
-      reduce_partials(w, nc, 1, sc.ptr + S_PAP, cs);
-      k_cg_alpha<<<1, 1, 0, cs>>>(sc.ptr, fl.ptr);
+      // p.Ap and alpha, then the update, r.r, r.z and beta (each with its levels in the kernel's
+      // last block), then p
+      k_cg_pap<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(pp, aa, n, lanes, nc, w.level[0].ptr, w.level[1].ptr,
+                                                         counter.ptr, sc.ptr, fl.ptr);
       k_cg_update<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, pp, aa, iv, x, rr, n, lanes, nc,
-                                                            w.level[0].ptr);
-      reduce_partials(w, nc, 2, sc.ptr + S_RR, cs);
-      k_cg_beta<<<1, 1, 0, cs>>>(sc.ptr, fl.ptr, max_it);
+                                                            w.level[0].ptr, w.level[1].ptr, counter.ptr, max_it);
       k_cg_p<T><<<ew(n), 256, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, pp, n);
       FX_LAUNCH_CHECK("cg_iteration");
     };
-    // the first block without a graph (it also builds any lazy state), then graphs of `block`
-    const int block = 8;
-    for (int i = 0; i < block; ++i) iteration();
-    read_state();
-    cudaGraphExec_t exec = nullptr;
-    while (!host_flags[F_DONE]) {
-      if (!exec) {
-        cudaGraph_t graph = nullptr;
-        FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    // The iterations run as one graph: a while node whose body is one iteration and the
+    // condition kernel, so the device loops until the solve is done with no host round trip.
+    // The begin above ran eagerly (its apply builds lazy state and this solver's coefficient
+    // tables); a new graph is captured when the vectors differ from the last solve's.
+    CgGraph& G = cg_graph[sizeof(T) == 4 ? 1 : 0];
+    const void* key[5] = {x, rr, pp, aa, iv};
+    if (G.exec && (std::memcmp(G.key, key, sizeof key) != 0 || G.max_it != max_it)) {
+      cudaGraphExecDestroy(G.exec);
+      G = CgGraph{};
+    }
+    if (!G.exec) {
+      cudaGraph_t g = nullptr;
+      FX_CUDA(cudaGraphCreate(&g, 0));
+      try {
+        cudaGraphConditionalHandle h;
+        FX_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        FX_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        FX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         try {
-          for (int i = 0; i < block; ++i) iteration();
+          iteration();
+          k_cg_cond<<<1, 1, 0, cs>>>(h, fl.ptr, passes.ptr, max_it + 2);
+          FX_LAUNCH_CHECK("cg_condition");
         } catch (...) {
-          cudaStreamEndCapture(cs, &graph);
-          if (graph) cudaGraphDestroy(graph);
+          cudaStreamEndCapture(cs, &body);
           throw;
         }
-        FX_CUDA(cudaStreamEndCapture(cs, &graph));
-        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        FX_CUDA(e);
+        FX_CUDA(cudaStreamEndCapture(cs, &body));
+        FX_CUDA(cudaGraphInstantiate(&G.exec, g, 0));
+      } catch (...) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G = CgGraph{};
+        cudaGraphDestroy(g);
+        throw;
       }
-      FX_CUDA(cudaGraphLaunch(exec, cs));
-      read_state();
+      cudaGraphDestroy(g);
+      std::memcpy(G.key, key, sizeof key);
+      G.max_it = max_it;
     }
-    if (exec) cudaGraphExecDestroy(exec);
+    FX_CUDA(cudaMemsetAsync(passes.ptr, 0, sizeof(int), cs));
+    FX_CUDA(cudaGraphLaunch(G.exec, cs));
+    read_state();
     res->converged = host_flags[F_CONV];
     res->iterations = host_flags[F_ITERS];
     res->indefinite = host_flags[F_INDEF];
@@ -592,6 +731,8 @@ int Solver::newmark(const double* fext, double* u, double* v, double* a, double 
     else general_force(fs, u, v, nres.ptr, cs);
     if (all_lumped) {
       k_mul<<<ew(n), 256, 0, cs>>>(fs.lumped_mass.ptr, a, nut.ptr, n);  // nut is free after the predict
+    } else if (fs.use_box()) {
+      box_mass_apply(fs, a, nut.ptr, cs);
     } else {
       const double km[3] = {0.0, 0.0, 1.0};
       const bool init = fs.initial;
@@ -691,6 +832,9 @@ int fx_solver_create(fx_force* f, int32_t method, fx_solve_opts o, fx_solver** o
       s.sc.alloc(S_NSCALAR);
       s.fl.alloc(F_NFLAG);
       s.zero_count.alloc(1);
+      s.passes.alloc(1);
+      s.counter.alloc(1);
+      FX_CUDA(cudaMemset(s.counter.ptr, 0, sizeof(unsigned)));
       s.hbuf.alloc(64);
       s.nres.alloc(n);
       s.ndu.alloc(n);
@@ -732,6 +876,7 @@ int fx_solver_setup(fx_solver* h, fx_coeffs k, void* stream) {
     if (!h) throw fx::Error(FX_E_INVALID, "fx_solver_setup: null handle");
     fx::Solver& s = h->s;
     auto st = static_cast<cudaStream_t>(stream);
+    s.drop_graphs();
     s.k[0] = k.stiffness;
     s.k[1] = k.damping;
     s.k[2] = k.mass;

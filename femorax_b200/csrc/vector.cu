@@ -28,13 +28,12 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_reduce_chunks(const dou
   const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
   double s = 0.0;
   if (lane < lanes) {
-    if (y) {
-#pragma unroll 8
-      for (int64_t k = lane; k < len; k += lanes) s = fma(xc[begin + k], y[begin + k], s);
-    } else {
-#pragma unroll 8
-      for (int64_t k = lane; k < len; k += lanes) s += xc[begin + k];
-    }
+    if (y)
+      lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 2>{{xc[i], y[i]}}; },
+                   [&](int64_t, const Ops<double, 2>& o) { s = fma(o.v[0], o.v[1], s); });
+    else
+      lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 1>{{xc[i]}}; },
+                   [&](int64_t, const Ops<double, 1>& o) { s += o.v[0]; });
   }
   // lane 0 adds the lane sums in lane order
   double total = 0.0;

@@ -8,7 +8,83 @@
 namespace fx {
 
 constexpr int64_t kChunk = 2048;
-inline int64_t chunks_of(int64_t n) { return (n + kChunk - 1) / kChunk; }
+__host__ __device__ inline int64_t chunks_of(int64_t n) { return (n + kChunk - 1) / kChunk; }
+
+// A lane's pass over a chunk in the documented order: use(i, load(i)) for i = begin + k,
+// k = lane, lane + lanes, ... < len, in that order, with the loads of U consecutive iterations
+// issued before their uses. A chunk is one warp's work and few warps share an SM, so one load in
+// flight at a time would leave the pass waiting on memory latency; the order of the uses (and so
+// of every sum) is unchanged.
+// the operands of one iteration of a lane_loop
+template <class T, int N>
+struct Ops {
+  T v[N];
+};
+
+template <int U, class Load, class Use>
+__device__ __forceinline__ void lane_loop(int64_t begin, int64_t len, int lane, int lanes, Load load, Use use) {
+  int64_t k = lane;
+  for (; k + (U - 1) * static_cast<int64_t>(lanes) < len; k += U * static_cast<int64_t>(lanes)) {
+    decltype(load(begin)) v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = load(begin + k + u * static_cast<int64_t>(lanes));
+#pragma unroll
+    for (int u = 0; u < U; ++u) use(begin + k + u * static_cast<int64_t>(lanes), v[u]);
+  }
+  for (; k < len; k += lanes) use(begin + k, load(begin + k));
+}
+
+// True in the last block of the grid to get here (a grid-wide counter, which that block resets
+// to 0 when it is done); every block's writes before the call are visible to it. Every thread of
+// the block must call it.
+__device__ __forceinline__ bool last_block(unsigned* counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  return last;
+}
+
+// The levels above a level of chunk sums, by one block, in the order of the level kernels
+// (k_reduce_chunks without y): `ncol` columns of n values at stride n in a, alternating with b
+// (each holding at least ncol * chunks_of(n) values), the sums in out[0 .. ncol). The values
+// were written by other blocks: read through L2.
+__device__ __forceinline__ void block_levels(double* a, double* b, int64_t n, int ncol, int lanes, double* out) {
+  const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+  const int nw = static_cast<int>(blockDim.x >> 5);
+  double* src = a;
+  double* dst = b;
+  for (;;) {
+    const int64_t nc = chunks_of(n);
+    for (int64_t item = warp; item < ncol * nc; item += nw) {
+      const int col = static_cast<int>(item / nc);
+      const int64_t c = item % nc;
+      const int64_t begin = c * kChunk;
+      const int64_t len = (n - begin < kChunk) ? n - begin : kChunk;
+      const double* x = src + col * n;
+      double s = 0.0;
+      if (lane < lanes)
+        lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 1>{{__ldcg(x + i)}}; },
+                     [&](int64_t, const Ops<double, 1>& o) { s += o.v[0]; });
+      double total = 0.0;
+      for (int j = 0; j < lanes; ++j) {
+        const double v = __shfl_sync(0xffffffffu, s, j);
+        total += v;
+      }
+      if (lane == 0) {
+        if (nc == 1) out[col] = total;
+        else dst[col * nc + c] = total;
+      }
+    }
+    __syncthreads();
+    if (nc == 1) return;
+    double* t = src;
+    src = dst;
+    dst = t;
+    n = nc;
+  }
+}
 
 // Partial sums for vectors of up to `capacity` entries (VectorOps' partial_[2]).
 struct ReduceWork {

@@ -85,6 +85,48 @@ def test_cg_warm_start_and_repeatability():
     assert r3.converged and r3.iterations == 0
 
 
+@pytest.mark.parametrize("name", ["per_set", "layered"])
+def test_cg_graph_kept_between_solves(name):
+    """A solver keeps its iteration graph for the next solve: the same vectors (graph reused),
+    other vectors (captured again), a setup with other coefficients (graph dropped), and an apply
+    with other coefficients between two solves (the coefficient tables rebuilt under it) all give
+    the bits of a fresh solver."""
+    spec = two_region_block(6, 5, 7) if name == "per_set" else meshes.layered_box(9, 8, 24, layers=3, seed=2)[0]
+    mesh, force, _ = build(spec)
+    n = mesh.num_equations
+    b = t(np.random.default_rng(4).standard_normal(n))
+    k1, k2 = fx.OperatorCoefficients(1.0, 0.2, 3.0), fx.OperatorCoefficients(1.0, 0.0, 50.0)
+    opts = fx.SolveOptions(relative_tolerance=1e-11)
+
+    def fresh(k):
+        s = fx.ConjugateGradient(opts)
+        s.setup(fx.MatrixFreeOperator(force, k))
+        x = torch.zeros(n, dtype=torch.float64, device=DEV)
+        r = s.solve(b, x)
+        assert r.iterations > 16  # past the eager block: the graph ran
+        return x, r.iterations
+
+    x_ref1, it1 = fresh(k1)
+    x_ref2, it2 = fresh(k2)
+    s = fx.ConjugateGradient(opts)
+    s.setup(fx.MatrixFreeOperator(force, k1))
+    xa = torch.zeros(n, dtype=torch.float64, device=DEV)
+    xb = torch.zeros(n, dtype=torch.float64, device=DEV)
+    for x in (xa, xa, xb):
+        x.zero_()
+        assert s.solve(b, x).iterations == it1
+        assert torch.equal(x, x_ref1)
+    y = torch.zeros_like(b)
+    force.apply_operator(k2, b, y)  # rebuilds the operator's coefficient tables for k2
+    xa.zero_()
+    s.solve(b, xa)
+    assert torch.equal(xa, x_ref1)
+    s.setup(fx.MatrixFreeOperator(force, k2))
+    xa.zero_()
+    assert s.solve(b, xa).iterations == it2
+    assert torch.equal(xa, x_ref2)
+
+
 def test_cg_indefinite_detection():
     """A negative stiffness coefficient makes p.Ap <= 0: CG reports indefinite, Krylov falls back."""
     mesh, force, _ = build(meshes.static_cube(4))
