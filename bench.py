@@ -19,7 +19,8 @@ own InternalForce::apply_operator (built here from its sources, oracle/_ref) on 
 `served` compares solves/s and p50/p99 latency at a 1e-8 FP64 residual on a stream of static solves:
 the batched mixed-precision engine behind the serving loop versus plain FP64 CG one at a time;
 `served_mixed` does the same on a stream of 70 % static solves and 30 % J2 load paths (J2 cohorts
-beside the engine's slots).
+beside the engine's slots); `served_rates` serves that mix with Poisson arrivals at 20, 200 and
+2000 requests/s in real time.
 
 The reference arm (--impl reference) times that reference CPU path alone, on every host thread.
 """
@@ -195,8 +196,8 @@ def explicit_comparison(force, mesh, comp, device, steps=4000):
     return out
 
 
-def newmark_comparison(device, n=48, steps=40, seed=0):
-    """The Newmark configuration on a bounded sample: a heterogeneous cube of n^3 boxes (per-element
+def newmark_comparison(device, n=100, steps=20, seed=0):
+    """The Newmark configuration on a bounded sample of its steps: a heterogeneous cube of n^3 boxes (per-element
     E log-normal, median 80 MPa, sigma 0.5; nu 0.3; base fixed), a harmonic horizontal surface load,
     Newmark beta 0.25 gamma 0.5 with one inner solve per step to a 1e-8 relative FP64 residual:
     plain FP64 CG against FP32 CG inside FP64 refinement. Steps/s by wall clock around each run
@@ -311,19 +312,18 @@ def serve_mixed_comparison(device, count=32, seed=2):
     from femorax_b200 import serving
     reqs = serving.mixed_stream(count, rate=1e9, j2_share=0.3, min_dof=1e4, max_dof=5e5, seed=seed,
                                 j2_sizes=(1, 2, 4, 8), j2_nz=(20, 40))
-    sy, b, L = 100e3, 0.5, 10.0
-    warm = [serving.Request(10_000, 4, 4, 4), serving.J2Request(10_001, 1, 1, 20, sigma_y=sy,
-                                                               total=1.2 * sy * b ** 3 / (6.0 * L))]
-    prepared, solvers = serving.resident(reqs + warm, device)
+    prepared, solvers = serving.resident(reqs, device)
     server_prep = {r.id: serving.prepare_j2(r, device) if isinstance(r, serving.J2Request) else prepared[r.id]
-                   for r in reqs + warm}
+                   for r in reqs}
     eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
 
     def server():
         return serving.Server(eng, hbm_budget=64 << 30, device=device, prepare_fn=lambda r, d: server_prep[r.id])
 
-    server().run(warm, realtime=False)  # untimed: module loading, first launches, graph set-up
-    serving.serve_one_at_a_time(warm, realtime=False, device=device, prepared=prepared, solvers=solvers)
+    # untimed: the whole stream once through each arm (module loading, first launches, graph
+    # set-up of every cohort and solver size), as a serving process that has run a while
+    server().run(reqs, realtime=False)
+    serving.serve_one_at_a_time(reqs, realtime=False, device=device, prepared=prepared, solvers=solvers)
     mixed, wall_m = server().run(reqs, realtime=False)
     plain, wall_p = serving.serve_one_at_a_time(reqs, 1e-8, realtime=False, device=device, prepared=prepared,
                                                 solvers=solvers)
@@ -339,6 +339,37 @@ def serve_mixed_comparison(device, count=32, seed=2):
             "plain_fp64_one_at_a_time": {k: p[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
             "speedup_solves_per_s": m["solves_per_s"] / p["solves_per_s"] if p["solves_per_s"] else None,
             "j2_bit_identical": bool(same)}
+
+
+def serve_rate_sweep(device, rates=(20.0, 200.0, 2000.0), count=24, seed=3):
+    """The mixed stream (70 % static solves, 30 % J2 load paths, sizes as serve_mixed_comparison)
+    with Poisson arrivals at each rate in `rates` requests/s, served in real time: solves/s and
+    p50/p99 latency from arrival to result, for the serving loop and for plain FP64 one at a
+    time."""
+    import femorax_b200 as fx
+    from femorax_b200 import serving
+    out = []
+    eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
+    warm = True
+    for i, rate in enumerate(rates):
+        reqs = serving.mixed_stream(count, rate=rate, j2_share=0.3, min_dof=1e4, max_dof=5e5, seed=seed + i,
+                                    j2_sizes=(1, 2, 4, 8), j2_nz=(20, 40))
+        prepared, solvers = serving.resident(reqs, device)
+        server_prep = {r.id: serving.prepare_j2(r, device) if isinstance(r, serving.J2Request) else prepared[r.id]
+                       for r in reqs}
+        srv = serving.Server(eng, hbm_budget=64 << 30, device=device, prepare_fn=lambda r, d: server_prep[r.id])
+        if warm:  # untimed: the first stream once through each arm, all at once
+            srv.run(reqs, realtime=False)
+            serving.serve_one_at_a_time(reqs, realtime=False, device=device, prepared=prepared, solvers=solvers)
+            warm = False
+        mixed, wall_m = srv.run(reqs, realtime=True)
+        plain, wall_p = serving.serve_one_at_a_time(reqs, 1e-8, realtime=True, device=device, prepared=prepared,
+                                                    solvers=solvers)
+        m, p = serving.summary(mixed, wall_m), serving.summary(plain, wall_p)
+        out.append({"rate_per_s": rate, "requests": count,
+                    "mixed_batched": {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
+                    "plain_fp64_one_at_a_time": {k: p[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")}})
+    return out
 
 
 def run_reference(args):
@@ -470,6 +501,7 @@ def run_ours(args):
     explicit = explicit_comparison(force, mesh, comp, local) if world == 1 and not args.no_serve else None
     served = serve_comparison(local) if world == 1 and not args.no_serve else None
     served_mixed = serve_mixed_comparison(local) if world == 1 and not args.no_serve else None
+    served_rates = serve_rate_sweep(local) if world == 1 and not args.no_serve else None
     batched_j2 = batched_j2_comparison(local) if world == 1 and not args.no_serve else None
     newmark = newmark_comparison(local) if world == 1 and not args.no_serve else None
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
@@ -491,6 +523,7 @@ def run_ours(args):
             "explicit": explicit,
             "served": served,
             "served_mixed": served_mixed,
+            "served_rates": served_rates,
             "batched_j2": batched_j2,
             "newmark": newmark}
     print(json.dumps(line))
