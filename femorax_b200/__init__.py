@@ -472,7 +472,8 @@ class LinearSolver:
     def newton(self, fext, u, tol: float = 1e-6, test: str = "NormUnbalance", max_newton: int = 25, stream=None):
         """Newton iterations of one quasi-static load step (fx_solver_newton) with the stage's
         absolute convergence test (NormUnbalance or NormDispIncr); u is updated in place; returns
-        (Newton iterations, SolveResult of the Newton test). CG solvers only."""
+        (Newton iterations, SolveResult of the Newton test). ConjugateGradient, or
+        MixedPrecisionSolver (FP32 CG on the tangent inside FP64 refinement)."""
         r = L.fx_solve_result()
         it = C.c_int32()
         t = L.FX_TEST_NORM_UNBALANCE if test == "NormUnbalance" else L.FX_TEST_NORM_DISP_INCR
@@ -516,7 +517,8 @@ class KrylovSolver(LinearSolver):
 
 
 class MixedPrecisionSolver(LinearSolver):
-    """FP32 PCG inside FP64 iterative refinement (box meshes)."""
+    """FP32 PCG inside FP64 iterative refinement (the FP32 operator: the box kernel, or the FP32
+    Gauss-point form on other meshes and J2 sets)."""
     METHOD = L.FX_SOLVER_IR
 
     def __init__(self, options: SolveOptions = None, inner_tolerance: float = 1e-4):

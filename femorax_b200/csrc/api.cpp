@@ -45,6 +45,7 @@ int64_t ForceState::device_bytes() const {
   b += box.node_eq.bytes() + box.elem_param.bytes() + box.escale.bytes() + box.escale32.bytes() + box.la.bytes();
   for (const auto& cs : box.cset) b += cs.coef.bytes() + cs.coef32.bytes() + cs.scoef.bytes() + cs.scoef32.bytes();
   b += j2_committed.bytes() + j2_trial.bytes() + j2_tan.bytes() + plastic_dev.bytes();
+  b += geom32.bytes() + nshape32.bytes() + slots32.bytes();
   return b;
 }
 
@@ -435,10 +436,10 @@ int fx_apply_operator_f32(fx_force* f, fx_coeffs k, const float* x, float* y, vo
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || (x && y)), "fx_apply_operator_f32: bad arguments");
     FX_REQUIRE(x != y, "fx_apply_operator_f32: x and y must not alias");
-    if (!f->s.use_box())
-      throw fx::Error(FX_E_UNSUPPORTED, "the FP32 operator runs on the box path only: " + f->s.box.why_not);
     const double kk[3] = {k.stiffness, k.damping, k.mass};
-    fx::box_apply_f32(f->s, kk, x, y, static_cast<cudaStream_t>(stream));
+    f->s.initial = k.initial != 0;
+    if (f->s.use_box()) fx::box_apply_f32(f->s, kk, x, y, static_cast<cudaStream_t>(stream));
+    else fx::general_apply_f32(f->s, kk, x, y, static_cast<cudaStream_t>(stream));
   });
 }
 

@@ -145,6 +145,7 @@ struct ForceState {
   DeviceArray<ParamGP> params;
   DeviceArray<int32_t> gstart, glist;  // per-equation slot lists in (element, DOF) order
   DeviceArray<double> slots;           // [24 * P]
+  DeviceArray<float> geom32, nshape32, slots32;  // FP32 operator: point geometry, shape values, slots
   DeviceArray<double> nodal_mass, nodal_alpha_mass, lumped_mass;
   DeviceArray<int8_t> eq_dof;
   bool has_nodal_mass = false, has_nodal_alpha = false;
@@ -168,6 +169,9 @@ struct ForceState {
 };
 
 // general.cu (Gauss-point path, built without fused multiply-adds)
+// the Gauss-point operator in FP32 (FP32 geometric factors built at the first call)
+void general_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st,
+                       const int* skip = nullptr);
 void general_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st,
                    const int* skip = nullptr);
 void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st);

@@ -106,7 +106,150 @@ __global__ void __launch_bounds__(256) k_gather(const int32_t* __restrict__ star
   y[q] = sum;
 }
 
+// ---- FP32 operator (the inner solves of FP32 CG in FP64 refinement on any mesh)
+// FP32 geometric factors of the Gauss points, computed once in FP64 by point_shape and rounded:
+// component c < 24 (dN/dx of node c % 8 along axis c / 8) and c = 24 (dvol) of point gp of
+// element e at [(c * 8 + gp) * P + e]; the shape values of the points (the same for every
+// element) at nshape[gp * 8 + k].
+constexpr int kGeom32 = 25;
+__global__ void __launch_bounds__(kBlock) k_geom32(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                    int32_t N, int32_t P, int32_t count, float* __restrict__ geom,
+                                                    float* __restrict__ nshape) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  double xl[3][8];
+  load_coords(coords, node, N, P, e, xl);
+  for (int gp = 0; gp < 8; ++gp) {
+    PointShape s;
+    point_shape(xl, gp, s);
+    for (int d = 0; d < 3; ++d)
+      for (int j = 0; j < 8; ++j) geom[static_cast<int64_t>(((d * 8 + j) * 8) + gp) * P + e] = static_cast<float>(s.dN[d][j]);
+    geom[static_cast<int64_t>(24 * 8 + gp) * P + e] = static_cast<float>(s.dvol);
+    if (e == 0)
+      for (int j = 0; j < 8; ++j) nshape[gp * 8 + j] = static_cast<float>(s.N[j]);
+  }
+}
+
+// y_e = K_eff,e x_e in FP32 point by point: strain B x, stress D_eff eps with the point's material
+// matrix in the compact form K 1 (x) 1 + 2 G theta I_dev - 2 G thetab n (x) n (elastic sets and
+// `initial`: theta = 1, thetab = 0, the elastic matrix), scaled by the stiffness factor, then
+// B^T sigma dvol and the mass term, into FP32 slots.
+__global__ void __launch_bounds__(kBlock) k_element_apply32(const int32_t* __restrict__ eq,
+                                                             const int32_t* __restrict__ param,
+                                                             const ParamGP* __restrict__ params, int32_t P,
+                                                             int32_t count, double ks, double kd, double km,
+                                                             const float* __restrict__ geom,
+                                                             const float* __restrict__ nshape,
+                                                             const float* __restrict__ x, float* __restrict__ slots,
+                                                             const int* skip, const double* __restrict__ j2tan,
+                                                             int initial) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count || (skip && *skip)) return;
+  const ParamGP p = params[param[e]];
+  const OpFactors f = op_factors(p, ks, kd, km);
+  // the elastic tangents are one matrix: D_eff = (cK + c0 + cc) D (J2 sets carry no
+  // stiffness-proportional damping, so c0 = cc = 0 there)
+  const float sk = static_cast<float>(f.cK + f.c0 + f.cc), cm = static_cast<float>(f.cM);
+  double Kd, Gd;
+  j2_moduli(p, Kd, Gd);
+  const float K = static_cast<float>(Kd), G2 = static_cast<float>(2.0 * Gd);
+  const float rho = static_cast<float>(p.rho);
+  const bool j2 = p.kind == 1 && !initial;
+  float xe[24], ye[24];
+  for (int a = 0; a < 24; ++a) {
+    const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+    xe[a] = q >= 0 ? x[q] : 0.f;
+    ye[a] = 0.f;
+  }
+  for (int gp = 0; gp < 8; ++gp) {
+    float dN[3][8];
+    for (int d = 0; d < 3; ++d)
+      for (int j = 0; j < 8; ++j) dN[d][j] = geom[static_cast<int64_t>(((d * 8 + j) * 8) + gp) * P + e];
+    const float dvol = geom[static_cast<int64_t>(24 * 8 + gp) * P + e];
+    float eps[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int j = 0; j < 8; ++j) {
+      const float dx = dN[0][j], dy = dN[1][j], dz = dN[2][j];
+      const float u0 = xe[3 * j], u1 = xe[3 * j + 1], u2 = xe[3 * j + 2];
+      eps[0] += dx * u0;
+      eps[1] += dy * u1;
+      eps[2] += dz * u2;
+      eps[3] += dy * u0 + dx * u1;
+      eps[4] += dz * u1 + dy * u2;
+      eps[5] += dz * u0 + dx * u2;
+    }
+    float theta = 1.f, thetab = 0.f, n[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (j2) {
+      const double* t = j2tan + e;
+      theta = static_cast<float>(t[static_cast<int64_t>(0 * 8 + gp) * P]);
+      thetab = static_cast<float>(t[static_cast<int64_t>(1 * 8 + gp) * P]);
+      for (int c = 0; c < 6; ++c) n[c] = static_cast<float>(t[static_cast<int64_t>((2 + c) * 8 + gp) * P]);
+    }
+    const float tr = eps[0] + eps[1] + eps[2];
+    float ne = 0.f;
+    for (int c = 0; c < 6; ++c) ne += n[c] * eps[c];
+    const float gt = G2 * theta, gb = G2 * thetab * ne;
+    float sg[6];
+    for (int c = 0; c < 3; ++c) sg[c] = sk * (K * tr + gt * (eps[c] - tr / 3.f) - gb * n[c]);
+    for (int c = 3; c < 6; ++c) sg[c] = sk * (0.5f * gt * eps[c] - gb * n[c]);
+    for (int c = 0; c < 6; ++c) sg[c] *= dvol;
+    for (int j = 0; j < 8; ++j) {
+      const float dx = dN[0][j], dy = dN[1][j], dz = dN[2][j];
+      ye[3 * j] += dx * sg[0] + dy * sg[3] + dz * sg[5];
+      ye[3 * j + 1] += dy * sg[1] + dx * sg[3] + dz * sg[4];
+      ye[3 * j + 2] += dz * sg[2] + dy * sg[4] + dx * sg[5];
+    }
+    if (cm != 0.f) {
+      const float* Ng = nshape + gp * 8;
+      float v[3] = {0.f, 0.f, 0.f};
+      if (p.mass_type == 0)
+        for (int k = 0; k < 8; ++k)
+          for (int q = 0; q < 3; ++q) v[q] += Ng[k] * xe[3 * k + q];
+      for (int j = 0; j < 8; ++j) {
+        const float t = cm * Ng[j] * dvol * rho;
+        for (int q = 0; q < 3; ++q) ye[3 * j + q] += t * (p.mass_type == 0 ? v[q] : xe[3 * j + q]);
+      }
+    }
+  }
+  for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
+}
+
+__global__ void __launch_bounds__(256) k_gather32(const int32_t* __restrict__ start, const int32_t* __restrict__ list,
+                                                   const float* __restrict__ slots, int32_t neq, double c1,
+                                                   const double* __restrict__ m1, double c2,
+                                                   const double* __restrict__ m2, const float* __restrict__ x,
+                                                   float* __restrict__ y, const int* skip) {
+  const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= neq || (skip && *skip)) return;
+  float sum = 0.f;
+  for (int32_t j = start[q]; j < start[q + 1]; ++j) sum += slots[list[j]];
+  if (m1) sum += static_cast<float>(c1 * m1[q]) * x[q];
+  if (m2) sum += static_cast<float>(c2 * m2[q]) * x[q];
+  y[q] = sum;
+}
+
 }  // namespace
+
+void general_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st, const int* skip) {
+  if (s.count > 0 && s.geom32.n == 0) {  // the FP32 geometric factors, once
+    s.geom32.alloc(static_cast<size_t>(kGeom32) * 8 * s.P);
+    s.nshape32.alloc(64);
+    s.slots32.alloc(static_cast<size_t>(24) * s.P);
+    k_geom32<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.N, s.P, s.count, s.geom32.ptr,
+                                                           s.nshape32.ptr);
+    FX_LAUNCH_CHECK("geom32");
+  }
+  if (s.count > 0)
+    k_element_apply32<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.eq.ptr, s.param.ptr, s.params.ptr, s.P, s.count,
+                                                                     k[0], k[1], k[2], s.geom32.ptr, s.nshape32.ptr, x,
+                                                                     s.slots32.ptr, skip, s.j2_tan.ptr, s.initial);
+  FX_LAUNCH_CHECK("element_apply32");
+  const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
+  const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
+  if (s.neq > 0)
+    k_gather32<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots32.ptr, s.neq, k[2], m1, k[1],
+                                                     m2, x, y, skip);
+  FX_LAUNCH_CHECK("slot_gather32");
+}
 
 void general_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
   if (s.count > 0)

@@ -398,7 +398,10 @@ struct Solver {
     if (f->s.use_box()) box_apply(f->s, k, x, y, cs, skip);
     else general_apply(f->s, k, x, y, cs, skip);
   }
-  void apply32(const float* x, float* y, const int* skip) { box_apply_f32(f->s, k, x, y, cs, skip); }
+  void apply32(const float* x, float* y, const int* skip) {
+    if (f->s.use_box()) box_apply_f32(f->s, k, x, y, cs, skip);
+    else general_apply_f32(f->s, k, x, y, cs, skip);
+  }
 
   void read_state() {
     FX_CUDA(cudaMemcpyAsync(host_flags, fl.ptr, sizeof(int) * F_NFLAG, cudaMemcpyDeviceToHost, cs));
@@ -683,12 +686,15 @@ int Solver::newton(const double* fext, double* u, int test, double tol, int max_
     if (it >= max_newton) break;
     general_diagonal(fs, k, diag.ptr, cs);
     k_reciprocal_t<double><<<ew(n), 256, 0, cs>>>(diag.ptr, inv.ptr, n);
+    if (method == FX_SOLVER_IR) k_reciprocal_t<float><<<ew(n), 256, 0, cs>>>(diag.ptr, inv32.ptr, n);
     FX_CUDA(cudaMemsetAsync(ndu.ptr, 0, sizeof(double) * n, cs));
     fx_solve_result lin{};
-    cg<double>(nres.ptr, ndu.ptr, r.ptr, p.ptr, ap.ptr, inv.ptr, o.rtol, o.atol, o.max_iterations, &lin);
+    if (method == FX_SOLVER_IR) ir(nres.ptr, ndu.ptr, &lin);  // FP32 CG on the tangent, FP64 refinement
+    else cg<double>(nres.ptr, ndu.ptr, r.ptr, p.ptr, ap.ptr, inv.ptr, o.rtol, o.atol, o.max_iterations, &lin);
     k_add64<<<ew(n), 256, 0, cs>>>(ndu.ptr, u, n);
     FX_LAUNCH_CHECK("newton_update");
     res->iterations += lin.iterations;
+    res->refinements += lin.refinements;
     res->indefinite |= lin.indefinite;
     ++it;
     const double dn = test == FX_TEST_NORM_DISP_INCR ? norm(ndu.ptr) : 0.0;
@@ -802,8 +808,6 @@ int fx_solver_create(fx_force* f, int32_t method, fx_solve_opts o, fx_solver** o
   return guard([&] {
     if (!f || !out) throw fx::Error(FX_E_INVALID, "fx_solver_create: bad arguments");
     if (method < FX_SOLVER_CG || method > FX_SOLVER_IR) throw fx::Error(FX_E_INVALID, "fx_solver_create: unknown method");
-    if (method == FX_SOLVER_IR && !f->s.use_box())
-      throw fx::Error(FX_E_UNSUPPORTED, "the FP32 inner solve runs on the box path only: " + f->s.box.why_not);
     if (o.lanes <= 0) o.lanes = 32;
     if (o.lanes > 32) throw fx::Error(FX_E_INVALID, "lanes must be in 1..32");
     if (o.restart <= 0) o.restart = 30;
@@ -951,7 +955,8 @@ int fx_solver_newton(fx_solver* h, const double* fext, double* u, int32_t test, 
       throw fx::Error(FX_E_INVALID, "fx_solver_newton: unknown convergence test");
     fx::Solver& s = h->s;
     if (!s.ready) throw fx::Error(FX_E_INVALID, "fx_solver_newton: call fx_solver_setup first");
-    if (s.method != FX_SOLVER_CG) throw fx::Error(FX_E_UNSUPPORTED, "fx_solver_newton: CG solvers only");
+    if (s.method != FX_SOLVER_CG && s.method != FX_SOLVER_IR)
+      throw fx::Error(FX_E_UNSUPPORTED, "fx_solver_newton: CG or refined FP32 CG solvers only");
     *r = fx_solve_result{};
     *newton_iterations = 0;
     if (s.n == 0) {

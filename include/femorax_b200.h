@@ -177,7 +177,10 @@ typedef struct fx_coeffs {
 /* y = K_eff x (InternalForce::apply_operator, internal_force.cpp:545-573; x, y device FP64,
  * never aliasing). */
 int fx_apply_operator(fx_force* f, fx_coeffs k, const double* x, double* y, void* stream);
-/* FP32 twin: x, y device FP32, parameters rounded to FP32 (the mixed-precision inner operator). */
+/* FP32 twin: x, y device FP32, parameters rounded to FP32 (the mixed-precision inner operator):
+ * on box grids the box kernel in FP32; on other meshes (J2 sets included, with their stored
+ * point tangents) the Gauss-point operator in FP32 with FP32 geometric factors of the points,
+ * computed once in FP64 and rounded. */
 int fx_apply_operator_f32(fx_force* f, fx_coeffs k, const float* x, float* y, void* stream);
 /* The same apply from HOST vectors (pinned or pageable): copies in, applies, copies out. */
 int fx_apply_operator_host(fx_force* f, fx_coeffs k, const double* x_host, double* y_host, void* stream);
@@ -266,14 +269,16 @@ typedef struct fx_solve_result {
  * the coefficients change); fx_solver_solve solves K_eff x = b with x holding the initial guess.
  * Methods:
  *   FX_SOLVER_CG      Jacobi-PCG (ConjugateGradient::solve, src/solvers/cg.cpp:24-71),
- *                     device-resident: scalars stay on the device, iterations run as a CUDA
- *                     graph, the host reads a convergence flag every few iterations.
+ *                     device-resident: scalars stay on the device, the iterations run as one
+ *                     CUDA graph that loops on the device until the solve is done (kept for the
+ *                     next solve on the same vectors); the host reads the result once.
  *   FX_SOLVER_GMRES   FGMRES(restart) with CGS2 (Gmres::solve, src/solvers/gmres.cpp:32-123).
  *   FX_SOLVER_KRYLOV  CG, then GMRES from the initial guess if CG meets p.Ap <= 0
  *                     (KrylovSolver::solve, src/solvers/krylov.cpp:25-41).
  *   FX_SOLVER_IR      CG in FP32 (FP32 operator and vectors) inside FP64 iterative refinement:
  *                     r = b - K x in FP64, K d = r by FP32 PCG to inner_rtol, x += d in FP64,
- *                     until ||b - K x|| <= rtol ||b|| in FP64. Box path only. */
+ *                     until ||b - K x|| <= rtol ||b|| in FP64. The FP32 operator is
+ *                     fx_apply_operator_f32's (box kernel, or the FP32 Gauss-point form). */
 #define FX_SOLVER_CG 0
 #define FX_SOLVER_GMRES 1
 #define FX_SOLVER_KRYLOV 2
@@ -293,8 +298,10 @@ int fx_solver_solve(fx_solver* s, const double* b, double* x, fx_solve_result* r
  * FX_TEST_NORM_DISP_INCR ||du|| <= tol (then the force is evaluated once more at the final u);
  * or max_newton solves. u (device) holds the start and receives the result; the trial material
  * state is u's, left for fx_force_commit. r: converged, iterations (CG iterations in all),
- * rhs_norm = ||f_ext||, initial/final_residual = ||r|| at the first and last evaluation. CG
- * solvers only (set up with the stiffness coefficient 1). */
+ * rhs_norm = ||f_ext||, initial/final_residual = ||r|| at the first and last evaluation.
+ * FX_SOLVER_CG, or FX_SOLVER_IR (FP32 CG on the tangent inside FP64 refinement: the FP32
+ * operator uses the points' stored tangents, the return map stays FP64); set up with the
+ * stiffness coefficient 1. */
 #define FX_TEST_NORM_UNBALANCE 0
 #define FX_TEST_NORM_DISP_INCR 1
 int fx_solver_newton(fx_solver* s, const double* fext, double* u, int32_t test, double tol, int32_t max_newton,
