@@ -609,9 +609,12 @@ class BatchedNewton:
     """Quasi-static load steps of many independent meshes at once (fx_nbatch_*): one combined
     mesh (instance i's equations at offsets[i] .. offsets[i] + equations[i]), one launch per element
     kernel for all instances, per-instance Newton test and Jacobi-PCG on the device; per instance
-    bit for bit LinearSolver.newton (NormUnbalance) on that mesh alone."""
+    bit for bit LinearSolver.newton (NormUnbalance) on that mesh alone. mixed: the Newton steps'
+    linear solves by FP32 CG inside FP64 refinement (inner_tolerance), per instance the bits of
+    MixedPrecisionSolver.newton on that mesh alone."""
 
-    def __init__(self, meshes, options: SolveOptions = None, device: int = 0):
+    def __init__(self, meshes, options: SolveOptions = None, device: int = 0, mixed: bool = False,
+                 inner_tolerance: float = 1e-4):
         o = options or SolveOptions(relative_tolerance=1e-12, max_iterations=20000)
         arr = (L.fx_mesh * len(meshes))()
         keep = []
@@ -632,6 +635,8 @@ class BatchedNewton:
         self.equations = np.array(neq[:])
         self.total = int(self.offsets[-1])
         self._force = lib().fx_nbatch_force(h)
+        if mixed:
+            check(lib().fx_nbatch_set_inner(h, L.FX_SOLVER_IR, inner_tolerance))
 
     def combine(self, per_instance) -> np.ndarray:
         """Host vectors of the instances -> one vector in the combined layout."""

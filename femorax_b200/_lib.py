@@ -130,6 +130,7 @@ PROTOTYPES = {
     "fx_explicit_run_f32": (C.c_int, [vp, vp, C.c_int32, p_f64, C.c_int32, C.c_double, vp, vp, vp, vp, vp]),
     "fx_explicit_record": (C.c_int, [vp, C.c_int32, vp, C.c_int32]),
     "fx_force_get_launches": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+    "fx_nbatch_set_inner": (C.c_int, [vp, C.c_int32, C.c_double]),
     "fx_motions_create": (C.c_int, [C.POINTER(vp)]),
     "fx_motions_destroy": (C.c_int, [vp]),
     "fx_motions_add": (C.c_int, [vp, C.c_int32, C.c_double, p_f64, p_f64, C.c_int32, C.c_double, C.c_double,

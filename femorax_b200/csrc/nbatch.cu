@@ -24,14 +24,23 @@ constexpr int kWarps = 8;
 constexpr int64_t kMaxInstanceChunks = 2048;  // one level of chunk sums per instance
 
 // per-instance scalars and flags
-enum : int { N_RN = 0, N_BB, N_RZ, N_PAP, N_ALPHA, N_BETA, N_RR, N_RZNEW, N_TOL, N_RNORM, NNS = 12 };
+enum : int {
+  N_RN = 0, N_BB, N_RZ, N_PAP, N_ALPHA, N_BETA, N_RR, N_RZNEW, N_TOL, N_RNORM,
+  N_QBB, N_QRR, N_QBNORM,  // refinement: b.b, q.q (q = b - K du), ||b||
+  NNS = 16
+};
 enum : int {
   G_NEWTON_DONE = 0,  // the Newton test has passed or the iteration limit is reached
   G_CONV,             // the Newton test passed
   G_ITERS,            // Newton solves
   G_CG_DONE,          // this CG solve is finished (the apply's and the vector kernels' gate)
   G_CG_ITERS, G_CG_TOTAL, G_CG_CONV, G_INDEF,
-  NNF = 8
+  G_CG_MAXIT,         // this CG solve's iteration limit
+  G_IR_DONE,          // refinement: this linear solve is finished
+  G_IR_OUTER,         // refinement rounds of this linear solve
+  G_IR_INNER,         // inner iterations of this linear solve
+  G_IR_REFS,          // refinement rounds in all
+  NNF = 16
 };
 
 struct Range {
@@ -44,8 +53,9 @@ __device__ __forceinline__ int64_t chunk_len(const Range& r, int64_t begin) {
 }
 
 // chunk sums of x.y over the chunks of instances whose flag `gate` is 0 (column 0 of part)
+template <class T>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_nb_dot(const double* __restrict__ x, const double* __restrict__ y, int64_t nchunks,
+    k_nb_dot(const T* __restrict__ x, const T* __restrict__ y, int64_t nchunks,
              const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl, int gate,
              int lanes, double* __restrict__ part) {
   const int lane = threadIdx.x & 31;
@@ -56,8 +66,10 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
   double acc = 0.0;
   if (lane < lanes)
-    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<double, 2>{{x[i], y[i]}}; },
-                 [&](int64_t, const Ops<double, 2>& o) { acc = fma(o.v[0], o.v[1], acc); });
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{x[i], y[i]}}; },
+                 [&](int64_t, const Ops<T, 2>& o) {
+                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
+                 });
   double total = 0.0;
   for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
   if (lane == 0) part[c] = total;
@@ -158,12 +170,15 @@ __global__ void __launch_bounds__(32 * kWarps)
 }
 
 // per instance: the CG start (ConjugateGradient's tolerance max(rtol ||b||, atol), b = r)
-__global__ void k_nb_cg_start(double* sc, int* fl, int count, double rtol, double atol, int max_it) {
+// (ir: the inner solve of a refinement round, whose limit is what the linear solve has left)
+__global__ void k_nb_cg_start(double* sc, int* fl, int count, double rtol, double atol, int max_it, int ir) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= count) return;
   int* f = fl + s * NNF;
   double* c = sc + s * NNS;
   if (f[G_CG_DONE]) return;
+  if (ir) max_it -= f[G_IR_INNER];
+  f[G_CG_MAXIT] = max_it;
   const double rhs = sqrt(c[N_RR]);  // b.b: the same sum as rr.rr at du = 0
   const double rn = sqrt(c[N_RR]);
   c[N_RZ] = c[N_RZNEW];
@@ -189,30 +204,30 @@ __global__ void k_nb_alpha(double* sc, int* fl, int count) {
   c[N_ALPHA] = c[N_RZ] / pap;
 }
 
-// du += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z
+// du += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (vectors of type T, sums in double)
+template <class T>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_nb_update(const double* __restrict__ sc, const int* __restrict__ fl, const double* __restrict__ p,
-                const double* __restrict__ ap, const double* __restrict__ inv, double* __restrict__ du,
-                double* __restrict__ rr, int64_t nchunks, const int* __restrict__ owner, const Range* __restrict__ rg,
-                int lanes, double* __restrict__ part, int64_t ld) {
+    k_nb_update(const double* __restrict__ sc, const int* __restrict__ fl, const T* __restrict__ p,
+                const T* __restrict__ ap, const T* __restrict__ inv, T* __restrict__ du, T* __restrict__ rr,
+                int64_t nchunks, const int* __restrict__ owner, const Range* __restrict__ rg, int lanes,
+                double* __restrict__ part, int64_t ld) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
   const int s = owner[c];
   if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
-  const double alpha = sc[s * NNS + N_ALPHA];
+  const T alpha = static_cast<T>(sc[s * NNS + N_ALPHA]);
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    lane_loop<4>(begin, len, lane, lanes,
-                 [&](int64_t i) { return Ops<double, 5>{{p[i], ap[i], inv[i], du[i], rr[i]}}; },
-                 [&](int64_t i, const Ops<double, 5>& o) {
+    lane_loop<4>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 5>{{p[i], ap[i], inv[i], du[i], rr[i]}}; },
+                 [&](int64_t i, const Ops<T, 5>& o) {
                    du[i] = fma(alpha, o.v[0], o.v[3]);
-                   const double ri = fma(-alpha, o.v[1], o.v[4]);
+                   const T ri = fma(-alpha, o.v[1], o.v[4]);
                    rr[i] = ri;
-                   const double zi = o.v[2] * ri;
-                   srr = fma(ri, ri, srr);
-                   srz = fma(ri, zi, srz);
+                   const T zi = o.v[2] * ri;
+                   srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+                   srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
                  });
   double trr = 0.0, trz = 0.0;
   for (int j = 0; j < lanes; ++j) {
@@ -225,12 +240,13 @@ __global__ void __launch_bounds__(32 * kWarps)
   }
 }
 
-__global__ void k_nb_beta(double* sc, int* fl, int count, int max_it) {
+__global__ void k_nb_beta(double* sc, int* fl, int count) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= count) return;
   int* f = fl + s * NNF;
   double* c = sc + s * NNS;
   if (f[G_CG_DONE]) return;
+  const int max_it = f[G_CG_MAXIT];
   const double rn = sqrt(c[N_RR]);
   const int it = ++f[G_CG_ITERS];
   if (rn <= c[N_TOL]) {
@@ -247,19 +263,20 @@ __global__ void k_nb_beta(double* sc, int* fl, int count, int max_it) {
 }
 
 // p = inv rr + beta p
+template <class T>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_nb_p(const double* __restrict__ sc, const int* __restrict__ fl, const double* __restrict__ inv,
-           const double* __restrict__ rr, double* __restrict__ p, int64_t nchunks, const int* __restrict__ owner,
+    k_nb_p(const double* __restrict__ sc, const int* __restrict__ fl, const T* __restrict__ inv,
+           const T* __restrict__ rr, T* __restrict__ p, int64_t nchunks, const int* __restrict__ owner,
            const Range* __restrict__ rg) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
   const int s = owner[c];
   if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
-  const double beta = sc[s * NNS + N_BETA];
+  const T beta = static_cast<T>(sc[s * NNS + N_BETA]);
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 3>{{p[i], inv[i], rr[i]}}; },
-               [&](int64_t i, const Ops<double, 3>& o) { p[i] = fma(beta, o.v[0], o.v[1] * o.v[2]); });
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<T, 3>{{p[i], inv[i], rr[i]}}; },
+               [&](int64_t i, const Ops<T, 3>& o) { p[i] = fma(beta, o.v[0], o.v[1] * o.v[2]); });
 }
 
 // u += du for instances that solved this iteration; their counters
@@ -274,6 +291,128 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
   lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{u[i], du[i]}}; },
                [&](int64_t i, const Ops<double, 2>& o) { u[i] = o.v[0] + o.v[1]; });
+}
+
+// ---- FP32 CG inside FP64 refinement per instance: Solver::ir on each instance's equations
+// the start of a linear solve: the instances still in Newton refine from du = 0
+__global__ void k_nb_ir_start(int* fl, int count) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  f[G_IR_DONE] = f[G_NEWTON_DONE];
+  f[G_IR_OUTER] = 0;
+  f[G_IR_INNER] = 0;
+  f[G_CG_DONE] = 1;
+}
+
+// q = b - K du (b: the Newton residual r; K du in ap) for instances still refining
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_ir_residual(const double* __restrict__ r, const double* __restrict__ ap, double* __restrict__ q,
+                     int64_t nchunks, const int* __restrict__ owner, const Range* __restrict__ rg,
+                     const int* __restrict__ fl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_IR_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{r[i], ap[i]}}; },
+               [&](int64_t i, const Ops<double, 2>& o) { q[i] = o.v[0] - o.v[1]; });
+}
+
+// the refinement test: finished at ||q|| <= max(rtol ||b||, atol) or at the round or inner
+// iteration limit; otherwise an inner solve follows (G_CG_DONE = 0)
+__global__ void k_nb_ir_test(double* sc, int* fl, int count, double rtol, double atol, int max_outer, int max_it) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  double* c = sc + s * NNS;
+  if (f[G_IR_DONE]) return;
+  if (f[G_IR_OUTER] == 0) c[N_QBNORM] = sqrt(c[N_QBB]);
+  const double rn = sqrt(c[N_QRR]);
+  const double tol = rtol * c[N_QBNORM];
+  if (rn <= (tol > atol ? tol : atol) || f[G_IR_OUTER] >= max_outer || f[G_IR_INNER] >= max_it) {
+    f[G_IR_DONE] = 1;
+    return;
+  }
+  f[G_CG_DONE] = 0;
+}
+
+// the inner solve's start, FP32 CG from d = 0 (K 0 = 0): r32 = (float) q, d = 0, rr = r32,
+// z = inv32 rr, p = z; chunk sums of rr.rr and rr.z (columns 0 and 1 of part)
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_ir_begin(const double* __restrict__ q, float* __restrict__ r32, float* __restrict__ d32,
+                  float* __restrict__ rr, float* __restrict__ p, const float* __restrict__ inv, int64_t nchunks,
+                  const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl, int lanes,
+                  double* __restrict__ part, int64_t ld) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 1>{{q[i]}}; },
+               [&](int64_t i, const Ops<double, 1>& o) {
+                 r32[i] = static_cast<float>(o.v[0]);
+                 d32[i] = 0.f;
+               });
+  __syncwarp();
+  double srr = 0.0, srz = 0.0;
+  if (lane < lanes)
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<float, 2>{{r32[i], inv[i]}}; },
+                 [&](int64_t i, const Ops<float, 2>& o) {
+                   const float ri = fmaf(-1.f, 0.f, o.v[0]);
+                   const float zi = o.v[1] * ri;
+                   rr[i] = ri;
+                   p[i] = zi;
+                   srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+                   srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+                 });
+  double trr = 0.0, trz = 0.0;
+  for (int j = 0; j < lanes; ++j) {
+    trr += __shfl_sync(0xffffffffu, srr, j);
+    trz += __shfl_sync(0xffffffffu, srz, j);
+  }
+  if (lane == 0) {
+    part[c] = trr;
+    part[ld + c] = trz;
+  }
+}
+
+// du += (double) d32 for instances that ran this round's inner solve
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_ir_correct(const float* __restrict__ d32, double* __restrict__ du, int64_t nchunks,
+                    const int* __restrict__ owner, const Range* __restrict__ rg, const int* __restrict__ fl) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_IR_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 2>{{du[i], static_cast<double>(d32[i])}}; },
+               [&](int64_t i, const Ops<double, 2>& o) { du[i] = o.v[0] + o.v[1]; });
+}
+
+// the end of a round: the counters, and the end of the solve when its inner solve made no
+// progress; the inner iterations are added to the Newton iteration's total here
+__global__ void k_nb_ir_round_end(int* fl, int count) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  int* f = fl + s * NNF;
+  if (f[G_IR_DONE]) return;
+  f[G_IR_INNER] += f[G_CG_ITERS];
+  f[G_CG_TOTAL] += f[G_CG_ITERS];
+  f[G_IR_OUTER] += 1;
+  f[G_IR_REFS] += 1;
+  if (f[G_CG_ITERS] == 0 && !f[G_CG_CONV]) f[G_IR_DONE] = 1;
+  f[G_CG_ITERS] = 0;
+}
+
+// the inverse of the tangent's diagonal in FP32 (0 at equations of no instance)
+__global__ void k_nb_inverse32(const double* __restrict__ d, float* __restrict__ inv, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    inv[i] = d[i] != 0.0 ? static_cast<float>(1.0 / d[i]) : 0.f;
 }
 
 __global__ void k_nb_iteration_end(int* fl, int count) {
@@ -309,9 +448,16 @@ struct NBatch {
   int* fl_h = nullptr;
   double* sc_h = nullptr;
   cudaGraphExec_t graph = nullptr;
+  // FP32 CG inside FP64 refinement (FX_SOLVER_IR): q = b - K du, the FP32 inner vectors
+  int method = FX_SOLVER_CG;
+  double inner_rtol = 1e-4;
+  DeviceArray<double> q;
+  DeviceArray<float> r32, d32, rr32, p32, ap32, inv32;
+  cudaGraphExec_t graph32 = nullptr;
 
   ~NBatch() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph32) cudaGraphExecDestroy(graph32);
     if (fl_h) cudaFreeHost(fl_h);
     if (sc_h) cudaFreeHost(sc_h);
     if (ev_in) cudaEventDestroy(ev_in);
@@ -337,16 +483,102 @@ struct NBatch {
     const double k[3] = {1.0, 0.0, 0.0};
     const unsigned g = chunk_grid(nchunks);
     general_apply(force->s, k, p.ptr, ap.ptr, cs);
-    k_nb_dot<<<g, 32 * kWarps, 0, cs>>>(p.ptr, ap.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_CG_DONE, o.lanes,
-                                        part.ptr);
+    k_nb_dot<double><<<g, 32 * kWarps, 0, cs>>>(p.ptr, ap.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_CG_DONE,
+                                                o.lanes, part.ptr);
     level(1, G_CG_DONE, N_PAP);
     k_nb_alpha<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
-    k_nb_update<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p.ptr, ap.ptr, inv.ptr, du.ptr, rr.ptr, nchunks, owner.ptr,
-                                           rg.ptr, o.lanes, part.ptr, nchunks);
+    k_nb_update<double><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p.ptr, ap.ptr, inv.ptr, du.ptr, rr.ptr, nchunks,
+                                                   owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks);
     level(2, G_CG_DONE, N_RR);
-    k_nb_beta<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, o.max_iterations);
-    k_nb_p<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv.ptr, rr.ptr, p.ptr, nchunks, owner.ptr, rg.ptr);
+    k_nb_beta<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+    k_nb_p<double><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv.ptr, rr.ptr, p.ptr, nchunks, owner.ptr, rg.ptr);
     FX_LAUNCH_CHECK("nbatch_cg");
+  }
+
+  // one iteration of the inner FP32 CG (the FP32 operator on the stored point tangents)
+  void cg_iteration32() {
+    const double k[3] = {1.0, 0.0, 0.0};
+    const unsigned g = chunk_grid(nchunks);
+    general_apply_f32(force->s, k, p32.ptr, ap32.ptr, cs);
+    k_nb_dot<float><<<g, 32 * kWarps, 0, cs>>>(p32.ptr, ap32.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_CG_DONE,
+                                               o.lanes, part.ptr);
+    level(1, G_CG_DONE, N_PAP);
+    k_nb_alpha<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+    k_nb_update<float><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr,
+                                                  nchunks, owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks);
+    level(2, G_CG_DONE, N_RR);
+    k_nb_beta<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+    k_nb_p<float><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv32.ptr, rr32.ptr, p32.ptr, nchunks, owner.ptr,
+                                             rg.ptr);
+    FX_LAUNCH_CHECK("nbatch_cg32");
+  }
+
+  // CG iterations until every instance's solve is done: a first block of 8 eagerly, then a
+  // captured graph of 8 (one per precision, kept), the flags read after each block
+  void cg_loop(bool f32) {
+    const int block = 8;
+    for (int i = 0; i < block; ++i) {
+      if (f32) cg_iteration32();
+      else cg_iteration();
+    }
+    read_flags();
+    cudaGraphExec_t& gx = f32 ? graph32 : graph;
+    while (any(G_CG_DONE, 0)) {
+      if (!gx) {
+        cudaGraph_t gr = nullptr;
+        FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int i = 0; i < block; ++i) {
+            if (f32) cg_iteration32();
+            else cg_iteration();
+          }
+        } catch (...) {
+          cudaStreamEndCapture(cs, &gr);
+          if (gr) cudaGraphDestroy(gr);
+          throw;
+        }
+        FX_CUDA(cudaStreamEndCapture(cs, &gr));
+        const cudaError_t e = cudaGraphInstantiate(&gx, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) gx = nullptr;
+        FX_CUDA(e);
+      }
+      FX_CUDA(cudaGraphLaunch(gx, cs));
+      read_flags();
+    }
+  }
+
+  // K_t du = r per instance by FP32 CG inside FP64 refinement (Solver::ir's rounds)
+  void linear_ir() {
+    const double k[3] = {1.0, 0.0, 0.0};
+    const unsigned g = chunk_grid(nchunks);
+    FX_CUDA(cudaMemsetAsync(du.ptr, 0, sizeof(double) * static_cast<size_t>(total), cs));
+    k_nb_ir_start<<<inst_grid(), 128, 0, cs>>>(fl.ptr, count);
+    for (int round = 0;; ++round) {
+      general_apply(force->s, k, du.ptr, ap.ptr, cs);
+      k_nb_ir_residual<<<g, 32 * kWarps, 0, cs>>>(r.ptr, ap.ptr, q.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr);
+      if (round == 0) {
+        k_nb_dot<double><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_IR_DONE,
+                                                    o.lanes, part.ptr);
+        level(1, G_IR_DONE, N_QBB);
+      }
+      k_nb_dot<double><<<g, 32 * kWarps, 0, cs>>>(q.ptr, q.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_IR_DONE, o.lanes,
+                                                  part.ptr);
+      level(1, G_IR_DONE, N_QRR);
+      k_nb_ir_test<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, o.rtol, o.atol, 50, o.max_iterations);
+      FX_LAUNCH_CHECK("nbatch_ir_test");
+      read_flags();
+      if (!any(G_IR_DONE, 0)) break;
+      k_nb_ir_begin<<<g, 32 * kWarps, 0, cs>>>(q.ptr, r32.ptr, d32.ptr, rr32.ptr, p32.ptr, inv32.ptr, nchunks,
+                                               owner.ptr, rg.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
+      level(2, G_CG_DONE, N_RR);
+      k_nb_cg_start<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, inner_rtol, 0.0, o.max_iterations, 1);
+      FX_LAUNCH_CHECK("nbatch_ir_inner_begin");
+      cg_loop(true);
+      k_nb_ir_correct<<<g, 32 * kWarps, 0, cs>>>(d32.ptr, du.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr);
+      k_nb_ir_round_end<<<inst_grid(), 128, 0, cs>>>(fl.ptr, count);
+      FX_LAUNCH_CHECK("nbatch_ir_round");
+    }
   }
 
   bool any(int flag, int value) const {
@@ -372,32 +604,16 @@ struct NBatch {
       if (!any(G_NEWTON_DONE, 0)) break;
       general_diagonal(force->s, k, d.ptr, cs);
       k_nb_inverse<<<ew(total), 256, 0, cs>>>(d.ptr, inv.ptr, total);
-      k_nb_cg_begin<<<g, 32 * kWarps, 0, cs>>>(r.ptr, du.ptr, rr.ptr, p.ptr, inv.ptr, nchunks, owner.ptr, rg.ptr,
-                                               fl.ptr, o.lanes, part.ptr, nchunks);
-      level(2, G_CG_DONE, N_RR);
-      k_nb_cg_start<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, o.rtol, o.atol, o.max_iterations);
-      FX_LAUNCH_CHECK("nbatch_cg_begin");
-      const int block = 8;
-      for (int i = 0; i < block; ++i) cg_iteration();
-      read_flags();
-      while (any(G_CG_DONE, 0)) {
-        if (!graph) {
-          cudaGraph_t gr = nullptr;
-          FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-          try {
-            for (int i = 0; i < block; ++i) cg_iteration();
-          } catch (...) {
-            cudaStreamEndCapture(cs, &gr);
-            if (gr) cudaGraphDestroy(gr);
-            throw;
-          }
-          FX_CUDA(cudaStreamEndCapture(cs, &gr));
-          const cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
-          cudaGraphDestroy(gr);
-          FX_CUDA(e);
-        }
-        FX_CUDA(cudaGraphLaunch(graph, cs));
-        read_flags();
+      if (method == FX_SOLVER_IR) {
+        k_nb_inverse32<<<ew(total), 256, 0, cs>>>(d.ptr, inv32.ptr, total);
+        linear_ir();
+      } else {
+        k_nb_cg_begin<<<g, 32 * kWarps, 0, cs>>>(r.ptr, du.ptr, rr.ptr, p.ptr, inv.ptr, nchunks, owner.ptr, rg.ptr,
+                                                 fl.ptr, o.lanes, part.ptr, nchunks);
+        level(2, G_CG_DONE, N_RR);
+        k_nb_cg_start<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count, o.rtol, o.atol, o.max_iterations, 0);
+        FX_LAUNCH_CHECK("nbatch_cg_begin");
+        cg_loop(false);
       }
       k_nb_correct<<<g, 32 * kWarps, 0, cs>>>(du.ptr, u, nchunks, owner.ptr, rg.ptr, fl.ptr);
       k_nb_iteration_end<<<inst_grid(), 128, 0, cs>>>(fl.ptr, count);
@@ -558,6 +774,27 @@ int fx_nbatch_layout(const fx_nbatch* h, int64_t* offsets, int64_t* equations) {
 
 fx_force* fx_nbatch_force(fx_nbatch* h) { return h ? h->b.force : nullptr; }
 
+int fx_nbatch_set_inner(fx_nbatch* h, int32_t method, double inner_rtol) {
+  return guard([&] {
+    if (!h || (method != FX_SOLVER_CG && method != FX_SOLVER_IR) || !(inner_rtol > 0.0 && inner_rtol < 1.0))
+      throw fx::Error(FX_E_INVALID, "fx_nbatch_set_inner: bad arguments");
+    fx::NBatch& b = h->b;
+    FX_CUDA(cudaSetDevice(b.device));
+    b.method = method;
+    b.inner_rtol = inner_rtol;
+    if (method == FX_SOLVER_IR && b.q.n == 0) {
+      const size_t n = static_cast<size_t>(std::max<int64_t>(b.total, 1));
+      b.q.alloc(n);
+      b.q.zero(b.cs);
+      for (auto* v : {&b.r32, &b.d32, &b.rr32, &b.p32, &b.ap32, &b.inv32}) {
+        v->alloc(n);
+        FX_CUDA(cudaMemsetAsync(v->ptr, 0, sizeof(float) * n, b.cs));
+      }
+      FX_CUDA(cudaStreamSynchronize(b.cs));
+    }
+  });
+}
+
 int fx_nbatch_step(fx_nbatch* h, const double* fext, double* u, double tol, int32_t max_newton,
                    int32_t* newton_iterations, fx_solve_result* results, void* stream) {
   return guard([&] {
@@ -579,6 +816,7 @@ int fx_nbatch_step(fx_nbatch* h, const double* fext, double* u, double tol, int3
         fx_solve_result r{};
         r.converged = f[fx::G_CONV];
         r.iterations = f[fx::G_CG_TOTAL];
+        r.refinements = f[fx::G_IR_REFS];
         r.final_residual = c[fx::N_RNORM];
         r.indefinite = f[fx::G_INDEF];
         r.status = r.converged ? FX_OK : (r.indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);

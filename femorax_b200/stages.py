@@ -113,14 +113,16 @@ class BatchedPathResult:
 
 
 def batched_load_path(meshes, fext_units, factors, monitor_eqs, tol: float = 1e-6, cg_rtol: float = 1e-12,
-                      max_newton: int = 25, device: int = 0) -> BatchedPathResult:
+                      max_newton: int = 25, device: int = 0, mixed: bool = False,
+                      inner_tolerance: float = 1e-4) -> BatchedPathResult:
     """`load_path` for many meshes at once (BatchedNewton): instance i under factor *
     fext_units[i] (host), monitoring its equation monitor_eqs[i]; per instance the same bits as
-    load_path on that mesh alone."""
+    load_path on that mesh alone (mixed: with a MixedPrecisionSolver of the same tolerances)."""
     import time
 
     import torch
-    b = BatchedNewton(meshes, SolveOptions(relative_tolerance=cg_rtol, max_iterations=20000), device)
+    b = BatchedNewton(meshes, SolveOptions(relative_tolerance=cg_rtol, max_iterations=20000), device, mixed=mixed,
+                      inner_tolerance=inner_tolerance)
     dev = torch.device("cuda", device)
     F = torch.as_tensor(b.combine(fext_units), device=dev)
     u = torch.zeros(b.total, dtype=torch.float64, device=dev)

@@ -388,6 +388,11 @@ int fx_newmark_update(int64_t n, const double* du, double* u, double* v, double*
  *                      instance's material state, fx_force_state reads it */
 typedef struct fx_nbatch fx_nbatch;
 int fx_nbatch_create(const fx_mesh* meshes, int32_t count, int32_t device, fx_solve_opts o, fx_nbatch** out);
+/* The linear solves of the Newton iterations: FX_SOLVER_CG (plain FP64 Jacobi-PCG, the default)
+ * or FX_SOLVER_IR (per instance FP32 Jacobi-PCG to inner_rtol inside FP64 refinement to the
+ * options' tolerance, as fx_solver_newton with an FX_SOLVER_IR solver: FP32 operator on the
+ * stored point tangents, FP64 return map and residuals; per instance the same bits). */
+int fx_nbatch_set_inner(fx_nbatch* b, int32_t method, double inner_rtol);
 void fx_nbatch_destroy(fx_nbatch* b);
 int fx_nbatch_layout(const fx_nbatch* b, int64_t* offsets, int64_t* equations);
 fx_force* fx_nbatch_force(fx_nbatch* b);

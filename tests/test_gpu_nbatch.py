@@ -53,3 +53,25 @@ def test_layout():
     v = [np.arange(n, dtype=float) + i for i, n in enumerate(b.equations)]
     back = b.split(b.combine(v))
     assert all(np.array_equal(a, c) for a, c in zip(back, v))
+
+
+def test_mixed_batched_newton_equals_single_mixed_paths():
+    """FP32 CG inside FP64 refinement per instance (fx_nbatch_set_inner): each instance's history
+    and Newton solve counts bit for bit those of the single-instance path with a
+    MixedPrecisionSolver of the same tolerances, and close to the plain FP64 batch."""
+    inst = instances()
+    factors = stages.cyclic_factors(1, 8)
+    args = ([m for m, _, _ in inst], [F for _, F, _ in inst], factors, [mon for _, _, mon in inst])
+    mixed = stages.batched_load_path(*args, tol=1e-6, mixed=True, inner_tolerance=1e-4)
+    plain = stages.batched_load_path(*args, tol=1e-6)
+    assert mixed.converged
+    for i, (mesh, F, mon) in enumerate(inst):
+        ir = fx.MixedPrecisionSolver(fx.SolveOptions(relative_tolerance=1e-12, max_iterations=20000),
+                                     inner_tolerance=1e-4)
+        single = stages.load_path(fx.InternalForce(mesh), torch.as_tensor(F, device=DEV), factors, mon, tol=1e-6,
+                                  solver=ir)
+        assert single.converged
+        assert np.array_equal(mixed.monitor[:, i], single.monitor), i
+        assert np.array_equal(mixed.newton[:, i], single.newton), i
+        peak = np.max(np.abs(plain.monitor[:, i]))
+        assert np.max(np.abs(mixed.monitor[:, i] - plain.monitor[:, i])) <= 1e-6 * peak, i
