@@ -236,7 +236,8 @@ def batched_j2_comparison(device, count=32, steps=8, seed=1):
     (nx = ny in {1, 2, 4, 8}, nz in [20, 40]) on one cyclic top-shear cycle of `steps` load steps
     (load-controlled, 1.2 x the first-yield bending load), Newton to ||r|| <= 1e-6 N per step
     with Jacobi-PCG to 1e-12: the batched Newton (one combined mesh, per-instance Newton and CG on
-    the device) against the same instances solved one at a time by the single-instance path.
+    the device) against the same instances solved one at a time by the single-instance path, and
+    the batch with FP32 CG inside FP64 refinement (the FP32 operator on the point tangents).
     Instance-steps/s by wall clock around each arm; the two arms' histories are compared bit for
     bit."""
     import torch
@@ -262,7 +263,15 @@ def batched_j2_comparison(device, count=32, steps=8, seed=1):
     torch.cuda.synchronize(dev)
     secs = time.perf_counter() - t0
     same = all(np.array_equal(b.monitor[:, i], single[i].monitor) for i in range(count))
+    # the same batch with FP32 CG inside FP64 refinement (FP32 apply, FP64 return map)
+    stages.batched_load_path(meshes[:2], fs[:2], factors[:1], mons[:2], device=device, mixed=True)  # warm-up
+    bm = stages.batched_load_path(meshes, fs, factors, mons, device=device, mixed=True)
+    peak = float(np.max(np.abs(b.monitor)))
     return {"instances": count, "elements": int(sum(m.count for m in meshes)),
+            "mixed_batched_instance_steps_per_s": count * len(factors) / bm.seconds,
+            "mixed_refinements_per_linear_solve": float(bm.refinements.sum() / max(1, bm.newton.sum())),
+            "mixed_converged": bool(bm.converged),
+            "mixed_vs_plain_max_abs_diff_over_peak": float(np.max(np.abs(bm.monitor - b.monitor))) / peak,
             "equations": int(sum(m.num_equations for m in meshes)), "load_steps": len(factors),
             "batched_instance_steps_per_s": count * len(factors) / b.seconds,
             "one_at_a_time_instance_steps_per_s": count * len(factors) / secs,

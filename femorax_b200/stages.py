@@ -110,6 +110,7 @@ class BatchedPathResult:
     newton: np.ndarray           # [steps, instances]: Newton solves
     converged: bool
     seconds: float               # wall time of the steps
+    refinements: np.ndarray = None  # [steps, instances]: refinement rounds (mixed)
 
 
 def batched_load_path(meshes, fext_units, factors, monitor_eqs, tol: float = 1e-6, cg_rtol: float = 1e-12,
@@ -127,7 +128,7 @@ def batched_load_path(meshes, fext_units, factors, monitor_eqs, tol: float = 1e-
     F = torch.as_tensor(b.combine(fext_units), device=dev)
     u = torch.zeros(b.total, dtype=torch.float64, device=dev)
     idx = torch.as_tensor(np.asarray(b.offsets[:-1]) + np.asarray(monitor_eqs), device=dev)
-    mon, nit = [], []
+    mon, nit, refs = [], [], []
     ok = True
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -137,9 +138,10 @@ def batched_load_path(meshes, fext_units, factors, monitor_eqs, tol: float = 1e-
         b.commit_state()
         mon.append(u[idx].clone())
         nit.append(it)
+        refs.append([r.refinements for r in res])
     torch.cuda.synchronize(dev)
     secs = time.perf_counter() - t0
-    return BatchedPathResult(torch.stack(mon).cpu().numpy(), np.array(nit), ok, secs)
+    return BatchedPathResult(torch.stack(mon).cpu().numpy(), np.array(nit), ok, secs, np.array(refs))
 
 
 def j2_instances(count: int, seed: int = 0, sizes=(1, 2, 4, 8, 16, 24), nz_range=(20, 400), h: float = 0.5,
