@@ -35,7 +35,7 @@ constexpr int64_t kMaxSlotChunks = 2048;  // one level of chunk sums: n <= 2048 
 // per-slot scalars
 enum : int {
   S_RZ = 0, S_PAP, S_ALPHA, S_BETA, S_RNORM, S_TOL, S_RHS, S_RR, S_RZNEW, S_INIT,  // inner CG
-  O_RR, O_BB, O_BNORM, O_RNORM, O_INIT,                                             // outer
+  O_RR, O_BB, O_BNORM, O_RNORM, O_INIT, O_PREV,                                     // outer
   NSC = 16
 };
 // per-slot flags
@@ -135,8 +135,9 @@ __global__ void __launch_bounds__(32 * kWarps)
   }
 }
 
-// per slot: the outer test (ir: ||b - K x|| <= max(rtol ||b||, atol)), then the inner solve's
-// limits, or the end of the slot's solve
+// per slot: the outer test (ir: ||b - K x|| <= max(rtol ||b||, atol); given up at the limits or
+// when a round did not halve ||b - K x||), then the inner solve's limits, or the end of the
+// slot's solve
 __global__ void k_b_outer(double* sc, int* fl, const int* used, int nslots, double rtol, double atol, int max_outer,
                           int max_it) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -154,9 +155,10 @@ __global__ void k_b_outer(double* sc, int* fl, const int* used, int nslots, doub
   if (rn <= (tol > atol ? tol : atol)) {
     f[G_CONV] = 1;
     f[G_FIN] = 1;
-  } else if (f[G_OUTER] >= max_outer || f[G_INNER] >= max_it) {
-    f[G_FIN] = 1;
+  } else if (f[G_OUTER] >= max_outer || f[G_INNER] >= max_it || (f[G_OUTER] > 0 && rn > kIrStall * c[O_PREV])) {
+    f[G_FIN] = 1;  // the limits, or a round that did not halve the FP64 residual
   }
+  c[O_PREV] = rn;
   if (f[G_FIN]) {
     f[F_DONE] = 1;
     f[G_INNER_RAN] = 0;

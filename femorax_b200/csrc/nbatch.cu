@@ -27,6 +27,7 @@ constexpr int64_t kMaxInstanceChunks = 2048;  // one level of chunk sums per ins
 enum : int {
   N_RN = 0, N_BB, N_RZ, N_PAP, N_ALPHA, N_BETA, N_RR, N_RZNEW, N_TOL, N_RNORM,
   N_QBB, N_QRR, N_QBNORM,  // refinement: b.b, q.q (q = b - K du), ||b||
+  N_QPREV,                 // refinement: ||q|| of the previous round
   NNS = 16
 };
 enum : int {
@@ -320,8 +321,10 @@ __global__ void __launch_bounds__(32 * kWarps)
                [&](int64_t i, const Ops<double, 2>& o) { q[i] = o.v[0] - o.v[1]; });
 }
 
-// the refinement test: finished at ||q|| <= max(rtol ||b||, atol) or at the round or inner
-// iteration limit; otherwise an inner solve follows (G_CG_DONE = 0)
+// the refinement test: finished at ||q|| <= max(rtol ||b||, atol), at the round or inner
+// iteration limit, or when the last round did not halve ||q|| (the FP64 residual has reached
+// what FP64 can resolve: Solver::ir's stagnation test); otherwise an inner solve follows
+// (G_CG_DONE = 0)
 __global__ void k_nb_ir_test(double* sc, int* fl, int count, double rtol, double atol, int max_outer, int max_it) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= count) return;
@@ -331,10 +334,12 @@ __global__ void k_nb_ir_test(double* sc, int* fl, int count, double rtol, double
   if (f[G_IR_OUTER] == 0) c[N_QBNORM] = sqrt(c[N_QBB]);
   const double rn = sqrt(c[N_QRR]);
   const double tol = rtol * c[N_QBNORM];
-  if (rn <= (tol > atol ? tol : atol) || f[G_IR_OUTER] >= max_outer || f[G_IR_INNER] >= max_it) {
+  const bool stalled = f[G_IR_OUTER] > 0 && rn > kIrStall * c[N_QPREV];
+  if (rn <= (tol > atol ? tol : atol) || stalled || f[G_IR_OUTER] >= max_outer || f[G_IR_INNER] >= max_it) {
     f[G_IR_DONE] = 1;
     return;
   }
+  c[N_QPREV] = rn;
   f[G_CG_DONE] = 0;
 }
 

@@ -606,7 +606,7 @@ void Solver::gmres(const double* b, double* x, fx_solve_result* res) {
 void Solver::ir(const double* b, double* x, fx_solve_result* res) {
   res->rhs_norm = -1.0;
   int outer = 0, inner_total = 0;
-  double bnorm = 0.0;
+  double bnorm = 0.0, prev = 0.0;
   const int max_outer = 50;
   for (;;) {
     apply64(x, ap.ptr, nullptr);
@@ -629,6 +629,10 @@ void Solver::ir(const double* b, double* x, fx_solve_result* res) {
       res->converged = 1;
       break;
     }
+    // a round that did not halve the FP64 residual: it has reached what FP64 resolves for this
+    // operator (the FP32 corrections now only move rounding), so more rounds gain nothing
+    if (outer > 0 && rn > kIrStall * prev) break;
+    prev = rn;
     if (outer >= max_outer || inner_total >= o.max_iterations) break;
     // inner: K d = r in FP32 from d = 0
     k_to_f32<<<ew(n), 256, 0, cs>>>(r.ptr, r32.ptr, n);

@@ -8,6 +8,11 @@
 namespace fx {
 
 constexpr int64_t kChunk = 2048;
+// Iterative refinement (FP32 inner solves, FP64 residuals) ends a linear solve when a round
+// leaves the FP64 residual above this fraction of the previous round's: the residual has then
+// reached the level that FP64 resolves for the operator, and further FP32 corrections only move
+// rounding (the stagnation test of mixed-precision refinement, Carson & Higham 2018).
+constexpr double kIrStall = 0.5;
 __host__ __device__ inline int64_t chunks_of(int64_t n) { return (n + kChunk - 1) / kChunk; }
 
 // A lane's pass over a chunk in the documented order: use(i, load(i)) for i = begin + k,

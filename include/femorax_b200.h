@@ -277,8 +277,11 @@ typedef struct fx_solve_result {
  *                     (KrylovSolver::solve, src/solvers/krylov.cpp:25-41).
  *   FX_SOLVER_IR      CG in FP32 (FP32 operator and vectors) inside FP64 iterative refinement:
  *                     r = b - K x in FP64, K d = r by FP32 PCG to inner_rtol, x += d in FP64,
- *                     until ||b - K x|| <= rtol ||b|| in FP64. The FP32 operator is
- *                     fx_apply_operator_f32's (box kernel, or the FP32 Gauss-point form). */
+ *                     until ||b - K x|| <= rtol ||b|| in FP64 (converged), or until a round
+ *                     leaves ||b - K x|| above half the previous round's (the FP64 residual's
+ *                     floor for this operator: not converged, x kept), or 50 rounds. The FP32
+ *                     operator is fx_apply_operator_f32's (box kernel, or the FP32 Gauss-point
+ *                     form). */
 #define FX_SOLVER_CG 0
 #define FX_SOLVER_GMRES 1
 #define FX_SOLVER_KRYLOV 2

@@ -4,7 +4,8 @@
 - CG / GMRES / Krylov: the solution of the oracle's solver within 1e-8 relative (iterates differ by
   rounding: the GPU vector kernels fuse multiply-adds), and the true FP64 residual, computed by
   the oracle's operator, below the requested tolerance;
-- FP32 CG in FP64 iterative refinement: true FP64 residual <= 1e-8 relative;
+- FP32 CG in FP64 iterative refinement: true FP64 residual <= 1e-8 relative; below the FP64
+  floor it stops when a round no longer halves the residual;
 - ExplicitDifference: displacements after 200 steps within 1e-10 relative of the oracle's; the
   FP32 run's recorded acceleration within 2e-3 of the largest FP64 value.
 """
@@ -152,6 +153,33 @@ def test_mixed_precision_refinement(name, oracle_mod):
     assert r.converged and r.refinements >= 1
     res = b - port.apply_operator(k, x.cpu().numpy())
     assert np.linalg.norm(res) <= 1.0001e-8 * np.linalg.norm(b)
+
+
+def test_refinement_stops_at_the_fp64_floor():
+    """A tolerance below what FP64 resolves (1e-20 relative): refinement stops at the first round
+    that does not halve the FP64 residual, well before the 50-round limit, unconverged, with a
+    residual at the FP64 level; the engine's slots stop by the same test."""
+    spec, k = SOLVE_CASES["static_cube"]
+    mesh, force, _ = build(spec)
+    b = np.random.default_rng(6).standard_normal(mesh.num_equations)
+    s = fx.MixedPrecisionSolver(fx.SolveOptions(relative_tolerance=1e-20, max_iterations=200000),
+                                inner_tolerance=1e-4)
+    s.setup(fx.MatrixFreeOperator(force, fx.OperatorCoefficients(*k)))
+    x = torch.zeros(mesh.num_equations, dtype=torch.float64, device=DEV)
+    r = s.solve(t(b), x)
+    assert not r.converged
+    assert 2 <= r.refinements < 15, r.refinements
+    assert r.final_residual <= 1e-12 * r.rhs_norm
+    e = fx.BatchEngine(1 << 20, 2, k=fx.OperatorCoefficients(*k),
+                       options=fx.SolveOptions(relative_tolerance=1e-20, max_iterations=200000))
+    slot = e.admit(force, b)
+    for _ in range(60):
+        e.round()
+        if e.finished(slot):
+            break
+    xe, re = e.retire(slot)
+    assert not re.converged and re.refinements == r.refinements
+    assert np.array_equal(xe, x.cpu().numpy())
 
 
 def test_explicit_difference_matches_oracle(oracle_mod):
