@@ -448,9 +448,13 @@ int fx_apply_operator_host(fx_force* f, fx_coeffs k, const double* xh, double* y
     FX_REQUIRE(f && (f->s.neq == 0 || (xh && yh)), "fx_apply_operator_host: bad arguments");
     auto st = static_cast<cudaStream_t>(stream);
     const size_t bytes = sizeof(double) * static_cast<size_t>(f->s.neq);
-    FX_CUDA(cudaMemcpyAsync(f->s.wx.ptr, xh, bytes, cudaMemcpyHostToDevice, st));
     const double kk[3] = {k.stiffness, k.damping, k.mass};
     f->s.initial = k.initial != 0;
+    if (fx::box_apply_host(f->s, kk, xh, yh, st)) {  // page-locked buffers: copies and tiles overlapped
+      FX_CUDA(cudaStreamSynchronize(st));
+      return;
+    }
+    FX_CUDA(cudaMemcpyAsync(f->s.wx.ptr, xh, bytes, cudaMemcpyHostToDevice, st));
     if (f->s.use_box()) fx::box_apply(f->s, kk, f->s.wx.ptr, f->s.wy.ptr, st);
     else fx::general_apply(f->s, kk, f->s.wx.ptr, f->s.wy.ptr, st);
     FX_CUDA(cudaMemcpyAsync(yh, f->s.wy.ptr, bytes, cudaMemcpyDeviceToHost, st));

@@ -322,6 +322,8 @@ void box_build_plan(ForceState& s) {
   p.nz = nz;
   for (int d = 0; d < 3; ++d) p.h[d] = h[d];
   p.node_eq.upload(packed);
+  p.node_eq_h = std::move(packed);
+  p.pipe.variant = -1;
   p.queue.upload(std::vector<int>(2, 0));
   p.elem_param.upload(eparam);
   p.grid_node_h = std::move(gnode);
@@ -551,6 +553,168 @@ void fill_args(ForceState& s, const double k[3], const void* x, void* y, const i
   std::memcpy(dst, &a, sizeof(a));
 }
 }  // namespace
+
+// ------------------------------------------------------------------ host-buffer apply in pieces
+BoxPlan::HostPipe::~HostPipe() {
+  for (cudaEvent_t e : ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : ev_comp) cudaEventDestroy(e);
+  if (ev_start) cudaEventDestroy(ev_start);
+  if (ev_done) cudaEventDestroy(ev_done);
+  if (in) cudaStreamDestroy(in);
+  if (comp) cudaStreamDestroy(comp);
+  if (out) cudaStreamDestroy(out);
+}
+
+namespace {
+
+constexpr int kHostChunks = 8;              // equation ranges of the host apply
+constexpr int64_t kHostPipeMinEq = 262144;  // smaller meshes: one copy each way
+
+// The ranges, the tile order and the final prefixes of y for the FP64 operator's shape. Tile
+// (bx, by, bz) reads the nodes i0 - 1 .. i0 + BX - 1, j0 - 1 .. j0 + BY - 1 of planes k0 - 1 .. k1
+// (the staged slots of box_tile, clipped to the grid) and owns, writing their equations,
+// i0 .. i0 + BX - 2, j0 .. j0 + BY - 2 of planes k0 .. k1 - 1.
+void build_pipe(ForceState& s) {
+  BoxPlan& p = s.box;
+  BoxPlan::HostPipe& h = p.pipe;
+  const BoxPlan::Shape& sh = p.shape[0][0];
+  if (h.variant == sh.variant && h.kz == sh.kz) return;
+  const int BX = kVariantBlock[sh.variant][0], BY = kVariantBlock[sh.variant][1], kz = sh.kz;
+  const int NX = p.nx + 1, NY = p.ny + 1, NZ = p.nz + 1;
+  const int gx = (NX + BX - 2) / (BX - 1), gy = (NY + BY - 2) / (BY - 1), gz = (NZ + kz - 1) / kz;
+  const int ntiles = gx * gy * gz;
+  // first and last equation of each grid node (-1: none free)
+  auto lo_of = [&](int64_t g) -> int64_t {
+    const uint32_t w = static_cast<uint32_t>(p.node_eq_h[g]);
+    return (w >> 29) ? static_cast<int64_t>(w & 0x1FFFFFFFu) : -1;
+  };
+  auto hi_of = [&](int64_t g) -> int64_t {
+    const uint32_t w = static_cast<uint32_t>(p.node_eq_h[g]);
+    const int n = __builtin_popcount(w >> 29);
+    return n ? static_cast<int64_t>(w & 0x1FFFFFFFu) + n - 1 : -1;
+  };
+  std::vector<int64_t> need(ntiles, -1);
+  for (int bz = 0; bz < gz; ++bz)
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx) {
+        const int t = (bz * gy + by) * gx + bx;
+        const int i0 = bx * (BX - 1), j0 = by * (BY - 1), k0 = bz * kz, k1 = std::min(k0 + kz, NZ);
+        for (int k = std::max(k0 - 1, 0); k <= std::min(k1, NZ - 1); ++k)
+          for (int j = std::max(j0 - 1, 0); j <= std::min(j0 + BY - 1, NY - 1); ++j)
+            for (int i = std::max(i0 - 1, 0); i <= std::min(i0 + BX - 1, NX - 1); ++i)
+              need[t] = std::max(need[t], hi_of(static_cast<int64_t>(k) * NY * NX + static_cast<int64_t>(j) * NX + i));
+      }
+  const int C = kHostChunks;
+  h.chunks = C;
+  h.edge.assign(C + 1, 0);
+  for (int c = 0; c <= C; ++c) h.edge[c] = static_cast<int64_t>(s.neq) * c / C;
+  auto range_of = [&](int64_t q) {  // the range holding equation q (q < 0: the first)
+    if (q < 0) return 0;
+    return static_cast<int>(std::upper_bound(h.edge.begin(), h.edge.end(), q) - h.edge.begin()) - 1;
+  };
+  std::vector<int> order(ntiles), rng(ntiles);
+  for (int t = 0; t < ntiles; ++t) {
+    order[t] = t;
+    rng[t] = range_of(need[t]);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rng[a] < rng[b]; });
+  h.seg.assign(C + 1, 0);
+  for (int t = 0; t < ntiles; ++t) ++h.seg[rng[t] + 1];
+  for (int c = 0; c < C; ++c) h.seg[c + 1] += h.seg[c];
+  // the range of each equation's owner tile, then y's final prefix after each range
+  std::vector<int8_t> eq_rng(static_cast<size_t>(s.neq), -1);
+  for (int bz = 0; bz < gz; ++bz)
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx) {
+        const int t = (bz * gy + by) * gx + bx;
+        const int i0 = bx * (BX - 1), j0 = by * (BY - 1), k0 = bz * kz, k1 = std::min(k0 + kz, NZ);
+        for (int k = k0; k < k1; ++k)
+          for (int j = j0; j <= std::min(j0 + BY - 2, NY - 1); ++j)
+            for (int i = i0; i <= std::min(i0 + BX - 2, NX - 1); ++i) {
+              const int64_t g = static_cast<int64_t>(k) * NY * NX + static_cast<int64_t>(j) * NX + i;
+              for (int64_t q = lo_of(g); q >= 0 && q <= hi_of(g); ++q) eq_rng[q] = static_cast<int8_t>(rng[t]);
+            }
+      }
+  h.ready.assign(C, s.neq);
+  int pm = -1, c = 0;
+  for (int64_t q = 0; q < s.neq; ++q) {
+    pm = std::max(pm, static_cast<int>(eq_rng[q]));
+    for (; c < pm; ++c) h.ready[c] = q;  // ranges before pm end their prefix at q
+  }
+  h.tiles.upload(order);
+  if (!h.in) {
+    FX_CUDA(cudaStreamCreateWithFlags(&h.in, cudaStreamNonBlocking));
+    FX_CUDA(cudaStreamCreateWithFlags(&h.comp, cudaStreamNonBlocking));
+    FX_CUDA(cudaStreamCreateWithFlags(&h.out, cudaStreamNonBlocking));
+    FX_CUDA(cudaEventCreateWithFlags(&h.ev_start, cudaEventDisableTiming));
+    FX_CUDA(cudaEventCreateWithFlags(&h.ev_done, cudaEventDisableTiming));
+  }
+  while (static_cast<int>(h.ev_in.size()) < C) {
+    cudaEvent_t a, b;
+    FX_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    FX_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    h.ev_in.push_back(a);
+    h.ev_comp.push_back(b);
+  }
+  h.variant = sh.variant;
+  h.kz = sh.kz;
+}
+
+bool page_locked(const void* ptr) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+bool box_apply_host(ForceState& s, const double k[3], const double* xh, double* yh, cudaStream_t st) {
+  if (!s.use_box() || s.neq < kHostPipeMinEq || !page_locked(xh) || !page_locked(yh)) return false;
+  ensure_coef(s, 0, k);
+  build_pipe(s);
+  BoxPlan::HostPipe& h = s.box.pipe;
+  BoxArgs<double> a = args<double>(s, 0, s.wx.ptr, nullptr, s.wy.ptr);
+  if (k[2] != 0.0 && s.has_nodal_mass) {
+    a.nm1 = s.nodal_mass.ptr;
+    a.c1 = k[2];
+  }
+  if (k[1] != 0.0 && s.has_nodal_alpha) {
+    a.nm2 = s.nodal_alpha_mass.ptr;
+    a.c2 = k[1];
+  }
+  a.kz = s.box.shape[0][0].kz;
+  // the three streams start after the work already on st
+  FX_CUDA(cudaEventRecord(h.ev_start, st));
+  FX_CUDA(cudaStreamWaitEvent(h.in, h.ev_start, 0));
+  FX_CUDA(cudaStreamWaitEvent(h.comp, h.ev_start, 0));
+  FX_CUDA(cudaStreamWaitEvent(h.out, h.ev_start, 0));
+  for (int c = 0; c < h.chunks; ++c) {
+    const int64_t e0 = h.edge[c], n = h.edge[c + 1] - e0;
+    if (n > 0) FX_CUDA(cudaMemcpyAsync(s.wx.ptr + e0, xh + e0, sizeof(double) * n, cudaMemcpyHostToDevice, h.in));
+    FX_CUDA(cudaEventRecord(h.ev_in[c], h.in));
+  }
+  int64_t sent = 0;
+  for (int c = 0; c < h.chunks; ++c) {
+    FX_CUDA(cudaStreamWaitEvent(h.comp, h.ev_in[c], 0));
+    a.tiles = h.tiles.ptr + h.seg[c];
+    a.ntiles = h.seg[c + 1] - h.seg[c];
+    launch<double, 0>(s.box, a, h.comp);
+    FX_CUDA(cudaEventRecord(h.ev_comp[c], h.comp));
+    // the last range's wait also keeps the call from returning before every tile has run
+    if (h.ready[c] > sent || c == h.chunks - 1) FX_CUDA(cudaStreamWaitEvent(h.out, h.ev_comp[c], 0));
+    if (h.ready[c] > sent) {
+      FX_CUDA(cudaMemcpyAsync(yh + sent, s.wy.ptr + sent, sizeof(double) * (h.ready[c] - sent),
+                              cudaMemcpyDeviceToHost, h.out));
+      sent = h.ready[c];
+    }
+  }
+  FX_CUDA(cudaEventRecord(h.ev_done, h.out));
+  FX_CUDA(cudaStreamWaitEvent(st, h.ev_done, 0));
+  return true;
+}
 
 size_t box_args_bytes(bool f32) { return f32 ? sizeof(BoxArgs<float>) : sizeof(BoxArgs<double>); }
 

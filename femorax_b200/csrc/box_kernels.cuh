@@ -53,7 +53,9 @@ struct BoxArgs {
   const int* skip;  // when set and nonzero on the device, the launch does nothing (a finished solve)
   const T* __restrict__ escale;  // per-element E scale (sets that differ only in E), or NULL
   int* queue;       // persistent launch: [next tile, CTAs done]; NULL: one CTA per tile (the grid)
-  int gx, gy, gz;   // tiles per axis (persistent launch)
+  const int* tiles;  // tile-list launch: CTA b takes tile tiles[b] (x fastest); NULL: the grid
+  int ntiles;        // (host side) the list's length
+  int gx, gy, gz;   // tiles per axis (persistent and tile-list launches)
   int cset;         // (host side) the coefficient set whose tables the launch passes
 };
 
@@ -514,6 +516,11 @@ __device__ __forceinline__ void box_tile(const BoxArgs<T>& a, const BoxTable<typ
 template <int BX, int BY, class T, int MODE, int MINB, bool CACHE, int CM, bool FULL>
 __global__ void __launch_bounds__(BX* BY, MINB)
     k_box(BoxArgs<T> a, const __grid_constant__ BoxTable<typename Coef<T>::type> tab) {
+  if (a.tiles) {  // a part of the grid's tiles, in the list's order
+    const int tile = a.tiles[blockIdx.x];
+    box_tile<BX, BY, T, MODE, CACHE, CM, FULL>(a, &tab, tile % a.gx, (tile / a.gx) % a.gy, tile / (a.gx * a.gy));
+    return;
+  }
   if (!a.queue) {
     box_tile<BX, BY, T, MODE, CACHE, CM, FULL>(a, &tab, blockIdx.x, blockIdx.y, blockIdx.z);
     return;
@@ -551,6 +558,9 @@ __global__ void __launch_bounds__(BX* BY, MINB)
 // ------------------------------------------------------------------ launch variants
 // (BX, BY, CTAs per SM for the register budget, face caching)
 constexpr int kNumVariants = 10;  // see launch()
+// the block of element columns (BX, BY) of each variant, for the host's tile geometry
+constexpr int kVariantBlock[kNumVariants][2] = {{32, 8}, {16, 16}, {16, 8}, {32, 16}, {16, 8},
+                                                {16, 8}, {16, 8},  {32, 4}, {16, 32}, {16, 8}};
 
 template <class T>
 const BoxTable<typename Coef<T>::type>& table_of(const BoxPlan& p, int mode);
@@ -579,7 +589,14 @@ void launch_kernel(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     resident = std::max(resident, 1);
   }
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
-  if (p.shape[sizeof(T) == 4 ? 1 : 0][MODE == 1 ? 1 : 0].persistent) {
+  if (a.tiles) {
+    BoxArgs<T> b = a;
+    b.queue = nullptr;
+    b.gx = static_cast<int>(grid.x);
+    b.gy = static_cast<int>(grid.y);
+    b.gz = static_cast<int>(grid.z);
+    if (a.ntiles > 0) kern<<<a.ntiles, BX * BY, S::bytes, st>>>(b, table_of<T>(p, a.cset));
+  } else if (p.shape[sizeof(T) == 4 ? 1 : 0][MODE == 1 ? 1 : 0].persistent) {
     BoxArgs<T> b = a;
     b.queue = p.queue.ptr;
     b.gx = static_cast<int>(grid.x);

@@ -114,6 +114,27 @@ struct BoxPlan {
     double k[3] = {0, 0, 0};
     bool built = false;
   } cset[3];
+  std::vector<int32_t> node_eq_h;  // node_eq on the host (the host apply's tile ranges)
+  // The host-buffer apply in pieces (box_apply_host): x arrives in `chunks` equation ranges on
+  // one stream, the tiles that read only arrived equations run as each range lands (tiles sorted
+  // by the last equation they read), and after the tiles of range c have run, y leaves up to
+  // ready[c], the longest prefix of equations whose owners have all run, on a third stream: the
+  // two copy directions overlap each other and the kernel. Built for the FP64 operator's launch
+  // shape (variant, kz).
+  struct HostPipe {
+    int variant = -1, kz = 0, chunks = 0;
+    std::vector<int64_t> edge;   // [chunks + 1] equation boundaries of the ranges
+    std::vector<int> seg;        // [chunks + 1]: the tiles of range c are tiles[seg[c] .. seg[c+1])
+    std::vector<int64_t> ready;  // [chunks]: y[0 .. ready[c]) is final after the tiles of range c
+    DeviceArray<int> tiles;     // tile ids (x fastest), by the last equation each reads
+    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    std::vector<cudaEvent_t> ev_in, ev_comp;
+    cudaEvent_t ev_start = nullptr, ev_done = nullptr;
+    HostPipe() = default;
+    HostPipe(const HostPipe&) = delete;
+    HostPipe& operator=(const HostPipe&) = delete;
+    ~HostPipe();
+  } pipe;
 };
 
 // Buffers of the explicit step loop (ground motion, step counter, force, recorded history),
@@ -203,6 +224,10 @@ void box_force_w_f32(ForceState& s, const float* w, const float* v, float* f, cu
 int box_num_variants();
 void box_set_launch(ForceState& s, int variant, int kz);
 void box_autotune(ForceState& s, cudaStream_t st);
+// y = K_eff x from and to host buffers on the box path, copies and kernel overlapped in equation
+// ranges (BoxPlan::HostPipe) when both buffers are page-locked and the mesh is large enough;
+// returns false, having done nothing, otherwise (the caller then copies, applies and copies back)
+bool box_apply_host(ForceState& s, const double k[3], const double* xh, double* yh, cudaStream_t st);
 // Batches of box grids in one launch: the per-grid descriptor (box_args_bytes bytes, written by
 // box_fill_args for y = K_eff x with operator coefficients k, FP64 or FP32 vectors x, y and a
 // skip flag), the grid's tile counts, and the launch over a work list of

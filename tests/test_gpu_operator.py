@@ -193,3 +193,35 @@ def test_launch_variants_agree(oracle_mod):
                 fref = f.clone()
             assert torch.equal(y, ref), (variant, kz)
             assert f is None or torch.equal(f, fref), (variant, kz)
+
+
+@pytest.mark.parametrize("name", ["layered", "rollers"])
+def test_host_apply_in_pieces_bitwise(name):
+    """The host-buffer apply on a box grid of more than 262,144 equations with page-locked buffers
+    copies x in and y out in equation ranges, overlapped with the tiles that read only arrived
+    equations: the device apply's bits for every launch shape (the tile order is rebuilt when the
+    shape changes, persistent shapes included), and the same as with pageable buffers (one copy
+    each way). Rollers: nodes with one or two free DOFs."""
+    spec = meshes.layered_box(64, 64, 24, layers=3, seed=2)[0] if name == "layered" else roller_block(70, 60, 40)
+    mesh, force, _ = build(spec)
+    n = mesh.num_equations
+    assert force.info()["path"] == "box" and n > 262144
+    k = fx.OperatorCoefficients(1.0, 0.3, 2.0)
+    x = np.random.default_rng(16).standard_normal(n)
+    xp = torch.from_numpy(x).pin_memory()
+    yp = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    yn = np.empty(n)
+    from femorax_b200 import _lib as L
+    lib = L.lib()
+    for shape in (None, (0, 5), (8, 12), (2, -10), (2, 10)):
+        if shape is not None:
+            L.check(lib.fx_force_set_launch(force._h, *shape))
+        y = torch.zeros(n, dtype=torch.float64, device=DEV)
+        force.apply_operator(k, t(x), y)
+        want = y.cpu().numpy()
+        yp.fill_(np.nan)
+        force.apply_operator_host(k, xp.numpy(), yp.numpy())
+        assert np.array_equal(yp.numpy(), want), shape
+        yn.fill(np.nan)
+        force.apply_operator_host(k, x, yn)
+        assert np.array_equal(yn, want), shape
