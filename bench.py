@@ -15,6 +15,7 @@ own InternalForce::apply_operator (built here from its sources, oracle/_ref) on 
 
 `explicit` times the explicit wave configuration's stepping (FP64 and FP32, 4000 steps);
 `newmark` compares the Newmark stage with plain FP64 and mixed-precision inner solves;
+`pimy` times PressureIndependMultiYield material-point updates on the device (and on one host core);
 `batched_j2` compares the batched J2 Newton with one instance at a time on a bounded sample;
 `served` compares solves/s and p50/p99 latency at a 1e-8 FP64 residual on a stream of static solves:
 the batched mixed-precision engine behind the serving loop versus plain FP64 CG one at a time;
@@ -194,6 +195,72 @@ def explicit_comparison(force, mesh, comp, device, steps=4000):
     peak = float(np.max(np.abs(hist["f64"])))
     out["f32_history_max_abs_diff_over_peak"] = float(np.max(np.abs(hist["f32"] - hist["f64"]))) / peak
     return out
+
+
+def pimy_points(device, n=1 << 20, steps=10, sample=8192, seed=0):
+    """PressureIndependMultiYield material points (fx_pimy_update): n points of a frictional sand
+    (20 surfaces, friction angle 30 degrees, pressure-dependent moduli) on seeded strain paths,
+    switched to the plastic stage under confinement, then `steps` cyclic-shear updates with the
+    tangent, timed by CUDA events on the launching stream. Point-updates/s and the HBM traffic one
+    update needs (committed and trial state, strain, stress, tangent); the host restatement of the
+    same arithmetic on `sample` points on one core beside it."""
+    import torch
+    import femorax_b200 as fx
+    m = fx.PressureIndependMultiYield(2.0, 60000, 150000, 5, 0.1, 30, 80, 0.5, 20)
+    dev = torch.device("cuda", device)
+    rng = np.random.default_rng(seed)
+    amp = torch.as_tensor(rng.uniform(2e-4, 2e-2, n), device=dev)
+    dirs = torch.as_tensor(rng.standard_normal((3, n)), device=dev)
+    dirs /= dirs.norm(dim=0)
+    conf = torch.as_tensor(rng.uniform(-2e-3, -5e-4, n), device=dev)
+    c, t = m.initial_state(n, device), torch.empty((m.nstate, n), dtype=torch.float64, device=dev)
+    sig = torch.empty((6, n), dtype=torch.float64, device=dev)
+    tan = torch.empty((36, n), dtype=torch.float64, device=dev)
+    failed = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def strain(k):
+        e = torch.zeros((6, n), dtype=torch.float64, device=dev)
+        e[0:3] = conf / 3
+        e[3:6] = amp * float(np.sin(2 * np.pi * k / steps)) * dirs
+        return e.contiguous()
+
+    eps = [strain(k) for k in range(steps + 1)]
+    m.update(0, c, t, eps[0], sig, tan, failed)  # confinement, elastic stage
+    c, t = t, c
+    m.update(1, c, t, eps[0], sig, tan, failed)  # the switch to the plastic stage
+    c, t = t, c
+    stream = torch.cuda.current_stream(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize(dev)
+    ev[0].record(stream)
+    for k in range(1, steps + 1):
+        m.update(1, c, t, eps[k], sig, tan, failed, stream)
+        c, t = t, c
+    ev[1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev[0].elapsed_time(ev[1])
+    per_point = 2 * m.nstate * 8 + 6 * 8 + 6 * 8 + 36 * 8
+    # host: the same arithmetic on a sample of the same points, one core
+    hs = slice(0, sample)
+    hc, ht = m.initial_state(sample), np.zeros((m.nstate, sample))
+    hsig, htan = np.zeros((6, sample)), np.zeros((36, sample))
+    heps = [np.ascontiguousarray(e[:, hs].cpu().numpy()) for e in eps]
+    m.update_host(0, hc, ht, heps[0], hsig, htan)
+    hc, ht = ht, hc
+    m.update_host(1, hc, ht, heps[0], hsig, htan)
+    hc, ht = ht, hc
+    t0 = time.perf_counter()
+    for k in range(1, steps + 1):
+        m.update_host(1, hc, ht, heps[k], hsig, htan)
+        hc, ht = ht, hc
+    host_s = time.perf_counter() - t0
+    same = bool(np.allclose(sig[:, hs].cpu().numpy(), hsig, rtol=0, atol=1e-12 * float(np.max(np.abs(hsig)))))
+    rate = n * steps / (ms * 1e-3)
+    return {"points": n, "surfaces": m.surfaces, "steps": steps, "ms_per_update": ms / steps,
+            "point_updates_per_s": rate, "bytes_per_point_update": per_point,
+            "achieved_gbs": rate * per_point / 1e9, "failed_points": int(failed.item()),
+            "host_one_core_point_updates_per_s": sample * steps / host_s, "host_sample_points": sample,
+            "device_vs_host_sample_within_1e-12": same}
 
 
 def newmark_comparison(device, n=100, steps=20, seed=0):
@@ -527,6 +594,7 @@ def run_ours(args):
     served_rates = serve_rate_sweep(local) if world == 1 and not args.no_serve else None
     batched_j2 = batched_j2_comparison(local) if world == 1 and not args.no_serve else None
     newmark = newmark_comparison(local) if world == 1 and not args.no_serve else None
+    pimy = pimy_points(local) if world == 1 and not args.no_serve else None
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -552,7 +620,8 @@ def run_ours(args):
             "served_mixed": served_mixed,
             "served_rates": served_rates,
             "batched_j2": batched_j2,
-            "newmark": newmark}
+            "newmark": newmark,
+            "pimy": pimy}
     print(json.dumps(line))
     return 0
 

@@ -358,6 +358,82 @@ class InternalForce:
             self._h = None
 
 
+class PressureIndependMultiYield:
+    """Material points of OpenSees' nDMaterial PressureIndependMultiYield, 3D (fx_pimy_*; the
+    reference's PressureIndependMultiYield<NS>, src/physics/materials/pressure_independ_multi_yield.hpp):
+    the constructor's arguments in OpenSees' order and defaults, `pairs` the (gamma, G/Gmax) pairs of
+    a user backbone (noYieldSurf pairs) or None.
+
+    States are [nstate, npoints] arrays (value-major: value k of every point contiguous), strains
+    and stresses [6, npoints] (11 22 33 12 23 31; engineering shear strains), tangents
+    [36, npoints] (entry 6 r + c). update() works on device tensors, update_host() on numpy arrays;
+    both write the trial state in full, so a commit is a swap of the committed and trial arrays.
+    `stage` is the material stage (0 elastic, 1 plastic: updateMaterialStage)."""
+
+    def __init__(self, rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng=0.0, refPress=100.0,
+                 pressDependCoe=0.0, noYieldSurf=20, pairs=None):
+        in9, p9 = _f64([rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng, refPress,
+                        pressDependCoe, noYieldSurf])
+        pp = None
+        if pairs is not None and len(pairs):
+            self._pairs = np.ascontiguousarray(pairs, np.float64).ravel()
+            if self._pairs.size != 2 * int(noYieldSurf):
+                raise ValueError("a user backbone has noYieldSurf (gamma, G/Gmax) pairs")
+            pp = self._pairs.ctypes.data_as(L.p_f64)
+        h = C.c_void_p()
+        check(lib().fx_pimy_create(p9, pp, C.byref(h)))
+        self._h = h
+        ns, nsurf = C.c_int32(), C.c_int32()
+        check(lib().fx_pimy_info(h, C.byref(ns), C.byref(nsurf)))
+        self.nstate, self.surfaces = ns.value, nsurf.value
+
+    def setup_values(self):
+        """(residual pressure, friction angle, cohesion), surface sizes [40], plastic moduli [40]."""
+        out = np.zeros(83)
+        check(lib().fx_pimy_setup_values(self._h, out.ctypes.data_as(L.p_f64)))
+        return out[:3], out[3:43], out[43:83]
+
+    def initial_state(self, npoints, device=None):
+        """The state of npoints new points: a torch tensor on `device` (an index), or numpy."""
+        if device is None:
+            s = np.zeros((self.nstate, npoints))
+            check(lib().fx_pimy_init_host(self._h, npoints, s.ctypes.data_as(L.p_f64)))
+            return s
+        import torch
+        s = torch.empty((self.nstate, npoints), dtype=torch.float64, device=torch.device("cuda", device))
+        check(lib().fx_pimy_init(self._h, npoints, _ptr(s), None))
+        return s
+
+    def update(self, stage, committed, trial, strain, stress, tangent=None, failed=None, stream=None):
+        n = committed.shape[1]
+        check(lib().fx_pimy_update(self._h, int(stage), n, _ptr(committed), _ptr(trial), _ptr(strain), _ptr(stress),
+                                   _ptr(tangent), _ptr(failed), _stream(stream)))
+
+    def update_host(self, stage, committed, trial, strain, stress, tangent=None) -> int:
+        """Returns the points that met a state OpenSees stops for (their stress is NaN)."""
+        n = committed.shape[1]
+        bad = C.c_int32(0)
+        arrs = [committed, trial, strain, stress] + ([tangent] if tangent is not None else [])
+        for a in arrs:
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("host arrays must be C-contiguous float64")
+        check(lib().fx_pimy_update_host(self._h, int(stage), n, committed.ctypes.data_as(L.p_f64),
+                                        trial.ctypes.data_as(L.p_f64), strain.ctypes.data_as(L.p_f64),
+                                        stress.ctypes.data_as(L.p_f64),
+                                        tangent.ctypes.data_as(L.p_f64) if tangent is not None else None,
+                                        C.byref(bad)))
+        return bad.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().fx_pimy_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
 class GroundMotions:
     """exec::GroundMotions (src/exec/ground_motion.hpp:22-70): UniformExcitation patterns with
     Path series, evaluated on the device. add(): one pattern in DOF `dof` (0-based) with factor

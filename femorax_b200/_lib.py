@@ -114,6 +114,15 @@ PROTOTYPES = {
     "fx_vops_destroy": (None, [vp]),
     "fx_vops_dot": (C.c_int, [vp, vp, vp, C.c_int64, vp, p_f64, vp]),
     "fx_dot_noalloc": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, p_f64, vp]),
+    "fx_pimy_create": (C.c_int, [p_f64, p_f64, C.POINTER(vp)]),
+    "fx_pimy_destroy": (None, [vp]),
+    "fx_pimy_info": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "fx_pimy_setup_values": (C.c_int, [vp, p_f64]),
+    "fx_pimy_init": (C.c_int, [vp, C.c_int64, vp, vp]),
+    "fx_pimy_update": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]),
+    "fx_pimy_init_host": (C.c_int, [vp, C.c_int64, p_f64]),
+    "fx_pimy_update_host": (C.c_int, [vp, C.c_int32, C.c_int64, p_f64, p_f64, p_f64, p_f64, p_f64,
+                                      C.POINTER(C.c_int32)]),
     "fx_axpy": (C.c_int, [C.c_double, vp, vp, C.c_int64, vp]),
     "fx_xpay": (C.c_int, [vp, C.c_double, vp, C.c_int64, vp]),
     "fx_multiply": (C.c_int, [vp, vp, vp, C.c_int64, vp]),

@@ -45,6 +45,7 @@ CUDA_SOURCES = [
     ("stepping.cu", []),
     ("batch.cu", []),
     ("nbatch.cu", []),
+    ("pimy.cu", ["--fmad=false"]),
 ]
 CXX_SOURCES = ["api.cpp", "compile.cpp"]
 

@@ -434,6 +434,41 @@ int fx_engine_finished(fx_engine* e, int32_t slot, int32_t* finished);
 int fx_engine_retire(fx_engine* e, int32_t slot, double* x_host, fx_solve_result* r);
 int fx_engine_info(const fx_engine* e, int64_t* info);
 
+/* ------------------------------------------------------------------ PressureIndependMultiYield
+ * Material points of the multi-yield-surface von Mises soil model (OpenSees nDMaterial
+ * PressureIndependMultiYield, 3D; the reference's PressureIndependMultiYield<NS>,
+ * src/physics/materials/pressure_independ_multi_yield.hpp: setup :102-139, initial_state :141-149,
+ * update :218-224, the material stage of updateMaterialStage as `stage`). At most 40 surfaces.
+ *   fx_pimy_create       in9 = rho, refShearModul, refBulkModul, cohesi, peakShearStra,
+ *                        frictionAng, refPress, pressDependCoe, noYieldSurf; pairs = noYieldSurf
+ *                        (gamma, G/Gmax) pairs of a user backbone, or NULL (hyperbolic backbone).
+ *                        FX_E_INVALID for inputs OpenSees rejects, FX_E_UNSUPPORTED above 40
+ *                        surfaces.
+ *   fx_pimy_info         state values per point (30 + 8 surfaces) and the surfaces.
+ *   fx_pimy_setup_values out[83] = residual pressure, friction angle, cohesion after setup, the 40
+ *                        surface sizes, the 40 plastic moduli (surfaces past noYieldSurf 0).
+ *   fx_pimy_init         the state of npoints new points (device; value k of point i at
+ *                        state[k npoints + i]).
+ *   fx_pimy_update       per point i: total strain strain[c npoints + i] (11 22 33 12 23 31,
+ *                        engineering shear) from the committed state to the trial state (both
+ *                        laid out as in fx_pimy_init; the trial state is written in full, so a
+ *                        commit is a swap of the two buffers), stress[c npoints + i], the tangent
+ *                        tangent[(6 r + c) npoints + i] (NULL: not stored), and *failed (device,
+ *                        may be NULL) += the points that met a state OpenSees stops the program
+ *                        for (their stress is NaN).
+ *   fx_pimy_*_host       the same arithmetic on host arrays (failed: a host counter). */
+typedef struct fx_pimy fx_pimy;
+int fx_pimy_create(const double* in9, const double* pairs, fx_pimy** out);
+void fx_pimy_destroy(fx_pimy* m);
+int fx_pimy_info(const fx_pimy* m, int32_t* nstate, int32_t* surfaces);
+int fx_pimy_setup_values(const fx_pimy* m, double* out);
+int fx_pimy_init(fx_pimy* m, int64_t npoints, double* state, void* stream);
+int fx_pimy_update(fx_pimy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
+                   const double* strain, double* stress, double* tangent, int32_t* failed, void* stream);
+int fx_pimy_init_host(const fx_pimy* m, int64_t npoints, double* state);
+int fx_pimy_update_host(const fx_pimy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
+                        const double* strain, double* stress, double* tangent, int32_t* failed);
+
 #ifdef __cplusplus
 }
 #endif

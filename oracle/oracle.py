@@ -84,6 +84,12 @@ def ref():
         L.fxref_brick_operator.argtypes = [p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, C.c_int, p_i32]
         L.fxref_brick_critical_dt.restype = C.c_double
         L.fxref_brick_critical_dt.argtypes = [p_f64, p_f64, C.c_int, p_f64]
+        L.fxref_pimy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
+        L.fxref_pimy_destroy.argtypes = [vp]
+        L.fxref_pimy_nstate.restype = C.c_int32
+        L.fxref_pimy_setup_values.argtypes = [vp, p_f64]
+        L.fxref_pimy_initial_state.argtypes = [vp, p_f64]
+        L.fxref_pimy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
         _ref = L
     return _ref
 
@@ -544,6 +550,56 @@ class RefMotions:
     def __del__(self):
         if getattr(self, "h", None):
             ref().fxref_motions_destroy(self.h)
+
+
+class RefPimy:
+    """The reference's PressureIndependMultiYield (40-surface bucket) at one material point
+    (oracle/_ref): params9 = rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng,
+    refPress, pressDependCoe, noYieldSurf; pairs: (gamma, G/Gmax) pairs or empty."""
+
+    def __init__(self, params9, pairs=()):
+        p9, pp = _f(params9)
+        pr = np.ascontiguousarray(pairs, np.float64)
+        h = vp()
+        rc = ref().fxref_pimy_create(pp, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2, C.byref(h))
+        assert rc == 0, rc
+        self.h = h
+        self.nstate = ref().fxref_pimy_nstate()
+
+    def setup_values(self):
+        """residualPress, frictionAngle, cohesion; surface sizes and plastic moduli (1..40)."""
+        out = np.zeros(83)
+        ref().fxref_pimy_setup_values(self.h, out.ctypes.data_as(p_f64))
+        return out[:3], out[3:43], out[43:83]
+
+    def initial_state(self):
+        s = np.zeros(self.nstate)
+        ref().fxref_pimy_initial_state(self.h, s.ctypes.data_as(p_f64))
+        return s
+
+    def update(self, stage, committed, eps):
+        """(trial state, stress, tangent) at total strain eps from the committed state."""
+        committed, pc = _f(committed)
+        eps, pe = _f(eps)
+        trial, sig, D = np.zeros(self.nstate), np.zeros(6), np.zeros((6, 6))
+        ref().fxref_pimy_update(self.h, stage, pc, trial.ctypes.data_as(p_f64), pe, sig.ctypes.data_as(p_f64),
+                                D.ctypes.data_as(p_f64))
+        return trial, sig, D
+
+    def replay(self, stage, pre, pre_eps, eps):
+        """A golden path: per step the stage, an optional discarded trial, the update, the commit.
+        Returns the stresses [n, 6] and tangents [n, 6, 6]."""
+        c = self.initial_state()
+        sig, D = np.zeros((len(eps), 6)), np.zeros((len(eps), 6, 6))
+        for k in range(len(eps)):
+            if pre[k]:
+                self.update(int(stage[k]), c, pre_eps[k])
+            c, sig[k], D[k] = self.update(int(stage[k]), c, eps[k])
+        return sig, D
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().fxref_pimy_destroy(self.h)
 
 
 def port_dot(x, y, lanes, fused):

@@ -21,6 +21,7 @@
 #include "exec/matrix_free_operator.hpp"
 #include "physics/elements/std_brick.hpp"
 #include "physics/materials/elastic_isotropic.hpp"
+#include "physics/materials/pressure_independ_multi_yield.hpp"
 #include "physics/operators/element_operator.hpp"
 #include "solvers/cg.hpp"
 #include "solvers/gmres.hpp"
@@ -439,6 +440,54 @@ int fxref_motions_evaluate(fxref_motions* h, double t, double* accel) {
   } catch (const std::exception& e) {
     return fail(e);
   }
+}
+
+// ---- PressureIndependMultiYield (the reference's material, 40-surface bucket), one point at a
+// time: in9 = rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng, refPress,
+// pressDependCoe, noYieldSurf; pairs (gamma, G/Gmax) or NULL.
+using Pimy40 = femorax::PressureIndependMultiYield<40>;
+struct fxref_pimy {
+  Pimy40::Params p{};
+  std::vector<double> pairs;
+};
+
+int fxref_pimy_create(const double* in9, const double* pairs, int32_t npairs, fxref_pimy** out) {
+  auto h = std::make_unique<fxref_pimy>();
+  if (pairs && npairs > 0) h->pairs.assign(pairs, pairs + 2 * npairs);
+  Pimy40::Input in{};
+  in.rho = in9[0];
+  in.refShearModul = in9[1];
+  in.refBulkModul = in9[2];
+  in.cohesi = in9[3];
+  in.peakShearStra = in9[4];
+  in.frictionAng = in9[5];
+  in.refPress = in9[6];
+  in.pressDependCoe = in9[7];
+  in.numberOfYieldSurf = static_cast<int>(in9[8]);
+  in.gredu = h->pairs.empty() ? nullptr : h->pairs.data();
+  const int rc = Pimy40::setup(in, h->p);
+  if (rc != Pimy40::Ok) return rc;
+  *out = h.release();
+  return 0;
+}
+void fxref_pimy_destroy(fxref_pimy* h) { delete h; }
+int32_t fxref_pimy_nstate() { return Pimy40::NSTATE; }
+// the setup's results: residualPress, frictionAngle, cohesion, then size[1..40], modulus[1..40]
+void fxref_pimy_setup_values(const fxref_pimy* h, double* out) {
+  out[0] = h->p.residualPress;
+  out[1] = h->p.frictionAngle;
+  out[2] = h->p.cohesion;
+  for (int i = 1; i <= 40; ++i) {
+    out[2 + i] = h->p.size[i];
+    out[42 + i] = h->p.modulus[i];
+  }
+}
+void fxref_pimy_initial_state(const fxref_pimy* h, double* s) { Pimy40::initial_state(h->p, {s, 1}); }
+// update at total strain eps (engineering shear) from `committed`: trial state, stress, tangent
+void fxref_pimy_update(fxref_pimy* h, int32_t stage, const double* committed, double* trial, const double* eps,
+                       double* sig, double* D) {
+  h->p.loadStage = stage;
+  Pimy40::update(h->p, {committed, 1}, {trial, 1}, eps, sig, reinterpret_cast<double(*)[6]>(D));
 }
 
 }  // extern "C"

@@ -9,8 +9,13 @@ the reference checkout and the oracle library exist):
   compile_maps.npz    the reference's compile_model output (oracle/_ref/libfxref.so) for two
                       small models: a 4 x 3 x 5 block with two Rayleigh regions (RCM, coloring)
                       and a 3 x 2 x 8 soil column with laminar equalDOF ties.
+  pimy_paths.npz      the reference's stored OpenSees PressureIndependMultiYield strain paths
+                      (tests/reference/data/nd/PressureIndependMultiYield_*.txt, read as text):
+                      per path the material's parameters and backbone pairs, and per step the
+                      load stage, the discarded trial strain (if any), the strain, and OpenSees'
+                      stress and tangent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [bricks|compile_maps|pimy_paths ...]
 """
 import glob
 import os
@@ -23,6 +28,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 DATA = "/root/reference/tests/reference/data/element"
+ND = "/root/reference/tests/reference/data/nd"
+PIMY_PARAMS = ("rho", "refShearModul", "refBulkModul", "cohesi", "peakShearStra", "frictionAng", "refPress",
+               "pressDependCoe", "noYieldSurf")
 
 
 def read_reference_file(path):
@@ -94,6 +102,30 @@ def compile_maps():
     print("compile_maps.npz written")
 
 
+def pimy_paths():
+    out, cases = {}, []
+    for path in sorted(glob.glob(os.path.join(ND, "PressureIndependMultiYield_*.txt"))):
+        name = os.path.basename(path)[len("PressureIndependMultiYield_"):-len(".txt")]
+        h, rows = read_reference_file(path)
+        col = {c: i for i, c in enumerate(h["columns"])}
+        p = h["params"]
+        params = dict(zip(p[0::2], map(float, p[1::2])))
+        out[name + "/params"] = np.array([params[k] for k in PIMY_PARAMS])
+        out[name + "/pairs"] = np.array(list(map(float, h.get("pairs", []))))
+        out[name + "/stage"] = rows[:, col["stage"]].astype(np.int8)
+        out[name + "/pre"] = rows[:, col["pre"]].astype(np.int8)
+        out[name + "/pre_eps"] = rows[:, col["pre0"]:col["pre0"] + 6]
+        out[name + "/eps"] = rows[:, col["eps0"]:col["eps0"] + 6]
+        out[name + "/sig"] = rows[:, col["sig0"]:col["sig0"] + 6]
+        out[name + "/D"] = rows[:, col["D00"]:col["D00"] + 36].reshape(-1, 6, 6)
+        cases.append(name)
+    out["cases"] = np.array(cases)
+    out["param_names"] = np.array(PIMY_PARAMS)
+    np.savez_compressed(os.path.join(HERE, "pimy_paths.npz"), **out)
+    print("pimy_paths.npz:", len(cases), "paths")
+
+
 if __name__ == "__main__":
-    bricks()
-    compile_maps()
+    what = sys.argv[1:] or ["bricks", "compile_maps", "pimy_paths"]
+    for w in what:
+        globals()[w]()
