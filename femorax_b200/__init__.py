@@ -277,13 +277,29 @@ class InternalForce:
         check(lib().fx_mass_times_ground(self._h, direction, _ptr(y), _stream(stream)))
 
     def commit_state(self, stream=None):
-        """InternalForce::commit_state (internal_force.cpp:507-509): the trial J2 state becomes
-        the committed one."""
+        """InternalForce::commit_state (internal_force.cpp:507-509): the trial J2 and
+        PressureIndependMultiYield states become the committed ones."""
         check(lib().fx_force_commit(self._h, _stream(stream)))
 
     def plastic_points(self) -> int:
         n = C.c_int64()
         check(lib().fx_force_plastic_points(self._h, C.byref(n)))
+        return n.value
+
+    def set_pimy(self, param_set: int, material: "PressureIndependMultiYield"):
+        """Binds a PressureIndependMultiYield material to a parameter set (fx_force_set_pimy): the
+        set's elements become stdBrick elements with that material's points, elastic stage."""
+        check(lib().fx_force_set_pimy(self._h, int(param_set), material._h))
+        self._materials = getattr(self, "_materials", {})
+        self._materials[int(param_set)] = material
+
+    def set_material_stage(self, param_set: int, stage: int):
+        """updateMaterialStage for a PressureIndependMultiYield set (InternalForce::set_material_stage)."""
+        check(lib().fx_force_set_material_stage(self._h, int(param_set), int(stage)))
+
+    def pimy_failed(self) -> int:
+        n = C.c_int64()
+        check(lib().fx_force_pimy_failed(self._h, C.byref(n)))
         return n.value
 
     J2_STATE = {"committed": (0, 13), "trial": (1, 13), "tangent": (2, 8)}

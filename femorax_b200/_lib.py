@@ -121,6 +121,9 @@ PROTOTYPES = {
     "fx_pimy_init": (C.c_int, [vp, C.c_int64, vp, vp]),
     "fx_pimy_update": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]),
     "fx_pimy_init_host": (C.c_int, [vp, C.c_int64, p_f64]),
+    "fx_force_set_pimy": (C.c_int, [vp, C.c_int32, vp]),
+    "fx_force_set_material_stage": (C.c_int, [vp, C.c_int32, C.c_int32]),
+    "fx_force_pimy_failed": (C.c_int, [vp, C.POINTER(C.c_int64)]),
     "fx_pimy_update_host": (C.c_int, [vp, C.c_int32, C.c_int64, p_f64, p_f64, p_f64, p_f64, p_f64,
                                       C.POINTER(C.c_int32)]),
     "fx_axpy": (C.c_int, [C.c_double, vp, vp, C.c_int64, vp]),

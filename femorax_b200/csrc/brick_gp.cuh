@@ -30,8 +30,9 @@ struct ParamGP {  // one parameter set as the element kernels read it
   double b[3];
   double alphaM, betaK, betaKinit, betaKcomm;
   int mass_type;  // 0 consistent, 1 lumped
-  int kind;       // 0 elastic, 1 J2
+  int kind;       // 0 elastic, 1 J2, 2 PressureIndependMultiYield
   double sigma_y, H, hk;
+  int table;      // kind 2: the set's entry in the PressureIndependMultiYield table
 };
 
 struct PointShape {

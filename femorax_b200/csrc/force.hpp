@@ -10,6 +10,7 @@
 
 #include "brick_gp.cuh"
 #include "common.cuh"
+#include "pimy_element.cuh"
 
 namespace fx {
 
@@ -183,6 +184,15 @@ struct ForceState {
   bool initial = false;  // the operator's stiffness term takes the initial (elastic) matrix
   DeviceArray<double> j2_committed, j2_trial, j2_tan;
   DeviceArray<int> plastic_dev;  // plastic points of the last force evaluation
+  // PressureIndependMultiYield sets (general path): the materials bound to parameter sets (table,
+  // with their stages), and per Gauss point value k of the state at [(k * 8 + gp) * P + e] (as many
+  // values as the largest material holds), value c of the compact tangent likewise
+  bool has_pimy = false;
+  std::vector<PimySet> pimy_h;
+  DeviceArray<PimySet> pimy_dev;
+  DeviceArray<double> pimy_committed, pimy_trial, pimy_tan;
+  DeviceArray<int> pimy_failed;  // points whose update met a state OpenSees stops for (cumulative)
+  int pimy_nstate = 0;
   ExplicitWork xw;
   bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
   bool use_box_force() const { return use_box() && box.force_ok; }

@@ -28,7 +28,8 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
                                                            int32_t count, double ks, double kd, double km, int unit_dir,
                                                            const double* __restrict__ x, double* __restrict__ slots,
                                                            const int* skip, const double* __restrict__ j2tan,
-                                                           int initial) {
+                                                           int initial, const PimySet* __restrict__ pimy,
+                                                           const double* __restrict__ ptan) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count || (skip && *skip)) return;
   const ParamGP p = params[param[e]];
@@ -41,6 +42,7 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
   }
   const OpFactors f = op_factors(p, ks, kd, km);
   if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
+  else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, P, f.cK, initial != 0});
   else element_apply(p, f, xl, xe, ye);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
 }
@@ -50,7 +52,8 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
                                                           const ParamGP* __restrict__ params, int32_t N, int32_t P,
                                                           int32_t count, double ks, double kd, double km,
                                                           double* __restrict__ slots, const double* __restrict__ j2tan,
-                                                          int initial) {
+                                                          int initial, const PimySet* __restrict__ pimy,
+                                                          const double* __restrict__ ptan) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -60,6 +63,8 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
   for (int a = 0; a < 24; ++a) eqe[a] = eq[static_cast<int64_t>(a) * P + e];
   const OpFactors f = op_factors(p, ks, kd, km);
   if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
+  else if (p.kind == 2)
+    element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, P, f.cK, initial != 0});
   else element_diagonal(p, f, xl, eqe, de);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = de[a];
 }
@@ -70,7 +75,10 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
                                                            int32_t count, const double* __restrict__ u,
                                                            const double* __restrict__ v, double* __restrict__ slots,
                                                            const double* __restrict__ j2c, double* __restrict__ j2t,
-                                                           double* __restrict__ j2tan, int* __restrict__ plastic) {
+                                                           double* __restrict__ j2tan, int* __restrict__ plastic,
+                                                           const PimySet* __restrict__ pimy,
+                                                           const double* __restrict__ pc, double* __restrict__ pt,
+                                                           double* __restrict__ ptan, int* __restrict__ failed) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -84,6 +92,11 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
   if (p.kind == 1) {
     const int np = element_force_j2(p, xl, ue, ve, j2c + e, j2t + e, j2tan + e, P, fe);
     if (np) atomicAdd(plastic, np);
+  } else if (p.kind == 2) {
+    int bad = 0;
+    const int np = element_force_pimy(p, pimy[p.table], xl, ue, ve, pc + e, pt + e, ptan + e, P, fe, &bad);
+    if (np) atomicAdd(plastic, np);
+    if (bad) atomicAdd(failed, bad);
   } else {
     element_force(p, xl, ue, ve, fe);
   }
@@ -230,6 +243,8 @@ __global__ void __launch_bounds__(256) k_gather32(const int32_t* __restrict__ st
 }  // namespace
 
 void general_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st, const int* skip) {
+  if (s.has_pimy)
+    throw Error(FX_E_UNSUPPORTED, "the FP32 operator has no PressureIndependMultiYield tangent form");
   if (s.count > 0 && s.geom32.n == 0) {  // the FP32 geometric factors, once
     s.geom32.alloc(static_cast<size_t>(kGeom32) * 8 * s.P);
     s.nshape32.alloc(64);
@@ -255,7 +270,8 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
   if (s.count > 0)
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
-                                                                   -1, x, s.slots.ptr, skip, s.j2_tan.ptr, s.initial);
+                                                                   -1, x, s.slots.ptr, skip, s.j2_tan.ptr, s.initial,
+                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr);
   FX_LAUNCH_CHECK("element_apply");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -269,7 +285,8 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
   if (s.count > 0)
     k_element_diag<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                   s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
-                                                                  s.slots.ptr, s.j2_tan.ptr, s.initial);
+                                                                  s.slots.ptr, s.j2_tan.ptr, s.initial,
+                                                                  s.pimy_dev.ptr, s.pimy_tan.ptr);
   FX_LAUNCH_CHECK("element_diagonal");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -280,12 +297,14 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
 }
 
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
-  if (s.has_j2) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
+  if (s.has_j2 || s.has_pimy) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
   if (s.count > 0)
     k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr,
                                                                    s.j2_committed.ptr, s.j2_trial.ptr, s.j2_tan.ptr,
-                                                                   s.plastic_dev.ptr);
+                                                                   s.plastic_dev.ptr, s.pimy_dev.ptr,
+                                                                   s.pimy_committed.ptr, s.pimy_trial.ptr,
+                                                                   s.pimy_tan.ptr, s.pimy_failed.ptr);
   FX_LAUNCH_CHECK("element_force");
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
@@ -307,7 +326,8 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
   if (s.count > 0)
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, 0.0, 0.0, 1.0, dir,
-                                                                   nullptr, s.slots.ptr, nullptr, s.j2_tan.ptr, 0);
+                                                                   nullptr, s.slots.ptr, nullptr, s.j2_tan.ptr, 0,
+                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr);
   FX_LAUNCH_CHECK("element_apply_unit");
   if (s.neq > 0)
     k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,

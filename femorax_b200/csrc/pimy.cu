@@ -10,6 +10,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "force.hpp"
 #include "host.hpp"
 #include "pimy.cuh"
 
@@ -61,6 +62,27 @@ __global__ void __launch_bounds__(128) k_pimy_update(const pimy::Params* __restr
 }
 
 unsigned blocks_for(int64_t n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+// The points of the elements of parameter set `set` (bound to table entry m): the material's new
+// state in both buffers and the elastic compact tangent of the material's moduli.
+__global__ void k_pimy_elements_init(const int32_t* __restrict__ param, int32_t count, int32_t P, int32_t set,
+                                     const PimySet* __restrict__ m, double* __restrict__ committed,
+                                     double* __restrict__ trial, double* __restrict__ tan) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count || param[e] != set) return;
+  const pimy::Params& p = m->p;
+  for (int gp = 0; gp < 8; ++gp) {
+    pimy::initial_state(p, pimy::Slab<double>{committed + static_cast<int64_t>(gp) * P + e, 8 * static_cast<int64_t>(P)});
+    pimy::initial_state(p, pimy::Slab<double>{trial + static_cast<int64_t>(gp) * P + e, 8 * static_cast<int64_t>(P)});
+    const double t[pimy::kTan] = {0.0, p.G0, p.K0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int c = 0; c < pimy::kTan; ++c) tan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = t[c];
+  }
+}
+
+// host table -> device, in place (kernels and captured graphs keep the pointer)
+void upload_table(ForceState& s) {
+  FX_CUDA(cudaMemcpy(s.pimy_dev.ptr, s.pimy_h.data(), sizeof(PimySet) * s.pimy_h.size(), cudaMemcpyHostToDevice));
+}
 
 }  // namespace
 }  // namespace fx
@@ -131,6 +153,79 @@ int fx_pimy_update(fx_pimy* h, int32_t stage, int64_t npoints, const double* com
     fx::k_pimy_update<<<fx::blocks_for(npoints, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
         h->dev.ptr, stage, npoints, committed, trial, strain, stress, tangent, failed);
     FX_LAUNCH_CHECK("pimy_update");
+  });
+}
+
+int fx_force_set_pimy(fx_force* f, int32_t set, const fx_pimy* m) {
+  return fx::guard([&] {
+    if (!f || !m) throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: bad arguments");
+    fx::ForceState& s = f->s;
+    if (set < 0 || set >= s.nparams) throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: no such parameter set");
+    fx::ParamGP& q = s.params_h[set];
+    if (q.kind == FX_MAT_J2) throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: the set is a J2 set");
+    if (q.betaK != 0.0 || q.betaKinit != 0.0 || q.betaKcomm != 0.0)
+      throw fx::Error(FX_E_UNSUPPORTED, "stiffness-proportional Rayleigh damping on a PressureIndependMultiYield set");
+    if (q.rho != m->p.rho)
+      throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: the set's density (its masses) differs from the material's");
+    const int need = fx::pimy::nstate(m->p.ns);
+    const int64_t P = s.P;
+    if (need > s.pimy_nstate) {  // (re)allocate the point arrays; earlier bindings start again
+      s.pimy_committed.alloc(static_cast<size_t>(need) * 8 * P);
+      s.pimy_trial.alloc(static_cast<size_t>(need) * 8 * P);
+      if (!s.pimy_tan.ptr) s.pimy_tan.alloc(static_cast<size_t>(fx::pimy::kTan) * 8 * P);
+      s.pimy_nstate = need;
+    }
+    if (!s.pimy_dev.ptr) s.pimy_dev.alloc(static_cast<size_t>(s.nparams));  // one entry per set at most
+    if (!s.plastic_dev.ptr) {
+      s.plastic_dev.alloc(1);
+      FX_CUDA(cudaMemset(s.plastic_dev.ptr, 0, sizeof(int)));
+    }
+    if (!s.pimy_failed.ptr) {
+      s.pimy_failed.alloc(1);
+      FX_CUDA(cudaMemset(s.pimy_failed.ptr, 0, sizeof(int)));
+    }
+    if (q.kind != 2) {
+      q.table = static_cast<int>(s.pimy_h.size());
+      s.pimy_h.push_back(fx::PimySet{m->p, 0});
+    } else {
+      s.pimy_h[q.table] = fx::PimySet{m->p, 0};
+    }
+    q.kind = 2;
+    fx::upload_table(s);
+    FX_CUDA(cudaMemcpy(s.params.ptr, s.params_h.data(), sizeof(fx::ParamGP) * s.params_h.size(), cudaMemcpyHostToDevice));
+    s.has_pimy = true;
+    s.box.qualifies = false;
+    s.box.why_not = "the mesh has PressureIndependMultiYield sets";
+    // every bound set's points start from their material's state (after a reallocation too)
+    for (int32_t k = 0; k < s.nparams; ++k)
+      if (s.params_h[k].kind == 2 && s.count > 0) {
+        fx::k_pimy_elements_init<<<fx::blocks_for(s.count, 128), 128>>>(s.param.ptr, s.count, s.P, k,
+                                                                        s.pimy_dev.ptr + s.params_h[k].table,
+                                                                        s.pimy_committed.ptr, s.pimy_trial.ptr,
+                                                                        s.pimy_tan.ptr);
+        FX_LAUNCH_CHECK("pimy_elements_init");
+      }
+    FX_CUDA(cudaStreamSynchronize(nullptr));
+  });
+}
+
+int fx_force_set_material_stage(fx_force* f, int32_t set, int32_t stage) {
+  return fx::guard([&] {
+    if (!f || (stage != 0 && stage != 1)) throw fx::Error(FX_E_INVALID, "fx_force_set_material_stage: bad arguments");
+    fx::ForceState& s = f->s;
+    if (set < 0 || set >= s.nparams || s.params_h[set].kind != 2)
+      throw fx::Error(FX_E_INVALID, "fx_force_set_material_stage: not a PressureIndependMultiYield set");
+    s.pimy_h[s.params_h[set].table].stage = stage;
+    fx::upload_table(s);
+  });
+}
+
+int fx_force_pimy_failed(const fx_force* f, int64_t* count) {
+  return fx::guard([&] {
+    if (!f || !count) throw fx::Error(FX_E_INVALID, "fx_force_pimy_failed: bad arguments");
+    int n = 0;
+    if (f->s.pimy_failed.ptr) FX_CUDA(cudaMemcpy(&n, f->s.pimy_failed.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    *count = n;
   });
 }
 

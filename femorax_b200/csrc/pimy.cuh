@@ -23,8 +23,10 @@
 #include <cmath>
 #include <cstdint>
 
-#ifndef FX_HD
-#define FX_HD __host__ __device__
+#ifdef __CUDACC__
+#define FX_PIMY_HD __host__ __device__
+#else
+#define FX_PIMY_HD
 #endif
 
 namespace fx {
@@ -37,7 +39,7 @@ constexpr double kVeryLarge = 1.0e200;      // a Vector divided by zero
 constexpr double kPi = 3.14159265358979;    // OpenSees' value
 
 enum : int { S_STRESS = 0, S_STRAIN = 13, S_ACTIVE = 26, S_E2P = 27, S_G = 28, S_K = 29, S_SURF = 30 };
-FX_HD constexpr int nstate(int ns) { return S_SURF + 8 * ns; }
+FX_PIMY_HD constexpr int nstate(int ns) { return S_SURF + 8 * ns; }
 
 // The material after setup: constructor values and the surfaces of setUpSurfaces ([0] unused).
 struct Params {
@@ -52,34 +54,34 @@ struct Params {
 enum : int { kOk = 0, kTooManySurfaces = 1, kBadFriction = 2, kBadModulus = 3, kTooFewPairs = 4, kBadInput = 5 };
 
 // ---- six-component vectors in OpenSees' Vector arithmetic
-FX_HD inline double dd(const double* a, const double* b) {  // tensor double-dot in vector form
+FX_PIMY_HD inline double dd(const double* a, const double* b) {  // tensor double-dot in vector form
   double r = 0.;
   for (int i = 0; i < 3; i++) r += a[i] * b[i] + 2 * a[i + 3] * b[i + 3];
   return r;
 }
-FX_HD inline void vset(double* a, const double* b) {
+FX_PIMY_HD inline void vset(double* a, const double* b) {
   for (int i = 0; i < 6; i++) a[i] = b[i];
 }
-FX_HD inline void vsub(double* a, const double* b) {
+FX_PIMY_HD inline void vsub(double* a, const double* b) {
   for (int i = 0; i < 6; i++) a[i] -= b[i];
 }
-FX_HD inline void vadd(double* a, const double* b) {
+FX_PIMY_HD inline void vadd(double* a, const double* b) {
   for (int i = 0; i < 6; i++) a[i] += b[i];
 }
-FX_HD inline void vscale(double* a, double f) {
+FX_PIMY_HD inline void vscale(double* a, double f) {
   for (int i = 0; i < 6; i++) a[i] *= f;
 }
-FX_HD inline void vdiv(double* a, double f) {
+FX_PIMY_HD inline void vdiv(double* a, double f) {
   if (f == 0.0) {
     for (int i = 0; i < 6; i++) a[i] = kVeryLarge;
   } else {
     for (int i = 0; i < 6; i++) a[i] /= f;
   }
 }
-FX_HD inline void vaxpy(double* a, const double* b, double f) {  // a += b f
+FX_PIMY_HD inline void vaxpy(double* a, const double* b, double f) {  // a += b f
   for (int i = 0; i < 6; i++) a[i] += b[i] * f;
 }
-FX_HD inline void vmul(double* a, const double* b, double f) {  // a = b f
+FX_PIMY_HD inline void vmul(double* a, const double* b, double f) {  // a = b f
   for (int i = 0; i < 6; i++) a[i] = b[i] * f;
 }
 
@@ -87,7 +89,7 @@ FX_HD inline void vmul(double* a, const double* b, double f) {  // a = b f
 // derived in the order of the setter that made it (so all 13 are kept, not recomputed).
 struct Ten {
   double t[6], d[6], m;
-  FX_HD void from_full(const double* v, bool engineering) {  // setData(vector, isEngrgStrain)
+  FX_PIMY_HD void from_full(const double* v, bool engineering) {  // setData(vector, isEngrgStrain)
     vset(t, v);
     m = (t[0] + t[1] + t[2]) / 3.0;
     for (int i = 0; i < 3; i++) {
@@ -99,7 +101,7 @@ struct Ten {
       }
     }
   }
-  FX_HD void from_dev(const double* dv, double mean) {  // setData(deviator, volume)
+  FX_PIMY_HD void from_dev(const double* dv, double mean) {  // setData(deviator, volume)
     m = mean;
     const double dm = (dv[0] + dv[1] + dv[2]) / 3.;
     for (int i = 0; i < 3; i++) {
@@ -109,25 +111,25 @@ struct Ten {
       t[i + 3] = d[i + 3];
     }
   }
-  FX_HD void engineering(double* out) const {  // t2Vector(1)
+  FX_PIMY_HD void engineering(double* out) const {  // t2Vector(1)
     vset(out, t);
     for (int i = 0; i < 3; i++) out[i + 3] *= 2.;
   }
-  FX_HD double dev_length() const { return sqrt(dd(d, d)); }
-  FX_HD double oct_shear() const { return sqrt(1. / 3.) * dev_length(); }
-  FX_HD bool zero() const {
+  FX_PIMY_HD double dev_length() const { return sqrt(dd(d, d)); }
+  FX_PIMY_HD double oct_shear() const { return sqrt(1. / 3.) * dev_length(); }
+  FX_PIMY_HD bool zero() const {
     for (int i = 0; i < 6; i++)
       if (t[i] != 0.0) return false;
     return true;
   }
   template <class V>
-  FX_HD void load(const V& s, int k) {
+  FX_PIMY_HD void load(const V& s, int k) {
     for (int i = 0; i < 6; i++) t[i] = s[k + i];
     for (int i = 0; i < 6; i++) d[i] = s[k + 6 + i];
     m = s[k + 12];
   }
   template <class V>
-  FX_HD void store(const V& s, int k) const {
+  FX_PIMY_HD void store(const V& s, int k) const {
     for (int i = 0; i < 6; i++) s[k + i] = t[i];
     for (int i = 0; i < 6; i++) s[k + 6 + i] = d[i];
     s[k + 12] = m;
@@ -139,12 +141,12 @@ template <class T>
 struct Slab {
   T* p;
   int64_t ld;
-  FX_HD T& operator[](int k) const { return p[k * ld]; }
+  FX_PIMY_HD T& operator[](int k) const { return p[k * ld]; }
 };
 
 // MultiYieldSurface's secondOrderEqn: the smaller non-negative root of A x^2 + B x + C; `ok` false
 // (and NaN) where OpenSees stops the program.
-FX_HD inline double quad_root(double A, double B, double C, bool& ok) {
+FX_PIMY_HD inline double quad_root(double A, double B, double C, bool& ok) {
   const double nan = static_cast<double>(NAN);
   if (A == 0) {
     ok = false;
@@ -178,7 +180,7 @@ FX_HD inline double quad_root(double A, double B, double C, bool& ok) {
   return r1 > r2 ? r2 : r1;
 }
 
-FX_HD inline void elastic_D(double G, double K, double* D) {  // D[6 i + j]
+FX_PIMY_HD inline void elastic_D(double G, double K, double* D) {  // D[6 i + j]
   for (int i = 0; i < 6; i++)
     for (int j = 0; j < 6; j++) {
       double v = 0.;
@@ -295,7 +297,7 @@ inline int setup(const double* in9, const double* pairs, Params& p) {
 }
 
 template <class V>
-FX_HD inline void initial_state(const Params& p, const V& s) {
+FX_PIMY_HD inline void initial_state(const Params& p, const V& s) {
   for (int k = 0; k < nstate(p.ns); ++k) s[k] = 0.0;
   s[S_G] = p.G0;
   s[S_K] = p.K0;
@@ -305,7 +307,29 @@ FX_HD inline void initial_state(const Params& p, const V& s) {
   }
 }
 
-FX_HD inline int to_int(double x) {  // C++ truncation, NaN 0 and clamped outside int
+// The tangent D[6 i + j] of a compact form t[kTan] (Point::compact): the elastic tangent of the
+// point's moduli in the elastic stage; in the plastic stage OpenSees' expression, elastic minus
+// coeff dv (x) dv (which is what it gives, signed zeros included, at an inactive point).
+constexpr int kTan = 10;
+FX_PIMY_HD inline void compact_D(const double* t, double* D) {
+  const double G = t[1], K = t[2];
+  if (t[0] != 1.0) {
+    elastic_D(G, K, D);
+    return;
+  }
+  const double coeff = t[3];
+  const double* dv = t + 4;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      double v = -coeff * dv[i] * dv[j];
+      if (i == j) v += G;
+      if (i < 3 && j < 3 && i == j) v += G;
+      if (i < 3 && j < 3) v += (K - 2. * G / 3.);
+      D[6 * i + j] = v;
+    }
+}
+
+FX_PIMY_HD inline int to_int(double x) {  // C++ truncation, NaN 0 and clamped outside int
   if (!(x == x)) return 0;
   if (x >= 2147483647.0) return 2147483647;
   if (x <= -2147483648.0) return -2147483647 - 1;
@@ -327,19 +351,19 @@ struct Point {
   int active_c = 0, active = 0, e2p = 0;
   double G = 0., K = 0.;
 
-  FX_HD Point(const Params& p, int st, CV c, TV t) : P(p), stage(st), C(c), T(t) {}
+  FX_PIMY_HD Point(const Params& p, int st, CV c, TV t) : P(p), stage(st), C(c), T(t) {}
 
-  FX_HD int at(int i) const { return S_SURF + 8 * (i - 1); }
-  FX_HD double size(int i) const { return i == 0 ? 0. : T[at(i)]; }
-  FX_HD double hmod(int i) const { return i == 0 ? 0. : T[at(i) + 1]; }
-  FX_HD void center(int i, double* c) const {
+  FX_PIMY_HD int at(int i) const { return S_SURF + 8 * (i - 1); }
+  FX_PIMY_HD double size(int i) const { return i == 0 ? 0. : T[at(i)]; }
+  FX_PIMY_HD double hmod(int i) const { return i == 0 ? 0. : T[at(i) + 1]; }
+  FX_PIMY_HD void center(int i, double* c) const {
     for (int k = 0; k < 6; ++k) c[k] = i == 0 ? 0. : T[at(i) + 2 + k];
   }
-  FX_HD void set_center(int i, const double* c) {
+  FX_PIMY_HD void set_center(int i, const double* c) {
     for (int k = 0; k < 6; ++k) T[at(i) + 2 + k] = c[k];
   }
 
-  FX_HD double yield(const Ten& s, int i) const {  // yieldFunc
+  FX_PIMY_HD double yield(const Ten& s, int i) const {  // yieldFunc
     double x[6], c[6];
     vset(x, s.d);
     center(i, c);
@@ -348,7 +372,7 @@ struct Point {
     return 3. / 2. * dd(x, x) - sz * sz;
   }
 
-  FX_HD void scale_deviator(Ten& s, int i) {  // deviatorScaling, its recursion as a loop
+  FX_PIMY_HD void scale_deviator(Ten& s, int i) {  // deviatorScaling, its recursion as a loop
     for (int it = 0; it < 100000; ++it) {
       const double diff = yield(s, i);
       if (i < P.ns && diff < 0.) {
@@ -374,7 +398,7 @@ struct Point {
     ok = false;
   }
 
-  FX_HD void init_surfaces() {  // initSurfaceUpdate
+  FX_PIMY_HD void init_surfaces() {  // initSurfaceUpdate
     if (active_c == 0) return;
     double dv[6];
     vset(dv, cur.d);
@@ -392,7 +416,7 @@ struct Point {
     }
   }
 
-  FX_HD void scale_to_confinement() {  // paramScaling
+  FX_PIMY_HD void scale_to_confinement() {  // paramScaling
     if (P.phi == 0.) return;
     const double h = -(cur.m - P.p_res);
     double f = -h / (P.pref - P.p_res);
@@ -408,7 +432,7 @@ struct Point {
     }
   }
 
-  FX_HD void elastic_to_plastic() {  // elast2Plast
+  FX_PIMY_HD void elastic_to_plastic() {  // elast2Plast
     e2p = 1;
     if (cur.m > 0. && P.phi > 0.) {  // tension dropped
       double dv[6];
@@ -428,7 +452,7 @@ struct Point {
     init_surfaces();
   }
 
-  FX_HD void set_trial_stress(const Ten& in) {  // setTrialStress (in may be `trial` itself)
+  FX_PIMY_HD void set_trial_stress(const Ten& in) {  // setTrialStress (in may be `trial` itself)
     const Ten s = in;
     double dv[6];
     vset(dv, s.d);
@@ -436,7 +460,7 @@ struct Point {
     trial.from_dev(dv, s.m);
   }
 
-  FX_HD int set_sub_rate() {  // setSubStrainRate
+  FX_PIMY_HD int set_sub_rate() {  // setSubStrainRate
     if (rate.zero()) return 0;
     double epm;
     if (active == 0) epm = 2 * G;
@@ -458,7 +482,7 @@ struct Point {
     return n;
   }
 
-  FX_HD void normal_at(const Ten& s, double* n) const {  // getSurfaceNormal
+  FX_PIMY_HD void normal_at(const Ten& s, double* n) const {  // getSurfaceNormal
     double c[6];
     vset(n, s.d);
     center(active, c);
@@ -466,7 +490,7 @@ struct Point {
     vdiv(n, sqrt(dd(n, n)));
   }
 
-  FX_HD void contact_stress(Ten& out) const {  // getContactStress
+  FX_PIMY_HD void contact_stress(Ten& out) const {  // getContactStress
     double c[6], dv[6];
     center(active, c);
     vset(dv, trial.d);
@@ -477,7 +501,7 @@ struct Point {
     out.from_dev(dv, trial.m);
   }
 
-  FX_HD bool reversal() const {  // isLoadReversal
+  FX_PIMY_HD bool reversal() const {  // isLoadReversal
     if (active == 0) return false;
     double n[6], a[6];
     normal_at(cur, n);
@@ -486,7 +510,7 @@ struct Point {
     return dd(a, n) < 0;
   }
 
-  FX_HD double loading(const Ten& contact, const double* n, int crossed) const {  // getLoadingFunc
+  FX_PIMY_HD double loading(const Ten& contact, const double* n, int crossed) const {  // getLoadingFunc
     const double t1 = 2. * G, t2 = hmod(active);
     const double t = t1 + t2;
     double x[6];
@@ -500,12 +524,12 @@ struct Point {
     return lf;
   }
 
-  FX_HD bool crossing_next() const {  // isCrossingNextSurface
+  FX_PIMY_HD bool crossing_next() const {  // isCrossingNextSurface
     if (active == P.ns) return false;
     return yield(trial, active + 1) > 0;
   }
 
-  FX_HD void correct(int crossed) {  // stressCorrection, its recursion as a loop
+  FX_PIMY_HD void correct(int crossed) {  // stressCorrection, its recursion as a loop
     for (;;) {
       Ten contact;
       contact_stress(contact);
@@ -525,7 +549,7 @@ struct Point {
     }
   }
 
-  FX_HD void move_active_surface() {  // updateActiveSurface
+  FX_PIMY_HD void move_active_surface() {  // updateActiveSurface
     if (active == P.ns) return;
     double t1[6], t2[6], x[6], c[6], oc[6];
     center(active, c);
@@ -570,7 +594,7 @@ struct Point {
     set_center(active, c);
   }
 
-  FX_HD void move_inner_surfaces() {  // updateInnerSurface
+  FX_PIMY_HD void move_inner_surfaces() {  // updateInnerSurface
     if (active <= 1) return;
     double dv[6], c[6];
     vset(dv, cur.d);
@@ -586,13 +610,14 @@ struct Point {
     }
   }
 
-  FX_HD void tangent(double* D) const {  // getTangent, D[6 i + j]
-    if (stage != 1) {
-      elastic_D(G, K, D);
-      return;
-    }
+  // getTangent in compact form (kTan values): stage, G, K, the rank-one coefficient and the
+  // deviator about the active surface's center; compact_D expands it to the 6 x 6 tangent.
+  FX_PIMY_HD void compact(double* t) const {
+    t[0] = stage;
+    t[1] = G;
+    t[2] = K;
     double coeff = 0., dv[6] = {0., 0., 0., 0., 0., 0.};
-    if (active > 0) {
+    if (stage == 1 && active > 0) {
       double c[6];
       vset(dv, trial.d);
       center(active, c);
@@ -600,17 +625,16 @@ struct Point {
       const double sz = size(active), h = hmod(active);
       coeff = 6. * G * G / (2. * G + h) / sz / sz;
     }
-    for (int i = 0; i < 6; i++)
-      for (int j = 0; j < 6; j++) {
-        double v = -coeff * dv[i] * dv[j];
-        if (i == j) v += G;
-        if (i < 3 && j < 3 && i == j) v += G;
-        if (i < 3 && j < 3) v += (K - 2. * G / 3.);
-        D[6 * i + j] = v;
-      }
+    t[3] = coeff;
+    for (int i = 0; i < 6; ++i) t[4 + i] = dv[i];
+  }
+  FX_PIMY_HD void tangent(double* D) const {  // getTangent, D[6 i + j]
+    double t[10];
+    compact(t);
+    compact_D(t, D);
   }
 
-  FX_HD void run(const double* eps) {  // setTrialStrain + getStress
+  FX_PIMY_HD void run(const double* eps) {  // setTrialStrain + getStress
     cur.load(C, S_STRESS);
     strain.load(C, S_STRAIN);
     active_c = static_cast<int>(C[S_ACTIVE]);
@@ -658,8 +682,8 @@ struct Point {
     trial.from_dev(dv, vol);
   }
 
-  FX_HD void finish(double* sig, double* D) {  // the tangent, the outputs, the trial state
-    tangent(D);
+  FX_PIMY_HD void finish(double* sig, double* D) {  // the tangent (D may be NULL), the outputs, the trial state
+    if (D) tangent(D);
     for (int i = 0; i < 6; ++i) sig[i] = ok ? trial.t[i] : static_cast<double>(NAN);
     double w[6];
     vset(w, strain.t);
@@ -677,10 +701,22 @@ struct Point {
 
 // The update of one point: trial state, stress and tangent (D[6 i + j]) at total strain eps.
 template <class CV, class TV>
-FX_HD inline bool update(const Params& p, int stage, CV C, TV T, const double* eps, double* sig, double* D) {
+FX_PIMY_HD inline bool update(const Params& p, int stage, CV C, TV T, const double* eps, double* sig, double* D) {
   Point<CV, TV> pt(p, stage, C, T);
   pt.run(eps);
   pt.finish(sig, D);
+  return pt.ok;
+}
+
+// The same with the tangent in compact form t[kTan]; *plastic: an active yield surface.
+template <class CV, class TV>
+FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, const double* eps, double* sig, double* t,
+                                 bool* plastic) {
+  Point<CV, TV> pt(p, stage, C, T);
+  pt.run(eps);
+  pt.finish(sig, nullptr);
+  pt.compact(t);
+  *plastic = stage == 1 && pt.active > 0;
   return pt.ok;
 }
 

@@ -1,0 +1,94 @@
+// stdBrick with PressureIndependMultiYield points (the reference's StdBrick<PressureIndependMultiYield<NS>>,
+// src/physics/elements/std_brick.hpp:398-540, with the material of pimy.cuh): the internal force
+// through the material update of every Gauss point, and the operator's material matrix from the
+// compact tangents that update stored. Point gp of element e keeps value k of its state at
+// [(k * 8 + gp) * P + e] and value c of its compact tangent at [(c * 8 + gp) * P + e].
+#pragma once
+
+#include "brick_gp.cuh"
+#include "pimy.cuh"
+
+namespace fx {
+
+// A parameter set's material (ParamGP::table indexes the table) and its stage.
+struct PimySet {
+  pimy::Params p;
+  int stage;  // 0 elastic, 1 plastic (updateMaterialStage)
+};
+
+// Internal force of one element (OpenSees' order: per point resid += B^T sigma dvol, resid -= body,
+// fdamp += alphaM M v; fe = resid + fdamp). No stiffness-proportional damping (refused for these
+// sets). Returns the points with an active yield surface; *failed counts points whose update met a
+// state OpenSees stops the program for.
+FX_HD int element_force_pimy(const ParamGP& p, const PimySet& m, const double xl[3][8], const double* ue,
+                             const double* ve, const double* committed, double* trial, double* tan, int64_t stride,
+                             double* fe, int* failed) {
+  double resid[24], fdamp[24];
+  for (int a = 0; a < 24; ++a) resid[a] = fdamp[a] = 0.0;
+  int plastic = 0;
+  for (int gp = 0; gp < 8; gp++) {
+    PointShape s;
+    point_shape(xl, gp, s);
+    double e[6], sg[6], vg[3], t[pimy::kTan];
+    strain_of(s, ue, e);
+    bool pl = false;
+    const bool ok = pimy::update_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride},
+                                         pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, &pl);
+    plastic += pl ? 1 : 0;
+    *failed += ok ? 0 : 1;
+    for (int c = 0; c < pimy::kTan; ++c) tan[(c * 8 + gp) * stride] = t[c];
+    vg[0] = vg[1] = vg[2] = 0.0;
+    if (p.alphaM != 0.0 && p.mass_type == 0)
+      for (int j = 0; j < 8; j++)
+        for (int q = 0; q < 3; q++) vg[q] += s.N[j] * ve[3 * j + q];
+    for (int j = 0; j < 8; j++) {
+      double r[3], body[3], dj[3];
+      node_force(s, sg, j, r);
+      for (int q = 0; q < 3; q++) body[q] = s.dvol * p.b[q] * s.N[j];
+      dj[0] = dj[1] = dj[2] = 0.0;
+      if (p.alphaM != 0.0) {
+        const double tm = s.N[j] * s.dvol * p.rho;
+        for (int q = 0; q < 3; q++) {
+          const double vq = p.mass_type == 0 ? vg[q] : ve[3 * j + q];
+          dj[q] += p.alphaM * tm * vq;
+        }
+      }
+      for (int q = 0; q < 3; q++) {
+        resid[3 * j + q] += r[q];
+        resid[3 * j + q] -= body[q];
+        fdamp[3 * j + q] += dj[q];
+      }
+    }
+  }
+  for (int a = 0; a < 24; ++a) fe[a] = resid[a] + fdamp[a];
+  return plastic;
+}
+
+// The material matrix of point gp for the operator: the stored tangent of the last force
+// evaluation scaled by the stiffness factor, or (ModifiedNewton -initial) the material's initial
+// tangent, the reference elastic one (the reference's PressureIndependMultiYield::initial_tangent).
+// The material declares its tangent symmetric, so it is stored as its upper triangle and the lower
+// one mirrors it (the reference's TangentStorage, src/physics/common/tangent_storage.hpp:17-31).
+struct PimyPointD {
+  const PimySet* m;
+  const double* tan;
+  int64_t stride;
+  double cK;
+  bool initial;
+  FX_HD void operator()(int gp, double De[6][6]) const {
+    double D[36];
+    if (initial) {
+      pimy::elastic_D(m->p.G0, m->p.K0, D);
+    } else {
+      double t[pimy::kTan];
+      for (int c = 0; c < pimy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
+      pimy::compact_D(t, D);
+    }
+    for (int a = 0; a < 6; ++a)
+      for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
+    for (int a = 0; a < 6; ++a)
+      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+  }
+};
+
+}  // namespace fx

@@ -27,6 +27,10 @@ class Group:
     sigma_y: float = 0.0
     H: float = 0.0
     hk: float = 0.0
+    # PressureIndependMultiYield: (the 9 constructor values, pairs or None). The library compiles
+    # the group as an elastic set (E, nu, rho) and binds the material to its parameter set
+    # (InternalForce.set_pimy); the reference's model gets the material itself.
+    pimy: tuple = None
 
 
 @dataclasses.dataclass

@@ -465,6 +465,23 @@ int fx_pimy_setup_values(const fx_pimy* m, double* out);
 int fx_pimy_init(fx_pimy* m, int64_t npoints, double* state, void* stream);
 int fx_pimy_update(fx_pimy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
                    const double* strain, double* stress, double* tangent, int32_t* failed, void* stream);
+/* Binds material m to parameter set `set` of a mesh (stdBrick with PressureIndependMultiYield
+ * points: the reference's StdBrick<PressureIndependMultiYield<NS>>, std_brick.hpp:398-540, a
+ * model material of that type). The set's elements run on the Gauss-point path (the box path is
+ * taken out for the mesh); their points start from the material's state, elastic stage. The set's
+ * density must equal the material's (the masses come from the set); stiffness-proportional Rayleigh
+ * damping on the set is FX_E_UNSUPPORTED. Bind before creating solvers or running stages on the
+ * mesh. fx_force_compute then updates every point (the trial state; fx_force_commit commits it),
+ * the operator and its diagonal use each point's tangent of the last fx_force_compute (the
+ * reference's stored tangents at that displacement; `initial` in fx_coeffs: the material's
+ * reference elastic tangent), fx_force_plastic_points counts points with an active surface.
+ *   fx_force_set_material_stage  updateMaterialStage for the set (InternalForce::set_material_stage,
+ *                                src/exec/internal_force.cpp:511-515): 0 elastic, 1 plastic.
+ *   fx_force_pimy_failed         points whose update met a state OpenSees stops for (stress NaN),
+ *                                counted over all evaluations. */
+int fx_force_set_pimy(fx_force* f, int32_t set, const fx_pimy* m);
+int fx_force_set_material_stage(fx_force* f, int32_t set, int32_t stage);
+int fx_force_pimy_failed(const fx_force* f, int64_t* count);
 int fx_pimy_init_host(const fx_pimy* m, int64_t npoints, double* state);
 int fx_pimy_update_host(const fx_pimy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
                         const double* strain, double* stress, double* tangent, int32_t* failed);

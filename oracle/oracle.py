@@ -85,6 +85,11 @@ def ref():
         L.fxref_brick_critical_dt.restype = C.c_double
         L.fxref_brick_critical_dt.argtypes = [p_f64, p_f64, C.c_int, p_f64]
         L.fxref_pimy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
+        L.fxref_model_add_group_pimy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
+        L.fxref_force_set_stage.argtypes = [vp, C.c_int32, C.c_int32]
+        L.fxref_force_commit.argtypes = [vp]
+        L.fxref_apply_operator_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64, p_f64]
+        L.fxref_operator_diagonal_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, p_f64, p_f64]
         L.fxref_pimy_destroy.argtypes = [vp]
         L.fxref_pimy_nstate.restype = C.c_int32
         L.fxref_pimy_setup_values.argtypes = [vp, p_f64]
@@ -118,7 +123,14 @@ class RefModel:
             b, pb = _f(np.array(g.b, np.float64))
             et, pet = _i(g.etags)
             cn, pcn = _i(np.asarray(g.conn).reshape(-1))
-            L.fxref_model_add_group(self.h, g.E, g.nu, g.rho, pb, int(g.lumped), len(et), pet, pcn)
+            if getattr(g, "pimy", None) is not None:
+                in9, pairs = g.pimy
+                p9, pp9 = _f(in9)
+                pr = np.ascontiguousarray(pairs if pairs is not None else [], np.float64)
+                L.fxref_model_add_group_pimy(self.h, pp9, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2,
+                                             pb, int(g.lumped), len(et), pet, pcn)
+            else:
+                L.fxref_model_add_group(self.h, g.E, g.nu, g.rho, pb, int(g.lumped), len(et), pet, pcn)
         if len(spec.fix_node):
             a, pa = _i(spec.fix_node)
             d, pd = _i(spec.fix_dof)
@@ -231,6 +243,31 @@ class RefForce:
         f = np.zeros(self.n)
         ref().fxref_force_compute(self.h, pu, pv, geometry, f.ctypes.data_as(p_f64))
         return f
+
+    def set_stage(self, material, stage):
+        """updateMaterialStage of model material `material` (0-based)."""
+        assert ref().fxref_force_set_stage(self.h, material, stage) == 0
+
+    def commit(self):
+        assert ref().fxref_force_commit(self.h) == 0
+
+    def apply_operator_at(self, k, u, x, initial=False):
+        """K_eff x with every point's tangent recomputed at displacement u (TangentSource::Recomputed)."""
+        u, pu = _f(u)
+        x, px = _f(x)
+        y = np.zeros(self.n)
+        rc = ref().fxref_apply_operator_at(self.h, k[0], k[1], k[2], int(initial), pu, px, y.ctypes.data_as(p_f64))
+        if rc:
+            raise RuntimeError(ref().fxref_last_error().decode())
+        return y
+
+    def operator_diagonal_at(self, k, u):
+        u, pu = _f(u)
+        d = np.zeros(self.n)
+        rc = ref().fxref_operator_diagonal_at(self.h, k[0], k[1], k[2], pu, d.ctypes.data_as(p_f64))
+        if rc:
+            raise RuntimeError(ref().fxref_last_error().decode())
+        return d
 
     def min_critical_dt(self, scheme="ExplicitDifference"):
         return ref().fxref_min_critical_dt(self.h, 1 if scheme == "ExplicitDifference" else 0)

@@ -85,6 +85,38 @@ int fxref_model_add_group(fxref_model* h, double E, double nu, double rho, const
   return 0;
 }
 
+// The same with a PressureIndependMultiYield material (in9 as fxref_pimy_create; npairs > 0: a user
+// backbone, noYieldSurf = -npairs as the model file gives it).
+int fxref_model_add_group_pimy(fxref_model* h, const double* in9, const double* pairs, int32_t npairs, const double* b,
+                               int lumped, int32_t count, const int32_t* etags, const int32_t* conn) {
+  io::NDMaterial mat;
+  mat.tag = static_cast<std::int32_t>(h->m.materials.size()) + 1;
+  io::PressureIndependMultiYieldData d;
+  d.nd = 3;
+  d.rho = in9[0];
+  d.refShearModul = in9[1];
+  d.refBulkModul = in9[2];
+  d.cohesi = in9[3];
+  d.peakShearStra = in9[4];
+  d.frictionAng = in9[5];
+  d.refPress = in9[6];
+  d.pressDependCoe = in9[7];
+  d.noYieldSurf = npairs > 0 ? -npairs : static_cast<std::int32_t>(in9[8]);
+  if (npairs > 0) d.pairs.assign(pairs, pairs + 2 * static_cast<std::size_t>(npairs));
+  mat.data = d;
+  h->m.materials.push_back(mat);
+  io::ElementGroup g;
+  g.id = std::to_string(h->m.elements.size());
+  g.type = io::ElementType::StdBrick;
+  g.material = mat.tag;
+  g.body_force = {b[0], b[1], b[2]};
+  g.lumped = lumped != 0;
+  g.tags.assign(etags, etags + count);
+  g.connectivity.assign(conn, conn + 8 * static_cast<std::size_t>(count));
+  h->m.elements.push_back(std::move(g));
+  return 0;
+}
+
 void fxref_model_add_fix(fxref_model* h, int32_t n, const int32_t* node, const int32_t* dof) {
   h->m.fix.node.insert(h->m.fix.node.end(), node, node + n);
   h->m.fix.dof.insert(h->m.fix.dof.end(), dof, dof + n);
@@ -215,6 +247,7 @@ int fxref_compiled_param(const fxref_compiled* h, int32_t p, double* out) {
 struct fxref_force {
   std::unique_ptr<exec::InternalForce> f;
   int32_t neq = 0;
+  bool stored = false;  // enable_stored_tangents done
 };
 
 // cache: 0 Off, 1 On (the geometry cache).
@@ -290,6 +323,61 @@ int fxref_force_compute(fxref_force* h, const double* u, const double* v, int ge
     s.geometry = geometry ? exec::Geometry::Cached : exec::Geometry::Recompute;
     F.compute(s);
     for (int32_t q = 0; q < h->neq; ++q) f[q] = F.f(q);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// updateMaterialStage of model material `material` (0-based), commitState.
+int fxref_force_set_stage(fxref_force* h, int32_t material, int32_t stage) {
+  try {
+    return h->f->set_material_stage(material, stage) ? 0 : 1;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+int fxref_force_commit(fxref_force* h) {
+  try {
+    h->f->commit_state();
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// y = K_eff x with each point's tangent determined at displacement u from the committed state and
+// stored (store_tangents, TangentSource::Stored: the reference's operator for materials with
+// history), and the diagonal likewise.
+namespace {
+exec::OperatorSettings stored_at(fxref_force* h, const double* u, exec::Vec& uu) {
+  if (!h->stored) {
+    h->f->enable_stored_tangents();
+    h->stored = true;
+  }
+  for (int32_t q = 0; q < h->neq; ++q) uu(q) = u[q];
+  exec::OperatorSettings s = op_settings(0, 1);
+  s.tangent = exec::TangentSource::Stored;
+  h->f->store_tangents(uu, s);
+  return s;
+}
+}  // namespace
+int fxref_apply_operator_at(fxref_force* h, double cK, double cC, double cM, int initial, const double* u,
+                            const double* x, double* y) {
+  try {
+    exec::Vec uu("u", static_cast<std::size_t>(h->neq));
+    const exec::OperatorSettings s = stored_at(h, u, uu);
+    h->f->apply_operator(OperatorCoefficients{cK, cC, cM, initial != 0}, s, uu, wrap(x, h->neq), wrap(y, h->neq));
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+int fxref_operator_diagonal_at(fxref_force* h, double cK, double cC, double cM, const double* u, double* d) {
+  try {
+    exec::Vec uu("u", static_cast<std::size_t>(h->neq));
+    const exec::OperatorSettings s = stored_at(h, u, uu);
+    h->f->operator_diagonal(OperatorCoefficients{cK, cC, cM, false}, s, uu, wrap(d, h->neq));
     return 0;
   } catch (const std::exception& e) {
     return fail(e);
