@@ -263,6 +263,48 @@ def pimy_points(device, n=1 << 20, steps=10, sample=8192, seed=0):
             "device_vs_host_sample_within_1e-12": same}
 
 
+PIMY_CLAY = (1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0)  # rho t/m3, G, K kPa, cohesion kPa, ...
+
+
+def pimy_explicit(device, n=100, warm=16, steps=64):
+    """The reference's plastic-box measurement (an n^3 stdBrick box of PressureIndependMultiYield
+    clay, 20 surfaces, in the plastic stage, under 0.3 g 2 Hz base shaking, explicit steps of 5e-4 s)
+    on the Gauss-point path: ExplicitDifference stage steps (the force with every point's material
+    update, the update pass, the commit of the material state), CUDA graphs of 16 steps; ms per
+    step by CUDA events after `warm` steps. 1 m elements, fixed base, lumped mass, no laminar ties
+    (the reference's generator is not in its repository)."""
+    import torch
+    import femorax_b200 as fx
+    from femorax_b200 import meshes
+    G, K = PIMY_CLAY[1], PIMY_CLAY[2]
+    E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
+    spec = meshes.box_model(n, n, n, size=(float(n), float(n), float(n)), E=E, nu=nu, rho=PIMY_CLAY[0], lumped=True)
+    comp = fx.Model(spec).compile()
+    mesh = comp.mesh()
+    force = fx.InternalForce(mesh, device=device)
+    force.set_pimy(0, fx.PressureIndependMultiYield(*PIMY_CLAY[:8], noYieldSurf=int(PIMY_CLAY[8])))
+    force.set_material_stage(0, 1)
+    dev = torch.device("cuda", device)
+    dt = 5e-4
+    total = warm + steps
+    t = np.arange(total + 2) * dt
+    motions = fx.GroundMotions([dict(dof=0, fact=1.0, values=0.3 * 9.81 * np.sin(2 * np.pi * 2.0 * t), dt=dt)])
+    m = torch.as_tensor(mesh.lumped_mass, device=dev)
+    u, v, a = (torch.zeros(mesh.num_equations, dtype=torch.float64, device=dev) for _ in range(3))
+    tm, _ = force.explicit_stage("ExplicitDifference", m, u, v, a, dt, warm, motions=motions)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    force.explicit_stage("ExplicitDifference", m, u, v, a, dt, steps, time=tm, motions=motions, resume=True)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    return {"elements": int(mesh.count), "points": 8 * int(mesh.count), "surfaces": int(PIMY_CLAY[8]),
+            "dt_s": dt, "steps_timed": steps, "ms_per_step": ms, "device_bytes": int(force.info()["device_bytes"]),
+            "plastic_points_last_step": int(force.plastic_points()), "failed_points": int(force.pimy_failed()),
+            "reference_h200_ms_per_step": 23.5}
+
+
 def newmark_comparison(device, n=100, steps=20, seed=0):
     """The Newmark configuration on a bounded sample of its steps: a heterogeneous cube of n^3 boxes (per-element
     E log-normal, median 80 MPa, sigma 0.5; nu 0.3; base fixed), a harmonic horizontal surface load,
@@ -595,6 +637,8 @@ def run_ours(args):
     batched_j2 = batched_j2_comparison(local) if world == 1 and not args.no_serve else None
     newmark = newmark_comparison(local) if world == 1 and not args.no_serve else None
     pimy = pimy_points(local) if world == 1 and not args.no_serve else None
+    if pimy is not None:
+        pimy["explicit_box"] = pimy_explicit(local)
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -46,7 +46,7 @@ int64_t ForceState::device_bytes() const {
   for (const auto& cs : box.cset) b += cs.coef.bytes() + cs.coef32.bytes() + cs.scoef.bytes() + cs.scoef32.bytes();
   b += j2_committed.bytes() + j2_trial.bytes() + j2_tan.bytes() + plastic_dev.bytes();
   b += geom32.bytes() + nshape32.bytes() + slots32.bytes();
-  b += pimy_dev.bytes() + pimy_committed.bytes() + pimy_trial.bytes() + pimy_tan.bytes() + pimy_failed.bytes();
+  b += pimy_dev.bytes() + pimy_committed.bytes() + pimy_trial.bytes() + pimy_tan.bytes() + pimy_failed.bytes() + pimy_sig.bytes();
   return b;
 }
 
@@ -504,9 +504,7 @@ int fx_force_commit(fx_force* f, void* stream) {
     if (s.has_j2)
       FX_CUDA(cudaMemcpyAsync(s.j2_committed.ptr, s.j2_trial.ptr, s.j2_committed.bytes(), cudaMemcpyDeviceToDevice,
                               static_cast<cudaStream_t>(stream)));
-    if (s.has_pimy)
-      FX_CUDA(cudaMemcpyAsync(s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_committed.bytes(),
-                              cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)));
+    fx::pimy_commit(s, static_cast<cudaStream_t>(stream));
   });
 }
 

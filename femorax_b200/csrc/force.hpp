@@ -191,6 +191,7 @@ struct ForceState {
   std::vector<PimySet> pimy_h;
   DeviceArray<PimySet> pimy_dev;
   DeviceArray<double> pimy_committed, pimy_trial, pimy_tan;
+  DeviceArray<double> pimy_sig;  // the points' stresses of the last force evaluation, [(c * 8 + gp) * P + e]
   DeviceArray<int> pimy_failed;  // points whose update met a state OpenSees stops for (cumulative)
   int pimy_nstate = 0;
   ExplicitWork xw;
@@ -208,6 +209,8 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
 void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st);
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
+// commitState of the PressureIndependMultiYield points (their trial surfaces are copy-on-write)
+void pimy_commit(ForceState& s, cudaStream_t st);
 
 // stepping.cu: the Newmark form-D kernels (implicit_stage.cpp:29-68)
 void newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,

@@ -75,13 +75,11 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
                                                            int32_t count, const double* __restrict__ u,
                                                            const double* __restrict__ v, double* __restrict__ slots,
                                                            const double* __restrict__ j2c, double* __restrict__ j2t,
-                                                           double* __restrict__ j2tan, int* __restrict__ plastic,
-                                                           const PimySet* __restrict__ pimy,
-                                                           const double* __restrict__ pc, double* __restrict__ pt,
-                                                           double* __restrict__ ptan, int* __restrict__ failed) {
+                                                           double* __restrict__ j2tan, int* __restrict__ plastic) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
+  if (p.kind == 2) return;  // k_pimy_points + k_pimy_force
   double xl[3][8], ue[24], ve[24], fe[24];
   load_coords(coords, node, N, P, e, xl);
   for (int a = 0; a < 24; ++a) {
@@ -92,15 +90,83 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
   if (p.kind == 1) {
     const int np = element_force_j2(p, xl, ue, ve, j2c + e, j2t + e, j2tan + e, P, fe);
     if (np) atomicAdd(plastic, np);
-  } else if (p.kind == 2) {
-    int bad = 0;
-    const int np = element_force_pimy(p, pimy[p.table], xl, ue, ve, pc + e, pt + e, ptan + e, P, fe, &bad);
-    if (np) atomicAdd(plastic, np);
-    if (bad) atomicAdd(failed, bad);
   } else {
     element_force(p, xl, ue, ve, fe);
   }
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = fe[a];
+}
+
+// PressureIndependMultiYield sets, point by point: thread t is point gp = t / P of element
+// e = t % P (consecutive threads, consecutive elements: every state value is read and written as
+// whole lines); stress and compact tangent out. Yielding and failed points counted per warp.
+__global__ void __launch_bounds__(128) k_pimy_points(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                     const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
+                                                     const ParamGP* __restrict__ params, const PimySet* __restrict__ pimy,
+                                                     int32_t N, int32_t P, int32_t count, const double* __restrict__ u,
+                                                     const double* __restrict__ pc, double* __restrict__ pt,
+                                                     double* __restrict__ ptan, double* __restrict__ psig,
+                                                     int* __restrict__ plastic, int* __restrict__ failed) {
+  const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const int32_t e = static_cast<int32_t>(t % P), gp = static_cast<int32_t>(t / P);
+  bool pl = false, bad = false;
+  if (gp < 8 && e < count) {
+    const ParamGP p = params[param[e]];
+    if (p.kind == 2) {
+      double xl[3][8], ue[24], sg[6], tc[pimy::kTan];
+      load_coords(coords, node, N, P, e, xl);
+      for (int a = 0; a < 24; ++a) {
+        const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+        ue[a] = q >= 0 ? u[q] : 0.0;
+      }
+      bad = !point_update_pimy(pimy[p.table], xl, ue, gp, pc + e, pt + e, P, sg, tc, &pl);
+      for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
+      for (int c = 0; c < pimy::kTan; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
+    }
+  }
+  const unsigned np = __popc(__ballot_sync(0xffffffffu, pl)), nb = __popc(__ballot_sync(0xffffffffu, bad));
+  if ((threadIdx.x & 31) == 0) {
+    if (np) atomicAdd(plastic, static_cast<int>(np));
+    if (nb) atomicAdd(failed, static_cast<int>(nb));
+  }
+}
+
+// ... then their elements' internal forces from the points' stresses, into the slots
+__global__ void __launch_bounds__(kBlock) k_pimy_force(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                        const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
+                                                        const ParamGP* __restrict__ params, int32_t N, int32_t P,
+                                                        int32_t count, const double* __restrict__ v,
+                                                        const double* __restrict__ psig, double* __restrict__ slots) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const ParamGP p = params[param[e]];
+  if (p.kind != 2) return;
+  double xl[3][8], ve[24], fe[24];
+  load_coords(coords, node, N, P, e, xl);
+  for (int a = 0; a < 24; ++a) {
+    const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+    ve[a] = q >= 0 ? v[q] : 0.0;
+  }
+  element_force_from_stress(p, xl, ve, psig + e, P, fe);
+  for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = fe[a];
+}
+
+// commitState of the PressureIndependMultiYield points: the scalar values of every point, the
+// surfaces of the points whose last update changed them (the others' committed surfaces stand).
+__global__ void __launch_bounds__(256) k_pimy_commit(const int32_t* __restrict__ param,
+                                                     const ParamGP* __restrict__ params,
+                                                     const PimySet* __restrict__ pimy, int32_t P, int32_t count,
+                                                     double* __restrict__ pc, const double* __restrict__ pt) {
+  const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const int32_t e = static_cast<int32_t>(t % P), gp = static_cast<int32_t>(t / P);
+  if (gp >= 8 || e >= count) return;
+  const ParamGP& p = params[param[e]];
+  if (p.kind != 2) return;
+  const int64_t base = static_cast<int64_t>(gp) * P + e, ld = 8 * static_cast<int64_t>(P);
+  for (int k = 0; k < pimy::S_SURF; ++k) pc[base + k * ld] = pt[base + k * ld];
+  if (pt[base + pimy::S_CHANGED * ld] != 0.0) {
+    const int n = pimy::nstate(pimy[p.table].p.ns);
+    for (int k = pimy::S_SURF; k < n; ++k) pc[base + k * ld] = pt[base + k * ld];
+  }
 }
 
 // y[q] = sum of q's slots in list order, then + c1 m1[q] x1[q] + c2 m2[q] x2[q] (the nodal-mass
@@ -302,15 +368,32 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
     k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr,
                                                                    s.j2_committed.ptr, s.j2_trial.ptr, s.j2_tan.ptr,
-                                                                   s.plastic_dev.ptr, s.pimy_dev.ptr,
-                                                                   s.pimy_committed.ptr, s.pimy_trial.ptr,
-                                                                   s.pimy_tan.ptr, s.pimy_failed.ptr);
+                                                                   s.plastic_dev.ptr);
   FX_LAUNCH_CHECK("element_force");
+  if (s.has_pimy && s.count > 0) {
+    const int64_t points = static_cast<int64_t>(8) * s.P;
+    k_pimy_points<<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+        s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.N, s.P, s.count, u,
+        s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
+    FX_LAUNCH_CHECK("pimy_points");
+    k_pimy_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                               s.params.ptr, s.N, s.P, s.count, v, s.pimy_sig.ptr,
+                                                               s.slots.ptr);
+    FX_LAUNCH_CHECK("pimy_force");
+  }
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
     k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
                                                    nullptr, 1.0, m2, v, f, nullptr);
   FX_LAUNCH_CHECK("slot_gather");
+}
+
+void pimy_commit(ForceState& s, cudaStream_t st) {
+  if (!s.has_pimy || s.count == 0) return;
+  const int64_t points = static_cast<int64_t>(8) * s.P;
+  k_pimy_commit<<<static_cast<unsigned>((points + 255) / 256), 256, 0, st>>>(
+      s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.P, s.count, s.pimy_committed.ptr, s.pimy_trial.ptr);
+  FX_LAUNCH_CHECK("pimy_commit");
 }
 
 // M r_dir: the operator with k = (0, 0, 1) on the rigid unit translation at every element DOF,

@@ -173,6 +173,7 @@ int fx_force_set_pimy(fx_force* f, int32_t set, const fx_pimy* m) {
       s.pimy_committed.alloc(static_cast<size_t>(need) * 8 * P);
       s.pimy_trial.alloc(static_cast<size_t>(need) * 8 * P);
       if (!s.pimy_tan.ptr) s.pimy_tan.alloc(static_cast<size_t>(fx::pimy::kTan) * 8 * P);
+      if (!s.pimy_sig.ptr) s.pimy_sig.alloc(static_cast<size_t>(6) * 8 * P);
       s.pimy_nstate = need;
     }
     if (!s.pimy_dev.ptr) s.pimy_dev.alloc(static_cast<size_t>(s.nparams));  // one entry per set at most

@@ -14,7 +14,9 @@
 //   0..12   stress: components (11 22 33 12 23 31, tensor shear), deviator, mean
 //   13..25  strain at the last commit, the same 13 values
 //   26      active surface, 27 switched to plastic (0/1), 28 shear modulus G, 29 bulk modulus K
-//   30 + 8 (i - 1) + {0, 1, 2..7}: surface i (1..ns): size, plastic modulus, center (6)
+//   30      the update changed the surfaces (a trial state's surfaces are valid only then, when the
+//           update ran copy-on-write; the full form writes them always and sets 1)
+//   31 + 8 (i - 1) + {0, 1, 2..7}: surface i (1..ns): size, plastic modulus, center (6)
 // The moduli and surfaces start at the material's values and are scaled by the confinement at the
 // switch to the plastic stage (when the friction angle is positive).
 #pragma once
@@ -38,7 +40,7 @@ constexpr double kUp = 1.0e+30;             // OpenSees UP_LIMIT
 constexpr double kVeryLarge = 1.0e200;      // a Vector divided by zero
 constexpr double kPi = 3.14159265358979;    // OpenSees' value
 
-enum : int { S_STRESS = 0, S_STRAIN = 13, S_ACTIVE = 26, S_E2P = 27, S_G = 28, S_K = 29, S_SURF = 30 };
+enum : int { S_STRESS = 0, S_STRAIN = 13, S_ACTIVE = 26, S_E2P = 27, S_G = 28, S_K = 29, S_CHANGED = 30, S_SURF = 31 };
 FX_PIMY_HD constexpr int nstate(int ns) { return S_SURF + 8 * ns; }
 
 // The material after setup: constructor values and the surfaces of setUpSurfaces ([0] unused).
@@ -338,14 +340,17 @@ FX_PIMY_HD inline int to_int(double x) {  // C++ truncation, NaN 0 and clamped o
 
 // One point's update from its committed state C to the trial state T at the total strain eps
 // (engineering shear): OpenSees' setTrialStrain + getStress + getTangent, the instance's members as
-// locals. The trial buffer holds the surfaces being worked on (copied from the committed ones
-// first, before the switch to the plastic stage may scale them).
+// locals. The surfaces are read from the committed state until the update first changes one; then
+// all of them are copied to the trial state, which holds them from there on (copy on write: most
+// updates change no surface). `full`: the trial state's surfaces are written in any case.
 template <class CV, class TV>
 struct Point {
   const Params& P;
   int stage;  // 0 elastic, 1 plastic (updateMaterialStage)
   CV C;
   TV T;
+  bool full = true;
+  bool dirty = false;  // the trial state holds the surfaces
   bool ok = true;  // false after a state OpenSees stops the program for
   Ten cur, strain, trial, rate, sub;  // currentStress, currentStrain, trialStress, strainRate, subStrainRate
   int active_c = 0, active = 0, e2p = 0;
@@ -354,12 +359,19 @@ struct Point {
   FX_PIMY_HD Point(const Params& p, int st, CV c, TV t) : P(p), stage(st), C(c), T(t) {}
 
   FX_PIMY_HD int at(int i) const { return S_SURF + 8 * (i - 1); }
-  FX_PIMY_HD double size(int i) const { return i == 0 ? 0. : T[at(i)]; }
-  FX_PIMY_HD double hmod(int i) const { return i == 0 ? 0. : T[at(i) + 1]; }
+  FX_PIMY_HD double sv(int k) const { return dirty ? T[k] : C[k]; }
+  FX_PIMY_HD void touch() {  // the first change: the surfaces into the trial state
+    if (dirty) return;
+    for (int k = S_SURF; k < nstate(P.ns); ++k) T[k] = C[k];
+    dirty = true;
+  }
+  FX_PIMY_HD double size(int i) const { return i == 0 ? 0. : sv(at(i)); }
+  FX_PIMY_HD double hmod(int i) const { return i == 0 ? 0. : sv(at(i) + 1); }
   FX_PIMY_HD void center(int i, double* c) const {
-    for (int k = 0; k < 6; ++k) c[k] = i == 0 ? 0. : T[at(i) + 2 + k];
+    for (int k = 0; k < 6; ++k) c[k] = i == 0 ? 0. : sv(at(i) + 2 + k);
   }
   FX_PIMY_HD void set_center(int i, const double* c) {
+    touch();
     for (int k = 0; k < 6; ++k) T[at(i) + 2 + k] = c[k];
   }
 
@@ -423,6 +435,7 @@ struct Point {
     f = pow(f, P.n_press);
     G *= f;
     K *= f;
+    touch();
     for (int i = 1; i <= P.ns; ++i) {
       const double hm = hmod(i) * f, sz = size(i) * h;
       T[at(i)] = sz;
@@ -647,7 +660,6 @@ struct Point {
     strain.engineering(cs);
     vsub(w, cs);
     rate.from_full(w, true);
-    for (int k = S_SURF; k < nstate(P.ns); ++k) T[k] = C[k];
     if (stage == 1 && e2p == 0) elastic_to_plastic();
     if (stage != 1) {  // linear elastic: sigma += D rate, column by column
       double D[36], a[6], r[6];
@@ -696,6 +708,8 @@ struct Point {
     T[S_G] = G;
     T[S_K] = K;
     T[S_ACTIVE] = stage == 1 ? active : active_c;
+    if (full) touch();
+    T[S_CHANGED] = dirty ? 1.0 : 0.0;
   }
 };
 
@@ -708,11 +722,14 @@ FX_PIMY_HD inline bool update(const Params& p, int stage, CV C, TV T, const doub
   return pt.ok;
 }
 
-// The same with the tangent in compact form t[kTan]; *plastic: an active yield surface.
+// The same with the tangent in compact form t[kTan]; *plastic: an active yield surface. Copy on
+// write: the trial state's surfaces are written only if the update changed them (value S_CHANGED),
+// so a commit copies the surfaces of those points only.
 template <class CV, class TV>
 FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, const double* eps, double* sig, double* t,
                                  bool* plastic) {
   Point<CV, TV> pt(p, stage, C, T);
+  pt.full = false;
   pt.run(eps);
   pt.finish(sig, nullptr);
   pt.compact(t);

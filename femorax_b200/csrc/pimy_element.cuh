@@ -16,27 +16,32 @@ struct PimySet {
   int stage;  // 0 elastic, 1 plastic (updateMaterialStage)
 };
 
-// Internal force of one element (OpenSees' order: per point resid += B^T sigma dvol, resid -= body,
-// fdamp += alphaM M v; fe = resid + fdamp). No stiffness-proportional damping (refused for these
-// sets). Returns the points with an active yield surface; *failed counts points whose update met a
-// state OpenSees stops the program for.
-FX_HD int element_force_pimy(const ParamGP& p, const PimySet& m, const double xl[3][8], const double* ue,
-                             const double* ve, const double* committed, double* trial, double* tan, int64_t stride,
-                             double* fe, int* failed) {
+// The update of point gp of element e (the reference's point_update_shape without stiffness
+// damping): strain at the point from the element's displacements, the material update from the
+// committed state to the trial one; the stress and the compact tangent out. Returns the update's ok.
+FX_HD bool point_update_pimy(const PimySet& m, const double xl[3][8], const double* ue, int gp,
+                             const double* committed, double* trial, int64_t stride, double sg[6],
+                             double t[pimy::kTan], bool* plastic) {
+  PointShape s;
+  point_shape(xl, gp, s);
+  double e[6];
+  strain_of(s, ue, e);
+  return pimy::update_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride},
+                              pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, plastic);
+}
+
+// Internal force of one element from its points' stresses (point gp's component c at
+// sig[(c * 8 + gp) * stride]), in OpenSees' order: per point resid += B^T sigma dvol, resid -= body,
+// fdamp += alphaM M v; fe = resid + fdamp. No stiffness-proportional damping (refused for these sets).
+FX_HD void element_force_from_stress(const ParamGP& p, const double xl[3][8], const double* ve, const double* sig,
+                                     int64_t stride, double* fe) {
   double resid[24], fdamp[24];
   for (int a = 0; a < 24; ++a) resid[a] = fdamp[a] = 0.0;
-  int plastic = 0;
   for (int gp = 0; gp < 8; gp++) {
     PointShape s;
     point_shape(xl, gp, s);
-    double e[6], sg[6], vg[3], t[pimy::kTan];
-    strain_of(s, ue, e);
-    bool pl = false;
-    const bool ok = pimy::update_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride},
-                                         pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, &pl);
-    plastic += pl ? 1 : 0;
-    *failed += ok ? 0 : 1;
-    for (int c = 0; c < pimy::kTan; ++c) tan[(c * 8 + gp) * stride] = t[c];
+    double sg[6], vg[3];
+    for (int c = 0; c < 6; ++c) sg[c] = sig[(c * 8 + gp) * stride];
     vg[0] = vg[1] = vg[2] = 0.0;
     if (p.alphaM != 0.0 && p.mass_type == 0)
       for (int j = 0; j < 8; j++)
@@ -61,7 +66,6 @@ FX_HD int element_force_pimy(const ParamGP& p, const PimySet& m, const double xl
     }
   }
   for (int a = 0; a < 24; ++a) fe[a] = resid[a] + fdamp[a];
-  return plastic;
 }
 
 // The material matrix of point gp for the operator: the stored tangent of the last force

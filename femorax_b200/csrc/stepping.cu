@@ -568,9 +568,7 @@ void explicit_stage(fx_force* f, int scheme, const double* mass, const double* c
     FX_LAUNCH_CHECK("explicit_stage_step");
     if (s.has_j2)  // Domain::commit after every step
       FX_CUDA(cudaMemcpyAsync(s.j2_committed.ptr, s.j2_trial.ptr, s.j2_committed.bytes(), cudaMemcpyDeviceToDevice, st));
-    if (s.has_pimy)
-      FX_CUDA(cudaMemcpyAsync(s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_committed.bytes(), cudaMemcpyDeviceToDevice,
-                              st));
+    pimy_commit(s, st);
   };
   // The last step does no prediction: u, v, a are the stage's end state; a resumed call
   // starts with the prediction (ED) or the garbage velocity (CD) from the carried vector.

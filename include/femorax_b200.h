@@ -444,7 +444,7 @@ int fx_engine_info(const fx_engine* e, int64_t* info);
  *                        (gamma, G/Gmax) pairs of a user backbone, or NULL (hyperbolic backbone).
  *                        FX_E_INVALID for inputs OpenSees rejects, FX_E_UNSUPPORTED above 40
  *                        surfaces.
- *   fx_pimy_info         state values per point (30 + 8 surfaces) and the surfaces.
+ *   fx_pimy_info         state values per point (31 + 8 surfaces) and the surfaces.
  *   fx_pimy_setup_values out[83] = residual pressure, friction angle, cohesion after setup, the 40
  *                        surface sizes, the 40 plastic moduli (surfaces past noYieldSurf 0).
  *   fx_pimy_init         the state of npoints new points (device; value k of point i at

@@ -74,7 +74,7 @@ def test_setup_matches_oracle(name, oracle_mod, ref_available):
     a, sz, hm = m.setup_values()
     b, sz2, hm2 = r.setup_values()
     assert np.array_equal(a, b) and np.array_equal(sz, sz2) and np.array_equal(hm, hm2)
-    assert m.nstate == 30 + 8 * int(GOLDEN[name + "/params"][8])
+    assert m.nstate == 31 + 8 * int(GOLDEN[name + "/params"][8])
 
 
 @pytest.mark.parametrize("name", CASES)
