@@ -680,7 +680,13 @@ def main():
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the explicit-stepping and served-versus-plain solve comparisons")
     ap.add_argument("--launch", default="", help="pin the box launch shape 'variant,kz' (profiling)")
+    ap.add_argument("--pimy-box", type=int, default=0,
+                    help="only the PressureIndependMultiYield plastic box section, n^3 elements (profiling)")
     args = ap.parse_args()
+    if args.pimy_box:
+        print(json.dumps(pimy_explicit(int(os.environ.get("LOCAL_RANK", "0")), n=args.pimy_box, warm=args.warmup,
+                                       steps=args.steps)))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
