@@ -15,7 +15,8 @@ own InternalForce::apply_operator (built here from its sources, oracle/_ref) on 
 
 `explicit` times the explicit wave configuration's stepping (FP64 and FP32, 4000 steps);
 `newmark` compares the Newmark stage with plain FP64 and mixed-precision inner solves;
-`pimy` times PressureIndependMultiYield material-point updates on the device (and on one host core);
+`pimy` times PressureIndependMultiYield material-point updates on the device (and on one host core) and
+an explicit step of a 1 M-element plastic box; `pdmy` the PressureDependMultiYield point updates;
 `batched_j2` compares the batched J2 Newton with one instance at a time on a bounded sample;
 `served` compares solves/s and p50/p99 latency at a 1e-8 FP64 residual on a stream of static solves:
 the batched mixed-precision engine behind the serving loop versus plain FP64 CG one at a time;
@@ -197,7 +198,16 @@ def explicit_comparison(force, mesh, comp, device, steps=4000):
     return out
 
 
-def pimy_points(device, n=1 << 20, steps=10, sample=8192, seed=0):
+def pdmy_points(device, n=1 << 20, steps=10, sample=4096, seed=0):
+    """PressureDependMultiYield material points (fx_pdmy_update): a dense sand (20 surfaces, friction
+    angle 40, phase transformation 27 degrees, dilatancy), otherwise as pimy_points."""
+    import femorax_b200 as fx
+    m = fx.PressureDependMultiYield(2.03, 145000, 314167, 40, 0.1, 80, 0.5, 27, 0.03, 0.8, 5, 0, 0, 0,
+                                    noYieldSurf=20, e=0.45)
+    return pimy_points(device, n, steps, sample, seed, material=m, amplitude=5e-3)
+
+
+def pimy_points(device, n=1 << 20, steps=10, sample=8192, seed=0, material=None, amplitude=2e-2):
     """PressureIndependMultiYield material points (fx_pimy_update): n points of a frictional sand
     (20 surfaces, friction angle 30 degrees, pressure-dependent moduli) on seeded strain paths,
     switched to the plastic stage under confinement, then `steps` cyclic-shear updates with the
@@ -206,10 +216,10 @@ def pimy_points(device, n=1 << 20, steps=10, sample=8192, seed=0):
     same arithmetic on `sample` points on one core beside it."""
     import torch
     import femorax_b200 as fx
-    m = fx.PressureIndependMultiYield(2.0, 60000, 150000, 5, 0.1, 30, 80, 0.5, 20)
+    m = material or fx.PressureIndependMultiYield(2.0, 60000, 150000, 5, 0.1, 30, 80, 0.5, 20)
     dev = torch.device("cuda", device)
     rng = np.random.default_rng(seed)
-    amp = torch.as_tensor(rng.uniform(2e-4, 2e-2, n), device=dev)
+    amp = torch.as_tensor(rng.uniform(2e-4, amplitude, n), device=dev)
     dirs = torch.as_tensor(rng.standard_normal((3, n)), device=dev)
     dirs /= dirs.norm(dim=0)
     conf = torch.as_tensor(rng.uniform(-2e-3, -5e-4, n), device=dev)
@@ -639,6 +649,7 @@ def run_ours(args):
     pimy = pimy_points(local) if world == 1 and not args.no_serve else None
     if pimy is not None:
         pimy["explicit_box"] = pimy_explicit(local)
+    pdmy = pdmy_points(local) if world == 1 and not args.no_serve else None
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -665,7 +676,8 @@ def run_ours(args):
             "served_rates": served_rates,
             "batched_j2": batched_j2,
             "newmark": newmark,
-            "pimy": pimy}
+            "pimy": pimy,
+            "pdmy": pdmy}
     print(json.dumps(line))
     return 0
 

@@ -374,56 +374,53 @@ class InternalForce:
             self._h = None
 
 
-class PressureIndependMultiYield:
-    """Material points of OpenSees' nDMaterial PressureIndependMultiYield, 3D (fx_pimy_*; the
-    reference's PressureIndependMultiYield<NS>, src/physics/materials/pressure_independ_multi_yield.hpp):
-    the constructor's arguments in OpenSees' order and defaults, `pairs` the (gamma, G/Gmax) pairs of
-    a user backbone (noYieldSurf pairs) or None.
+class _MaterialPoints:
+    """Material points of a soil model behind fx_<model>_* (the PressureIndependMultiYield and
+    PressureDependMultiYield classes below). States are [nstate, npoints] arrays (value-major: value
+    k of every point contiguous), strains and stresses [6, npoints] (11 22 33 12 23 31; engineering
+    shear strains), tangents [36, npoints] (entry 6 r + c). update() works on device tensors,
+    update_host() on numpy arrays; both write the trial state in full, so a commit is a swap of the
+    committed and trial arrays. `stage` is the material stage (0 elastic, 1 plastic:
+    updateMaterialStage)."""
 
-    States are [nstate, npoints] arrays (value-major: value k of every point contiguous), strains
-    and stresses [6, npoints] (11 22 33 12 23 31; engineering shear strains), tangents
-    [36, npoints] (entry 6 r + c). update() works on device tensors, update_host() on numpy arrays;
-    both write the trial state in full, so a commit is a swap of the committed and trial arrays.
-    `stage` is the material stage (0 elastic, 1 plastic: updateMaterialStage)."""
+    _fn = ""
+    _nsetup = 0
 
-    def __init__(self, rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng=0.0, refPress=100.0,
-                 pressDependCoe=0.0, noYieldSurf=20, pairs=None):
-        in9, p9 = _f64([rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng, refPress,
-                        pressDependCoe, noYieldSurf])
+    def _make(self, values, pairs, surfaces):
+        v, pv = _f64(values)
         pp = None
         if pairs is not None and len(pairs):
             self._pairs = np.ascontiguousarray(pairs, np.float64).ravel()
-            if self._pairs.size != 2 * int(noYieldSurf):
+            if self._pairs.size != 2 * int(surfaces):
                 raise ValueError("a user backbone has noYieldSurf (gamma, G/Gmax) pairs")
             pp = self._pairs.ctypes.data_as(L.p_f64)
         h = C.c_void_p()
-        check(lib().fx_pimy_create(p9, pp, C.byref(h)))
+        check(getattr(lib(), self._fn + "_create")(pv, pp, C.byref(h)))
         self._h = h
         ns, nsurf = C.c_int32(), C.c_int32()
-        check(lib().fx_pimy_info(h, C.byref(ns), C.byref(nsurf)))
+        check(getattr(lib(), self._fn + "_info")(h, C.byref(ns), C.byref(nsurf)))
         self.nstate, self.surfaces = ns.value, nsurf.value
 
-    def setup_values(self):
-        """(residual pressure, friction angle, cohesion), surface sizes [40], plastic moduli [40]."""
-        out = np.zeros(83)
-        check(lib().fx_pimy_setup_values(self._h, out.ctypes.data_as(L.p_f64)))
-        return out[:3], out[3:43], out[43:83]
+    def _setup_values(self):
+        out = np.zeros(self._nsetup)
+        check(getattr(lib(), self._fn + "_setup_values")(self._h, out.ctypes.data_as(L.p_f64)))
+        return out
 
     def initial_state(self, npoints, device=None):
         """The state of npoints new points: a torch tensor on `device` (an index), or numpy."""
         if device is None:
             s = np.zeros((self.nstate, npoints))
-            check(lib().fx_pimy_init_host(self._h, npoints, s.ctypes.data_as(L.p_f64)))
+            check(getattr(lib(), self._fn + "_init_host")(self._h, npoints, s.ctypes.data_as(L.p_f64)))
             return s
         import torch
         s = torch.empty((self.nstate, npoints), dtype=torch.float64, device=torch.device("cuda", device))
-        check(lib().fx_pimy_init(self._h, npoints, _ptr(s), None))
+        check(getattr(lib(), self._fn + "_init")(self._h, npoints, _ptr(s), None))
         return s
 
     def update(self, stage, committed, trial, strain, stress, tangent=None, failed=None, stream=None):
         n = committed.shape[1]
-        check(lib().fx_pimy_update(self._h, int(stage), n, _ptr(committed), _ptr(trial), _ptr(strain), _ptr(stress),
-                                   _ptr(tangent), _ptr(failed), _stream(stream)))
+        check(getattr(lib(), self._fn + "_update")(self._h, int(stage), n, _ptr(committed), _ptr(trial), _ptr(strain),
+                                                   _ptr(stress), _ptr(tangent), _ptr(failed), _stream(stream)))
 
     def update_host(self, stage, committed, trial, strain, stress, tangent=None) -> int:
         """Returns the points that met a state OpenSees stops for (their stress is NaN)."""
@@ -433,21 +430,64 @@ class PressureIndependMultiYield:
         for a in arrs:
             if a.dtype != np.float64 or not a.flags.c_contiguous:
                 raise ValueError("host arrays must be C-contiguous float64")
-        check(lib().fx_pimy_update_host(self._h, int(stage), n, committed.ctypes.data_as(L.p_f64),
-                                        trial.ctypes.data_as(L.p_f64), strain.ctypes.data_as(L.p_f64),
-                                        stress.ctypes.data_as(L.p_f64),
-                                        tangent.ctypes.data_as(L.p_f64) if tangent is not None else None,
-                                        C.byref(bad)))
+        check(getattr(lib(), self._fn + "_update_host")(
+            self._h, int(stage), n, committed.ctypes.data_as(L.p_f64), trial.ctypes.data_as(L.p_f64),
+            strain.ctypes.data_as(L.p_f64), stress.ctypes.data_as(L.p_f64),
+            tangent.ctypes.data_as(L.p_f64) if tangent is not None else None, C.byref(bad)))
         return bad.value
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
             try:
-                lib().fx_pimy_destroy(h)
+                getattr(lib(), self._fn + "_destroy")(h)
             except Exception:
                 pass
             self._h = None
+
+
+class PressureIndependMultiYield(_MaterialPoints):
+    """OpenSees' nDMaterial PressureIndependMultiYield, 3D (fx_pimy_*; the reference's
+    PressureIndependMultiYield<NS>, src/physics/materials/pressure_independ_multi_yield.hpp): the
+    constructor's arguments in OpenSees' order and defaults, `pairs` the (gamma, G/Gmax) pairs of a
+    user backbone (noYieldSurf pairs) or None. Also bound to mesh parameter sets
+    (InternalForce.set_pimy)."""
+
+    _fn = "fx_pimy"
+    _nsetup = 83
+
+    def __init__(self, rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng=0.0, refPress=100.0,
+                 pressDependCoe=0.0, noYieldSurf=20, pairs=None):
+        self._make([rho, refShearModul, refBulkModul, cohesi, peakShearStra, frictionAng, refPress, pressDependCoe,
+                    noYieldSurf], pairs, noYieldSurf)
+
+    def setup_values(self):
+        """(residual pressure, friction angle, cohesion), surface sizes [40], plastic moduli [40]."""
+        out = self._setup_values()
+        return out[:3], out[3:43], out[43:83]
+
+
+class PressureDependMultiYield(_MaterialPoints):
+    """OpenSees' nDMaterial PressureDependMultiYield, 3D (fx_pdmy_*; the reference's
+    PressureDependMultiYield<NS>, src/physics/materials/pressure_depend_multi_yield.hpp): the
+    constructor's arguments in OpenSees' order and the Tcl parser's defaults (liquefac3 is OpenSees'
+    liquefactionParam4), hv and pv the volumetric plasticity terms (0 and 1: none)."""
+
+    _fn = "fx_pdmy"
+    _nsetup = 85
+
+    def __init__(self, rho, refShearModul, refBulkModul, frictionAng, peakShearStra, refPress, pressDependCoe,
+                 PTAng, contrac, dilat1, dilat2, liquefac1, liquefac2, liquefac3, noYieldSurf=20, pairs=None, e=0.6,
+                 cs1=0.9, cs2=0.02, cs3=0.7, pa=101.0, c=0.3, hv=0.0, pv=1.0):
+        self._make([rho, refShearModul, refBulkModul, frictionAng, peakShearStra, refPress, pressDependCoe, PTAng,
+                    contrac, dilat1, dilat2, liquefac1, liquefac2, liquefac3, noYieldSurf, e, cs1, cs2, cs3, pa, c,
+                    hv, pv], pairs, noYieldSurf)
+
+    def setup_values(self):
+        """(residual pressure, friction angle, phase-transformation angle, its stress ratio, its
+        octahedral strain), surface sizes [40], plastic moduli [40]."""
+        out = self._setup_values()
+        return out[:5], out[5:45], out[45:85]
 
 
 class GroundMotions:

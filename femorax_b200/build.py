@@ -46,6 +46,7 @@ CUDA_SOURCES = [
     ("batch.cu", []),
     ("nbatch.cu", []),
     ("pimy.cu", ["--fmad=false"]),
+    ("pdmy.cu", ["--fmad=false"]),
 ]
 CXX_SOURCES = ["api.cpp", "compile.cpp"]
 

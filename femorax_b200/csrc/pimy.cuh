@@ -119,6 +119,16 @@ struct Ten {
   }
   FX_PIMY_HD double dev_length() const { return sqrt(dd(d, d)); }
   FX_PIMY_HD double oct_shear() const { return sqrt(1. / 3.) * dev_length(); }
+  FX_PIMY_HD double oct_shear_engr() const { return 2. * sqrt(1. / 3.) * dev_length(); }  // of a strain
+  FX_PIMY_HD double dev_ratio(double p_res) const {  // deviatorRatio
+    return sqrt(3. / 2. * dd(d, d)) / (fabs(m) + fabs(p_res));
+  }
+  FX_PIMY_HD void unit(double* out) const {  // unitT2: the components over their length
+    vset(out, t);
+    const double len = sqrt(dd(t, t));
+    if (len <= kLow) vdiv(out, kLow);
+    else vdiv(out, len);
+  }
   FX_PIMY_HD bool zero() const {
     for (int i = 0; i < 6; i++)
       if (t[i] != 0.0) return false;

@@ -486,6 +486,33 @@ int fx_pimy_init_host(const fx_pimy* m, int64_t npoints, double* state);
 int fx_pimy_update_host(const fx_pimy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
                         const double* strain, double* stress, double* tangent, int32_t* failed);
 
+/* ------------------------------------------------------------------ PressureDependMultiYield
+ * Material points of the pressure-dependent multi-yield-surface soil model with dilatancy and the
+ * phase-transformation zone (OpenSees nDMaterial PressureDependMultiYield, 3D; the reference's
+ * PressureDependMultiYield<NS>, src/physics/materials/pressure_depend_multi_yield.hpp: setup
+ * :122-170, initial_state :173-177, update :248-262; `stage` is updateMaterialStage's 0 or 1; the
+ * reference has no stage 2). At most 40 surfaces. The same calls as fx_pimy_*:
+ *   fx_pdmy_create       in23 = rho, refShearModul, refBulkModul, frictionAng, peakShearStra,
+ *                        refPress, pressDependCoe, PTAng, contrac, dilat1, dilat2, liquefac1,
+ *                        liquefac2, liquefac3, noYieldSurf, e, cs1, cs2, cs3, pa, c, hv, pv (OpenSees'
+ *                        order; hv = 0, pv = 1 for no volumetric plasticity); pairs or NULL.
+ *   fx_pdmy_info         state values per point (89 + 6 surfaces) and the surfaces.
+ *   fx_pdmy_setup_values out[85] = residual pressure, friction angle, phase-transformation angle,
+ *                        its stress ratio, its octahedral strain, then 40 sizes, 40 plastic moduli.
+ *   fx_pdmy_init / fx_pdmy_update / fx_pdmy_*_host as fx_pimy_* (value-major arrays; the trial
+ *                        state is written in full, so a commit is a swap). */
+typedef struct fx_pdmy fx_pdmy;
+int fx_pdmy_create(const double* in23, const double* pairs, fx_pdmy** out);
+void fx_pdmy_destroy(fx_pdmy* m);
+int fx_pdmy_info(const fx_pdmy* m, int32_t* nstate, int32_t* surfaces);
+int fx_pdmy_setup_values(const fx_pdmy* m, double* out);
+int fx_pdmy_init(fx_pdmy* m, int64_t npoints, double* state, void* stream);
+int fx_pdmy_update(fx_pdmy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
+                   const double* strain, double* stress, double* tangent, int32_t* failed, void* stream);
+int fx_pdmy_init_host(const fx_pdmy* m, int64_t npoints, double* state);
+int fx_pdmy_update_host(const fx_pdmy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
+                        const double* strain, double* stress, double* tangent, int32_t* failed);
+
 #ifdef __cplusplus
 }
 #endif

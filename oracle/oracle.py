@@ -85,6 +85,12 @@ def ref():
         L.fxref_brick_critical_dt.restype = C.c_double
         L.fxref_brick_critical_dt.argtypes = [p_f64, p_f64, C.c_int, p_f64]
         L.fxref_pimy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
+        L.fxref_pdmy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
+        L.fxref_pdmy_destroy.argtypes = [vp]
+        L.fxref_pdmy_nstate.restype = C.c_int32
+        L.fxref_pdmy_setup_values.argtypes = [vp, p_f64]
+        L.fxref_pdmy_initial_state.argtypes = [vp, p_f64]
+        L.fxref_pdmy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
         L.fxref_model_add_group_pimy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
         L.fxref_force_set_stage.argtypes = [vp, C.c_int32, C.c_int32]
         L.fxref_force_commit.argtypes = [vp]
@@ -637,6 +643,46 @@ class RefPimy:
     def __del__(self):
         if getattr(self, "h", None):
             ref().fxref_pimy_destroy(self.h)
+
+
+class RefPdmy(RefPimy):
+    """The reference's PressureDependMultiYield (40-surface bucket) at one material point
+    (oracle/_ref): params23 = the 21 constructor values of the stored paths' header (rho ... c)
+    then hv, pv; pairs: (gamma, G/Gmax) pairs or empty."""
+
+    def __init__(self, params23, pairs=()):
+        p, pp = _f(params23)
+        pr = np.ascontiguousarray(pairs, np.float64)
+        h = vp()
+        rc = ref().fxref_pdmy_create(pp, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2, C.byref(h))
+        assert rc == 0, rc
+        self.h = h
+        self.nstate = ref().fxref_pdmy_nstate()
+
+    def setup_values(self):
+        """residualPress, frictionAngle, phaseTransfAngle, stressRatioPT, strainPTOcta; sizes and
+        plastic moduli (1..40)."""
+        out = np.zeros(85)
+        ref().fxref_pdmy_setup_values(self.h, out.ctypes.data_as(p_f64))
+        return out[:5], out[5:45], out[45:85]
+
+    def initial_state(self):
+        s = np.zeros(self.nstate)
+        ref().fxref_pdmy_initial_state(self.h, s.ctypes.data_as(p_f64))
+        return s
+
+    def update(self, stage, committed, eps):
+        committed, pc = _f(committed)
+        eps, pe = _f(eps)
+        trial, sig, D = np.zeros(self.nstate), np.zeros(6), np.zeros((6, 6))
+        ref().fxref_pdmy_update(self.h, stage, pc, trial.ctypes.data_as(p_f64), pe, sig.ctypes.data_as(p_f64),
+                                D.ctypes.data_as(p_f64))
+        return trial, sig, D
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().fxref_pdmy_destroy(self.h)
+            self.h = None
 
 
 def port_dot(x, y, lanes, fused):

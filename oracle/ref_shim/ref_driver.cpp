@@ -21,6 +21,7 @@
 #include "exec/matrix_free_operator.hpp"
 #include "physics/elements/std_brick.hpp"
 #include "physics/materials/elastic_isotropic.hpp"
+#include "physics/materials/pressure_depend_multi_yield.hpp"
 #include "physics/materials/pressure_independ_multi_yield.hpp"
 #include "physics/operators/element_operator.hpp"
 #include "solvers/cg.hpp"
@@ -576,6 +577,70 @@ void fxref_pimy_update(fxref_pimy* h, int32_t stage, const double* committed, do
                        double* sig, double* D) {
   h->p.loadStage = stage;
   Pimy40::update(h->p, {committed, 1}, {trial, 1}, eps, sig, reinterpret_cast<double(*)[6]>(D));
+}
+
+// ---- PressureDependMultiYield (the reference's material, 40-surface bucket), one point at a time:
+// in23 = rho, refShearModul, refBulkModul, frictionAng, peakShearStra, refPress, pressDependCoe,
+// PTAng, contrac, dilat1, dilat2, liquefac1, liquefac2, liquefac3, noYieldSurf, e, cs1, cs2, cs3, pa,
+// c, hv, pv; pairs (gamma, G/Gmax) or NULL.
+using Pdmy40 = femorax::PressureDependMultiYield<40>;
+struct fxref_pdmy {
+  Pdmy40::Params p{};
+  std::vector<double> pairs;
+};
+
+int fxref_pdmy_create(const double* in, const double* pairs, int32_t npairs, fxref_pdmy** out) {
+  auto h = std::make_unique<fxref_pdmy>();
+  if (pairs && npairs > 0) h->pairs.assign(pairs, pairs + 2 * npairs);
+  Pdmy40::Input d{};
+  d.rho = in[0];
+  d.refShearModul = in[1];
+  d.refBulkModul = in[2];
+  d.frictionAng = in[3];
+  d.peakShearStra = in[4];
+  d.refPress = in[5];
+  d.pressDependCoe = in[6];
+  d.phaseTransformAng = in[7];
+  d.contractionParam1 = in[8];
+  d.dilationParam1 = in[9];
+  d.dilationParam2 = in[10];
+  d.liquefactionParam1 = in[11];
+  d.liquefactionParam2 = in[12];
+  d.liquefactionParam4 = in[13];
+  d.numberOfYieldSurf = static_cast<int>(in[14]);
+  d.gredu = h->pairs.empty() ? nullptr : h->pairs.data();
+  d.e = in[15];
+  d.volLimit1 = in[16];
+  d.volLimit2 = in[17];
+  d.volLimit3 = in[18];
+  d.atm = in[19];
+  d.cohesi = in[20];
+  d.hv = in[21];
+  d.pv = in[22];
+  const int rc = Pdmy40::setup(d, h->p);
+  if (rc != Pdmy40::Ok) return rc;
+  *out = h.release();
+  return 0;
+}
+void fxref_pdmy_destroy(fxref_pdmy* h) { delete h; }
+int32_t fxref_pdmy_nstate() { return Pdmy40::NSTATE; }
+// residualPress, frictionAngle, phaseTransfAngle, stressRatioPT, strainPTOcta, size[1..40], modulus[1..40]
+void fxref_pdmy_setup_values(const fxref_pdmy* h, double* out) {
+  out[0] = h->p.residualPress;
+  out[1] = h->p.frictionAngle;
+  out[2] = h->p.phaseTransfAngle;
+  out[3] = h->p.stressRatioPT;
+  out[4] = h->p.strainPTOcta;
+  for (int i = 1; i <= 40; ++i) {
+    out[4 + i] = h->p.size[i];
+    out[44 + i] = h->p.modulus[i];
+  }
+}
+void fxref_pdmy_initial_state(const fxref_pdmy* h, double* s) { Pdmy40::initial_state(h->p, {s, 1}); }
+void fxref_pdmy_update(fxref_pdmy* h, int32_t stage, const double* committed, double* trial, const double* eps,
+                       double* sig, double* D) {
+  h->p.loadStage = stage;
+  Pdmy40::update(h->p, {committed, 1}, {trial, 1}, eps, sig, reinterpret_cast<double(*)[6]>(D));
 }
 
 }  // extern "C"

@@ -9,13 +9,15 @@ the reference checkout and the oracle library exist):
   compile_maps.npz    the reference's compile_model output (oracle/_ref/libfxref.so) for two
                       small models: a 4 x 3 x 5 block with two Rayleigh regions (RCM, coloring)
                       and a 3 x 2 x 8 soil column with laminar equalDOF ties.
+  pdmy_paths.npz      the same for PressureDependMultiYield (tests/reference/data/nd/
+                      PressureDependMultiYield_*.txt).
   pimy_paths.npz      the reference's stored OpenSees PressureIndependMultiYield strain paths
                       (tests/reference/data/nd/PressureIndependMultiYield_*.txt, read as text):
                       per path the material's parameters and backbone pairs, and per step the
                       load stage, the discarded trial strain (if any), the strain, and OpenSees'
                       stress and tangent.
 
-    python tests/golden/make_golden.py [bricks|compile_maps|pimy_paths ...]
+    python tests/golden/make_golden.py [bricks|compile_maps|pimy_paths|pdmy_paths ...]
 """
 import glob
 import os
@@ -29,6 +31,9 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 DATA = "/root/reference/tests/reference/data/element"
 ND = "/root/reference/tests/reference/data/nd"
+PDMY_PARAMS = ("rho", "refShearModul", "refBulkModul", "frictionAng", "peakShearStra", "refPress", "pressDependCoe",
+               "PTAng", "contrac", "dilat1", "dilat2", "liquefac1", "liquefac2", "liquefac3", "noYieldSurf", "e", "cs1",
+               "cs2", "cs3", "pa", "c")
 PIMY_PARAMS = ("rho", "refShearModul", "refBulkModul", "cohesi", "peakShearStra", "frictionAng", "refPress",
                "pressDependCoe", "noYieldSurf")
 
@@ -102,15 +107,16 @@ def compile_maps():
     print("compile_maps.npz written")
 
 
-def pimy_paths():
+def pimy_paths(material="PressureIndependMultiYield", names=None, out_name="pimy_paths.npz"):
+    names = names or PIMY_PARAMS
     out, cases = {}, []
-    for path in sorted(glob.glob(os.path.join(ND, "PressureIndependMultiYield_*.txt"))):
-        name = os.path.basename(path)[len("PressureIndependMultiYield_"):-len(".txt")]
+    for path in sorted(glob.glob(os.path.join(ND, material + "_*.txt"))):
+        name = os.path.basename(path)[len(material) + 1:-len(".txt")]
         h, rows = read_reference_file(path)
         col = {c: i for i, c in enumerate(h["columns"])}
         p = h["params"]
         params = dict(zip(p[0::2], map(float, p[1::2])))
-        out[name + "/params"] = np.array([params[k] for k in PIMY_PARAMS])
+        out[name + "/params"] = np.array([params[k] for k in names])
         out[name + "/pairs"] = np.array(list(map(float, h.get("pairs", []))))
         out[name + "/stage"] = rows[:, col["stage"]].astype(np.int8)
         out[name + "/pre"] = rows[:, col["pre"]].astype(np.int8)
@@ -120,12 +126,16 @@ def pimy_paths():
         out[name + "/D"] = rows[:, col["D00"]:col["D00"] + 36].reshape(-1, 6, 6)
         cases.append(name)
     out["cases"] = np.array(cases)
-    out["param_names"] = np.array(PIMY_PARAMS)
-    np.savez_compressed(os.path.join(HERE, "pimy_paths.npz"), **out)
-    print("pimy_paths.npz:", len(cases), "paths")
+    out["param_names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, out_name), **out)
+    print(out_name + ":", len(cases), "paths")
+
+
+def pdmy_paths():
+    pimy_paths("PressureDependMultiYield", PDMY_PARAMS, "pdmy_paths.npz")
 
 
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["bricks", "compile_maps", "pimy_paths"]
+    what = sys.argv[1:] or ["bricks", "compile_maps", "pimy_paths", "pdmy_paths"]
     for w in what:
         globals()[w]()
