@@ -293,6 +293,12 @@ class InternalForce:
         self._materials = getattr(self, "_materials", {})
         self._materials[int(param_set)] = material
 
+    def set_pdmy(self, param_set: int, material: "PressureDependMultiYield"):
+        """Binds a PressureDependMultiYield material to a parameter set (fx_force_set_pdmy)."""
+        check(lib().fx_force_set_pdmy(self._h, int(param_set), material._h))
+        self._materials = getattr(self, "_materials", {})
+        self._materials[int(param_set)] = material
+
     def set_material_stage(self, param_set: int, stage: int):
         """updateMaterialStage for a PressureIndependMultiYield set (InternalForce::set_material_stage)."""
         check(lib().fx_force_set_material_stage(self._h, int(param_set), int(stage)))

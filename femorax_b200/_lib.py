@@ -122,6 +122,7 @@ PROTOTYPES = {
     "fx_pimy_update": (C.c_int, [vp, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp]),
     "fx_pimy_init_host": (C.c_int, [vp, C.c_int64, p_f64]),
     "fx_force_set_pimy": (C.c_int, [vp, C.c_int32, vp]),
+    "fx_force_set_pdmy": (C.c_int, [vp, C.c_int32, vp]),
     "fx_pdmy_create": (C.c_int, [p_f64, p_f64, C.POINTER(vp)]),
     "fx_pdmy_destroy": (None, [vp]),
     "fx_pdmy_info": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),

@@ -47,6 +47,7 @@ int64_t ForceState::device_bytes() const {
   b += j2_committed.bytes() + j2_trial.bytes() + j2_tan.bytes() + plastic_dev.bytes();
   b += geom32.bytes() + nshape32.bytes() + slots32.bytes();
   b += pimy_dev.bytes() + pimy_committed.bytes() + pimy_trial.bytes() + pimy_tan.bytes() + pimy_failed.bytes() + pimy_sig.bytes();
+  b += pdmy_dev.bytes() + pdmy_committed.bytes() + pdmy_trial.bytes() + pdmy_tan.bytes() + pdmy_sig.bytes();
   return b;
 }
 
@@ -546,7 +547,8 @@ int fx_force_plastic_points(fx_force* f, int64_t* count) {
   return guarded([&] {
     FX_REQUIRE(f && count, "fx_force_plastic_points: bad arguments");
     int n = 0;
-    if (f->s.has_j2 || f->s.has_pimy) FX_CUDA(cudaMemcpy(&n, f->s.plastic_dev.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f->s.has_j2 || f->s.has_pimy || f->s.has_pdmy)
+      FX_CUDA(cudaMemcpy(&n, f->s.plastic_dev.ptr, sizeof(int), cudaMemcpyDeviceToHost));
     f->s.plastic_points = n;
     *count = n;
   });

@@ -194,6 +194,12 @@ struct ForceState {
   DeviceArray<double> pimy_sig;  // the points' stresses of the last force evaluation, [(c * 8 + gp) * P + e]
   DeviceArray<int> pimy_failed;  // points whose update met a state OpenSees stops for (cumulative)
   int pimy_nstate = 0;
+  // PressureDependMultiYield sets, laid out the same way (their trial state is written in full)
+  bool has_pdmy = false;
+  std::vector<PdmySet> pdmy_h;
+  DeviceArray<PdmySet> pdmy_dev;
+  DeviceArray<double> pdmy_committed, pdmy_trial, pdmy_tan, pdmy_sig;
+  int pdmy_nstate = 0;
   ExplicitWork xw;
   bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
   bool use_box_force() const { return use_box() && box.force_ok; }
@@ -209,7 +215,8 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
 void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st);
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
-// commitState of the PressureIndependMultiYield points (their trial surfaces are copy-on-write)
+// commitState of the multi-yield soil points (PressureIndependMultiYield: copy-on-write surfaces;
+// PressureDependMultiYield: the whole trial state)
 void pimy_commit(ForceState& s, cudaStream_t st);
 
 // stepping.cu: the Newmark form-D kernels (implicit_stage.cpp:29-68)

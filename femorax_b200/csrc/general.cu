@@ -29,7 +29,9 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
                                                            const double* __restrict__ x, double* __restrict__ slots,
                                                            const int* skip, const double* __restrict__ j2tan,
                                                            int initial, const PimySet* __restrict__ pimy,
-                                                           const double* __restrict__ ptan) {
+                                                           const double* __restrict__ ptan,
+                                                           const PdmySet* __restrict__ pdmy,
+                                                           const double* __restrict__ dtan) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count || (skip && *skip)) return;
   const ParamGP p = params[param[e]];
@@ -43,6 +45,7 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
   const OpFactors f = op_factors(p, ks, kd, km);
   if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
   else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, P, f.cK, initial != 0});
+  else if (p.kind == 3) element_apply_d(p, f, xl, xe, ye, PdmyPointD{pdmy + p.table, dtan + e, P, f.cK, initial != 0});
   else element_apply(p, f, xl, xe, ye);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
 }
@@ -53,7 +56,9 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
                                                           int32_t count, double ks, double kd, double km,
                                                           double* __restrict__ slots, const double* __restrict__ j2tan,
                                                           int initial, const PimySet* __restrict__ pimy,
-                                                          const double* __restrict__ ptan) {
+                                                          const double* __restrict__ ptan,
+                                                          const PdmySet* __restrict__ pdmy,
+                                                          const double* __restrict__ dtan) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -65,6 +70,8 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
   if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
   else if (p.kind == 2)
     element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, P, f.cK, initial != 0});
+  else if (p.kind == 3)
+    element_diagonal_d(p, f, xl, eqe, de, PdmyPointD{pdmy + p.table, dtan + e, P, f.cK, initial != 0});
   else element_diagonal(p, f, xl, eqe, de);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = de[a];
 }
@@ -79,7 +86,7 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
-  if (p.kind == 2) return;  // k_pimy_points + k_pimy_force
+  if (p.kind >= 2) return;  // soil materials: k_soil_points + k_soil_force
   double xl[3][8], ue[24], ve[24], fe[24];
   load_coords(coords, node, N, P, e, xl);
   for (int a = 0; a < 24; ++a) {
@@ -96,12 +103,22 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = fe[a];
 }
 
-// PressureIndependMultiYield sets, point by point: thread t is point gp = t / P of element
-// e = t % P (consecutive threads, consecutive elements: every state value is read and written as
-// whole lines); stress and compact tangent out. Yielding and failed points counted per warp.
-__global__ void __launch_bounds__(128) k_pimy_points(const double* __restrict__ coords, const int32_t* __restrict__ node,
+// Soil-material sets (PressureIndependMultiYield: kind 2, PressureDependMultiYield: kind 3), point by
+// point: thread t is point gp = t / P of element e = t % P (consecutive threads, consecutive elements:
+// every state value is read and written as whole lines); stress and compact tangent out. Yielding
+// and failed points counted per warp.
+FX_HD bool soil_point_update(const PimySet& m, const double xl[3][8], const double* ue, int gp, const double* c,
+                             double* t, int64_t stride, double* sg, double* tc, bool* pl) {
+  return point_update_pimy(m, xl, ue, gp, c, t, stride, sg, tc, pl);
+}
+FX_HD bool soil_point_update(const PdmySet& m, const double xl[3][8], const double* ue, int gp, const double* c,
+                             double* t, int64_t stride, double* sg, double* tc, bool* pl) {
+  return point_update_pdmy(m, xl, ue, gp, c, t, stride, sg, tc, pl);
+}
+template <class Set, int KIND, int KTAN>
+__global__ void __launch_bounds__(128) k_soil_points(const double* __restrict__ coords, const int32_t* __restrict__ node,
                                                      const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
-                                                     const ParamGP* __restrict__ params, const PimySet* __restrict__ pimy,
+                                                     const ParamGP* __restrict__ params, const Set* __restrict__ sets,
                                                      int32_t N, int32_t P, int32_t count, const double* __restrict__ u,
                                                      const double* __restrict__ pc, double* __restrict__ pt,
                                                      double* __restrict__ ptan, double* __restrict__ psig,
@@ -111,16 +128,16 @@ __global__ void __launch_bounds__(128) k_pimy_points(const double* __restrict__ 
   bool pl = false, bad = false;
   if (gp < 8 && e < count) {
     const ParamGP p = params[param[e]];
-    if (p.kind == 2) {
-      double xl[3][8], ue[24], sg[6], tc[pimy::kTan];
+    if (p.kind == KIND) {
+      double xl[3][8], ue[24], sg[6], tc[KTAN];
       load_coords(coords, node, N, P, e, xl);
       for (int a = 0; a < 24; ++a) {
         const int32_t q = eq[static_cast<int64_t>(a) * P + e];
         ue[a] = q >= 0 ? u[q] : 0.0;
       }
-      bad = !point_update_pimy(pimy[p.table], xl, ue, gp, pc + e, pt + e, P, sg, tc, &pl);
+      bad = !soil_point_update(sets[p.table], xl, ue, gp, pc + e, pt + e, P, sg, tc, &pl);
       for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
-      for (int c = 0; c < pimy::kTan; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
+      for (int c = 0; c < KTAN; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
     }
   }
   const unsigned np = __popc(__ballot_sync(0xffffffffu, pl)), nb = __popc(__ballot_sync(0xffffffffu, bad));
@@ -131,15 +148,16 @@ __global__ void __launch_bounds__(128) k_pimy_points(const double* __restrict__ 
 }
 
 // ... then their elements' internal forces from the points' stresses, into the slots
-__global__ void __launch_bounds__(kBlock) k_pimy_force(const double* __restrict__ coords, const int32_t* __restrict__ node,
+__global__ void __launch_bounds__(kBlock) k_soil_force(const double* __restrict__ coords, const int32_t* __restrict__ node,
                                                         const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
                                                         const ParamGP* __restrict__ params, int32_t N, int32_t P,
                                                         int32_t count, const double* __restrict__ v,
-                                                        const double* __restrict__ psig, double* __restrict__ slots) {
+                                                        const double* __restrict__ psig, double* __restrict__ slots,
+                                                        int kind) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
-  if (p.kind != 2) return;
+  if (p.kind != kind) return;
   double xl[3][8], ve[24], fe[24];
   load_coords(coords, node, N, P, e, xl);
   for (int a = 0; a < 24; ++a) {
@@ -309,8 +327,8 @@ __global__ void __launch_bounds__(256) k_gather32(const int32_t* __restrict__ st
 }  // namespace
 
 void general_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st, const int* skip) {
-  if (s.has_pimy)
-    throw Error(FX_E_UNSUPPORTED, "the FP32 operator has no PressureIndependMultiYield tangent form");
+  if (s.has_pimy || s.has_pdmy)
+    throw Error(FX_E_UNSUPPORTED, "the FP32 operator has no multi-yield soil tangent form");
   if (s.count > 0 && s.geom32.n == 0) {  // the FP32 geometric factors, once
     s.geom32.alloc(static_cast<size_t>(kGeom32) * 8 * s.P);
     s.nshape32.alloc(64);
@@ -337,7 +355,8 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
                                                                    -1, x, s.slots.ptr, skip, s.j2_tan.ptr, s.initial,
-                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr);
+                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
+                                                                   s.pdmy_tan.ptr);
   FX_LAUNCH_CHECK("element_apply");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -352,7 +371,8 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
     k_element_diag<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                   s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
                                                                   s.slots.ptr, s.j2_tan.ptr, s.initial,
-                                                                  s.pimy_dev.ptr, s.pimy_tan.ptr);
+                                                                  s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
+                                                                  s.pdmy_tan.ptr);
   FX_LAUNCH_CHECK("element_diagonal");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -363,23 +383,33 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
 }
 
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
-  if (s.has_j2 || s.has_pimy) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
+  if (s.has_j2 || s.has_pimy || s.has_pdmy) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
   if (s.count > 0)
     k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr,
                                                                    s.j2_committed.ptr, s.j2_trial.ptr, s.j2_tan.ptr,
                                                                    s.plastic_dev.ptr);
   FX_LAUNCH_CHECK("element_force");
+  const int64_t points = static_cast<int64_t>(8) * s.P;
   if (s.has_pimy && s.count > 0) {
-    const int64_t points = static_cast<int64_t>(8) * s.P;
-    k_pimy_points<<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+    k_soil_points<PimySet, 2, pimy::kTan><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.N, s.P, s.count, u,
         s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
     FX_LAUNCH_CHECK("pimy_points");
-    k_pimy_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+    k_soil_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                s.params.ptr, s.N, s.P, s.count, v, s.pimy_sig.ptr,
-                                                               s.slots.ptr);
+                                                               s.slots.ptr, 2);
     FX_LAUNCH_CHECK("pimy_force");
+  }
+  if (s.has_pdmy && s.count > 0) {
+    k_soil_points<PdmySet, 3, pdmy::kTan><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+        s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pdmy_dev.ptr, s.N, s.P, s.count, u,
+        s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_tan.ptr, s.pdmy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
+    FX_LAUNCH_CHECK("pdmy_points");
+    k_soil_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                               s.params.ptr, s.N, s.P, s.count, v, s.pdmy_sig.ptr,
+                                                               s.slots.ptr, 3);
+    FX_LAUNCH_CHECK("pdmy_force");
   }
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
@@ -389,6 +419,9 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
 }
 
 void pimy_commit(ForceState& s, cudaStream_t st) {
+  if (s.has_pdmy)  // written in full: the whole trial state
+    FX_CUDA(cudaMemcpyAsync(s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_committed.bytes(), cudaMemcpyDeviceToDevice,
+                            st));
   if (!s.has_pimy || s.count == 0) return;
   const int64_t points = static_cast<int64_t>(8) * s.P;
   k_pimy_commit<<<static_cast<unsigned>((points + 255) / 256), 256, 0, st>>>(
@@ -410,7 +443,8 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, 0.0, 0.0, 1.0, dir,
                                                                    nullptr, s.slots.ptr, nullptr, s.j2_tan.ptr, 0,
-                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr);
+                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
+                                                                   s.pdmy_tan.ptr);
   FX_LAUNCH_CHECK("element_apply_unit");
   if (s.neq > 0)
     k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "force.hpp"
 #include "host.hpp"
 #include "pdmy.cuh"
 
@@ -55,6 +56,21 @@ __global__ void __launch_bounds__(128) k_pdmy_update(const pdmy::Params* __restr
 }
 
 unsigned blocks_for(int64_t n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+// The points of the elements of parameter set `set` (table entry m): the material's new state in both
+// buffers and the elastic compact tangent.
+__global__ void k_pdmy_elements_init(const int32_t* __restrict__ param, int32_t count, int32_t P, int32_t set,
+                                     const PdmySet* __restrict__ m, double* __restrict__ committed,
+                                     double* __restrict__ trial, double* __restrict__ tan) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count || param[e] != set) return;
+  for (int gp = 0; gp < 8; ++gp) {
+    const int64_t base = static_cast<int64_t>(gp) * P + e, ld = 8 * static_cast<int64_t>(P);
+    pdmy::initial_state(m->p, pimy::Slab<double>{committed + base, ld});
+    pdmy::initial_state(m->p, pimy::Slab<double>{trial + base, ld});
+    for (int c = 0; c < pdmy::kTan; ++c) tan[base + c * ld] = 0.0;  // stage 0: the elastic tangent
+  }
+}
 
 void check_update(const fx_pdmy* h, int32_t stage, int64_t n, const double* c, const double* t, const double* e,
                   const double* s, const char* who) {
@@ -132,6 +148,59 @@ int fx_pdmy_update(fx_pdmy* h, int32_t stage, int64_t npoints, const double* com
     fx::k_pdmy_update<<<fx::blocks_for(npoints, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
         h->dev.ptr, stage, npoints, committed, trial, strain, stress, tangent, failed);
     FX_LAUNCH_CHECK("pdmy_update");
+  });
+}
+
+int fx_force_set_pdmy(fx_force* f, int32_t set, const fx_pdmy* m) {
+  return fx::guard([&] {
+    if (!f || !m) throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: bad arguments");
+    fx::ForceState& s = f->s;
+    if (set < 0 || set >= s.nparams) throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: no such parameter set");
+    fx::ParamGP& q = s.params_h[set];
+    if (q.kind == FX_MAT_J2 || q.kind == 2) throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: the set has another material");
+    if (q.betaK != 0.0 || q.betaKinit != 0.0 || q.betaKcomm != 0.0)
+      throw fx::Error(FX_E_UNSUPPORTED, "stiffness-proportional Rayleigh damping on a PressureDependMultiYield set");
+    if (q.rho != m->p.rho)
+      throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: the set's density (its masses) differs from the material's");
+    const int need = fx::pdmy::nstate(m->p.ns);
+    const int64_t P = s.P;
+    if (need > s.pdmy_nstate) {  // (re)allocate the point arrays; earlier bindings start again
+      s.pdmy_committed.alloc(static_cast<size_t>(need) * 8 * P);
+      s.pdmy_trial.alloc(static_cast<size_t>(need) * 8 * P);
+      if (!s.pdmy_tan.ptr) s.pdmy_tan.alloc(static_cast<size_t>(fx::pdmy::kTan) * 8 * P);
+      if (!s.pdmy_sig.ptr) s.pdmy_sig.alloc(static_cast<size_t>(6) * 8 * P);
+      s.pdmy_nstate = need;
+    }
+    if (!s.pdmy_dev.ptr) s.pdmy_dev.alloc(static_cast<size_t>(s.nparams));
+    if (!s.plastic_dev.ptr) {
+      s.plastic_dev.alloc(1);
+      FX_CUDA(cudaMemset(s.plastic_dev.ptr, 0, sizeof(int)));
+    }
+    if (!s.pimy_failed.ptr) {
+      s.pimy_failed.alloc(1);
+      FX_CUDA(cudaMemset(s.pimy_failed.ptr, 0, sizeof(int)));
+    }
+    if (q.kind != 3) {
+      q.table = static_cast<int>(s.pdmy_h.size());
+      s.pdmy_h.push_back(fx::PdmySet{m->p, 0});
+    } else {
+      s.pdmy_h[q.table] = fx::PdmySet{m->p, 0};
+    }
+    q.kind = 3;
+    FX_CUDA(cudaMemcpy(s.pdmy_dev.ptr, s.pdmy_h.data(), sizeof(fx::PdmySet) * s.pdmy_h.size(), cudaMemcpyHostToDevice));
+    FX_CUDA(cudaMemcpy(s.params.ptr, s.params_h.data(), sizeof(fx::ParamGP) * s.params_h.size(), cudaMemcpyHostToDevice));
+    s.has_pdmy = true;
+    s.box.qualifies = false;
+    s.box.why_not = "the mesh has PressureDependMultiYield sets";
+    for (int32_t k = 0; k < s.nparams; ++k)
+      if (s.params_h[k].kind == 3 && s.count > 0) {
+        fx::k_pdmy_elements_init<<<fx::blocks_for(s.count, 128), 128>>>(s.param.ptr, s.count, s.P, k,
+                                                                        s.pdmy_dev.ptr + s.params_h[k].table,
+                                                                        s.pdmy_committed.ptr, s.pdmy_trial.ptr,
+                                                                        s.pdmy_tan.ptr);
+        FX_LAUNCH_CHECK("pdmy_elements_init");
+      }
+    FX_CUDA(cudaStreamSynchronize(nullptr));
   });
 }
 

@@ -184,6 +184,27 @@ FX_PIMY_HD inline void elastic_D(const Params& p, double factor, double* D) {  /
     }
 }
 
+// The tangent D[6 i + j] of a compact form t[kTan] (Point::compact): the reference elastic tangent in
+// the elastic stage; in the plastic stage getTangent's expression from the point's moduli G, K, its
+// coefficients c1 (volumetric) and c2 and the normal's deviator w.
+constexpr int kTan = 11;
+FX_PIMY_HD inline void compact_D(const Params& p, const double* t, double* D) {
+  if (t[0] != 1.0) {
+    elastic_D(p, 1.0, D);
+    return;
+  }
+  const double G = t[1], Kb = t[2], c1 = t[3], c2 = t[4];
+  const double* w = t + 5;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      double v = -c2 * w[i] * w[j];
+      if (i == j) v += G;
+      if (i < 3 && j < 3 && i == j) v += G;
+      if (i < 3 && j < 3) v += (Kb - 2. * G / 3. - c1);
+      D[6 * i + j] = v;
+    }
+}
+
 // One point's update from the committed state C to the trial state T at total strain eps
 // (engineering shear): OpenSees' setTrialStrain + getStress + getTangent, the instance's members as
 // locals, the trial buffer holding the surface centers being worked on.
@@ -686,11 +707,12 @@ struct Point {
     }
   }
 
-  FX_PIMY_HD void tangent(double* D) const {  // getTangent, D[6 i + j]
-    if (stage != 1) {
-      elastic_D(P, 1.0, D);
-      return;
-    }
+  // getTangent in compact form (kTan values): stage, G, K, the two rank-one coefficients and the
+  // normal's deviator; compact_D expands it.
+  FX_PIMY_HD void compact(double* t) const {
+    t[0] = stage;
+    for (int k = 1; k < kTan; ++k) t[k] = 0.;
+    if (stage != 1) return;
     const double f = modulus_factor(cur);
     const double G = f * P.G0;
     double Kb = f * P.K0;
@@ -709,14 +731,16 @@ struct Point {
       c1 = 9. * Kb * Kb * vol * vol / (Ho + pm);
       c2 = 4. * G * G / (Ho + pm);
     }
-    for (int i = 0; i < 6; i++)
-      for (int j = 0; j < 6; j++) {
-        double v = -c2 * w[i] * w[j];
-        if (i == j) v += G;
-        if (i < 3 && j < 3 && i == j) v += G;
-        if (i < 3 && j < 3) v += (Kb - 2. * G / 3. - c1);
-        D[6 * i + j] = v;
-      }
+    t[1] = G;
+    t[2] = Kb;
+    t[3] = c1;
+    t[4] = c2;
+    for (int k = 0; k < 6; ++k) t[5 + k] = w[k];
+  }
+  FX_PIMY_HD void tangent(double* D) const {  // getTangent, D[6 i + j]
+    double t[kTan];
+    compact(t);
+    compact_D(P, t, D);
   }
 
   FX_PIMY_HD bool predict(const double* eps) {  // getStress up to the elastic-or-plastic decision
@@ -822,6 +846,18 @@ FX_PIMY_HD inline bool update(const Params& p, int stage, CV C, TV T, const doub
   Point<CV, TV> pt(p, stage, C, T);
   if (pt.predict(eps)) pt.correct();
   pt.finish(sig, D);
+  return pt.ok;
+}
+
+// The same with the tangent in compact form t[kTan]; *plastic: an active yield surface.
+template <class CV, class TV>
+FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, const double* eps, double* sig, double* t,
+                                      bool* plastic) {
+  Point<CV, TV> pt(p, stage, C, T);
+  if (pt.predict(eps)) pt.correct();
+  pt.finish(sig, nullptr);
+  pt.compact(t);
+  *plastic = stage == 1 && pt.active > 0;
   return pt.ok;
 }
 

@@ -162,7 +162,7 @@ int fx_force_set_pimy(fx_force* f, int32_t set, const fx_pimy* m) {
     fx::ForceState& s = f->s;
     if (set < 0 || set >= s.nparams) throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: no such parameter set");
     fx::ParamGP& q = s.params_h[set];
-    if (q.kind == FX_MAT_J2) throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: the set is a J2 set");
+    if (q.kind == FX_MAT_J2 || q.kind == 3) throw fx::Error(FX_E_INVALID, "fx_force_set_pimy: the set has another material");
     if (q.betaK != 0.0 || q.betaKinit != 0.0 || q.betaKcomm != 0.0)
       throw fx::Error(FX_E_UNSUPPORTED, "stiffness-proportional Rayleigh damping on a PressureIndependMultiYield set");
     if (q.rho != m->p.rho)
@@ -214,10 +214,16 @@ int fx_force_set_material_stage(fx_force* f, int32_t set, int32_t stage) {
   return fx::guard([&] {
     if (!f || (stage != 0 && stage != 1)) throw fx::Error(FX_E_INVALID, "fx_force_set_material_stage: bad arguments");
     fx::ForceState& s = f->s;
-    if (set < 0 || set >= s.nparams || s.params_h[set].kind != 2)
-      throw fx::Error(FX_E_INVALID, "fx_force_set_material_stage: not a PressureIndependMultiYield set");
-    s.pimy_h[s.params_h[set].table].stage = stage;
-    fx::upload_table(s);
+    if (set < 0 || set >= s.nparams || (s.params_h[set].kind != 2 && s.params_h[set].kind != 3))
+      throw fx::Error(FX_E_INVALID, "fx_force_set_material_stage: not a multi-yield soil set");
+    if (s.params_h[set].kind == 2) {
+      s.pimy_h[s.params_h[set].table].stage = stage;
+      fx::upload_table(s);
+    } else {
+      s.pdmy_h[s.params_h[set].table].stage = stage;
+      FX_CUDA(cudaMemcpy(s.pdmy_dev.ptr, s.pdmy_h.data(), sizeof(fx::PdmySet) * s.pdmy_h.size(),
+                         cudaMemcpyHostToDevice));
+    }
   });
 }
 

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "brick_gp.cuh"
+#include "pdmy.cuh"
 #include "pimy.cuh"
 
 namespace fx {
@@ -14,6 +15,12 @@ namespace fx {
 struct PimySet {
   pimy::Params p;
   int stage;  // 0 elastic, 1 plastic (updateMaterialStage)
+};
+
+// A parameter set's PressureDependMultiYield material (ParamGP::table indexes its table) and stage.
+struct PdmySet {
+  pdmy::Params p;
+  int stage;
 };
 
 // The update of point gp of element e (the reference's point_update_shape without stiffness
@@ -27,6 +34,18 @@ FX_HD bool point_update_pimy(const PimySet& m, const double xl[3][8], const doub
   double e[6];
   strain_of(s, ue, e);
   return pimy::update_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride},
+                              pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, plastic);
+}
+
+// The same for a PressureDependMultiYield point (its trial state written in full).
+FX_HD bool point_update_pdmy(const PdmySet& m, const double xl[3][8], const double* ue, int gp,
+                             const double* committed, double* trial, int64_t stride, double sg[6],
+                             double t[pdmy::kTan], bool* plastic) {
+  PointShape s;
+  point_shape(xl, gp, s);
+  double e[6];
+  strain_of(s, ue, e);
+  return pdmy::update_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride},
                               pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, plastic);
 }
 
@@ -87,6 +106,30 @@ struct PimyPointD {
       double t[pimy::kTan];
       for (int c = 0; c < pimy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
       pimy::compact_D(t, D);
+    }
+    for (int a = 0; a < 6; ++a)
+      for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
+    for (int a = 0; a < 6; ++a)
+      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+  }
+};
+
+// The operator's material matrix of a PressureDependMultiYield point: its stored tangent (upper
+// triangle mirrored) scaled by the stiffness factor, or the reference elastic tangent (initial).
+struct PdmyPointD {
+  const PdmySet* m;
+  const double* tan;
+  int64_t stride;
+  double cK;
+  bool initial;
+  FX_HD void operator()(int gp, double De[6][6]) const {
+    double D[36];
+    if (initial) {
+      pdmy::elastic_D(m->p, 1.0, D);
+    } else {
+      double t[pdmy::kTan];
+      for (int c = 0; c < pdmy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
+      pdmy::compact_D(m->p, t, D);
     }
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];

@@ -31,6 +31,7 @@ class Group:
     # the group as an elastic set (E, nu, rho) and binds the material to its parameter set
     # (InternalForce.set_pimy); the reference's model gets the material itself.
     pimy: tuple = None
+    pdmy: tuple = None  # PressureDependMultiYield: (the 23 values of fx_pdmy_create, pairs or None), likewise
 
 
 @dataclasses.dataclass

@@ -475,7 +475,8 @@ int fx_pimy_update(fx_pimy* m, int32_t stage, int64_t npoints, const double* com
  * the operator and its diagonal use each point's tangent of the last fx_force_compute (the
  * reference's stored tangents at that displacement; `initial` in fx_coeffs: the material's
  * reference elastic tangent), fx_force_plastic_points counts points with an active surface.
- *   fx_force_set_material_stage  updateMaterialStage for the set (InternalForce::set_material_stage,
+ *   fx_force_set_material_stage  updateMaterialStage for the set, PressureIndependMultiYield or
+ *                                PressureDependMultiYield (InternalForce::set_material_stage,
  *                                src/exec/internal_force.cpp:511-515): 0 elastic, 1 plastic.
  *   fx_force_pimy_failed         points whose update met a state OpenSees stops for (stress NaN),
  *                                counted over all evaluations. */
@@ -509,6 +510,12 @@ int fx_pdmy_setup_values(const fx_pdmy* m, double* out);
 int fx_pdmy_init(fx_pdmy* m, int64_t npoints, double* state, void* stream);
 int fx_pdmy_update(fx_pdmy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
                    const double* strain, double* stress, double* tangent, int32_t* failed, void* stream);
+/* Binds material m to parameter set `set` of a mesh, as fx_force_set_pimy (the reference's
+ * StdBrick<PressureDependMultiYield<NS>>): Gauss-point path, elastic stage at first, the set's
+ * density equal to the material's, no stiffness-proportional damping; fx_force_set_material_stage,
+ * fx_force_compute / commit, the operator (each point's stored tangent of the last compute, upper
+ * triangle mirrored) and fx_force_pimy_failed work on it as on PressureIndependMultiYield sets. */
+int fx_force_set_pdmy(fx_force* f, int32_t set, const fx_pdmy* m);
 int fx_pdmy_init_host(const fx_pdmy* m, int64_t npoints, double* state);
 int fx_pdmy_update_host(const fx_pdmy* m, int32_t stage, int64_t npoints, const double* committed, double* trial,
                         const double* strain, double* stress, double* tangent, int32_t* failed);

@@ -92,6 +92,7 @@ def ref():
         L.fxref_pdmy_initial_state.argtypes = [vp, p_f64]
         L.fxref_pdmy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
         L.fxref_model_add_group_pimy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
+        L.fxref_model_add_group_pdmy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
         L.fxref_force_set_stage.argtypes = [vp, C.c_int32, C.c_int32]
         L.fxref_force_commit.argtypes = [vp]
         L.fxref_apply_operator_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64, p_f64]
@@ -129,7 +130,13 @@ class RefModel:
             b, pb = _f(np.array(g.b, np.float64))
             et, pet = _i(g.etags)
             cn, pcn = _i(np.asarray(g.conn).reshape(-1))
-            if getattr(g, "pimy", None) is not None:
+            if getattr(g, "pdmy", None) is not None:
+                in23, pairs = g.pdmy
+                p23, pp23 = _f(in23)
+                pr = np.ascontiguousarray(pairs if pairs is not None else [], np.float64)
+                L.fxref_model_add_group_pdmy(self.h, pp23, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2,
+                                             pb, int(g.lumped), len(et), pet, pcn)
+            elif getattr(g, "pimy", None) is not None:
                 in9, pairs = g.pimy
                 p9, pp9 = _f(in9)
                 pr = np.ascontiguousarray(pairs if pairs is not None else [], np.float64)

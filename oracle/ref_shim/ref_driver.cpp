@@ -118,6 +118,50 @@ int fxref_model_add_group_pimy(fxref_model* h, const double* in9, const double* 
   return 0;
 }
 
+// The same with a PressureDependMultiYield material (in23 as fxref_pdmy_create but hv, pv unused:
+// the model file has none; npairs > 0: a user backbone, noYieldSurf = -npairs).
+int fxref_model_add_group_pdmy(fxref_model* h, const double* in, const double* pairs, int32_t npairs, const double* b,
+                               int lumped, int32_t count, const int32_t* etags, const int32_t* conn) {
+  io::NDMaterial mat;
+  mat.tag = static_cast<std::int32_t>(h->m.materials.size()) + 1;
+  io::PressureDependMultiYieldData d;
+  d.nd = 3;
+  d.rho = in[0];
+  d.refShearModul = in[1];
+  d.refBulkModul = in[2];
+  d.frictionAng = in[3];
+  d.peakShearStra = in[4];
+  d.refPress = in[5];
+  d.pressDependCoe = in[6];
+  d.PTAng = in[7];
+  d.contrac = in[8];
+  d.dilat1 = in[9];
+  d.dilat2 = in[10];
+  d.liquefac1 = in[11];
+  d.liquefac2 = in[12];
+  d.liquefac3 = in[13];
+  d.noYieldSurf = npairs > 0 ? -npairs : static_cast<std::int32_t>(in[14]);
+  if (npairs > 0) d.pairs.assign(pairs, pairs + 2 * static_cast<std::size_t>(npairs));
+  d.e = in[15];
+  d.cs1 = in[16];
+  d.cs2 = in[17];
+  d.cs3 = in[18];
+  d.pa = in[19];
+  d.c = in[20];
+  mat.data = d;
+  h->m.materials.push_back(mat);
+  io::ElementGroup g;
+  g.id = std::to_string(h->m.elements.size());
+  g.type = io::ElementType::StdBrick;
+  g.material = mat.tag;
+  g.body_force = {b[0], b[1], b[2]};
+  g.lumped = lumped != 0;
+  g.tags.assign(etags, etags + count);
+  g.connectivity.assign(conn, conn + 8 * static_cast<std::size_t>(count));
+  h->m.elements.push_back(std::move(g));
+  return 0;
+}
+
 void fxref_model_add_fix(fxref_model* h, int32_t n, const int32_t* node, const int32_t* dof) {
   h->m.fix.node.insert(h->m.fix.node.end(), node, node + n);
   h->m.fix.dof.insert(h->m.fix.dof.end(), dof, dof + n);
