@@ -198,6 +198,67 @@ def explicit_comparison(force, mesh, comp, device, steps=4000):
     return out
 
 
+PDMY_SAND = (2.0285423037716614, 145000.0, 314166.66666666663, 40.0, 0.1, 80.0, 0.5, 27.0, 0.03, 0.8, 5.0, 0.0, 0.0,
+             0.0, 20.0, 0.45, 0.9, 0.02, 0.7, 101.0, 0.3, 0.0, 1.0)  # dense sand of the stored paths
+
+
+def pdmy_force_box(device, n=40, evals=20):
+    """The reference's PressureDependMultiYield force measurement (the internal force of an n^3
+    stdBrick box of dense sand, 20 surfaces, in the plastic stage; 7.85 ms at 40^3 on an H200,
+    reference benchmarks/baselines/tacc-vista-gh-cuda270336.json:769, explicit_force_pdmy/40^3/plastic):
+    the box is confined (a uniform 2e-4 volumetric strain, elastic
+    stage, committed), switched to the plastic stage and sheared (committed), then `evals` force
+    evaluations at further shear strains (each every point's update from the committed state and the
+    element forces), timed by CUDA events."""
+    import torch
+    import femorax_b200 as fx
+    from femorax_b200 import meshes
+    G, K = PDMY_SAND[1], PDMY_SAND[2]
+    E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
+    spec = meshes.box_model(n, n, n, size=(float(n), float(n), float(n)), E=E, nu=nu, rho=PDMY_SAND[0], lumped=True)
+    mesh = fx.Model(spec).compile().mesh()
+    force = fx.InternalForce(mesh, device=device)
+    m = fx.PressureDependMultiYield(*PDMY_SAND[:14], noYieldSurf=int(PDMY_SAND[14]), e=PDMY_SAND[15],
+                                    cs1=PDMY_SAND[16], cs2=PDMY_SAND[17], cs3=PDMY_SAND[18], pa=PDMY_SAND[19],
+                                    c=PDMY_SAND[20])
+    force.set_pdmy(0, m)
+    dev = torch.device("cuda", device)
+    neq, P = mesh.num_equations, mesh.padded
+    node, eq, X = mesh.node.reshape(8, P), mesh.eq.reshape(24, P), mesh.coords.reshape(3, -1)
+    xq, zq, dof = np.zeros(neq), np.zeros(neq), np.full(neq, -1)
+    for a in range(8):
+        for d in range(3):
+            q = eq[3 * a + d, :mesh.count]
+            ok = q >= 0
+            xq[q[ok]], zq[q[ok]] = X[0, node[a, :mesh.count][ok]], X[2, node[a, :mesh.count][ok]]
+            dof[q[ok]] = d
+    conf = np.where(dof == 2, -2e-4 / 3 * zq, 0.0) + np.where(dof == 0, -2e-4 / 3 * xq, 0.0)
+    v = torch.zeros(neq, dtype=torch.float64, device=dev)
+    f = torch.zeros(neq, dtype=torch.float64, device=dev)
+
+    def u_at(gam):
+        return torch.as_tensor(conf + np.where(dof == 0, gam * zq, 0.0), device=dev)
+
+    force.compute(u_at(0.0), v, f)
+    force.commit_state()
+    force.set_material_stage(0, 1)
+    force.compute(u_at(2e-4), v, f)
+    force.commit_state()
+    us = [u_at(2e-4 + 1e-4 * np.sin(0.3 * k)) for k in range(evals + 3)]
+    for k in range(3):
+        force.compute(us[k], v, f)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(evals):
+        force.compute(us[3 + k], v, f)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return {"elements": int(mesh.count), "points": 8 * int(mesh.count), "ms_per_force": e0.elapsed_time(e1) / evals,
+            "plastic_points": int(force.plastic_points()), "failed_points": int(force.pimy_failed()),
+            "reference_h200_ms": 7.85}
+
+
 def pdmy_points(device, n=1 << 20, steps=10, sample=4096, seed=0):
     """PressureDependMultiYield material points (fx_pdmy_update): a dense sand (20 surfaces, friction
     angle 40, phase transformation 27 degrees, dilatancy), otherwise as pimy_points."""
@@ -650,6 +711,8 @@ def run_ours(args):
     if pimy is not None:
         pimy["explicit_box"] = pimy_explicit(local)
     pdmy = pdmy_points(local) if world == 1 and not args.no_serve else None
+    if pdmy is not None:
+        pdmy["force_box"] = pdmy_force_box(local)
     cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
