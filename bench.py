@@ -757,7 +757,12 @@ def main():
     ap.add_argument("--launch", default="", help="pin the box launch shape 'variant,kz' (profiling)")
     ap.add_argument("--pimy-box", type=int, default=0,
                     help="only the PressureIndependMultiYield plastic box section, n^3 elements (profiling)")
+    ap.add_argument("--pdmy-box", type=int, default=0,
+                    help="only the PressureDependMultiYield plastic force section, n^3 elements (profiling)")
     args = ap.parse_args()
+    if args.pdmy_box:
+        print(json.dumps(pdmy_force_box(int(os.environ.get("LOCAL_RANK", "0")), n=args.pdmy_box, evals=args.steps)))
+        return 0
     if args.pimy_box:
         print(json.dumps(pimy_explicit(int(os.environ.get("LOCAL_RANK", "0")), n=args.pimy_box, warm=args.warmup,
                                        steps=args.steps)))

@@ -115,8 +115,8 @@ FX_HD bool soil_point_update(const PdmySet& m, const double xl[3][8], const doub
                              double* t, int64_t stride, double* sg, double* tc, bool* pl) {
   return point_update_pdmy(m, xl, ue, gp, c, t, stride, sg, tc, pl);
 }
-template <class Set, int KIND, int KTAN>
-__global__ void __launch_bounds__(128) k_soil_points(const double* __restrict__ coords, const int32_t* __restrict__ node,
+template <class Set, int KIND, int KTAN, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restrict__ coords, const int32_t* __restrict__ node,
                                                      const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
                                                      const ParamGP* __restrict__ params, const Set* __restrict__ sets,
                                                      int32_t N, int32_t P, int32_t count, const double* __restrict__ u,
@@ -392,7 +392,7 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
   FX_LAUNCH_CHECK("element_force");
   const int64_t points = static_cast<int64_t>(8) * s.P;
   if (s.has_pimy && s.count > 0) {
-    k_soil_points<PimySet, 2, pimy::kTan><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+    k_soil_points<PimySet, 2, pimy::kTan, 3><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.N, s.P, s.count, u,
         s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
     FX_LAUNCH_CHECK("pimy_points");
@@ -402,7 +402,7 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
     FX_LAUNCH_CHECK("pimy_force");
   }
   if (s.has_pdmy && s.count > 0) {
-    k_soil_points<PdmySet, 3, pdmy::kTan><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+    k_soil_points<PdmySet, 3, pdmy::kTan, 2><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pdmy_dev.ptr, s.N, s.P, s.count, u,
         s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_tan.ptr, s.pdmy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
     FX_LAUNCH_CHECK("pdmy_points");
