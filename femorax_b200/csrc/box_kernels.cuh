@@ -557,10 +557,10 @@ __global__ void __launch_bounds__(BX* BY, MINB)
 
 // ------------------------------------------------------------------ launch variants
 // (BX, BY, CTAs per SM for the register budget, face caching)
-constexpr int kNumVariants = 10;  // see launch()
+constexpr int kNumVariants = 11;  // see launch()
 // the block of element columns (BX, BY) of each variant, for the host's tile geometry
-constexpr int kVariantBlock[kNumVariants][2] = {{32, 8}, {16, 16}, {16, 8}, {32, 16}, {16, 8},
-                                                {16, 8}, {16, 8},  {32, 4}, {16, 32}, {16, 8}};
+constexpr int kVariantBlock[kNumVariants][2] = {{32, 8}, {16, 16}, {16, 8}, {32, 16}, {16, 8}, {16, 8},
+                                                {16, 8}, {32, 4},  {16, 32}, {16, 8}, {16, 8}};
 
 template <class T>
 const BoxTable<typename Coef<T>::type>& table_of(const BoxPlan& p, int mode);
@@ -637,7 +637,8 @@ void launch(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
     case 6: return launch_one<16, 8, 6, false, T, MODE>(p, a, st);
     case 7: return launch_one<32, 4, 4, false, T, MODE>(p, a, st);
     case 8: return launch_one<16, 32, 1, false, T, MODE>(p, a, st);
-    default: return launch_one<16, 8, 3, true, T, MODE>(p, a, st);
+    case 9: return launch_one<16, 8, 3, true, T, MODE>(p, a, st);
+    default: return launch_one<16, 8, 4, true, T, MODE>(p, a, st);
   }
 }
 

@@ -176,7 +176,7 @@ def test_launch_variants_agree(oracle_mod):
     ref = fref = None
     from femorax_b200 import _lib as L
     lib = L.lib()
-    for variant in range(10):
+    for variant in range(11):
         for kz in (1, 3, 8, 64, -3, -8):
             L.check(lib.fx_force_set_launch(force._h, variant, kz))
             y = torch.zeros(mesh.num_equations, dtype=torch.float64, device=DEV)
