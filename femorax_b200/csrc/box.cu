@@ -467,8 +467,14 @@ void box_autotune(ForceState& s, cudaStream_t st) {
   FX_CUDA(cudaEventCreate(&e0));
   FX_CUDA(cudaEventCreate(&e1));
   // plane counts: fewer planes add redundant bottom planes (1 in kz + 1), more planes leave fewer
-  // tiles to balance over the SMs; the best depends on the grid
-  const int kzs[] = {5, 6, 7, 8, 10, 12, 16, 32, 64};
+  // tiles to balance over the SMs; the best depends on the grid. Besides a fixed ladder, the counts
+  // that split the grid's nz + 1 node planes evenly into 2 to 12 tiles (no short last tile).
+  std::vector<int> kzs = {5, 6, 7, 8, 10, 12, 16, 32, 64};
+  for (int t = 2; t <= 12; ++t) {
+    const int kz = (s.box.nz + 1 + t - 1) / t;
+    if (kz >= 5 && std::find(kzs.begin(), kzs.end(), kz) == kzs.end()) kzs.push_back(kz);
+  }
+  std::sort(kzs.begin(), kzs.end());
   // the internal force (ExplicitDifference steps, Newton residuals) stages u and v: its own shape
   for (int job = 0; job < 4; ++job) {
     const int prec = job & 1, mode = job >> 1;
