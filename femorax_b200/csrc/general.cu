@@ -392,7 +392,7 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
   FX_LAUNCH_CHECK("element_force");
   const int64_t points = static_cast<int64_t>(8) * s.P;
   if (s.has_pimy && s.count > 0) {
-    k_soil_points<PimySet, 2, pimy::kTan, 3><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+    k_soil_points<PimySet, 2, pimy::kTan, 6><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.N, s.P, s.count, u,
         s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
     FX_LAUNCH_CHECK("pimy_points");
@@ -402,7 +402,7 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
     FX_LAUNCH_CHECK("pimy_force");
   }
   if (s.has_pdmy && s.count > 0) {
-    k_soil_points<PdmySet, 3, pdmy::kTan, 2><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+    k_soil_points<PdmySet, 3, pdmy::kTan, 4><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pdmy_dev.ptr, s.N, s.P, s.count, u,
         s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_tan.ptr, s.pdmy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
     FX_LAUNCH_CHECK("pdmy_points");
