@@ -39,7 +39,7 @@ __global__ void k_pdmy_init(const pdmy::Params* __restrict__ p, int64_t n, doubl
   pdmy::initial_state(*p, pimy::Slab<double>{s + i, n});
 }
 
-__global__ void __launch_bounds__(128) k_pdmy_update(const pdmy::Params* __restrict__ pp, int stage, int64_t n,
+__global__ void __launch_bounds__(128, 4) k_pdmy_update(const pdmy::Params* __restrict__ pp, int stage, int64_t n,
                                                      const double* __restrict__ committed, double* __restrict__ trial,
                                                      const double* __restrict__ eps, double* __restrict__ sig,
                                                      double* __restrict__ D, int* __restrict__ failed) {

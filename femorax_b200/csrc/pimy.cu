@@ -44,7 +44,7 @@ __global__ void k_pimy_init(const pimy::Params* __restrict__ p, int64_t n, doubl
 
 // Point i: strain eps[c n + i], stress sig[c n + i], tangent D[(6 r + c) n + i] (NULL: not stored),
 // failures counted in *failed (NULL: not counted).
-__global__ void __launch_bounds__(128) k_pimy_update(const pimy::Params* __restrict__ pp, int stage, int64_t n,
+__global__ void __launch_bounds__(128, 6) k_pimy_update(const pimy::Params* __restrict__ pp, int stage, int64_t n,
                                                      const double* __restrict__ committed, double* __restrict__ trial,
                                                      const double* __restrict__ eps, double* __restrict__ sig,
                                                      double* __restrict__ D, int* __restrict__ failed) {
