@@ -18,7 +18,9 @@ same alone and in any mix (tests/test_gpu_batch.py checks it).
 J2 load paths run in cohorts: when the J2 lane is idle, the prepared J2 requests waiting (in
 arrival order, up to `max_cohort`, the same load path) become one BatchedNewton (one combined
 mesh, per-instance Newton and CG on the device), which advances one load step per pass of the
-loop, between the engine's rounds, and retires all its requests at the end of the path. Each
+loop, between the engine's rounds, and retires all its requests at the end of the path. A cohort
+takes no members once it runs, so while the engine is busy an idle lane waits (at most
+`cohort_window` seconds) for the requests queued behind a prepared head to be prepared too. Each
 instance's arithmetic is that of the load path alone, bit for bit (tests/test_gpu_serving.py).
 
 `serve_one_at_a_time` is the comparison: the same stream, first come first served, each request
@@ -27,6 +29,7 @@ solved alone by the plain FP64 path (Jacobi-PCG; for J2, Newton with Jacobi-PCG 
 from __future__ import annotations
 
 import collections
+import itertools
 import concurrent.futures as cf
 import dataclasses
 import math
@@ -274,7 +277,7 @@ class Server:
     paths, in cohorts of up to max_cohort)."""
 
     def __init__(self, engine: BatchEngine, hbm_budget: int, device: int = 0, prep_threads: int = 4,
-                 prepare_fn=None, lane=None, max_cohort: int = 32):
+                 prepare_fn=None, lane=None, max_cohort: int = 32, cohort_window: float = 0.25):
         self.engine = engine
         self.budget = int(hbm_budget)
         self.device = device
@@ -282,6 +285,9 @@ class Server:
         self.prepare = prepare_fn or prepare_any
         self.lane = lane if lane is not None else J2Lane(device)
         self.max_cohort = max_cohort
+        # a running cohort takes no new members, so an idle lane waits up to this many seconds for
+        # the J2 requests queued behind a prepared head (same load path) while the engine is busy
+        self.cohort_window = float(cohort_window)
         self.resident = 0  # footprint of the admitted requests
 
     def _start_cohort(self, pending_j2, slots, t0):
@@ -317,6 +323,7 @@ class Server:
         slots = {}                        # slot -> (request, footprint, admitted time)
         served = []
         nxt = 0
+        head_ready = None  # when the J2 queue's head was first seen prepared with the lane idle
         try:
             while nxt < len(reqs) or pending or pending_j2 or slots or not self.lane.idle:
                 # arrivals
@@ -341,9 +348,19 @@ class Server:
                     slots[slot] = (req, foot, time.perf_counter() - t0)
                 if not slots and self.lane.idle and pending and pending[0][1].done():
                     raise RuntimeError(f"request {pending[0][0].id} does not fit the engine even alone")
-                # a new J2 cohort when the lane is free
+                # a new J2 cohort when the lane is free: when the requests queued behind a prepared
+                # head with its load path are all prepared too, when the engine runs nothing (the
+                # GPU would wait), or when the head has waited cohort_window seconds
                 if self.lane.idle and pending_j2 and pending_j2[0][1].done():
-                    self._start_cohort(pending_j2, slots, t0)
+                    if head_ready is None:
+                        head_ready = time.perf_counter()
+                    path = pending_j2[0][0].path
+                    queued = list(itertools.islice(itertools.takewhile(lambda q: q[0].path == path, pending_j2),
+                                                   self.max_cohort))
+                    if (all(f.done() for _, f in queued) or not slots
+                            or time.perf_counter() - head_ready >= self.cohort_window):
+                        self._start_cohort(pending_j2, slots, t0)
+                        head_ready = None
                 if not slots and self.lane.idle:
                     # nothing on the GPU: wait for the next preparation or arrival
                     heads = [q[0][1] for q in (pending, pending_j2) if q]
