@@ -48,6 +48,7 @@ int64_t ForceState::device_bytes() const {
   b += geom32.bytes() + nshape32.bytes() + slots32.bytes();
   b += pimy_dev.bytes() + pimy_committed.bytes() + pimy_trial.bytes() + pimy_tan.bytes() + pimy_failed.bytes() + pimy_sig.bytes();
   b += pdmy_dev.bytes() + pdmy_committed.bytes() + pdmy_trial.bytes() + pdmy_tan.bytes() + pdmy_sig.bytes();
+  b += soil_sd.bytes();
   return b;
 }
 

@@ -200,6 +200,9 @@ struct ForceState {
   DeviceArray<PdmySet> pdmy_dev;
   DeviceArray<double> pdmy_committed, pdmy_trial, pdmy_tan, pdmy_sig;
   int pdmy_nstate = 0;
+  // the soil points' stiffness-proportional damping stresses (sets with betaK), [(c * 8 + gp) * P + e];
+  // unallocated (NULL) when no soil set is damped
+  DeviceArray<double> soil_sd;
   ExplicitWork xw;
   bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
   bool use_box_force() const { return use_box() && box.force_ok; }

@@ -115,6 +115,8 @@ FX_HD bool soil_point_update(const PdmySet& m, const double xl[3][8], const doub
                              double* t, int64_t stride, double* sg, double* tc, bool* pl) {
   return point_update_pdmy(m, xl, ue, gp, c, t, stride, sg, tc, pl);
 }
+FX_HD void soil_compact_D(const PimySet&, const double* t, double* D) { pimy::compact_D(t, D); }
+FX_HD void soil_compact_D(const PdmySet& m, const double* t, double* D) { pdmy::compact_D(m.p, t, D); }
 template <class Set, int KIND, int KTAN, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restrict__ coords, const int32_t* __restrict__ node,
                                                      const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
@@ -122,7 +124,8 @@ __global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restr
                                                      int32_t N, int32_t P, int32_t count, const double* __restrict__ u,
                                                      const double* __restrict__ pc, double* __restrict__ pt,
                                                      double* __restrict__ ptan, double* __restrict__ psig,
-                                                     int* __restrict__ plastic, int* __restrict__ failed) {
+                                                     int* __restrict__ plastic, int* __restrict__ failed,
+                                                     const double* __restrict__ v, double* __restrict__ psd) {
   const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   const int32_t e = static_cast<int32_t>(t % P), gp = static_cast<int32_t>(t / P);
   bool pl = false, bad = false;
@@ -138,6 +141,16 @@ __global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restr
       bad = !soil_point_update(sets[p.table], xl, ue, gp, pc + e, pt + e, P, sg, tc, &pl);
       for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
       for (int c = 0; c < KTAN; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
+      if (psd && p.betaK != 0.0) {  // the damping stress of this update's tangent
+        double D[36], ve[24], sd[6];
+        soil_compact_D(sets[p.table], tc, D);
+        for (int a = 0; a < 24; ++a) {
+          const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+          ve[a] = q >= 0 ? v[q] : 0.0;
+        }
+        damping_stress(D, p.betaK, xl, ve, gp, sd);
+        for (int c = 0; c < 6; ++c) psd[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sd[c];
+      }
     }
   }
   const unsigned np = __popc(__ballot_sync(0xffffffffu, pl)), nb = __popc(__ballot_sync(0xffffffffu, bad));
@@ -152,7 +165,8 @@ __global__ void __launch_bounds__(kBlock) k_soil_force(const double* __restrict_
                                                         const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
                                                         const ParamGP* __restrict__ params, int32_t N, int32_t P,
                                                         int32_t count, const double* __restrict__ v,
-                                                        const double* __restrict__ psig, double* __restrict__ slots,
+                                                        const double* __restrict__ psig,
+                                                        const double* __restrict__ psd, double* __restrict__ slots,
                                                         int kind) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
@@ -164,7 +178,8 @@ __global__ void __launch_bounds__(kBlock) k_soil_force(const double* __restrict_
     const int32_t q = eq[static_cast<int64_t>(a) * P + e];
     ve[a] = q >= 0 ? v[q] : 0.0;
   }
-  element_force_from_stress(p, xl, ve, psig + e, P, fe);
+  const bool damped = psd && (p.betaK != 0.0 || p.betaKinit != 0.0 || p.betaKcomm != 0.0);
+  element_force_from_stress(p, xl, ve, psig + e, damped ? psd + e : nullptr, P, fe);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = fe[a];
 }
 
@@ -394,21 +409,23 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
   if (s.has_pimy && s.count > 0) {
     k_soil_points<PimySet, 2, pimy::kTan, 6><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.N, s.P, s.count, u,
-        s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
+        s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr,
+        v, s.soil_sd.ptr);
     FX_LAUNCH_CHECK("pimy_points");
     k_soil_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                s.params.ptr, s.N, s.P, s.count, v, s.pimy_sig.ptr,
-                                                               s.slots.ptr, 2);
+                                                               s.soil_sd.ptr, s.slots.ptr, 2);
     FX_LAUNCH_CHECK("pimy_force");
   }
   if (s.has_pdmy && s.count > 0) {
     k_soil_points<PdmySet, 3, pdmy::kTan, 4><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pdmy_dev.ptr, s.N, s.P, s.count, u,
-        s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_tan.ptr, s.pdmy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr);
+        s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_tan.ptr, s.pdmy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr,
+        v, s.soil_sd.ptr);
     FX_LAUNCH_CHECK("pdmy_points");
     k_soil_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                s.params.ptr, s.N, s.P, s.count, v, s.pdmy_sig.ptr,
-                                                               s.slots.ptr, 3);
+                                                               s.soil_sd.ptr, s.slots.ptr, 3);
     FX_LAUNCH_CHECK("pdmy_force");
   }
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;

@@ -49,11 +49,31 @@ FX_HD bool point_update_pdmy(const PdmySet& m, const double xl[3][8], const doub
                               pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, plastic);
 }
 
+// Stiffness-proportional damping stress of a point (the reference's point_update_shape with betaK
+// only): sd[a] = sum_c (betaK D[a][c]) rate[c], D the point's tangent of this update (as the material
+// returned it, before any mirroring), rate the strain of the element velocities at the point.
+FX_HD void damping_stress(const double* D, double betaK, const double xl[3][8], const double* ve, int gp,
+                          double sd[6]) {
+  PointShape s;
+  point_shape(xl, gp, s);
+  double rate[6];
+  strain_of(s, ve, rate);
+  for (int a = 0; a < 6; ++a) {
+    double sum = 0.0;
+    for (int c = 0; c < 6; ++c) {
+      const double Dac = betaK * D[6 * a + c];
+      sum += Dac * rate[c];
+    }
+    sd[a] = sum;
+  }
+}
+
 // Internal force of one element from its points' stresses (point gp's component c at
-// sig[(c * 8 + gp) * stride]), in OpenSees' order: per point resid += B^T sigma dvol, resid -= body,
-// fdamp += alphaM M v; fe = resid + fdamp. No stiffness-proportional damping (refused for these sets).
+// sig[(c * 8 + gp) * stride]) and damping stresses (sdamp, likewise, or NULL), in OpenSees' order:
+// per point resid += B^T sigma dvol, resid -= body, fdamp += B^T sigma_d dvol + alphaM M v;
+// fe = resid + fdamp.
 FX_HD void element_force_from_stress(const ParamGP& p, const double xl[3][8], const double* ve, const double* sig,
-                                     int64_t stride, double* fe) {
+                                     const double* sdamp, int64_t stride, double* fe) {
   double resid[24], fdamp[24];
   for (int a = 0; a < 24; ++a) resid[a] = fdamp[a] = 0.0;
   for (int gp = 0; gp < 8; gp++) {
@@ -65,11 +85,15 @@ FX_HD void element_force_from_stress(const ParamGP& p, const double xl[3][8], co
     if (p.alphaM != 0.0 && p.mass_type == 0)
       for (int j = 0; j < 8; j++)
         for (int q = 0; q < 3; q++) vg[q] += s.N[j] * ve[3 * j + q];
+    double sd[6];
+    if (sdamp)
+      for (int c = 0; c < 6; ++c) sd[c] = sdamp[(c * 8 + gp) * stride];
     for (int j = 0; j < 8; j++) {
       double r[3], body[3], dj[3];
       node_force(s, sg, j, r);
       for (int q = 0; q < 3; q++) body[q] = s.dvol * p.b[q] * s.N[j];
       dj[0] = dj[1] = dj[2] = 0.0;
+      if (sdamp) node_force(s, sd, j, dj);
       if (p.alphaM != 0.0) {
         const double tm = s.N[j] * s.dvol * p.rho;
         for (int q = 0; q < 3; q++) {

@@ -469,8 +469,9 @@ int fx_pimy_update(fx_pimy* m, int32_t stage, int64_t npoints, const double* com
  * points: the reference's StdBrick<PressureIndependMultiYield<NS>>, std_brick.hpp:398-540, a
  * model material of that type). The set's elements run on the Gauss-point path (the box path is
  * taken out for the mesh); their points start from the material's state, elastic stage. The set's
- * density must equal the material's (the masses come from the set); stiffness-proportional Rayleigh
- * damping on the set is FX_E_UNSUPPORTED. Bind before creating solvers or running stages on the
+ * density must equal the material's (the masses come from the set); betaK Rayleigh damping acts
+ * through each point's current tangent (the reference's damping stress); betaKinit and betaKcomm on
+ * the set are FX_E_UNSUPPORTED. Bind before creating solvers or running stages on the
  * mesh. fx_force_compute then updates every point (the trial state; fx_force_commit commits it),
  * the operator and its diagonal use each point's tangent of the last fx_force_compute (the
  * reference's stored tangents at that displacement; `initial` in fx_coeffs: the material's
@@ -512,7 +513,7 @@ int fx_pdmy_update(fx_pdmy* m, int32_t stage, int64_t npoints, const double* com
                    const double* strain, double* stress, double* tangent, int32_t* failed, void* stream);
 /* Binds material m to parameter set `set` of a mesh, as fx_force_set_pimy (the reference's
  * StdBrick<PressureDependMultiYield<NS>>): Gauss-point path, elastic stage at first, the set's
- * density equal to the material's, no stiffness-proportional damping; fx_force_set_material_stage,
+ * density equal to the material's, betaK damping only; fx_force_set_material_stage,
  * fx_force_compute / commit, the operator (each point's stored tangent of the last compute, upper
  * triangle mirrored) and fx_force_pimy_failed work on it as on PressureIndependMultiYield sets. */
 int fx_force_set_pdmy(fx_force* f, int32_t set, const fx_pdmy* m);

@@ -24,11 +24,13 @@ LIQ = (1.9469928644240571, 75000.0, 162499.99999999997, 29.0, 0.1, 80.0, 0.5, 29
        1.0, 20.0, 0.85, 0.9, 0.02, 0.7, 101.0, 0.3, 0.0, 1.0)
 
 
-def column(p):
+def column(p, damped=False):
     G, K = p[1], p[2]
     E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
     spec = meshes.box_model(2, 2, 5, size=(1.0, 1.0, 2.5), E=E, nu=nu, rho=p[0])
     spec.groups[0].pdmy = (np.array(p), None)
+    if damped:  # Rayleigh damping, betaK through each point's current tangent
+        spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.0, spec.groups[0].etags)]
     return spec
 
 
@@ -36,11 +38,12 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.mark.parametrize("p", [SAND, LIQ], ids=["dense_sand", "loose_sand_ppz"])
-def test_column_path_matches_reference(p, oracle_mod, ref_available):
+@pytest.mark.parametrize("p,damped", [(SAND, False), (LIQ, False), (SAND, True)],
+                         ids=["dense_sand", "loose_sand_ppz", "dense_sand_damped"])
+def test_column_path_matches_reference(p, damped, oracle_mod, ref_available):
     if not ref_available:
         pytest.skip("the reference build is not available")
-    spec = column(p)
+    spec = column(p, damped)
     mesh = fx.Model(spec).compile().mesh()
     force = fx.InternalForce(mesh)
     force.set_pdmy(0, fx.PressureDependMultiYield(*p[:14], noYieldSurf=int(p[14]), e=p[15], cs1=p[16], cs2=p[17],
@@ -58,7 +61,7 @@ def test_column_path_matches_reference(p, oracle_mod, ref_available):
             dof[q[ok]] = d
     rng = np.random.default_rng(22)
     noise = rng.standard_normal(n) * 2e-6
-    k = (1.0, 0.0, 0.5)
+    k = (1.0, 0.3, 0.5) if damped else (1.0, 0.0, 0.5)
     plastic_seen = 0
     for step in range(14):
         if step == 3:
@@ -67,7 +70,7 @@ def test_column_path_matches_reference(p, oracle_mod, ref_available):
         ev = 2e-4 * min(step + 1, 3) / 3
         gam = 0.0 if step < 3 else 1e-3 * np.sin(2 * np.pi * (step - 3) / 8)
         u = np.where(dof == 2, -ev * zq, 0.0) + np.where(dof == 0, gam * zq, 0.0) + noise * (step >= 3)
-        v = np.zeros(n)
+        v = rng.standard_normal(n) * 1e-3 if damped else np.zeros(n)
         f = torch.zeros(n, dtype=torch.float64, device=DEV)
         force.compute(torch.as_tensor(u, device=DEV), torch.as_tensor(v, device=DEV), f)
         assert rel(f.cpu().numpy(), ref.force(u, v)) <= 1e-10, step

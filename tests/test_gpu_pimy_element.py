@@ -4,7 +4,8 @@ confinement in the elastic stage, the switch to the plastic stage (updateMateria
 shear with commits. At every step the internal force, the operator y = K_t x + c M x with every
 point's tangent at that displacement (the reference's TangentSource::Recomputed) and its diagonal
 agree within 1e-12 of their largest entries, and bit for bit for the materials whose update calls
-no pow (friction angle 0); the plastic stage yields points."""
+no pow (friction angle 0); the plastic stage yields points. One case carries Rayleigh damping
+(alphaM, and betaK through each point's current tangent)."""
 import numpy as np
 import pytest
 
@@ -20,6 +21,7 @@ DEV = torch.device("cuda:0")
 BACKBONE = [1e-05, 0.98, 3e-05, 0.95, 0.0001, 0.85, 0.0003, 0.65, 0.001, 0.35, 0.003, 0.15, 0.01, 0.05, 0.03, 0.018]
 MATERIALS = {
     "clay": ((1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0), None),
+    "clay_damped": ((1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0), None),
     "sand": ((2.0, 60000.0, 150000.0, 5.0, 0.1, 30.0, 80.0, 0.5, 20.0), None),
     "backbone_clay": ((1.8, 40500.0, 108000.0, 10.0, 0.1, 0.0, 100.0, 0.0, 8.0), BACKBONE),
 }
@@ -31,6 +33,8 @@ def column(name):
     E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
     spec = meshes.box_model(2, 2, 5, size=(1.0, 1.0, 2.5), E=E, nu=nu, rho=in9[0])
     spec.groups[0].pimy = (np.array(in9), None if pairs is None else np.array(pairs))
+    if name.endswith("_damped"):  # stiffness-proportional Rayleigh damping through the current tangent
+        spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.0, spec.groups[0].etags)]
     return spec
 
 
@@ -67,7 +71,8 @@ def test_column_path_matches_reference(name, oracle_mod, ref_available):
             dof[q[ok]] = d
     rng = np.random.default_rng(21)
     noise = rng.standard_normal(n) * 2e-5
-    k = (1.0, 0.0, 0.5)
+    damped = name.endswith("_damped")
+    k = (1.0, 0.3, 0.5) if damped else (1.0, 0.0, 0.5)
     bitwise = in9[5] == 0.0
     plastic_seen = 0
     for step in range(16):
@@ -78,7 +83,7 @@ def test_column_path_matches_reference(name, oracle_mod, ref_available):
         ev = 1e-3 * min(step + 1, 3) / 3
         gam = 0.0 if step < 3 else 8e-3 * np.sin(2 * np.pi * (step - 3) / 8)
         u = np.where(dof == 2, -ev * zq, 0.0) + np.where(dof == 0, gam * zq, 0.0) + noise * (step >= 3)
-        v = np.zeros(n)
+        v = rng.standard_normal(n) * 1e-2 if damped else np.zeros(n)
         f = torch.zeros(n, dtype=torch.float64, device=DEV)
         force.compute(torch.as_tensor(u, device=DEV), torch.as_tensor(v, device=DEV), f)
         fr = ref.force(u, v)
