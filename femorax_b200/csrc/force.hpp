@@ -200,7 +200,8 @@ struct ForceState {
   DeviceArray<PdmySet> pdmy_dev;
   DeviceArray<double> pdmy_committed, pdmy_trial, pdmy_tan, pdmy_sig;
   int pdmy_nstate = 0;
-  // the soil points' stiffness-proportional damping stresses (sets with betaK), [(c * 8 + gp) * P + e];
+  // the soil points' stiffness-proportional damping stresses (sets with betaK or betaKcomm),
+  // [(c * 8 + gp) * P + e];
   // unallocated (NULL) when no soil set is damped
   DeviceArray<double> soil_sd;
   ExplicitWork xw;

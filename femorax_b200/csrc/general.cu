@@ -31,7 +31,9 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
                                                            int initial, const PimySet* __restrict__ pimy,
                                                            const double* __restrict__ ptan,
                                                            const PdmySet* __restrict__ pdmy,
-                                                           const double* __restrict__ dtan) {
+                                                           const double* __restrict__ dtan,
+                                                           const double* __restrict__ pcs,
+                                                           const double* __restrict__ dcs) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count || (skip && *skip)) return;
   const ParamGP p = params[param[e]];
@@ -44,8 +46,8 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
   }
   const OpFactors f = op_factors(p, ks, kd, km);
   if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
-  else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, P, f.cK, initial != 0});
-  else if (p.kind == 3) element_apply_d(p, f, xl, xe, ye, PdmyPointD{pdmy + p.table, dtan + e, P, f.cK, initial != 0});
+  else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc, initial != 0});
+  else if (p.kind == 3) element_apply_d(p, f, xl, xe, ye, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.cc, initial != 0});
   else element_apply(p, f, xl, xe, ye);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
 }
@@ -58,7 +60,9 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
                                                           int initial, const PimySet* __restrict__ pimy,
                                                           const double* __restrict__ ptan,
                                                           const PdmySet* __restrict__ pdmy,
-                                                          const double* __restrict__ dtan) {
+                                                          const double* __restrict__ dtan,
+                                                          const double* __restrict__ pcs,
+                                                          const double* __restrict__ dcs) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -69,9 +73,9 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
   const OpFactors f = op_factors(p, ks, kd, km);
   if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
   else if (p.kind == 2)
-    element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, P, f.cK, initial != 0});
+    element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc, initial != 0});
   else if (p.kind == 3)
-    element_diagonal_d(p, f, xl, eqe, de, PdmyPointD{pdmy + p.table, dtan + e, P, f.cK, initial != 0});
+    element_diagonal_d(p, f, xl, eqe, de, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.cc, initial != 0});
   else element_diagonal(p, f, xl, eqe, de);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = de[a];
 }
@@ -141,14 +145,15 @@ __global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restr
       bad = !soil_point_update(sets[p.table], xl, ue, gp, pc + e, pt + e, P, sg, tc, &pl);
       for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
       for (int c = 0; c < KTAN; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
-      if (psd && p.betaK != 0.0) {  // the damping stress of this update's tangent
-        double D[36], ve[24], sd[6];
+      if (psd && (p.betaK != 0.0 || p.betaKcomm != 0.0)) {  // the damping stress: this update's tangent
+        double D[36], Dc[36], ve[24], sd[6];                 // and the committed one
         soil_compact_D(sets[p.table], tc, D);
+        if (p.betaKcomm != 0.0) committed_D(sets[p.table], pc + e, gp, P, Dc);
         for (int a = 0; a < 24; ++a) {
           const int32_t q = eq[static_cast<int64_t>(a) * P + e];
           ve[a] = q >= 0 ? v[q] : 0.0;
         }
-        damping_stress(D, p.betaK, xl, ve, gp, sd);
+        damping_stress(D, p.betaK, Dc, p.betaKcomm, xl, ve, gp, sd);
         for (int c = 0; c < 6; ++c) psd[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sd[c];
       }
     }
@@ -371,7 +376,8 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
                                                                    s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
                                                                    -1, x, s.slots.ptr, skip, s.j2_tan.ptr, s.initial,
                                                                    s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
-                                                                   s.pdmy_tan.ptr);
+                                                                   s.pdmy_tan.ptr, s.pimy_committed.ptr,
+                                                                   s.pdmy_committed.ptr);
   FX_LAUNCH_CHECK("element_apply");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -387,7 +393,8 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
                                                                   s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
                                                                   s.slots.ptr, s.j2_tan.ptr, s.initial,
                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
-                                                                  s.pdmy_tan.ptr);
+                                                                  s.pdmy_tan.ptr, s.pimy_committed.ptr,
+                                                                  s.pdmy_committed.ptr);
   FX_LAUNCH_CHECK("element_diagonal");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -461,7 +468,8 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
                                                                    s.params.ptr, s.N, s.P, s.count, 0.0, 0.0, 1.0, dir,
                                                                    nullptr, s.slots.ptr, nullptr, s.j2_tan.ptr, 0,
                                                                    s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
-                                                                   s.pdmy_tan.ptr);
+                                                                   s.pdmy_tan.ptr, s.pimy_committed.ptr,
+                                                                   s.pdmy_committed.ptr);
   FX_LAUNCH_CHECK("element_apply_unit");
   if (s.neq > 0)
     k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,

@@ -158,9 +158,10 @@ int fx_force_set_pdmy(fx_force* f, int32_t set, const fx_pdmy* m) {
     if (set < 0 || set >= s.nparams) throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: no such parameter set");
     fx::ParamGP& q = s.params_h[set];
     if (q.kind == FX_MAT_J2 || q.kind == 2) throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: the set has another material");
-    if (q.betaKinit != 0.0 || q.betaKcomm != 0.0)
-      throw fx::Error(FX_E_UNSUPPORTED, "betaKinit or betaKcomm Rayleigh damping on a PressureDependMultiYield set");
-    if (q.betaK != 0.0 && !s.soil_sd.ptr) s.soil_sd.alloc(static_cast<size_t>(6) * 8 * s.P);
+    if (q.betaKinit != 0.0)
+      throw fx::Error(FX_E_UNSUPPORTED, "betaKinit Rayleigh damping on a PressureDependMultiYield set");
+    if ((q.betaK != 0.0 || q.betaKcomm != 0.0) && !s.soil_sd.ptr)
+      s.soil_sd.alloc(static_cast<size_t>(6) * 8 * s.P);
     if (q.rho != m->p.rho)
       throw fx::Error(FX_E_INVALID, "fx_force_set_pdmy: the set's density (its masses) differs from the material's");
     const int need = fx::pdmy::nstate(m->p.ns);

@@ -861,5 +861,25 @@ FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, co
   return pt.ok;
 }
 
+// The tangent at the committed state in compact form t[kTan] (betaKcomm damping; the reference's
+// PressureDependMultiYield::committed_tangent, src/physics/materials/
+// pressure_depend_multi_yield.hpp:186-200): the reference elastic tangent in the elastic stage or
+// before the switch to plastic; otherwise getTangent after commitState, the trial stress and the
+// surface centers the committed ones and no strain rate (so no volumetric softening).
+template <class CV>
+FX_PIMY_HD inline void committed_compact(const Params& p, int stage, CV C, double* t) {
+  if (stage != 1 || C[S_E2P] == 0.0) {
+    t[0] = 0.;
+    for (int k = 1; k < kTan; ++k) t[k] = 0.;
+    return;
+  }
+  Point<CV, CV> pt(p, stage, C, C);  // the centers read from C
+  pt.load();
+  pt.trial = pt.cur;
+  double z[6] = {0., 0., 0., 0., 0., 0.};
+  pt.rate.from_full(z, true);
+  pt.compact(t);
+}
+
 }  // namespace pdmy
 }  // namespace fx

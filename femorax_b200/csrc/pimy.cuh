@@ -747,5 +747,20 @@ FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, co
   return pt.ok;
 }
 
+// The tangent at the committed state in compact form t[kTan] (betaKcomm damping; the reference's
+// PressureIndependMultiYield::committed_tangent, src/physics/materials/
+// pressure_independ_multi_yield.hpp:160-168): getTangent after commitState, the trial stress,
+// active surface, moduli and surfaces all the committed ones. C holds every surface.
+template <class CV>
+FX_PIMY_HD inline void committed_compact(const Params& p, int stage, CV C, double* t) {
+  Point<CV, CV> pt(p, stage, C, C);
+  pt.cur.load(C, S_STRESS);
+  pt.trial = pt.cur;
+  pt.active = static_cast<int>(C[S_ACTIVE]);
+  pt.G = C[S_G];
+  pt.K = C[S_K];
+  pt.compact(t);
+}
+
 }  // namespace pimy
 }  // namespace fx

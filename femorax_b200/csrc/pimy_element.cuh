@@ -49,11 +49,26 @@ FX_HD bool point_update_pdmy(const PdmySet& m, const double xl[3][8], const doub
                               pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, plastic);
 }
 
-// Stiffness-proportional damping stress of a point (the reference's point_update_shape with betaK
-// only): sd[a] = sum_c (betaK D[a][c]) rate[c], D the point's tangent of this update (as the material
-// returned it, before any mirroring), rate the strain of the element velocities at the point.
-FX_HD void damping_stress(const double* D, double betaK, const double xl[3][8], const double* ve, int gp,
-                          double sd[6]) {
+// The tangent at the committed state of point gp (betaKcomm damping), D[6 i + j] as the material
+// returns it (the reference's Mat::committed_tangent; not mirrored).
+FX_HD void committed_D(const PimySet& m, const double* committed, int gp, int64_t stride, double* D) {
+  double t[pimy::kTan];
+  pimy::committed_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride}, t);
+  pimy::compact_D(t, D);
+}
+FX_HD void committed_D(const PdmySet& m, const double* committed, int gp, int64_t stride, double* D) {
+  double t[pdmy::kTan];
+  pdmy::committed_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride}, t);
+  pdmy::compact_D(m.p, t, D);
+}
+
+// Stiffness-proportional damping stress of a point (the reference's point_update_shape,
+// src/physics/elements/std_brick.hpp:419-434, without betaKinit): sd[a] = sum_c (betaK D[a][c] +
+// betaKcomm Dc[a][c]) rate[c], D the point's tangent of this update (as the material returned it,
+// before any mirroring), Dc its committed tangent (read only when betaKcomm is not zero), rate the
+// strain of the element velocities at the point.
+FX_HD void damping_stress(const double* D, double betaK, const double* Dc, double betaKcomm, const double xl[3][8],
+                          const double* ve, int gp, double sd[6]) {
   PointShape s;
   point_shape(xl, gp, s);
   double rate[6];
@@ -61,7 +76,8 @@ FX_HD void damping_stress(const double* D, double betaK, const double xl[3][8], 
   for (int a = 0; a < 6; ++a) {
     double sum = 0.0;
     for (int c = 0; c < 6; ++c) {
-      const double Dac = betaK * D[6 * a + c];
+      double Dac = betaK * D[6 * a + c];
+      if (betaKcomm != 0.0) Dac += betaKcomm * Dc[6 * a + c];
       sum += Dac * rate[c];
     }
     sd[a] = sum;
@@ -111,16 +127,19 @@ FX_HD void element_force_from_stress(const ParamGP& p, const double xl[3][8], co
   for (int a = 0; a < 24; ++a) fe[a] = resid[a] + fdamp[a];
 }
 
-// The material matrix of point gp for the operator: the stored tangent of the last force
-// evaluation scaled by the stiffness factor, or (ModifiedNewton -initial) the material's initial
-// tangent, the reference elastic one (the reference's PressureIndependMultiYield::initial_tangent).
+// The material matrix of point gp for the operator (the reference's effective_tangent,
+// src/physics/operators/element_operator.hpp:58-75, without betaKinit): the stored tangent of the
+// last force evaluation, or (ModifiedNewton -initial) the material's initial tangent, the reference
+// elastic one (the reference's PressureIndependMultiYield::initial_tangent), scaled by the stiffness
+// factor, plus cc times the tangent at the committed state (betaKcomm damping, not mirrored).
 // The material declares its tangent symmetric, so it is stored as its upper triangle and the lower
 // one mirrors it (the reference's TangentStorage, src/physics/common/tangent_storage.hpp:17-31).
 struct PimyPointD {
   const PimySet* m;
   const double* tan;
+  const double* committed;  // the committed states (read only when cc is not zero)
   int64_t stride;
-  double cK;
+  double cK, cc;
   bool initial;
   FX_HD void operator()(int gp, double De[6][6]) const {
     double D[36];
@@ -133,18 +152,26 @@ struct PimyPointD {
     }
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
+    double Dc[36];
+    if (cc != 0.0) committed_D(*m, committed, gp, stride, Dc);
     for (int a = 0; a < 6; ++a)
-      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+      for (int c = 0; c < 6; ++c) {
+        double v = cK * D[6 * a + c];
+        if (cc != 0.0) v += cc * Dc[6 * a + c];
+        De[a][c] = v;
+      }
   }
 };
 
 // The operator's material matrix of a PressureDependMultiYield point: its stored tangent (upper
-// triangle mirrored) scaled by the stiffness factor, or the reference elastic tangent (initial).
+// triangle mirrored) or the reference elastic tangent (initial), scaled by the stiffness factor,
+// plus cc times its committed tangent.
 struct PdmyPointD {
   const PdmySet* m;
   const double* tan;
+  const double* committed;  // the committed states (read only when cc is not zero)
   int64_t stride;
-  double cK;
+  double cK, cc;
   bool initial;
   FX_HD void operator()(int gp, double De[6][6]) const {
     double D[36];
@@ -157,8 +184,14 @@ struct PdmyPointD {
     }
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
+    double Dc[36];
+    if (cc != 0.0) committed_D(*m, committed, gp, stride, Dc);
     for (int a = 0; a < 6; ++a)
-      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+      for (int c = 0; c < 6; ++c) {
+        double v = cK * D[6 * a + c];
+        if (cc != 0.0) v += cc * Dc[6 * a + c];
+        De[a][c] = v;
+      }
   }
 };
 

@@ -469,9 +469,10 @@ int fx_pimy_update(fx_pimy* m, int32_t stage, int64_t npoints, const double* com
  * points: the reference's StdBrick<PressureIndependMultiYield<NS>>, std_brick.hpp:398-540, a
  * model material of that type). The set's elements run on the Gauss-point path (the box path is
  * taken out for the mesh); their points start from the material's state, elastic stage. The set's
- * density must equal the material's (the masses come from the set); betaK Rayleigh damping acts
- * through each point's current tangent (the reference's damping stress); betaKinit and betaKcomm on
- * the set are FX_E_UNSUPPORTED. Bind before creating solvers or running stages on the
+ * density must equal the material's (the masses come from the set); betaK and betaKcomm Rayleigh
+ * damping act through each point's current and committed tangents (the reference's damping stress,
+ * std_brick.hpp:419-434, and effective_tangent, element_operator.hpp:58-75); betaKinit on the set
+ * is FX_E_UNSUPPORTED (the reference refuses it too). Bind before creating solvers or running stages on the
  * mesh. fx_force_compute then updates every point (the trial state; fx_force_commit commits it),
  * the operator and its diagonal use each point's tangent of the last fx_force_compute (the
  * reference's stored tangents at that displacement; `initial` in fx_coeffs: the material's

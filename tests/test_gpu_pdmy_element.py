@@ -29,8 +29,8 @@ def column(p, damped=False):
     E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
     spec = meshes.box_model(2, 2, 5, size=(1.0, 1.0, 2.5), E=E, nu=nu, rho=p[0])
     spec.groups[0].pdmy = (np.array(p), None)
-    if damped:  # Rayleigh damping, betaK through each point's current tangent
-        spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.0, spec.groups[0].etags)]
+    if damped:  # Rayleigh damping, betaK through each point's current tangent, betaKcomm its committed one
+        spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.001, spec.groups[0].etags)]
     return spec
 
 

@@ -5,7 +5,7 @@ shear with commits. At every step the internal force, the operator y = K_t x + c
 point's tangent at that displacement (the reference's TangentSource::Recomputed) and its diagonal
 agree within 1e-12 of their largest entries, and bit for bit for the materials whose update calls
 no pow (friction angle 0); the plastic stage yields points. One case carries Rayleigh damping
-(alphaM, and betaK through each point's current tangent)."""
+(alphaM; betaK through each point's current tangent, betaKcomm through its committed one)."""
 import numpy as np
 import pytest
 
@@ -33,8 +33,8 @@ def column(name):
     E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
     spec = meshes.box_model(2, 2, 5, size=(1.0, 1.0, 2.5), E=E, nu=nu, rho=in9[0])
     spec.groups[0].pimy = (np.array(in9), None if pairs is None else np.array(pairs))
-    if name.endswith("_damped"):  # stiffness-proportional Rayleigh damping through the current tangent
-        spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.0, spec.groups[0].etags)]
+    if name.endswith("_damped"):  # stiffness-proportional damping, current and committed tangents
+        spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.001, spec.groups[0].etags)]
     return spec
 
 
@@ -128,6 +128,11 @@ def test_binding_rules():
     with pytest.raises(fx.FxError) as e:  # no FP32 form of these tangents
         force.apply_operator(fx.OperatorCoefficients(), x, y)
     assert e.value.code == 2
+    spec = column("clay")
+    spec.rayleigh = [meshes.Rayleigh(0.0, 0.0, 0.001, 0.0, spec.groups[0].etags)]
+    with pytest.raises(fx.FxError):  # betaKinit damping on the set (the reference refuses it too)
+        fx.InternalForce(fx.Model(spec).compile().mesh()).set_pimy(0, fx.PressureIndependMultiYield(*in9[:8],
+                                                                                                 noYieldSurf=20))
 
 
 def test_newton_load_path_on_clay_column():
