@@ -145,15 +145,16 @@ __global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restr
       bad = !soil_point_update(sets[p.table], xl, ue, gp, pc + e, pt + e, P, sg, tc, &pl);
       for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
       for (int c = 0; c < KTAN; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
-      if (psd && (p.betaK != 0.0 || p.betaKcomm != 0.0)) {  // the damping stress: this update's tangent
-        double D[36], Dc[36], ve[24], sd[6];                 // and the committed one
-        soil_compact_D(sets[p.table], tc, D);
-        if (p.betaKcomm != 0.0) committed_D(sets[p.table], pc + e, gp, P, Dc);
+      if (psd && (p.betaK != 0.0 || p.betaKcomm != 0.0)) {  // the damping stress: betaK times this
+        double D[36], ve[24], sd[6];                         // update's tangent + betaKcomm times the
+        soil_compact_D(sets[p.table], tc, D);                // committed one
+        for (int i = 0; i < 36; ++i) D[i] = p.betaK * D[i];
+        if (p.betaKcomm != 0.0) add_committed_D(sets[p.table], pc + e, gp, P, p.betaKcomm, D);
         for (int a = 0; a < 24; ++a) {
           const int32_t q = eq[static_cast<int64_t>(a) * P + e];
           ve[a] = q >= 0 ? v[q] : 0.0;
         }
-        damping_stress(D, p.betaK, Dc, p.betaKcomm, xl, ve, gp, sd);
+        damping_stress(D, xl, ve, gp, sd);
         for (int c = 0; c < 6; ++c) psd[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sd[c];
       }
     }

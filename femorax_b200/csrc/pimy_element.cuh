@@ -49,37 +49,44 @@ FX_HD bool point_update_pdmy(const PdmySet& m, const double xl[3][8], const doub
                               pimy::Slab<double>{trial + gp * stride, 8 * stride}, e, sg, t, plastic);
 }
 
-// The tangent at the committed state of point gp (betaKcomm damping), D[6 i + j] as the material
-// returns it (the reference's Mat::committed_tangent; not mirrored).
-FX_HD void committed_D(const PimySet& m, const double* committed, int gp, int64_t stride, double* D) {
-  double t[pimy::kTan];
+// Out of line on the device: only betaKcomm sets form the committed tangent, and inlined it would take
+// registers from the common path of the kernels that call it.
+#if defined(__CUDACC__)
+#define FX_HD_COLD inline __host__ __device__ __noinline__
+#else
+#define FX_HD_COLD inline
+#endif
+
+// M[6 i + j] += f Dc[6 i + j], Dc the tangent at the committed state of point gp (betaKcomm
+// damping) as the material returns it (the reference's Mat::committed_tangent; not mirrored).
+FX_HD_COLD void add_committed_D(const PimySet& m, const double* committed, int gp, int64_t stride, double f,
+                                double* M) {
+  double t[pimy::kTan], Dc[36];
   pimy::committed_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride}, t);
-  pimy::compact_D(t, D);
+  pimy::compact_D(t, Dc);
+  for (int i = 0; i < 36; ++i) M[i] += f * Dc[i];
 }
-FX_HD void committed_D(const PdmySet& m, const double* committed, int gp, int64_t stride, double* D) {
-  double t[pdmy::kTan];
+FX_HD_COLD void add_committed_D(const PdmySet& m, const double* committed, int gp, int64_t stride, double f,
+                                double* M) {
+  double t[pdmy::kTan], Dc[36];
   pdmy::committed_compact(m.p, m.stage, pimy::Slab<const double>{committed + gp * stride, 8 * stride}, t);
-  pdmy::compact_D(m.p, t, D);
+  pdmy::compact_D(m.p, t, Dc);
+  for (int i = 0; i < 36; ++i) M[i] += f * Dc[i];
 }
 
 // Stiffness-proportional damping stress of a point (the reference's point_update_shape,
-// src/physics/elements/std_brick.hpp:419-434, without betaKinit): sd[a] = sum_c (betaK D[a][c] +
-// betaKcomm Dc[a][c]) rate[c], D the point's tangent of this update (as the material returned it,
-// before any mirroring), Dc its committed tangent (read only when betaKcomm is not zero), rate the
-// strain of the element velocities at the point.
-FX_HD void damping_stress(const double* D, double betaK, const double* Dc, double betaKcomm, const double xl[3][8],
-                          const double* ve, int gp, double sd[6]) {
+// src/physics/elements/std_brick.hpp:419-434, without betaKinit): sd[a] = sum_c Dd[a][c] rate[c],
+// Dd = betaK D (+ betaKcomm Dc when betaKcomm is not zero: add_committed_D), D the point's tangent of
+// this update (as the material returned it, before any mirroring), Dc its committed tangent, rate
+// the strain of the element velocities at the point.
+FX_HD void damping_stress(const double* Dd, const double xl[3][8], const double* ve, int gp, double sd[6]) {
   PointShape s;
   point_shape(xl, gp, s);
   double rate[6];
   strain_of(s, ve, rate);
   for (int a = 0; a < 6; ++a) {
     double sum = 0.0;
-    for (int c = 0; c < 6; ++c) {
-      double Dac = betaK * D[6 * a + c];
-      if (betaKcomm != 0.0) Dac += betaKcomm * Dc[6 * a + c];
-      sum += Dac * rate[c];
-    }
+    for (int c = 0; c < 6; ++c) sum += Dd[6 * a + c] * rate[c];
     sd[a] = sum;
   }
 }
@@ -152,14 +159,9 @@ struct PimyPointD {
     }
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
-    double Dc[36];
-    if (cc != 0.0) committed_D(*m, committed, gp, stride, Dc);
     for (int a = 0; a < 6; ++a)
-      for (int c = 0; c < 6; ++c) {
-        double v = cK * D[6 * a + c];
-        if (cc != 0.0) v += cc * Dc[6 * a + c];
-        De[a][c] = v;
-      }
+      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+    if (cc != 0.0) add_committed_D(*m, committed, gp, stride, cc, &De[0][0]);
   }
 };
 
@@ -184,14 +186,9 @@ struct PdmyPointD {
     }
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
-    double Dc[36];
-    if (cc != 0.0) committed_D(*m, committed, gp, stride, Dc);
     for (int a = 0; a < 6; ++a)
-      for (int c = 0; c < 6; ++c) {
-        double v = cK * D[6 * a + c];
-        if (cc != 0.0) v += cc * Dc[6 * a + c];
-        De[a][c] = v;
-      }
+      for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+    if (cc != 0.0) add_committed_D(*m, committed, gp, stride, cc, &De[0][0]);
   }
 };
 
