@@ -132,24 +132,60 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def mesh_builders():
+    """The mesh generators (femorax_b200/meshes.py, plain numpy) loaded as a module of their own,
+    without importing the package: importing femorax_b200 loads its library, and the reference arm
+    maps no file of this library."""
+    name = "femorax_mesh_builders"
+    if name not in sys.modules:
+        import importlib.util
+        s = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "femorax_b200", "meshes.py"))
+        m = importlib.util.module_from_spec(s)
+        sys.modules[name] = m
+        s.loader.exec_module(m)
+    return sys.modules[name]
+
+
+def bench_spec():
+    return mesh_builders().layered_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], WORKLOAD["layers"],
+                                       seed=WORKLOAD["seed"])[0]
+
+
+def bench_config(neq, n_el, n_nodes, gpus):
+    """The workload's `config`, the same dict in both arms."""
+    return dict(WORKLOAD, neq=int(neq), elements=int(n_el), nodes=int(n_nodes), parallelism=f"replicas x{gpus}",
+                l2="GPU arm: L2 flushed by a 256 MB write between timed applies; host arm: a 1 GB working set "
+                   "(maps, geometry cache, slots), past every host cache")
+
+
 def build_mesh():
     import femorax_b200 as fx
-    from femorax_b200 import meshes
-    spec, _ = meshes.layered_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], WORKLOAD["layers"], seed=WORKLOAD["seed"])
+    spec = bench_spec()
     return spec, fx.Model(spec).compile(renumbering="rcm", simd_width=32)
 
 
-def cpu_reference_apply(spec, max_seconds=20.0, max_reps=5):
-    """The reference's InternalForce::apply_operator (gather scatter, cached geometry, constant
-    tangent) on the host, OpenMP over every host thread: GDoF/s over a bounded number of applies."""
+def reference_force(spec):
+    """The reference's own compile step and InternalForce (oracle/_ref, every host thread) on `spec`,
+    or None where that library is missing."""
     import oracle as O
     if not O.have_ref():
         return None
-    threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     c = O.RefModel(spec).compile(renumbering="rcm", simd_width=32)
-    rf = O.RefForce(c, cache=True)
-    x = np.random.default_rng(0).standard_normal(c.num_equations)
+    return O.RefForce(c, cache=True)
+
+
+def rel_err(a, b):
+    """max |a - b| over max |b|."""
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(np.asarray(b))), 1e-300))
+
+
+def cpu_reference_apply(rf, x, max_seconds=20.0, max_reps=5):
+    """The reference's InternalForce::apply_operator (gather scatter, cached geometry, constant
+    tangent) on the host, OpenMP over every host thread: GDoF/s over a bounded number of applies."""
+    if rf is None:
+        return None
+    threads = os.cpu_count() or 1
     rf.apply_operator((1.0, 0.0, 0.0), x)  # warm-up (first touch of the cache and slots)
     times = []
     t_start = time.perf_counter()
@@ -158,11 +194,81 @@ def cpu_reference_apply(spec, max_seconds=20.0, max_reps=5):
         rf.apply_operator((1.0, 0.0, 0.0), x)
         times.append(time.perf_counter() - t0)
     best = min(times)
-    return dict(value=c.num_equations / best / 1e9, unit="GDoF/s", cores=int(os.environ.get("OMP_NUM_THREADS", threads)),
+    return dict(value=rf.n / best / 1e9, unit="GDoF/s", cores=int(os.environ.get("OMP_NUM_THREADS", threads)),
                 kind="reference",
                 sample=f"{len(times)} applies of the full 128x128x64 layered box (min time {best * 1e3:.1f} ms) through "
                        "the reference's own InternalForce::apply_operator (gather scatter, geometry cache, constant "
                        "tangent), built from its sources with a serial/OpenMP Kokkos-subset shim")
+
+
+def layered_parity(rf, force, x, y, device):
+    """The timed apply's y on the layered box against the reference's apply_operator on the same x,
+    and one FP64 internal force (seeded u, v; the box's alphaM and betaK damping) against the
+    reference's InternalForce::compute: max |ours - reference| over max |reference|."""
+    import torch
+    dev = torch.device("cuda", device)
+    y_ref = rf.apply_operator((1.0, 0.0, 0.0), x)
+    rng = np.random.default_rng(11)
+    u, v = 1e-3 * rng.standard_normal(rf.n), 1e-2 * rng.standard_normal(rf.n)
+    f = torch.zeros(rf.n, dtype=torch.float64, device=dev)
+    force.compute(torch.as_tensor(u, device=dev), torch.as_tensor(v, device=dev), f)
+    torch.cuda.synchronize(dev)
+    f_ref = rf.force(u, v)
+    return {"apply_max_rel_err": rel_err(y.cpu().numpy(), y_ref),
+            "force_max_rel_err": rel_err(f.cpu().numpy(), f_ref),
+            "against": "the reference's own InternalForce (apply_operator, compute) built from its sources",
+            "tolerance": 1e-12}
+
+
+def static_c1(device, solves=10):
+    """The static configuration as specified: a 32^3 stdBrick cube (1 m, E 50 MPa, nu 0.3, base fixed)
+    under a 100 kPa downward top traction, Jacobi-PCG to a 1e-10 relative residual. Plain FP64 CG and
+    FP32 CG inside FP64 refinement, solves/s by CUDA events over `solves` solves from x = 0 after one
+    warm-up solve each; the FP64 solution against the reference's own ConjugateGradient (oracle/_ref,
+    lanes 32) on the same compiled model, and each solution's true FP64 residual by the reference's
+    operator."""
+    import torch
+    import femorax_b200 as fx
+    mb = mesh_builders()
+    spec = mb.static_cube(32)
+    comp = fx.Model(spec).compile()
+    mesh = comp.mesh()
+    force = fx.InternalForce(mesh, device=device)
+    neq = mesh.num_equations
+    b = mb.top_traction_vector(spec, mb.equation_map(comp), neq)
+    dev = torch.device("cuda", device)
+    bt = torch.as_tensor(b, device=dev)
+    out = {"mesh": f"cube 32^3, {neq} equations", "rtol": 1e-10, "solves": solves}
+    xs = {}
+    for name, cls in (("plain_fp64", fx.ConjugateGradient), ("mixed", fx.MixedPrecisionSolver)):
+        s = cls(fx.SolveOptions(relative_tolerance=1e-10, max_iterations=20000))
+        s.setup(fx.MatrixFreeOperator(force))
+        x = torch.zeros(neq, dtype=torch.float64, device=dev)
+        r = s.solve(bt, x)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lat = []
+        for _ in range(solves):
+            x.zero_()
+            torch.cuda.synchronize(dev)
+            e0.record()
+            r = s.solve(bt, x)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            lat.append(e0.elapsed_time(e1) * 1e-3)
+        xs[name] = x.cpu().numpy()
+        out[name] = {"solves_per_s": solves / sum(lat), "p50_s": float(np.percentile(lat, 50)),
+                     "p99_s": float(np.percentile(lat, 99)), "iterations": int(r.iterations),
+                     "refinements": int(r.refinements), "converged": bool(r.converged)}
+    out["mixed_speedup"] = out["mixed"]["solves_per_s"] / out["plain_fp64"]["solves_per_s"]
+    rf = reference_force(spec)
+    if rf is not None:
+        x_ref, info = rf.solve(b, method="cg", rtol=1e-10, lanes=32)
+        nb = float(np.linalg.norm(b))
+        out["reference_cg_iterations"] = info["iterations"]
+        out["plain_fp64_vs_reference_max_rel_err"] = rel_err(xs["plain_fp64"], x_ref)
+        for name in xs:
+            out[name]["true_relative_residual"] = float(np.linalg.norm(b - rf.apply_operator((1.0, 0.0, 0.0), xs[name])) / nb)
+    return out
 
 
 def explicit_comparison(force, mesh, comp, device, steps=4000):
@@ -408,6 +514,16 @@ def newmark_comparison(device, n=100, steps=20, seed=0):
     peak = float(np.max(np.abs(runs[False].monitor)))
     out["mixed_vs_plain_max_abs_diff_over_peak"] = float(np.max(np.abs(runs[True].monitor - runs[False].monitor))) / peak
     out["converged"] = bool(runs[False].converged and runs[True].converged)
+    # one FP64 apply of the cube's operator (per-element E) against the reference's apply_operator
+    rf = reference_force(spec)
+    if rf is not None:
+        dev = torch.device("cuda", device)
+        xr = np.random.default_rng(5).standard_normal(mesh.num_equations)
+        y = torch.zeros(mesh.num_equations, dtype=torch.float64, device=dev)
+        force.apply_operator(fx.OperatorCoefficients(1.0, 0.0, 0.0), torch.as_tensor(xr, device=dev), y)
+        torch.cuda.synchronize(dev)
+        out["apply_parity"] = {"apply_max_rel_err": rel_err(y.cpu().numpy(), rf.apply_operator((1.0, 0.0, 0.0), xr)),
+                               "against": "the reference's own InternalForce::apply_operator", "tolerance": 1e-12}
     return out
 
 
@@ -579,16 +695,16 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    spec, _ = build_mesh()
     import oracle as O
     if not O.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfxref.so (the reference built from "
                                                                "its sources) is missing"}))
         return 0
+    spec = bench_spec()
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    c = O.RefModel(spec).compile(renumbering="rcm", simd_width=32)
-    rf = O.RefForce(c, cache=True)
+    rf = reference_force(spec)
+    c = rf.c
     x = np.random.default_rng(0).standard_normal(c.num_equations)
     for _ in range(args.warmup):
         rf.apply_operator((1.0, 0.0, 0.0), x)
@@ -600,13 +716,15 @@ def run_reference(args):
     total = sum(times)
     value = c.num_equations * args.steps / total / 1e9
     cores = int(os.environ.get("OMP_NUM_THREADS", threads))
+    n_nodes = len(c.array("node_tag"))
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(WORKLOAD, neq=c.num_equations, elements=c.count, parallelism="host OpenMP"),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded layer properties)",
+            "config": bench_config(c.num_equations, c.count, n_nodes, args.gpus),
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "GDoF/s", "cores": cores, "kind": "reference",
-                             "sample": f"{args.steps} applies of the full workload, each one step"},
+                             "sample": f"{args.steps} applies of the full workload, each one step, through the "
+                                       "reference's own InternalForce::apply_operator on every host thread"},
             "e2e": {"value": value, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -713,15 +831,20 @@ def run_ours(args):
     pdmy = pdmy_points(local) if world == 1 and not args.no_serve else None
     if pdmy is not None:
         pdmy["force_box"] = pdmy_force_box(local)
-    cpu = cpu_reference_apply(spec) if world == 1 and not args.no_cpu else None
+    rf = reference_force(spec) if world == 1 else None
+    xn0 = x.cpu().numpy()
+    parity = layered_parity(rf, force, xn0, y, local) if rf is not None else None
+    cpu = cpu_reference_apply(rf, xn0) if rf is not None and not args.no_cpu else None
+    del rf
+    static = static_c1(local) if world == 1 and not args.no_serve else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded layer properties)",
-            "config": dict(WORKLOAD, neq=neq, elements=n_el, nodes=n_nodes, path=info["path"],
-                           parallelism=f"replicas x{world}" if world > 1 else "single GPU",
-                           launch={"variant": int(launch[0]), "kz": int(launch[1]),
-                                   "chosen_by": "option" if args.launch else "autotuner", "all": tuned},
-                           l2="flushed (256 MB write) between timed applies"),
+            "config": bench_config(neq, n_el, n_nodes, world),
+            "path": info["path"],
+            "launch": {"variant": int(launch[0]), "kz": int(launch[1]),
+                       "chosen_by": "option" if args.launch else "autotuner", "all": tuned},
+            "parity": parity,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg},
@@ -734,6 +857,7 @@ def run_ours(args):
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
             "explicit": explicit,
+            "static_c1": static,
             "served": served,
             "served_mixed": served_mixed,
             "served_rates": served_rates,

@@ -31,112 +31,164 @@ namespace {
 
 using Index = int32_t;
 
-struct Graph {
-  std::vector<Index> start, adj;
-  Index degree(Index v) const { return start[v + 1] - start[v]; }
+// ---- node order: reverse Cuthill-McKee
+//
+// Rules the numbering follows, so that it equals the reference's node by node
+// (src/compile/renumber.cpp:58-177):
+//   R1 the graph joins the nodes at two different corner positions of one element, and the two
+//      nodes of each equalDOF pair (in both directions); a node's degree counts its distinct
+//      neighbours;
+//   R2 "lighter" compares nodes by degree, then by model index;
+//   R3 components are numbered one after another, in the order of their lowest model index;
+//   R4 a component's root comes from its lightest node by the George-Liu walk: level the
+//      component from the current root and, while the number of levels grows (at most 32
+//      levelings), move the root to the lightest node of the last level;
+//   R5 from the root, breadth first, each node's neighbours not yet reached are appended
+//      lightest first; the component's sequence is then reversed.
+// Elements follow by the smallest rank among their nodes, ties in model order.
+
+// Adjacency in compressed rows, built by counting: row v lists v's neighbours ascending.
+class NodeAdjacency {
+ public:
+  NodeAdjacency(const fx_model& m, const std::unordered_map<int32_t, Index>& idx) {
+    const Index N = static_cast<Index>(m.tags.size());
+    std::vector<Index> corner;  // model index per element corner, group after group
+    for (const auto& g : m.groups)
+      for (int32_t t : g.conn) corner.push_back(idx.at(t));
+    std::vector<Index> tie_a(m.eqd_retained.size()), tie_b(m.eqd_retained.size());
+    for (size_t r = 0; r < tie_a.size(); ++r) {
+      tie_a[r] = idx.at(m.eqd_retained[r]);
+      tie_b[r] = idx.at(m.eqd_constrained[r]);
+    }
+    // pass 1: row lengths with repeats; pass 2: fill; then each row sorted and compacted
+    std::vector<int64_t> cap(static_cast<size_t>(N) + 1, 0);
+    for (Index v : corner) cap[v + 1] += 7;
+    for (size_t r = 0; r < tie_a.size(); ++r) ++cap[tie_a[r] + 1], ++cap[tie_b[r] + 1];
+    for (Index v = 0; v < N; ++v) cap[v + 1] += cap[v];
+    std::vector<Index> raw(static_cast<size_t>(cap[N]));
+    std::vector<int64_t> fill(cap.begin(), cap.end() - 1);
+    for (size_t e = 0; e + 8 <= corner.size(); e += 8)
+      for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j)
+          if (i != j) raw[fill[corner[e + i]]++] = corner[e + j];
+    for (size_t r = 0; r < tie_a.size(); ++r) {
+      raw[fill[tie_a[r]]++] = tie_b[r];
+      raw[fill[tie_b[r]]++] = tie_a[r];
+    }
+    row_.assign(static_cast<size_t>(N) + 1, 0);
+    col_.reserve(raw.size() / 2);
+    for (Index v = 0; v < N; ++v) {
+      auto* lo = raw.data() + cap[v];
+      auto* hi = raw.data() + cap[v + 1];
+      std::sort(lo, hi);
+      hi = std::unique(lo, hi);
+      col_.insert(col_.end(), lo, hi);
+      row_[v + 1] = static_cast<Index>(col_.size());
+    }
+  }
+  Index nodes() const { return static_cast<Index>(row_.size()) - 1; }
+  Index degree(Index v) const { return row_[v + 1] - row_[v]; }
+  const Index* begin(Index v) const { return col_.data() + row_[v]; }
+  const Index* end(Index v) const { return col_.data() + row_[v + 1]; }
+  bool lighter(Index a, Index b) const {
+    const Index da = degree(a), db = degree(b);
+    return da != db ? da < db : a < b;
+  }
+
+ private:
+  std::vector<Index> row_, col_;
 };
 
-Graph node_graph(const fx_model& m, const std::unordered_map<int32_t, Index>& idx) {
-  const Index N = static_cast<Index>(m.tags.size());
-  std::vector<std::vector<Index>> nbr(static_cast<size_t>(N));
-  for (const auto& g : m.groups) {
-    const size_t ne = g.tags.size();
-    for (size_t e = 0; e < ne; ++e)
-      for (int a = 0; a < 8; ++a)
-        for (int b = 0; b < 8; ++b)
-          if (a != b) nbr[idx.at(g.conn[e * 8 + a])].push_back(idx.at(g.conn[e * 8 + b]));
-  }
-  for (size_t r = 0; r < m.eqd_retained.size(); ++r) {
-    const Index a = idx.at(m.eqd_retained[r]), b = idx.at(m.eqd_constrained[r]);
-    nbr[a].push_back(b);
-    nbr[b].push_back(a);
-  }
-  Graph G;
-  G.start.assign(static_cast<size_t>(N) + 1, 0);
-  for (Index v = 0; v < N; ++v) {
-    auto& l = nbr[v];
-    std::sort(l.begin(), l.end());
-    l.erase(std::unique(l.begin(), l.end()), l.end());
-    G.start[v + 1] = G.start[v] + static_cast<Index>(l.size());
-  }
-  G.adj.reserve(static_cast<size_t>(G.start[N]));
-  for (auto& l : nbr) G.adj.insert(G.adj.end(), l.begin(), l.end());
-  return G;
-}
+// Breadth-first traversals over the nodes not numbered yet. A node's mark is kNumbered once it
+// has a number, and equals the pass counter while the current traversal has reached it.
+class LevelWalker {
+ public:
+  explicit LevelWalker(const NodeAdjacency& g) : g_(g), mark_(static_cast<size_t>(g.nodes()), 0) {}
 
-// Breadth-first levels from root over the nodes not yet numbered; the last level and the depth.
-std::vector<Index> last_level(const Graph& G, Index root, const std::vector<char>& done, int& depth) {
-  std::vector<Index> level{root}, last = level;
-  std::vector<char> seen(done);
-  seen[root] = 1;
-  depth = 0;
-  while (!level.empty()) {
-    last = level;
-    std::vector<Index> next;
-    for (Index v : level)
-      for (Index k = G.start[v]; k < G.start[v + 1]; ++k)
-        if (!seen[G.adj[k]]) {
-          seen[G.adj[k]] = 1;
-          next.push_back(G.adj[k]);
-        }
-    if (!next.empty()) ++depth;
-    level = std::move(next);
-  }
-  return last;
-}
-
-std::vector<Index> rcm_order(const Graph& G) {
-  const Index N = static_cast<Index>(G.start.size()) - 1;
-  auto lighter = [&](Index a, Index b) { return G.degree(a) != G.degree(b) ? G.degree(a) < G.degree(b) : a < b; };
-  std::vector<char> done(static_cast<size_t>(N), 0);
-  std::vector<Index> order;
-  order.reserve(static_cast<size_t>(N));
-  for (Index s = 0; s < N; ++s) {
-    if (done[s]) continue;
-    // lightest node of s's component (degree, then index)
-    Index best = s;
-    {
-      std::vector<Index> stack{s};
-      std::vector<char> seen(done);
-      seen[s] = 1;
-      while (!stack.empty()) {
-        const Index v = stack.back();
-        stack.pop_back();
-        if (lighter(v, best)) best = v;
-        for (Index k = G.start[v]; k < G.start[v + 1]; ++k)
-          if (!seen[G.adj[k]]) {
-            seen[G.adj[k]] = 1;
-            stack.push_back(G.adj[k]);
+  // Visits everything reachable from root; `seq` holds the nodes in visiting order, level after
+  // level. With `lightest_first`, each node's newly reached neighbours enter lightest first (R5).
+  // Returns the number of levels.
+  int walk(Index root, bool lightest_first) {
+    ++pass_;
+    seq.clear();
+    seq.push_back(root);
+    mark_[root] = pass_;
+    size_t level_begin = 0;
+    int levels = 0;
+    last_level = 0;
+    while (level_begin < seq.size()) {
+      const size_t level_end = seq.size();
+      ++levels;
+      last_level = level_begin;
+      for (size_t h = level_begin; h < level_end; ++h) {
+        const size_t grown = seq.size();
+        for (const Index* w = g_.begin(seq[h]); w != g_.end(seq[h]); ++w)
+          if (mark_[*w] != kNumbered && mark_[*w] != pass_) {
+            mark_[*w] = pass_;
+            seq.push_back(*w);
           }
+        if (lightest_first)
+          std::sort(seq.begin() + static_cast<std::ptrdiff_t>(grown), seq.end(),
+                    [this](Index a, Index b) { return g_.lighter(a, b); });
       }
+      level_begin = level_end;
     }
-    // pseudo-peripheral root: follow the lightest node of the last level while depth grows
-    Index root = best;
-    int depth = -1;
-    for (int it = 0; it < 32; ++it) {
-      int d;
-      const auto last = last_level(G, root, done, d);
-      if (d <= depth) break;
-      depth = d;
-      root = *std::min_element(last.begin(), last.end(), lighter);
+    return levels;
+  }
+
+  bool numbered(Index v) const { return mark_[v] == kNumbered; }
+  void number_visited() {
+    for (Index v : seq) mark_[v] = kNumbered;
+  }
+  Index lightest(size_t from) const {
+    Index best = seq[from];
+    for (size_t i = from + 1; i < seq.size(); ++i)
+      if (g_.lighter(seq[i], best)) best = seq[i];
+    return best;
+  }
+
+  std::vector<Index> seq;
+  size_t last_level = 0;  // where the last level starts in seq
+
+ private:
+  static constexpr int32_t kNumbered = -1;
+  const NodeAdjacency& g_;
+  std::vector<int32_t> mark_;
+  int32_t pass_ = 0;
+};
+
+std::vector<Index> rcm_node_order(const fx_model& m, const std::unordered_map<int32_t, Index>& idx) {
+  const NodeAdjacency g(m, idx);
+  LevelWalker walker(g);
+  std::vector<Index> order;
+  order.reserve(static_cast<size_t>(g.nodes()));
+  for (Index s = 0; s < g.nodes(); ++s) {  // R3
+    if (walker.numbered(s)) continue;
+    walker.walk(s, false);
+    Index root = walker.lightest(0);  // R4: the component's lightest node
+    int levels = 0;
+    for (int round = 0; round < 32; ++round) {
+      const int l = walker.walk(root, false);
+      if (l <= levels) break;
+      levels = l;
+      root = walker.lightest(walker.last_level);
     }
-    const size_t first = order.size();
-    order.push_back(root);
-    done[root] = 1;
-    for (size_t head = first; head < order.size(); ++head) {
-      const Index v = order[head];
-      std::vector<Index> next;
-      for (Index k = G.start[v]; k < G.start[v + 1]; ++k)
-        if (!done[G.adj[k]]) {
-          done[G.adj[k]] = 1;
-          next.push_back(G.adj[k]);
-        }
-      std::sort(next.begin(), next.end(), lighter);
-      for (Index w : next) order.push_back(w);
-    }
-    std::reverse(order.begin() + static_cast<std::ptrdiff_t>(first), order.end());
+    walker.walk(root, true);  // R5
+    walker.number_visited();
+    order.insert(order.end(), walker.seq.rbegin(), walker.seq.rend());
   }
   return order;
+}
+
+// Element order: ascending key (the smallest node rank of the element), equal keys in model
+// order; a counting sort over the key range, stable by construction.
+std::vector<Index> order_by_key(const std::vector<Index>& key, Index key_range) {
+  std::vector<Index> first(static_cast<size_t>(key_range) + 1, 0);
+  for (Index k : key) ++first[k + 1];
+  for (Index k = 0; k < key_range; ++k) first[k + 1] += first[k];
+  std::vector<Index> out(key.size());
+  for (size_t e = 0; e < key.size(); ++e) out[first[key[e]]++] = static_cast<Index>(e);
+  return out;
 }
 
 struct UnionFind {
@@ -178,7 +230,7 @@ void compile_model(const fx_model& m, int renumbering, int simd_width, bool colo
 
   // ---- node order and element order
   if (renumbering == FX_RENUMBER_RCM) {
-    c.node_order = rcm_order(node_graph(m, idx));
+    c.node_order = rcm_node_order(m, idx);
   } else {
     c.node_order.resize(static_cast<size_t>(N));
     std::iota(c.node_order.begin(), c.node_order.end(), 0);
@@ -196,10 +248,12 @@ void compile_model(const fx_model& m, int renumbering, int simd_width, bool colo
       where.emplace_back(static_cast<Index>(gi), static_cast<Index>(e));
     }
   }
-  c.element_order.resize(key.size());
-  std::iota(c.element_order.begin(), c.element_order.end(), 0);
-  if (renumbering == FX_RENUMBER_RCM)
-    std::stable_sort(c.element_order.begin(), c.element_order.end(), [&](Index a, Index b) { return key[a] < key[b]; });
+  if (renumbering == FX_RENUMBER_RCM) {
+    c.element_order = order_by_key(key, N);
+  } else {
+    c.element_order.resize(key.size());
+    std::iota(c.element_order.begin(), c.element_order.end(), 0);
+  }
 
   // ---- DOF numbering
   c.num_nodes = N;

@@ -133,6 +133,28 @@ def top_traction_rhs(spec, eq_of, q=-100e3):
     return f
 
 
+def equation_map(compiled):
+    """eq[tag, dof]: the equation of (node tag, dof 0..2), -1 fixed, from a compile step's arrays
+    (`node_tag`, `dof_offset`, `eq` by name: this library's Compiled or the reference's)."""
+    tags = compiled.array("node_tag")
+    off = compiled.array("dof_offset")
+    eq = compiled.array("eq")
+    out = np.full((int(tags.max()) + 1, 3), -1, dtype=np.int64)
+    for d in range(3):
+        out[tags, d] = eq[off[:-1] + d]
+    return out
+
+
+def top_traction_vector(spec, eqmap, neq, q=-100e3):
+    """top_traction_rhs as an equation-space vector of neq entries (vertical DOF of each top node)."""
+    b = np.zeros(neq)
+    for tag, f in top_traction_rhs(spec, None, q).items():
+        e = int(eqmap[tag, 2])
+        if e >= 0:
+            b[e] += f
+    return b
+
+
 def rayleigh_coefficients(xi, f1, f2):
     """alphaM, betaK for damping ratio xi at frequencies f1 and f2 (Hz)."""
     w1, w2 = 2 * math.pi * f1, 2 * math.pi * f2

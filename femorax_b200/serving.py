@@ -113,13 +113,7 @@ class Served:
 def equation_map(compiled):
     """eq[tag, dof]: the equation of (node tag, dof 0..2), -1 fixed, as an array indexed by tag,
     from the compile step's arrays."""
-    tags = compiled.array("node_tag")
-    off = compiled.array("dof_offset")
-    eq = compiled.array("eq")
-    out = np.full((int(tags.max()) + 1, 3), -1, dtype=np.int64)
-    for d in range(3):
-        out[tags, d] = eq[off[:-1] + d]
-    return out
+    return meshes.equation_map(compiled)
 
 
 def top_load(req: Request, eqmap) -> np.ndarray:

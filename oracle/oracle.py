@@ -28,10 +28,14 @@ _ref = None
 _port = None
 
 
-def build(ref: bool = True) -> None:
-    """Builds the oracle libraries (the reference one only where its sources exist)."""
-    targets = ["port"] + (["ref"] if ref and os.path.isdir("/root/reference/src") else [])
-    subprocess.run(["make", "-s", "-j8"] + targets, cwd=HERE, check=True)
+def build(reference_dir: str = None) -> None:
+    """Builds the oracle libraries: the C restatement always, the reference's own sources where
+    `reference_dir` (default: the environment variable FEMORAX_REFERENCE) holds its checkout."""
+    reference_dir = reference_dir or os.environ.get("FEMORAX_REFERENCE", "")
+    have = bool(reference_dir) and os.path.isdir(os.path.join(reference_dir, "src"))
+    subprocess.run(["make", "-s", "-j8", "port"], cwd=HERE, check=True)
+    if have:
+        subprocess.run(["make", "-s", "-j8", "ref", f"REF={reference_dir}"], cwd=HERE, check=True)
 
 
 def have_ref() -> bool:

@@ -17,7 +17,7 @@ def pytest_configure(config):
 def oracle_mod():
     import oracle as O
     if not os.path.exists(O.PORT_LIB):
-        O.build(ref=False)
+        O.build("")
     return O
 
 

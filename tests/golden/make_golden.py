@@ -9,6 +9,9 @@ the reference checkout and the oracle library exist):
   compile_maps.npz    the reference's compile_model output (oracle/_ref/libfxref.so) for two
                       small models: a 4 x 3 x 5 block with two Rayleigh regions (RCM, coloring)
                       and a 3 x 2 x 8 soil column with laminar equalDOF ties.
+  compile_digests.json  sha256 digests of every compile_model array (oracle/_ref/libfxref.so)
+                      for the three benchmark configurations' models (the 32^3 static cube,
+                      the 128 x 128 x 64 layered box, the 100^3 per-element-E cube).
   pdmy_paths.npz      the same for PressureDependMultiYield (tests/reference/data/nd/
                       PressureDependMultiYield_*.txt).
   pimy_paths.npz      the reference's stored OpenSees PressureIndependMultiYield strain paths
@@ -17,7 +20,7 @@ the reference checkout and the oracle library exist):
                       load stage, the discarded trial strain (if any), the strain, and OpenSees'
                       stress and tangent.
 
-    python tests/golden/make_golden.py [bricks|compile_maps|pimy_paths|pdmy_paths ...]
+    FEMORAX_REFERENCE=<reference checkout> python tests/golden/make_golden.py [bricks|compile_maps|pimy_paths|pdmy_paths ...]
 """
 import glob
 import os
@@ -29,8 +32,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
-DATA = "/root/reference/tests/reference/data/element"
-ND = "/root/reference/tests/reference/data/nd"
+REFERENCE = os.environ.get("FEMORAX_REFERENCE", "")  # the reference checkout (read as text)
+DATA = os.path.join(REFERENCE, "tests/reference/data/element")
+ND = os.path.join(REFERENCE, "tests/reference/data/nd")
 PDMY_PARAMS = ("rho", "refShearModul", "refBulkModul", "frictionAng", "peakShearStra", "refPress", "pressDependCoe",
                "PTAng", "contrac", "dilat1", "dilat2", "liquefac1", "liquefac2", "liquefac3", "noYieldSurf", "e", "cs1",
                "cs2", "cs3", "pa", "c")
@@ -107,6 +111,44 @@ def compile_maps():
     print("compile_maps.npz written")
 
 
+CONFIG_MODELS = ("static_cube_32", "layered_box_128x128x64", "heterogeneous_cube_100")
+
+
+def config_model(name):
+    """The models of the benchmark configurations: the 32^3 static cube, the 128 x 128 x 64 layered
+    box (seed 0) and the 100^3 cube with per-element E (seed 0)."""
+    from femorax_b200 import meshes
+    if name == "static_cube_32":
+        return meshes.static_cube(32)
+    if name == "layered_box_128x128x64":
+        return meshes.layered_box(128, 128, 64, 8, seed=0)[0]
+    return meshes.heterogeneous_cube(100, seed=0, size=50.0)
+
+
+def array_digest(a):
+    """sha256 of an array's dtype, shape and little-endian bytes."""
+    import hashlib
+    a = np.ascontiguousarray(a)
+    h = hashlib.sha256(f"{a.dtype.str}{a.shape}".encode())
+    h.update(a.astype(a.dtype.newbyteorder("<")).tobytes())
+    return h.hexdigest()
+
+
+def compile_digests():
+    """compile_digests.json: digests of every array the reference's compile_model returns (RCM,
+    SIMD width 32) for the benchmark configurations' models; the arrays themselves are too large
+    to commit."""
+    import json
+    import oracle as O
+    out = {}
+    for name in CONFIG_MODELS:
+        c = O.RefModel(config_model(name)).compile(renumbering="rcm", simd_width=32)
+        names = O.RefCompiled.I32 + ("coords", "lumped_mass", "lumped_alpha_mass", "nodal_mass", "nodal_alpha_mass")
+        out[name] = {a: array_digest(c.array(a)) for a in names}
+    json.dump(out, open(os.path.join(HERE, "compile_digests.json"), "w"), indent=1, sort_keys=True)
+    print("compile_digests.json written")
+
+
 def pimy_paths(material="PressureIndependMultiYield", names=None, out_name="pimy_paths.npz"):
     names = names or PIMY_PARAMS
     out, cases = {}, []
@@ -136,6 +178,6 @@ def pdmy_paths():
 
 
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["bricks", "compile_maps", "pimy_paths", "pdmy_paths"]
+    what = sys.argv[1:] or ["bricks", "compile_maps", "compile_digests", "pimy_paths", "pdmy_paths"]
     for w in what:
         globals()[w]()

@@ -1,6 +1,7 @@
 """The compile step's arrays are the reference's (compile::compile_model) value for value: against
 the stored fixtures (tests/golden/compile_maps.npz), and against the reference built here on a
 range of block sizes when its library is present."""
+import json
 import os
 
 import numpy as np
@@ -63,3 +64,16 @@ def test_invalid_models_are_refused():
     bad.groups[0].conn[0, 0] = 99999
     with pytest.raises(fx.FxError):
         fx.Model(bad).compile()
+
+
+@pytest.mark.parametrize("name", ["static_cube_32", "layered_box_128x128x64", "heterogeneous_cube_100"])
+def test_maps_at_benchmark_configs(name):
+    """Every compile array of the benchmark configurations' models (the 32^3 static cube, the
+    128 x 128 x 64 layered box, the 100^3 per-element-E cube) has the digest of the reference's
+    compile_model output (tests/golden/compile_digests.json, written from oracle/_ref)."""
+    from tests.golden import make_golden as G
+    want = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "compile_digests.json")))[name]
+    c = fx.Model(G.config_model(name)).compile(renumbering="rcm", simd_width=32)
+    got = {a: G.array_digest(c.array(a)) for a in want}
+    assert set(want) == set(ARRAYS)
+    assert got == want
