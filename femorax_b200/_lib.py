@@ -103,6 +103,7 @@ PROTOTYPES = {
     "fx_apply_operator": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_apply_operator_f32": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_apply_operator_host": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
+    "fx_operator_diagonal_host": (C.c_int, [vp, fx_coeffs, vp, vp]),
     "fx_operator_diagonal": (C.c_int, [vp, fx_coeffs, vp, vp]),
     "fx_force_compute": (C.c_int, [vp, vp, vp, vp, vp]),
     "fx_force_compute_f32": (C.c_int, [vp, vp, vp, vp, vp]),

@@ -474,6 +474,19 @@ int fx_operator_diagonal(fx_force* f, fx_coeffs k, double* d, void* stream) {
   });
 }
 
+int fx_operator_diagonal_host(fx_force* f, fx_coeffs k, double* dh, void* stream) {
+  return guarded([&] {
+    FX_REQUIRE(f && (f->s.neq == 0 || dh), "fx_operator_diagonal_host: bad arguments");
+    auto st = static_cast<cudaStream_t>(stream);
+    const double kk[3] = {k.stiffness, k.damping, k.mass};
+    f->s.initial = k.initial != 0;
+    fx::general_diagonal(f->s, kk, f->s.wy.ptr, st);
+    FX_CUDA(cudaMemcpyAsync(dh, f->s.wy.ptr, sizeof(double) * static_cast<size_t>(f->s.neq), cudaMemcpyDeviceToHost,
+                            st));
+    FX_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
 int fx_force_compute(fx_force* f, const double* u, const double* v, double* out, void* stream) {
   return guarded([&] {
     FX_REQUIRE(f && (f->s.neq == 0 || (u && v && out)), "fx_force_compute: bad arguments");

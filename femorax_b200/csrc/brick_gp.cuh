@@ -269,14 +269,16 @@ FX_HD void j2_D(const ParamGP& p, const double tan[kJ2Tan], double D[6][6]) {
 }
 
 // Operator factors (element_operator.hpp:45-56; stdBrick's initial stiffness is not its
-// tangent): k = {stiffness, damping, mass}.
+// tangent): k = {stiffness, damping, mass}. cK scales the point's tangent, c0 the initial
+// (elastic) tangent, cc the committed tangent; with `initial` (ModifiedNewton -initial) the
+// stiffness term moves from the tangent to the initial tangent, the damping terms stay.
 struct OpFactors {
   double cK, c0, cc, cM;
 };
-FX_HD OpFactors op_factors(const ParamGP& p, double ks, double kd, double km) {
+FX_HD OpFactors op_factors(const ParamGP& p, double ks, double kd, double km, bool initial = false) {
   OpFactors f;
-  f.cK = ks + kd * p.betaK;
-  f.c0 = kd * p.betaKinit;
+  f.cK = initial ? kd * p.betaK : ks + kd * p.betaK;
+  f.c0 = initial ? ks + kd * p.betaKinit : kd * p.betaKinit;
   f.cc = kd * p.betaKcomm;
   f.cM = km + kd * p.alphaM;
   return f;
@@ -297,8 +299,8 @@ FX_HD void effective_D(const OpFactors& f, const ParamGP& p, double De[6][6]) {
 
 // Sources of the effective material matrix at a point: the constant elastic one, or a J2
 // element's consistent tangent per point (component c of point gp at tan[(c * 8 + gp) * stride]),
-// scaled by the stiffness factor (J2 sets carry no stiffness-proportional damping); `initial`
-// takes the elastic matrix (ModifiedNewton -initial).
+// scaled by the stiffness factor (J2 sets carry no stiffness-proportional damping, so the
+// factor is cK, or c0 on the elastic matrix with `initial`: ModifiedNewton -initial).
 struct ConstD {
   double De[6][6];
   FX_HD void operator()(int, double D[6][6]) const {

@@ -44,10 +44,10 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
     if (unit_dir >= 0) xe[a] = (a % 3) == unit_dir ? 1.0 : 0.0;
     else xe[a] = q >= 0 ? x[q] : 0.0;
   }
-  const OpFactors f = op_factors(p, ks, kd, km);
-  if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
-  else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc, initial != 0});
-  else if (p.kind == 3) element_apply_d(p, f, xl, xe, ye, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.cc, initial != 0});
+  const OpFactors f = op_factors(p, ks, kd, km, initial != 0);
+  if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, initial ? f.c0 : f.cK, initial != 0});
+  else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc});
+  else if (p.kind == 3) element_apply_d(p, f, xl, xe, ye, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.c0, f.cc});
   else element_apply(p, f, xl, xe, ye);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = ye[a];
 }
@@ -70,12 +70,12 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
   int eqe[24];
   load_coords(coords, node, N, P, e, xl);
   for (int a = 0; a < 24; ++a) eqe[a] = eq[static_cast<int64_t>(a) * P + e];
-  const OpFactors f = op_factors(p, ks, kd, km);
-  if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, f.cK, initial != 0});
+  const OpFactors f = op_factors(p, ks, kd, km, initial != 0);
+  if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, initial ? f.c0 : f.cK, initial != 0});
   else if (p.kind == 2)
-    element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc, initial != 0});
+    element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc});
   else if (p.kind == 3)
-    element_diagonal_d(p, f, xl, eqe, de, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.cc, initial != 0});
+    element_diagonal_d(p, f, xl, eqe, de, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.c0, f.cc});
   else element_diagonal(p, f, xl, eqe, de);
   for (int a = 0; a < 24; ++a) slots[static_cast<int64_t>(a) * P + e] = de[a];
 }
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kBlock) k_element_apply32(const int32_t* __res
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count || (skip && *skip)) return;
   const ParamGP p = params[param[e]];
-  const OpFactors f = op_factors(p, ks, kd, km);
+  const OpFactors f = op_factors(p, ks, kd, km, initial != 0);
   // the elastic tangents are one matrix: D_eff = (cK + c0 + cc) D (J2 sets carry no
   // stiffness-proportional damping, so c0 = cc = 0 there)
   const float sk = static_cast<float>(f.cK + f.c0 + f.cc), cm = static_cast<float>(f.cM);
@@ -371,7 +371,17 @@ void general_apply_f32(ForceState& s, const double k[3], const float* x, float* 
   FX_LAUNCH_CHECK("slot_gather32");
 }
 
+// ModifiedNewton -initial with PressureIndependMultiYield is refused, as the reference refuses it
+// (src/io/support.cpp:120-127): OpenSees scales that material's initial tangent per point at the
+// switch to the plastic stage, and that scaled tangent is not kept.
+static void refuse_pimy_initial(const ForceState& s) {
+  if (s.initial && s.has_pimy)
+    throw Error(FX_E_UNSUPPORTED, "ModifiedNewton -initial (the initial stiffness in the operator) with "
+                                  "PressureIndependMultiYield");
+}
+
 void general_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
+  refuse_pimy_initial(s);
   if (s.count > 0)
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
@@ -389,6 +399,7 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
 }
 
 void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st) {
+  refuse_pimy_initial(s);
   if (s.count > 0)
     k_element_diag<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                   s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],

@@ -136,9 +136,9 @@ FX_HD void element_force_from_stress(const ParamGP& p, const double xl[3][8], co
 
 // The material matrix of point gp for the operator (the reference's effective_tangent,
 // src/physics/operators/element_operator.hpp:58-75, without betaKinit): the stored tangent of the
-// last force evaluation, or (ModifiedNewton -initial) the material's initial tangent, the reference
-// elastic one (the reference's PressureIndependMultiYield::initial_tangent), scaled by the stiffness
-// factor, plus cc times the tangent at the committed state (betaKcomm damping, not mirrored).
+// last force evaluation scaled by the stiffness factor, plus cc times the tangent at the committed
+// state (betaKcomm damping, not mirrored). ModifiedNewton -initial is refused on these sets, as the
+// reference refuses it (general.cu, refuse_pimy_initial).
 // The material declares its tangent symmetric, so it is stored as its upper triangle and the lower
 // one mirrors it (the reference's TangentStorage, src/physics/common/tangent_storage.hpp:17-31).
 struct PimyPointD {
@@ -147,16 +147,11 @@ struct PimyPointD {
   const double* committed;  // the committed states (read only when cc is not zero)
   int64_t stride;
   double cK, cc;
-  bool initial;
   FX_HD void operator()(int gp, double De[6][6]) const {
     double D[36];
-    if (initial) {
-      pimy::elastic_D(m->p.G0, m->p.K0, D);
-    } else {
-      double t[pimy::kTan];
-      for (int c = 0; c < pimy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
-      pimy::compact_D(t, D);
-    }
+    double t[pimy::kTan];
+    for (int c = 0; c < pimy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
+    pimy::compact_D(t, D);
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
     for (int a = 0; a < 6; ++a)
@@ -165,29 +160,30 @@ struct PimyPointD {
   }
 };
 
-// The operator's material matrix of a PressureDependMultiYield point: its stored tangent (upper
-// triangle mirrored) or the reference elastic tangent (initial), scaled by the stiffness factor,
-// plus cc times its committed tangent.
+// The operator's material matrix of a PressureDependMultiYield point (effective_tangent,
+// element_operator.hpp:60-75): cK times its stored tangent (upper triangle mirrored), plus c0
+// times the material's initial tangent (the reference elastic tangent: the stiffness term under
+// ModifiedNewton -initial), plus cc times its committed tangent.
 struct PdmyPointD {
   const PdmySet* m;
   const double* tan;
   const double* committed;  // the committed states (read only when cc is not zero)
   int64_t stride;
-  double cK, cc;
-  bool initial;
+  double cK, c0, cc;
   FX_HD void operator()(int gp, double De[6][6]) const {
     double D[36];
-    if (initial) {
-      pdmy::elastic_D(m->p, 1.0, D);
-    } else {
-      double t[pdmy::kTan];
-      for (int c = 0; c < pdmy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
-      pdmy::compact_D(m->p, t, D);
-    }
+    double t[pdmy::kTan];
+    for (int c = 0; c < pdmy::kTan; ++c) t[c] = tan[(c * 8 + gp) * stride];
+    pdmy::compact_D(m->p, t, D);
     for (int a = 0; a < 6; ++a)
       for (int c = a + 1; c < 6; ++c) D[6 * c + a] = D[6 * a + c];
     for (int a = 0; a < 6; ++a)
       for (int c = 0; c < 6; ++c) De[a][c] = cK * D[6 * a + c];
+    if (c0 != 0.0) {
+      double D0[36];
+      pdmy::elastic_D(m->p, 1.0, D0);
+      for (int i = 0; i < 36; ++i) (&De[0][0])[i] += c0 * D0[i];
+    }
     if (cc != 0.0) add_committed_D(*m, committed, gp, stride, cc, &De[0][0]);
   }
 };

@@ -187,15 +187,31 @@ constexpr int64_t kNoAllocMaxN = int64_t(1) << 27;                     // entrie
 constexpr int64_t kNoAllocL0 = (kNoAllocMaxN + kChunk - 1) / kChunk;  // 65536 chunk sums
 constexpr int64_t kNoAllocL1 = (kNoAllocL0 + kChunk - 1) / kChunk;    // 32 sums of those
 constexpr int kNoAllocDevices = 64;
+static_assert((kNoAllocL0 + kChunk - 1) / kChunk <= kNoAllocL1, "level 1 holds the sums of level 0's chunks");
+static_assert((kNoAllocL1 + kChunk - 1) / kChunk <= kNoAllocL0, "level 0 holds the sums of level 1's chunks");
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocL0 + kNoAllocL1 + 1];
 
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocDevices] = {};
 
-// The scratch array's address on the current device, looked up on the first call there.
-double* noalloc_scratch() {
+// Device memory on `dev` (or managed memory): the vectors a kernel on the current device reads.
+bool on_device(const void* p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();  // clear the query's error state
+    return false;
+  }
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
+}
+
+// The scratch array's address on the current device, looked up on the first call there. The
+// vectors must live on that device: the address is only valid there.
+double* noalloc_scratch(const double* x, const double* y, int64_t n) {
   int dev = 0;
   FX_CUDA(cudaGetDevice(&dev));
+  if (n > 0 && (!on_device(x, dev) || !on_device(y, dev)))
+    throw Error(FX_E_INVALID, "fx_dot_noalloc: x and y must be device memory of the current device (" +
+                                  std::to_string(dev) + ")");
   if (dev < 0 || dev >= kNoAllocDevices) throw Error(FX_E_UNSUPPORTED, "fx_dot_noalloc: device index above 63");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_ptr[dev]) {
@@ -218,7 +234,7 @@ void dot_noalloc(const double* x, const double* y, int64_t n, int lanes, double*
     throw Error(FX_E_INVALID, "fx_dot_noalloc: n = " + std::to_string(n) + " exceeds the scratch limit of " +
                                   std::to_string(kNoAllocMaxN) + " entries");
   if (!result && !result_host) throw Error(FX_E_INVALID, "fx_dot_noalloc: no result pointer given");
-  double* scratch = noalloc_scratch();
+  double* scratch = noalloc_scratch(x, y, n);
   double* level[2] = {scratch, scratch + kNoAllocL0};
   double* r = result ? result : scratch + kNoAllocL0 + kNoAllocL1;
   if (n == 0) {
@@ -231,6 +247,7 @@ void dot_noalloc(const double* x, const double* y, int64_t n, int lanes, double*
     int cur = 0;
     while (nc > 1) {
       const int64_t m = chunks_of(nc);
+      if (m > (cur ? kNoAllocL0 : kNoAllocL1)) throw Error(FX_E_INVALID, "fx_dot_noalloc: level overflow");
       dim3 g(static_cast<unsigned>((m + kWarpsPerBlock - 1) / kWarpsPerBlock), 1);
       k_reduce_chunks<<<g, 32 * kWarpsPerBlock, 0, st>>>(level[cur], 0, nullptr, nc, lanes, m,
                                                          m == 1 ? r : level[cur ^ 1]);

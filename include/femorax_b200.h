@@ -186,6 +186,9 @@ int fx_apply_operator_f32(fx_force* f, fx_coeffs k, const float* x, float* y, vo
 int fx_apply_operator_host(fx_force* f, fx_coeffs k, const double* x_host, double* y_host, void* stream);
 /* d = diag(K_eff) (InternalForce::operator_diagonal, internal_force.cpp:575-599). */
 int fx_operator_diagonal(fx_force* f, fx_coeffs k, double* d, void* stream);
+/* The same diagonal into a HOST vector (Jacobi::setup of a solver whose vectors live on the host,
+ * jacobi.cpp:10-26): computed on the device, copied out; returns after the copy. */
+int fx_operator_diagonal_host(fx_force* f, fx_coeffs k, double* d_host, void* stream);
 /* f = f_int(u) + Rayleigh damping forces at v + nodal alphaM M v (InternalForce::compute,
  * internal_force.cpp:354-377). u, v, f device FP64. */
 int fx_force_compute(fx_force* f, const double* u, const double* v, double* out, void* stream);
@@ -224,7 +227,9 @@ void fx_vops_destroy(fx_vops* v);
  * given, and to *result_host (after a stream synchronisation) when given. */
 int fx_vops_dot(fx_vops* v, const double* x, const double* y, int64_t n, double* result_dev, double* result_host,
                 void* stream);
-/* x.y of n entries on the current device, in the same order and with the same bits as
+/* x.y of n entries on the current device (x and y must be that device's memory, or managed
+ * memory; others are rejected with FX_E_INVALID, and `stream` must belong to that device), in the
+ * same order and with the same bits as
  * fx_vops_dot with the same lanes, but allocating nothing: no cudaMalloc, no cudaFree and no
  * allocating library routine. It has no counterpart in the reference. It is for callers that
  * must not allocate device memory: an application that hands all of the GPU's memory to its own

@@ -36,6 +36,8 @@ def build(reference_dir: str = None) -> None:
     subprocess.run(["make", "-s", "-j8", "port"], cwd=HERE, check=True)
     if have:
         subprocess.run(["make", "-s", "-j8", "ref", f"REF={reference_dir}"], cwd=HERE, check=True)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "femorax_b200", "libfemorax_b200.so")):
+            subprocess.run(["make", "-s", "adapter", f"REF={reference_dir}"], cwd=HERE, check=True)
 
 
 def have_ref() -> bool:
@@ -100,7 +102,7 @@ def ref():
         L.fxref_force_set_stage.argtypes = [vp, C.c_int32, C.c_int32]
         L.fxref_force_commit.argtypes = [vp]
         L.fxref_apply_operator_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64, p_f64]
-        L.fxref_operator_diagonal_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, p_f64, p_f64]
+        L.fxref_operator_diagonal_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64]
         L.fxref_pimy_destroy.argtypes = [vp]
         L.fxref_pimy_nstate.restype = C.c_int32
         L.fxref_pimy_setup_values.argtypes = [vp, p_f64]
@@ -278,10 +280,10 @@ class RefForce:
             raise RuntimeError(ref().fxref_last_error().decode())
         return y
 
-    def operator_diagonal_at(self, k, u):
+    def operator_diagonal_at(self, k, u, initial=False):
         u, pu = _f(u)
         d = np.zeros(self.n)
-        rc = ref().fxref_operator_diagonal_at(self.h, k[0], k[1], k[2], pu, d.ctypes.data_as(p_f64))
+        rc = ref().fxref_operator_diagonal_at(self.h, k[0], k[1], k[2], int(initial), pu, d.ctypes.data_as(p_f64))
         if rc:
             raise RuntimeError(ref().fxref_last_error().decode())
         return d

@@ -418,11 +418,12 @@ int fxref_apply_operator_at(fxref_force* h, double cK, double cC, double cM, int
     return fail(e);
   }
 }
-int fxref_operator_diagonal_at(fxref_force* h, double cK, double cC, double cM, const double* u, double* d) {
+int fxref_operator_diagonal_at(fxref_force* h, double cK, double cC, double cM, int initial, const double* u,
+                               double* d) {
   try {
     exec::Vec uu("u", static_cast<std::size_t>(h->neq));
     const exec::OperatorSettings s = stored_at(h, u, uu);
-    h->f->operator_diagonal(OperatorCoefficients{cK, cC, cM, false}, s, uu, wrap(d, h->neq));
+    h->f->operator_diagonal(OperatorCoefficients{cK, cC, cM, initial != 0}, s, uu, wrap(d, h->neq));
     return 0;
   } catch (const std::exception& e) {
     return fail(e);

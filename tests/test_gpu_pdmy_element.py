@@ -3,7 +3,10 @@ reference's own InternalForce with the same material (oracle/_ref), step by step
 elastic stage, the switch to the plastic stage, cyclic shear with commits. Force, operator (each
 point's stored tangent at that displacement, upper triangle mirrored as the reference stores it)
 and diagonal within 1e-10 of their largest entries: the device's pow (the modulus factor of every
-update) may differ from the host's in the last place, so this material is not held bit for bit."""
+update) may differ from the host's in the last place, so this material is not held bit for bit.
+Damped cases: alphaM with betaK (each point's current tangent) and betaKcomm (its committed one);
+betaKcomm alone; and ModifiedNewton -initial with damping, where the stiffness term takes the
+material's initial tangent and betaK damping stays on the current one (element_operator.hpp:45-56)."""
 import numpy as np
 import pytest
 
@@ -24,12 +27,14 @@ LIQ = (1.9469928644240571, 75000.0, 162499.99999999997, 29.0, 0.1, 80.0, 0.5, 29
        1.0, 20.0, 0.85, 0.9, 0.02, 0.7, 101.0, 0.3, 0.0, 1.0)
 
 
-def column(p, damped=False):
+def column(p, damping=None):
     G, K = p[1], p[2]
     E, nu = 9 * K * G / (3 * K + G), (3 * K - 2 * G) / (2 * (3 * K + G))
     spec = meshes.box_model(2, 2, 5, size=(1.0, 1.0, 2.5), E=E, nu=nu, rho=p[0])
     spec.groups[0].pdmy = (np.array(p), None)
-    if damped:  # Rayleigh damping, betaK through each point's current tangent, betaKcomm its committed one
+    if damping == "comm":  # betaKcomm alone: each point's committed tangent
+        spec.rayleigh = [meshes.Rayleigh(0.0, 0.0, 0.0, 0.001, spec.groups[0].etags)]
+    elif damping:  # Rayleigh damping, betaK through each point's current tangent, betaKcomm its committed one
         spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.001, spec.groups[0].etags)]
     return spec
 
@@ -38,12 +43,15 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.mark.parametrize("p,damped", [(SAND, False), (LIQ, False), (SAND, True)],
-                         ids=["dense_sand", "loose_sand_ppz", "dense_sand_damped"])
-def test_column_path_matches_reference(p, damped, oracle_mod, ref_available):
+@pytest.mark.parametrize("p,damping", [(SAND, None), (LIQ, None), (SAND, "full"), (LIQ, "comm"), (SAND, "initial")],
+                         ids=["dense_sand", "loose_sand_ppz", "dense_sand_damped", "loose_sand_betaKcomm",
+                              "dense_sand_damped_initial"])
+def test_column_path_matches_reference(p, damping, oracle_mod, ref_available):
     if not ref_available:
         pytest.skip("the reference build is not available")
-    spec = column(p, damped)
+    spec = column(p, damping)
+    damped = damping is not None
+    initial = damping == "initial"
     mesh = fx.Model(spec).compile().mesh()
     force = fx.InternalForce(mesh)
     force.set_pdmy(0, fx.PressureDependMultiYield(*p[:14], noYieldSurf=int(p[14]), e=p[15], cs1=p[16], cs2=p[17],
@@ -76,11 +84,11 @@ def test_column_path_matches_reference(p, damped, oracle_mod, ref_available):
         assert rel(f.cpu().numpy(), ref.force(u, v)) <= 1e-10, step
         x = rng.standard_normal(n)
         y = torch.zeros(n, dtype=torch.float64, device=DEV)
-        force.apply_operator(fx.OperatorCoefficients(*k), torch.as_tensor(x, device=DEV), y)
-        assert rel(y.cpu().numpy(), ref.apply_operator_at(k, u, x)) <= 1e-10, step
+        force.apply_operator(fx.OperatorCoefficients(*k, initial=initial), torch.as_tensor(x, device=DEV), y)
+        assert rel(y.cpu().numpy(), ref.apply_operator_at(k, u, x, initial=initial)) <= 1e-10, step
         dg = torch.zeros(n, dtype=torch.float64, device=DEV)
-        force.operator_diagonal(fx.OperatorCoefficients(*k), dg)
-        assert rel(dg.cpu().numpy(), ref.operator_diagonal_at(k, u)) <= 1e-10, step
+        force.operator_diagonal(fx.OperatorCoefficients(*k, initial=initial), dg)
+        assert rel(dg.cpu().numpy(), ref.operator_diagonal_at(k, u, initial=initial)) <= 1e-10, step
         if step >= 3:
             plastic_seen = max(plastic_seen, force.plastic_points())
         force.commit_state()

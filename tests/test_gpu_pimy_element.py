@@ -5,7 +5,8 @@ shear with commits. At every step the internal force, the operator y = K_t x + c
 point's tangent at that displacement (the reference's TangentSource::Recomputed) and its diagonal
 agree within 1e-12 of their largest entries, and bit for bit for the materials whose update calls
 no pow (friction angle 0); the plastic stage yields points. One case carries Rayleigh damping
-(alphaM; betaK through each point's current tangent, betaKcomm through its committed one)."""
+(alphaM; betaK through each point's current tangent, betaKcomm through its committed one), one
+betaKcomm alone. ModifiedNewton -initial is refused on these sets, as the reference refuses it."""
 import numpy as np
 import pytest
 
@@ -22,6 +23,7 @@ BACKBONE = [1e-05, 0.98, 3e-05, 0.95, 0.0001, 0.85, 0.0003, 0.65, 0.001, 0.35, 0
 MATERIALS = {
     "clay": ((1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0), None),
     "clay_damped": ((1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0), None),
+    "sand_betaKcomm": ((2.0, 60000.0, 150000.0, 5.0, 0.1, 30.0, 80.0, 0.5, 20.0), None),
     "sand": ((2.0, 60000.0, 150000.0, 5.0, 0.1, 30.0, 80.0, 0.5, 20.0), None),
     "backbone_clay": ((1.8, 40500.0, 108000.0, 10.0, 0.1, 0.0, 100.0, 0.0, 8.0), BACKBONE),
 }
@@ -35,6 +37,8 @@ def column(name):
     spec.groups[0].pimy = (np.array(in9), None if pairs is None else np.array(pairs))
     if name.endswith("_damped"):  # stiffness-proportional damping, current and committed tangents
         spec.rayleigh = [meshes.Rayleigh(0.05, 0.002, 0.0, 0.001, spec.groups[0].etags)]
+    elif name.endswith("_betaKcomm"):  # betaKcomm alone: each point's committed tangent
+        spec.rayleigh = [meshes.Rayleigh(0.0, 0.0, 0.0, 0.001, spec.groups[0].etags)]
     return spec
 
 
@@ -71,7 +75,7 @@ def test_column_path_matches_reference(name, oracle_mod, ref_available):
             dof[q[ok]] = d
     rng = np.random.default_rng(21)
     noise = rng.standard_normal(n) * 2e-5
-    damped = name.endswith("_damped")
+    damped = name.endswith(("_damped", "_betaKcomm"))
     k = (1.0, 0.3, 0.5) if damped else (1.0, 0.0, 0.5)
     bitwise = in9[5] == 0.0
     plastic_seen = 0
@@ -128,6 +132,11 @@ def test_binding_rules():
     with pytest.raises(fx.FxError) as e:  # no FP32 form of these tangents
         force.apply_operator(fx.OperatorCoefficients(), x, y)
     assert e.value.code == 2
+    x64, y64 = x.double(), y.double()
+    for call in (lambda k: force.apply_operator(k, x64, y64), lambda k: force.operator_diagonal(k, y64)):
+        with pytest.raises(fx.FxError) as e:  # ModifiedNewton -initial (src/io/support.cpp:120-127)
+            call(fx.OperatorCoefficients(initial=True))
+        assert e.value.code == 2
     spec = column("clay")
     spec.rayleigh = [meshes.Rayleigh(0.0, 0.0, 0.001, 0.0, spec.groups[0].etags)]
     with pytest.raises(fx.FxError):  # betaKinit damping on the set (the reference refuses it too)
