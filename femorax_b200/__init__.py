@@ -328,6 +328,36 @@ class InternalForce:
         check(lib().fx_min_critical_dt(self._h, 1 if scheme == "ExplicitDifference" else 0, C.byref(dt)))
         return dt.value
 
+    def element_critical_dts(self, scheme: str = "ExplicitDifference"):
+        """Every element's stable step (InternalForce::element_critical_dts), a device FP64 tensor
+        in batch order."""
+        import torch
+        out = torch.zeros(max(self.mesh.count, 1), dtype=torch.float64, device=torch.device("cuda", self.device))
+        check(lib().fx_element_critical_dts(self._h, 1 if scheme == "ExplicitDifference" else 0, _ptr(out), None))
+        return out[:self.mesh.count]
+
+    def stability_may_change(self) -> bool:
+        out = C.c_int32()
+        check(lib().fx_stability_may_change(self._h, C.byref(out)))
+        return bool(out.value)
+
+    def prepare_stability_bounds(self, stream=None):
+        check(lib().fx_stability_prepare(self._h, _stream(stream)))
+
+    def min_critical_dt_bound(self, scheme: str = "ExplicitDifference", stream=None) -> float:
+        dt = C.c_double()
+        check(lib().fx_min_critical_dt_bound(self._h, 1 if scheme == "ExplicitDifference" else 0, C.byref(dt),
+                                             _stream(stream)))
+        return dt.value
+
+    def set_explicit_checks(self, nan_check_interval: int = 100, stable_step_check_interval: int = 100,
+                            allow_unstable_dt: bool = False):
+        """The checks of later explicit stages (exec::RunOptions): non-finite displacements every
+        nan_check_interval steps and at the end of each call (FX_E_DIVERGED), the stable step at
+        the start and every stable_step_check_interval steps where it can change (FX_E_UNSTABLE)."""
+        check(lib().fx_explicit_checks(self._h, nan_check_interval, stable_step_check_interval,
+                                       1 if allow_unstable_dt else 0))
+
     def explicit_run(self, mass, u, vh, a, v, dt, steps, ag=None, direction=0, record_eq=None, stream=None):
         """`steps` ExplicitDifference steps (explicit_analysis.cpp:62-84, 687-705) with ground
         acceleration ag[step] (host array) in `direction`; returns the recorded acceleration

@@ -18,6 +18,7 @@ FX_E_NOT_SPD = 4
 FX_E_DIVERGED = 5
 FX_E_TIMEOUT = 6
 FX_E_CUDA = 7
+FX_E_UNSTABLE = 8
 
 FX_MAT_ELASTIC = 0
 FX_MAT_J2 = 1
@@ -109,6 +110,11 @@ PROTOTYPES = {
     "fx_force_compute_f32": (C.c_int, [vp, vp, vp, vp, vp]),
     "fx_mass_times_ground": (C.c_int, [vp, C.c_int32, vp, vp]),
     "fx_min_critical_dt": (C.c_int, [vp, C.c_int32, p_f64]),
+    "fx_element_critical_dts": (C.c_int, [vp, C.c_int32, vp, vp]),
+    "fx_stability_may_change": (C.c_int, [vp, p_i32]),
+    "fx_stability_prepare": (C.c_int, [vp, vp]),
+    "fx_min_critical_dt_bound": (C.c_int, [vp, C.c_int32, p_f64, vp]),
+    "fx_explicit_checks": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
     "fx_force_commit": (C.c_int, [vp, vp]),
     "fx_force_plastic_points": (C.c_int, [vp, p_i64]),
     "fx_vops_create": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]),

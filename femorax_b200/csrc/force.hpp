@@ -153,6 +153,16 @@ struct ExplicitWork {
   DeviceArray<double> w64;  // w = u + beta v of the next force evaluation (box path)
   DeviceArray<float> w32;
   int carry_scheme = -1;
+  // the stage's checks (exec::RunOptions nan_check_interval and stable_step_check_interval, the
+  // stage's allow_unstable_dt; 0 turns a periodic check off) and their progress: steps taken in
+  // the stage so far (resumed calls continue it), the start's stable step, whether the re-check
+  // runs and whether an allowed unstable step was met
+  int32_t nan_interval = 100, stable_interval = 100;
+  bool allow_unstable = false;
+  int64_t stage_step = 0;
+  double stage_dt_crit = 0.0;
+  bool recheck = false, warned = false;
+  DeviceArray<int> bad;  // non-finite count
 };
 
 struct ForceState {
@@ -205,6 +215,11 @@ struct ForceState {
   // unallocated (NULL) when no soil set is damped
   DeviceArray<double> soil_sd;
   ExplicitWork xw;
+  // stable time step: the minimum's key (general.cu) and, for the periodic re-check, each
+  // element's omega^2 with its reference stability tangent (prepare_stability_bounds)
+  DeviceArray<unsigned long long> dt_key;
+  DeviceArray<double> w2_ref;
+  bool bounds_ready = false;
   bool use_box() const { return box.qualifies && path != FX_PATH_GENERAL; }
   bool use_box_force() const { return use_box() && box.force_ok; }
   int64_t device_bytes() const;
@@ -219,6 +234,17 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
 void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st);
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
+// Stable explicit step on the device (one warp per element, the reference's eigen-solve bit for
+// bit): the minimum over the elements of `list` (all elements when NULL, n of them), each
+// element's step into dt_out when given (device, n values). scheme 0 CentralDifference, 1
+// ExplicitDifference.
+double general_min_critical_dt(ForceState& s, int scheme, const int32_t* list, int32_t n, double* dt_out,
+                               cudaStream_t st);
+// the periodic re-check: whether a set's stable step can change during a stage (the multi-yield
+// soils), each element's reference omega^2 (once per stage), and the bound from the points' factors
+bool stability_may_change(const ForceState& s);
+void prepare_stability_bounds(ForceState& s, cudaStream_t st);
+double min_critical_dt_bound(ForceState& s, int scheme, cudaStream_t st);
 // commitState of the multi-yield soil points (PressureIndependMultiYield: copy-on-write surfaces;
 // PressureDependMultiYield: the whole trial state)
 void pimy_commit(ForceState& s, cudaStream_t st);

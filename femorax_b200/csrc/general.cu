@@ -7,6 +7,8 @@
 // This is the reference's deterministic gather scatter (src/exec/assembly.hpp:25-55,
 // assembly.cpp:28-38, pair order internal_force.cpp:121-134). Built with --fmad=false, its sums
 // are the reference host build's sums bit for bit.
+#include <cstring>
+
 #include "force.hpp"
 
 namespace fx {
@@ -345,6 +347,218 @@ __global__ void __launch_bounds__(256) k_gather32(const int32_t* __restrict__ st
   y[q] = sum;
 }
 
+// ---- stable time step (StdBrick::max_omega_sq_with, std_brick.hpp:658-688; the element's
+// largest omega^2 of K phi = omega^2 M phi with the lumped mass, by the cyclic Jacobi rotations of
+// src/physics/common/sym_eigen.hpp; stable_dt, src/physics/explicit_stability.hpp:16-32).
+// One warp per element: the lanes assemble the 24 x 24 matrix M^-1/2 K M^-1/2 in shared memory
+// (two of the 64 node pairs each, the Gauss points summed in the reference's order), then apply
+// the rotations in the reference's (p, q) order, lane k updating entry k of the two rows and
+// columns: each entry sees the reference's operations, so omega^2 is the reference's bit for bit.
+constexpr int kDtWarps = 4;
+
+// The stable step's material matrix of point gp (contracts.hpp, stability_tangent): the elastic
+// matrix for elastic and J2 sets (J2 unloads elastically); for the multi-yield soils the elastic
+// moduli at the committed state (PressureIndependMultiYield::stability_tangent,
+// pressure_independ_multi_yield.hpp:170-201; PressureDependMultiYield::stability_tangent,
+// pressure_depend_multi_yield.hpp:203-218), or with `reference` their reference tangent
+// (stability_reference: the ScaledStability bound's per-element eigenvalue).
+__device__ void stability_D(const ParamGP& p, const PimySet* __restrict__ pimy, const PdmySet* __restrict__ pdmy,
+                            const double* __restrict__ pcs, const double* __restrict__ dcs, int64_t P, int32_t e,
+                            int gp, bool reference, double D[6][6]) {
+  if (p.kind == 2) {
+    const PimySet& m = pimy[p.table];
+    double G = m.p.G0, K = m.p.K0;
+    if (!reference) {
+      const pimy::Slab<const double> c{pcs + e + static_cast<int64_t>(gp) * P, 8 * P};
+      G = c[pimy::S_G];
+      K = c[pimy::S_K];
+      if (m.stage == 1 && c[pimy::S_E2P] == 0.0 && m.p.phi != 0.) {
+        double vol = c[pimy::S_STRESS + 12];
+        if (vol > 0.) vol = 0.;  // elast2Plast drops the tension first
+        const double con = -(vol - m.p.p_res);
+        const double scale = pow(-con / (m.p.pref - m.p.p_res), m.p.n_press);
+        G *= scale;
+        K *= scale;
+      }
+    }
+    double d[36];
+    pimy::elastic_D(G, K, d);
+    for (int a = 0; a < 36; ++a) D[a / 6][a % 6] = d[a];
+  } else if (p.kind == 3) {
+    const PdmySet& m = pdmy[p.table];
+    double f = 1.0;
+    if (!reference && m.stage == 1) {
+      const pimy::Slab<const double> c{dcs + e + static_cast<int64_t>(gp) * P, 8 * P};
+      const double h = c[pdmy::S_STRESS + 12] - m.p.p_res;  // getModulusFactor of the committed stress
+      f = pow(h / (m.p.pref - m.p.p_res), m.p.n_press);
+      f = (1.e-10 > f) ? 1.e-10 : f;
+    }
+    double d[36];
+    pdmy::elastic_D(m.p, f, d);
+    for (int a = 0; a < 36; ++a) D[a / 6][a % 6] = d[a];
+  } else {
+    elastic_D(p, D);
+  }
+}
+
+__device__ __forceinline__ double stable_dt_of(int scheme, const ParamGP& p, double w2) {
+  if (!(w2 > 0.0)) return INFINITY;
+  const double w = sqrt(w2);
+  if (scheme == 0) return 2.0 / w;
+  const double beta = p.betaK + p.betaKinit + p.betaKcomm;
+  const double c = p.alphaM + beta * w2;
+  return 4.0 / (sqrt(c * c + 4.0 * w2) + c);
+}
+
+// dt >= 0 (or +inf) as an unsigned key that orders as the values do: atomicMin over keys is the
+// minimum, exactly and in any order.
+__device__ __forceinline__ void min_dt(unsigned long long* out, double dt) {
+  atomicMin(out, static_cast<unsigned long long>(__double_as_longlong(dt)));
+}
+
+// Per element (list[i], or i without a list): omega^2 into w2_out, its stable step into dt_out,
+// the minimum step into *dt_min (each optional).
+__global__ void __launch_bounds__(32 * kDtWarps)
+    k_element_omega_sq(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                       const int32_t* __restrict__ param, const ParamGP* __restrict__ params, int32_t N, int32_t P,
+                       const int32_t* __restrict__ list, int32_t n, const PimySet* __restrict__ pimy,
+                       const PdmySet* __restrict__ pdmy, const double* __restrict__ pcs,
+                       const double* __restrict__ dcs, int reference, int scheme, double* __restrict__ w2_out,
+                       double* __restrict__ dt_out, unsigned long long* __restrict__ dt_min) {
+  __shared__ double As[kDtWarps][24][25];  // a padded row: the column updates touch 24 banks
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  double(*A)[25] = As[wp];
+  for (int32_t i = blockIdx.x * kDtWarps + wp; i < n; i += gridDim.x * kDtWarps) {
+    const int32_t e = list ? list[i] : i;
+    const ParamGP p = params[param[e]];
+    double xl[3][8], m[8];
+    load_coords(coords, node, N, P, e, xl);
+    lumped_mass(p, xl, m);
+    double acc[2][3][3];
+    for (int h = 0; h < 2; ++h)
+      for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) acc[h][a][c] = 0.0;
+    for (int gp = 0; gp < 8; ++gp) {
+      PointShape s;
+      point_shape(xl, gp, s);
+      double D[6][6];
+      stability_D(p, pimy, pdmy, pcs, dcs, P, e, gp, reference != 0, D);
+      for (int h = 0; h < 2; ++h) {
+        const int q = lane + 32 * h;
+        double blk[3][3];
+        block_tangent(s, D, q >> 3, q & 7, blk);
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) acc[h][a][c] += blk[a][c];
+      }
+    }
+    bool massless = false;
+    double ism[8];
+    for (int j = 0; j < 8; ++j) {
+      if (!(m[j] > 0.0)) massless = true;
+      ism[j] = massless ? 0.0 : 1.0 / sqrt(m[j]);
+    }
+    double w2 = 0.0;  // a massless element sets no limit
+    if (!massless) {
+      for (int h = 0; h < 2; ++h) {
+        const int q = lane + 32 * h, j = q >> 3, k = q & 7;
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) A[3 * j + a][3 * k + c] = acc[h][a][c] * (ism[j] * ism[k]);
+      }
+      __syncwarp();
+      for (int sweep = 0; sweep < 60; ++sweep) {
+        int stop = 0;
+        if (lane == 0) {
+          double off = 0.0, dg = 0.0;
+          for (int r = 0; r < 24; ++r) {
+            dg += A[r][r] * A[r][r];
+            for (int c = r + 1; c < 24; ++c) off += A[r][c] * A[r][c];
+          }
+          stop = off <= 1e-30 * dg || off == 0.0;
+        }
+        if (__shfl_sync(0xffffffffu, stop, 0)) break;
+        for (int pp = 0; pp < 23; ++pp)
+          for (int qq = pp + 1; qq < 24; ++qq) {
+            const double apq = A[pp][qq];
+            if (apq == 0.0) continue;  // the same value in every lane
+            const double theta = (A[qq][qq] - A[pp][pp]) / (2.0 * apq);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            const double c = 1.0 / sqrt(t * t + 1.0);
+            const double sn = t * c;
+            __syncwarp();  // every lane has read the pivot entries
+            if (lane < 24) {  // A <- A J
+              const double akp = A[lane][pp], akq = A[lane][qq];
+              A[lane][pp] = c * akp - sn * akq;
+              A[lane][qq] = sn * akp + c * akq;
+            }
+            __syncwarp();
+            if (lane < 24) {  // A <- J^T A
+              const double apk = A[pp][lane], aqk = A[qq][lane];
+              A[pp][lane] = c * apk - sn * aqk;
+              A[qq][lane] = sn * apk + c * aqk;
+            }
+            __syncwarp();
+            if (lane == 0) A[pp][qq] = A[qq][pp] = 0.0;
+            __syncwarp();
+          }
+      }
+      w2 = A[0][0];
+      for (int r = 1; r < 24; ++r) w2 = A[r][r] > w2 ? A[r][r] : w2;
+      __syncwarp();  // the next element reuses A
+    }
+    if (lane == 0) {
+      if (w2_out) w2_out[i] = w2;
+      const double dt = stable_dt_of(scheme, p, w2);
+      if (dt_out) dt_out[i] = dt;
+      if (dt_min) min_dt(dt_min, dt);
+    }
+  }
+}
+
+// The periodic re-check's bound (StdBrick::max_omega_sq_bound, std_brick.hpp:645-656): for the
+// multi-yield soil sets the largest stability factor of the element's points times its reference
+// omega^2, a hair above (never below the element's omega^2); the other sets keep w2_ref, their
+// exact omega^2 (their stable tangent does not change). One thread per element of the list.
+__global__ void k_element_dt_bound(const int32_t* __restrict__ param, const ParamGP* __restrict__ params, int32_t P,
+                                   const int32_t* __restrict__ list, int32_t n, const PimySet* __restrict__ pimy,
+                                   const PdmySet* __restrict__ pdmy, const double* __restrict__ pcs,
+                                   const double* __restrict__ dcs, const double* __restrict__ w2_ref, int scheme,
+                                   unsigned long long* __restrict__ dt_min) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t e = list ? list[i] : i;
+  const ParamGP p = params[param[e]];
+  double w2 = w2_ref[i];
+  if (p.kind >= 2) {
+    double sc = 0.0;
+    for (int gp = 0; gp < 8; ++gp) {
+      double si;
+      if (p.kind == 2) {
+        const PimySet& m = pimy[p.table];
+        const pimy::Slab<const double> c{pcs + e + static_cast<int64_t>(gp) * P, 8 * P};
+        double G = c[pimy::S_G];  // stability_scale: the stability modulus over the reference one
+        if (m.stage == 1 && c[pimy::S_E2P] == 0.0 && m.p.phi != 0.) {
+          double vol = c[pimy::S_STRESS + 12];
+          if (vol > 0.) vol = 0.;
+          const double con = -(vol - m.p.p_res);
+          G *= pow(-con / (m.p.pref - m.p.p_res), m.p.n_press);
+        }
+        si = G / m.p.G0;
+      } else {
+        const PdmySet& m = pdmy[p.table];
+        si = 1.0;
+        if (m.stage == 1) {
+          const pimy::Slab<const double> c{dcs + e + static_cast<int64_t>(gp) * P, 8 * P};
+          si = pow((c[pdmy::S_STRESS + 12] - m.p.p_res) / (m.p.pref - m.p.p_res), m.p.n_press);
+          si = (1.e-10 > si) ? 1.e-10 : si;
+        }
+      }
+      sc = si > sc ? si : sc;
+    }
+    w2 = sc * w2 * (1.0 + 1e-12);
+  }
+  min_dt(dt_min, stable_dt_of(scheme, p, w2));
+}
+
 }  // namespace
 
 void general_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st, const int* skip) {
@@ -489,6 +703,69 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
   if (s.has_nodal_mass && s.neq > 0)
     k_ground_nodal<<<grid_for(s.neq, 256), 256, 0, st>>>(s.nodal_mass.ptr, s.eq_dof.ptr, s.neq, dir, y);
   FX_LAUNCH_CHECK("ground_mass");
+}
+
+
+namespace {
+unsigned long long* dt_min_slot(ForceState& s) {
+  if (s.dt_key.n == 0) s.dt_key.alloc(1);
+  return s.dt_key.ptr;
+}
+double read_dt_min(ForceState& s, cudaStream_t st) {
+  unsigned long long key = 0;
+  FX_CUDA(cudaMemcpyAsync(&key, s.dt_key.ptr, sizeof(key), cudaMemcpyDeviceToHost, st));
+  FX_CUDA(cudaStreamSynchronize(st));
+  double dt;
+  static_assert(sizeof(dt) == sizeof(key), "64-bit keys");
+  std::memcpy(&dt, &key, sizeof(dt));
+  return dt;
+}
+void reset_dt_min(ForceState& s, cudaStream_t st) {
+  const double inf = INFINITY;
+  unsigned long long key;
+  std::memcpy(&key, &inf, sizeof(key));
+  FX_CUDA(cudaMemcpyAsync(dt_min_slot(s), &key, sizeof(key), cudaMemcpyHostToDevice, st));
+}
+unsigned dt_grid(int32_t n) {
+  const int64_t blocks = (static_cast<int64_t>(n) + kDtWarps - 1) / kDtWarps;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, static_cast<int64_t>(num_sms()) * 16)));
+}
+}  // namespace
+
+double general_min_critical_dt(ForceState& s, int scheme, const int32_t* list, int32_t n, double* dt_out,
+                               cudaStream_t st) {
+  reset_dt_min(s, st);
+  if (n > 0)
+    k_element_omega_sq<<<dt_grid(n), 32 * kDtWarps, 0, st>>>(
+        s.coords.ptr, s.node.ptr, s.param.ptr, s.params.ptr, s.N, s.P, list, n, s.pimy_dev.ptr, s.pdmy_dev.ptr,
+        s.pimy_committed.ptr, s.pdmy_committed.ptr, 0, scheme, nullptr, dt_out, s.dt_key.ptr);
+  FX_LAUNCH_CHECK("element_critical_dt");
+  return read_dt_min(s, st);
+}
+
+bool stability_may_change(const ForceState& s) { return s.has_pimy || s.has_pdmy; }
+
+void prepare_stability_bounds(ForceState& s, cudaStream_t st) {
+  const int32_t n = s.count;
+  if (s.w2_ref.n < static_cast<size_t>(std::max(n, 1))) s.w2_ref.alloc(static_cast<size_t>(std::max(n, 1)));
+  if (n > 0)
+    k_element_omega_sq<<<dt_grid(n), 32 * kDtWarps, 0, st>>>(
+        s.coords.ptr, s.node.ptr, s.param.ptr, s.params.ptr, s.N, s.P, nullptr, n, s.pimy_dev.ptr, s.pdmy_dev.ptr,
+        s.pimy_committed.ptr, s.pdmy_committed.ptr, 1, 0, s.w2_ref.ptr, nullptr, nullptr);
+  FX_LAUNCH_CHECK("element_reference_omega_sq");
+  s.bounds_ready = true;
+}
+
+double min_critical_dt_bound(ForceState& s, int scheme, cudaStream_t st) {
+  if (!s.bounds_ready) throw Error(FX_E_INVALID, "the stability bounds are not prepared (fx_stability_prepare)");
+  reset_dt_min(s, st);
+  if (s.count > 0)
+    k_element_dt_bound<<<grid_for(s.count, 256), 256, 0, st>>>(s.param.ptr, s.params.ptr, s.P, nullptr, s.count,
+                                                                s.pimy_dev.ptr, s.pdmy_dev.ptr, s.pimy_committed.ptr,
+                                                                s.pdmy_committed.ptr, s.w2_ref.ptr, scheme,
+                                                                s.dt_key.ptr);
+  FX_LAUNCH_CHECK("element_dt_bound");
+  return read_dt_min(s, st);
 }
 
 }  // namespace fx

@@ -235,6 +235,16 @@ __global__ void k_stage_cd_solve(const double* __restrict__ f, const double* __r
   }
 }
 
+// Non-finite displacements (explicit_analysis.cpp:369-378, all_finite): a count, exact in any order.
+__global__ void k_count_nonfinite(const double* __restrict__ u, int64_t n, int* __restrict__ bad) {
+  int local = 0;
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    local += isfinite(u[q]) ? 0 : 1;
+  local = __reduce_add_sync(0xffffffffu, local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(bad, local);
+}
+
 __global__ void k_newmark_predict(double* __restrict__ u, double* __restrict__ v, double* __restrict__ a,
                                   double* __restrict__ ut, double* __restrict__ vt, double* __restrict__ at, double a1,
                                   double a2, double a3, double a4, int64_t n) {
@@ -498,6 +508,40 @@ struct fx_motions {
 
 namespace {
 
+// Smallest stable step of the elements (InternalForce::min_critical_dt): on a box grid of elastic
+// or J2 sets, whose elements of one parameter set are congruent, one eigenproblem per set on the
+// host; otherwise every element's on the device (general_min_critical_dt).
+double exact_min_dt(fx::ForceState& s, int scheme, cudaStream_t st) {
+  using namespace fx;
+  if (!s.box.qualifies || s.has_pimy || s.has_pdmy) return general_min_critical_dt(s, scheme, nullptr, s.count, nullptr, st);
+  double best = 1e300;
+  std::vector<char> seen(static_cast<size_t>(s.nparams), 0);
+  for (int32_t e = 0; e < s.count; ++e) {
+    const int32_t pi = s.param_h[e];
+    if (seen[pi]) continue;
+    seen[pi] = 1;
+    double xl[3][8];
+    for (int a = 0; a < 8; ++a) {
+      const int32_t nd = s.node_h[static_cast<size_t>(a) * s.P + e];
+      for (int d = 0; d < 3; ++d) xl[d][a] = s.coords_h[static_cast<size_t>(d) * s.N + nd];
+    }
+    const ParamGP& p = s.params_h[pi];
+    best = std::min(best, stable_dt(scheme, p, element_omega_sq(p, xl)));
+  }
+  return best;
+}
+
+int count_nonfinite(fx::ExplicitWork& w, const double* u, int64_t n, cudaStream_t st) {
+  if (w.bad.n == 0) w.bad.alloc(1);
+  FX_CUDA(cudaMemsetAsync(w.bad.ptr, 0, sizeof(int), st));
+  if (n > 0) fx::k_count_nonfinite<<<fx::ew(n), 256, 0, st>>>(u, n, w.bad.ptr);
+  FX_LAUNCH_CHECK("nan_check");
+  int bad = 0;
+  FX_CUDA(cudaMemcpyAsync(&bad, w.bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FX_CUDA(cudaStreamSynchronize(st));
+  return bad;
+}
+
 // An explicit stage (src/exec/explicit_analysis.cpp:665-725 without local time stepping, exact
 // constraints, DRM or recorders). Per ExplicitDifference step: [motions: time += dt, ag(time)]
 // [force at (u, vh)] [ed_correct + the next ed_predict] [commit]; per CentralDifference step:
@@ -533,6 +577,19 @@ void explicit_stage(fx_force* f, int scheme, const double* mass, const double* c
     FX_CUDA(cudaMemcpyAsync(carry, scheme == 1 ? v : u, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   }
   w.carry_scheme = scheme;
+  if (!resume) {  // the stage's stable step against dt (explicit_analysis.cpp:582-653)
+    w.stage_step = 0;
+    w.warned = false;
+    w.stage_dt_crit = exact_min_dt(s, scheme, st);
+    if (dt > w.stage_dt_crit) {
+      if (!w.allow_unstable)
+        throw Error(FX_E_UNSTABLE, "fx_explicit_stage: dt = " + std::to_string(dt) + " is above the stable step " +
+                                       std::to_string(w.stage_dt_crit) + " (reduce dt, or allow an unstable dt)");
+      w.warned = true;
+    }
+    w.recheck = w.stable_interval > 0 && stability_may_change(s);
+    if (w.recheck) prepare_stability_bounds(s, st);
+  }
   if (steps == 0) {
     FX_CUDA(cudaStreamSynchronize(st));
     return;
@@ -589,28 +646,78 @@ void explicit_stage(fx_force* f, int scheme, const double* mass, const double* c
   }
   st = cs;
   cudaGraphExec_t exec = nullptr;
-  while (done < steps) {
-    if (steps - done > block) {
-      if (!exec) {
-        cudaGraph_t g = nullptr;
-        FX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < block; ++i) one_step(1);
-        FX_CUDA(cudaStreamEndCapture(st, &g));
-        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
-        cudaGraphDestroy(g);
-        FX_CUDA(e);
+  // the periodic checks (explicit_analysis.cpp:732-765) after the steps whose stage index is a
+  // multiple of their interval: the steps run in pieces that end there
+  auto to_next = [&](int32_t interval, int64_t k) -> int64_t {
+    return interval > 0 ? interval - k % interval : INT64_MAX;
+  };
+  auto finish = [&]() {  // the stage time back to the host; the private stream released
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    FX_CUDA(cudaMemcpyAsync(time, w.time.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+    FX_CUDA(cudaStreamSynchronize(st));
+    if (own_stream) cudaStreamDestroy(cs);
+    own_stream = false;
+  };
+  std::string failure;
+  int failure_code = FX_OK;
+  auto checks = [&](int64_t k) {  // after stage step k
+    if (w.recheck && w.stable_interval > 0 && k % w.stable_interval == 0) {
+      // the bound never overstates the step; where it falls below dt the exact check decides
+      double dtc = min_critical_dt_bound(s, scheme, st);
+      if (dt > dtc) dtc = general_min_critical_dt(s, scheme, nullptr, s.count, nullptr, st);
+      if (dt > dtc && !w.warned) {
+        if (!w.allow_unstable) {
+          failure_code = FX_E_UNSTABLE;
+          failure = "fx_explicit_stage: at step " + std::to_string(k) + " the stable step fell to " +
+                    std::to_string(dtc) + " (" + std::to_string(w.stage_dt_crit) + " at the start of the stage), below dt = " +
+                    std::to_string(dt) + ": the material stiffened";
+          return false;
+        }
+        w.warned = true;
       }
-      FX_CUDA(cudaGraphLaunch(exec, st));
-      done += block;
-    } else {
-      one_step(steps - done > 1);
-      ++done;
     }
+    if (w.nan_interval > 0 && k % w.nan_interval == 0 && count_nonfinite(w, u, n, st) > 0) {
+      failure_code = FX_E_DIVERGED;
+      failure = "fx_explicit_stage: displacements are not finite at step " + std::to_string(k) +
+                ": the analysis is unstable";
+      return false;
+    }
+    return true;
+  };
+  bool ok = checks(w.stage_step + done);
+  while (ok && done < steps) {
+    const int64_t k = w.stage_step + done;
+    const int64_t piece = std::min<int64_t>({steps - done, to_next(w.nan_interval, k), to_next(w.stable_interval, k)});
+    for (int64_t i = 0; i < piece;) {
+      if (piece - i > block) {
+        if (!exec) {
+          cudaGraph_t g = nullptr;
+          FX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+          for (int j = 0; j < block; ++j) one_step(1);
+          FX_CUDA(cudaStreamEndCapture(st, &g));
+          const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+          cudaGraphDestroy(g);
+          FX_CUDA(e);
+        }
+        FX_CUDA(cudaGraphLaunch(exec, st));
+        i += block;
+      } else {
+        one_step(steps - (done + i) > 1);
+        ++i;
+      }
+    }
+    done += static_cast<int>(piece);
+    ok = checks(w.stage_step + done);
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  FX_CUDA(cudaMemcpyAsync(time, w.time.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
-  FX_CUDA(cudaStreamSynchronize(st));
-  if (own_stream) cudaStreamDestroy(cs);
+  w.stage_step += done;
+  if (ok && count_nonfinite(w, u, n, st) > 0) {  // the end of every call
+    failure_code = FX_E_DIVERGED;
+    failure = "fx_explicit_stage: displacements are not finite at the end of the stage (step " +
+              std::to_string(w.stage_step) + ")";
+  }
+  finish();
+  if (failure_code != FX_OK) throw Error(failure_code, failure);
 }
 }  // namespace
 
@@ -731,23 +838,49 @@ int fx_newmark_update(int64_t n, const double* du, double* u, double* v, double*
 int fx_min_critical_dt(fx_force* f, int32_t scheme, double* dt) {
   return guard([&] {
     if (!f || !dt || (scheme != 0 && scheme != 1)) throw fx::Error(FX_E_INVALID, "fx_min_critical_dt: bad arguments");
-    const fx::ForceState& s = f->s;
-    double best = 1e300;
-    // elements of one parameter set on a box grid are congruent: one eigenproblem per set
-    std::vector<char> seen(static_cast<size_t>(s.nparams), 0);
-    for (int32_t e = 0; e < s.count; ++e) {
-      const int32_t pi = s.param_h[e];
-      if (s.box.qualifies && seen[pi]) continue;
-      seen[pi] = 1;
-      double xl[3][8];
-      for (int a = 0; a < 8; ++a) {
-        const int32_t nd = s.node_h[static_cast<size_t>(a) * s.P + e];
-        for (int d = 0; d < 3; ++d) xl[d][a] = s.coords_h[static_cast<size_t>(d) * s.N + nd];
-      }
-      const fx::ParamGP& p = s.params_h[pi];
-      best = std::min(best, fx::stable_dt(scheme, p, fx::element_omega_sq(p, xl)));
-    }
-    *dt = best;
+    *dt = exact_min_dt(f->s, scheme, nullptr);
+  });
+}
+
+int fx_element_critical_dts(fx_force* f, int32_t scheme, double* dt_dev, void* stream) {
+  return guard([&] {
+    if (!f || (f->s.count > 0 && !dt_dev) || (scheme != 0 && scheme != 1))
+      throw fx::Error(FX_E_INVALID, "fx_element_critical_dts: bad arguments");
+    fx::general_min_critical_dt(f->s, scheme, nullptr, f->s.count, dt_dev, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fx_stability_prepare(fx_force* f, void* stream) {
+  return guard([&] {
+    if (!f) throw fx::Error(FX_E_INVALID, "fx_stability_prepare: bad arguments");
+    fx::prepare_stability_bounds(f->s, static_cast<cudaStream_t>(stream));
+    FX_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  });
+}
+
+int fx_min_critical_dt_bound(fx_force* f, int32_t scheme, double* dt, void* stream) {
+  return guard([&] {
+    if (!f || !dt || (scheme != 0 && scheme != 1)) throw fx::Error(FX_E_INVALID, "fx_min_critical_dt_bound: bad arguments");
+    *dt = fx::min_critical_dt_bound(f->s, scheme, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int fx_stability_may_change(const fx_force* f, int32_t* out) {
+  return guard([&] {
+    if (!f || !out) throw fx::Error(FX_E_INVALID, "fx_stability_may_change: bad arguments");
+    *out = fx::stability_may_change(f->s) ? 1 : 0;
+  });
+}
+
+int fx_explicit_checks(fx_force* f, int32_t nan_check_interval, int32_t stable_step_check_interval,
+                       int32_t allow_unstable_dt) {
+  return guard([&] {
+    if (!f || nan_check_interval < 0 || stable_step_check_interval < 0)
+      throw fx::Error(FX_E_INVALID, "fx_explicit_checks: bad arguments");
+    fx::ExplicitWork& w = work_of(f);
+    w.nan_interval = nan_check_interval;
+    w.stable_interval = stable_step_check_interval;
+    w.allow_unstable = allow_unstable_dt != 0;
   });
 }
 

@@ -29,8 +29,9 @@ extern "C" {
 #define FX_E_NOMEM 3       /* device or host allocation failed */
 #define FX_E_NOT_SPD 4     /* CG met p.Ap <= 0 (SolveResult::indefinite) */
 #define FX_E_DIVERGED 5    /* non-finite values or no convergence */
-#define FX_E_TIMEOUT 6     /* a bounded device wait gave up */
+#define FX_E_TIMEOUT 6     /* a bounded device wait gave up (reserved: no entry point waits on the device) */
 #define FX_E_CUDA 7        /* a CUDA runtime error (message in fx_last_error) */
+#define FX_E_UNSTABLE 8    /* an explicit step above the stable step (the stage's io::ModelError) */
 
 /* Message of the last failed call on this host thread. */
 const char* fx_last_error(void);
@@ -197,8 +198,23 @@ int fx_force_compute_f32(fx_force* f, const float* u, const float* v, float* out
  * internal_force.cpp:601-626). */
 int fx_mass_times_ground(fx_force* f, int32_t dir, double* y, void* stream);
 /* Smallest stable step of the elements (InternalForce::min_critical_dt,
- * internal_force.hpp:201): scheme 0 CentralDifference, 1 ExplicitDifference. Host result. */
+ * internal_force.hpp:201): scheme 0 CentralDifference, 1 ExplicitDifference. Host result. Each
+ * element's largest omega^2 with the lumped mass and the material's stability tangent (the elastic
+ * moduli at the committed state for the multi-yield soils, contracts.hpp:355-365) by the
+ * reference's cyclic Jacobi rotations (sym_eigen.hpp), one warp per element on the device, bit for
+ * bit the reference's; on box grids of elastic or J2 sets one element per parameter set. */
 int fx_min_critical_dt(fx_force* f, int32_t scheme, double* dt);
+/* Every element's stable step into dt_dev[count] (device, batch order):
+ * InternalForce::element_critical_dts (internal_force.hpp:202-204). */
+int fx_element_critical_dts(fx_force* f, int32_t scheme, double* dt_dev, void* stream);
+/* The periodic stable-step re-check (InternalForce::stability_may_change, prepare_stability_bounds,
+ * min_critical_dt_bound; internal_force.hpp:205-210): whether a set's stable step can change in a
+ * stage (the multi-yield soils), each element's omega^2 with the reference tangent (once per stage),
+ * and the smallest step from the bound: the soil points' largest stability factor times that
+ * omega^2, never above the exact omega^2 (so the bound never overstates the step). */
+int fx_stability_may_change(const fx_force* f, int32_t* out);
+int fx_stability_prepare(fx_force* f, void* stream);
+int fx_min_critical_dt_bound(fx_force* f, int32_t scheme, double* dt, void* stream);
 /* Material state: commit the trial state (InternalForce::commit_state, internal_force.cpp:507). */
 int fx_force_commit(fx_force* f, void* stream);
 /* Number of Gauss points that were plastic at the last force evaluation (J2). */
@@ -364,10 +380,20 @@ int fx_motions_evaluate(fx_motions* m, double t, double* accel_host);
  * (host) receives the end time. resume = 0 starts a stage (ED: half-step velocity = v; CD:
  * previous displacement = u); resume = 1 continues the previous call of the same scheme, so that
  * a stage run in pieces equals one call. fx_explicit_record's equation is recorded (the
- * acceleration after each step). */
+ * acceleration after each step). The stage's checks (explicit_analysis.cpp:582-653, 732-771): a
+ * starting call compares dt with the stable step (FX_E_UNSTABLE above it, unless allowed);
+ * every stable_step_check_interval steps of the stage (sets whose stable step can change) the
+ * bound, then the exact step where the bound falls below dt, stops the stage with FX_E_UNSTABLE;
+ * every nan_check_interval steps, and at the end of every call, non-finite displacements stop
+ * it with FX_E_DIVERGED (the state then is that of the failing step). */
 int fx_explicit_stage(fx_force* f, int32_t scheme, const double* mass, const double* alpha_mass, fx_motions* motions,
                       int32_t steps, double dt, double* time, double* u, double* v, double* a, int32_t resume,
                       void* stream);
+/* The checks of later fx_explicit_stage calls on this force: exec::RunOptions nan_check_interval
+ * and stable_step_check_interval (0 turns that periodic check off; defaults 100 and 100) and the
+ * stage's allow_unstable_dt (default 0: an unstable step stops the stage). */
+int fx_explicit_checks(fx_force* f, int32_t nan_check_interval, int32_t stable_step_check_interval,
+                       int32_t allow_unstable_dt);
 
 /* Newmark form D kernels (src/exec/implicit_stage.cpp:29-68). */
 int fx_newmark_predict(int64_t n, double* u, double* v, double* a, double* ut, double* vt, double* at, double a1,

@@ -79,6 +79,11 @@ def ref():
         L.fxref_operator_diagonal.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64]
         L.fxref_mass_times_ground.argtypes = [vp, C.c_int, p_f64]
         L.fxref_force_compute.argtypes = [vp, p_f64, p_f64, C.c_int, p_f64]
+        L.fxref_element_critical_dts.argtypes = [vp, C.c_int, p_f64]
+        L.fxref_stability_may_change.argtypes = [vp]
+        L.fxref_prepare_stability_bounds.argtypes = [vp]
+        L.fxref_min_critical_dt_bound.restype = C.c_double
+        L.fxref_min_critical_dt_bound.argtypes = [vp, C.c_int]
         L.fxref_min_critical_dt.restype = C.c_double
         L.fxref_min_critical_dt.argtypes = [vp, C.c_int]
         L.fxref_solve.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -290,6 +295,23 @@ class RefForce:
 
     def min_critical_dt(self, scheme="ExplicitDifference"):
         return ref().fxref_min_critical_dt(self.h, 1 if scheme == "ExplicitDifference" else 0)
+
+    def element_critical_dts(self, scheme="ExplicitDifference"):
+        out = np.zeros(self.c.count)
+        k = ref().fxref_element_critical_dts(self.h, 1 if scheme == "ExplicitDifference" else 0,
+                                             out.ctypes.data_as(p_f64))
+        if k < 0:
+            raise RuntimeError(ref().fxref_last_error().decode())
+        return out[:k]
+
+    def stability_may_change(self):
+        return bool(ref().fxref_stability_may_change(self.h))
+
+    def prepare_stability_bounds(self):
+        assert ref().fxref_prepare_stability_bounds(self.h) == 0
+
+    def min_critical_dt_bound(self, scheme="ExplicitDifference"):
+        return ref().fxref_min_critical_dt_bound(self.h, 1 if scheme == "ExplicitDifference" else 0)
 
     def solve(self, b, x0=None, k=(1.0, 0.0, 0.0), method="cg", rtol=1e-10, atol=0.0, max_it=10000, lanes=1,
               restart=30):

@@ -435,6 +435,32 @@ double fxref_min_critical_dt(fxref_force* h, int scheme) {
   return h->f->min_critical_dt(scheme ? ExplicitScheme::ExplicitDifference : ExplicitScheme::CentralDifference);
 }
 
+// Every element's stable step, the batches' in order (dt[] holds the model's element count).
+int fxref_element_critical_dts(fxref_force* h, int scheme, double* dt) {
+  try {
+    const auto all = h->f->element_critical_dts(scheme ? ExplicitScheme::ExplicitDifference
+                                                        : ExplicitScheme::CentralDifference);
+    std::size_t k = 0;
+    for (const auto& b : all)
+      for (double v : b) dt[k++] = v;
+    return static_cast<int>(k);
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+int fxref_stability_may_change(fxref_force* h) { return h->f->stability_may_change() ? 1 : 0; }
+int fxref_prepare_stability_bounds(fxref_force* h) {
+  try {
+    h->f->prepare_stability_bounds();
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+double fxref_min_critical_dt_bound(fxref_force* h, int scheme) {
+  return h->f->min_critical_dt_bound(scheme ? ExplicitScheme::ExplicitDifference : ExplicitScheme::CentralDifference);
+}
+
 // ------------------------------------------------------------------------------ solvers
 // result: [converged, iterations, rhs_norm, initial_residual, final_residual, indefinite]
 int fxref_solve(fxref_force* h, int method, double cK, double cC, double cM, double rtol, double atol, int max_it,
