@@ -1,5 +1,8 @@
-"""The oracle's J2 restatement (oracle/port/fx_oracle.c): it has no counterpart in the reference
-(parity unpinned), so it is checked against its own defining properties on the CPU:
+"""The oracle's J2 restatement (oracle/port/fx_oracle.c). The reference has no J2 material; the
+restatement is pinned to the reference's own PressureIndependMultiYield in its two-surface,
+pressure-independent form, which under proportional straining is linear kinematic hardening
+(stresses equal within 1e-12 through loading and reversal), and checked against its own defining
+properties on the CPU:
 - after a plastic step the stress lies on the yield surface of the hardened state;
 - the returned tangent is the derivative of the stress (central differences, 1e-6);
 - at the mesh level the J2 tangent operator is the derivative of the internal force, and with
@@ -80,3 +83,48 @@ def test_mesh_tangent_is_the_force_derivative(oracle_mod):
         e = np.zeros(n)
         e[q] = 1.0
         assert d[q] == pytest.approx(pm.apply_j2(D, (1.0, 0.0, 0.0), e)[q], rel=1e-12)
+
+
+@pytest.mark.parametrize("direction", [(0, 0, 0, 1, 0, 0), (0.3, -0.3, 0, 1, 0.5, -0.2)], ids=["simple_shear", "mixed"])
+def test_kinematic_j2_pinned_to_reference_two_surface_pimy(direction, oracle_mod, ref_available):
+    """The pin of the J2 restatement against the reference: the reference's own
+    PressureIndependMultiYield (oracle/_ref), pressure-independent (friction angle 0) with a
+    two-point user backbone, is von Mises plasticity with one yield surface and a failure surface;
+    under proportional deviatoric straining, as long as the stress stays inside the failure surface,
+    it is linear kinematic (Prager) hardening. Backbone: the first point on the elastic line at the
+    J2 yield stress in shear, sigma_y / sqrt(3); the segment to the second point with J2's
+    elasto-plastic shear modulus G H / (3 G + H) (the reference then sets the plastic modulus
+    2 H / 3, Simo-Hughes' kinematic coefficient); the second point far beyond the path. Along a
+    monotonic path to ten times the yield strain and a full reversal, the stresses of the J2 return
+    map with purely kinematic hardening (hk = 1) equal the reference's within 1e-12 of the largest
+    stress."""
+    if not ref_available:
+        pytest.skip("reference library not built")
+    O = oracle_mod
+    G0, K0 = 20e6, 50e6
+    e_mod, nu = 9 * K0 * G0 / (3 * K0 + G0), (3 * K0 - 2 * G0) / (2 * (3 * K0 + G0))
+    tau1 = SY / np.sqrt(3.0)
+    g1 = tau1 / G0
+    g2 = 60 * g1
+    tau2 = tau1 + G0 * H / (3 * G0 + H) * (g2 - g1)
+    ref = O.RefPimy((2.0, G0, K0, 10.0, 0.1, 0.0, 100.0, 0.0, 2), (g1, 1.0, g2, tau2 / (G0 * g2)))
+    sizes, moduli = ref.setup_values()[1:]
+    assert abs(sizes[0] - np.sqrt(3.0) * tau1) <= 1e-9 * sizes[0] and abs(moduli[0] - 2 * H / 3) <= 1e-9 * moduli[0]
+    d = np.array(direction, float)
+    path = list(np.linspace(0.0, 10 * g1, 41)[1:]) + list(np.linspace(10 * g1, -10 * g1, 81)[1:])
+    c_ref, c_j2 = ref.initial_state(), np.zeros(13)
+    worst = peak = 0.0
+    plastic = 0
+    p = O.p_f64
+    for gam in path:
+        eps = np.ascontiguousarray(gam * d)
+        c_ref, s_ref, _ = ref.update(1, c_ref, eps)
+        trial, s_j2, D = np.zeros(13), np.zeros(6), np.zeros(36)
+        plastic += O.port().fxo_j2_update(e_mod, nu, SY, H, 1.0, np.ascontiguousarray(c_j2).ctypes.data_as(p),
+                                          trial.ctypes.data_as(p), eps.ctypes.data_as(p), s_j2.ctypes.data_as(p),
+                                          D.ctypes.data_as(p))
+        c_j2 = trial
+        worst = max(worst, float(np.max(np.abs(s_j2 - s_ref))))
+        peak = max(peak, float(np.max(np.abs(s_ref))))
+    assert plastic > 60  # most of the path is plastic, on loading and after the reversal
+    assert worst <= 1e-12 * peak, worst / peak
