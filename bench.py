@@ -603,7 +603,7 @@ def serve_comparison(device, count=32, seed=1):
     eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
 
     def server():
-        return serving.Server(eng, hbm_budget=64 << 30, device=device, prepare_fn=lambda r, d: prepared[r.id])
+        return serving.Server(eng, device=device, prepare_fn=lambda r, d: prepared[r.id])
 
     server().run(warm, realtime=False)  # untimed: module loading, first launches, graph set-up
     serving.serve_one_at_a_time(warm, realtime=False, device=device, prepared=prepared, solvers=solvers)
@@ -637,7 +637,7 @@ def serve_mixed_comparison(device, count=32, seed=2):
     eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
 
     def server():
-        return serving.Server(eng, hbm_budget=64 << 30, device=device, prepare_fn=lambda r, d: server_prep[r.id])
+        return serving.Server(eng, device=device, prepare_fn=lambda r, d: server_prep[r.id])
 
     # untimed: the whole stream once through each arm (module loading, first launches, graph
     # set-up of every cohort and solver size), as a serving process that has run a while
@@ -676,7 +676,7 @@ def serve_rate_sweep(device, rates=(20.0, 200.0, 2000.0), count=24, seed=3):
         prepared, solvers = serving.resident(reqs, device)
         server_prep = {r.id: serving.prepare_j2(r, device) if isinstance(r, serving.J2Request) else prepared[r.id]
                        for r in reqs}
-        srv = serving.Server(eng, hbm_budget=64 << 30, device=device, prepare_fn=lambda r, d: server_prep[r.id])
+        srv = serving.Server(eng, device=device, prepare_fn=lambda r, d: server_prep[r.id])
         if warm:  # untimed: the first stream once through each arm, all at once
             srv.run(reqs, realtime=False)
             serving.serve_one_at_a_time(reqs, realtime=False, device=device, prepared=prepared, solvers=solvers)

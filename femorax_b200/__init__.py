@@ -19,7 +19,8 @@ from .meshes import ModelSpec
 
 __all__ = ["Model", "Compiled", "MeshArrays", "InternalForce", "OperatorCoefficients", "MatrixFreeOperator",
            "SolveOptions", "SolveResult", "LinearSolver", "ConjugateGradient", "Gmres", "KrylovSolver",
-           "MixedPrecisionSolver", "BatchEngine", "BatchedNewton", "VectorOps", "GroundMotions", "FxError", "ModelSpec"]
+           "MixedPrecisionSolver", "BatchEngine", "BatchedNewton", "VectorOps", "GroundMotions", "FxError", "ModelSpec",
+           "device_memory"]
 
 
 def _i32(a):
@@ -49,6 +50,13 @@ def _stream(stream):
     if isinstance(stream, int):
         return stream
     return stream.cuda_stream
+
+
+def device_memory(device: int = 0):
+    """(free, total) bytes of device memory on `device` (fx_device_memory, cudaMemGetInfo)."""
+    fr, tot = C.c_int64(), C.c_int64()
+    check(lib().fx_device_memory(device, C.byref(fr), C.byref(tot)))
+    return fr.value, tot.value
 
 
 # ------------------------------------------------------------------ model and compile step

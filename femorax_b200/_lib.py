@@ -103,6 +103,7 @@ PROTOTYPES = {
     "fx_force_tune": (C.c_int, [vp, vp]),
     "fx_apply_operator": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_apply_operator_f32": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
+    "fx_device_memory": (C.c_int, [C.c_int32, p_i64, p_i64]),
     "fx_apply_operator_host": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_operator_diagonal_host": (C.c_int, [vp, fx_coeffs, vp, vp]),
     "fx_operator_diagonal": (C.c_int, [vp, fx_coeffs, vp, vp]),

@@ -61,6 +61,21 @@ extern "C" {
 const char* fx_last_error(void) { return fx::g_error.c_str(); }
 const char* fx_version(void) { return "femorax_b200 0.1 (sm_100a)"; }
 
+int fx_device_memory(int32_t device, int64_t* free_bytes, int64_t* total_bytes) {
+  return guarded([&] {
+    FX_REQUIRE(free_bytes && total_bytes && device >= 0, "fx_device_memory: bad arguments");
+    int cur = 0;
+    FX_CUDA(cudaGetDevice(&cur));
+    FX_CUDA(cudaSetDevice(device));
+    size_t fr = 0, tot = 0;
+    const cudaError_t e = cudaMemGetInfo(&fr, &tot);
+    cudaSetDevice(cur);
+    FX_CUDA(e);
+    *free_bytes = static_cast<int64_t>(fr);
+    *total_bytes = static_cast<int64_t>(tot);
+  });
+}
+
 // ------------------------------------------------------------------ model
 int fx_model_create(int32_t num_nodes, const int32_t* tags, const double* coords, fx_model** out) {
   return guarded([&] {

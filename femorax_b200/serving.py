@@ -38,7 +38,7 @@ import time
 import numpy as np
 
 from . import (BatchEngine, BatchedNewton, ConjugateGradient, InternalForce, MatrixFreeOperator, Model,
-               OperatorCoefficients, SolveOptions, SolveResult, meshes, stages)
+               OperatorCoefficients, SolveOptions, SolveResult, device_memory, meshes, stages)
 
 
 @dataclasses.dataclass
@@ -270,9 +270,16 @@ class Server:
     """The continuous-batching loop over one BatchEngine (static solves) and one J2Lane (J2 load
     paths, in cohorts of up to max_cohort)."""
 
-    def __init__(self, engine: BatchEngine, hbm_budget: int, device: int = 0, prep_threads: int = 4,
-                 prepare_fn=None, lane=None, max_cohort: int = 32, cohort_window: float = 0.25):
+    def __init__(self, engine: BatchEngine, hbm_budget: int = None, device: int = 0, prep_threads: int = 4,
+                 prepare_fn=None, lane=None, max_cohort: int = 32, cohort_window: float = 0.25,
+                 reserve: int = 2 << 30):
+        """hbm_budget: the bytes the admitted requests' footprints may hold; None sizes it from the
+        device's free memory now (fx_device_memory, as the reference sizes against cudaMemGetInfo),
+        less `reserve` for the work vectors and the library's own buffers."""
         self.engine = engine
+        if hbm_budget is None:
+            free, _ = device_memory(device)
+            hbm_budget = max(0, free - int(reserve))
         self.budget = int(hbm_budget)
         self.device = device
         self.prep_threads = prep_threads

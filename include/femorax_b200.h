@@ -37,6 +37,10 @@ extern "C" {
 const char* fx_last_error(void);
 /* Library version string. */
 const char* fx_version(void);
+/* Free and total bytes of device memory on `device` (cudaMemGetInfo with that device current; the
+ * caller's current device is restored): native::cuda_free_memory_bytes
+ * (src/native/device_memory_cuda.cpp:7-11), what the serving loop sizes its admissions against. */
+int fx_device_memory(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
 
 /* ------------------------------------------------------------------ model description
  * The fields of io::Model the hot path reads (src/io/model.hpp:34-172), as flat arrays.

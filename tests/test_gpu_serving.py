@@ -62,3 +62,13 @@ def test_mixed_stream_same_alone_and_in_the_mix():
     assert srv.resident == 0
     summ = serving.summary(served, wall)
     assert summ["converged"] == len(stream)
+
+
+def test_admission_budget_from_free_device_memory():
+    """Without a given budget the loop sizes admissions against the device's free memory
+    (fx_device_memory, cudaMemGetInfo) less its reserve."""
+    free0, total = fx.device_memory(0)
+    assert 0 < free0 <= total
+    srv = serving.Server(engine(), reserve=1 << 30)
+    assert 0 < srv.budget <= total - (1 << 30)
+    assert abs(srv.budget - (free0 - (1 << 30))) <= total // 10
