@@ -670,6 +670,36 @@ class LinearSolver:
         return it.value, SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual,
                                      r.final_residual, bool(r.indefinite), r.refinements)
 
+    def newmark_step_recover(self, fext0, fext1, u, v, a, dt: float, beta: float = 0.25, gamma: float = 0.5,
+                             tol: float = 1e-6, test: str = "NormUnbalance", max_newton: int = 25,
+                             max_retries: int = 0, num_sublevels: int = 0, num_substeps: int = 2, stream=None):
+        """One Newmark step with the reference's retry and substep recovery
+        (fx_solver_newmark_recover): the load ramps from fext0 (None: fext1) to fext1 over the
+        step; a converged step (or substep) commits the materials. Returns (stats, SolveResult),
+        stats = dict(attempts, failed, retries, substepped, newton)."""
+        r = L.fx_solve_result()
+        st = (C.c_int32 * 5)()
+        t = L.FX_TEST_NORM_UNBALANCE if test == "NormUnbalance" else L.FX_TEST_NORM_DISP_INCR
+        check(lib().fx_solver_newmark_recover(self._h, _ptr(fext0), _ptr(fext1), _ptr(u), _ptr(v), _ptr(a), dt, beta,
+                                              gamma, t, tol, max_newton, max_retries, num_sublevels, num_substeps, st,
+                                              C.byref(r), _stream(stream)))
+        return (dict(zip(("attempts", "failed", "retries", "substepped", "newton"), list(st))),
+                SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual, r.final_residual,
+                            bool(r.indefinite), r.refinements))
+
+    def newton_recover(self, fext, u, tol: float = 1e-6, test: str = "NormUnbalance", max_newton: int = 25,
+                       max_retries: int = 0, stream=None):
+        """One quasi-static load step with retries (fx_solver_newton_recover); a converged step
+        commits the materials, a failed one leaves u at its committed value."""
+        r = L.fx_solve_result()
+        st = (C.c_int32 * 5)()
+        t = L.FX_TEST_NORM_UNBALANCE if test == "NormUnbalance" else L.FX_TEST_NORM_DISP_INCR
+        check(lib().fx_solver_newton_recover(self._h, _ptr(fext), _ptr(u), t, tol, max_newton, max_retries, st,
+                                             C.byref(r), _stream(stream)))
+        return (dict(zip(("attempts", "failed", "retries", "substepped", "newton"), list(st))),
+                SolveResult(bool(r.converged), r.iterations, r.rhs_norm, r.initial_residual, r.final_residual,
+                            bool(r.indefinite), r.refinements))
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

@@ -154,6 +154,11 @@ PROTOTYPES = {
     "fx_solver_solve": (C.c_int, [vp, vp, vp, C.POINTER(fx_solve_result), vp]),
     "fx_solver_newmark": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_double,
                                     C.c_int32, C.POINTER(C.c_int32), C.POINTER(fx_solve_result), vp]),
+    "fx_solver_newmark_recover": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                            C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int32, p_i32,
+                                            C.POINTER(fx_solve_result), vp]),
+    "fx_solver_newton_recover": (C.c_int, [vp, vp, vp, C.c_int32, C.c_double, C.c_int32, C.c_int32, p_i32,
+                                           C.POINTER(fx_solve_result), vp]),
     "fx_solver_newton": (C.c_int, [vp, vp, vp, C.c_int32, C.c_double, C.c_int32, C.POINTER(C.c_int32),
                                    C.POINTER(fx_solve_result), vp]),
     "fx_explicit_run": (C.c_int, [vp, vp, C.c_int32, p_f64, C.c_int32, C.c_double, vp, vp, vp, vp, vp]),

@@ -9,6 +9,7 @@
 // reads the `done` flag after each block of iterations. Every kernel returns at once when the
 // solve is done, so the iterate is frozen at the converged one. All reductions use the
 // documented chunk/lane order (fused multiply-adds), so a solve gives the same bits every run.
+#include <functional>
 #include <algorithm>
 #include <cstring>
 #include <cmath>
@@ -368,6 +369,7 @@ struct Solver {
   DeviceArray<double> V, Z, wv, hbuf;  // GMRES
   DeviceArray<double> nres, ndu;       // Newton: residual and increment
   DeviceArray<double> nut, nvt, nat;   // Newmark: the last step's u, v, a
+  DeviceArray<double> cu, cv, ca, fx_t;  // recovery: the committed u, v, a of an attempt; its load
   int* host_flags = nullptr;           // pinned
   double* host_sc = nullptr;           // pinned
   // The CG loop graph of the last solve per precision (0: FP64, 1: FP32 inner), kept for the next
@@ -498,6 +500,16 @@ struct Solver {
   void gmres(const double* b, double* x, fx_solve_result* res);
   void ir(const double* b, double* x, fx_solve_result* res);
   int newton(const double* fext, double* u, int test, double tol, int max_newton, fx_solve_result* res);
+  void setup_coefficients(const double kk[3], bool initial, cudaStream_t st);
+  struct Recovery {
+    int max_retries = 0, num_sublevels = 0, num_substeps = 2;
+    int attempts = 0, failed = 0, retries = 0, substepped = 0, newton = 0;
+  };
+  bool newmark_recover(const double* fext0, const double* fext1, double* u, double* v, double* a, double h,
+                       double beta, double gamma, int test, double tol, int max_newton, Recovery& rc,
+                       fx_solve_result* res);
+  bool newton_recover(const double* fext, double* u, int test, double tol, int max_newton, Recovery& rc,
+                      fx_solve_result* res);
   int newmark(const double* fext, double* u, double* v, double* a, double h, double beta, double gamma, int test,
               double tol, int max_newton, fx_solve_result* res);
 };
@@ -784,6 +796,148 @@ int Solver::newmark(const double* fext, double* u, double* v, double* a, double 
   return it;
 }
 
+// The Jacobi preconditioner and the operator tables for coefficients kk (fx_solver_setup).
+void Solver::setup_coefficients(const double kk[3], bool initial, cudaStream_t st) {
+  drop_graphs();
+  k[0] = kk[0];
+  k[1] = kk[1];
+  k[2] = kk[2];
+  f->s.initial = initial;
+  if (n == 0) return;
+  general_diagonal(f->s, k, diag.ptr, st);
+  FX_CUDA(cudaMemsetAsync(zero_count.ptr, 0, sizeof(int), st));
+  k_count_zero<<<ew(n), 256, 0, st>>>(diag.ptr, n, zero_count.ptr);
+  int zeros = 0;
+  FX_CUDA(cudaMemcpyAsync(&zeros, zero_count.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FX_CUDA(cudaStreamSynchronize(st));
+  if (zeros > 0) throw Error(FX_E_INVALID, "Jacobi: " + std::to_string(zeros) + " zero diagonal entries");
+  k_reciprocal_t<double><<<ew(n), 256, 0, st>>>(diag.ptr, inv.ptr, n);
+  if (method == FX_SOLVER_IR) k_reciprocal_t<float><<<ew(n), 256, 0, st>>>(diag.ptr, inv32.ptr, n);
+  FX_LAUNCH_CHECK("jacobi_setup");
+  if (f->s.use_box()) box_prepare(f->s, k);
+  FX_CUDA(cudaStreamSynchronize(st));
+}
+
+namespace {
+__global__ void k_lerp(const double* __restrict__ a, const double* __restrict__ b, double t, double* __restrict__ out,
+                       int64_t n) {
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[q] = t == 1.0 ? b[q] : a[q] + t * (b[q] - a[q]);
+}
+void commit_materials(ForceState& fs, cudaStream_t st) {  // Domain::commit
+  if (fs.has_j2)
+    FX_CUDA(cudaMemcpyAsync(fs.j2_committed.ptr, fs.j2_trial.ptr, fs.j2_committed.bytes(), cudaMemcpyDeviceToDevice, st));
+  pimy_commit(fs, st);
+}
+}  // namespace
+
+// Femora's retry and substep recovery around one Newmark step (implicit_stage.cpp:261-402): an
+// attempt that does not converge goes back to the committed state (u, v, a; the materials' trial
+// state is rebuilt from their committed one by the next force evaluation) and is retried at the
+// same size up to max_retries times; then, below num_sublevels, the step is split into
+// num_substeps steps one level down, each with the same recovery. Every converged attempt commits
+// the materials (Domain::commit). The load of an attempt ending at the fraction theta of the step
+// is fext0 + theta (fext1 - fext0). The solver is set up for each attempt's size and back for h.
+bool Solver::newmark_recover(const double* fext0, const double* fext1, double* u, double* v, double* a, double h,
+                             double beta, double gamma, int test, double tol, int max_newton, Recovery& rc,
+                             fx_solve_result* res) {
+  const size_t nn = static_cast<size_t>(n);
+  if (cu.n < nn) {
+    cu.alloc(nn);
+    cv.alloc(nn);
+    ca.alloc(nn);
+    fx_t.alloc(nn);
+  }
+  const double k0[3] = {k[0], k[1], k[2]};
+  const bool init0 = f->s.initial;
+  const size_t bytes = sizeof(double) * nn;
+  double theta = 0.0;
+  auto attempt = [&](double hs) -> bool {
+    ++rc.attempts;
+    FX_CUDA(cudaMemcpyAsync(cu.ptr, u, bytes, cudaMemcpyDeviceToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(cv.ptr, v, bytes, cudaMemcpyDeviceToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(ca.ptr, a, bytes, cudaMemcpyDeviceToDevice, cs));
+    const double end = hs == h ? 1.0 : std::min(1.0, theta + hs / h);
+    k_lerp<<<ew(n), 256, 0, cs>>>(fext0 ? fext0 : fext1, fext1, end, fx_t.ptr, n);
+    FX_LAUNCH_CHECK("recovery_load");
+    const double kk[3] = {1.0, gamma / (beta * hs), 1.0 / (beta * hs * hs)};
+    if (kk[0] != k[0] || kk[1] != k[1] || kk[2] != k[2]) setup_coefficients(kk, init0, cs);
+    fx_solve_result one{};
+    rc.newton += newmark(fx_t.ptr, u, v, a, hs, beta, gamma, test, tol, max_newton, &one);
+    res->iterations += one.iterations;
+    res->refinements += one.refinements;
+    res->indefinite |= one.indefinite;
+    res->rhs_norm = one.rhs_norm;
+    res->initial_residual = one.initial_residual;
+    res->final_residual = one.final_residual;
+    if (one.converged) {
+      commit_materials(f->s, cs);
+      theta = end;
+      return true;
+    }
+    ++rc.failed;
+    FX_CUDA(cudaMemcpyAsync(u, cu.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(v, cv.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
+    FX_CUDA(cudaMemcpyAsync(a, ca.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
+    return false;
+  };
+  std::function<bool(double, int)> recover = [&](double hs, int level) -> bool {
+    if (attempt(hs)) return true;
+    for (int r = 1; r <= rc.max_retries; ++r) {
+      ++rc.retries;
+      if (attempt(hs)) return true;
+    }
+    if (level >= rc.num_sublevels) return false;
+    ++rc.substepped;
+    const double sub = hs / static_cast<double>(rc.num_substeps);
+    for (int i = 0; i < rc.num_substeps; ++i)
+      if (!recover(sub, level + 1)) return false;
+    return true;
+  };
+  const bool ok = recover(h, 0);
+  if (k[0] != k0[0] || k[1] != k0[1] || k[2] != k0[2]) setup_coefficients(k0, init0, cs);
+  res->converged = ok ? 1 : 0;
+  return ok;
+}
+
+// The same recovery for a quasi-static load step: a failed step returns to the committed
+// displacement and is retried, up to max_retries times (static stages retry only,
+// implicit_stage.cpp:263-266); a converged one commits the materials.
+bool Solver::newton_recover(const double* fext, double* u, int test, double tol, int max_newton, Recovery& rc,
+                            fx_solve_result* res) {
+  const size_t nn = static_cast<size_t>(n);
+  if (cu.n < nn) {
+    cu.alloc(nn);
+    cv.alloc(nn);
+    ca.alloc(nn);
+    fx_t.alloc(nn);
+  }
+  const size_t bytes = sizeof(double) * nn;
+  for (int r = 0; r <= rc.max_retries; ++r) {
+    if (r > 0) ++rc.retries;
+    ++rc.attempts;
+    FX_CUDA(cudaMemcpyAsync(cu.ptr, u, bytes, cudaMemcpyDeviceToDevice, cs));
+    fx_solve_result one{};
+    rc.newton += newton(fext, u, test, tol, max_newton, &one);
+    res->iterations += one.iterations;
+    res->refinements += one.refinements;
+    res->indefinite |= one.indefinite;
+    res->rhs_norm = one.rhs_norm;
+    res->initial_residual = one.initial_residual;
+    res->final_residual = one.final_residual;
+    if (one.converged) {
+      commit_materials(f->s, cs);
+      res->converged = 1;
+      return true;
+    }
+    ++rc.failed;
+    FX_CUDA(cudaMemcpyAsync(u, cu.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
+  }
+  res->converged = 0;
+  return false;
+}
+
 }  // namespace fx
 
 struct fx_solver {
@@ -883,26 +1037,8 @@ int fx_solver_setup(fx_solver* h, fx_coeffs k, void* stream) {
   return guard([&] {
     if (!h) throw fx::Error(FX_E_INVALID, "fx_solver_setup: null handle");
     fx::Solver& s = h->s;
-    auto st = static_cast<cudaStream_t>(stream);
-    s.drop_graphs();
-    s.k[0] = k.stiffness;
-    s.k[1] = k.damping;
-    s.k[2] = k.mass;
-    s.f->s.initial = k.initial != 0;
-    if (s.n > 0) {
-      fx::general_diagonal(s.f->s, s.k, s.diag.ptr, st);
-      FX_CUDA(cudaMemsetAsync(s.zero_count.ptr, 0, sizeof(int), st));
-      fx::k_count_zero<<<fx::ew(s.n), 256, 0, st>>>(s.diag.ptr, s.n, s.zero_count.ptr);
-      int zeros = 0;
-      FX_CUDA(cudaMemcpyAsync(&zeros, s.zero_count.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
-      FX_CUDA(cudaStreamSynchronize(st));
-      if (zeros > 0) throw fx::Error(FX_E_INVALID, "Jacobi: " + std::to_string(zeros) + " zero diagonal entries");
-      fx::k_reciprocal_t<double><<<fx::ew(s.n), 256, 0, st>>>(s.diag.ptr, s.inv.ptr, s.n);
-      if (s.method == FX_SOLVER_IR) fx::k_reciprocal_t<float><<<fx::ew(s.n), 256, 0, st>>>(s.diag.ptr, s.inv32.ptr, s.n);
-      FX_LAUNCH_CHECK("jacobi_setup");
-      if (s.f->s.use_box()) fx::box_prepare(s.f->s, s.k);
-      FX_CUDA(cudaStreamSynchronize(st));
-    }
+    const double kk[3] = {k.stiffness, k.damping, k.mass};
+    s.setup_coefficients(kk, k.initial != 0, static_cast<cudaStream_t>(stream));
     s.ready = true;
   });
 }
@@ -1000,6 +1136,78 @@ int fx_solver_newmark(fx_solver* h, const double* fext, double* u, double* v, do
     FX_CUDA(cudaEventRecord(s.ev_in, st));
     FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
     *newton_iterations = s.newmark(fext, u, v, a, dt, beta, gamma, test, tol, max_newton, r);
+    FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
+    FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
+    r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);
+  });
+}
+
+int fx_solver_newmark_recover(fx_solver* h, const double* fext0, const double* fext1, double* u, double* v, double* a,
+                              double dt, double beta, double gamma, int32_t test, double tol, int32_t max_newton,
+                              int32_t max_retries, int32_t num_sublevels, int32_t num_substeps, int32_t* stats,
+                              fx_solve_result* r, void* stream) {
+  return guard([&] {
+    if (!h || !r || !stats || (h->s.n > 0 && (!fext1 || !u || !v || !a)) || max_newton < 0 || !(tol >= 0.0) ||
+        !(dt > 0.0) || !(beta > 0.0) || !(gamma > 0.0) || max_retries < 0 || num_sublevels < 0 || num_substeps < 1)
+      throw fx::Error(FX_E_INVALID, "fx_solver_newmark_recover: bad arguments");
+    if (test != FX_TEST_NORM_UNBALANCE && test != FX_TEST_NORM_DISP_INCR)
+      throw fx::Error(FX_E_INVALID, "fx_solver_newmark_recover: unknown convergence test");
+    fx::Solver& s = h->s;
+    if (!s.ready) throw fx::Error(FX_E_INVALID, "fx_solver_newmark_recover: call fx_solver_setup first");
+    if (s.method != FX_SOLVER_CG && s.method != FX_SOLVER_IR)
+      throw fx::Error(FX_E_UNSUPPORTED, "fx_solver_newmark_recover: CG or IR solvers only");
+    *r = fx_solve_result{};
+    for (int i = 0; i < 5; ++i) stats[i] = 0;
+    if (s.n == 0) {
+      r->converged = 1;
+      return;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    FX_CUDA(cudaEventRecord(s.ev_in, st));
+    FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
+    fx::Solver::Recovery rc;
+    rc.max_retries = max_retries;
+    rc.num_sublevels = num_sublevels;
+    rc.num_substeps = num_substeps;
+    s.newmark_recover(fext0, fext1, u, v, a, dt, beta, gamma, test, tol, max_newton, rc, r);
+    stats[0] = rc.attempts;
+    stats[1] = rc.failed;
+    stats[2] = rc.retries;
+    stats[3] = rc.substepped;
+    stats[4] = rc.newton;
+    FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
+    FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
+    r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);
+  });
+}
+
+int fx_solver_newton_recover(fx_solver* h, const double* fext, double* u, int32_t test, double tol, int32_t max_newton,
+                             int32_t max_retries, int32_t* stats, fx_solve_result* r, void* stream) {
+  return guard([&] {
+    if (!h || !r || !stats || (h->s.n > 0 && (!fext || !u)) || max_newton < 0 || !(tol >= 0.0) || max_retries < 0)
+      throw fx::Error(FX_E_INVALID, "fx_solver_newton_recover: bad arguments");
+    if (test != FX_TEST_NORM_UNBALANCE && test != FX_TEST_NORM_DISP_INCR)
+      throw fx::Error(FX_E_INVALID, "fx_solver_newton_recover: unknown convergence test");
+    fx::Solver& s = h->s;
+    if (!s.ready) throw fx::Error(FX_E_INVALID, "fx_solver_newton_recover: call fx_solver_setup first");
+    if (s.method != FX_SOLVER_CG && s.method != FX_SOLVER_IR)
+      throw fx::Error(FX_E_UNSUPPORTED, "fx_solver_newton_recover: CG or refined FP32 CG solvers only");
+    *r = fx_solve_result{};
+    for (int i = 0; i < 5; ++i) stats[i] = 0;
+    if (s.n == 0) {
+      r->converged = 1;
+      return;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    FX_CUDA(cudaEventRecord(s.ev_in, st));
+    FX_CUDA(cudaStreamWaitEvent(s.cs, s.ev_in, 0));
+    fx::Solver::Recovery rc;
+    rc.max_retries = max_retries;
+    s.newton_recover(fext, u, test, tol, max_newton, rc, r);
+    stats[0] = rc.attempts;
+    stats[1] = rc.failed;
+    stats[2] = rc.retries;
+    stats[4] = rc.newton;
     FX_CUDA(cudaEventRecord(s.ev_out, s.cs));
     FX_CUDA(cudaStreamWaitEvent(st, s.ev_out, 0));
     r->status = r->converged ? FX_OK : (r->indefinite ? FX_E_NOT_SPD : FX_E_DIVERGED);

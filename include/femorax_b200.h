@@ -344,6 +344,24 @@ int fx_solver_newton(fx_solver* s, const double* fext, double* u, int32_t test, 
 int fx_solver_newmark(fx_solver* s, const double* fext, double* u, double* v, double* a, double dt, double beta,
                       double gamma, int32_t test, double tol, int32_t max_newton, int32_t* newton_iterations,
                       fx_solve_result* r, void* stream);
+/* Femora's retry and substep recovery around one Newmark step (ImplicitStage,
+ * implicit_stage.cpp:261-402): an attempt whose Newton iterations do not converge goes back to the
+ * committed u, v, a and is retried at the same size up to max_retries times; then, below
+ * num_sublevels levels, the step is split into num_substeps steps one level down, each with the
+ * same recovery. Every converged attempt commits the material state (Domain::commit); the caller
+ * need not commit again. The load of an attempt that ends at the fraction theta of the step is
+ * fext0 + theta (fext1 - fext0) (device vectors; fext0 NULL: fext1 throughout). The solver is set
+ * up for each attempt's size (1, gamma/(beta h_s), 1/(beta h_s^2)) and back to dt's at the end.
+ * stats[5] = attempts, failed attempts, retries, substeppings, Newton iterations. Returns FX_OK
+ * with r->status FX_E_DIVERGED when every attempt failed (the state is then the committed one). */
+int fx_solver_newmark_recover(fx_solver* h, const double* fext0, const double* fext1, double* u, double* v, double* a,
+                              double dt, double beta, double gamma, int32_t test, double tol, int32_t max_newton,
+                              int32_t max_retries, int32_t num_sublevels, int32_t num_substeps, int32_t* stats,
+                              fx_solve_result* r, void* stream);
+/* The same for a quasi-static load step (fx_solver_newton): retries only, as the reference's static
+ * stages; a converged step commits the material state. stats as above (no substeppings). */
+int fx_solver_newton_recover(fx_solver* h, const double* fext, double* u, int32_t test, double tol, int32_t max_newton,
+                             int32_t max_retries, int32_t* stats, fx_solve_result* r, void* stream);
 
 /* ------------------------------------------------------------------ time stepping
  * ExplicitDifference steps (src/exec/explicit_analysis.cpp:62-84, 687-705): per step
