@@ -370,6 +370,7 @@ struct Solver {
   DeviceArray<double> nres, ndu;       // Newton: residual and increment
   DeviceArray<double> nut, nvt, nat;   // Newmark: the last step's u, v, a
   DeviceArray<double> cu, cv, ca, fx_t;  // recovery: the committed u, v, a of an attempt; its load
+  DeviceArray<double> ct_j2, ct_pimy, ct_pdmy;  // recovery: the points' tangents before an attempt
   int* host_flags = nullptr;           // pinned
   double* host_sc = nullptr;           // pinned
   // The CG loop graph of the last solve per precision (0: FP64, 1: FP32 inner), kept for the next
@@ -833,8 +834,9 @@ void commit_materials(ForceState& fs, cudaStream_t st) {  // Domain::commit
 }  // namespace
 
 // Femora's retry and substep recovery around one Newmark step (implicit_stage.cpp:261-402): an
-// attempt that does not converge goes back to the committed state (u, v, a; the materials' trial
-// state is rebuilt from their committed one by the next force evaluation) and is retried at the
+// attempt that does not converge goes back to the committed state (u, v, a and the points'
+// tangents; the materials' trial state is rebuilt from their committed one by the next force
+// evaluation) and is retried at the
 // same size up to max_retries times; then, below num_sublevels, the step is split into
 // num_substeps steps one level down, each with the same recovery. Every converged attempt commits
 // the materials (Domain::commit). The load of an attempt ending at the fraction theta of the step
@@ -852,12 +854,27 @@ bool Solver::newmark_recover(const double* fext0, const double* fext1, double* u
   const double k0[3] = {k[0], k[1], k[2]};
   const bool init0 = f->s.initial;
   const size_t bytes = sizeof(double) * nn;
+  // The points' tangents of the last force evaluation feed the Jacobi preconditioner set up for an
+  // attempt's size: a failed attempt gives them back with u, v, a, so that every attempt starts
+  // from the state the step started from.
+  ForceState& fs = f->s;
+  std::pair<DeviceArray<double>*, DeviceArray<double>*> tangents[3] = {
+      {&fs.j2_tan, &ct_j2}, {&fs.pimy_tan, &ct_pimy}, {&fs.pdmy_tan, &ct_pdmy}};
+  for (auto& t : tangents)
+    if (t.first->n > 0 && t.second->n != t.first->n) t.second->alloc(t.first->n);
+  auto keep = [&](bool restore) {
+    for (auto& t : tangents)
+      if (t.first->n > 0)
+        FX_CUDA(cudaMemcpyAsync(restore ? t.first->ptr : t.second->ptr, restore ? t.second->ptr : t.first->ptr,
+                                t.first->bytes(), cudaMemcpyDeviceToDevice, cs));
+  };
   double theta = 0.0;
   auto attempt = [&](double hs) -> bool {
     ++rc.attempts;
     FX_CUDA(cudaMemcpyAsync(cu.ptr, u, bytes, cudaMemcpyDeviceToDevice, cs));
     FX_CUDA(cudaMemcpyAsync(cv.ptr, v, bytes, cudaMemcpyDeviceToDevice, cs));
     FX_CUDA(cudaMemcpyAsync(ca.ptr, a, bytes, cudaMemcpyDeviceToDevice, cs));
+    keep(false);
     const double end = hs == h ? 1.0 : std::min(1.0, theta + hs / h);
     k_lerp<<<ew(n), 256, 0, cs>>>(fext0 ? fext0 : fext1, fext1, end, fx_t.ptr, n);
     FX_LAUNCH_CHECK("recovery_load");
@@ -880,6 +897,7 @@ bool Solver::newmark_recover(const double* fext0, const double* fext1, double* u
     FX_CUDA(cudaMemcpyAsync(u, cu.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
     FX_CUDA(cudaMemcpyAsync(v, cv.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
     FX_CUDA(cudaMemcpyAsync(a, ca.ptr, bytes, cudaMemcpyDeviceToDevice, cs));
+    keep(true);
     return false;
   };
   std::function<bool(double, int)> recover = [&](double hs, int level) -> bool {

@@ -82,41 +82,58 @@ def test_converged_step_equals_plain_step_and_commit():
     assert runs[1][3] > 0  # the column yields
 
 
+def newton_counts(mesh, F, h):
+    """Newton iterations of one step of h from rest, and of its two halves taken in turn."""
+    n = mesh.num_equations
+    probe = fx.InternalForce(mesh)
+    full_it, r = solver_for(probe, h).newmark_step(F, *state(n), h, BETA, GAMMA, tol=1e-6)
+    if not r.converged:
+        return None, None
+    probe = fx.InternalForce(mesh)
+    half = solver_for(probe, h / 2)
+    uh, vh, ah = state(n)
+    its = []
+    for f in (F * 0.5, F):
+        it, r = half.newmark_step(f, uh, vh, ah, h / 2, BETA, GAMMA, tol=1e-6)
+        if not r.converged:
+            return None, None
+        probe.commit_state()
+        its.append(it)
+    return full_it, max(its)
+
+
 def test_substeps_equal_two_half_steps():
-    mesh, F, _ = setup()
+    # a load and step size where the full step needs more Newton iterations than either half
+    case = None
+    for total in (60e3, 120e3, 240e3):
+        mesh, F, _ = setup(total)
+        for h in (2e-3, 2e-2, 2e-1):
+            full_it, half_it = newton_counts(mesh, F, h)
+            if full_it is not None and half_it < full_it:
+                case = (mesh, F, h, full_it - 1)
+                break
+        if case:
+            break
+    assert case is not None, "no load and step size where the halves converge in fewer Newton iterations"
+    mesh, F, h, limit = case
     n = mesh.num_equations
     zero = torch.zeros(n, dtype=torch.float64, device=DEV)
-    # Newton iterations of the full step and of its halves, from rest
-    probe = fx.InternalForce(mesh)
-    full_it, r = solver_for(probe, H).newmark_step(F, *state(n), H, BETA, GAMMA, tol=1e-6)
-    assert r.converged
-    half = solver_for(probe, H / 2)
-    uh, vh, ah = state(n)
-    half_its = []
-    for f in (F * 0.5, F):
-        it, r = half.newmark_step(f, uh, vh, ah, H / 2, BETA, GAMMA, tol=1e-6)
-        assert r.converged
-        probe.commit_state()
-        half_its.append(it)
-    limit = full_it - 1
-    if max(half_its) > limit:
-        pytest.skip(f"the halves need as many Newton iterations as the full step ({half_its} vs {full_it})")
     # manual: two half steps with the ramped load, each committed
     f_man = fx.InternalForce(mesh)
-    sm = solver_for(f_man, H / 2)
+    sm = solver_for(f_man, h / 2)
     um, vm, am = state(n)
     for f in (zero + 0.5 * (F - zero), F):
-        it, r = sm.newmark_step(f, um, vm, am, H / 2, BETA, GAMMA, tol=1e-6, max_newton=limit)
+        it, r = sm.newmark_step(f, um, vm, am, h / 2, BETA, GAMMA, tol=1e-6, max_newton=limit)
         assert r.converged
         f_man.commit_state()
     # recovered: the full step fails at the limit, two substeps converge
     f_rec = fx.InternalForce(mesh)
-    sr = solver_for(f_rec, H)
+    sr = solver_for(f_rec, h)
     ur, vr, ar = state(n)
-    st, r = sr.newmark_step_recover(zero, F, ur, vr, ar, H, BETA, GAMMA, tol=1e-6, max_newton=limit, num_sublevels=1)
+    st, r = sr.newmark_step_recover(zero, F, ur, vr, ar, h, BETA, GAMMA, tol=1e-6, max_newton=limit, num_sublevels=1)
     assert r.converged and st["substepped"] == 1 and st["attempts"] == 3 and st["failed"] == 1
     assert torch.equal(ur, um) and torch.equal(vr, vm) and torch.equal(ar, am)
     assert f_rec.plastic_points() == f_man.plastic_points()
     # the solver is set up for the full step again: a plain step runs
-    it, r = sr.newmark_step(F, ur, vr, ar, H, BETA, GAMMA, tol=1e-6)
+    it, r = sr.newmark_step(F, ur, vr, ar, h, BETA, GAMMA, tol=1e-6)
     assert r.converged
