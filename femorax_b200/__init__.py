@@ -71,7 +71,8 @@ class Model:
         check(lib().fx_model_create(len(tags), pt, pc, C.byref(h)))
         self._h = h
         for g in spec.groups:
-            mat = L.fx_material(kind=g.kind, E=g.E, nu=g.nu, rho=g.rho, sigma_y=g.sigma_y, H=g.H, hk=g.hk)
+            mat = L.fx_material(kind=g.kind, element=g.element, E=g.E, nu=g.nu, rho=g.rho, sigma_y=g.sigma_y, H=g.H,
+                                hk=g.hk)
             b, pb = _f64(np.array(g.b, dtype=np.float64))
             et, pet = _i32(g.etags)
             cn, pcn = _i32(np.asarray(g.conn).reshape(-1))
@@ -165,16 +166,25 @@ class Compiled:
 
 
 PARAM_FIELDS = ("kind", "mass_type", "E", "nu", "rho", "b0", "b1", "b2", "alphaM", "betaK", "betaKinit",
-                "betaKcomm", "sigma_y", "H", "hk")
+                "betaKcomm", "sigma_y", "H", "hk", "element")
 
 
 def params_table(ps) -> np.ndarray:
-    """Parameter sets as a float64 table [P, 15] in PARAM_FIELDS order."""
+    """Parameter sets as a float64 table [P, 16] in PARAM_FIELDS order."""
     out = np.zeros((len(ps), len(PARAM_FIELDS)))
     for i, p in enumerate(ps):
         out[i] = [p.kind, p.mass_type, p.E, p.nu, p.rho, p.b[0], p.b[1], p.b[2], p.alphaM, p.betaK, p.betaKinit,
-                  p.betaKcomm, p.sigma_y, p.H, p.hk]
+                  p.betaKcomm, p.sigma_y, p.H, p.hk, p.element]
     return out
+
+
+def ssp_element_constants(xl, E, nu):
+    """One SSPbrick element's cached data (fx_ssp_element_constants): (geo[33], con[110]) for corner
+    coordinates xl[3][8] and an elastic material."""
+    xl, px = _f64(np.asarray(xl, np.float64).reshape(3, 8))
+    geo, con = np.zeros(33), np.zeros(110)
+    check(lib().fx_ssp_element_constants(px, E, nu, geo.ctypes.data_as(L.p_f64), con.ctypes.data_as(L.p_f64)))
+    return geo, con
 
 
 @dataclasses.dataclass
@@ -216,6 +226,7 @@ class MeshArrays:
             q.b[0], q.b[1], q.b[2] = row[5], row[6], row[7]
             q.alphaM, q.betaK, q.betaKinit, q.betaKcomm = row[8], row[9], row[10], row[11]
             q.sigma_y, q.H, q.hk = row[12], row[13], row[14]
+            q.element = int(row[15]) if len(row) > 15 else 0
         keep.append(P)
         m.num_params = len(self.params)
         m.params = C.cast(P, C.POINTER(L.fx_param_set))

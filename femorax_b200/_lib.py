@@ -20,6 +20,8 @@ FX_E_TIMEOUT = 6
 FX_E_CUDA = 7
 FX_E_UNSTABLE = 8
 
+FX_ELEM_STDBRICK = 0
+FX_ELEM_SSPBRICK = 1
 FX_MAT_ELASTIC = 0
 FX_MAT_J2 = 1
 FX_RENUMBER_OFF = 0
@@ -40,7 +42,7 @@ vp = C.c_void_p
 
 
 class fx_material(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("pad_", C.c_int32), ("E", C.c_double), ("nu", C.c_double),
+    _fields_ = [("kind", C.c_int32), ("element", C.c_int32), ("E", C.c_double), ("nu", C.c_double),
                 ("rho", C.c_double), ("sigma_y", C.c_double), ("H", C.c_double), ("hk", C.c_double)]
 
 
@@ -48,7 +50,7 @@ class fx_param_set(C.Structure):
     _fields_ = [("kind", C.c_int32), ("mass_type", C.c_int32), ("E", C.c_double), ("nu", C.c_double),
                 ("rho", C.c_double), ("b", C.c_double * 3), ("alphaM", C.c_double), ("betaK", C.c_double),
                 ("betaKinit", C.c_double), ("betaKcomm", C.c_double), ("sigma_y", C.c_double), ("H", C.c_double),
-                ("hk", C.c_double)]
+                ("hk", C.c_double), ("element", C.c_int32), ("pad_", C.c_int32)]
 
 
 class fx_mesh(C.Structure):
@@ -104,6 +106,7 @@ PROTOTYPES = {
     "fx_apply_operator": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_apply_operator_f32": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_device_memory": (C.c_int, [C.c_int32, p_i64, p_i64]),
+    "fx_ssp_element_constants": (C.c_int, [p_f64, C.c_double, C.c_double, p_f64, p_f64]),
     "fx_apply_operator_host": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_operator_diagonal_host": (C.c_int, [vp, fx_coeffs, vp, vp]),
     "fx_operator_diagonal": (C.c_int, [vp, fx_coeffs, vp, vp]),

@@ -11,6 +11,7 @@
 
 #include "force.hpp"
 #include "host.hpp"
+#include "ssp_brick.cuh"
 
 namespace fx {
 namespace {
@@ -94,6 +95,10 @@ int fx_model_add_group(fx_model* m, const fx_material* mat, const double* b, int
     FX_REQUIRE(m && mat && b && count >= 0 && (count == 0 || (element_tags && connectivity)),
                "fx_model_add_group: bad arguments");
     FX_REQUIRE(mat->kind == FX_MAT_ELASTIC || mat->kind == FX_MAT_J2, "fx_model_add_group: unknown material kind");
+    FX_REQUIRE(mat->element == FX_ELEM_STDBRICK || mat->element == FX_ELEM_SSPBRICK,
+               "fx_model_add_group: unknown element type");
+    if (mat->element == FX_ELEM_SSPBRICK && mat->kind != FX_MAT_ELASTIC)
+      throw fx::Error(FX_E_UNSUPPORTED, "fx_model_add_group: SSPbrick groups take the elastic material");
     FX_REQUIRE(mat->E > 0 && mat->nu > -1.0 && mat->nu < 0.5, "fx_model_add_group: E > 0 and -1 < nu < 0.5 required");
     fx::Group g;
     g.mat = *mat;
@@ -104,6 +109,22 @@ int fx_model_add_group(fx_model* m, const fx_material* mat, const double* b, int
     m->groups.push_back(std::move(g));
   });
 }
+int fx_ssp_element_constants(const double* xl, double E, double nu, double* geo, double* con) {
+  return guarded([&] {
+    FX_REQUIRE(xl && geo && con && E > 0 && nu > -1.0 && nu < 0.5, "fx_ssp_element_constants: bad arguments");
+    double x[3][8];
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < 8; ++a) x[d][a] = xl[8 * d + a];
+    fx::ParamGP p{};
+    p.E = E;
+    p.nu = nu;
+    double D[6][6];
+    fx::elastic_D(p, D);
+    fx::ssp::element_setup(x, D[0][0], D[0][1], D[3][3], fx::pimy::Slab<double>{geo, 1},
+                           fx::pimy::Slab<double>{con, 1});
+  });
+}
+
 int fx_model_add_fix(fx_model* m, int32_t n, const int32_t* node, const int32_t* dof) {
   return guarded([&] {
     FX_REQUIRE(m && n >= 0 && (n == 0 || (node && dof)), "fx_model_add_fix: bad arguments");
@@ -279,6 +300,13 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
         p.sigma_y = q.sigma_y;
         p.H = q.H;
         p.hk = q.hk;
+        p.element = q.element;
+        FX_REQUIRE(p.element == FX_ELEM_STDBRICK || p.element == FX_ELEM_SSPBRICK, "fx_force_create: unknown element type");
+        if (p.element == FX_ELEM_SSPBRICK) {
+          if (p.kind != FX_MAT_ELASTIC)
+            throw fx::Error(FX_E_UNSUPPORTED, "fx_force_create: SSPbrick sets take the elastic material");
+          s.has_ssp = true;
+        }
       }
       // per-equation slot lists in (element, DOF) order
       std::vector<int32_t> start(static_cast<size_t>(s.neq) + 1, 0);
@@ -302,6 +330,7 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
       s.gstart.upload(start);
       s.glist.upload(list);
       s.slots.alloc(24 * P);
+      if (s.has_ssp) fx::ssp_setup(s);  // SSPbrick: each element's geometry and stabilization constants
       // J2 sets: state and tangent per Gauss point (virgin state, elastic tangent)
       for (const auto& q : s.params_h)
         if (q.kind == FX_MAT_J2) {

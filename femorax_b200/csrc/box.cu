@@ -165,6 +165,7 @@ void box_build_plan(ForceState& s) {
   bool all_lumped = true;
   for (const auto& q : s.params_h) {
     if (q.kind != 0) return no("a parameter set is not elastic");
+    if (q.element != 0) return no("a parameter set is not stdBrick");
     if (q.mass_type == 0) all_lumped = false;
   }
   const int32_t N = s.N, P = s.P;

@@ -33,6 +33,7 @@ struct ParamGP {  // one parameter set as the element kernels read it
   int kind;       // 0 elastic, 1 J2, 2 PressureIndependMultiYield
   double sigma_y, H, hk;
   int table;      // kind 2: the set's entry in the PressureIndependMultiYield table
+  int element;    // 0 stdBrick, 1 SSPbrick
 };
 
 struct PointShape {

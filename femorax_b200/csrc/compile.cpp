@@ -13,7 +13,7 @@
 //   batch          batches.cpp:110-228 (parameter sets per (group, region) in first-use order;
 //                  value[k * padded + e]; padding -1 / 0)
 //   lumped mass    batches.cpp:204-224 and 231-261 (element masses in batch order, then nodal
-//                  masses)
+//                  masses; SSPbrick: density times each node's volume weight, ssp_brick.hpp)
 //   coloring       batches.cpp:21-50 (greedy in batch order)
 // Models with exact constraints (rigid links, embedded nodes), beams and other elements are
 // outside this path and are refused.
@@ -25,6 +25,7 @@
 
 #include "brick_gp.cuh"
 #include "host.hpp"
+#include "ssp_brick.cuh"
 
 namespace fx {
 namespace {
@@ -339,7 +340,8 @@ void compile_model(const fx_model& m, int renumbering, int simd_width, bool colo
     if (fresh) {
       fx_param_set ps{};
       ps.kind = g.mat.kind;
-      ps.mass_type = g.lumped ? 1 : 0;
+      ps.element = g.mat.element;
+      ps.mass_type = (g.lumped || g.mat.element == FX_ELEM_SSPBRICK) ? 1 : 0;  // SSPbrick always lumps
       ps.E = g.mat.E;
       ps.nu = g.mat.nu;
       ps.rho = g.mat.rho;
@@ -370,7 +372,13 @@ void compile_model(const fx_model& m, int renumbering, int simd_width, bool colo
     ParamGP pg{};
     pg.rho = ps.rho;
     double mj[8];
-    lumped_mass(pg, xl, mj);
+    if (ps.element == FX_ELEM_SSPBRICK) {  // density times each node's volume weight
+      double nv[8];
+      ssp::node_volumes(xl, nv);
+      for (int j = 0; j < 8; ++j) mj[j] = ps.rho * nv[j];
+    } else {
+      lumped_mass(pg, xl, mj);
+    }
     for (int k = 0; k < 24; ++k) {
       const Index q = c.b_eq[static_cast<size_t>(k) * P + e];
       if (q < 0) continue;

@@ -215,6 +215,10 @@ struct ForceState {
   // unallocated (NULL) when no soil set is damped
   DeviceArray<double> soil_sd;
   ExplicitWork xw;
+  // SSPbrick sets: per element the geometry record and the stabilization constants,
+  // value k of element e at [k * P + e] (ssp_brick.cuh: kGeo, kCon values)
+  bool has_ssp = false;
+  DeviceArray<double> ssp_geo, ssp_con;
   // stable time step: the minimum's key (general.cu) and, for the periodic re-check, each
   // element's omega^2 with its reference stability tangent (prepare_stability_bounds)
   DeviceArray<unsigned long long> dt_key;
@@ -234,6 +238,8 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
 void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t st);
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
+// SSPbrick sets: every element's geometry record and stabilization constants on the device
+void ssp_setup(ForceState& s);
 // Stable explicit step on the device (one warp per element, the reference's eigen-solve bit for
 // bit): the minimum over the elements of `list` (all elements when NULL, n of them), each
 // element's step into dt_out when given (device, n values). scheme 0 CentralDifference, 1

@@ -10,11 +10,24 @@
 #include <cstring>
 
 #include "force.hpp"
+#include "ssp_brick.cuh"
 
 namespace fx {
 namespace {
 
 constexpr int kBlock = 128;
+
+// Value k of element e in an SSPbrick per-element array ([k * P + e]).
+struct Col {
+  const double* p;
+  int64_t ld;
+  __device__ double operator[](int k) const { return p[k * ld]; }
+};
+struct ColW {
+  double* p;
+  int64_t ld;
+  __device__ double& operator[](int k) const { return p[k * ld]; }
+};
 
 __device__ __forceinline__ void load_coords(const double* __restrict__ coords, const int32_t* __restrict__ node,
                                             int32_t N, int32_t P, int32_t e, double xl[3][8]) {
@@ -35,7 +48,9 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
                                                            const PdmySet* __restrict__ pdmy,
                                                            const double* __restrict__ dtan,
                                                            const double* __restrict__ pcs,
-                                                           const double* __restrict__ dcs) {
+                                                           const double* __restrict__ dcs,
+                                                           const double* __restrict__ sgeo,
+                                                           const double* __restrict__ scon) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count || (skip && *skip)) return;
   const ParamGP p = params[param[e]];
@@ -47,7 +62,8 @@ __global__ void __launch_bounds__(kBlock) k_element_apply(const double* __restri
     else xe[a] = q >= 0 ? x[q] : 0.0;
   }
   const OpFactors f = op_factors(p, ks, kd, km, initial != 0);
-  if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, initial ? f.c0 : f.cK, initial != 0});
+  if (p.element == 1) ssp::element_apply(p, ssp::factors(p, ks, kd, km), Col{sgeo + e, P}, Col{scon + e, P}, xe, ye);
+  else if (p.kind == 1) element_apply_d(p, f, xl, xe, ye, J2PointD{&p, j2tan + e, P, initial ? f.c0 : f.cK, initial != 0});
   else if (p.kind == 2) element_apply_d(p, f, xl, xe, ye, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc});
   else if (p.kind == 3) element_apply_d(p, f, xl, xe, ye, PdmyPointD{pdmy + p.table, dtan + e, dcs + e, P, f.cK, f.c0, f.cc});
   else element_apply(p, f, xl, xe, ye);
@@ -64,7 +80,9 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
                                                           const PdmySet* __restrict__ pdmy,
                                                           const double* __restrict__ dtan,
                                                           const double* __restrict__ pcs,
-                                                          const double* __restrict__ dcs) {
+                                                          const double* __restrict__ dcs,
+                                                          const double* __restrict__ sgeo,
+                                                          const double* __restrict__ scon) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -73,7 +91,9 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const double* __restric
   load_coords(coords, node, N, P, e, xl);
   for (int a = 0; a < 24; ++a) eqe[a] = eq[static_cast<int64_t>(a) * P + e];
   const OpFactors f = op_factors(p, ks, kd, km, initial != 0);
-  if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, initial ? f.c0 : f.cK, initial != 0});
+  if (p.element == 1)
+    ssp::element_diagonal(p, ssp::factors(p, ks, kd, km), Col{sgeo + e, P}, Col{scon + e, P}, eqe, de);
+  else if (p.kind == 1) element_diagonal_d(p, f, xl, eqe, de, J2PointD{&p, j2tan + e, P, initial ? f.c0 : f.cK, initial != 0});
   else if (p.kind == 2)
     element_diagonal_d(p, f, xl, eqe, de, PimyPointD{pimy + p.table, ptan + e, pcs + e, P, f.cK, f.cc});
   else if (p.kind == 3)
@@ -88,7 +108,9 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
                                                            int32_t count, const double* __restrict__ u,
                                                            const double* __restrict__ v, double* __restrict__ slots,
                                                            const double* __restrict__ j2c, double* __restrict__ j2t,
-                                                           double* __restrict__ j2tan, int* __restrict__ plastic) {
+                                                           double* __restrict__ j2tan, int* __restrict__ plastic,
+                                                           const double* __restrict__ sgeo,
+                                                           const double* __restrict__ scon) {
   const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= count) return;
   const ParamGP p = params[param[e]];
@@ -100,7 +122,9 @@ __global__ void __launch_bounds__(kBlock) k_element_force(const double* __restri
     ue[a] = q >= 0 ? u[q] : 0.0;
     ve[a] = q >= 0 ? v[q] : 0.0;
   }
-  if (p.kind == 1) {
+  if (p.element == 1) {
+    ssp::element_force(p, Col{sgeo + e, P}, Col{scon + e, P}, ue, ve, fe);
+  } else if (p.kind == 1) {
     const int np = element_force_j2(p, xl, ue, ve, j2c + e, j2t + e, j2tan + e, P, fe);
     if (np) atomicAdd(plastic, np);
   } else {
@@ -423,7 +447,8 @@ __global__ void __launch_bounds__(32 * kDtWarps)
                        const int32_t* __restrict__ param, const ParamGP* __restrict__ params, int32_t N, int32_t P,
                        const int32_t* __restrict__ list, int32_t n, const PimySet* __restrict__ pimy,
                        const PdmySet* __restrict__ pdmy, const double* __restrict__ pcs,
-                       const double* __restrict__ dcs, int reference, int scheme, double* __restrict__ w2_out,
+                       const double* __restrict__ dcs, const double* __restrict__ sgeo,
+                       const double* __restrict__ scon, int reference, int scheme, double* __restrict__ w2_out,
                        double* __restrict__ dt_out, unsigned long long* __restrict__ dt_min) {
   __shared__ double As[kDtWarps][24][25];  // a padded row: the column updates touch 24 banks
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -433,12 +458,26 @@ __global__ void __launch_bounds__(32 * kDtWarps)
     const ParamGP p = params[param[e]];
     double xl[3][8], m[8];
     load_coords(coords, node, N, P, e, xl);
-    lumped_mass(p, xl, m);
     double acc[2][3][3];
-    for (int h = 0; h < 2; ++h)
-      for (int a = 0; a < 3; ++a)
-        for (int c = 0; c < 3; ++c) acc[h][a][c] = 0.0;
-    for (int gp = 0; gp < 8; ++gp) {
+    if (p.element == 1) {  // SSPbrick (ssp_brick.hpp max_omega_sq_with): Kstab, then the one point
+      const Col g{sgeo + e, P}, c{scon + e, P};
+      for (int j = 0; j < 8; ++j) m[j] = p.rho * g[25 + j];
+      double D[6][6];
+      stability_D(p, pimy, pdmy, pcs, dcs, P, e, 0, reference != 0, D);
+      for (int h = 0; h < 2; ++h) {
+        const int q = lane + 32 * h, j = q >> 3, k = q & 7;
+        double blk[3][3];
+        ssp::block(g, D, j, k, blk);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) acc[h][a][b] = ssp::stab_entry(c, 3 * j + a, 3 * k + b) + blk[a][b];
+      }
+    } else {
+      lumped_mass(p, xl, m);
+      for (int h = 0; h < 2; ++h)
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) acc[h][a][c] = 0.0;
+    }
+    for (int gp = 0; gp < (p.element == 1 ? 0 : 8); ++gp) {
       PointShape s;
       point_shape(xl, gp, s);
       double D[6][6];
@@ -564,6 +603,7 @@ __global__ void k_element_dt_bound(const int32_t* __restrict__ param, const Para
 void general_apply_f32(ForceState& s, const double k[3], const float* x, float* y, cudaStream_t st, const int* skip) {
   if (s.has_pimy || s.has_pdmy)
     throw Error(FX_E_UNSUPPORTED, "the FP32 operator has no multi-yield soil tangent form");
+  if (s.has_ssp) throw Error(FX_E_UNSUPPORTED, "the FP32 operator has no SSPbrick form");
   if (s.count > 0 && s.geom32.n == 0) {  // the FP32 geometric factors, once
     s.geom32.alloc(static_cast<size_t>(kGeom32) * 8 * s.P);
     s.nshape32.alloc(64);
@@ -602,7 +642,7 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
                                                                    -1, x, s.slots.ptr, skip, s.j2_tan.ptr, s.initial,
                                                                    s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
                                                                    s.pdmy_tan.ptr, s.pimy_committed.ptr,
-                                                                   s.pdmy_committed.ptr);
+                                                                   s.pdmy_committed.ptr, s.ssp_geo.ptr, s.ssp_con.ptr);
   FX_LAUNCH_CHECK("element_apply");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -620,7 +660,7 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
                                                                   s.slots.ptr, s.j2_tan.ptr, s.initial,
                                                                   s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
                                                                   s.pdmy_tan.ptr, s.pimy_committed.ptr,
-                                                                  s.pdmy_committed.ptr);
+                                                                  s.pdmy_committed.ptr, s.ssp_geo.ptr, s.ssp_con.ptr);
   FX_LAUNCH_CHECK("element_diagonal");
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
@@ -636,7 +676,7 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
     k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, u, v, s.slots.ptr,
                                                                    s.j2_committed.ptr, s.j2_trial.ptr, s.j2_tan.ptr,
-                                                                   s.plastic_dev.ptr);
+                                                                   s.plastic_dev.ptr, s.ssp_geo.ptr, s.ssp_con.ptr);
   FX_LAUNCH_CHECK("element_force");
   const int64_t points = static_cast<int64_t>(8) * s.P;
   if (s.has_pimy && s.count > 0) {
@@ -695,7 +735,7 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
                                                                    nullptr, s.slots.ptr, nullptr, s.j2_tan.ptr, 0,
                                                                    s.pimy_dev.ptr, s.pimy_tan.ptr, s.pdmy_dev.ptr,
                                                                    s.pdmy_tan.ptr, s.pimy_committed.ptr,
-                                                                   s.pdmy_committed.ptr);
+                                                                   s.pdmy_committed.ptr, s.ssp_geo.ptr, s.ssp_con.ptr);
   FX_LAUNCH_CHECK("element_apply_unit");
   if (s.neq > 0)
     k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
@@ -705,6 +745,35 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
   FX_LAUNCH_CHECK("ground_mass");
 }
 
+
+namespace {
+// SSPbrick sets: one thread per element computes its geometry record and stabilization constants
+// (ssp::element_setup) from the material's initial tangent (C1 = D00, C2 = D01, C3 = D33).
+__global__ void k_ssp_setup(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                            const int32_t* __restrict__ param, const ParamGP* __restrict__ params, int32_t N,
+                            int32_t P, int32_t count, double* __restrict__ geo, double* __restrict__ con) {
+  const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  const ParamGP p = params[param[e]];
+  if (p.element != 1) return;
+  double xl[3][8], D[6][6];
+  load_coords(coords, node, N, P, e, xl);
+  elastic_D(p, D);
+  ssp::element_setup(xl, D[0][0], D[0][1], D[3][3], ColW{geo + e, P}, ColW{con + e, P});
+}
+}  // namespace
+
+void ssp_setup(ForceState& s) {
+  s.ssp_geo.alloc(static_cast<size_t>(ssp::kGeo) * std::max(s.P, 1));
+  s.ssp_con.alloc(static_cast<size_t>(ssp::kCon) * std::max(s.P, 1));
+  FX_CUDA(cudaMemset(s.ssp_geo.ptr, 0, s.ssp_geo.bytes()));
+  FX_CUDA(cudaMemset(s.ssp_con.ptr, 0, s.ssp_con.bytes()));
+  if (s.count > 0)
+    k_ssp_setup<<<grid_for(s.count, 64), 64>>>(s.coords.ptr, s.node.ptr, s.param.ptr, s.params.ptr, s.N, s.P,
+                                               s.count, s.ssp_geo.ptr, s.ssp_con.ptr);
+  FX_LAUNCH_CHECK("ssp_setup");
+  FX_CUDA(cudaDeviceSynchronize());
+}
 
 namespace {
 unsigned long long* dt_min_slot(ForceState& s) {
@@ -738,7 +807,8 @@ double general_min_critical_dt(ForceState& s, int scheme, const int32_t* list, i
   if (n > 0)
     k_element_omega_sq<<<dt_grid(n), 32 * kDtWarps, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.param.ptr, s.params.ptr, s.N, s.P, list, n, s.pimy_dev.ptr, s.pdmy_dev.ptr,
-        s.pimy_committed.ptr, s.pdmy_committed.ptr, 0, scheme, nullptr, dt_out, s.dt_key.ptr);
+        s.pimy_committed.ptr, s.pdmy_committed.ptr, s.ssp_geo.ptr, s.ssp_con.ptr, 0, scheme, nullptr, dt_out,
+        s.dt_key.ptr);
   FX_LAUNCH_CHECK("element_critical_dt");
   return read_dt_min(s, st);
 }
@@ -751,7 +821,8 @@ void prepare_stability_bounds(ForceState& s, cudaStream_t st) {
   if (n > 0)
     k_element_omega_sq<<<dt_grid(n), 32 * kDtWarps, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.param.ptr, s.params.ptr, s.N, s.P, nullptr, n, s.pimy_dev.ptr, s.pdmy_dev.ptr,
-        s.pimy_committed.ptr, s.pdmy_committed.ptr, 1, 0, s.w2_ref.ptr, nullptr, nullptr);
+        s.pimy_committed.ptr, s.pdmy_committed.ptr, s.ssp_geo.ptr, s.ssp_con.ptr, 1, 0, s.w2_ref.ptr, nullptr,
+        nullptr);
   FX_LAUNCH_CHECK("element_reference_omega_sq");
   s.bounds_ready = true;
 }

@@ -24,6 +24,7 @@ class Group:
     b: tuple = (0.0, 0.0, 0.0)
     lumped: bool = False
     kind: int = 0  # 0 ElasticIsotropic, 1 J2
+    element: int = 0  # 0 stdBrick, 1 SSPbrick (one point, physical stabilization; always lumped)
     sigma_y: float = 0.0
     H: float = 0.0
     hk: float = 0.0

@@ -53,9 +53,13 @@ typedef struct fx_model fx_model;
 
 /* One material: kind and its constants. J2 uses E, nu, rho, sigma_y, H (hardening modulus) and
  * hk (kinematic share of H, 0 = isotropic, 1 = kinematic). */
+/* element types of a group (io::ElementType, src/io/model.hpp:93) */
+#define FX_ELEM_STDBRICK 0
+#define FX_ELEM_SSPBRICK 1 /* SSPbrick: one point, physical stabilization; elastic material; lumped mass */
+
 typedef struct fx_material {
   int32_t kind;
-  int32_t pad_;
+  int32_t element; /* FX_ELEM_*: the group's element type */
   double E, nu, rho;
   double sigma_y, H, hk;
 } fx_material;
@@ -67,6 +71,13 @@ void fx_model_destroy(fx_model* m);
  * body force b[3], -lumped flag, element tags, 8 node tags per element in stdBrick order. */
 int fx_model_add_group(fx_model* m, const fx_material* mat, const double* b, int32_t lumped, int32_t count,
                        const int32_t* element_tags, const int32_t* connectivity);
+/* One SSPbrick element's per-element data as the device path caches it, computed on the host:
+ * xl[3][8] its corner coordinates (x of the 8 corners, then y, then z), E and nu its elastic
+ * material; geo[33] = dNmod (8 x 3, node-major: the rows of Bnot), the volume and each node's
+ * volume weight; con[110] = the hourglass vectors gamma_st, gamma_ut, gamma_us, gamma_stu (8 each,
+ * Mben's rows) and the upper triangle of the stabilization's 12 x 12 interior matrix, row by row
+ * (SSPbrick::point_store_geometry and element_constants, src/physics/elements/ssp_brick.hpp). */
+int fx_ssp_element_constants(const double* xl, double E, double nu, double* geo, double* con);
 /* fix rows (node tag, 1-based DOF), model.hpp:134-137. */
 int fx_model_add_fix(fx_model* m, int32_t n, const int32_t* node, const int32_t* dof);
 /* equalDOF rows (retained, constrained, 1-based DOF), model.hpp:157-162. */
@@ -111,6 +122,8 @@ typedef struct fx_param_set {
   double b[3];                                /* body force per unit volume */
   double alphaM, betaK, betaKinit, betaKcomm; /* Rayleigh (physics/contracts.hpp:69-75) */
   double sigma_y, H, hk;                      /* J2 only */
+  int32_t element;                            /* FX_ELEM_* */
+  int32_t pad_;
 } fx_param_set;
 
 typedef struct fx_mesh {

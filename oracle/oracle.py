@@ -53,7 +53,8 @@ def ref():
         L.fxref_model_create.argtypes = [C.c_int32, p_i32, p_f64]
         L.fxref_model_destroy.argtypes = [vp]
         L.fxref_model_add_group.argtypes = [vp, C.c_double, C.c_double, C.c_double, p_f64, C.c_int, C.c_int32, p_i32,
-                                            p_i32]
+                                            p_i32, C.c_int]
+        L.fxref_ssp_constants.argtypes = [p_f64, C.c_double, C.c_double, p_f64, p_f64]
         L.fxref_model_add_fix.argtypes = [vp, C.c_int32, p_i32, p_i32]
         L.fxref_model_add_equal_dof.argtypes = [vp, C.c_int32, p_i32, p_i32, p_i32]
         L.fxref_model_add_rayleigh.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, p_i32]
@@ -154,7 +155,8 @@ class RefModel:
                 L.fxref_model_add_group_pimy(self.h, pp9, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2,
                                              pb, int(g.lumped), len(et), pet, pcn)
             else:
-                L.fxref_model_add_group(self.h, g.E, g.nu, g.rho, pb, int(g.lumped), len(et), pet, pcn)
+                L.fxref_model_add_group(self.h, g.E, g.nu, g.rho, pb, int(g.lumped), len(et), pet, pcn,
+                                        int(getattr(g, "element", 0)))
         if len(spec.fix_node):
             a, pa = _i(spec.fix_node)
             d, pd = _i(spec.fix_dof)
@@ -718,6 +720,14 @@ class RefPdmy(RefPimy):
         if getattr(self, "h", None):
             ref().fxref_pdmy_destroy(self.h)
             self.h = None
+
+
+def ref_ssp_constants(xl, E, nu):
+    """The reference's SSPbrick geometry record (33) and element constants (110) of one element."""
+    xl, px = _f(np.asarray(xl, np.float64).reshape(3, 8))
+    geo, con = np.zeros(33), np.zeros(110)
+    ref().fxref_ssp_constants(px, E, nu, geo.ctypes.data_as(p_f64), con.ctypes.data_as(p_f64))
+    return geo, con
 
 
 def port_dot(x, y, lanes, fused):

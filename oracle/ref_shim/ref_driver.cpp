@@ -19,6 +19,7 @@
 #include "exec/ground_motion.hpp"
 #include "exec/internal_force.hpp"
 #include "exec/matrix_free_operator.hpp"
+#include "physics/elements/ssp_brick.hpp"
 #include "physics/elements/std_brick.hpp"
 #include "physics/materials/elastic_isotropic.hpp"
 #include "physics/materials/pressure_depend_multi_yield.hpp"
@@ -68,15 +69,16 @@ fxref_model* fxref_model_create(int32_t N, const int32_t* tags, const double* co
 void fxref_model_destroy(fxref_model* h) { delete h; }
 
 // Adds one material (tag = index + 1) and one stdBrick element group that uses it.
+// element: 0 stdBrick, 1 SSPbrick.
 int fxref_model_add_group(fxref_model* h, double E, double nu, double rho, const double* b, int lumped,
-                          int32_t count, const int32_t* etags, const int32_t* conn) {
+                          int32_t count, const int32_t* etags, const int32_t* conn, int element) {
   io::NDMaterial mat;
   mat.tag = static_cast<std::int32_t>(h->m.materials.size()) + 1;
   mat.data = io::ElasticIsotropicData{E, nu, rho};
   h->m.materials.push_back(mat);
   io::ElementGroup g;
   g.id = std::to_string(h->m.elements.size());
-  g.type = io::ElementType::StdBrick;
+  g.type = element ? io::ElementType::SSPbrick : io::ElementType::StdBrick;
   g.material = mat.tag;
   g.body_force = {b[0], b[1], b[2]};
   g.lumped = lumped != 0;
@@ -503,6 +505,20 @@ double fxref_host_dot(const double* x, const double* y, int64_t n, int lanes) {
 }
 
 // ------------------------------------------------------------------------------ element level
+// One SSPbrick's geometry record (33) and element constants (110) with an elastic material:
+// xl[3][8] corner coordinates (x of the 8 corners, then y, then z).
+int fxref_ssp_constants(const double* xl, double E, double nu, double* geo, double* con) {
+  using Ssp = SSPbrick<ElasticIsotropic>;
+  double x[3][8];
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < 8; ++a) x[d][a] = xl[8 * d + a];
+  Ssp::Params p{};
+  p.mat = ElasticIsotropic::Params{E, nu, 0.0};
+  Ssp::point_store_geometry(x, 0, Strided<double>{geo, 1});
+  Ssp::element_constants(p, x, Strided<double>{con, 1});
+  return 0;
+}
+
 // p = [E, nu, rho, b0, b1, b2, massType]; damp = [alphaM, betaK, betaKinit, betaKcomm];
 // xe[8][3]. Outputs fe[24] and, if Ke != NULL, Ke[24][24] row-major.
 int fxref_brick_compute(const double* p, const double* damp, const double* xe, const double* u, const double* v,

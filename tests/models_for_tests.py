@@ -94,3 +94,23 @@ def roller_block(nx=5, ny=4, nz=6):
     spec.fix_node = np.concatenate([spec.fix_node, np.array(nodes, np.int32)])
     spec.fix_dof = np.concatenate([spec.fix_dof, np.array(dofs, np.int32)])
     return spec
+
+
+def as_ssp(spec):
+    """The same model with every group an SSPbrick group (lumped by construction)."""
+    for g in spec.groups:
+        g.element = 1
+        g.lumped = True
+    return spec
+
+
+def ssp_block(nx=4, ny=3, nz=5, distort=0.0, seed=0):
+    """An SSPbrick block on a fixed base (optionally distorted: a general mesh), two Rayleigh regions
+    (all four factors) and a body force."""
+    spec = meshes.box_model(nx, ny, nz, (2.0, 1.5, 2.5), E=2.0e5, nu=0.3, rho=1.9, lumped=True, b=(0.1, -0.2, -9.8))
+    if distort:
+        spec = meshes.distort(spec, distort, seed=seed)
+    as_ssp(spec)
+    et = spec.groups[0].etags
+    spec.rayleigh = [meshes.Rayleigh(0.3, 1e-3, 0.0, 0.0, et), meshes.Rayleigh(0.5, 2e-3, 5e-4, 1e-4, et[::3])]
+    return spec
