@@ -220,6 +220,79 @@ def layered_parity(rf, force, x, y, device):
             "tolerance": 1e-12}
 
 
+# The reference's own 40^3 laminar-column measurements on an H200 (GH200; reference
+# benchmarks/baselines/tacc-vista-gh-cuda270336.json, min over 20 calls): its default variant, its
+# fastest deterministic (gather) variant and its fastest variant overall, in microseconds.
+H200_COLUMN_40 = {
+    "operator": {"default": 242.3, "fastest_deterministic": 137.3, "fastest": 73.1,
+                 "names": "operator/40^3/gather_cached_constant, gather_recompute_recomputed, "
+                          "atomic_recompute_recomputed"},
+    "explicit_force": {"default": 335.2, "fastest_deterministic": 173.3, "fastest": 103.3,
+                       "names": "explicit_force/40^3/team_gather_ept4_cached, flat_gather, flat_atomic"},
+    "operator_ssp": {"default": 142.0, "fastest_deterministic": 142.0, "fastest": 78.0,
+                     "names": "operator_ssp/40^3/gather_cached_constant, gather_cached_constant, "
+                              "atomic_cached_constant"},
+}
+
+
+def column_40(device, reps=50):
+    """The reference's benchmark model, the 40^3 laminar soil column (tests/common/
+    synthetic_models.hpp; 64,000 bricks, equalDOF ties, two Rayleigh regions), on the Gauss-point
+    path (every result in the reference's own arithmetic order, deterministic): the stdBrick
+    operator (consistent mass, K + 2e3 C + 1.6e7 M, as bench_operator.cpp), the explicit internal
+    force (lumped, damped, u = 1e-4, v = 1e-3, as bench_explicit.cpp) and the SSPbrick operator.
+    Per leg: min and median over `reps` calls by CUDA events (the reference's harness takes the min
+    with the operands warm in cache), the median with L2 flushed before each call, and the result
+    against the reference's own InternalForce (oracle/_ref) on the same inputs."""
+    import torch
+    import femorax_b200 as fx
+    mb = mesh_builders()
+    dev = torch.device("cuda", device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    out = {"mesh": "laminar column 40^3 (64,000 bricks)", "reference_h200_us": H200_COLUMN_40}
+    legs = {"operator": (mb.laminar_column(40, 40, 40, lumped=False), "apply"),
+            "explicit_force": (mb.laminar_column(40, 40, 40, lumped=True), "force"),
+            "operator_ssp": (mb.laminar_column(40, 40, 40, element=1), "apply")}
+    k = (1.0, 2e3, 1.6e7)
+    for name, (spec, kind) in legs.items():
+        mesh = fx.Model(spec).compile().mesh()
+        force = fx.InternalForce(mesh, device=device)
+        n = mesh.num_equations
+        if kind == "apply":
+            xn = np.full(n, 1e-3)
+            x, y = torch.as_tensor(xn, device=dev), torch.zeros(n, dtype=torch.float64, device=dev)
+            call = lambda: force.apply_operator(fx.OperatorCoefficients(*k), x, y)
+        else:
+            un, vn = np.full(n, 1e-4), np.full(n, 1e-3)
+            u, v = torch.as_tensor(un, device=dev), torch.as_tensor(vn, device=dev)
+            y = torch.zeros(n, dtype=torch.float64, device=dev)
+            call = lambda: force.compute(u, v, y)
+        for _ in range(5):
+            call()
+        hot, cold = [], []
+        for flushed in (False, True):
+            for i in range(reps):
+                if flushed:
+                    flush.fill_(float(i))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                call()
+                e1.record()
+                torch.cuda.synchronize(dev)
+                (cold if flushed else hot).append(e0.elapsed_time(e1) * 1e3)
+        leg = {"equations": n, "elements": mesh.count, "us_min": float(np.min(hot)),
+               "us_median": float(np.median(hot)), "us_median_l2_flushed": float(np.median(cold)),
+               "path": force.info()["path"]}
+        rf = reference_force(spec)
+        if rf is not None:
+            want = rf.apply_operator(k, xn) if kind == "apply" else rf.force(un, vn)
+            leg["max_rel_err_vs_reference"] = rel_err(y.cpu().numpy(), want)
+        leg["vs_h200_default"] = H200_COLUMN_40[name]["default"] / leg["us_min"]
+        leg["vs_h200_fastest"] = H200_COLUMN_40[name]["fastest"] / leg["us_min"]
+        out[name] = leg
+    return out
+
+
 def static_c1(device, solves=10):
     """The static configuration as specified: a 32^3 stdBrick cube (1 m, E 50 MPa, nu 0.3, base fixed)
     under a 100 kPa downward top traction, Jacobi-PCG to a 1e-10 relative residual. Plain FP64 CG and
@@ -837,6 +910,7 @@ def run_ours(args):
     cpu = cpu_reference_apply(rf, xn0) if rf is not None and not args.no_cpu else None
     del rf
     static = static_c1(local) if world == 1 and not args.no_serve else None
+    column = column_40(local) if world == 1 and not args.no_serve else None
     line = {"metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded layer properties)",
@@ -858,6 +932,7 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "explicit": explicit,
             "static_c1": static,
+            "column_40": column,
             "served": served,
             "served_mixed": served_mixed,
             "served_rates": served_rates,
@@ -881,9 +956,14 @@ def main():
     ap.add_argument("--launch", default="", help="pin the box launch shape 'variant,kz' (profiling)")
     ap.add_argument("--pimy-box", type=int, default=0,
                     help="only the PressureIndependMultiYield plastic box section, n^3 elements (profiling)")
+    ap.add_argument("--column", action="store_true",
+                    help="only the 40^3 laminar-column legs (the reference's benchmark model)")
     ap.add_argument("--pdmy-box", type=int, default=0,
                     help="only the PressureDependMultiYield plastic force section, n^3 elements (profiling)")
     args = ap.parse_args()
+    if args.column:
+        print(json.dumps(column_40(int(os.environ.get("LOCAL_RANK", "0")), reps=args.steps)))
+        return 0
     if args.pdmy_box:
         print(json.dumps(pdmy_force_box(int(os.environ.get("LOCAL_RANK", "0")), n=args.pdmy_box, evals=args.steps)))
         return 0

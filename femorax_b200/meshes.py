@@ -206,6 +206,47 @@ def heterogeneous_cube(n=100, median_E=80e6, sigma=0.5, nu=0.3, rho=2000.0, seed
     return spec
 
 
+def laminar_column(nx=2, ny=2, nz=8, dx=1.0, dy=1.0, dz=0.5, lumped=True, damping=True, element=0):
+    """The layered soil column of the reference's tests and benchmarks (tests/common/
+    synthetic_models.hpp:24-94): nx x ny x nz bricks (stdBrick, or SSPbrick with element 1, always
+    lumped) of dx x dy x dz with the top at z = 0, a lower and an upper material (E 377 and 109.2 kPa,
+    nu 0.3), body force, base fixed, the side nodes of every elevation above the base tied to the
+    first side node in DOFs 1 2 3 (equalDOF stars), Rayleigh damping over everything and a second
+    region over the top layer (the later region wins)."""
+    NX, NY, NZ = nx + 1, ny + 1, nz + 1
+    tags, coords = block_nodes(nx, ny, nz, dx, dy, dz, origin=(0.0, 0.0, -nz * dz))
+    groups = []
+    for layer in range(2):
+        k0, k1 = (0, nz // 2) if layer == 0 else (nz // 2, nz)
+        et, cn = block_connectivity(nx, ny, nz, k0, k1)
+        groups.append(Group(377000.0 if layer == 0 else 109200.0, 0.3, 2.0285 if layer == 0 else 2.0183, et, cn,
+                            b=(0.0, 0.0, -19.9 if layer == 0 else -19.8), lumped=lumped or element == 1,
+                            element=element))
+    spec = ModelSpec(tags=tags, coords=coords, groups=groups)
+    spec.fix_node, spec.fix_dof = fix_base(nx, ny)
+    ret, con, dof = [], [], []
+    for k in range(1, NZ):
+        master = -1
+        for j in range(NY):
+            for i in range(NX):
+                if not (i == 0 or i == nx or j == 0 or j == ny):
+                    continue
+                t = node_tag(i, j, k, nx, ny)
+                if master < 0:
+                    master = t
+                    continue
+                for d in (1, 2, 3):
+                    ret.append(master)
+                    con.append(t)
+                    dof.append(d)
+    spec.eqd_retained, spec.eqd_constrained, spec.eqd_dof = [np.array(a, np.int32) for a in (ret, con, dof)]
+    if damping:
+        all_e = np.concatenate([g.etags for g in groups])
+        spec.rayleigh = [Rayleigh(0.6, 5.8e-4, 0.0, 0.0, all_e),
+                         Rayleigh(0.9, 3e-4, 1e-4, 0.0, groups[1].etags[-nx * ny:])]
+    return spec
+
+
 def ricker(t, f0=5.0, t0=None, amplitude=1.0):
     """Ricker wavelet of peak frequency f0 (Hz), centred at t0 (default 1.2 / f0)."""
     t0 = 1.2 / f0 if t0 is None else t0

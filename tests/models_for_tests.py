@@ -8,39 +8,10 @@ from femorax_b200 import meshes
 
 def soil_column(nx=3, ny=2, nz=8, lumped=True):
     """The layered column the reference's tests build in memory (tests/common/synthetic_models.hpp
-    shape): stdBrick, lower and upper material, fixed base, side nodes at each elevation tied to
-    the first side node in DOFs 1 2 3, a Rayleigh region over everything and one over the top
-    layer."""
-    NX, NY, NZ = nx + 1, ny + 1, nz + 1
-    tags, coords = meshes.block_nodes(nx, ny, nz, 1.0, 1.0, 0.5, origin=(0.0, 0.0, -nz * 0.5))
-    groups = []
-    for layer in range(2):
-        k0, k1 = (0, nz // 2) if layer == 0 else (nz // 2, nz)
-        et, cn = meshes.block_connectivity(nx, ny, nz, k0, k1)
-        groups.append(meshes.Group(377000.0 if layer == 0 else 109200.0, 0.3, 2.0285 if layer == 0 else 2.0183, et, cn,
-                                   b=(0.0, 0.0, -19.9 if layer == 0 else -19.8), lumped=lumped))
-    spec = meshes.ModelSpec(tags=tags, coords=coords, groups=groups)
-    spec.fix_node, spec.fix_dof = meshes.fix_base(nx, ny)
-    ret, con, dof = [], [], []
-    for k in range(1, NZ):
-        master = -1
-        for j in range(NY):
-            for i in range(NX):
-                if not (i == 0 or i == nx or j == 0 or j == ny):
-                    continue
-                t = meshes.node_tag(i, j, k, nx, ny)
-                if master < 0:
-                    master = t
-                    continue
-                for d in (1, 2, 3):
-                    ret.append(master)
-                    con.append(t)
-                    dof.append(d)
-    spec.eqd_retained, spec.eqd_constrained, spec.eqd_dof = [np.array(a, np.int32) for a in (ret, con, dof)]
-    all_e = np.concatenate([g.etags for g in groups])
-    spec.rayleigh = [meshes.Rayleigh(0.6, 5.8e-4, 0.0, 0.0, all_e),
-                     meshes.Rayleigh(0.9, 3e-4, 1e-4, 0.0, groups[1].etags[-nx * ny:])]
-    return spec
+    shape; meshes.laminar_column): stdBrick, lower and upper material, fixed base, side nodes at
+    each elevation tied to the first side node in DOFs 1 2 3, a Rayleigh region over everything and
+    one over the top layer."""
+    return meshes.laminar_column(nx, ny, nz, lumped=lumped)
 
 
 def two_region_block(nx=4, ny=3, nz=5, lumped=False):
