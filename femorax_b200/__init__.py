@@ -266,6 +266,11 @@ class InternalForce:
         self.device = device
         self.num_equations = mesh.num_equations
 
+    def set_general_mode(self, mode: str):
+        """The Gauss-point path's form: "exact" (the reference's arithmetic, bit for bit) or "fast"
+        (eight threads per element, fused multiply-adds, within 1e-12; elastic stdBrick meshes)."""
+        check(lib().fx_force_set_general_mode(self._h, {"exact": 0, "fast": 1}[mode]))
+
     def set_path(self, path: str):
         check(lib().fx_force_set_path(self._h, self.PATHS[path]))
 

@@ -33,6 +33,7 @@ CXX_COMMON = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" +
 # (source, extra flags)
 CUDA_SOURCES = [
     ("general.cu", ["--fmad=false"]),
+    ("general_fast.cu", []),
     ("box.cu", []),
     ("box_f64_apply.cu", []),
     ("box_f64_force.cu", []),

@@ -218,6 +218,9 @@ struct ForceState {
   // SSPbrick sets: per element the geometry record and the stabilization constants,
   // value k of element e at [k * P + e] (ssp_brick.cuh: kGeo, kCon values)
   bool has_ssp = false;
+  // the Gauss-point path's form: exact (false: the reference's arithmetic order, bit for bit) or
+  // fast (true: eight threads per element, fused multiply-adds; elastic stdBrick sets only)
+  bool fast_general = false;
   DeviceArray<double> ssp_geo, ssp_con;
   // stable time step: the minimum's key (general.cu) and, for the periodic re-check, each
   // element's omega^2 with its reference stability tangent (prepare_stability_bounds)
@@ -240,6 +243,14 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
 void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t st);
 // SSPbrick sets: every element's geometry record and stabilization constants on the device
 void ssp_setup(ForceState& s);
+// the slot gathers of the operator (with the nodal-mass terms) and of the internal force
+void general_gather(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip);
+void general_force_gather(ForceState& s, const double* v, double* f, cudaStream_t st);
+// general_fast.cu: the fast form, where it applies (fast_general set, every set elastic stdBrick)
+bool general_fast_applies(const ForceState& s);
+void general_apply_fast(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st,
+                        const int* skip);
+void general_force_fast(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st);
 // Stable explicit step on the device (one warp per element, the reference's eigen-solve bit for
 // bit): the minimum over the elements of `list` (all elements when NULL, n of them), each
 // element's step into dt_out when given (device, n values). scheme 0 CentralDifference, 1

@@ -634,8 +634,26 @@ static void refuse_pimy_initial(const ForceState& s) {
                                   "PressureIndependMultiYield");
 }
 
+void general_gather(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
+  const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
+  const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
+  if (s.neq > 0)
+    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, k[2], m1, x, k[1], m2,
+                                                   x, y, skip);
+  FX_LAUNCH_CHECK("slot_gather");
+}
+
+void general_force_gather(ForceState& s, const double* v, double* f, cudaStream_t st) {
+  const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
+  if (s.neq > 0)
+    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
+                                                   nullptr, 1.0, m2, v, f, nullptr);
+  FX_LAUNCH_CHECK("slot_gather");
+}
+
 void general_apply(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
   refuse_pimy_initial(s);
+  if (general_fast_applies(s)) return general_apply_fast(s, k, x, y, st, skip);
   if (s.count > 0)
     k_element_apply<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                    s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
@@ -671,6 +689,7 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
 }
 
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
+  if (general_fast_applies(s)) return general_force_fast(s, u, v, f, st);
   if (s.has_j2 || s.has_pimy || s.has_pdmy) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
   if (s.count > 0)
     k_element_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,

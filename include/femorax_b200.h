@@ -164,6 +164,14 @@ typedef struct fx_force fx_force;
 int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out);
 void fx_force_destroy(fx_force* f);
 int fx_force_set_path(fx_force* f, int32_t path);
+/* The Gauss-point path's form (meshes off the box path): FX_GENERAL_EXACT (default) evaluates every
+ * element in the reference's arithmetic order, bit for bit its results; FX_GENERAL_FAST evaluates
+ * elastic stdBrick elements with eight threads each (one per Gauss point) and fused multiply-adds,
+ * within 1e-12 of the largest entry of the exact form, for the operator and the internal force.
+ * Meshes with J2, multi-yield soil or SSPbrick sets keep the exact form. */
+#define FX_GENERAL_EXACT 0
+#define FX_GENERAL_FAST 1
+int fx_force_set_general_mode(fx_force* f, int32_t mode);
 /* info[9] = num_equations, num_elements, path of the operator, box qualifies (0/1), grid nx, ny,
  * nz, device bytes held, force form on the box path (0/1: lumped masses and one beta). */
 int fx_force_info(const fx_force* f, int64_t* info);
