@@ -49,7 +49,7 @@ __device__ __forceinline__ void emit_corner(const double (*part)[kPart], int j, 
 }
 
 // y_e = K_eff,e x_e (element_operator_apply, element_operator.hpp:82-130) for elastic sets.
-__global__ void __launch_bounds__(kThreads) k_apply_fast(const double* __restrict__ coords,
+__global__ void __launch_bounds__(kThreads, 4) k_apply_fast(const double* __restrict__ coords,
                                                          const int32_t* __restrict__ node,
                                                          const int32_t* __restrict__ eq,
                                                          const int32_t* __restrict__ param,
@@ -66,20 +66,17 @@ __global__ void __launch_bounds__(kThreads) k_apply_fast(const double* __restric
   if (ok) load_corner(coords, node, eq, N, P, e, gp, x, nullptr, S.xl[le], S.ve[le], nullptr);
   __syncthreads();
   if (ok) {
-    const ParamGP p = params[param[e]];
+    const ParamGP& p = params[param[e]];
     const OpFactors f = op_factors(p, ks, kd, km);
-    double De[6][6];
-    effective_D(f, p, De);
     PointShape s;
     point_shape(S.xl[le], gp, s);
     const double* xe = S.ve[le];
     double ep[6], sg[6];
     strain_of(s, xe, ep);
-    for (int a = 0; a < 6; ++a) {
-      double sum = 0.0;
-      for (int c = 0; c < 6; ++c) sum += De[a][c] * ep[c];
-      sg[a] = sum;
-    }
+    // elastic sets: D_eff = (cK + c0 + cc) D, D the isotropic matrix
+    elastic_stress(p, ep, sg);
+    const double c = f.cK + f.c0 + f.cc;
+    for (int a = 0; a < 6; ++a) sg[a] *= c;
     double vg[3] = {0.0, 0.0, 0.0};
     if (f.cM != 0.0 && p.mass_type == 0)
       for (int k = 0; k < 8; ++k)
@@ -102,7 +99,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_fast(const double* __restric
 // f_e = internal force + Rayleigh damping forces (StdBrick::compute_with, std_brick.hpp:492-543)
 // for elastic sets: per point the stress and damping stress node forces, minus the body force,
 // plus the alphaM mass force.
-__global__ void __launch_bounds__(kThreads) k_force_fast(const double* __restrict__ coords,
+__global__ void __launch_bounds__(kThreads, 4) k_force_fast(const double* __restrict__ coords,
                                                          const int32_t* __restrict__ node,
                                                          const int32_t* __restrict__ eq,
                                                          const int32_t* __restrict__ param,
@@ -117,7 +114,7 @@ __global__ void __launch_bounds__(kThreads) k_force_fast(const double* __restric
   if (ok) load_corner(coords, node, eq, N, P, e, gp, u, v, S.xl[le], S.ue[le], S.ve[le]);
   __syncthreads();
   if (ok) {
-    const ParamGP p = params[param[e]];
+    const ParamGP& p = params[param[e]];
     PointShape s;
     point_shape(S.xl[le], gp, s);
     const double* ue = S.ue[le];
