@@ -445,18 +445,26 @@ def pdmy_force_box(device, n=40, evals=20):
     force.compute(u_at(2e-4), v, f)
     force.commit_state()
     us = [u_at(2e-4 + 1e-4 * np.sin(0.3 * k)) for k in range(evals + 3)]
-    for k in range(3):
-        force.compute(us[k], v, f)
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for k in range(evals):
-        force.compute(us[3 + k], v, f)
-    e1.record()
-    torch.cuda.synchronize(dev)
-    return {"elements": int(mesh.count), "points": 8 * int(mesh.count), "ms_per_force": e0.elapsed_time(e1) / evals,
-            "plastic_points": int(force.plastic_points()), "failed_points": int(force.pimy_failed()),
-            "reference_h200_ms": 7.85}
+    out = {"elements": int(mesh.count), "points": 8 * int(mesh.count), "reference_h200_ms": 7.85}
+    results = {}
+    for corrector in ("fused", "compacted"):  # every evaluation from the same committed state
+        force.set_soil_corrector(corrector)
+        for k in range(3):
+            force.compute(us[k], v, f)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(evals):
+            force.compute(us[3 + k], v, f)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        results[corrector] = f.cpu().numpy()
+        key = "ms_per_force" if corrector == "fused" else "compacted_ms_per_force"
+        out[key] = e0.elapsed_time(e1) / evals
+    out["compacted_bit_identical"] = bool(np.array_equal(results["fused"], results["compacted"]))
+    out["plastic_points"] = int(force.plastic_points())
+    out["failed_points"] = int(force.pimy_failed())
+    return out
 
 
 def pdmy_points(device, n=1 << 20, steps=10, sample=4096, seed=0):
@@ -538,6 +546,17 @@ PIMY_CLAY = (1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0)  # rho t/m
 
 
 def pimy_explicit(device, n=100, warm=16, steps=64):
+    """pimy_explicit_run with the fused point pass and with the compacted plastic corrector; the two
+    runs' final displacements compared bit for bit."""
+    fused = pimy_explicit_run(device, n, warm, steps, "fused")
+    comp = pimy_explicit_run(device, n, warm, steps, "compacted")
+    u_f, u_c = fused.pop("_u"), comp.pop("_u")
+    fused["compacted"] = comp
+    fused["compacted_bit_identical"] = bool(np.array_equal(u_f, u_c))
+    return fused
+
+
+def pimy_explicit_run(device, n=100, warm=16, steps=64, corrector="fused"):
     """The reference's plastic-box measurement (an n^3 stdBrick box of PressureIndependMultiYield
     clay, 20 surfaces, in the plastic stage, under 0.3 g 2 Hz base shaking, explicit steps of 5e-4 s)
     on the Gauss-point path: ExplicitDifference stage steps (the force with every point's material
@@ -555,6 +574,7 @@ def pimy_explicit(device, n=100, warm=16, steps=64):
     force = fx.InternalForce(mesh, device=device)
     force.set_pimy(0, fx.PressureIndependMultiYield(*PIMY_CLAY[:8], noYieldSurf=int(PIMY_CLAY[8])))
     force.set_material_stage(0, 1)
+    force.set_soil_corrector(corrector)
     dev = torch.device("cuda", device)
     dt = 5e-4
     total = warm + steps
@@ -573,7 +593,7 @@ def pimy_explicit(device, n=100, warm=16, steps=64):
     return {"elements": int(mesh.count), "points": 8 * int(mesh.count), "surfaces": int(PIMY_CLAY[8]),
             "dt_s": dt, "steps_timed": steps, "ms_per_step": ms, "device_bytes": int(force.info()["device_bytes"]),
             "plastic_points_last_step": int(force.plastic_points()), "failed_points": int(force.pimy_failed()),
-            "reference_h200_ms_per_step": 23.5}
+            "reference_h200_ms_per_step": 23.5, "corrector": corrector, "_u": u.cpu().numpy()}
 
 
 def newmark_comparison(device, n=100, steps=20, seed=0):

@@ -266,6 +266,11 @@ class InternalForce:
         self.device = device
         self.num_equations = mesh.num_equations
 
+    def set_soil_corrector(self, mode: str):
+        """The multi-yield soil points' update: "fused" (one pass) or "compacted" (predictor,
+        compaction of the plastic points, corrector on those only); the same bits either way."""
+        check(lib().fx_force_set_soil_corrector(self._h, {"fused": 0, "compacted": 1}[mode]))
+
     def set_general_mode(self, mode: str):
         """The Gauss-point path's form: "exact" (the reference's arithmetic, bit for bit) or "fast"
         (eight threads per element, fused multiply-adds, within 1e-12; elastic stdBrick meshes)."""

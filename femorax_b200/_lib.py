@@ -108,6 +108,7 @@ PROTOTYPES = {
     "fx_device_memory": (C.c_int, [C.c_int32, p_i64, p_i64]),
     "fx_ssp_element_constants": (C.c_int, [p_f64, C.c_double, C.c_double, p_f64, p_f64]),
     "fx_force_set_general_mode": (C.c_int, [vp, C.c_int32]),
+    "fx_force_set_soil_corrector": (C.c_int, [vp, C.c_int32]),
     "fx_apply_operator_host": (C.c_int, [vp, fx_coeffs, vp, vp, vp]),
     "fx_operator_diagonal_host": (C.c_int, [vp, fx_coeffs, vp, vp]),
     "fx_operator_diagonal": (C.c_int, [vp, fx_coeffs, vp, vp]),

@@ -405,6 +405,13 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
 
 void fx_force_destroy(fx_force* f) { delete f; }
 
+int fx_force_set_soil_corrector(fx_force* f, int32_t mode) {
+  return guarded([&] {
+    FX_REQUIRE(f && (mode == FX_SOIL_FUSED || mode == FX_SOIL_COMPACTED), "fx_force_set_soil_corrector: bad arguments");
+    f->s.compact_soil = mode == FX_SOIL_COMPACTED;
+  });
+}
+
 int fx_force_set_general_mode(fx_force* f, int32_t mode) {
   return guarded([&] {
     FX_REQUIRE(f && (mode == FX_GENERAL_EXACT || mode == FX_GENERAL_FAST), "fx_force_set_general_mode: bad arguments");

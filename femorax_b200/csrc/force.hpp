@@ -214,6 +214,11 @@ struct ForceState {
   // [(c * 8 + gp) * P + e];
   // unallocated (NULL) when no soil set is damped
   DeviceArray<double> soil_sd;
+  // the compacted plastic corrector (compact_soil): per point the strain and strain rate of the
+  // predictor, its flag, the list of flagged points, block counts and their total
+  bool compact_soil = false;
+  DeviceArray<double> soil_eps, soil_rate;
+  DeviceArray<int> soil_flag, soil_list, soil_counts, soil_total;
   ExplicitWork xw;
   // SSPbrick sets: per element the geometry record and the stabilization constants,
   // value k of element e at [k * P + e] (ssp_brick.cuh: kGeo, kCon values)

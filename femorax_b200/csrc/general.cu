@@ -192,6 +192,192 @@ __global__ void __launch_bounds__(128, MINB) k_soil_points(const double* __restr
   }
 }
 
+// ---- the compacted plastic corrector (src/exec/compacted_kernels.hpp:1-25, 135-181): the same point
+// updates in three passes, so that the branchy, expensive corrector runs on full warps of plastic
+// points only. 1. predict (one thread per point): strain, the material's predictor; a point that
+// stays elastic is finished (stress, compact tangent, trial state, damping stress), a plastic one is
+// flagged with its strain (and strain rate) kept; 2. compaction: the flagged points listed in point
+// order (block counts, one block's scan, an ordered write), the count left on the device; 3. correct
+// (one thread per listed point): the whole update from the committed state. The corrector is the
+// fused path's function, so every point's results are the fused path's bits.
+FX_HD bool soil_predict(const PimySet& m, const double* eps, int gp, const double* c, double* t, int64_t stride,
+                        double* sg, double* tc, bool* ok) {
+  return pimy::predict_compact(m.p, m.stage, pimy::Slab<const double>{c + gp * stride, 8 * stride},
+                               pimy::Slab<double>{t + gp * stride, 8 * stride}, eps, sg, tc, ok);
+}
+FX_HD bool soil_predict(const PdmySet& m, const double* eps, int gp, const double* c, double* t, int64_t stride,
+                        double* sg, double* tc, bool* ok) {
+  return pdmy::predict_compact(m.p, m.stage, pimy::Slab<const double>{c + gp * stride, 8 * stride},
+                               pimy::Slab<double>{t + gp * stride, 8 * stride}, eps, sg, tc, ok);
+}
+FX_HD bool soil_update_strain(const PimySet& m, const double* eps, int gp, const double* c, double* t, int64_t stride,
+                              double* sg, double* tc, bool* pl) {
+  return pimy::update_compact(m.p, m.stage, pimy::Slab<const double>{c + gp * stride, 8 * stride},
+                              pimy::Slab<double>{t + gp * stride, 8 * stride}, eps, sg, tc, pl);
+}
+FX_HD bool soil_update_strain(const PdmySet& m, const double* eps, int gp, const double* c, double* t, int64_t stride,
+                              double* sg, double* tc, bool* pl) {
+  return pdmy::update_compact(m.p, m.stage, pimy::Slab<const double>{c + gp * stride, 8 * stride},
+                              pimy::Slab<double>{t + gp * stride, 8 * stride}, eps, sg, tc, pl);
+}
+
+// The damping stress of a point from its strain rate: betaK times this update's tangent plus betaKcomm
+// times the committed one (damping_stress's sum, the rate already formed).
+template <class Set, int KTAN>
+__device__ void soil_damping(const Set& m, const ParamGP& p, const double* tc, const double* pc, int gp, int64_t P,
+                             const double rate[6], double sd[6]) {
+  double D[36];
+  soil_compact_D(m, tc, D);
+  for (int i = 0; i < 36; ++i) D[i] = p.betaK * D[i];
+  if (p.betaKcomm != 0.0) add_committed_D(m, pc, gp, P, p.betaKcomm, D);
+  for (int a = 0; a < 6; ++a) {
+    double sum = 0.0;
+    for (int c = 0; c < 6; ++c) sum += D[6 * a + c] * rate[c];
+    sd[a] = sum;
+  }
+}
+
+template <class Set, int KIND, int KTAN, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_soil_predict(const double* __restrict__ coords, const int32_t* __restrict__ node,
+                                                      const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
+                                                      const ParamGP* __restrict__ params, const Set* __restrict__ sets,
+                                                      int32_t N, int32_t P, int32_t count, const double* __restrict__ u,
+                                                      const double* __restrict__ pc, double* __restrict__ pt,
+                                                      double* __restrict__ ptan, double* __restrict__ psig,
+                                                      int* __restrict__ failed, const double* __restrict__ v,
+                                                      double* __restrict__ psd, double* __restrict__ peps,
+                                                      double* __restrict__ prate, int* __restrict__ flag) {
+  const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const int32_t e = static_cast<int32_t>(t % P), gp = static_cast<int32_t>(t / P);
+  bool bad = false;
+  if (gp < 8) {  // every point of the padded batch gets its flag (padding: 0)
+    int f = 0;
+    const ParamGP p = params[param[e < count ? e : 0]];
+    if (e < count && p.kind == KIND) {
+      double xl[3][8], ue[24], eps[6], sg[6], tc[KTAN], rate[6];
+      load_coords(coords, node, N, P, e, xl);
+      for (int a = 0; a < 24; ++a) {
+        const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+        ue[a] = q >= 0 ? u[q] : 0.0;
+      }
+      PointShape s;
+      point_shape(xl, gp, s);
+      strain_of(s, ue, eps);
+      const bool damped = psd && (p.betaK != 0.0 || p.betaKcomm != 0.0);
+      if (damped) {
+        double ve[24];
+        for (int a = 0; a < 24; ++a) {
+          const int32_t q = eq[static_cast<int64_t>(a) * P + e];
+          ve[a] = q >= 0 ? v[q] : 0.0;
+        }
+        strain_of(s, ve, rate);
+      }
+      bool ok = true;
+      if (soil_predict(sets[p.table], eps, gp, pc + e, pt + e, P, sg, tc, &ok)) {
+        f = 1;
+        for (int c = 0; c < 6; ++c) peps[(static_cast<int64_t>(c) * 8 + gp) * P + e] = eps[c];
+        if (damped)
+          for (int c = 0; c < 6; ++c) prate[(static_cast<int64_t>(c) * 8 + gp) * P + e] = rate[c];
+      } else {
+        bad = !ok;
+        for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
+        for (int c = 0; c < KTAN; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
+        if (damped) {
+          double sd[6];
+          soil_damping<Set, KTAN>(sets[p.table], p, tc, pc + e, gp, P, rate, sd);
+          for (int c = 0; c < 6; ++c) psd[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sd[c];
+        }
+      }
+    }
+    flag[t] = f;
+  }
+  const unsigned nb = __popc(__ballot_sync(0xffffffffu, bad));
+  if ((threadIdx.x & 31) == 0 && nb) atomicAdd(failed, static_cast<int>(nb));
+}
+
+constexpr int kScanBlock = 256;
+// Flagged entries per block of kScanBlock.
+__global__ void __launch_bounds__(kScanBlock) k_flag_counts(const int* __restrict__ flag, int64_t n,
+                                                            int* __restrict__ counts) {
+  const int64_t i = blockIdx.x * static_cast<int64_t>(kScanBlock) + threadIdx.x;
+  const int c = __syncthreads_count(i < n && flag[i]);
+  if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+// One block: the exclusive prefix sums of the block counts, in place, and their total.
+__global__ void __launch_bounds__(1024) k_flag_offsets(int* __restrict__ counts, int nb, int* __restrict__ total) {
+  __shared__ int part[1024];
+  const int per = (nb + 1023) / 1024, lo = threadIdx.x * per, hi = min(nb, lo + per);
+  int sum = 0;
+  for (int b = lo; b < hi; ++b) sum += counts[b];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // inclusive scan of the thread sums
+    const int add = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+    __syncthreads();
+    part[threadIdx.x] += add;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;
+  for (int b = lo; b < hi; ++b) {
+    const int c = counts[b];
+    counts[b] = run;
+    run += c;
+  }
+  if (threadIdx.x == 1023) *total = part[1023];
+}
+// The flagged entries' indices in order.
+__global__ void __launch_bounds__(kScanBlock) k_flag_list(const int* __restrict__ flag, int64_t n,
+                                                          const int* __restrict__ offsets, int* __restrict__ list) {
+  __shared__ int warp_base[kScanBlock / 32];
+  const int64_t i = blockIdx.x * static_cast<int64_t>(kScanBlock) + threadIdx.x;
+  const bool f = i < n && flag[i];
+  const unsigned ball = __ballot_sync(0xffffffffu, f);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) warp_base[w] = __popc(ball);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int k = 0; k < kScanBlock / 32; ++k) {
+      const int c = warp_base[k];
+      warp_base[k] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  if (f) list[offsets[blockIdx.x] + warp_base[w] + __popc(ball & ((1u << lane) - 1u))] = static_cast<int>(i);
+}
+
+template <class Set, int KIND, int KTAN, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_soil_correct(const int32_t* __restrict__ param,
+                                                      const ParamGP* __restrict__ params, const Set* __restrict__ sets,
+                                                      int32_t P, const int* __restrict__ list,
+                                                      const int* __restrict__ total, const double* __restrict__ pc,
+                                                      double* __restrict__ pt, double* __restrict__ ptan,
+                                                      double* __restrict__ psig, int* __restrict__ plastic,
+                                                      int* __restrict__ failed, const double* __restrict__ peps,
+                                                      const double* __restrict__ prate, double* __restrict__ psd) {
+  const int n = *total;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int64_t t = list[i];
+    const int32_t e = static_cast<int32_t>(t % P), gp = static_cast<int32_t>(t / P);
+    const ParamGP p = params[param[e]];
+    double eps[6], sg[6], tc[KTAN];
+    for (int c = 0; c < 6; ++c) eps[c] = peps[(static_cast<int64_t>(c) * 8 + gp) * P + e];
+    bool pl = false;
+    const bool ok = soil_update_strain(sets[p.table], eps, gp, pc + e, pt + e, P, sg, tc, &pl);
+    for (int c = 0; c < 6; ++c) psig[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sg[c];
+    for (int c = 0; c < KTAN; ++c) ptan[(static_cast<int64_t>(c) * 8 + gp) * P + e] = tc[c];
+    if (psd && (p.betaK != 0.0 || p.betaKcomm != 0.0)) {
+      double rate[6], sd[6];
+      for (int c = 0; c < 6; ++c) rate[c] = prate[(static_cast<int64_t>(c) * 8 + gp) * P + e];
+      soil_damping<Set, KTAN>(sets[p.table], p, tc, pc + e, gp, P, rate, sd);
+      for (int c = 0; c < 6; ++c) psd[(static_cast<int64_t>(c) * 8 + gp) * P + e] = sd[c];
+    }
+    if (pl) atomicAdd(plastic, 1);
+    if (!ok) atomicAdd(failed, 1);
+  }
+}
+
 // ... then their elements' internal forces from the points' stresses, into the slots
 __global__ void __launch_bounds__(kBlock) k_soil_force(const double* __restrict__ coords, const int32_t* __restrict__ node,
                                                         const int32_t* __restrict__ eq, const int32_t* __restrict__ param,
@@ -688,6 +874,37 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
   FX_LAUNCH_CHECK("slot_gather");
 }
 
+// The compacted corrector's passes for the points of one soil kind (the per-point buffers allocated
+// at the first call: strain and strain rate, 48 bytes per point each, a flag and a list entry).
+template <class Set, int KIND, int KTAN, int MINB>
+void soil_points_compacted(ForceState& s, const Set* sets, const double* u, const double* v, const double* pc,
+                           double* pt, double* ptan, double* psig, cudaStream_t st) {
+  const int64_t points = static_cast<int64_t>(8) * s.P;
+  const unsigned nb = static_cast<unsigned>((points + kScanBlock - 1) / kScanBlock);
+  if (s.soil_eps.n < static_cast<size_t>(6 * points)) {
+    s.soil_eps.alloc(static_cast<size_t>(6 * points));
+    if (s.soil_sd.n) s.soil_rate.alloc(static_cast<size_t>(6 * points));
+    s.soil_flag.alloc(static_cast<size_t>(points));
+    s.soil_list.alloc(static_cast<size_t>(points));
+    s.soil_counts.alloc(nb);
+    s.soil_total.alloc(1);
+  }
+  k_soil_predict<Set, KIND, KTAN, MINB><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
+      s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, sets, s.N, s.P, s.count, u, pc, pt, ptan, psig,
+      s.pimy_failed.ptr, v, s.soil_sd.ptr, s.soil_eps.ptr, s.soil_rate.ptr, s.soil_flag.ptr);
+  FX_LAUNCH_CHECK("soil_predict");
+  k_flag_counts<<<nb, kScanBlock, 0, st>>>(s.soil_flag.ptr, points, s.soil_counts.ptr);
+  k_flag_offsets<<<1, 1024, 0, st>>>(s.soil_counts.ptr, static_cast<int>(nb), s.soil_total.ptr);
+  k_flag_list<<<nb, kScanBlock, 0, st>>>(s.soil_flag.ptr, points, s.soil_counts.ptr, s.soil_list.ptr);
+  FX_LAUNCH_CHECK("soil_compaction");
+  const unsigned cg = static_cast<unsigned>(std::min<int64_t>((points + 127) / 128, static_cast<int64_t>(num_sms()) * 8));
+  k_soil_correct<Set, KIND, KTAN, MINB><<<cg, 128, 0, st>>>(s.param.ptr, s.params.ptr, sets, s.P, s.soil_list.ptr,
+                                                             s.soil_total.ptr, pc, pt, ptan, psig, s.plastic_dev.ptr,
+                                                             s.pimy_failed.ptr, s.soil_eps.ptr, s.soil_rate.ptr,
+                                                             s.soil_sd.ptr);
+  FX_LAUNCH_CHECK("soil_correct");
+}
+
 void general_force(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
   if (general_fast_applies(s)) return general_force_fast(s, u, v, f, st);
   if (s.has_j2 || s.has_pimy || s.has_pdmy) FX_CUDA(cudaMemsetAsync(s.plastic_dev.ptr, 0, sizeof(int), st));
@@ -698,7 +915,14 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
                                                                    s.plastic_dev.ptr, s.ssp_geo.ptr, s.ssp_con.ptr);
   FX_LAUNCH_CHECK("element_force");
   const int64_t points = static_cast<int64_t>(8) * s.P;
-  if (s.has_pimy && s.count > 0) {
+  if (s.has_pimy && s.count > 0 && s.compact_soil) {
+    soil_points_compacted<PimySet, 2, pimy::kTan, 6>(s, s.pimy_dev.ptr, u, v, s.pimy_committed.ptr, s.pimy_trial.ptr,
+                                                      s.pimy_tan.ptr, s.pimy_sig.ptr, st);
+    k_soil_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                               s.params.ptr, s.N, s.P, s.count, v, s.pimy_sig.ptr,
+                                                               s.soil_sd.ptr, s.slots.ptr, 2);
+    FX_LAUNCH_CHECK("pimy_force");
+  } else if (s.has_pimy && s.count > 0) {
     k_soil_points<PimySet, 2, pimy::kTan, 6><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pimy_dev.ptr, s.N, s.P, s.count, u,
         s.pimy_committed.ptr, s.pimy_trial.ptr, s.pimy_tan.ptr, s.pimy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr,
@@ -709,7 +933,14 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
                                                                s.soil_sd.ptr, s.slots.ptr, 2);
     FX_LAUNCH_CHECK("pimy_force");
   }
-  if (s.has_pdmy && s.count > 0) {
+  if (s.has_pdmy && s.count > 0 && s.compact_soil) {
+    soil_points_compacted<PdmySet, 3, pdmy::kTan, 4>(s, s.pdmy_dev.ptr, u, v, s.pdmy_committed.ptr, s.pdmy_trial.ptr,
+                                                      s.pdmy_tan.ptr, s.pdmy_sig.ptr, st);
+    k_soil_force<<<grid_for(s.count, kBlock), kBlock, 0, st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
+                                                               s.params.ptr, s.N, s.P, s.count, v, s.pdmy_sig.ptr,
+                                                               s.soil_sd.ptr, s.slots.ptr, 3);
+    FX_LAUNCH_CHECK("pdmy_force");
+  } else if (s.has_pdmy && s.count > 0) {
     k_soil_points<PdmySet, 3, pdmy::kTan, 4><<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(
         s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr, s.params.ptr, s.pdmy_dev.ptr, s.N, s.P, s.count, u,
         s.pdmy_committed.ptr, s.pdmy_trial.ptr, s.pdmy_tan.ptr, s.pdmy_sig.ptr, s.plastic_dev.ptr, s.pimy_failed.ptr,

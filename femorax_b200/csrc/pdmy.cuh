@@ -861,6 +861,21 @@ FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, co
   return pt.ok;
 }
 
+// The compacted corrector's predictor (the reference's PressureDependMultiYield::predict,
+// pressure_depend_multi_yield.hpp:260-283): the elastic predictor; a point that stays elastic is
+// finished as update_compact finishes it and false returned; otherwise true, and update_compact
+// redoes the update (predictor and corrector: the same bits as the fused path).
+template <class CV, class TV>
+FX_PIMY_HD inline bool predict_compact(const Params& p, int stage, CV C, TV T, const double* eps, double* sig,
+                                       double* t, bool* ok) {
+  Point<CV, TV> pt(p, stage, C, T);
+  if (pt.predict(eps)) return true;
+  pt.finish(sig, nullptr);
+  pt.compact(t);
+  *ok = pt.ok;
+  return false;
+}
+
 // The tangent at the committed state in compact form t[kTan] (betaKcomm damping; the reference's
 // PressureDependMultiYield::committed_tangent, src/physics/materials/
 // pressure_depend_multi_yield.hpp:186-200): the reference elastic tangent in the elastic stage or

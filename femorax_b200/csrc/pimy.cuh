@@ -657,7 +657,9 @@ struct Point {
     compact_D(t, D);
   }
 
-  FX_PIMY_HD void run(const double* eps) {  // setTrialStrain + getStress
+  // setTrialStrain + getStress; with `stop`, the compacted corrector's predictor: returns true at the
+  // first stress correction (the trial state then is partial: update_compact redoes the update)
+  FX_PIMY_HD bool run(const double* eps, bool stop = false) {
     cur.load(C, S_STRESS);
     strain.load(C, S_STRAIN);
     active_c = static_cast<int>(C[S_ACTIVE]);
@@ -679,7 +681,7 @@ struct Point {
       for (int i = 0; i < 6; i++)
         for (int j = 0; j < 6; j++) a[j] += D[6 * j + i] * r[i];
       trial.from_full(a, false);
-      return;
+      return false;
     }
     active = active_c;
     sub = rate;
@@ -693,6 +695,7 @@ struct Point {
       if (i == 0) set_trial_stress(cur);
       else set_trial_stress(trial);
       if (active == 0 && !crossing_next()) continue;
+      if (stop) return true;
       if (active == 0) active++;
       correct(0);
       move_active_surface();
@@ -702,6 +705,7 @@ struct Point {
     double dv[6];
     vset(dv, trial.d);
     trial.from_dev(dv, vol);
+    return false;
   }
 
   FX_PIMY_HD void finish(double* sig, double* D) {  // the tangent (D may be NULL), the outputs, the trial state
@@ -745,6 +749,23 @@ FX_PIMY_HD inline bool update_compact(const Params& p, int stage, CV C, TV T, co
   pt.compact(t);
   *plastic = stage == 1 && pt.active > 0;
   return pt.ok;
+}
+
+// The compacted corrector's predictor (the reference's PressureIndependMultiYield::predict,
+// pressure_independ_multi_yield.hpp:243-253): the update up to its first stress correction. A point
+// that needs none is finished as update_compact finishes it (stress, compact tangent, trial state)
+// and false returned; otherwise true, and update_compact redoes the whole update (the same
+// function: the same bits as the fused path).
+template <class CV, class TV>
+FX_PIMY_HD inline bool predict_compact(const Params& p, int stage, CV C, TV T, const double* eps, double* sig,
+                                       double* t, bool* ok) {
+  Point<CV, TV> pt(p, stage, C, T);
+  pt.full = false;
+  if (pt.run(eps, true)) return true;
+  pt.finish(sig, nullptr);
+  pt.compact(t);
+  *ok = pt.ok;
+  return false;
 }
 
 // The tangent at the committed state in compact form t[kTan] (betaKcomm damping; the reference's

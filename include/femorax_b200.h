@@ -169,6 +169,14 @@ int fx_force_set_path(fx_force* f, int32_t path);
  * elastic stdBrick elements with eight threads each (one per Gauss point) and fused multiply-adds,
  * within 1e-12 of the largest entry of the exact form, for the operator and the internal force.
  * Meshes with J2, multi-yield soil or SSPbrick sets keep the exact form. */
+/* The multi-yield soil points' update: FX_SOIL_FUSED (default) updates every point in one pass;
+ * FX_SOIL_COMPACTED runs the compacted plastic corrector (src/exec/compacted_kernels.hpp): a
+ * predictor pass that finishes the points that stay elastic and flags the others, a compaction
+ * that lists the flagged points in order, and the corrector on the listed points only. Both give
+ * every point the same bits. */
+#define FX_SOIL_FUSED 0
+#define FX_SOIL_COMPACTED 1
+int fx_force_set_soil_corrector(fx_force* f, int32_t mode);
 #define FX_GENERAL_EXACT 0
 #define FX_GENERAL_FAST 1
 int fx_force_set_general_mode(fx_force* f, int32_t mode);
