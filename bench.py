@@ -596,8 +596,8 @@ def pimy_explicit_run(device, n=100, warm=16, steps=64, corrector="fused"):
             "reference_h200_ms_per_step": 23.5, "corrector": corrector, "_u": u.cpu().numpy()}
 
 
-def newmark_comparison(device, n=100, steps=20, seed=0):
-    """The Newmark configuration on a bounded sample of its steps: a heterogeneous cube of n^3 boxes (per-element
+def newmark_comparison(device, n=100, steps=200, seed=0):
+    """The Newmark configuration at its 200 steps: a heterogeneous cube of n^3 boxes (per-element
     E log-normal, median 80 MPa, sigma 0.5; nu 0.3; base fixed), a harmonic horizontal surface load,
     Newmark beta 0.25 gamma 0.5 with one inner solve per step to a 1e-8 relative FP64 residual:
     plain FP64 CG against FP32 CG inside FP64 refinement. Steps/s by wall clock around each run
@@ -703,105 +703,90 @@ def batched_j2_comparison(device, count=32, steps=8, seed=1):
             "converged": bool(b.converged and all(r.converged for r in single)), "bit_identical": bool(same)}
 
 
-def serve_comparison(device, count=32, seed=1):
-    """Solves/s and p50/p99 latency at a 1e-8 relative FP64 residual on a stream of static solves
-    on resident meshes (structured blocks, log-uniform 1e4 - 5e5 equations, all arriving at once;
-    the meshes' compile step, device maps and the plain arm's solvers are set up before timing):
-    the batched mixed-precision engine behind the serving loop versus the same stream solved one at
-    a time by plain FP64 Jacobi-PCG. Latency runs from arrival to the solution on the host."""
+def served_streams(device, count=1000, rates=((10.0, 40), (100.0, 400), (500.0, 400), (2000.0, 1000)), seed=3,
+                   models=32, j2_models=12):
+    """The served configuration at its sizes, on resident models (serving.pooled_stream: `models`
+    elastic blocks log-uniform in 1e4 - 2e6 equations, `j2_models` J2 blocks as the batched J2
+    sample's, every request its own load), each stream through three arms:
+      - mixed_batched: the serving loop over the batched engine, FP32 inner solves inside FP64
+        refinement (the served form);
+      - fp64_batched: the same loop and engine with FP64 inner solves (batching without reduced
+        precision: the ablation that splits the speed-up into batching and precision);
+      - plain_fp64_one_at_a_time: first come first served, each request alone by the plain FP64 path.
+    Static solves end at a 1e-8 relative FP64 residual; J2 requests run one cyclic top-shear cycle
+    of 8 load steps (Newton to 1e-6 N) in cohorts beside them. Streams: `count` static solves all
+    at t = 0 ("served"), `count` mixed requests (70 % static, 30 % J2) all at t = 0
+    ("served_mixed", the J2 results of the batched and one-at-a-time arms compared bit for bit),
+    and the mixed stream with Poisson arrivals at each (rate, requests) of `rates` in real time
+    ("served_rates"). Before timing, one request of every model goes through every arm (the
+    models' resident state, module loading, each model's first solve). Latency runs from arrival to
+    the result on the host; solves/s is requests over the arm's wall time, arrival window included."""
     import femorax_b200 as fx
     from femorax_b200 import serving
-    reqs = serving.synthetic_stream(count, rate=1e9, min_dof=1e4, max_dof=5e5, seed=seed)
-    warm = [serving.Request(10_000 + i, 4, 4, 4) for i in range(2)]
-    prepared, solvers = serving.resident(reqs + warm, device)
-    eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
+    opts = fx.SolveOptions(relative_tolerance=1e-8)
+    engines = {"mixed_batched": fx.BatchEngine(1 << 26, 256, options=opts, device=device),
+               "fp64_batched": fx.BatchEngine(1 << 26, 256, options=opts, inner_tolerance=0.5e-8, inner="fp64",
+                                              device=device)}
+    cache = {}
 
-    def server():
-        return serving.Server(eng, device=device, prepare_fn=lambda r, d: prepared[r.id])
+    def arms(reqs, realtime):
+        prepared, solvers, host = serving.resident(reqs, device, j2_host=True, cache=cache)
+        prep = {r.id: host[r.id] if isinstance(r, serving.J2Request) else prepared[r.id] for r in reqs}
+        out = {}
+        for name, eng in engines.items():
+            srv = serving.Server(eng, device=device, prepare_fn=lambda r, d: prep[r.id])
+            out[name] = srv.run(reqs, realtime=realtime)
+        out["plain_fp64_one_at_a_time"] = serving.serve_one_at_a_time(reqs, 1e-8, realtime=realtime, device=device,
+                                                                      prepared=prepared, solvers=solvers)
+        return out
 
-    server().run(warm, realtime=False)  # untimed: module loading, first launches, graph set-up
-    serving.serve_one_at_a_time(warm, realtime=False, device=device, prepared=prepared, solvers=solvers)
-    mixed, wall_m = server().run(reqs, realtime=False)
-    plain, wall_p = serving.serve_one_at_a_time(reqs, 1e-8, realtime=False, device=device, prepared=prepared,
-                                                solvers=solvers)
-    m, p = serving.summary(mixed, wall_m), serving.summary(plain, wall_p)
-    return {"stream": f"{count} static solves on resident structured blocks, log-uniform 1e4-5e5 equations, "
-                      f"all at t=0 (seed {seed}), rtol 1e-8 in FP64",
-            "equations": int(sum(r.equations for r in reqs)),
-            "mixed_batched": {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
-            "plain_fp64_one_at_a_time": {k: p[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
-            "speedup_solves_per_s": m["solves_per_s"] / p["solves_per_s"] if p["solves_per_s"] else None,
-            "engine_rounds": eng.info()["rounds"]}
+    def report(runs, reqs):
+        rep = {}
+        for name, (served, wall) in runs.items():
+            m = serving.summary(served, wall)
+            rep[name] = {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged", "wall_s")}
+        plain = rep["plain_fp64_one_at_a_time"]["solves_per_s"]
+        for name in engines:
+            rep[name]["speedup_solves_per_s"] = rep[name]["solves_per_s"] / plain if plain else None
+        rep["requests"] = len(reqs)
+        rep["j2_requests"] = sum(isinstance(r, serving.J2Request) for r in reqs)
+        rep["equations"] = int(sum(r.equations for r in reqs))
+        return rep
 
+    t_prep = time.perf_counter()
 
-def serve_mixed_comparison(device, count=32, seed=2):
-    """The served mixed stream on a bounded sample: `count` requests all arriving at once, 70 % static
-    solves as in serve_comparison and 30 % J2 load paths (the batched J2 sample's instances: nx = ny
-    in {1, 2, 4, 8}, nz in [20, 40], one cyclic top-shear cycle of 8 load steps). The serving loop
-    (BatchEngine slots for the static solves, J2 cohorts of up to 32 beside them) against the same
-    stream solved one at a time by the plain FP64 path. The J2 results of the two arms are compared
-    bit for bit."""
-    import femorax_b200 as fx
-    from femorax_b200 import serving
-    reqs = serving.mixed_stream(count, rate=1e9, j2_share=0.3, min_dof=1e4, max_dof=5e5, seed=seed,
-                                j2_sizes=(1, 2, 4, 8), j2_nz=(20, 40))
-    prepared, solvers = serving.resident(reqs, device)
-    server_prep = {r.id: serving.prepare_j2(r, device) if isinstance(r, serving.J2Request) else prepared[r.id]
-                   for r in reqs}
-    eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
+    def stream(n, rate, j2_share=0.3, s=seed):
+        return serving.pooled_stream(n, rate, models=models, j2_models=j2_models, j2_share=j2_share, seed=s)
 
-    def server():
-        return serving.Server(eng, device=device, prepare_fn=lambda r, d: server_prep[r.id])
-
-    # untimed: the whole stream once through each arm (module loading, first launches, graph
-    # set-up of every cohort and solver size), as a serving process that has run a while
-    server().run(reqs, realtime=False)
-    serving.serve_one_at_a_time(reqs, realtime=False, device=device, prepared=prepared, solvers=solvers)
-    mixed, wall_m = server().run(reqs, realtime=False)
-    plain, wall_p = serving.serve_one_at_a_time(reqs, 1e-8, realtime=False, device=device, prepared=prepared,
-                                                solvers=solvers)
-    m, p = serving.summary(mixed, wall_m), serving.summary(plain, wall_p)
-    j2_ids = [r.id for r in reqs if isinstance(r, serving.J2Request)]
-    pm, pp = {s.id: s for s in mixed}, {s.id: s for s in plain}
-    same = all(np.array_equal(pm[i].x, pp[i].x) and np.array_equal(pm[i].result.monitor, pp[i].result.monitor)
-               for i in j2_ids)
-    return {"stream": f"{count} requests all at t=0 (seed {seed}): {count - len(j2_ids)} static solves on "
-                      f"structured blocks (log-uniform 1e4-5e5 equations, rtol 1e-8 in FP64), {len(j2_ids)} J2 "
-                      f"load paths (nx = ny in {{1, 2, 4, 8}}, nz in [20, 40], one cycle of 8 load steps)",
-            "mixed_batched": {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
-            "plain_fp64_one_at_a_time": {k: p[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
-            "speedup_solves_per_s": m["solves_per_s"] / p["solves_per_s"] if p["solves_per_s"] else None,
-            "j2_bit_identical": bool(same)}
-
-
-def serve_rate_sweep(device, rates=(20.0, 200.0, 2000.0), count=24, seed=3):
-    """The mixed stream (70 % static solves, 30 % J2 load paths, sizes as serve_mixed_comparison)
-    with Poisson arrivals at each rate in `rates` requests/s, served in real time: solves/s and
-    p50/p99 latency from arrival to result, for the serving loop and for plain FP64 one at a
-    time."""
-    import femorax_b200 as fx
-    from femorax_b200 import serving
-    out = []
-    eng = fx.BatchEngine(1 << 26, 256, options=fx.SolveOptions(relative_tolerance=1e-8), device=device)
-    warm = True
-    for i, rate in enumerate(rates):
-        reqs = serving.mixed_stream(count, rate=rate, j2_share=0.3, min_dof=1e4, max_dof=5e5, seed=seed + i,
-                                    j2_sizes=(1, 2, 4, 8), j2_nz=(20, 40))
-        prepared, solvers = serving.resident(reqs, device)
-        server_prep = {r.id: serving.prepare_j2(r, device) if isinstance(r, serving.J2Request) else prepared[r.id]
-                       for r in reqs}
-        srv = serving.Server(eng, device=device, prepare_fn=lambda r, d: server_prep[r.id])
-        if warm:  # untimed: the first stream once through each arm, all at once
-            srv.run(reqs, realtime=False)
-            serving.serve_one_at_a_time(reqs, realtime=False, device=device, prepared=prepared, solvers=solvers)
-            warm = False
-        mixed, wall_m = srv.run(reqs, realtime=True)
-        plain, wall_p = serving.serve_one_at_a_time(reqs, 1e-8, realtime=True, device=device, prepared=prepared,
-                                                    solvers=solvers)
-        m, p = serving.summary(mixed, wall_m), serving.summary(plain, wall_p)
-        out.append({"rate_per_s": rate, "requests": count,
-                    "mixed_batched": {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")},
-                    "plain_fp64_one_at_a_time": {k: p[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged")}})
+    # untimed: one request of every model through every arm
+    firsts = {}
+    for r in stream(40 * (models + j2_models), 1e9, s=seed):
+        firsts.setdefault(serving.model_key(r), r)
+    warm = sorted(firsts.values(), key=lambda r: r.id)
+    arms(warm, False)
+    static = stream(count, 1e9, j2_share=0.0)
+    out = {"models": f"{models} elastic blocks (log-uniform 1e4-2e6 equations, E U[50,200] MPa, nu U[0.25,0.40]) and "
+                     f"{j2_models} J2 blocks (nx = ny in {{1,2,4,8}}, nz in [20,40], sigma_y U[50,200] kPa, one cycle of "
+                     f"8 load steps) resident on the device ({len(warm)} of them in use); each request its own load "
+                     f"(static: top traction q U[-150,-50] kPa)",
+           "preparation_s": time.perf_counter() - t_prep}
+    out["served"] = report(arms(static, False), static)
+    mixed = stream(count, 1e9, s=seed + 1)
+    runs = arms(mixed, False)
+    out["served_mixed"] = report(runs, mixed)
+    pm = {x.id: x for x in runs["mixed_batched"][0]}
+    pp = {x.id: x for x in runs["plain_fp64_one_at_a_time"][0]}
+    j2 = [r.id for r in mixed if isinstance(r, serving.J2Request)]
+    out["served_mixed"]["j2_bit_identical"] = bool(all(
+        np.array_equal(pm[i].x, pp[i].x) and np.array_equal(pm[i].result.monitor, pp[i].result.monitor) for i in j2))
+    rates_out = []
+    for i, (rate, n) in enumerate(rates):
+        reqs = stream(n, rate, s=seed + 2 + i)
+        r = report(arms(reqs, True), reqs)
+        r["rate_per_s"] = rate
+        rates_out.append(r)
+    out["served_rates"] = rates_out
+    out["seconds"] = time.perf_counter() - t_prep
     return out
 
 
@@ -909,6 +894,24 @@ def run_ours(args):
     total_ms = max_over_ranks([total_ms], dist, dev)[0]
     value = replica_value(world, neq, args.steps, total_ms)
 
+    # the FP32 apply (the precision form) on the same x, timed the same way, outside the FP64 figures
+    x32 = x.float()
+    y32 = torch.zeros(neq, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        force.apply_operator(k, x32, y32, stream)
+    f32_ms = []
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        a32, b32 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a32.record(stream)
+        force.apply_operator(k, x32, y32, stream)
+        b32.record(stream)
+        f32_ms.append((a32, b32))
+    torch.cuda.synchronize(dev)
+    f32_ms = [a32.elapsed_time(b32) for a32, b32 in f32_ms]
+    f32_err = float(((y32.double() - y).abs().max() / y.abs().max()).item())
+    del x32, y32
+
     # e2e: the public host-buffer call, copies included
     xh = torch.empty(neq, dtype=torch.float64, pin_memory=True)
     xh.copy_(x.cpu())
@@ -927,6 +930,11 @@ def run_ours(args):
     alg = algorithmic_bytes(neq, n_el, n_nodes)
     achieved = alg / (total_ms / args.steps * 1e-3) / 1e9
     traffic = load_traffic()
+    alg32 = alg - 8 * neq  # x read and y written as 4-byte values
+    ach32 = alg32 / (float(np.mean(f32_ms)) * 1e-3) / 1e9
+    f32 = {"ms_per_apply": float(np.mean(f32_ms)), "gdof_per_s": neq / (float(np.mean(f32_ms)) * 1e-3) / 1e9,
+           "achieved_gbs": ach32, "frac": ach32 / peak, "algorithmic_bytes_per_launch": alg32,
+           "max_rel_err_vs_fp64": f32_err}
 
     if dist:
         dist.barrier()
@@ -934,9 +942,7 @@ def run_ours(args):
     if rank != 0:
         return 0
     explicit = explicit_comparison(force, mesh, comp, local) if world == 1 and not args.no_serve else None
-    served = serve_comparison(local) if world == 1 and not args.no_serve else None
-    served_mixed = serve_mixed_comparison(local) if world == 1 and not args.no_serve else None
-    served_rates = serve_rate_sweep(local) if world == 1 and not args.no_serve else None
+    streams = served_streams(local) if world == 1 and not args.no_serve else None
     batched_j2 = batched_j2_comparison(local) if world == 1 and not args.no_serve else None
     newmark = newmark_comparison(local) if world == 1 and not args.no_serve else None
     pimy = pimy_points(local) if world == 1 and not args.no_serve else None
@@ -963,6 +969,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg},
+            "fp32_apply": f32,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * neq, "d2h_bytes_per_step": 8 * neq,
                     "ms_per_step": float(np.mean(e_ms)), "ms_per_step_min": float(np.min(e_ms)),
@@ -974,13 +981,18 @@ def run_ours(args):
             "explicit": explicit,
             "static_c1": static,
             "column_40": column,
-            "served": served,
-            "served_mixed": served_mixed,
-            "served_rates": served_rates,
             "batched_j2": batched_j2,
             "newmark": newmark,
             "pimy": pimy,
             "pdmy": pdmy}
+    # the served figures last, so that they stay in view at the end of the line
+    if streams is not None:
+        line["served_models"] = streams["models"]
+        line["served_seconds"] = streams["seconds"]
+        line["served_preparation_s"] = streams["preparation_s"]
+        line["served_rates"] = streams["served_rates"]
+        line["served_mixed"] = streams["served_mixed"]
+        line["served"] = streams["served"]
     print(json.dumps(line))
     return 0
 
@@ -997,11 +1009,19 @@ def main():
     ap.add_argument("--launch", default="", help="pin the box launch shape 'variant,kz' (profiling)")
     ap.add_argument("--pimy-box", type=int, default=0,
                     help="only the PressureIndependMultiYield plastic box section, n^3 elements (profiling)")
+    ap.add_argument("--served", type=int, default=0,
+                    help="only the served streams, this many requests per stream (profiling)")
     ap.add_argument("--column", action="store_true",
                     help="only the 40^3 laminar-column legs (the reference's benchmark model)")
     ap.add_argument("--pdmy-box", type=int, default=0,
                     help="only the PressureDependMultiYield plastic force section, n^3 elements (profiling)")
     args = ap.parse_args()
+    if args.served:
+        n = args.served
+        print(json.dumps(served_streams(int(os.environ.get("LOCAL_RANK", "0")), count=n,
+                                        rates=((10.0, max(10, n // 16)), (100.0, max(10, 2 * n // 5)),
+                                               (500.0, max(10, 2 * n // 5)), (2000.0, n)))))
+        return 0
     if args.column:
         print(json.dumps(column_40(int(os.environ.get("LOCAL_RANK", "0")), reps=args.steps)))
         return 0

@@ -765,16 +765,25 @@ class BatchEngine:
     admit() takes an InternalForce (kept alive here until its slot is retired) and a host
     right-hand side; round() advances every running slot by one refinement round; finished() and
     retire() hand results back. try_admit() returns None instead of raising when the engine is full.
+    inner="fp64" makes the inner solves FP64 Jacobi-PCG with the FP64 operator (the batched engine
+    without reduced precision; give an inner_tolerance at or below the outer relative tolerance).
+    The same InternalForce may be admitted into several slots at once (its maps and tables are only
+    read); each slot has its own vectors.
     """
 
     def __init__(self, capacity: int, max_slots: int, k: OperatorCoefficients = None, options: SolveOptions = None,
-                 inner_tolerance: float = 1e-4, device: int = 0):
+                 inner_tolerance: float = 1e-4, device: int = 0, inner: str = "fp32"):
         o = options or SolveOptions(relative_tolerance=1e-8)
         k = k or OperatorCoefficients()
         opts = L.fx_solve_opts(o.relative_tolerance, o.absolute_tolerance, o.max_iterations, o.lanes, o.restart, 0)
         h = C.c_void_p()
         check(lib().fx_engine_create(device, capacity, max_slots, k.c(), opts, inner_tolerance, C.byref(h)))
         self._h = h
+        if inner not in ("fp32", "fp64"):
+            raise ValueError("inner must be 'fp32' or 'fp64'")
+        self.inner = inner
+        if inner == "fp64":
+            check(lib().fx_engine_set_precision(h, L.FX_ENGINE_INNER_FP64))
         self.device = device
         self._forces = {}
 

@@ -33,6 +33,8 @@ FX_SOLVER_CG = 0
 FX_SOLVER_GMRES = 1
 FX_SOLVER_KRYLOV = 2
 FX_SOLVER_IR = 3
+FX_ENGINE_INNER_FP32 = 0
+FX_ENGINE_INNER_FP64 = 1
 
 p_i32 = C.POINTER(C.c_int32)
 p_i64 = C.POINTER(C.c_int64)
@@ -192,6 +194,7 @@ PROTOTYPES = {
     "fx_engine_create": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, fx_coeffs, fx_solve_opts, C.c_double,
                                    C.POINTER(vp)]),
     "fx_engine_destroy": (None, [vp]),
+    "fx_engine_set_precision": (C.c_int, [vp, C.c_int32]),
     "fx_engine_admit": (C.c_int, [vp, vp, p_f64, C.POINTER(C.c_int32)]),
     "fx_engine_round": (C.c_int, [vp, C.POINTER(C.c_int32)]),
     "fx_engine_finished": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_int32)]),

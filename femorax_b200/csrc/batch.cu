@@ -56,6 +56,10 @@ struct SlotDev {
 
 __device__ __forceinline__ int slot_of_chunk(const int* chunk_slot, int64_t c) { return chunk_slot[c]; }
 
+// a fused multiply-add in the inner solve's precision
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+
 // chunk sums of x.y (T accumulated in double, fused multiply-adds, lane order) of the chunks of
 // slots whose flag `gate` is 0; column `col` of part
 template <class T>
@@ -169,11 +173,12 @@ __global__ void k_b_outer(double* sc, int* fl, const int* used, int nslots, doub
   f[G_INNER_RAN] = 1;
 }
 
-// inner setup: r32 = (float) r, d = 0; CG begin from d = 0 (K d = 0): rr = r32, z = inv r32,
-// p = z; chunk sums of rr.rr (column 0) and rr.z (column 1, at part + ld)
+// inner setup (TI: the inner solve's type): ri = (TI) r, d = 0; CG begin from d = 0 (K d = 0):
+// rr = ri, z = inv ri, p = z; chunk sums of rr.rr (column 0) and rr.z (column 1, at part + ld)
+template <class TI>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_b_inner_begin(const double* __restrict__ r, float* __restrict__ r32, float* __restrict__ d,
-                    float* __restrict__ rr, float* __restrict__ p, const float* __restrict__ inv, int64_t nchunks,
+    k_b_inner_begin(const double* __restrict__ r, TI* __restrict__ r32, TI* __restrict__ d,
+                    TI* __restrict__ rr, TI* __restrict__ p, const TI* __restrict__ inv, int64_t nchunks,
                     const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, const int* __restrict__ fl,
                     int lanes, double* __restrict__ part, int64_t ld) {
   const int lane = threadIdx.x & 31;
@@ -186,16 +191,16 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
   lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<double, 1>{{r[i]}}; },
                [&](int64_t i, const Ops<double, 1>& o) {
-                 r32[i] = static_cast<float>(o.v[0]);
-                 d[i] = 0.f;
+                 r32[i] = static_cast<TI>(o.v[0]);
+                 d[i] = TI(0);
                });
   __syncwarp();
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<float, 2>{{r32[i], inv[i]}}; },
-                 [&](int64_t i, const Ops<float, 2>& o) {
-                   const float ri = fmaf(-1.f, 0.f, o.v[0]);
-                   const float zi = o.v[1] * ri;
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<TI, 2>{{r32[i], inv[i]}}; },
+                 [&](int64_t i, const Ops<TI, 2>& o) {
+                   const TI ri = fma_t(TI(-1), TI(0), o.v[0]);
+                   const TI zi = o.v[1] * ri;
                    rr[i] = ri;
                    p[i] = zi;
                    srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
@@ -247,28 +252,29 @@ __global__ void k_b_alpha(double* sc, int* fl, const int* used, int nslots) {
 }
 
 // d += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (column 1 at part + ld)
+template <class TI>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_b_update(const double* __restrict__ sc, const int* __restrict__ fl, const float* __restrict__ p,
-               const float* __restrict__ ap, const float* __restrict__ inv, float* __restrict__ d,
-               float* __restrict__ rr, int64_t nchunks, const int* __restrict__ chunk_slot,
+    k_b_update(const double* __restrict__ sc, const int* __restrict__ fl, const TI* __restrict__ p,
+               const TI* __restrict__ ap, const TI* __restrict__ inv, TI* __restrict__ d,
+               TI* __restrict__ rr, int64_t nchunks, const int* __restrict__ chunk_slot,
                const SlotDev* __restrict__ sd, int lanes, double* __restrict__ part, int64_t ld) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
   const int s = slot_of_chunk(chunk_slot, c);
   if (s < 0 || fl[s * NFL + F_DONE]) return;
-  const float alpha = static_cast<float>(sc[s * NSC + S_ALPHA]);
+  const TI alpha = static_cast<TI>(sc[s * NSC + S_ALPHA]);
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
   double srr = 0.0, srz = 0.0;
   if (lane < lanes)
-    lane_loop<4>(begin, len, lane, lanes, [&](int64_t i) { return Ops<float, 5>{{p[i], ap[i], inv[i], d[i], rr[i]}}; },
-                 [&](int64_t i, const Ops<float, 5>& o) {
-                   d[i] = fmaf(alpha, o.v[0], o.v[3]);
-                   const float ri = fmaf(-alpha, o.v[1], o.v[4]);
+    lane_loop<4>(begin, len, lane, lanes, [&](int64_t i) { return Ops<TI, 5>{{p[i], ap[i], inv[i], d[i], rr[i]}}; },
+                 [&](int64_t i, const Ops<TI, 5>& o) {
+                   d[i] = fma_t(alpha, o.v[0], o.v[3]);
+                   const TI ri = fma_t(-alpha, o.v[1], o.v[4]);
                    rr[i] = ri;
-                   const float zi = o.v[2] * ri;
+                   const TI zi = o.v[2] * ri;
                    srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
                    srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
                  });
@@ -307,26 +313,28 @@ __global__ void k_b_beta(double* sc, int* fl, const int* used, int nslots) {
 
 // p = inv rr + beta p (the beta of a slot that finished this iteration is stale: its p is
 // never read again)
+template <class TI>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_b_p(const double* __restrict__ sc, const int* __restrict__ fl, const float* __restrict__ inv,
-          const float* __restrict__ rr, float* __restrict__ p, int64_t nchunks, const int* __restrict__ chunk_slot,
+    k_b_p(const double* __restrict__ sc, const int* __restrict__ fl, const TI* __restrict__ inv,
+          const TI* __restrict__ rr, TI* __restrict__ p, int64_t nchunks, const int* __restrict__ chunk_slot,
           const SlotDev* __restrict__ sd) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
   const int s = slot_of_chunk(chunk_slot, c);
   if (s < 0 || fl[s * NFL + F_DONE]) return;
-  const float beta = static_cast<float>(sc[s * NSC + S_BETA]);
+  const TI beta = static_cast<TI>(sc[s * NSC + S_BETA]);
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<float, 3>{{p[i], inv[i], rr[i]}}; },
-               [&](int64_t i, const Ops<float, 3>& o) { p[i] = fmaf(beta, o.v[0], o.v[1] * o.v[2]); });
+  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<TI, 3>{{p[i], inv[i], rr[i]}}; },
+               [&](int64_t i, const Ops<TI, 3>& o) { p[i] = fma_t(beta, o.v[0], o.v[1] * o.v[2]); });
 }
 
 // x += (double) d for slots that ran an inner solve this round; the round's counters
+template <class TI>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_b_correct(const float* __restrict__ d, double* __restrict__ x, int64_t nchunks,
+    k_b_correct(const TI* __restrict__ d, double* __restrict__ x, int64_t nchunks,
                 const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, const int* __restrict__ fl) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
@@ -381,12 +389,17 @@ struct Engine {
   // vectors over the capacity
   DeviceArray<double> b, x, r, ap, inv;
   DeviceArray<float> r32, d32, rr32, p32, ap32, inv32;
+  // FP64 inner solves (fx_engine_set_precision): the inner vectors in double, the preconditioner
+  // inv, the operator's FP64 form on p64 -> ap64
+  bool inner64 = false;
+  DeviceArray<double> r64, d64, rr64, p64, ap64;
   DeviceArray<int> chunk_slot;
   DeviceArray<double> part;  // [2][nchunks]
   DeviceArray<double> sc;
   DeviceArray<int> fl, used_dev, zeros;
   DeviceArray<SlotDev> sd_dev;
   DeviceArray<unsigned char> inst64, inst32;  // descriptors per slot
+  DeviceArray<unsigned char> inst64i;         // FP64 inner solves: the inner apply's descriptors
   DeviceArray<int4> work;
   int nwork = 0;
   // host state
@@ -470,19 +483,40 @@ struct Engine {
   }
   unsigned slot_grid() const { return static_cast<unsigned>((max_slots + 127) / 128); }
 
-  void inner_iteration() {
+  template <class TI>
+  void inner_iteration_t(const unsigned char* inst, TI* p, TI* ap, const TI* iv, TI* d, TI* rr) {
     const unsigned g = chunk_grid(high);
-    box_batch_apply(true, inst32.ptr, work.ptr, nwork, cs);
-    k_b_dot<float><<<g, 32 * kWarps, 0, cs>>>(p32.ptr, ap32.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, F_DONE,
-                                              o.lanes, part.ptr);
+    box_batch_apply(sizeof(TI) == 4, inst, work.ptr, nwork, cs);
+    k_b_dot<TI><<<g, 32 * kWarps, 0, cs>>>(p, ap, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, F_DONE, o.lanes, part.ptr);
     level(1, F_DONE, S_PAP);
     k_b_alpha<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots);
-    k_b_update<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr, high,
-                                          chunk_slot.ptr, sd_dev.ptr, o.lanes, part.ptr, nchunks);
+    k_b_update<TI><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p, ap, iv, d, rr, high, chunk_slot.ptr, sd_dev.ptr,
+                                              o.lanes, part.ptr, nchunks);
     level(2, F_DONE, S_RR);
     k_b_beta<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots);
-    k_b_p<<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv32.ptr, rr32.ptr, p32.ptr, high, chunk_slot.ptr, sd_dev.ptr);
+    k_b_p<TI><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, p, high, chunk_slot.ptr, sd_dev.ptr);
     FX_LAUNCH_CHECK("batch_inner");
+  }
+  void inner_iteration() {
+    if (inner64) inner_iteration_t<double>(inst64i.ptr, p64.ptr, ap64.ptr, inv.ptr, d64.ptr, rr64.ptr);
+    else inner_iteration_t<float>(inst32.ptr, p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr);
+  }
+
+  // the inner solves in FP64 (on) or FP32 (off); only while no slot is in use
+  void set_inner64(bool on) {
+    for (const auto& sl : slots)
+      if (sl.used) throw Error(FX_E_INVALID, "fx_engine_set_precision: slots are in use");
+    if (on && !r64.ptr) {
+      const size_t n = static_cast<size_t>(nchunks * kChunk);
+      for (auto* v : {&r64, &d64, &rr64, &p64, &ap64}) v->alloc(n);
+      inst64i.alloc(a64 * max_slots);
+    }
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    inner64 = on;
+    dirty = true;
   }
 
   bool any_inner_running() const {
@@ -515,9 +549,13 @@ struct Engine {
     level(2, G_SKIP, O_RR);
     k_b_outer<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, o.rtol, o.atol, max_outer,
                                            o.max_iterations);
-    // inner: FP32 PCG from d = 0
-    k_b_inner_begin<<<g, 32 * kWarps, 0, cs>>>(r.ptr, r32.ptr, d32.ptr, rr32.ptr, p32.ptr, inv32.ptr, high,
-                                               chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
+    // inner: FP32 (or FP64) PCG from d = 0
+    if (inner64)
+      k_b_inner_begin<double><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r64.ptr, d64.ptr, rr64.ptr, p64.ptr, inv.ptr, high,
+                                                         chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
+    else
+      k_b_inner_begin<float><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r32.ptr, d32.ptr, rr32.ptr, p32.ptr, inv32.ptr, high,
+                                                        chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
     level(2, F_DONE, S_RR);
     k_b_inner_start<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, inner_rtol);
     FX_LAUNCH_CHECK("batch_outer");
@@ -544,7 +582,8 @@ struct Engine {
       FX_CUDA(cudaGraphLaunch(graph, cs));
       read_flags();
     }
-    k_b_correct<<<g, 32 * kWarps, 0, cs>>>(d32.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
+    if (inner64) k_b_correct<double><<<g, 32 * kWarps, 0, cs>>>(d64.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
+    else k_b_correct<float><<<g, 32 * kWarps, 0, cs>>>(d32.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
     k_b_round_end<<<slot_grid(), 128, 0, cs>>>(fl.ptr, used_dev.ptr, max_slots);
     FX_LAUNCH_CHECK("batch_correct");
     read_flags();
@@ -581,6 +620,9 @@ struct Engine {
     FX_CUDA(cudaMemsetAsync(inv.ptr + off, 0, sizeof(double) * span, cs));
     for (float* v : {r32.ptr, d32.ptr, rr32.ptr, p32.ptr, ap32.ptr, inv32.ptr})
       FX_CUDA(cudaMemsetAsync(v + off, 0, sizeof(float) * span, cs));
+    if (inner64)
+      for (double* v : {r64.ptr, d64.ptr, rr64.ptr, p64.ptr, ap64.ptr})
+        FX_CUDA(cudaMemsetAsync(v + off, 0, sizeof(double) * span, cs));
     FX_CUDA(cudaMemcpyAsync(b.ptr + off, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, cs));
     general_diagonal(s, k, r.ptr + off, cs);  // the diagonal, in r for now
     FX_CUDA(cudaMemsetAsync(zeros.ptr, 0, sizeof(int), cs));
@@ -596,6 +638,13 @@ struct Engine {
     box_fill_args(s, k, true, p32.ptr + off, ap32.ptr + off, fl.ptr + slot * NFL + F_DONE, d32h.data());
     FX_CUDA(cudaMemcpyAsync(inst64.ptr + static_cast<size_t>(slot) * a64, d64.data(), a64, cudaMemcpyHostToDevice, cs));
     FX_CUDA(cudaMemcpyAsync(inst32.ptr + static_cast<size_t>(slot) * a32, d32h.data(), a32, cudaMemcpyHostToDevice, cs));
+    std::vector<unsigned char> d64i;
+    if (inner64) {  // FP64 operator p64 -> ap64 (skipped once the inner solve is done)
+      d64i.resize(a64);
+      box_fill_args(s, k, false, p64.ptr + off, ap64.ptr + off, fl.ptr + slot * NFL + F_DONE, d64i.data());
+      FX_CUDA(cudaMemcpyAsync(inst64i.ptr + static_cast<size_t>(slot) * a64, d64i.data(), a64, cudaMemcpyHostToDevice,
+                              cs));
+    }
     std::vector<int> f0(NFL, 0);
     f0[F_DONE] = 1;
     std::vector<double> s0(NSC, 0.0);
@@ -720,6 +769,15 @@ int fx_engine_create(int32_t device, int64_t capacity, int32_t max_slots, fx_coe
 }
 
 void fx_engine_destroy(fx_engine* e) { delete e; }
+
+int fx_engine_set_precision(fx_engine* e, int32_t inner) {
+  return guard([&] {
+    if (!e || (inner != FX_ENGINE_INNER_FP32 && inner != FX_ENGINE_INNER_FP64))
+      throw fx::Error(FX_E_INVALID, "fx_engine_set_precision: bad arguments");
+    FX_CUDA(cudaSetDevice(e->e.device));
+    e->e.set_inner64(inner == FX_ENGINE_INNER_FP64);
+  });
+}
 
 int fx_engine_admit(fx_engine* e, fx_force* f, const double* b_host, int32_t* slot) {
   return guard([&] {

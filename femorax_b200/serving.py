@@ -184,6 +184,40 @@ def synthetic_stream(count: int, rate: float, min_dof: float = 1e4, max_dof: flo
     return out
 
 
+def pooled_stream(count: int, rate: float, models: int = 48, j2_share: float = 0.3, j2_models: int = 16,
+                  min_dof: float = 1e4, max_dof: float = 2e6, seed: int = 0, cycles: int = 1, steps_per_cycle: int = 8,
+                  j2_sizes=(1, 2, 4, 8), j2_nz=(20, 40)):
+    """A served stream over resident models: `models` elastic blocks (sizes log-uniform in [min_dof,
+    max_dof] equations, E ~ U[50, 200] MPa, nu ~ U[0.25, 0.40]) and `j2_models` J2 blocks (as
+    mixed_stream's J2 requests); Poisson arrivals at `rate`, a share j2_share of the requests J2
+    load paths on a J2 model, the others static solves on an elastic model with their own top
+    traction q ~ U[-150, -50] kPa. Requests on the same model share its resident state (resident()
+    keys it by the model's parameters)."""
+    rng = np.random.default_rng(seed)
+    pool = synthetic_stream(models, 1.0, min_dof, max_dof, seed + 7)
+    j2pool = [r for r in mixed_stream(4 * j2_models, 1.0, j2_share=1.0, seed=seed + 11, cycles=cycles,
+                                      steps_per_cycle=steps_per_cycle, j2_sizes=j2_sizes, j2_nz=j2_nz)][:j2_models]
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        if rng.uniform() < j2_share:
+            m = j2pool[int(rng.integers(len(j2pool)))]
+            out.append(dataclasses.replace(m, id=i, arrival=t))
+        else:
+            m = pool[int(rng.integers(len(pool)))]
+            out.append(dataclasses.replace(m, id=i, q=float(rng.uniform(-150e3, -50e3)), arrival=t))
+    return out
+
+
+def model_key(req):
+    """The parameters of a request's model (mesh, material, load pattern), without its load
+    magnitude: requests with equal keys share their resident state."""
+    if isinstance(req, J2Request):
+        return ("j2", req.nx, req.ny, req.nz, req.E, req.sigma_y, req.total, req.h, req.path)
+    return ("el", req.nx, req.ny, req.nz, req.E, req.nu, req.h)
+
+
 def mixed_stream(count: int, rate: float, j2_share: float = 0.3, min_dof: float = 1e4, max_dof: float = 2e6,
                  seed: int = 0, cycles: int = 1, steps_per_cycle: int = 8, j2_sizes=(1, 2, 4, 8, 16, 24),
                  j2_nz=(20, 400)):
@@ -389,24 +423,43 @@ class Server:
         return served, time.perf_counter() - t0
 
 
-def resident(requests, device: int = 0, rtol: float = 1e-8):
+def resident(requests, device: int = 0, rtol: float = 1e-8, j2_host: bool = False, cache: dict = None):
     """Prepare every request's mesh up front (the resident state a serving process keeps):
     {id: (force, b, n)} for static solves and {id: (force, unit load, monitored equation, n)} for
     J2 paths, and for the one-at-a-time arm a plain FP64 CG per mesh, already created (its work
-    vectors allocated): {id: solver}."""
+    vectors allocated): {id: solver}. Requests with the same model_key share the model's force,
+    solver and (J2) load; a static solve's right-hand side is its own (the model's unit traction
+    load times its q). With j2_host, also {id: prepare_j2 result} (the serving loop's J2 cohorts
+    build from these host arrays), shared per model too. `cache` (a dict) keeps the models between
+    calls."""
     import torch
-    prepared, solvers = {}, {}
+    prepared, solvers, host = {}, {}, {}
+    models = cache if cache is not None else {}
     for r in requests:
+        key = model_key(r)
+        if key not in models:
+            if isinstance(r, J2Request):
+                mesh, f, mon, n = prepare_j2(r, device)
+                force = InternalForce(mesh, device=device)
+                models[key] = ((force, torch.as_tensor(f, device=torch.device("cuda", device)), mon, n),
+                               ConjugateGradient(SolveOptions(relative_tolerance=1e-12, max_iterations=20000)),
+                               (mesh, f, mon, n))
+            else:
+                unit = dataclasses.replace(r, q=1.0)
+                force, b1, n = prepare(unit, device)
+                cg = ConjugateGradient(SolveOptions(relative_tolerance=rtol))
+                cg.setup(MatrixFreeOperator(force, OperatorCoefficients()))
+                models[key] = ((force, b1, n), cg, None)
+        state, solver, h = models[key]
         if isinstance(r, J2Request):
-            mesh, f, mon, n = prepare_j2(r, device)
-            prepared[r.id] = (InternalForce(mesh, device=device), torch.as_tensor(f, device=torch.device("cuda", device)),
-                              mon, n)
-            solvers[r.id] = ConjugateGradient(SolveOptions(relative_tolerance=1e-12, max_iterations=20000))
+            prepared[r.id] = state
+            host[r.id] = h
         else:
-            prepared[r.id] = prepare(r, device)
-            cg = ConjugateGradient(SolveOptions(relative_tolerance=rtol))
-            cg.setup(MatrixFreeOperator(prepared[r.id][0], OperatorCoefficients()))
-            solvers[r.id] = cg
+            force, b1, n = state
+            prepared[r.id] = (force, r.q * b1, n)
+        solvers[r.id] = solver
+    if j2_host:
+        return prepared, solvers, host
     return prepared, solvers
 
 

@@ -505,11 +505,19 @@ int fx_nbatch_step(fx_nbatch* b, const double* fext, double* u, double tol, int3
  *   fx_engine_finished whether a slot's solve has ended (converged or given up).
  *   fx_engine_retire   copies x (host, may be NULL) and the result out and frees the slot.
  *   fx_engine_info     info[6] = capacity (equations), equations in use, max slots, slots in
- *                      use, rounds run, device bytes of the engine's vectors. */
+ *                      use, rounds run, device bytes of the engine's vectors.
+ *   fx_engine_set_precision  the inner solves' precision while no slot is in use:
+ *                      FX_ENGINE_INNER_FP32 (the default, above) or FX_ENGINE_INNER_FP64 (FP64
+ *                      Jacobi-PCG with the FP64 operator inside the same refinement rounds: the
+ *                      batched engine without reduced precision, with inner_rtol at or below the
+ *                      outer rtol a slot converges in its first round). */
+#define FX_ENGINE_INNER_FP32 0
+#define FX_ENGINE_INNER_FP64 1
 typedef struct fx_engine fx_engine;
 int fx_engine_create(int32_t device, int64_t capacity, int32_t max_slots, fx_coeffs k, fx_solve_opts o,
                      double inner_rtol, fx_engine** out);
 void fx_engine_destroy(fx_engine* e);
+int fx_engine_set_precision(fx_engine* e, int32_t inner);
 int fx_engine_admit(fx_engine* e, fx_force* f, const double* b_host, int32_t* slot);
 int fx_engine_round(fx_engine* e, int32_t* running);
 int fx_engine_finished(fx_engine* e, int32_t slot, int32_t* finished);

@@ -140,3 +140,43 @@ def test_server_stream(alone):
         assert np.array_equal(s.x, alone[s.id][0]), s.id
     summ = serving.summary(served, wall)
     assert summ["converged"] == 4 and summ["p99_s"] >= summ["p50_s"] > 0
+
+
+def test_fp64_inner_engine(prepared):
+    """inner="fp64": the same engine with FP64 inner solves (the batching without reduced
+    precision). Every slot meets the 1e-8 FP64 residual in one refinement round, agrees with the
+    plain FP64 CG solution to 1e-8 relative, and is bit for bit the same alone and in a mix; the
+    same InternalForce admitted into two slots at once gives the same bits in both."""
+    def eng():
+        return fx.BatchEngine(1 << 20, 8, options=fx.SolveOptions(relative_tolerance=RTOL), inner_tolerance=0.5 * RTOL,
+                              inner="fp64")
+    alone64 = {}
+    for rid, (force, b, n) in prepared.items():
+        e = eng()
+        s = e.admit(force, b)
+        alone64[rid] = run_to_end(e, {s: rid})[rid]
+    e = eng()
+    slots = {e.admit(f, b): rid for rid, (f, b, _) in prepared.items()}
+    f0, b0, _ = prepared[0]
+    slots[e.admit(f0, b0)] = "again"
+    mix = run_to_end(e, slots)
+    assert np.array_equal(mix["again"][0], mix[0][0])
+    for rid, (force, b, n) in prepared.items():
+        x, r = alone64[rid]
+        assert r.converged and r.refinements == 1, (rid, r)
+        assert np.array_equal(mix[rid][0], x), rid
+        op = fx.MatrixFreeOperator(force, fx.OperatorCoefficients())
+        y = torch.zeros(n, dtype=torch.float64, device=DEV)
+        op.apply(torch.as_tensor(x, device=DEV), y)
+        res = np.linalg.norm(b - y.cpu().numpy()) / np.linalg.norm(b)
+        assert res <= RTOL, (rid, res)
+        cg = fx.ConjugateGradient(fx.SolveOptions(relative_tolerance=RTOL))
+        cg.setup(op)
+        xc = torch.zeros(n, dtype=torch.float64, device=DEV)
+        assert cg.solve(torch.as_tensor(b, device=DEV), xc).converged
+        xc = xc.cpu().numpy()
+        assert np.max(np.abs(x - xc)) <= 1e-7 * np.max(np.abs(xc)), rid
+    e2 = eng()
+    e2.admit(f0, b0)
+    with pytest.raises(fx.FxError):  # the precision is fixed while slots are in use
+        fx._lib.check(fx._lib.lib().fx_engine_set_precision(e2._h, 0))
