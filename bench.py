@@ -175,6 +175,46 @@ def reference_force(spec):
     return O.RefForce(c, cache=True)
 
 
+def grid_order_equations(spec, comp):
+    """The free equations of the box's nodes in grid order (z planes, then y rows, then x, then the
+    three components): the order in which the apply's tiles gather x."""
+    eq = mesh_builders().equation_map(comp)[spec.tags]
+    c = spec.coords
+    key = [np.rint((c[:, d] - c[:, d].min()) * 1e6).astype(np.int64) for d in range(3)]
+    order = np.lexsort((key[0], key[1], key[2]))
+    e = eq[order].reshape(-1)
+    return e[e >= 0].astype(np.int64)
+
+
+def gather_floor(spec, comp, x, flush, stream, reps=20):
+    """What one pass over x in the apply's access order costs on this device by itself: every free
+    equation of the box gathered in grid order (torch.index_select, a library kernel used here as a
+    measuring stick only, reading an 8-byte index per value), beside a contiguous copy of the same
+    bytes; L2 flushed before each launch as for the timed applies."""
+    import torch
+    idx = torch.as_tensor(grid_order_equations(spec, comp), device=x.device)
+    out = torch.empty(idx.numel(), dtype=x.dtype, device=x.device)
+    res = {}
+    for name, fn in (("rcm_gather_of_x", lambda: torch.index_select(x, 0, idx, out=out)),
+                     ("contiguous_copy_of_x", lambda: out[: x.numel()].copy_(x))):
+        for _ in range(3):
+            fn()
+        ev = []
+        for i in range(reps):
+            flush.fill_(float(i))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            ev.append((a, b))
+        torch.cuda.synchronize(x.device)
+        res[name + "_us"] = float(np.median([a.elapsed_time(b) for a, b in ev]) * 1e3)
+    res["values"] = int(idx.numel())
+    res["what"] = ("x alone, in the apply's gather order (grid order of the RCM-numbered equations) and contiguous; "
+                   "library kernels, L2 flushed before each launch; index read 8 B per value")
+    return res
+
+
 def rel_err(a, b):
     """max |a - b| over max |b|."""
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(np.asarray(b))), 1e-300))
@@ -894,6 +934,7 @@ def run_ours(args):
     total_ms = max_over_ranks([total_ms], dist, dev)[0]
     value = replica_value(world, neq, args.steps, total_ms)
 
+    floor = gather_floor(spec, comp, x, flush, stream) if world == 1 else None
     # the FP32 apply (the precision form) on the same x, timed the same way, outside the FP64 figures
     x32 = x.float()
     y32 = torch.zeros(neq, dtype=torch.float32, device=dev)
@@ -970,6 +1011,7 @@ def run_ours(args):
                          "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg},
             "fp32_apply": f32,
+            "gather_floor": floor,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": 8 * neq, "d2h_bytes_per_step": 8 * neq,
                     "ms_per_step": float(np.mean(e_ms)), "ms_per_step_min": float(np.min(e_ms)),
