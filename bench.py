@@ -573,13 +573,18 @@ def pimy_points(device, n=1 << 20, steps=10, sample=8192, seed=0, material=None,
         m.update_host(1, hc, ht, heps[k], hsig, htan)
         hc, ht = ht, hc
     host_s = time.perf_counter() - t0
-    same = bool(np.allclose(sig[:, hs].cpu().numpy(), hsig, rtol=0, atol=1e-12 * float(np.max(np.abs(hsig)))))
+    dsig = sig[:, hs].cpu().numpy()
+    rel = np.max(np.abs(dsig - hsig), axis=0) / float(np.max(np.abs(hsig)))
     rate = n * steps / (ms * 1e-3)
     return {"points": n, "surfaces": m.surfaces, "steps": steps, "ms_per_update": ms / steps,
             "point_updates_per_s": rate, "bytes_per_point_update": per_point,
             "achieved_gbs": rate * per_point / 1e9, "failed_points": int(failed.item()),
             "host_one_core_point_updates_per_s": sample * steps / host_s, "host_sample_points": sample,
-            "device_vs_host_sample_within_1e-12": same}
+            "device_vs_host_sample": {
+                "bit_identical": float(np.mean(rel == 0)), "within_1e-12": float(np.mean(rel <= 1e-12)),
+                "host": "this library's host restatement with the host C library's elementary functions (the "
+                        "device's pow/exp/log/cos are its own, or CUDA's for PressureIndependMultiYield): points on "
+                        "another branch after a last-place difference count against both fractions"}}
 
 
 PIMY_CLAY = (1.8, 40500.0, 108000.0, 8.0, 0.1, 0.0, 100.0, 0.0, 20.0)  # rho t/m3, G, K kPa, cohesion kPa, ...

@@ -757,6 +757,36 @@ class MixedPrecisionSolver(LinearSolver):
         check(lib().fx_solver_set_inner_tolerance(self._h, self.inner_tolerance))
 
 
+MATH_FUNCTIONS = {"exp": L.FX_MATH_EXP, "log": L.FX_MATH_LOG, "pow": L.FX_MATH_POW, "cos": L.FX_MATH_COS}
+
+
+def math_eval(name: str, x, y=None, stream=None):
+    """fx_math_eval: the PressureDependMultiYield device update's exp, log, pow or cos (`name`) of a
+    float64 device tensor x (and y, for pow), element by element; returns a new tensor."""
+    import torch
+    fn = MATH_FUNCTIONS[name]
+    x = x.contiguous()
+    if x.dtype != torch.float64 or (y is not None and (y.dtype != torch.float64 or y.shape != x.shape)):
+        raise ValueError("math_eval takes float64 tensors of one shape")
+    y = y.contiguous() if y is not None else None
+    out = torch.empty_like(x)
+    check(lib().fx_math_eval(fn, _ptr(x), _ptr(y) if y is not None else None, _ptr(out), x.numel(), _stream(stream)))
+    return out
+
+
+def math_eval_host(name: str, x: np.ndarray, y: np.ndarray = None) -> np.ndarray:
+    """fx_math_eval_host: the same functions on the host (the same bits as math_eval)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    yy = np.ascontiguousarray(y, dtype=np.float64) if y is not None else None
+    if yy is not None and yy.shape != x.shape:
+        raise ValueError("x and y must have one shape")
+    out = np.empty_like(x)
+    check(lib().fx_math_eval_host(MATH_FUNCTIONS[name], x.ctypes.data_as(L.p_f64),
+                                  yy.ctypes.data_as(L.p_f64) if yy is not None else None, out.ctypes.data_as(L.p_f64),
+                                  x.size))
+    return out
+
+
 class BatchEngine:
     """Many box meshes resident on one device and solved together (fx_engine_*): per slot FP32
     Jacobi-PCG inside FP64 iterative refinement, the same bits as MixedPrecisionSolver on that mesh

@@ -35,6 +35,7 @@ FX_SOLVER_KRYLOV = 2
 FX_SOLVER_IR = 3
 FX_ENGINE_INNER_FP32 = 0
 FX_ENGINE_INNER_FP64 = 1
+FX_MATH_EXP, FX_MATH_LOG, FX_MATH_POW, FX_MATH_COS = 0, 1, 2, 3
 
 p_i32 = C.POINTER(C.c_int32)
 p_i64 = C.POINTER(C.c_int64)
@@ -195,6 +196,8 @@ PROTOTYPES = {
                                    C.POINTER(vp)]),
     "fx_engine_destroy": (None, [vp]),
     "fx_engine_set_precision": (C.c_int, [vp, C.c_int32]),
+    "fx_math_eval": (C.c_int, [C.c_int32, vp, vp, vp, C.c_int64, vp]),
+    "fx_math_eval_host": (C.c_int, [C.c_int32, p_f64, p_f64, p_f64, C.c_int64]),
     "fx_engine_admit": (C.c_int, [vp, vp, p_f64, C.POINTER(C.c_int32)]),
     "fx_engine_round": (C.c_int, [vp, C.POINTER(C.c_int32)]),
     "fx_engine_finished": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_int32)]),

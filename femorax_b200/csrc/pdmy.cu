@@ -3,6 +3,7 @@
 // Built with --fmad=false: the update is the reference's sequence of operations, uncontracted.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <exception>
 #include <string>
 
@@ -70,6 +71,21 @@ __global__ void k_pdmy_elements_init(const int32_t* __restrict__ param, int32_t 
     pdmy::initial_state(m->p, pimy::Slab<double>{trial + base, ld});
     for (int c = 0; c < pdmy::kTan; ++c) tan[base + c * ld] = 0.0;  // stage 0: the elastic tangent
   }
+}
+
+// fx_math.h's function `fn` (FX_MATH_*) of x (and y for pow), element by element
+FX_HD double math_of(int fn, double x, double y) {
+  return fn == FX_MATH_EXP ? fxm_exp(x) : fn == FX_MATH_LOG ? fxm_log(x) : fn == FX_MATH_POW ? fxm_pow(x, y) : fxm_cos(x);
+}
+__global__ void k_math_eval(int fn, const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ out,
+                            int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = math_of(fn, x[i], y ? y[i] : 0.0);
+}
+void check_math(int32_t fn, const double* x, const double* y, const double* out, int64_t n, const char* who) {
+  if (fn < FX_MATH_EXP || fn > FX_MATH_COS || n < 0 || (n > 0 && (!x || !out || (fn == FX_MATH_POW && !y))))
+    throw Error(FX_E_INVALID, std::string(who) + ": bad arguments");
 }
 
 void check_update(const fx_pdmy* h, int32_t stage, int64_t n, const double* c, const double* t, const double* e,
@@ -229,6 +245,23 @@ int fx_pdmy_update_host(const fx_pdmy* h, int32_t stage, int64_t npoints, const 
       bad += !ok;
     }
     if (failed) *failed += bad;
+  });
+}
+
+int fx_math_eval(int32_t fn, const double* x, const double* y, double* out, int64_t n, void* stream) {
+  return fx::guard([&] {
+    fx::check_math(fn, x, y, out, n, "fx_math_eval");
+    if (n == 0) return;
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>((n + 255) / 256, 148 * 16));
+    fx::k_math_eval<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(fn, x, fn == FX_MATH_POW ? y : nullptr, out, n);
+    FX_LAUNCH_CHECK("math_eval");
+  });
+}
+
+int fx_math_eval_host(int32_t fn, const double* x, const double* y, double* out, int64_t n) {
+  return fx::guard([&] {
+    fx::check_math(fn, x, y, out, n, "fx_math_eval_host");
+    for (int64_t i = 0; i < n; ++i) out[i] = fx::math_of(fn, x[i], fn == FX_MATH_POW ? y[i] : 0.0);
   });
 }
 

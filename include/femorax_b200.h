@@ -484,6 +484,20 @@ fx_force* fx_nbatch_force(fx_nbatch* b);
 int fx_nbatch_step(fx_nbatch* b, const double* fext, double* u, double tol, int32_t max_newton,
                    int32_t* newton_iterations, fx_solve_result* results, void* stream);
 
+/* ------------------------------------------------------------------ elementary functions
+ * The exp, log, pow and cos of the PressureDependMultiYield device update (fx_math.h: built from
+ * IEEE-exact operations, so a host and a device evaluation give the same bits; within 0.54 ulp and
+ * one ulp of the host C library's). fx_math_eval runs them on device arrays (x, y, out on the
+ * current device; y only for pow) on `stream`; fx_math_eval_host on host arrays. For checking the
+ * device update against the reference's material linked to the same functions. No counterpart in
+ * the reference, which calls its host C library (src/physics/materials/pressure_depend_multi_yield.hpp). */
+#define FX_MATH_EXP 0
+#define FX_MATH_LOG 1
+#define FX_MATH_POW 2
+#define FX_MATH_COS 3
+int fx_math_eval(int32_t fn, const double* x, const double* y, double* out, int64_t n, void* stream);
+int fx_math_eval_host(int32_t fn, const double* x, const double* y, double* out, int64_t n);
+
 /* ------------------------------------------------------------------ batched and served solves
  * An engine holds many independent meshes ("slots", each one fx_force on the box path, a
  * structured grid of equal boxes) resident on one device and solves K_eff x = b for all of them

@@ -16,6 +16,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libfxref.so")
+# the same reference objects with pow, exp, log and cos bound to the device update's functions
+REF_FXMATH_LIB = os.path.join(HERE, "_ref", "libfxref_fxmath.so")
 PORT_LIB = os.path.join(HERE, "_ref", "libfxport.so")
 
 p_i32 = C.POINTER(C.c_int32)
@@ -25,6 +27,7 @@ p_i8 = C.POINTER(C.c_int8)
 vp = C.c_void_p
 
 _ref = None
+_ref_fxmath = None
 _port = None
 
 
@@ -44,78 +47,91 @@ def have_ref() -> bool:
     return os.path.exists(REF_LIB)
 
 
-def ref():
-    global _ref
+def have_ref_fxmath() -> bool:
+    return os.path.exists(REF_FXMATH_LIB)
+
+
+def ref(math: str = "libm"):
+    """The reference library: with the C library's elementary functions ("libm"), or with pow,
+    exp, log and cos bound to those of this library's device PressureDependMultiYield update ("fx")."""
+    global _ref, _ref_fxmath
+    if math == "fx":
+        if _ref_fxmath is None:
+            _ref_fxmath = _declare_ref(C.CDLL(REF_FXMATH_LIB))
+        return _ref_fxmath
     if _ref is None:
-        L = C.CDLL(REF_LIB)
-        L.fxref_last_error.restype = C.c_char_p
-        L.fxref_model_create.restype = vp
-        L.fxref_model_create.argtypes = [C.c_int32, p_i32, p_f64]
-        L.fxref_model_destroy.argtypes = [vp]
-        L.fxref_model_add_group.argtypes = [vp, C.c_double, C.c_double, C.c_double, p_f64, C.c_int, C.c_int32, p_i32,
-                                            p_i32, C.c_int]
-        L.fxref_ssp_constants.argtypes = [p_f64, C.c_double, C.c_double, p_f64, p_f64]
-        L.fxref_model_add_fix.argtypes = [vp, C.c_int32, p_i32, p_i32]
-        L.fxref_model_add_equal_dof.argtypes = [vp, C.c_int32, p_i32, p_i32, p_i32]
-        L.fxref_model_add_rayleigh.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, p_i32]
-        L.fxref_model_add_mass.argtypes = [vp, C.c_int32, p_i32, p_i32, p_f64]
-        L.fxref_motions_create.restype = vp
-        L.fxref_motions_destroy.argtypes = [vp]
-        L.fxref_motions_add.argtypes = [vp, C.c_int32, C.c_double, p_f64, p_f64, C.c_int32, C.c_double, C.c_double,
-                                        C.c_int32, C.c_int32]
-        L.fxref_motions_evaluate.argtypes = [vp, C.c_double, p_f64]
-        L.fxref_compile.restype = vp
-        L.fxref_compile.argtypes = [vp, C.c_int, C.c_int, C.c_int]
-        L.fxref_compiled_destroy.argtypes = [vp]
-        L.fxref_compiled_sizes.argtypes = [vp, p_i64]
-        L.fxref_compiled_array_i32.restype = C.c_int64
-        L.fxref_compiled_array_i32.argtypes = [vp, C.c_char_p, p_i32]
-        L.fxref_compiled_array_f64.restype = C.c_int64
-        L.fxref_compiled_array_f64.argtypes = [vp, C.c_char_p, p_f64]
-        L.fxref_compiled_param.argtypes = [vp, C.c_int32, p_f64]
-        L.fxref_force_create.restype = vp
-        L.fxref_force_create.argtypes = [vp, C.c_int]
-        L.fxref_force_destroy.argtypes = [vp]
-        L.fxref_apply_operator.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, p_f64, p_f64]
-        L.fxref_operator_diagonal.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64]
-        L.fxref_mass_times_ground.argtypes = [vp, C.c_int, p_f64]
-        L.fxref_force_compute.argtypes = [vp, p_f64, p_f64, C.c_int, p_f64]
-        L.fxref_element_critical_dts.argtypes = [vp, C.c_int, p_f64]
-        L.fxref_stability_may_change.argtypes = [vp]
-        L.fxref_prepare_stability_bounds.argtypes = [vp]
-        L.fxref_min_critical_dt_bound.restype = C.c_double
-        L.fxref_min_critical_dt_bound.argtypes = [vp, C.c_int]
-        L.fxref_min_critical_dt.restype = C.c_double
-        L.fxref_min_critical_dt.argtypes = [vp, C.c_int]
-        L.fxref_solve.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
-                                  C.c_int, C.c_int, p_f64, p_f64, p_f64]
-        L.fxref_host_dot.restype = C.c_double
-        L.fxref_host_dot.argtypes = [p_f64, p_f64, C.c_int64, C.c_int]
-        L.fxref_brick_compute.argtypes = [p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, p_f64]
-        L.fxref_brick_mass.argtypes = [p_f64, p_f64, p_f64, p_f64]
-        L.fxref_brick_operator.argtypes = [p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, C.c_int, p_i32]
-        L.fxref_brick_critical_dt.restype = C.c_double
-        L.fxref_brick_critical_dt.argtypes = [p_f64, p_f64, C.c_int, p_f64]
-        L.fxref_pimy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
-        L.fxref_pdmy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
-        L.fxref_pdmy_destroy.argtypes = [vp]
-        L.fxref_pdmy_nstate.restype = C.c_int32
-        L.fxref_pdmy_setup_values.argtypes = [vp, p_f64]
-        L.fxref_pdmy_initial_state.argtypes = [vp, p_f64]
-        L.fxref_pdmy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
-        L.fxref_model_add_group_pimy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
-        L.fxref_model_add_group_pdmy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
-        L.fxref_force_set_stage.argtypes = [vp, C.c_int32, C.c_int32]
-        L.fxref_force_commit.argtypes = [vp]
-        L.fxref_apply_operator_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64, p_f64]
-        L.fxref_operator_diagonal_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64]
-        L.fxref_pimy_destroy.argtypes = [vp]
-        L.fxref_pimy_nstate.restype = C.c_int32
-        L.fxref_pimy_setup_values.argtypes = [vp, p_f64]
-        L.fxref_pimy_initial_state.argtypes = [vp, p_f64]
-        L.fxref_pimy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
-        _ref = L
+        _ref = _declare_ref(C.CDLL(REF_LIB))
     return _ref
+
+
+def _declare_ref(L):
+    L.fxref_last_error.restype = C.c_char_p
+    L.fxref_model_create.restype = vp
+    L.fxref_model_create.argtypes = [C.c_int32, p_i32, p_f64]
+    L.fxref_model_destroy.argtypes = [vp]
+    L.fxref_model_add_group.argtypes = [vp, C.c_double, C.c_double, C.c_double, p_f64, C.c_int, C.c_int32, p_i32,
+                                        p_i32, C.c_int]
+    L.fxref_ssp_constants.argtypes = [p_f64, C.c_double, C.c_double, p_f64, p_f64]
+    L.fxref_model_add_fix.argtypes = [vp, C.c_int32, p_i32, p_i32]
+    L.fxref_model_add_equal_dof.argtypes = [vp, C.c_int32, p_i32, p_i32, p_i32]
+    L.fxref_model_add_rayleigh.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, p_i32]
+    L.fxref_model_add_mass.argtypes = [vp, C.c_int32, p_i32, p_i32, p_f64]
+    L.fxref_motions_create.restype = vp
+    L.fxref_motions_destroy.argtypes = [vp]
+    L.fxref_motions_add.argtypes = [vp, C.c_int32, C.c_double, p_f64, p_f64, C.c_int32, C.c_double, C.c_double,
+                                    C.c_int32, C.c_int32]
+    L.fxref_motions_evaluate.argtypes = [vp, C.c_double, p_f64]
+    L.fxref_compile.restype = vp
+    L.fxref_compile.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    L.fxref_compiled_destroy.argtypes = [vp]
+    L.fxref_compiled_sizes.argtypes = [vp, p_i64]
+    L.fxref_compiled_array_i32.restype = C.c_int64
+    L.fxref_compiled_array_i32.argtypes = [vp, C.c_char_p, p_i32]
+    L.fxref_compiled_array_f64.restype = C.c_int64
+    L.fxref_compiled_array_f64.argtypes = [vp, C.c_char_p, p_f64]
+    L.fxref_compiled_param.argtypes = [vp, C.c_int32, p_f64]
+    L.fxref_force_create.restype = vp
+    L.fxref_force_create.argtypes = [vp, C.c_int]
+    L.fxref_force_destroy.argtypes = [vp]
+    L.fxref_apply_operator.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, p_f64, p_f64]
+    L.fxref_operator_diagonal.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64]
+    L.fxref_mass_times_ground.argtypes = [vp, C.c_int, p_f64]
+    L.fxref_force_compute.argtypes = [vp, p_f64, p_f64, C.c_int, p_f64]
+    L.fxref_element_critical_dts.argtypes = [vp, C.c_int, p_f64]
+    L.fxref_stability_may_change.argtypes = [vp]
+    L.fxref_prepare_stability_bounds.argtypes = [vp]
+    L.fxref_min_critical_dt_bound.restype = C.c_double
+    L.fxref_min_critical_dt_bound.argtypes = [vp, C.c_int]
+    L.fxref_min_critical_dt.restype = C.c_double
+    L.fxref_min_critical_dt.argtypes = [vp, C.c_int]
+    L.fxref_solve.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                              C.c_int, C.c_int, p_f64, p_f64, p_f64]
+    L.fxref_host_dot.restype = C.c_double
+    L.fxref_host_dot.argtypes = [p_f64, p_f64, C.c_int64, C.c_int]
+    L.fxref_brick_compute.argtypes = [p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, p_f64]
+    L.fxref_brick_mass.argtypes = [p_f64, p_f64, p_f64, p_f64]
+    L.fxref_brick_operator.argtypes = [p_f64, p_f64, p_f64, p_f64, p_f64, p_f64, C.c_int, p_i32]
+    L.fxref_brick_critical_dt.restype = C.c_double
+    L.fxref_brick_critical_dt.argtypes = [p_f64, p_f64, C.c_int, p_f64]
+    L.fxref_pimy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
+    L.fxref_pdmy_create.argtypes = [p_f64, p_f64, C.c_int32, C.POINTER(vp)]
+    L.fxref_pdmy_destroy.argtypes = [vp]
+    L.fxref_pdmy_nstate.restype = C.c_int32
+    L.fxref_pdmy_setup_values.argtypes = [vp, p_f64]
+    L.fxref_pdmy_initial_state.argtypes = [vp, p_f64]
+    L.fxref_pdmy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
+    L.fxref_model_add_group_pimy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
+    L.fxref_model_add_group_pdmy.argtypes = [vp, p_f64, p_f64, C.c_int32, p_f64, C.c_int, C.c_int32, p_i32, p_i32]
+    L.fxref_force_set_stage.argtypes = [vp, C.c_int32, C.c_int32]
+    L.fxref_force_commit.argtypes = [vp]
+    L.fxref_apply_operator_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64, p_f64]
+    L.fxref_operator_diagonal_at.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int, p_f64, p_f64]
+    L.fxref_pimy_destroy.argtypes = [vp]
+    L.fxref_pimy_nstate.restype = C.c_int32
+    L.fxref_pimy_setup_values.argtypes = [vp, p_f64]
+    L.fxref_pimy_initial_state.argtypes = [vp, p_f64]
+    L.fxref_pimy_update.argtypes = [vp, C.c_int32, p_f64, p_f64, p_f64, p_f64, p_f64]
+    return L
 
 
 def _f(a):
@@ -357,6 +373,7 @@ def port():
     global _port
     if _port is None:
         L = C.CDLL(PORT_LIB)
+        L.fxo_libm_eval.argtypes = [C.c_int, p_f64, p_f64, p_f64, C.c_int64]
         P = C.POINTER(fxo_param)
         M = C.POINTER(fxo_mesh)
         L.fxo_brick_compute.argtypes = [P, p_f64, p_f64, p_f64, p_f64, p_f64]
@@ -685,41 +702,53 @@ class RefPimy:
 class RefPdmy(RefPimy):
     """The reference's PressureDependMultiYield (40-surface bucket) at one material point
     (oracle/_ref): params23 = the 21 constructor values of the stored paths' header (rho ... c)
-    then hv, pv; pairs: (gamma, G/Gmax) pairs or empty."""
+    then hv, pv; pairs: (gamma, G/Gmax) pairs or empty. math: "libm" (the C library's elementary
+    functions, as the reference ships) or "fx" (pow, exp, log and cos bound to those of this
+    library's device update, oracle/_ref/libfxref_fxmath.so)."""
 
-    def __init__(self, params23, pairs=()):
+    def __init__(self, params23, pairs=(), math="libm"):
+        self.L = ref(math)
         p, pp = _f(params23)
         pr = np.ascontiguousarray(pairs, np.float64)
         h = vp()
-        rc = ref().fxref_pdmy_create(pp, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2, C.byref(h))
+        rc = self.L.fxref_pdmy_create(pp, pr.ctypes.data_as(p_f64) if pr.size else None, pr.size // 2, C.byref(h))
         assert rc == 0, rc
         self.h = h
-        self.nstate = ref().fxref_pdmy_nstate()
+        self.nstate = self.L.fxref_pdmy_nstate()
 
     def setup_values(self):
         """residualPress, frictionAngle, phaseTransfAngle, stressRatioPT, strainPTOcta; sizes and
         plastic moduli (1..40)."""
         out = np.zeros(85)
-        ref().fxref_pdmy_setup_values(self.h, out.ctypes.data_as(p_f64))
+        self.L.fxref_pdmy_setup_values(self.h, out.ctypes.data_as(p_f64))
         return out[:5], out[5:45], out[45:85]
 
     def initial_state(self):
         s = np.zeros(self.nstate)
-        ref().fxref_pdmy_initial_state(self.h, s.ctypes.data_as(p_f64))
+        self.L.fxref_pdmy_initial_state(self.h, s.ctypes.data_as(p_f64))
         return s
 
     def update(self, stage, committed, eps):
         committed, pc = _f(committed)
         eps, pe = _f(eps)
         trial, sig, D = np.zeros(self.nstate), np.zeros(6), np.zeros((6, 6))
-        ref().fxref_pdmy_update(self.h, stage, pc, trial.ctypes.data_as(p_f64), pe, sig.ctypes.data_as(p_f64),
+        self.L.fxref_pdmy_update(self.h, stage, pc, trial.ctypes.data_as(p_f64), pe, sig.ctypes.data_as(p_f64),
                                 D.ctypes.data_as(p_f64))
         return trial, sig, D
 
     def __del__(self):
         if getattr(self, "h", None):
-            ref().fxref_pdmy_destroy(self.h)
+            self.L.fxref_pdmy_destroy(self.h)
             self.h = None
+
+
+def libm_eval(fn: int, x, y=None):
+    """The host C library's exp (0), log (1), pow (2) or cos (3) of x (and y), element by element."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(x if y is None else y, np.float64)
+    out = np.empty_like(x)
+    port().fxo_libm_eval(fn, x.ctypes.data_as(p_f64), y.ctypes.data_as(p_f64), out.ctypes.data_as(p_f64), x.size)
+    return out
 
 
 def ref_ssp_constants(xl, E, nu):

@@ -1169,3 +1169,8 @@ void fxo_diagonal_j2(const fxo_mesh* m, const double* j2, const double* Dpts, co
   if (k[1] != 0.0 && m->nodal_alpha_mass)
     for (int32_t q = 0; q < m->num_equations; ++q) d[q] += k[1] * m->nodal_alpha_mass[q] * 1.0;
 }
+
+void fxo_libm_eval(int fn, const double* x, const double* y, double* out, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    out[i] = fn == 0 ? exp(x[i]) : fn == 1 ? log(x[i]) : fn == 2 ? pow(x[i], y[i]) : cos(x[i]);
+}

@@ -117,6 +117,11 @@ void fxo_apply_j2(const fxo_mesh* m, const double* j2, const double* Dpts, const
 void fxo_diagonal_j2(const fxo_mesh* m, const double* j2, const double* Dpts, const double* k, int initial,
                      double* d);
 
+/* The host C library's exp (fn 0), log (1), pow (2, of x and y) and cos (3), element by element:
+   the functions the reference calls, beside which the device update's own (fx_math_eval_host of
+   the product library) are measured. */
+void fxo_libm_eval(int fn, const double* x, const double* y, double* out, int64_t n);
+
 #ifdef __cplusplus
 }
 #endif
