@@ -753,8 +753,8 @@ def served_streams(device, count=1000, rates=((10.0, 40), (100.0, 400), (500.0, 
     """The served configuration at its sizes, on resident models (serving.pooled_stream: `models`
     elastic blocks log-uniform in 1e4 - 2e6 equations, `j2_models` J2 blocks as the batched J2
     sample's, every request its own load), each stream through three arms:
-      - mixed_batched: the serving loop over the batched engine, FP32 inner solves inside FP64
-        refinement (the served form);
+      - mixed_batched: the serving loop (in C++, serving.NativeServer over fx_server_*) over the
+        batched engine, FP32 inner solves inside FP64 refinement (the served form);
       - fp64_batched: the same loop and engine with FP64 inner solves (batching without reduced
         precision: the ablation that splits the speed-up into batching and precision);
       - plain_fp64_one_at_a_time: first come first served, each request alone by the plain FP64 path.
@@ -779,7 +779,7 @@ def served_streams(device, count=1000, rates=((10.0, 40), (100.0, 400), (500.0, 
         prep = {r.id: host[r.id] if isinstance(r, serving.J2Request) else prepared[r.id] for r in reqs}
         out = {}
         for name, eng in engines.items():
-            srv = serving.Server(eng, device=device, prepare_fn=lambda r, d: prep[r.id])
+            srv = serving.NativeServer(eng, device=device, prepare_fn=lambda r, d: prep[r.id])
             out[name] = srv.run(reqs, realtime=realtime)
         out["plain_fp64_one_at_a_time"] = serving.serve_one_at_a_time(reqs, 1e-8, realtime=realtime, device=device,
                                                                       prepared=prepared, solvers=solvers)

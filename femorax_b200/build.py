@@ -46,6 +46,7 @@ CUDA_SOURCES = [
     ("stepping.cu", []),
     ("batch.cu", []),
     ("nbatch.cu", []),
+    ("serve.cu", []),
     ("pimy.cu", ["--fmad=false"]),
     ("pdmy.cu", ["--fmad=false"]),
 ]

@@ -423,6 +423,78 @@ class Server:
         return served, time.perf_counter() - t0
 
 
+class NativeServer:
+    """The serving loop in C++ (fx_server_*, serve.cu) over one BatchEngine: the same admission by
+    footprint, engine rounds for the static solves and J2 cohorts (up to max_cohort, fx_nbatch) as
+    Server, with the loop, the arrival gating and the clock in the library; latency is measured by
+    the host's steady clock inside it. run() takes the requests with their prepared state
+    (prepare_fn(request, device) as for Server: (force, b, n) for a static solve, prepare_j2's
+    (mesh, unit load, monitored equation, n) for a J2 path) and returns (served, wall seconds)."""
+
+    def __init__(self, engine: BatchEngine, hbm_budget: int = None, device: int = 0, prepare_fn=None,
+                 max_cohort: int = 32, reserve: int = 2 << 30, tol: float = 1e-6, max_newton: int = 25,
+                 cg_rtol: float = 1e-12, cg_max_iterations: int = 20000):
+        self.engine = engine
+        if hbm_budget is None:
+            free, _ = device_memory(device)
+            hbm_budget = max(0, free - int(reserve))
+        self.budget = int(hbm_budget)
+        self.device = device
+        self.prepare = prepare_fn or prepare_any
+        self.max_cohort = int(max_cohort)
+        self.j2_settings = (float(tol), int(max_newton), float(cg_rtol), int(cg_max_iterations))
+
+    def run(self, requests, realtime: bool = True):
+        import ctypes as C
+        from . import _lib as L
+        from ._lib import check, lib
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        h = C.c_void_p()
+        check(lib().fx_server_create(self.engine._h, self.device, self.budget, self.max_cohort, C.byref(h)))
+        keep, sizes = [], {}
+        try:
+            tol, max_newton, cg_rtol, cg_max_it = self.j2_settings
+            for r in reqs:
+                prep = self.prepare(r, self.device)
+                if isinstance(r, J2Request):
+                    mesh, f, mon, n = prep
+                    cm, k = mesh.to_c()
+                    f = np.ascontiguousarray(f, dtype=np.float64)
+                    keep += [cm, k, f]
+                    check(lib().fx_server_add_j2(h, r.id, C.byref(cm), f.ctypes.data_as(L.p_f64), int(mon), r.cycles,
+                                                 r.steps_per_cycle, tol, max_newton, cg_rtol, cg_max_it,
+                                                 float(r.arrival) if realtime else 0.0))
+                    sizes[r.id] = (n, r.cycles * r.steps_per_cycle)
+                else:
+                    force, b, n = prep
+                    b = np.ascontiguousarray(b, dtype=np.float64)
+                    keep += [force, b]
+                    check(lib().fx_server_add_static(h, r.id, force._h, b.ctypes.data_as(L.p_f64),
+                                                     float(r.arrival) if realtime else 0.0))
+                    sizes[r.id] = (n, 0)
+            wall = C.c_double()
+            check(lib().fx_server_run(h, 1 if realtime else 0, C.byref(wall)))
+            served = []
+            for r in reqs:
+                n, steps = sizes[r.id]
+                x = np.empty(n)
+                res = L.fx_solve_result()
+                t = (C.c_double * 3)()
+                mon = np.empty(max(steps, 1))
+                nit = np.empty(max(steps, 1), dtype=np.int32)
+                check(lib().fx_server_result(h, r.id, x.ctypes.data_as(L.p_f64), C.byref(res), t,
+                                             mon.ctypes.data_as(L.p_f64), nit.ctypes.data_as(L.p_i32)))
+                if steps:
+                    result = J2Result(mon[:steps].copy(), nit[:steps].astype(np.int64), bool(res.converged))
+                else:
+                    result = SolveResult(bool(res.converged), res.iterations, res.rhs_norm, res.initial_residual,
+                                         res.final_residual, bool(res.indefinite), res.refinements)
+                served.append(Served(r.id, x, result, t[0], t[1], t[2]))
+            return served, wall.value
+        finally:
+            lib().fx_server_destroy(h)
+
+
 def resident(requests, device: int = 0, rtol: float = 1e-8, j2_host: bool = False, cache: dict = None):
     """Prepare every request's mesh up front (the resident state a serving process keeps):
     {id: (force, b, n)} for static solves and {id: (force, unit load, monitored equation, n)} for

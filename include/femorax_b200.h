@@ -486,7 +486,7 @@ int fx_nbatch_step(fx_nbatch* b, const double* fext, double* u, double tol, int3
 
 /* ------------------------------------------------------------------ elementary functions
  * The exp, log, pow and cos of the PressureDependMultiYield device update (fx_math.h: built from
- * IEEE-exact operations, so a host and a device evaluation give the same bits; within 0.54 ulp and
+ * IEEE-exact operations, so a host and a device evaluation give the same bits; within 0.51 ulp and
  * one ulp of the host C library's). fx_math_eval runs them on device arrays (x, y, out on the
  * current device; y only for pow) on `stream`; fx_math_eval_host on host arrays. For checking the
  * device update against the reference's material linked to the same functions. No counterpart in
@@ -537,6 +537,35 @@ int fx_engine_round(fx_engine* e, int32_t* running);
 int fx_engine_finished(fx_engine* e, int32_t slot, int32_t* finished);
 int fx_engine_retire(fx_engine* e, int32_t slot, double* x_host, fx_solve_result* r);
 int fx_engine_info(const fx_engine* e, int64_t* info);
+
+/* ------------------------------------------------------------------ the serving loop
+ * Requests arriving over time, served on one device with continuous batching (serve.cu): static
+ * solves K x = b on resident fx_force meshes (several requests may share one) through an engine
+ * (fx_engine_*), and quasi-static J2 load paths on compiled meshes in cohorts (fx_nbatch_*) between
+ * the engine's rounds. Prepared requests are added with their arrival time (seconds from the start);
+ * fx_server_run serves them once: in arrival order (in real time, or all visible at once), static
+ * solves admitted while the footprint of the admitted requests (mesh device bytes; a J2 instance's
+ * estimate) fits hbm_budget and the engine has room; one engine round and one J2 load step per pass.
+ *   fx_server_add_j2   mesh (fx_compiled_mesh; its arrays must live until the run ends), the load at
+ *                      factor 1 (host, num_equations), the monitored equation, the load path (cycles
+ *                      of steps_per_cycle steps, 0 -> 1 -> -1 -> 0), Newton ||r|| <= tol in at most
+ *                      max_newton solves, CG (Jacobi) to cg_rtol in at most cg_max_iterations;
+ *                      requests with the same path and settings share a cohort (up to max_cohort).
+ *   fx_server_result   x (num_equations), the result, times[3] = arrival, admitted, done (seconds
+ *                      from the start of the run, steady clock); J2: the monitored displacement and
+ *                      the Newton solves after each step (cycles * steps_per_cycle each).
+ * A result is bit for bit the request's alone (the engine's solve of its mesh; the batched Newton
+ * path of its mesh). No counterpart in the reference, which runs one analysis per process. */
+typedef struct fx_server fx_server;
+int fx_server_create(fx_engine* engine, int32_t device, int64_t hbm_budget, int32_t max_cohort, fx_server** out);
+void fx_server_destroy(fx_server* s);
+int fx_server_add_static(fx_server* s, int64_t id, fx_force* f, const double* b_host, double arrival);
+int fx_server_add_j2(fx_server* s, int64_t id, const fx_mesh* mesh, const double* unit_load, int64_t monitor,
+                     int32_t cycles, int32_t steps_per_cycle, double tol, int32_t max_newton, double cg_rtol,
+                     int32_t cg_max_iterations, double arrival);
+int fx_server_run(fx_server* s, int32_t realtime, double* wall_seconds);
+int fx_server_result(const fx_server* s, int64_t id, double* x_host, fx_solve_result* r, double* times,
+                     double* monitor, int32_t* newton);
 
 /* ------------------------------------------------------------------ PressureIndependMultiYield
  * Material points of the multi-yield-surface von Mises soil model (OpenSees nDMaterial

@@ -72,3 +72,51 @@ def test_admission_budget_from_free_device_memory():
     srv = serving.Server(engine(), reserve=1 << 30)
     assert 0 < srv.budget <= total - (1 << 30)
     assert abs(srv.budget - (free0 - (1 << 30))) <= total // 10
+
+
+def test_native_server_same_alone_and_in_the_mix():
+    """The loop in C++ (fx_server_*, serving.NativeServer) on the same mixed stream: every J2 result
+    bit for bit the load path alone, every static solution bit for bit the Python loop's (the same
+    engine arithmetic), two requests on one shared InternalForce included."""
+    stream = with_loads(STREAM)
+    prep = {r.id: serving.prepare_any(r) for r in stream}
+    twin = serving.Request(99, 6, 5, 9, E=70e6, nu=0.3, q=-60e3)
+    force0, b0, n0 = prep[0]
+    prep[99] = (force0, b0 * 0.6, n0)  # the same mesh and force as request 0, its own load
+    stream = stream + [twin]
+    srv = serving.NativeServer(engine(), hbm_budget=1 << 34, prepare_fn=lambda r, d: prep[r.id], max_cohort=2)
+    served, wall = srv.run(stream, realtime=False)
+    assert sorted(s.id for s in served) == sorted(r.id for r in stream) and wall > 0
+    by_id = {s.id: s for s in served}
+    py, _ = serving.Server(engine(), hbm_budget=1 << 34, prepare_fn=lambda r, d: prep[r.id]).run(
+        [r for r in stream if not isinstance(r, serving.J2Request)], realtime=False)
+    py = {s.id: s for s in py}
+    for r in stream:
+        s = by_id[r.id]
+        assert s.result.converged, r.id
+        assert 0.0 <= s.admitted <= s.done
+        if isinstance(r, serving.J2Request):
+            mesh, f, mon, n = prep[r.id]
+            force = fx.InternalForce(mesh)
+            u, res = serving.solve_j2_alone(r, force, torch.as_tensor(f, device=DEV), mon)
+            assert np.array_equal(s.x, u), r.id
+            assert np.array_equal(s.result.monitor, res.monitor), r.id
+            assert np.array_equal(s.result.newton, res.newton), r.id
+        else:
+            assert np.array_equal(s.x, py[r.id].x), r.id
+    op = fx.MatrixFreeOperator(force0, fx.OperatorCoefficients())
+    for rid, b in ((0, b0), (99, b0 * 0.6)):
+        y = torch.zeros(n0, dtype=torch.float64, device=DEV)
+        op.apply(torch.as_tensor(by_id[rid].x, device=DEV), y)
+        assert np.linalg.norm(b - y.cpu().numpy()) <= RTOL * np.linalg.norm(b)
+
+
+def test_native_server_real_time():
+    """Arrivals in real time: no request is admitted before it arrives, every one is served, and the
+    latencies come from the library's clock."""
+    stream = [serving.Request(i, 4 + i % 3, 4, 6 + i, arrival=0.02 * i) for i in range(8)]
+    served, wall = serving.NativeServer(engine(), hbm_budget=1 << 34).run(stream, realtime=True)
+    assert len(served) == 8 and all(s.result.converged for s in served)
+    for s in served:
+        assert s.admitted >= s.arrival - 1e-9 and s.done >= s.admitted, s
+    assert wall >= 0.14
