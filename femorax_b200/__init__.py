@@ -817,6 +817,10 @@ class BatchEngine:
         self.device = device
         self._forces = {}
 
+    def set_persistent(self, on: bool = True):
+        """The batched apply as a persistent wave of CTAs over the work list (or one CTA per item)."""
+        check(lib().fx_engine_set_persistent(self._h, 1 if on else 0))
+
     def admit(self, force: InternalForce, b: np.ndarray) -> int:
         b = np.ascontiguousarray(b, dtype=np.float64)
         slot = C.c_int32()

@@ -196,8 +196,9 @@ PROTOTYPES = {
                                    C.POINTER(vp)]),
     "fx_engine_destroy": (None, [vp]),
     "fx_engine_set_precision": (C.c_int, [vp, C.c_int32]),
+    "fx_engine_set_persistent": (C.c_int, [vp, C.c_int32]),
     "fx_math_eval": (C.c_int, [C.c_int32, vp, vp, vp, C.c_int64, vp]),
-    "fx_server_create": (C.c_int, [vp, C.c_int32, C.c_int64, C.c_int32, C.POINTER(vp)]),
+    "fx_server_create": (C.c_int, [vp, C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]),
     "fx_server_destroy": (None, [vp]),
     "fx_server_add_static": (C.c_int, [vp, C.c_int64, vp, p_f64, C.c_double]),
     "fx_server_add_j2": (C.c_int, [vp, C.c_int64, C.POINTER(fx_mesh), p_f64, C.c_int64, C.c_int32, C.c_int32,

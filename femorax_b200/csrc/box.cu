@@ -530,16 +530,17 @@ template <class T>
 constexpr int kBatchMinB = sizeof(T) == 4 ? 6 : 4;  // FP32 fits 6 CTAs per SM without spills
 
 template <class T>
-void batch_launch(const void* inst, const int4* work, int nwork, cudaStream_t st) {
+void batch_launch(const void* inst, const int4* work, int nwork, int* queue, cudaStream_t st) {
   using S = Smem<kBatchBX, kBatchBY, T, 0, kPerSet>;
-  static bool configured = false;
-  if (!configured) {
-    FX_CUDA(cudaFuncSetAttribute(k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB<T>>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
-    configured = true;
+  auto kern = k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB<T>>;
+  static int resident = 0;  // CTAs per SM
+  if (!resident) {
+    FX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
+    FX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kBatchBX * kBatchBY, S::bytes));
+    resident = std::max(resident, 1);
   }
-  k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB<T>>
-      <<<nwork, kBatchBX * kBatchBY, S::bytes, st>>>(static_cast<const BoxArgs<T>*>(inst), work);
+  const int ctas = queue ? std::min(nwork, resident * num_sms()) : nwork;
+  kern<<<ctas, kBatchBX * kBatchBY, S::bytes, st>>>(static_cast<const BoxArgs<T>*>(inst), work, nwork, queue);
   FX_LAUNCH_CHECK("box_batch");
 }
 
@@ -738,10 +739,10 @@ void box_batch_tiles(const ForceState& s, int& gx, int& gy, int& gz) {
   gz = (s.box.nz + 1 + kBatchKz - 1) / kBatchKz;
 }
 
-void box_batch_apply(bool f32, const void* inst, const int4* work, int nwork, cudaStream_t st) {
+void box_batch_apply(bool f32, const void* inst, const int4* work, int nwork, int* queue, cudaStream_t st) {
   if (nwork <= 0) return;
-  if (f32) batch_launch<float>(inst, work, nwork, st);
-  else batch_launch<double>(inst, work, nwork, st);
+  if (f32) batch_launch<float>(inst, work, nwork, queue, st);
+  else batch_launch<double>(inst, work, nwork, queue, st);
 }
 
 }  // namespace fx

@@ -545,14 +545,36 @@ __global__ void __launch_bounds__(BX* BY, MINB)
   }
 }
 
-// Many grids in one launch: CTA b takes work item work[b] = (grid, tile x, tile y, tile z) of the
-// grids inst[] describes (each with its own maps, tables, vectors and skip flag).
+// Many grids in one launch: work items work[i] = (grid, tile x, tile y, tile z) of the grids inst[]
+// describes (each with its own maps, tables, vectors and skip flag). With queue == NULL, CTA b takes
+// item b (one CTA per item); otherwise a persistent wave of CTAs takes the items in list order from
+// the counter queue[0] until none is left, and the last CTA to finish resets queue[0..1] for the
+// next launch (every CTA has stopped taking items then), as k_box's persistent form.
 template <int BX, int BY, class T, int MODE, int MINB>
 __global__ void __launch_bounds__(BX* BY, MINB)
-    k_box_batch(const BoxArgs<T>* __restrict__ inst, const int4* __restrict__ work) {
-  const int4 w = work[blockIdx.x];
-  const BoxArgs<T> a = inst[w.x];
-  box_tile<BX, BY, T, MODE, false, kPerSet, false>(a, nullptr, w.y, w.z, w.w);
+    k_box_batch(const BoxArgs<T>* __restrict__ inst, const int4* __restrict__ work, int nwork, int* queue) {
+  if (!queue) {
+    const int4 w = work[blockIdx.x];
+    const BoxArgs<T> a = inst[w.x];
+    box_tile<BX, BY, T, MODE, false, kPerSet, false>(a, nullptr, w.y, w.z, w.w);
+    return;
+  }
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(&queue[0], 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= nwork) break;
+    const int4 w = work[item];
+    const BoxArgs<T> a = inst[w.x];
+    box_tile<BX, BY, T, MODE, false, kPerSet, false>(a, nullptr, w.y, w.z, w.w);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && atomicAdd(&queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
+    queue[0] = 0;
+    queue[1] = 0;
+  }
 }
 
 // ------------------------------------------------------------------ launch variants

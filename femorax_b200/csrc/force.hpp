@@ -307,7 +307,8 @@ bool box_apply_host(ForceState& s, const double k[3], const double* xh, double* 
 size_t box_args_bytes(bool f32);
 void box_fill_args(ForceState& s, const double k[3], bool f32, const void* x, void* y, const int* skip, void* dst);
 void box_batch_tiles(const ForceState& s, int& gx, int& gy, int& gz);
-void box_batch_apply(bool f32, const void* inst, const int4* work, int nwork, cudaStream_t st);
+// queue: a device int[2], zero between launches, for the persistent form (NULL: one CTA per item)
+void box_batch_apply(bool f32, const void* inst, const int4* work, int nwork, int* queue, cudaStream_t st);
 
 }  // namespace fx
 

@@ -11,10 +11,12 @@
 //     engine has a slot and a range of chunks; every pass of the loop runs one refinement round of
 //     every admitted solve (one batched launch per operator apply for all of them), so requests that
 //     arrive while others run join at the next round;
-//   - J2 load paths run in cohorts: when the J2 lane is idle, the waiting requests with the head's
-//     load path (in arrival order, up to max_cohort, while the footprint fits) become one batched
-//     Newton (fx_nbatch_*: one combined mesh, per-instance Newton and CG on the device), which
-//     advances one load step per pass of the loop, between the engine's rounds;
+//   - J2 load paths run in cohorts on up to max_lanes lanes: while a lane is free, the waiting
+//     requests with the head's load path (in arrival order, up to max_cohort, while the footprint
+//     fits) become one batched Newton (fx_nbatch_*: one combined mesh, per-instance Newton and CG on
+//     the device) on it; every cohort advances one load step per pass of the loop, between the
+//     engine's rounds. A running cohort takes no new members (its combined mesh is fixed), so J2
+//     requests that arrive while it runs start the next cohort on another lane;
 //   - finished requests are retired and their results kept.
 // Each request's arithmetic is that of the request alone, so its result is bit for bit the same
 // alone and in any mix: a static solve as the engine's (the FX_SOLVER_IR solve of its mesh), a J2
@@ -133,6 +135,7 @@ struct Server {
   int device = 0;
   int64_t budget = 0;
   int max_cohort = 32;
+  int max_lanes = 4;
   std::vector<Request> reqs;
   std::unordered_map<int64_t, size_t> by_id;
   bool ran = false;
@@ -240,10 +243,10 @@ struct Server {
     auto now = [&]() { return std::chrono::duration<double>(clock::now() - t0).count(); };
     std::deque<size_t> pending, pending_j2;
     std::map<int32_t, size_t> slots;
-    std::unique_ptr<Cohort> lane;
+    std::vector<std::unique_ptr<Cohort>> lanes;
     int64_t resident = 0;
     size_t nxt = 0;
-    while (nxt < order.size() || !pending.empty() || !pending_j2.empty() || !slots.empty() || lane) {
+    while (nxt < order.size() || !pending.empty() || !pending_j2.empty() || !slots.empty() || !lanes.empty()) {
       const double t = realtime ? now() : INFINITY;
       while (nxt < order.size() && reqs[order[nxt]].arrival <= t) {
         const size_t i = order[nxt++];
@@ -252,7 +255,7 @@ struct Server {
       // admissions in arrival order, while the footprint fits and the engine has room
       while (!pending.empty()) {
         Request& r = reqs[pending.front()];
-        if ((!slots.empty() || lane) && resident + r.footprint > budget) break;
+        if ((!slots.empty() || !lanes.empty()) && resident + r.footprint > budget) break;
         int32_t slot = -1;
         const int rc = fx_engine_admit(engine, r.f, r.b.data(), &slot);
         if (rc == FX_E_NOMEM) break;
@@ -262,20 +265,21 @@ struct Server {
         resident += r.footprint;
         r.admitted = now();
       }
-      if (slots.empty() && !lane && !pending.empty())
+      if (slots.empty() && lanes.empty() && !pending.empty())
         throw Error(FX_E_NOMEM, "fx_server: request " + std::to_string(reqs[pending.front()].id) +
                                     " does not fit the engine even alone");
-      if (!lane && !pending_j2.empty()) {
-        lane = std::make_unique<Cohort>();
-        start_cohort(pending_j2, *lane, resident, !slots.empty(), now());
-        if (lane->members.empty()) {
-          lane.reset();
-          if (slots.empty())
+      while (static_cast<int>(lanes.size()) < max_lanes && !pending_j2.empty()) {
+        auto c = std::make_unique<Cohort>();
+        start_cohort(pending_j2, *c, resident, !slots.empty() || !lanes.empty(), now());
+        if (c->members.empty()) {
+          if (slots.empty() && lanes.empty())
             throw Error(FX_E_NOMEM, "fx_server: J2 request " + std::to_string(reqs[pending_j2.front()].id) +
                                         " does not fit the budget even alone");
+          break;
         }
+        lanes.push_back(std::move(c));
       }
-      if (slots.empty() && !lane) {
+      if (slots.empty() && lanes.empty()) {
         if (nxt < order.size() && realtime) {
           const double wait = std::min(0.01, reqs[order[nxt]].arrival - now());
           if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
@@ -300,11 +304,13 @@ struct Server {
           it = slots.erase(it);
         }
       }
-      if (lane) {
+      for (auto it = lanes.begin(); it != lanes.end();) {
         double done_at = 0.0;
-        if (step_cohort(*lane, done_at, now)) {
-          resident -= lane->footprint;
-          lane.reset();
+        if (step_cohort(**it, done_at, now)) {
+          resident -= (*it)->footprint;
+          it = lanes.erase(it);
+        } else {
+          ++it;
         }
       }
     }
@@ -322,15 +328,17 @@ struct fx_server {
 
 extern "C" {
 
-int fx_server_create(fx_engine* engine, int32_t device, int64_t hbm_budget, int32_t max_cohort, fx_server** out) {
+int fx_server_create(fx_engine* engine, int32_t device, int64_t hbm_budget, int32_t max_cohort, int32_t max_lanes,
+                     fx_server** out) {
   return fx::guard([&] {
-    if (!engine || !out || hbm_budget < 0 || max_cohort <= 0)
+    if (!engine || !out || hbm_budget < 0 || max_cohort <= 0 || max_lanes <= 0)
       throw fx::Error(FX_E_INVALID, "fx_server_create: bad arguments");
     auto* h = new fx_server;
     h->s.engine = engine;
     h->s.device = device;
     h->s.budget = hbm_budget;
     h->s.max_cohort = max_cohort;
+    h->s.max_lanes = max_lanes;
     *out = h;
   });
 }

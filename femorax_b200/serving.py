@@ -426,14 +426,15 @@ class Server:
 class NativeServer:
     """The serving loop in C++ (fx_server_*, serve.cu) over one BatchEngine: the same admission by
     footprint, engine rounds for the static solves and J2 cohorts (up to max_cohort, fx_nbatch) as
-    Server, with the loop, the arrival gating and the clock in the library; latency is measured by
+    Server, with up to max_lanes cohorts running at once (J2 requests that arrive while one runs
+    start the next), the loop, the arrival gating and the clock in the library; latency is measured by
     the host's steady clock inside it. run() takes the requests with their prepared state
     (prepare_fn(request, device) as for Server: (force, b, n) for a static solve, prepare_j2's
     (mesh, unit load, monitored equation, n) for a J2 path) and returns (served, wall seconds)."""
 
     def __init__(self, engine: BatchEngine, hbm_budget: int = None, device: int = 0, prepare_fn=None,
-                 max_cohort: int = 32, reserve: int = 2 << 30, tol: float = 1e-6, max_newton: int = 25,
-                 cg_rtol: float = 1e-12, cg_max_iterations: int = 20000):
+                 max_cohort: int = 32, max_lanes: int = 4, reserve: int = 2 << 30, tol: float = 1e-6,
+                 max_newton: int = 25, cg_rtol: float = 1e-12, cg_max_iterations: int = 20000):
         self.engine = engine
         if hbm_budget is None:
             free, _ = device_memory(device)
@@ -442,6 +443,7 @@ class NativeServer:
         self.device = device
         self.prepare = prepare_fn or prepare_any
         self.max_cohort = int(max_cohort)
+        self.max_lanes = int(max_lanes)
         self.j2_settings = (float(tol), int(max_newton), float(cg_rtol), int(cg_max_iterations))
 
     def run(self, requests, realtime: bool = True):
@@ -450,7 +452,8 @@ class NativeServer:
         from ._lib import check, lib
         reqs = sorted(requests, key=lambda r: r.arrival)
         h = C.c_void_p()
-        check(lib().fx_server_create(self.engine._h, self.device, self.budget, self.max_cohort, C.byref(h)))
+        check(lib().fx_server_create(self.engine._h, self.device, self.budget, self.max_cohort, self.max_lanes,
+                                     C.byref(h)))
         keep, sizes = [], {}
         try:
             tol, max_newton, cg_rtol, cg_max_it = self.j2_settings

@@ -532,6 +532,9 @@ int fx_engine_create(int32_t device, int64_t capacity, int32_t max_slots, fx_coe
                      double inner_rtol, fx_engine** out);
 void fx_engine_destroy(fx_engine* e);
 int fx_engine_set_precision(fx_engine* e, int32_t inner);
+/* The batched apply as one CTA per (slot, tile) work item (on = 0, the default) or as a persistent
+ * wave of CTAs taking the items from a counter (on = 1); the same bits either way. */
+int fx_engine_set_persistent(fx_engine* e, int32_t on);
 int fx_engine_admit(fx_engine* e, fx_force* f, const double* b_host, int32_t* slot);
 int fx_engine_round(fx_engine* e, int32_t* running);
 int fx_engine_finished(fx_engine* e, int32_t slot, int32_t* finished);
@@ -550,14 +553,17 @@ int fx_engine_info(const fx_engine* e, int64_t* info);
  *                      factor 1 (host, num_equations), the monitored equation, the load path (cycles
  *                      of steps_per_cycle steps, 0 -> 1 -> -1 -> 0), Newton ||r|| <= tol in at most
  *                      max_newton solves, CG (Jacobi) to cg_rtol in at most cg_max_iterations;
- *                      requests with the same path and settings share a cohort (up to max_cohort).
+ *                      requests with the same path and settings share a cohort (up to max_cohort);
+ *                      up to max_lanes cohorts run at once (one step each per pass), so J2 requests
+ *                      arriving while a cohort runs start the next one.
  *   fx_server_result   x (num_equations), the result, times[3] = arrival, admitted, done (seconds
  *                      from the start of the run, steady clock); J2: the monitored displacement and
  *                      the Newton solves after each step (cycles * steps_per_cycle each).
  * A result is bit for bit the request's alone (the engine's solve of its mesh; the batched Newton
  * path of its mesh). No counterpart in the reference, which runs one analysis per process. */
 typedef struct fx_server fx_server;
-int fx_server_create(fx_engine* engine, int32_t device, int64_t hbm_budget, int32_t max_cohort, fx_server** out);
+int fx_server_create(fx_engine* engine, int32_t device, int64_t hbm_budget, int32_t max_cohort, int32_t max_lanes,
+                     fx_server** out);
 void fx_server_destroy(fx_server* s);
 int fx_server_add_static(fx_server* s, int64_t id, fx_force* f, const double* b_host, double arrival);
 int fx_server_add_j2(fx_server* s, int64_t id, const fx_mesh* mesh, const double* unit_load, int64_t monitor,

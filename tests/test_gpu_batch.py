@@ -180,3 +180,14 @@ def test_fp64_inner_engine(prepared):
     e2.admit(f0, b0)
     with pytest.raises(fx.FxError):  # the precision is fixed while slots are in use
         fx._lib.check(fx._lib.lib().fx_engine_set_precision(e2._h, 0))
+
+
+def test_persistent_work_list_same_bits(prepared, alone):
+    """The batched apply as a persistent wave of CTAs over the work list gives every slot the same bits."""
+    e = engine()
+    e.set_persistent(True)
+    slots = {e.admit(f, b): rid for rid, (f, b, _) in prepared.items()}
+    out = run_to_end(e, slots)
+    for rid in prepared:
+        assert np.array_equal(out[rid][0], alone[rid][0]), rid
+        assert out[rid][1].iterations == alone[rid][1].iterations

@@ -120,3 +120,24 @@ def test_native_server_real_time():
     for s in served:
         assert s.admitted >= s.arrival - 1e-9 and s.done >= s.admitted, s
     assert wall >= 0.14
+
+
+def test_native_server_second_cohort_starts_while_first_runs():
+    """A J2 request that arrives while a cohort runs starts another cohort on a free lane (it does not
+    wait for the first path to end), and both results are bit for bit their paths alone."""
+    a0 = with_loads([serving.J2Request(0, 2, 2, 30, E=90e6, sigma_y=150e3, total=0.0, steps_per_cycle=8)])[0]
+    a = serving.J2Request(0, a0.nx, a0.ny, a0.nz, a0.E, a0.sigma_y, a0.total, a0.h, cycles=3, steps_per_cycle=8,
+                          arrival=0.0)
+    b0 = with_loads([serving.J2Request(1, 1, 1, 24, E=60e6, sigma_y=80e3, total=0.0, steps_per_cycle=4)])[0]
+    b = serving.J2Request(1, b0.nx, b0.ny, b0.nz, b0.E, b0.sigma_y, b0.total, b0.h, cycles=1, steps_per_cycle=4,
+                          arrival=0.02)
+    prep = {r.id: serving.prepare_j2(r) for r in (a, b)}
+    srv = serving.NativeServer(engine(), hbm_budget=1 << 34, prepare_fn=lambda r, d: prep[r.id], max_lanes=2)
+    served, _ = srv.run([a, b], realtime=True)
+    s = {x.id: x for x in served}
+    assert s[1].admitted < s[0].done, (s[1].admitted, s[0].done)
+    for r in (a, b):
+        mesh, f, mon, n = prep[r.id]
+        u, res = serving.solve_j2_alone(r, fx.InternalForce(mesh), torch.as_tensor(f, device=DEV), mon)
+        assert s[r.id].result.converged
+        assert np.array_equal(s[r.id].x, u) and np.array_equal(s[r.id].result.monitor, res.monitor), r.id
