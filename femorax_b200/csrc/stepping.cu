@@ -33,7 +33,8 @@ __global__ void k_ed_predict(T* __restrict__ u, T* __restrict__ vh, const T* __r
   }
 }
 
-// correction of step `step` and prediction of step `step + 1`
+// correction of step `step` and prediction of step `step + 1`; the full-step velocity v is written by
+// the call's last step only (predict == 0): the steps between read the half-step velocity vh
 template <class T>
 __global__ void k_ed_correct_predict(const T* __restrict__ f, const T* __restrict__ m, const int8_t* __restrict__ dof,
                                      const double* __restrict__ ag, int* __restrict__ step, int dir, T dt,
@@ -52,7 +53,7 @@ __global__ void k_ed_correct_predict(const T* __restrict__ f, const T* __restric
     const T an = R / mq;
     const T t = T(3) * an + a[q];
     const T vhq = vh[q];
-    v[q] = vhq + t * halfT;
+    if (!predict) v[q] = vhq + t * halfT;  // (read only after the call's last step, which does not predict)
     a[q] = an;
     if (q == record_eq && hist) hist[s] = static_cast<double>(an);
     if (predict) {
