@@ -329,6 +329,11 @@ int fx_force_create(const fx_mesh* mesh, int32_t device, fx_force** out) {
       s.params.upload(s.params_h);
       s.gstart.upload(start);
       s.glist.upload(list);
+      std::vector<int32_t> heavy;
+      for (int32_t q = 0; q < s.neq; ++q)
+        if (start[q + 1] - start[q] > fx::kHeavySlots) heavy.push_back(q);
+      s.nheavy = static_cast<int32_t>(heavy.size());
+      if (!heavy.empty()) s.gheavy.upload(heavy);
       s.slots.alloc(24 * P);
       if (s.has_ssp) fx::ssp_setup(s);  // SSPbrick: each element's geometry and stabilization constants
       // J2 sets: state and tangent per Gauss point (virgin state, elastic tangent)

@@ -14,6 +14,9 @@
 
 namespace fx {
 
+// equations whose slot sum runs a warp each (k_gather_heavy) instead of a thread
+constexpr int32_t kHeavySlots = 64;
+
 // Coefficients of the exact modal element operator of one parameter set on the box grid, for
 // the current operator coefficients (box.cu builds them). Scaled by 1/64 where the two
 // Walsh-Hadamard transforms (unnormalised) would otherwise multiply the result by 64.
@@ -176,6 +179,8 @@ struct ForceState {
   DeviceArray<int32_t> node, eq, param;
   DeviceArray<ParamGP> params;
   DeviceArray<int32_t> gstart, glist;  // per-equation slot lists in (element, DOF) order
+  DeviceArray<int32_t> gheavy;          // the equations with more than kHeavySlots slots (tied DOFs), a warp each
+  int32_t nheavy = 0;
   DeviceArray<double> slots;           // [24 * P]
   DeviceArray<float> geom32, nshape32, slots32;  // FP32 operator: point geometry, shape values, slots
   DeviceArray<double> nodal_mass, nodal_alpha_mass, lumped_mass;

@@ -453,19 +453,63 @@ __device__ __forceinline__ T slot_sum(const int32_t* __restrict__ list, const T*
   return sum;
 }
 
+// The same sum by one warp, for equations with many slots (a tied DOF gathers whole rows of
+// elements): 32 slots loaded at once, then added in list order by every lane.
+template <class T>
+__device__ __forceinline__ T slot_sum_warp(const int32_t* __restrict__ list, const T* __restrict__ slots, int32_t j0,
+                                           int32_t j1) {
+  const int lane = threadIdx.x & 31;
+  T sum = T(0);
+  for (int32_t b = j0; b < j1; b += 32) {
+    const int32_t j = b + lane;
+    const T v = j < j1 ? slots[list[j]] : T(0);
+    const int cnt = j1 - b < 32 ? j1 - b : 32;
+    for (int u = 0; u < cnt; ++u) sum += __shfl_sync(0xffffffffu, v, u);
+  }
+  return sum;
+}
+
 // y[q] = sum of q's slots in list order, then + c1 m1[q] x1[q] + c2 m2[q] x2[q] (the nodal-mass
-// kernels of internal_force.cpp:368-375, 442-448, same expression, same order).
+// kernels of internal_force.cpp:368-375, 442-448, same expression, same order). The first `hblocks`
+// blocks take the equations heavy[0 .. nheavy) (more than kHeavySlots slots each: tied DOFs) a warp
+// each, so that their long sums start first and overlap the others; the other blocks a thread per
+// equation, leaving the heavy ones.
 __global__ void __launch_bounds__(256) k_gather(const int32_t* __restrict__ start, const int32_t* __restrict__ list,
-                                                 const double* __restrict__ slots, int32_t neq, double c1,
-                                                 const double* __restrict__ m1, const double* __restrict__ x1, double c2,
+                                                 const double* __restrict__ slots, int32_t neq,
+                                                 const int32_t* __restrict__ heavy, int32_t nheavy, int32_t hblocks,
+                                                 double c1, const double* __restrict__ m1,
+                                                 const double* __restrict__ x1, double c2,
                                                  const double* __restrict__ m2, const double* __restrict__ x2,
                                                  double* __restrict__ y, const int* skip) {
-  const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= neq || (skip && *skip)) return;
-  double sum = slot_sum(list, slots, start[q], start[q + 1]);
+  if (skip && *skip) return;
+  double sum;
+  int32_t q;
+  if (static_cast<int32_t>(blockIdx.x) < hblocks) {
+    const int32_t w = static_cast<int32_t>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= nheavy) return;  // (the same for the whole warp)
+    q = heavy[w];
+    sum = slot_sum_warp(list, slots, start[q], start[q + 1]);
+    if ((threadIdx.x & 31) != 0) return;
+  } else {
+    q = (static_cast<int32_t>(blockIdx.x) - hblocks) * static_cast<int32_t>(blockDim.x) + static_cast<int32_t>(threadIdx.x);
+    if (q >= neq) return;
+    const int32_t j0 = start[q], j1 = start[q + 1];
+    if (j1 - j0 > kHeavySlots) return;
+    sum = slot_sum(list, slots, j0, j1);
+  }
   if (m1) sum += c1 * m1[q] * (x1 ? x1[q] : 1.0);
   if (m2) sum += c2 * m2[q] * (x2 ? x2[q] : 1.0);
   y[q] = sum;
+}
+
+// y = every equation's slot sum and nodal terms (one k_gather launch)
+void gather_slots(const ForceState& s, double c1, const double* m1, const double* x1, double c2, const double* m2,
+                  const double* x2, double* y, const int* skip, cudaStream_t st) {
+  if (s.neq <= 0) return;
+  const int32_t hblocks = static_cast<int32_t>(s.nheavy > 0 ? grid_for(32 * static_cast<int64_t>(s.nheavy), 256) : 0);
+  k_gather<<<hblocks + grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq,
+                                                           s.gheavy.ptr, s.nheavy, hblocks, c1, m1, x1, c2, m2, x2, y,
+                                                           skip);
 }
 
 // ---- FP32 operator (the inner solves of FP32 CG in FP64 refinement on any mesh)
@@ -576,13 +620,27 @@ __global__ void __launch_bounds__(kBlock) k_element_apply32(const int32_t* __res
 }
 
 __global__ void __launch_bounds__(256) k_gather32(const int32_t* __restrict__ start, const int32_t* __restrict__ list,
-                                                   const float* __restrict__ slots, int32_t neq, double c1,
-                                                   const double* __restrict__ m1, double c2,
+                                                   const float* __restrict__ slots, int32_t neq,
+                                                   const int32_t* __restrict__ heavy, int32_t nheavy, int32_t hblocks,
+                                                   double c1, const double* __restrict__ m1, double c2,
                                                    const double* __restrict__ m2, const float* __restrict__ x,
                                                    float* __restrict__ y, const int* skip) {
-  const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= neq || (skip && *skip)) return;
-  float sum = slot_sum(list, slots, start[q], start[q + 1]);
+  if (skip && *skip) return;
+  float sum;
+  int32_t q;
+  if (static_cast<int32_t>(blockIdx.x) < hblocks) {  // the heavy equations, a warp each (as k_gather)
+    const int32_t w = static_cast<int32_t>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= nheavy) return;
+    q = heavy[w];
+    sum = slot_sum_warp(list, slots, start[q], start[q + 1]);
+    if ((threadIdx.x & 31) != 0) return;
+  } else {
+    q = (static_cast<int32_t>(blockIdx.x) - hblocks) * static_cast<int32_t>(blockDim.x) + static_cast<int32_t>(threadIdx.x);
+    if (q >= neq) return;
+    const int32_t j0 = start[q], j1 = start[q + 1];
+    if (j1 - j0 > kHeavySlots) return;
+    sum = slot_sum(list, slots, j0, j1);
+  }
   if (m1) sum += static_cast<float>(c1 * m1[q]) * x[q];
   if (m2) sum += static_cast<float>(c2 * m2[q]) * x[q];
   y[q] = sum;
@@ -837,8 +895,10 @@ void general_apply_f32(ForceState& s, const double k[3], const float* x, float* 
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
-    k_gather32<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots32.ptr, s.neq, k[2], m1, k[1],
-                                                     m2, x, y, skip);
+    k_gather32<<<(s.nheavy > 0 ? grid_for(32 * static_cast<int64_t>(s.nheavy), 256) : 0) + grid_for(s.neq, 256), 256, 0,
+                 st>>>(s.gstart.ptr, s.glist.ptr, s.slots32.ptr, s.neq, s.gheavy.ptr, s.nheavy,
+                       static_cast<int32_t>(s.nheavy > 0 ? grid_for(32 * static_cast<int64_t>(s.nheavy), 256) : 0),
+                       k[2], m1, k[1], m2, x, y, skip);
   FX_LAUNCH_CHECK("slot_gather32");
 }
 
@@ -855,16 +915,14 @@ void general_gather(ForceState& s, const double k[3], const double* x, double* y
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
-    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, k[2], m1, x, k[1], m2,
-                                                   x, y, skip);
+    gather_slots(s, k[2], m1, x, k[1], m2, x, y, skip, st);
   FX_LAUNCH_CHECK("slot_gather");
 }
 
 void general_force_gather(ForceState& s, const double* v, double* f, cudaStream_t st) {
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
-    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
-                                                   nullptr, 1.0, m2, v, f, nullptr);
+    gather_slots(s, 0.0, nullptr, nullptr, 1.0, m2, v, f, nullptr, st);
   FX_LAUNCH_CHECK("slot_gather");
 }
 
@@ -882,8 +940,7 @@ void general_apply(ForceState& s, const double k[3], const double* x, double* y,
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
-    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, k[2], m1, x, k[1], m2,
-                                                   x, y, skip);
+    gather_slots(s, k[2], m1, x, k[1], m2, x, y, skip, st);
   FX_LAUNCH_CHECK("slot_gather");
 }
 
@@ -900,8 +957,7 @@ void general_diagonal(ForceState& s, const double k[3], double* d, cudaStream_t 
   const double* m1 = (k[2] != 0.0 && s.has_nodal_mass) ? s.nodal_mass.ptr : nullptr;
   const double* m2 = (k[1] != 0.0 && s.has_nodal_alpha) ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
-    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, k[2], m1, nullptr,
-                                                   k[1], m2, nullptr, d, nullptr);
+    gather_slots(s, k[2], m1, nullptr, k[1], m2, nullptr, d, nullptr, st);
   FX_LAUNCH_CHECK("slot_gather");
 }
 
@@ -984,8 +1040,7 @@ void general_force(ForceState& s, const double* u, const double* v, double* f, c
   }
   const double* m2 = s.has_nodal_alpha ? s.nodal_alpha_mass.ptr : nullptr;
   if (s.neq > 0)
-    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
-                                                   nullptr, 1.0, m2, v, f, nullptr);
+    gather_slots(s, 0.0, nullptr, nullptr, 1.0, m2, v, f, nullptr, st);
   FX_LAUNCH_CHECK("slot_gather");
 }
 
@@ -1019,8 +1074,7 @@ void general_mass_times_ground(ForceState& s, int dir, double* y, cudaStream_t s
                                                                    s.pdmy_committed.ptr, s.ssp_geo.ptr, s.ssp_con.ptr);
   FX_LAUNCH_CHECK("element_apply_unit");
   if (s.neq > 0)
-    k_gather<<<grid_for(s.neq, 256), 256, 0, st>>>(s.gstart.ptr, s.glist.ptr, s.slots.ptr, s.neq, 0.0, nullptr,
-                                                   nullptr, 0.0, nullptr, nullptr, y, nullptr);
+    gather_slots(s, 0.0, nullptr, nullptr, 0.0, nullptr, nullptr, y, nullptr, st);
   if (s.has_nodal_mass && s.neq > 0)
     k_ground_nodal<<<grid_for(s.neq, 256), 256, 0, st>>>(s.nodal_mass.ptr, s.eq_dof.ptr, s.neq, dir, y);
   FX_LAUNCH_CHECK("ground_mass");
