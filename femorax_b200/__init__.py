@@ -793,8 +793,9 @@ class BatchEngine:
     alone; one launch per operator apply over every running slot's element tiles.
 
     admit() takes an InternalForce (kept alive here until its slot is retired) and a host
-    right-hand side; round() advances every running slot by one refinement round; finished() and
-    retire() hand results back. try_admit() returns None instead of raising when the engine is full.
+    right-hand side; round() advances every running slot by one tick (its correction and outer step
+    when due, then 8 inner iterations); finished() and retire() hand results back. try_admit()
+    returns None instead of raising when the engine is full.
     inner="fp64" makes the inner solves FP64 Jacobi-PCG with the FP64 operator (the batched engine
     without reduced precision; give an inner_tolerance at or below the outer relative tolerance).
     The same InternalForce may be admitted into several slots at once (its maps and tables are only

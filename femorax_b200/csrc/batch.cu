@@ -15,9 +15,13 @@
 // range (the second level a warp per slot over its chunk sums), exactly as a single solve of
 // the same mesh: a slot's result is bit for bit the same alone and in any mix.
 //
-// Serving (the host loop above) works in rounds: fx_engine_round runs one refinement round
-// (FP64 residual, FP32 inner solve, FP64 correction) of every running slot; between rounds the
-// host admits new requests into free slots and chunk ranges and retires finished ones.
+// The engine advances in ticks (fx_engine_round): a tick corrects the slots whose inner solve has
+// ended (x += d, the round's counters), gives them and newly admitted slots their outer step (FP64
+// residual and test, then the inner solve's start), and runs 8 inner iterations of every slot whose
+// inner solve is running; each slot's phase is held in device flags, so no slot waits for another's
+// inner solve to end. Every slot performs the same operations in the same order as FX_SOLVER_IR
+// on its mesh alone. Between ticks the host admits new requests into free slots and chunk ranges
+// (they join at the next tick) and retires finished ones.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -46,7 +50,9 @@ enum : int {
   G_FIN,       // finished (converged or given up)
   G_CONV,      // converged to the FP64 tolerance
   G_OUTER, G_INNER, G_INNER_RAN,
-  NFL = 12
+  G_NEED_OUTER,  // due for an outer step (admitted, or corrected and not finished)
+  F_BEGIN,       // its inner solve starts in this tick (set by the outer step)
+  NFL = 13
 };
 
 struct SlotDev {
@@ -86,15 +92,16 @@ __global__ void __launch_bounds__(32 * kWarps)
 }
 
 // second level: slot s's `ncol` columns of chunk sums (column j at part + j * nchunks) into
-// sc[s * NSC + dst + j], one warp per (slot, column), for slots whose flag `gate` is 0
+// sc[s * NSC + dst + j], one warp per (slot, column), for slots whose flag `gate` is 0 (inv = 0) or
+// nonzero (inv = 1)
 __global__ void k_b_level(const double* __restrict__ part, int64_t nchunks, int ncol, const SlotDev* __restrict__ sd,
-                          const int* __restrict__ fl, int gate, int nslots, int lanes, const int* __restrict__ used,
-                          double* __restrict__ sc, int dst) {
+                          const int* __restrict__ fl, int gate, int inv, int nslots, int lanes,
+                          const int* __restrict__ used, double* __restrict__ sc, int dst) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= nslots * ncol) return;
   const int s = w / ncol, j = w % ncol;
-  if (!used[s] || fl[s * NFL + gate]) return;
+  if (!used[s] || ((fl[s * NFL + gate] != 0) != (inv != 0))) return;
   const double* p = part + static_cast<int64_t>(j) * nchunks + sd[s].c0;
   const int64_t nc = sd[s].nc;
   double acc = 0.0;
@@ -149,6 +156,7 @@ __global__ void k_b_outer(double* sc, int* fl, const int* used, int nslots, doub
   int* f = fl + s * NFL;
   double* c = sc + s * NSC;
   if (f[G_SKIP]) return;
+  f[G_NEED_OUTER] = 0;
   if (f[G_OUTER] == 0) {
     c[O_BNORM] = sqrt(c[O_BB]);
     c[O_INIT] = sqrt(c[O_RR]);
@@ -171,6 +179,7 @@ __global__ void k_b_outer(double* sc, int* fl, const int* used, int nslots, doub
   f[F_DONE] = 0;
   f[F_MAXIT] = max_it - f[G_INNER];
   f[G_INNER_RAN] = 1;
+  f[F_BEGIN] = 1;
 }
 
 // inner setup (TI: the inner solve's type): ri = (TI) r, d = 0; CG begin from d = 0 (K d = 0):
@@ -185,7 +194,7 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
   const int s = slot_of_chunk(chunk_slot, c);
-  if (s < 0 || fl[s * NFL + F_DONE]) return;
+  if (s < 0 || !fl[s * NFL + F_BEGIN]) return;
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
@@ -222,7 +231,8 @@ __global__ void k_b_inner_start(double* sc, int* fl, const int* used, int nslots
   if (s >= nslots || !used[s]) return;
   int* f = fl + s * NFL;
   double* c = sc + s * NSC;
-  if (f[F_DONE]) return;
+  if (!f[F_BEGIN]) return;
+  f[F_BEGIN] = 0;
   c[S_RHS] = sqrt(c[S_RR]);  // b.b of the inner system: the same sum as r.r at d = 0
   const double rn = sqrt(c[S_RR]);
   c[S_RNORM] = rn;
@@ -340,7 +350,7 @@ __global__ void __launch_bounds__(32 * kWarps)
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
   const int s = slot_of_chunk(chunk_slot, c);
-  if (s < 0 || fl[s * NFL + G_SKIP] || !fl[s * NFL + G_INNER_RAN]) return;
+  if (s < 0 || !fl[s * NFL + F_DONE] || !fl[s * NFL + G_INNER_RAN]) return;  // its inner solve has ended
   const int64_t begin = c * kChunk;
   const int64_t end = sd[s].off + sd[s].n;
   const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
@@ -352,11 +362,20 @@ __global__ void k_b_round_end(int* fl, const int* used, int nslots) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots || !used[s]) return;
   int* f = fl + s * NFL;
-  if (f[G_SKIP] || !f[G_INNER_RAN]) return;
+  if (!f[F_DONE] || !f[G_INNER_RAN]) return;
   f[G_INNER] += f[F_ITERS];
   f[G_OUTER] += 1;
   if (f[F_ITERS] == 0 && !f[F_CONV]) f[G_FIN] = 1;  // the inner solve made no progress
   f[G_INNER_RAN] = 0;
+  if (!f[G_FIN]) f[G_NEED_OUTER] = 1;
+}
+
+// the tick's outer step: the slots due for one (the FP64 apply's skip flag is G_SKIP)
+__global__ void k_b_phase(int* fl, const int* used, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !used[s]) return;
+  int* f = fl + s * NFL;
+  f[G_SKIP] = f[G_FIN] || !f[G_NEED_OUTER];
 }
 
 // slot set-up: inverse diagonal (FP64 and FP32), zero x
@@ -480,9 +499,9 @@ struct Engine {
     dirty = false;
   }
 
-  void level(int ncol, int gate, int dst) {
+  void level(int ncol, int gate, int dst, int inv = 0) {
     const int warps = max_slots * ncol;
-    k_b_level<<<(warps + 7) / 8, 256, 0, cs>>>(part.ptr, nchunks, ncol, sd_dev.ptr, fl.ptr, gate, max_slots, o.lanes,
+    k_b_level<<<(warps + 7) / 8, 256, 0, cs>>>(part.ptr, nchunks, ncol, sd_dev.ptr, fl.ptr, gate, inv, max_slots, o.lanes,
                                                used_dev.ptr, sc.ptr, dst);
     FX_LAUNCH_CHECK("batch_level");
   }
@@ -524,73 +543,69 @@ struct Engine {
     dirty = true;
   }
 
-  bool any_inner_running() const {
-    for (int s = 0; s < max_slots; ++s)
-      if (slots[s].used && !fl_h[s * NFL + F_DONE]) return true;
-    return false;
-  }
 
-  // one refinement round of every running slot; returns the number of running slots it saw
+
+  // One tick (see the top of the file); returns the number of unfinished slots it saw. The host's
+  // copy of the flags is read at the end of every tick, so finished() sees the tick's outcome.
   int round() {
-    read_flags();
     int running = 0;
+    bool any_corr = false, any_outer = false;
     for (int s = 0; s < max_slots; ++s) {
-      if (!slots[s].used) continue;
-      const bool run = !fl_h[s * NFL + G_FIN];
-      running += run;
-      if (fl_h[s * NFL + G_SKIP] != !run) {
-        fl_h[s * NFL + G_SKIP] = !run;
-        FX_CUDA(cudaMemcpyAsync(fl.ptr + s * NFL + G_SKIP, fl_h + s * NFL + G_SKIP, sizeof(int),
-                                cudaMemcpyHostToDevice, cs));
-      }
+      if (!slots[s].used || fl_h[s * NFL + G_FIN]) continue;
+      ++running;
+      any_corr |= fl_h[s * NFL + F_DONE] && fl_h[s * NFL + G_INNER_RAN];
+      any_outer |= fl_h[s * NFL + G_NEED_OUTER] != 0;
     }
     if (!running) return 0;
     upload_tables();
     const unsigned g = chunk_grid(high);
-    // outer: r = b - K x (FP64), norms, test
-    box_batch_apply(false, inst64.ptr, work.ptr, nwork, persistent ? queue.ptr : nullptr, cs);
-    k_b_residual<<<g, 32 * kWarps, 0, cs>>>(b.ptr, ap.ptr, r.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
-                                            part.ptr, nchunks);
-    level(2, G_SKIP, O_RR);
-    k_b_outer<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, o.rtol, o.atol, max_outer,
-                                           o.max_iterations);
-    // inner: FP32 (or FP64) PCG from d = 0
-    if (inner64)
-      k_b_inner_begin<double><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r64.ptr, d64.ptr, rr64.ptr, p64.ptr, inv.ptr, high,
-                                                         chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
-    else
-      k_b_inner_begin<float><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r32.ptr, d32.ptr, rr32.ptr, p32.ptr, inv32.ptr, high,
-                                                        chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr, nchunks);
-    level(2, F_DONE, S_RR);
-    k_b_inner_start<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, inner_rtol);
-    FX_LAUNCH_CHECK("batch_outer");
-    // the first block of iterations directly, then graphs of 8
-    const int block = 8;
-    for (int i = 0; i < block; ++i) inner_iteration();
-    read_flags();
-    while (any_inner_running()) {
-      if (!graph) {
-        cudaGraph_t gr = nullptr;
-        FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        try {
-          for (int i = 0; i < block; ++i) inner_iteration();
-        } catch (...) {
-          cudaStreamEndCapture(cs, &gr);
-          if (gr) cudaGraphDestroy(gr);
-          throw;
-        }
-        FX_CUDA(cudaStreamEndCapture(cs, &gr));
-        const cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
-        cudaGraphDestroy(gr);
-        FX_CUDA(e);
-      }
-      FX_CUDA(cudaGraphLaunch(graph, cs));
-      read_flags();
+    if (any_corr) {  // the slots whose inner solve has ended: x += d, the round's counters
+      if (inner64)
+        k_b_correct<double><<<g, 32 * kWarps, 0, cs>>>(d64.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
+      else
+        k_b_correct<float><<<g, 32 * kWarps, 0, cs>>>(d32.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
+      k_b_round_end<<<slot_grid(), 128, 0, cs>>>(fl.ptr, used_dev.ptr, max_slots);
+      FX_LAUNCH_CHECK("batch_correct");
+      any_outer = true;
     }
-    if (inner64) k_b_correct<double><<<g, 32 * kWarps, 0, cs>>>(d64.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
-    else k_b_correct<float><<<g, 32 * kWarps, 0, cs>>>(d32.ptr, x.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr);
-    k_b_round_end<<<slot_grid(), 128, 0, cs>>>(fl.ptr, used_dev.ptr, max_slots);
-    FX_LAUNCH_CHECK("batch_correct");
+    if (any_outer) {  // the slots due for it: r = b - K x (FP64), norms, test, the inner solve's start
+      k_b_phase<<<slot_grid(), 128, 0, cs>>>(fl.ptr, used_dev.ptr, max_slots);
+      box_batch_apply(false, inst64.ptr, work.ptr, nwork, persistent ? queue.ptr : nullptr, cs);
+      k_b_residual<<<g, 32 * kWarps, 0, cs>>>(b.ptr, ap.ptr, r.ptr, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
+                                              part.ptr, nchunks);
+      level(2, G_SKIP, O_RR);
+      k_b_outer<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, o.rtol, o.atol, max_outer,
+                                             o.max_iterations);
+      if (inner64)
+        k_b_inner_begin<double><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r64.ptr, d64.ptr, rr64.ptr, p64.ptr, inv.ptr, high,
+                                                           chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr,
+                                                           nchunks);
+      else
+        k_b_inner_begin<float><<<g, 32 * kWarps, 0, cs>>>(r.ptr, r32.ptr, d32.ptr, rr32.ptr, p32.ptr, inv32.ptr, high,
+                                                          chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes, part.ptr,
+                                                          nchunks);
+      level(2, F_BEGIN, S_RR, 1);
+      k_b_inner_start<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots, inner_rtol);
+      FX_LAUNCH_CHECK("batch_outer");
+    }
+    // 8 inner iterations of every slot whose inner solve runs (a CUDA graph, kept until the work list changes)
+    const int block = 8;
+    if (!graph) {
+      cudaGraph_t gr = nullptr;
+      FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      try {
+        for (int i = 0; i < block; ++i) inner_iteration();
+      } catch (...) {
+        cudaStreamEndCapture(cs, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+      }
+      FX_CUDA(cudaStreamEndCapture(cs, &gr));
+      const cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
+      cudaGraphDestroy(gr);
+      FX_CUDA(e);
+    }
+    FX_CUDA(cudaGraphLaunch(graph, cs));
     read_flags();
     // slots that finished leave the work list
     for (int s = 0; s < max_slots; ++s)
@@ -652,6 +667,7 @@ struct Engine {
     }
     std::vector<int> f0(NFL, 0);
     f0[F_DONE] = 1;
+    f0[G_NEED_OUTER] = 1;
     std::vector<double> s0(NSC, 0.0);
     FX_CUDA(cudaMemcpyAsync(fl.ptr + slot * NFL, f0.data(), sizeof(int) * NFL, cudaMemcpyHostToDevice, cs));
     FX_CUDA(cudaMemcpyAsync(sc.ptr + slot * NSC, s0.data(), sizeof(double) * NSC, cudaMemcpyHostToDevice, cs));

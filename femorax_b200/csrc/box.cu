@@ -533,12 +533,13 @@ template <class T>
 void batch_launch(const void* inst, const int4* work, int nwork, int* queue, cudaStream_t st) {
   using S = Smem<kBatchBX, kBatchBY, T, 0, kPerSet>;
   auto kern = k_box_batch<kBatchBX, kBatchBY, T, 0, kBatchMinB<T>>;
-  static int resident = 0;  // CTAs per SM
-  if (!resident) {
+  // CTAs per SM (set once, thread-safe: serving threads launch this concurrently)
+  static const int resident = [&] {
+    int r = 0;
     FX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
-    FX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kBatchBX * kBatchBY, S::bytes));
-    resident = std::max(resident, 1);
-  }
+    FX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, kern, kBatchBX * kBatchBY, S::bytes));
+    return std::max(r, 1);
+  }();
   const int ctas = queue ? std::min(nwork, resident * num_sms()) : nwork;
   kern<<<ctas, kBatchBX * kBatchBY, S::bytes, st>>>(static_cast<const BoxArgs<T>*>(inst), work, nwork, queue);
   FX_LAUNCH_CHECK("box_batch");

@@ -599,17 +599,17 @@ template <int BX, int BY, int MINB, bool CACHE, int CM, bool FULL, class T, int 
 void launch_kernel(const BoxPlan& p, const BoxArgs<T>& a, cudaStream_t st) {
   using S = Smem<BX, BY, T, MODE, CM>;
   auto kern = k_box<BX, BY, T, MODE, MINB, CACHE, CM, FULL>;
-  static int resident = 0;  // CTAs per SM at this shape's registers and shared memory
-  if (!resident) {
-    int dev = 0, max_smem = 0;
+  // CTAs per SM at this shape's registers and shared memory (set once, thread-safe)
+  static const int resident = [&] {
+    int dev = 0, max_smem = 0, r = 0;
     FX_CUDA(cudaGetDevice(&dev));
     FX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (S::bytes > static_cast<size_t>(max_smem))
       throw Error(FX_E_UNSUPPORTED, "box launch shape: its staging needs more shared memory than a CTA can have");
     FX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes)));
-    FX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, BX * BY, S::bytes));
-    resident = std::max(resident, 1);
-  }
+    FX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, kern, BX * BY, S::bytes));
+    return std::max(r, 1);
+  }();
   dim3 grid((p.nx + 1 + BX - 2) / (BX - 1), (p.ny + 1 + BY - 2) / (BY - 1), (p.nz + 1 + a.kz - 1) / a.kz);
   if (a.tiles) {
     BoxArgs<T> b = a;

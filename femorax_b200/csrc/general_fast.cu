@@ -161,13 +161,18 @@ bool general_fast_applies(const ForceState& s) {
   return true;
 }
 
-void general_apply_fast(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
-  static bool attr = false;
-  if (!attr) {
+// the kernels' shared-memory limit, set once (thread-safe)
+void fast_attributes() {
+  static const bool once = [] {
     FX_CUDA(cudaFuncSetAttribute(k_apply_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(Stage)));
     FX_CUDA(cudaFuncSetAttribute(k_force_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(Stage)));
-    attr = true;
-  }
+    return true;
+  }();
+  (void)once;
+}
+
+void general_apply_fast(ForceState& s, const double k[3], const double* x, double* y, cudaStream_t st, const int* skip) {
+  fast_attributes();
   if (s.count > 0)
     k_apply_fast<<<fast_grid(s.count), kThreads, sizeof(Stage), st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                       s.params.ptr, s.N, s.P, s.count, k[0], k[1], k[2],
@@ -177,12 +182,7 @@ void general_apply_fast(ForceState& s, const double k[3], const double* x, doubl
 }
 
 void general_force_fast(ForceState& s, const double* u, const double* v, double* f, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    FX_CUDA(cudaFuncSetAttribute(k_apply_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(Stage)));
-    FX_CUDA(cudaFuncSetAttribute(k_force_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(Stage)));
-    attr = true;
-  }
+  fast_attributes();
   if (s.count > 0)
     k_force_fast<<<fast_grid(s.count), kThreads, sizeof(Stage), st>>>(s.coords.ptr, s.node.ptr, s.eq.ptr, s.param.ptr,
                                                                       s.params.ptr, s.N, s.P, s.count, u, v,

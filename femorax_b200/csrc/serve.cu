@@ -8,21 +8,23 @@
 //   - a request becomes visible at its arrival (real time) or at once;
 //   - static solves are admitted, in arrival order, into the batched engine (fx_engine_*) while
 //     the footprint of the admitted requests (their meshes' device bytes) fits the budget and the
-//     engine has a slot and a range of chunks; every pass of the loop runs one refinement round of
-//     every admitted solve (one batched launch per operator apply for all of them), so requests that
-//     arrive while others run join at the next round;
+//     engine has a slot and a range of chunks; the engine advances every admitted solve in ticks of 8
+//     inner iterations (one batched launch per operator apply for all of them; each solve in its own
+//     phase), so requests that arrive while others run join at the next tick;
 //   - J2 load paths run in cohorts on up to max_lanes lanes: while a lane is free, the waiting
 //     requests with the head's load path (in arrival order, up to max_cohort, while the footprint
 //     fits) become one batched Newton (fx_nbatch_*: one combined mesh, per-instance Newton and CG on
-//     the device) on it; every cohort advances one load step per pass of the loop, between the
-//     engine's rounds. A running cohort takes no new members (its combined mesh is fixed), so J2
-//     requests that arrive while it runs start the next cohort on another lane;
+//     the device) on it. A lane is a host thread with its own stream that steps its cohort through
+//     the load path, so the cohorts' launches and host waits overlap the engine's ticks (run by the
+//     loop's own thread) on the device. A running cohort takes no new members (its combined mesh is
+//     fixed), so J2 requests that arrive while it runs start the next cohort on another lane;
 //   - finished requests are retired and their results kept.
 // Each request's arithmetic is that of the request alone, so its result is bit for bit the same
 // alone and in any mix: a static solve as the engine's (the FX_SOLVER_IR solve of its mesh), a J2
 // path as fx_nbatch_step's (the single-mesh Newton path, tests/test_gpu_nbatch.py).
 // No counterpart in the reference, which runs one analysis per process.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -65,6 +67,9 @@ __global__ void k_pick(const double* __restrict__ u, const int64_t* __restrict__
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n) hist[j] = u[idx[j]];
 }
+
+// With no engine slot in use, the loop polls its lanes and the arrivals at this interval (seconds).
+constexpr double kPoll = 2e-4;
 
 void ck(int rc, const char* what) {
   if (rc != FX_OK) throw Error(rc, std::string(what) + ": " + fx_last_error());
@@ -116,6 +121,7 @@ int64_t j2_footprint(const fx_mesh& m) {
 
 struct Cohort {
   fx_nbatch* nb = nullptr;
+  cudaStream_t st = nullptr;
   std::vector<size_t> members;
   std::vector<double> factors;
   std::vector<int64_t> offsets, neq;
@@ -125,9 +131,29 @@ struct Cohort {
   std::vector<char> conv;
   std::vector<std::vector<int32_t>> newton;
   int64_t footprint = 0;
-  ~Cohort() {
+  // the batched Newton, its stream and device vectors (the lane's thread frees them when the path ends)
+  void release() {
     if (nb) fx_nbatch_destroy(nb);
+    nb = nullptr;
+    F.release();
+    fext.release();
+    u.release();
+    hist.release();
+    idx.release();
+    if (st) cudaStreamDestroy(st);
+    st = nullptr;
   }
+  ~Cohort() { release(); }
+};
+
+// A lane: the thread that steps one cohort through its load path. state 0 running, 1 done, 2 failed
+// (code and message kept for the loop's thread, which joins it).
+struct Lane {
+  std::unique_ptr<Cohort> c;
+  std::thread th;
+  std::atomic<int> state{0};
+  int code = FX_OK;
+  std::string err;
 };
 
 struct Server {
@@ -162,6 +188,7 @@ struct Server {
     o.atol = 0.0;
     o.max_iterations = head.cg_max_it;
     o.lanes = 32;
+    FX_CUDA(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
     ck(fx_nbatch_create(meshes.data(), static_cast<int32_t>(meshes.size()), device, o, &c.nb), "fx_nbatch_create");
     const size_t m = members.size();
     c.offsets.assign(m + 1, 0);
@@ -181,7 +208,7 @@ struct Server {
     c.F.upload(F);
     c.fext.alloc(static_cast<size_t>(total));
     c.u.alloc(static_cast<size_t>(total));
-    c.u.zero(nullptr);
+    c.u.zero(c.st);
     c.idx.upload(idx);
     c.hist.alloc(c.factors.size() * m);
     c.members = members;
@@ -198,16 +225,16 @@ struct Server {
     const size_t m = c.members.size();
     const int64_t total = c.offsets[m];
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 4096)));
-    k_scaled<<<grid, 256>>>(c.F.ptr, c.factors[c.k], c.fext.ptr, total);
+    k_scaled<<<grid, 256, 0, c.st>>>(c.F.ptr, c.factors[c.k], c.fext.ptr, total);
     FX_LAUNCH_CHECK("server_load");
     std::vector<int32_t> it(m);
     std::vector<fx_solve_result> res(m);
     const Request& head = reqs[c.members[0]];
-    ck(fx_nbatch_step(c.nb, c.fext.ptr, c.u.ptr, head.tol, head.max_newton, it.data(), res.data(), nullptr),
+    ck(fx_nbatch_step(c.nb, c.fext.ptr, c.u.ptr, head.tol, head.max_newton, it.data(), res.data(), c.st),
        "fx_nbatch_step");
-    ck(fx_force_commit(fx_nbatch_force(c.nb), nullptr), "fx_force_commit");
-    k_pick<<<static_cast<unsigned>((m + 127) / 128), 128>>>(c.u.ptr, c.idx.ptr, static_cast<int>(m),
-                                                           c.hist.ptr + static_cast<size_t>(c.k) * m);
+    ck(fx_force_commit(fx_nbatch_force(c.nb), c.st), "fx_force_commit");
+    k_pick<<<static_cast<unsigned>((m + 127) / 128), 128, 0, c.st>>>(c.u.ptr, c.idx.ptr, static_cast<int>(m),
+                                                                   c.hist.ptr + static_cast<size_t>(c.k) * m);
     FX_LAUNCH_CHECK("server_monitor");
     for (size_t i = 0; i < m; ++i) {
       c.conv[i] = c.conv[i] && res[i].converged;
@@ -215,8 +242,9 @@ struct Server {
     }
     if (++c.k < static_cast<int>(c.factors.size())) return false;
     std::vector<double> u(static_cast<size_t>(total)), hist(c.hist.n);
-    FX_CUDA(cudaMemcpy(u.data(), c.u.ptr, sizeof(double) * u.size(), cudaMemcpyDeviceToHost));
-    FX_CUDA(cudaMemcpy(hist.data(), c.hist.ptr, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost));
+    FX_CUDA(cudaMemcpyAsync(u.data(), c.u.ptr, sizeof(double) * u.size(), cudaMemcpyDeviceToHost, c.st));
+    FX_CUDA(cudaMemcpyAsync(hist.data(), c.hist.ptr, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, c.st));
+    FX_CUDA(cudaStreamSynchronize(c.st));
     now_out = now();
     for (size_t i = 0; i < m; ++i) {
       Request& r = reqs[c.members[i]];
@@ -233,7 +261,42 @@ struct Server {
     return true;
   }
 
+  // a lane's thread: the cohort's load steps until its path ends or the loop stops
+  void lane_main(Lane& L, const std::atomic<bool>& stop, const std::function<double()>& now) {
+    try {
+      FX_CUDA(cudaSetDevice(device));
+      double done_at = 0.0;
+      while (!stop.load(std::memory_order_relaxed) && !step_cohort(*L.c, done_at, now)) {
+      }
+      L.c->release();
+      L.state.store(1);
+    } catch (const Error& e) {
+      L.code = e.code;
+      L.err = e.what();
+      L.state.store(2);
+    } catch (const std::exception& e) {
+      L.code = FX_E_INVALID;
+      L.err = e.what();
+      L.state.store(2);
+    }
+  }
+
   double run(bool realtime) {
+    std::vector<std::unique_ptr<Lane>> lanes;
+    std::atomic<bool> stop{false};
+    try {
+      const double t = serve(realtime, lanes, stop);
+      ran = true;
+      return t;
+    } catch (...) {
+      stop.store(true);
+      for (auto& L : lanes)
+        if (L->th.joinable()) L->th.join();
+      throw;
+    }
+  }
+
+  double serve(bool realtime, std::vector<std::unique_ptr<Lane>>& lanes, std::atomic<bool>& stop) {
     using clock = std::chrono::steady_clock;
     FX_CUDA(cudaSetDevice(device));
     std::vector<size_t> order(reqs.size());
@@ -241,9 +304,9 @@ struct Server {
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return reqs[a].arrival < reqs[b].arrival; });
     const auto t0 = clock::now();
     auto now = [&]() { return std::chrono::duration<double>(clock::now() - t0).count(); };
+    const std::function<double()> now_fn = now;
     std::deque<size_t> pending, pending_j2;
     std::map<int32_t, size_t> slots;
-    std::vector<std::unique_ptr<Cohort>> lanes;
     int64_t resident = 0;
     size_t nxt = 0;
     while (nxt < order.size() || !pending.empty() || !pending_j2.empty() || !slots.empty() || !lanes.empty()) {
@@ -268,53 +331,59 @@ struct Server {
       if (slots.empty() && lanes.empty() && !pending.empty())
         throw Error(FX_E_NOMEM, "fx_server: request " + std::to_string(reqs[pending.front()].id) +
                                     " does not fit the engine even alone");
+      // lanes whose path has ended: joined, their footprint released
+      for (auto it = lanes.begin(); it != lanes.end();) {
+        Lane& L = **it;
+        const int st = L.state.load();
+        if (st == 0) {
+          ++it;
+          continue;
+        }
+        L.th.join();
+        if (st == 2) throw Error(L.code, L.err);
+        resident -= L.c->footprint;
+        it = lanes.erase(it);
+      }
       while (static_cast<int>(lanes.size()) < max_lanes && !pending_j2.empty()) {
-        auto c = std::make_unique<Cohort>();
-        start_cohort(pending_j2, *c, resident, !slots.empty() || !lanes.empty(), now());
-        if (c->members.empty()) {
+        auto L = std::make_unique<Lane>();
+        L->c = std::make_unique<Cohort>();
+        start_cohort(pending_j2, *L->c, resident, !slots.empty() || !lanes.empty(), now());
+        if (L->c->members.empty()) {
           if (slots.empty() && lanes.empty())
             throw Error(FX_E_NOMEM, "fx_server: J2 request " + std::to_string(reqs[pending_j2.front()].id) +
                                         " does not fit the budget even alone");
           break;
         }
-        lanes.push_back(std::move(c));
+        Lane* lp = L.get();
+        lanes.push_back(std::move(L));
+        lp->th = std::thread([this, lp, &stop, &now_fn]() { lane_main(*lp, stop, now_fn); });
       }
-      if (slots.empty() && lanes.empty()) {
-        if (nxt < order.size() && realtime) {
-          const double wait = std::min(0.01, reqs[order[nxt]].arrival - now());
-          if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
-        }
+      if (slots.empty()) {
+        // nothing for this thread to advance: wait for an arrival or a lane's end
+        double wait = lanes.empty() ? 0.01 : kPoll;
+        if (nxt < order.size() && realtime) wait = std::min(wait, reqs[order[nxt]].arrival - now());
+        else if (lanes.empty()) continue;
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
         continue;
       }
-      if (!slots.empty()) {
-        int32_t running = 0;
-        ck(fx_engine_round(engine, &running), "fx_engine_round");
-        for (auto it = slots.begin(); it != slots.end();) {
-          int32_t fin = 0;
-          ck(fx_engine_finished(engine, it->first, &fin), "fx_engine_finished");
-          if (!fin) {
-            ++it;
-            continue;
-          }
-          Request& r = reqs[it->second];
-          r.x.assign(static_cast<size_t>(r.n), 0.0);
-          ck(fx_engine_retire(engine, it->first, r.x.data(), &r.res), "fx_engine_retire");
-          r.done = now();
-          resident -= r.footprint;
-          it = slots.erase(it);
-        }
-      }
-      for (auto it = lanes.begin(); it != lanes.end();) {
-        double done_at = 0.0;
-        if (step_cohort(**it, done_at, now)) {
-          resident -= (*it)->footprint;
-          it = lanes.erase(it);
-        } else {
+      // one engine tick (8 inner iterations; admissions and arrivals are looked at between ticks)
+      int32_t running = 0;
+      ck(fx_engine_round(engine, &running), "fx_engine_round");
+      for (auto it = slots.begin(); it != slots.end();) {
+        int32_t fin = 0;
+        ck(fx_engine_finished(engine, it->first, &fin), "fx_engine_finished");
+        if (!fin) {
           ++it;
+          continue;
         }
+        Request& r = reqs[it->second];
+        r.x.assign(static_cast<size_t>(r.n), 0.0);
+        ck(fx_engine_retire(engine, it->first, r.x.data(), &r.res), "fx_engine_retire");
+        r.done = now();
+        resident -= r.footprint;
+        it = slots.erase(it);
       }
     }
-    ran = true;
     return now();
   }
 };

@@ -7,9 +7,10 @@ or a quasi-static J2 load path (`J2Request`). For the static solves the loop
     this allocates) on a pool of host threads, in arrival order;
   - admits prepared requests, in arrival order, into the engine while their HBM footprint (the
     mesh's device bytes) fits the budget and the engine has a free slot and range;
-  - advances every admitted solve by one refinement round per pass (one batched launch per
-    operator apply for all of them), so requests that arrive while others run join at the next
-    round and their work overlaps on the device;
+  - advances every admitted solve in ticks of 8 inner iterations (one batched launch per operator
+    apply for all of them, each solve in its own phase: outer FP64 residual, inner solve,
+    correction), so requests that arrive while others run join at the next tick and their work
+    overlaps on the device;
   - retires finished solves, frees their footprint, and records the latency from arrival to the
     solution on the host.
 Each slot's arithmetic does not depend on the others, so a request's solution is bit for bit the
@@ -18,7 +19,8 @@ same alone and in any mix (tests/test_gpu_batch.py checks it).
 J2 load paths run in cohorts: when the J2 lane is idle, the prepared J2 requests waiting (in
 arrival order, up to `max_cohort`, the same load path) become one BatchedNewton (one combined
 mesh, per-instance Newton and CG on the device), which advances one load step per pass of the
-loop, between the engine's rounds, and retires all its requests at the end of the path. A cohort
+loop, after engine ticks that take as long as its last step did, and retires all its requests at
+the end of the path (NativeServer runs each cohort on a thread of its own instead). A cohort
 takes no members once it runs, so while the engine is busy an idle lane waits (at most
 `cohort_window` seconds) for the requests queued behind a prepared head to be prepared too. Each
 instance's arithmetic is that of the load path alone, bit for bit (tests/test_gpu_serving.py).
@@ -323,6 +325,9 @@ class Server:
         # a running cohort takes no new members, so an idle lane waits up to this many seconds for
         # the J2 requests queued behind a prepared head (same load path) while the engine is busy
         self.cohort_window = float(cohort_window)
+        # while a J2 cohort runs, a pass runs engine ticks (8 inner iterations each) for at least this
+        # many seconds (and as long as the cohort's last load step took) before its next load step
+        self.tick_budget = 0.02
         self.resident = 0  # footprint of the admitted requests
 
     def _start_cohort(self, pending_j2, slots, t0):
@@ -359,6 +364,7 @@ class Server:
         served = []
         nxt = 0
         head_ready = None  # when the J2 queue's head was first seen prepared with the lane idle
+        lane_s = 0.0  # seconds the lane's last load step took
         try:
             while nxt < len(reqs) or pending or pending_j2 or slots or not self.lane.idle:
                 # arrivals
@@ -405,16 +411,25 @@ class Server:
                         time.sleep(max(0.0, min(0.01, reqs[nxt].arrival - now())))
                     continue
                 if slots:
-                    self.engine.round()
-                    for slot in list(slots):
-                        if self.engine.finished(slot):
-                            req, foot, adm = slots.pop(slot)
-                            x, res = self.engine.retire(slot)
-                            self.resident -= foot
-                            done = time.perf_counter() - t0
-                            served.append(Served(req.id, x, res, req.arrival if realtime else 0.0, adm, done))
+                    # engine ticks: one per pass with the J2 lane idle, else for as long as the lane's
+                    # last load step took (at least tick_budget seconds): the two share the time
+                    until = time.perf_counter() + (0.0 if self.lane.idle else max(self.tick_budget, lane_s))
+                    while True:
+                        self.engine.round()
+                        for slot in list(slots):
+                            if self.engine.finished(slot):
+                                req, foot, adm = slots.pop(slot)
+                                x, res = self.engine.retire(slot)
+                                self.resident -= foot
+                                done = time.perf_counter() - t0
+                                served.append(Served(req.id, x, res, req.arrival if realtime else 0.0, adm, done))
+                        if not slots or time.perf_counter() >= until:
+                            break
                 if not self.lane.idle:
-                    for req, foot, adm, u, res in self.lane.step():
+                    t_lane = time.perf_counter()
+                    finished = self.lane.step()
+                    lane_s = time.perf_counter() - t_lane
+                    for req, foot, adm, u, res in finished:
                         self.resident -= foot
                         done = time.perf_counter() - t0
                         served.append(Served(req.id, u, res, req.arrival if realtime else 0.0, adm, done))
@@ -425,9 +440,10 @@ class Server:
 
 class NativeServer:
     """The serving loop in C++ (fx_server_*, serve.cu) over one BatchEngine: the same admission by
-    footprint, engine rounds for the static solves and J2 cohorts (up to max_cohort, fx_nbatch) as
-    Server, with up to max_lanes cohorts running at once (J2 requests that arrive while one runs
-    start the next), the loop, the arrival gating and the clock in the library; latency is measured by
+    footprint, engine ticks for the static solves and J2 cohorts (up to max_cohort, fx_nbatch) as
+    Server, with up to max_lanes cohorts running at once, each on a thread and a stream of its own
+    that overlap the engine's work on the device (J2 requests that arrive while one runs start the
+    next), the loop, the arrival gating and the clock in the library; latency is measured by
     the host's steady clock inside it. run() takes the requests with their prepared state
     (prepare_fn(request, device) as for Server: (force, b, n) for a static solve, prepare_j2's
     (mesh, unit load, monitored equation, n) for a J2 path) and returns (served, wall seconds)."""

@@ -514,8 +514,11 @@ int fx_math_eval_host(int32_t fn, const double* x, const double* y, double* out,
  *                      right-hand side (host, num_equations doubles) into a free slot: copies
  *                      b, builds the Jacobi diagonal, x = 0. FX_E_NOMEM when no slot or no
  *                      contiguous range of chunks is free (admit again after a retire).
- *   fx_engine_round    one refinement round of every running slot (FP64 residual and test,
- *                      FP32 inner solve, FP64 correction); *running = the slots it advanced.
+ *   fx_engine_round    one tick: the slots whose inner solve has ended get their FP64
+ *                      correction, those due get their outer step (FP64 residual and test, the
+ *                      inner solve's start), then every running inner solve 8 iterations; each
+ *                      slot in its own phase (no slot waits for another's inner solve);
+ *                      *running = the unfinished slots it advanced.
  *   fx_engine_finished whether a slot's solve has ended (converged or given up).
  *   fx_engine_retire   copies x (host, may be NULL) and the result out and frees the slot.
  *   fx_engine_info     info[6] = capacity (equations), equations in use, max slots, slots in
@@ -544,17 +547,19 @@ int fx_engine_info(const fx_engine* e, int64_t* info);
 /* ------------------------------------------------------------------ the serving loop
  * Requests arriving over time, served on one device with continuous batching (serve.cu): static
  * solves K x = b on resident fx_force meshes (several requests may share one) through an engine
- * (fx_engine_*), and quasi-static J2 load paths on compiled meshes in cohorts (fx_nbatch_*) between
- * the engine's rounds. Prepared requests are added with their arrival time (seconds from the start);
+ * (fx_engine_*), and quasi-static J2 load paths on compiled meshes in cohorts (fx_nbatch_*) beside
+ * the engine. Prepared requests are added with their arrival time (seconds from the start);
  * fx_server_run serves them once: in arrival order (in real time, or all visible at once), static
  * solves admitted while the footprint of the admitted requests (mesh device bytes; a J2 instance's
- * estimate) fits hbm_budget and the engine has room; one engine round and one J2 load step per pass.
+ * estimate) fits hbm_budget and the engine has room; one engine tick per pass of the calling
+ * thread's loop, each J2 cohort stepped through its path by a thread of its own on its own stream
+ * (the cohorts' work overlaps the engine's on the device).
  *   fx_server_add_j2   mesh (fx_compiled_mesh; its arrays must live until the run ends), the load at
  *                      factor 1 (host, num_equations), the monitored equation, the load path (cycles
  *                      of steps_per_cycle steps, 0 -> 1 -> -1 -> 0), Newton ||r|| <= tol in at most
  *                      max_newton solves, CG (Jacobi) to cg_rtol in at most cg_max_iterations;
  *                      requests with the same path and settings share a cohort (up to max_cohort);
- *                      up to max_lanes cohorts run at once (one step each per pass), so J2 requests
+ *                      up to max_lanes cohorts run at once (a thread each), so J2 requests
  *                      arriving while a cohort runs start the next one.
  *   fx_server_result   x (num_equations), the result, times[3] = arrival, admitted, done (seconds
  *                      from the start of the run, steady clock); J2: the monitored displacement and
