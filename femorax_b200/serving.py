@@ -602,6 +602,11 @@ def serve_one_at_a_time(requests, rtol: float = 1e-8, realtime: bool = True, dev
 
 def summary(served, wall):
     lat = [s.latency for s in served]
-    return {"solves": len(served), "solves_per_s": len(served) / wall if wall > 0 else float("nan"),
-            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99),
-            "converged": int(sum(s.result.converged for s in served)), "wall_s": wall}
+    out = {"solves": len(served), "solves_per_s": len(served) / wall if wall > 0 else float("nan"),
+           "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99),
+           "converged": int(sum(s.result.converged for s in served)), "wall_s": wall}
+    j2 = [s.latency for s in served if isinstance(s.result, J2Result)]
+    if j2:  # the J2 load paths' latencies apart (a path is many solves)
+        out["j2_p50_s"] = percentile(j2, 50)
+        out["j2_p99_s"] = percentile(j2, 99)
+    return out
