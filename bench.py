@@ -789,7 +789,8 @@ def served_streams(device, count=1000, rates=((10.0, 40), (100.0, 400), (500.0, 
         rep = {}
         for name, (served, wall) in runs.items():
             m = serving.summary(served, wall)
-            rep[name] = {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged", "wall_s")}
+            rep[name] = {k: m[k] for k in ("solves_per_s", "p50_s", "p99_s", "converged", "wall_s", "j2_p50_s",
+                                           "j2_p99_s") if k in m}
         plain = rep["plain_fp64_one_at_a_time"]["solves_per_s"]
         for name in engines:
             rep[name]["speedup_solves_per_s"] = rep[name]["solves_per_s"] / plain if plain else None

@@ -66,29 +66,35 @@ __device__ __forceinline__ int slot_of_chunk(const int* chunk_slot, int64_t c) {
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 
-// chunk sums of x.y (T accumulated in double, fused multiply-adds, lane order) of the chunks of
-// slots whose flag `gate` is 0; column `col` of part
-template <class T>
-__global__ void __launch_bounds__(32 * kWarps)
-    k_b_dot(const T* __restrict__ x, const T* __restrict__ y, int64_t nchunks, const int* __restrict__ chunk_slot,
-            const SlotDev* __restrict__ sd, const int* __restrict__ fl, int gate, int lanes, double* __restrict__ part) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = slot_of_chunk(chunk_slot, c);
-  if (s < 0 || fl[s * NFL + gate]) return;
-  const int64_t begin = c * kChunk;
-  const int64_t end = sd[s].off + sd[s].n;
-  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+// Called by every lane of the warp whose lane 0 has just written chunk sums of a slot: true (in
+// all lanes) in the warp that counted the slot's last chunk, which then sees every chunk sum of the
+// slot and resets the slot's counter for the next launch.
+__device__ __forceinline__ bool slot_last(unsigned* cnt, int64_t nc, int lane) {
+  unsigned t = 0;
+  if (lane == 0) {
+    __threadfence();
+    t = atomicAdd(cnt, 1u);
+  }
+  t = __shfl_sync(0xffffffffu, t, 0);
+  const bool last = t == static_cast<unsigned>(nc - 1);
+  if (last) {
+    if (lane == 0) *cnt = 0u;
+    __threadfence();
+  }
+  return last;
+}
+
+// The second level of one slot's column j of chunk sums (k_b_level's order), by one warp, the
+// chunk sums read through L2 (other warps of the launch wrote them); the sum in every lane.
+__device__ __forceinline__ double slot_level(const double* part, int64_t ld, int j, const SlotDev& sd, int lanes,
+                                             int lane) {
+  const double* p = part + static_cast<int64_t>(j) * ld + sd.c0;
   double acc = 0.0;
   if (lane < lanes)
-    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{x[i], y[i]}}; },
-                 [&](int64_t, const Ops<T, 2>& o) {
-                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
-                 });
+    for (int64_t k = lane; k < sd.nc; k += lanes) acc += __ldcg(p + k);
   double total = 0.0;
-  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
-  if (lane == 0) part[c] = total;
+  for (int l = 0; l < lanes; ++l) total += __shfl_sync(0xffffffffu, acc, l);
+  return total;
 }
 
 // second level: slot s's `ncol` columns of chunk sums (column j at part + j * nchunks) into
@@ -246,28 +252,56 @@ __global__ void k_b_inner_start(double* sc, int* fl, const int* used, int nslots
   f[F_DONE] = f[F_CONV] || f[F_MAXIT] <= 0;
 }
 
-__global__ void k_b_alpha(double* sc, int* fl, const int* used, int nslots) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nslots || !used[s]) return;
-  int* f = fl + s * NFL;
-  double* c = sc + s * NSC;
-  if (f[F_DONE]) return;
-  const double pap = c[S_PAP];
-  if (!(pap > 0.0)) {
-    f[F_INDEF] = 1;
-    f[F_DONE] = 1;
-    return;
-  }
-  c[S_ALPHA] = c[S_RZ] / pap;
-}
-
-// d += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (column 1 at part + ld)
+// An inner iteration's p.ap: chunk sums of the running slots (T accumulated in double, fused
+// multiply-adds, lane order), then in the warp that counts a slot's last chunk its second level
+// and ConjugateGradient's alpha step (p.ap <= 0: indefinite, the inner solve ends).
 template <class TI>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_b_update(const double* __restrict__ sc, const int* __restrict__ fl, const TI* __restrict__ p,
+    k_b_pap(const TI* __restrict__ p, const TI* __restrict__ ap, int64_t nchunks, int64_t ld,
+            const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, int* __restrict__ fl, int lanes,
+            double* __restrict__ part, double* __restrict__ sc, unsigned* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = slot_of_chunk(chunk_slot, c);
+  if (s < 0 || fl[s * NFL + F_DONE]) return;
+  const int64_t begin = c * kChunk;
+  const int64_t end = sd[s].off + sd[s].n;
+  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+  double acc = 0.0;
+  if (lane < lanes)
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<TI, 2>{{p[i], ap[i]}}; },
+                 [&](int64_t, const Ops<TI, 2>& o) {
+                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
+                 });
+  double total = 0.0;
+  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  if (lane == 0) part[c] = total;
+  if (!slot_last(cnt + s, sd[s].nc, lane)) return;
+  const double pap = slot_level(part, ld, 0, sd[s], lanes, lane);
+  if (lane == 0) {
+    int* f = fl + s * NFL;
+    double* cs = sc + s * NSC;
+    cs[S_PAP] = pap;
+    if (!(pap > 0.0)) {
+      f[F_INDEF] = 1;
+      f[F_DONE] = 1;
+    } else {
+      cs[S_ALPHA] = cs[S_RZ] / pap;
+    }
+  }
+}
+
+// d += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (column 1 at part + ld); then in the
+// warp that counts a slot's last chunk the two second levels and the iteration's end
+// (ConjugateGradient's test on ||rr||, the iteration limit, beta)
+template <class TI>
+__global__ void __launch_bounds__(32 * kWarps)
+    k_b_update(double* __restrict__ sc, int* __restrict__ fl, const TI* __restrict__ p,
                const TI* __restrict__ ap, const TI* __restrict__ inv, TI* __restrict__ d,
                TI* __restrict__ rr, int64_t nchunks, const int* __restrict__ chunk_slot,
-               const SlotDev* __restrict__ sd, int lanes, double* __restrict__ part, int64_t ld) {
+               const SlotDev* __restrict__ sd, int lanes, double* __restrict__ part, int64_t ld,
+               unsigned* __restrict__ cnt) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
@@ -297,18 +331,18 @@ __global__ void __launch_bounds__(32 * kWarps)
     part[c] = trr;
     part[ld + c] = trz;
   }
-}
-
-__global__ void k_b_beta(double* sc, int* fl, const int* used, int nslots) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nslots || !used[s]) return;
+  if (!slot_last(cnt + s, sd[s].nc, lane)) return;
+  const double srr_all = slot_level(part, ld, 0, sd[s], lanes, lane);
+  const double srz_all = slot_level(part, ld, 1, sd[s], lanes, lane);
+  if (lane != 0) return;
   int* f = fl + s * NFL;
-  double* c = sc + s * NSC;
-  if (f[F_DONE]) return;
-  const double rn = sqrt(c[S_RR]);
-  c[S_RNORM] = rn;
+  double* cs = sc + s * NSC;
+  cs[S_RR] = srr_all;
+  cs[S_RZNEW] = srz_all;
+  const double rn = sqrt(cs[S_RR]);
+  cs[S_RNORM] = rn;
   const int it = ++f[F_ITERS];
-  if (rn <= c[S_TOL]) {
+  if (rn <= cs[S_TOL]) {
     f[F_CONV] = 1;
     f[F_DONE] = 1;
     return;
@@ -317,8 +351,8 @@ __global__ void k_b_beta(double* sc, int* fl, const int* used, int nslots) {
     f[F_DONE] = 1;
     return;
   }
-  c[S_BETA] = c[S_RZNEW] / c[S_RZ];
-  c[S_RZ] = c[S_RZNEW];
+  cs[S_BETA] = cs[S_RZNEW] / cs[S_RZ];
+  cs[S_RZ] = cs[S_RZNEW];
 }
 
 // p = inv rr + beta p (the beta of a slot that finished this iteration is stale: its p is
@@ -416,6 +450,7 @@ struct Engine {
   DeviceArray<double> part;  // [2][nchunks]
   DeviceArray<double> sc;
   DeviceArray<int> fl, used_dev, zeros;
+  DeviceArray<unsigned> cnt;  // per slot: chunks counted by the fused reductions (0 between launches)
   DeviceArray<SlotDev> sd_dev;
   DeviceArray<unsigned char> inst64, inst32;  // descriptors per slot
   DeviceArray<unsigned char> inst64i;         // FP64 inner solves: the inner apply's descriptors
@@ -511,13 +546,10 @@ struct Engine {
   void inner_iteration_t(const unsigned char* inst, TI* p, TI* ap, const TI* iv, TI* d, TI* rr) {
     const unsigned g = chunk_grid(high);
     box_batch_apply(sizeof(TI) == 4, inst, work.ptr, nwork, persistent ? queue.ptr : nullptr, cs);
-    k_b_dot<TI><<<g, 32 * kWarps, 0, cs>>>(p, ap, high, chunk_slot.ptr, sd_dev.ptr, fl.ptr, F_DONE, o.lanes, part.ptr);
-    level(1, F_DONE, S_PAP);
-    k_b_alpha<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots);
+    k_b_pap<TI><<<g, 32 * kWarps, 0, cs>>>(p, ap, high, nchunks, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
+                                           part.ptr, sc.ptr, cnt.ptr);
     k_b_update<TI><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p, ap, iv, d, rr, high, chunk_slot.ptr, sd_dev.ptr,
-                                              o.lanes, part.ptr, nchunks);
-    level(2, F_DONE, S_RR);
-    k_b_beta<<<slot_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, used_dev.ptr, max_slots);
+                                              o.lanes, part.ptr, nchunks, cnt.ptr);
     k_b_p<TI><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, p, high, chunk_slot.ptr, sd_dev.ptr);
     FX_LAUNCH_CHECK("batch_inner");
   }
@@ -763,6 +795,8 @@ int fx_engine_create(int32_t device, int64_t capacity, int32_t max_slots, fx_coe
       e.sc.alloc(static_cast<size_t>(max_slots) * fx::NSC);
       e.fl.alloc(static_cast<size_t>(max_slots) * fx::NFL);
       e.used_dev.alloc(static_cast<size_t>(max_slots));
+      e.cnt.alloc(static_cast<size_t>(max_slots));
+      FX_CUDA(cudaMemset(e.cnt.ptr, 0, sizeof(unsigned) * max_slots));
       e.zeros.alloc(1);
       e.sd_dev.alloc(static_cast<size_t>(max_slots));
       e.a64 = fx::box_args_bytes(false);

@@ -282,10 +282,14 @@ struct Server {
   }
 
   double run(bool realtime) {
+    // the clock, the lanes and the stop flag outlive every lane thread (joined here on an error)
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
+    const std::function<double()> now = [t0]() { return std::chrono::duration<double>(clock::now() - t0).count(); };
     std::vector<std::unique_ptr<Lane>> lanes;
     std::atomic<bool> stop{false};
     try {
-      const double t = serve(realtime, lanes, stop);
+      const double t = serve(realtime, now, lanes, stop);
       ran = true;
       return t;
     } catch (...) {
@@ -296,15 +300,12 @@ struct Server {
     }
   }
 
-  double serve(bool realtime, std::vector<std::unique_ptr<Lane>>& lanes, std::atomic<bool>& stop) {
-    using clock = std::chrono::steady_clock;
+  double serve(bool realtime, const std::function<double()>& now, std::vector<std::unique_ptr<Lane>>& lanes,
+               std::atomic<bool>& stop) {
     FX_CUDA(cudaSetDevice(device));
     std::vector<size_t> order(reqs.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return reqs[a].arrival < reqs[b].arrival; });
-    const auto t0 = clock::now();
-    auto now = [&]() { return std::chrono::duration<double>(clock::now() - t0).count(); };
-    const std::function<double()> now_fn = now;
     std::deque<size_t> pending, pending_j2;
     std::map<int32_t, size_t> slots;
     int64_t resident = 0;
@@ -356,7 +357,7 @@ struct Server {
         }
         Lane* lp = L.get();
         lanes.push_back(std::move(L));
-        lp->th = std::thread([this, lp, &stop, &now_fn]() { lane_main(*lp, stop, now_fn); });
+        lp->th = std::thread([this, lp, &stop, &now]() { lane_main(*lp, stop, now); });
       }
       if (slots.empty()) {
         // nothing for this thread to advance: wait for an arrival or a lane's end
