@@ -1,7 +1,8 @@
 // Batched quasi-static Newton on many independent meshes (the batched J2 configuration): the
 // meshes are concatenated into one mesh whose element kernels and gather run every instance in
 // one launch each, and each instance keeps its own Newton test and its own Jacobi-PCG recurrence
-// on the device (scalars and stopping flags per instance; CG iterations as CUDA graphs).
+// on the device (scalars and stopping flags per instance; each CG loop one CUDA graph with a
+// device-side while node).
 //
 // Instance s owns the equations [off_s, off_s + n_s) of the combined numbering, off_s a multiple
 // of the 2048-entry reduction chunk; its elements keep their order, so every equation's gather
@@ -51,6 +52,37 @@ struct Range {
 __device__ __forceinline__ int64_t chunk_len(const Range& r, int64_t begin) {
   const int64_t end = r.off + r.n;
   return (end - begin < kChunk) ? end - begin : kChunk;
+}
+
+// Called by every lane of the warp whose lane 0 has just written chunk sums of an instance: true
+// (in all lanes) in the warp that counted the instance's last chunk, which then sees every chunk
+// sum of the instance and resets its counter for the next launch.
+__device__ __forceinline__ bool instance_last(unsigned* cnt, int64_t nc, int lane) {
+  unsigned t = 0;
+  if (lane == 0) {
+    __threadfence();
+    t = atomicAdd(cnt, 1u);
+  }
+  t = __shfl_sync(0xffffffffu, t, 0);
+  const bool last = t == static_cast<unsigned>(nc - 1);
+  if (last) {
+    if (lane == 0) *cnt = 0u;
+    __threadfence();
+  }
+  return last;
+}
+
+// The second level of one instance's column j of chunk sums (k_nb_level's order), by one warp, the
+// chunk sums read through L2 (other warps of the launch wrote them); the sum in every lane.
+__device__ __forceinline__ double instance_level(const double* part, int64_t ld, int j, const Range& r, int lanes,
+                                                 int lane) {
+  const double* p = part + static_cast<int64_t>(j) * ld + r.c0;
+  double acc = 0.0;
+  if (lane < lanes)
+    for (int64_t k = lane; k < r.nc; k += lanes) acc += __ldcg(p + k);
+  double total = 0.0;
+  for (int l = 0; l < lanes; ++l) total += __shfl_sync(0xffffffffu, acc, l);
+  return total;
 }
 
 // chunk sums of x.y over the chunks of instances whose flag `gate` is 0 (column 0 of part)
@@ -190,28 +222,53 @@ __global__ void k_nb_cg_start(double* sc, int* fl, int count, double rtol, doubl
   f[G_CG_DONE] = f[G_CG_CONV] || max_it <= 0;
 }
 
-__global__ void k_nb_alpha(double* sc, int* fl, int count) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= count) return;
-  int* f = fl + s * NNF;
-  double* c = sc + s * NNS;
-  if (f[G_CG_DONE]) return;
-  const double pap = c[N_PAP];
-  if (!(pap > 0.0)) {
-    f[G_INDEF] = 1;
-    f[G_CG_DONE] = 1;
-    return;
-  }
-  c[N_ALPHA] = c[N_RZ] / pap;
-}
-
-// du += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (vectors of type T, sums in double)
+// A CG iteration's p.ap: chunk sums of the instances still solving (T accumulated in double, fused
+// multiply-adds, lane order), then in the warp that counts an instance's last chunk its second
+// level and ConjugateGradient's alpha step (p.ap <= 0: indefinite, the solve ends).
 template <class T>
 __global__ void __launch_bounds__(32 * kWarps)
-    k_nb_update(const double* __restrict__ sc, const int* __restrict__ fl, const T* __restrict__ p,
+    k_nb_pap(const T* __restrict__ p, const T* __restrict__ ap, int64_t nchunks, const int* __restrict__ owner,
+             const Range* __restrict__ rg, int* __restrict__ fl, int lanes, double* __restrict__ part,
+             double* __restrict__ sc, unsigned* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  if (c >= nchunks) return;
+  const int s = owner[c];
+  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+  double acc = 0.0;
+  if (lane < lanes)
+    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{p[i], ap[i]}}; },
+                 [&](int64_t, const Ops<T, 2>& o) {
+                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
+                 });
+  double total = 0.0;
+  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  if (lane == 0) part[c] = total;
+  if (!instance_last(cnt + s, rg[s].nc, lane)) return;
+  const double pap = instance_level(part, nchunks, 0, rg[s], lanes, lane);
+  if (lane == 0) {
+    int* f = fl + s * NNF;
+    double* cs = sc + s * NNS;
+    cs[N_PAP] = pap;
+    if (!(pap > 0.0)) {
+      f[G_INDEF] = 1;
+      f[G_CG_DONE] = 1;
+    } else {
+      cs[N_ALPHA] = cs[N_RZ] / pap;
+    }
+  }
+}
+
+// du += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (vectors of type T, sums in double);
+// then in the warp that counts an instance's last chunk the two second levels and the iteration's
+// end (ConjugateGradient's test on ||rr||, the iteration limit, beta)
+template <class T>
+__global__ void __launch_bounds__(32 * kWarps)
+    k_nb_update(double* __restrict__ sc, int* __restrict__ fl, const T* __restrict__ p,
                 const T* __restrict__ ap, const T* __restrict__ inv, T* __restrict__ du, T* __restrict__ rr,
                 int64_t nchunks, const int* __restrict__ owner, const Range* __restrict__ rg, int lanes,
-                double* __restrict__ part, int64_t ld) {
+                double* __restrict__ part, int64_t ld, unsigned* __restrict__ cnt) {
   const int lane = threadIdx.x & 31;
   const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
   if (c >= nchunks) return;
@@ -239,18 +296,18 @@ __global__ void __launch_bounds__(32 * kWarps)
     part[c] = trr;
     part[ld + c] = trz;
   }
-}
-
-__global__ void k_nb_beta(double* sc, int* fl, int count) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= count) return;
+  if (!instance_last(cnt + s, rg[s].nc, lane)) return;
+  const double srr_all = instance_level(part, ld, 0, rg[s], lanes, lane);
+  const double srz_all = instance_level(part, ld, 1, rg[s], lanes, lane);
+  if (lane != 0) return;
   int* f = fl + s * NNF;
-  double* c = sc + s * NNS;
-  if (f[G_CG_DONE]) return;
+  double* cs = sc + s * NNS;
+  cs[N_RR] = srr_all;
+  cs[N_RZNEW] = srz_all;
   const int max_it = f[G_CG_MAXIT];
-  const double rn = sqrt(c[N_RR]);
+  const double rn = sqrt(cs[N_RR]);
   const int it = ++f[G_CG_ITERS];
-  if (rn <= c[N_TOL]) {
+  if (rn <= cs[N_TOL]) {
     f[G_CG_CONV] = 1;
     f[G_CG_DONE] = 1;
     return;
@@ -259,8 +316,8 @@ __global__ void k_nb_beta(double* sc, int* fl, int count) {
     f[G_CG_DONE] = 1;
     return;
   }
-  c[N_BETA] = c[N_RZNEW] / c[N_RZ];
-  c[N_RZ] = c[N_RZNEW];
+  cs[N_BETA] = cs[N_RZNEW] / cs[N_RZ];
+  cs[N_RZ] = cs[N_RZNEW];
 }
 
 // p = inv rr + beta p
@@ -384,6 +441,18 @@ __global__ void __launch_bounds__(32 * kWarps)
   }
 }
 
+// the CG loop's condition: another pass while an instance's solve is running, at most `cap` passes
+__global__ void k_nb_cond(cudaGraphConditionalHandle h, const int* __restrict__ fl, int count, int* __restrict__ passes,
+                          int cap) {
+  int mine = 0;
+  for (int s = threadIdx.x; s < count; s += blockDim.x) mine |= !fl[s * NNF + G_CG_DONE];
+  const int running = __syncthreads_or(mine);
+  if (threadIdx.x == 0) {
+    const int c = ++*passes;
+    cudaGraphSetConditional(h, (running && c < cap) ? 1u : 0u);
+  }
+}
+
 // du += (double) d32 for instances that ran this round's inner solve
 __global__ void __launch_bounds__(32 * kWarps)
     k_nb_ir_correct(const float* __restrict__ d32, double* __restrict__ du, int64_t nchunks,
@@ -450,6 +519,8 @@ struct NBatch {
   DeviceArray<int> owner;
   DeviceArray<double> r, du, rr, p, ap, d, inv, zero, part, sc;
   DeviceArray<int> fl;
+  DeviceArray<unsigned> cnt;  // per instance: chunks counted by the fused reductions (0 between launches)
+  DeviceArray<int> passes;    // the CG loop graph's pass count
   int* fl_h = nullptr;
   double* sc_h = nullptr;
   cudaGraphExec_t graph = nullptr;
@@ -488,14 +559,10 @@ struct NBatch {
     const double k[3] = {1.0, 0.0, 0.0};
     const unsigned g = chunk_grid(nchunks);
     general_apply(force->s, k, p.ptr, ap.ptr, cs);
-    k_nb_dot<double><<<g, 32 * kWarps, 0, cs>>>(p.ptr, ap.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_CG_DONE,
-                                                o.lanes, part.ptr);
-    level(1, G_CG_DONE, N_PAP);
-    k_nb_alpha<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+    k_nb_pap<double><<<g, 32 * kWarps, 0, cs>>>(p.ptr, ap.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, o.lanes, part.ptr,
+                                                sc.ptr, cnt.ptr);
     k_nb_update<double><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p.ptr, ap.ptr, inv.ptr, du.ptr, rr.ptr, nchunks,
-                                                   owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks);
-    level(2, G_CG_DONE, N_RR);
-    k_nb_beta<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+                                                   owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
     k_nb_p<double><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv.ptr, rr.ptr, p.ptr, nchunks, owner.ptr, rg.ptr);
     FX_LAUNCH_CHECK("nbatch_cg");
   }
@@ -505,21 +572,18 @@ struct NBatch {
     const double k[3] = {1.0, 0.0, 0.0};
     const unsigned g = chunk_grid(nchunks);
     general_apply_f32(force->s, k, p32.ptr, ap32.ptr, cs);
-    k_nb_dot<float><<<g, 32 * kWarps, 0, cs>>>(p32.ptr, ap32.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, G_CG_DONE,
-                                               o.lanes, part.ptr);
-    level(1, G_CG_DONE, N_PAP);
-    k_nb_alpha<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+    k_nb_pap<float><<<g, 32 * kWarps, 0, cs>>>(p32.ptr, ap32.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, o.lanes,
+                                               part.ptr, sc.ptr, cnt.ptr);
     k_nb_update<float><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr,
-                                                  nchunks, owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks);
-    level(2, G_CG_DONE, N_RR);
-    k_nb_beta<<<inst_grid(), 128, 0, cs>>>(sc.ptr, fl.ptr, count);
+                                                  nchunks, owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
     k_nb_p<float><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv32.ptr, rr32.ptr, p32.ptr, nchunks, owner.ptr,
                                              rg.ptr);
     FX_LAUNCH_CHECK("nbatch_cg32");
   }
 
-  // CG iterations until every instance's solve is done: a first block of 8 eagerly, then a
-  // captured graph of 8 (one per precision, kept), the flags read after each block
+  // CG iterations until every instance's solve is done: a first block of 8 eagerly (the first
+  // applies build lazy state), then a kept graph (one per precision) whose while node runs blocks of
+  // 8 iterations and a condition kernel until no instance is running, with one host read at the end
   void cg_loop(bool f32) {
     const int block = 8;
     for (int i = 0; i < block; ++i) {
@@ -528,28 +592,50 @@ struct NBatch {
     }
     read_flags();
     cudaGraphExec_t& gx = f32 ? graph32 : graph;
-    while (any(G_CG_DONE, 0)) {
+    if (any(G_CG_DONE, 0)) {
       if (!gx) {
-        cudaGraph_t gr = nullptr;
-        FX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t g = nullptr;
+        FX_CUDA(cudaGraphCreate(&g, 0));
         try {
-          for (int i = 0; i < block; ++i) {
-            if (f32) cg_iteration32();
-            else cg_iteration();
+          cudaGraphConditionalHandle h;
+          FX_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+          cudaGraphNodeParams cp{};
+          cp.type = cudaGraphNodeTypeConditional;
+          cp.conditional.handle = h;
+          cp.conditional.type = cudaGraphCondTypeWhile;
+          cp.conditional.size = 1;
+          cudaGraphNode_t node;
+          FX_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+          cudaGraph_t body = cp.conditional.phGraph_out[0];
+          FX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+          try {
+            for (int i = 0; i < block; ++i) {
+              if (f32) cg_iteration32();
+              else cg_iteration();
+            }
+            // every solve ends within its iteration limit; the cap only bounds the loop
+            const int cap = (std::max(o.max_iterations, 0) + block - 1) / block + 2;
+            k_nb_cond<<<1, 128, 0, cs>>>(h, fl.ptr, count, passes.ptr, cap);
+            FX_LAUNCH_CHECK("nbatch_cg_condition");
+          } catch (...) {
+            cudaStreamEndCapture(cs, &body);
+            throw;
           }
+          FX_CUDA(cudaStreamEndCapture(cs, &body));
+          FX_CUDA(cudaGraphInstantiate(&gx, g, 0));
         } catch (...) {
-          cudaStreamEndCapture(cs, &gr);
-          if (gr) cudaGraphDestroy(gr);
+          if (gx) cudaGraphExecDestroy(gx);
+          gx = nullptr;
+          cudaGraphDestroy(g);
           throw;
         }
-        FX_CUDA(cudaStreamEndCapture(cs, &gr));
-        const cudaError_t e = cudaGraphInstantiate(&gx, gr, 0);
-        cudaGraphDestroy(gr);
-        if (e != cudaSuccess) gx = nullptr;
-        FX_CUDA(e);
+        cudaGraphDestroy(g);
       }
+      FX_CUDA(cudaMemsetAsync(passes.ptr, 0, sizeof(int), cs));
       FX_CUDA(cudaGraphLaunch(gx, cs));
       read_flags();
+      // every solve ends within its iteration limit, well inside the loop's cap
+      if (any(G_CG_DONE, 0)) throw Error(FX_E_INVALID, "batched CG: a solve did not end within its iteration limit");
     }
   }
 
@@ -751,6 +837,9 @@ int fx_nbatch_create(const fx_mesh* meshes, int32_t count, int32_t device, fx_so
       b.part.alloc(static_cast<size_t>(b.nchunks) * 2);
       b.sc.alloc(static_cast<size_t>(count) * fx::NNS);
       b.fl.alloc(static_cast<size_t>(count) * fx::NNF);
+      b.cnt.alloc(static_cast<size_t>(count));
+      b.cnt.zero(nullptr);
+      b.passes.alloc(1);
       FX_CUDA(cudaMallocHost(&b.fl_h, sizeof(int) * fx::NNF * count));
       FX_CUDA(cudaMallocHost(&b.sc_h, sizeof(double) * fx::NNS * count));
       // the creation's work is on the legacy stream; a device-wide synchronization would also wait
