@@ -34,6 +34,7 @@ namespace fx {
 namespace {
 
 constexpr int kWarps = 8;
+static_assert(32 * kWarps == 256 && kChunkBlock == 256, "both forms of the CG kernels launch 256 threads");
 constexpr int64_t kMaxSlotChunks = 2048;  // one level of chunk sums: n <= 2048 * 2048 per slot
 
 // per-slot scalars
@@ -252,30 +253,70 @@ __global__ void k_b_inner_start(double* sc, int* fl, const int* used, int nslots
   f[F_DONE] = f[F_CONV] || f[F_MAXIT] <= 0;
 }
 
+// The inner CG's vector kernels in two forms with the same arithmetic and sums: BLOCK, a block of
+// kChunkBlock threads per chunk (every entry's loads in flight at once, the chunk's sums by one warp
+// from shared memory), for batches of at most kBlockChunks chunks; otherwise a warp per chunk (8 per
+// block, lane_loop). Both launch 256 threads per block.
+
 // An inner iteration's p.ap: chunk sums of the running slots (T accumulated in double, fused
 // multiply-adds, lane order), then in the warp that counts a slot's last chunk its second level
 // and ConjugateGradient's alpha step (p.ap <= 0: indefinite, the inner solve ends).
-template <class TI>
-__global__ void __launch_bounds__(32 * kWarps)
+template <class TI, bool BLOCK>
+__global__ void __launch_bounds__(256)
     k_b_pap(const TI* __restrict__ p, const TI* __restrict__ ap, int64_t nchunks, int64_t ld,
             const int* __restrict__ chunk_slot, const SlotDev* __restrict__ sd, int* __restrict__ fl, int lanes,
             double* __restrict__ part, double* __restrict__ sc, unsigned* __restrict__ cnt) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = slot_of_chunk(chunk_slot, c);
-  if (s < 0 || fl[s * NFL + F_DONE]) return;
-  const int64_t begin = c * kChunk;
-  const int64_t end = sd[s].off + sd[s].n;
-  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  double acc = 0.0;
-  if (lane < lanes)
-    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<TI, 2>{{p[i], ap[i]}}; },
-                 [&](int64_t, const Ops<TI, 2>& o) {
-                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
-                 });
-  double total = 0.0;
-  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  int lane;
+  int64_t c;
+  int s;
+  double total;
+  if constexpr (BLOCK) {
+    __shared__ TI sa[kChunk], sb[kChunk];
+    c = blockIdx.x;
+    s = slot_of_chunk(chunk_slot, c);
+    if (s < 0 || fl[s * NFL + F_DONE]) return;
+    const int64_t begin = c * kChunk;
+    const int64_t end = sd[s].off + sd[s].n;
+    const int len = static_cast<int>((end - begin < kChunk) ? end - begin : kChunk);
+    TI va[kChunkPer], vb[kChunkPer];
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        va[k] = p[begin + j];
+        vb[k] = ap[begin + j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        sa[j] = va[k];
+        sb[j] = vb[k];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    lane = threadIdx.x;
+    total = chunk_fma_sum(sa, sb, len, lanes, lane);
+  } else {
+    lane = threadIdx.x & 31;
+    c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    if (c >= nchunks) return;
+    s = slot_of_chunk(chunk_slot, c);
+    if (s < 0 || fl[s * NFL + F_DONE]) return;
+    const int64_t begin = c * kChunk;
+    const int64_t end = sd[s].off + sd[s].n;
+    const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+    double acc = 0.0;
+    if (lane < lanes)
+      lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<TI, 2>{{p[i], ap[i]}}; },
+                   [&](int64_t, const Ops<TI, 2>& o) {
+                     acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
+                   });
+    total = 0.0;
+    for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  }
   if (lane == 0) part[c] = total;
   if (!slot_last(cnt + s, sd[s].nc, lane)) return;
   const double pap = slot_level(part, ld, 0, sd[s], lanes, lane);
@@ -295,37 +336,84 @@ __global__ void __launch_bounds__(32 * kWarps)
 // d += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (column 1 at part + ld); then in the
 // warp that counts a slot's last chunk the two second levels and the iteration's end
 // (ConjugateGradient's test on ||rr||, the iteration limit, beta)
-template <class TI>
-__global__ void __launch_bounds__(32 * kWarps)
+template <class TI, bool BLOCK>
+__global__ void __launch_bounds__(256)
     k_b_update(double* __restrict__ sc, int* __restrict__ fl, const TI* __restrict__ p,
                const TI* __restrict__ ap, const TI* __restrict__ inv, TI* __restrict__ d,
                TI* __restrict__ rr, int64_t nchunks, const int* __restrict__ chunk_slot,
                const SlotDev* __restrict__ sd, int lanes, double* __restrict__ part, int64_t ld,
                unsigned* __restrict__ cnt) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = slot_of_chunk(chunk_slot, c);
-  if (s < 0 || fl[s * NFL + F_DONE]) return;
-  const TI alpha = static_cast<TI>(sc[s * NSC + S_ALPHA]);
-  const int64_t begin = c * kChunk;
-  const int64_t end = sd[s].off + sd[s].n;
-  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  double srr = 0.0, srz = 0.0;
-  if (lane < lanes)
-    lane_loop<4>(begin, len, lane, lanes, [&](int64_t i) { return Ops<TI, 5>{{p[i], ap[i], inv[i], d[i], rr[i]}}; },
-                 [&](int64_t i, const Ops<TI, 5>& o) {
-                   d[i] = fma_t(alpha, o.v[0], o.v[3]);
-                   const TI ri = fma_t(-alpha, o.v[1], o.v[4]);
-                   rr[i] = ri;
-                   const TI zi = o.v[2] * ri;
-                   srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
-                   srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
-                 });
-  double trr = 0.0, trz = 0.0;
-  for (int j = 0; j < lanes; ++j) {
-    trr += __shfl_sync(0xffffffffu, srr, j);
-    trz += __shfl_sync(0xffffffffu, srz, j);
+  int lane;
+  int64_t c;
+  int s;
+  double trr, trz;
+  if constexpr (BLOCK) {
+    __shared__ TI sr[kChunk], sz[kChunk];
+    c = blockIdx.x;
+    s = slot_of_chunk(chunk_slot, c);
+    if (s < 0 || fl[s * NFL + F_DONE]) return;
+    const TI alpha = static_cast<TI>(sc[s * NSC + S_ALPHA]);
+    const int64_t begin = c * kChunk;
+    const int64_t end = sd[s].off + sd[s].n;
+    const int len = static_cast<int>((end - begin < kChunk) ? end - begin : kChunk);
+    TI vp[kChunkPer], vap[kChunkPer], vinv[kChunkPer], vd[kChunkPer], vrr[kChunkPer];
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        const int64_t i = begin + j;
+        vp[k] = p[i];
+        vap[k] = ap[i];
+        vinv[k] = inv[i];
+        vd[k] = d[i];
+        vrr[k] = rr[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        const int64_t i = begin + j;
+        d[i] = fma_t(alpha, vp[k], vd[k]);
+        const TI ri = fma_t(-alpha, vap[k], vrr[k]);
+        rr[i] = ri;
+        sr[j] = ri;
+        sz[j] = vinv[k] * ri;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    lane = threadIdx.x;
+    trr = chunk_fma_sum(sr, sr, len, lanes, lane);
+    trz = chunk_fma_sum(sr, sz, len, lanes, lane);
+  } else {
+    lane = threadIdx.x & 31;
+    c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    if (c >= nchunks) return;
+    s = slot_of_chunk(chunk_slot, c);
+    if (s < 0 || fl[s * NFL + F_DONE]) return;
+    const TI alpha = static_cast<TI>(sc[s * NSC + S_ALPHA]);
+    const int64_t begin = c * kChunk;
+    const int64_t end = sd[s].off + sd[s].n;
+    const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+    double srr = 0.0, srz = 0.0;
+    if (lane < lanes)
+      lane_loop<4>(begin, len, lane, lanes,
+                   [&](int64_t i) { return Ops<TI, 5>{{p[i], ap[i], inv[i], d[i], rr[i]}}; },
+                   [&](int64_t i, const Ops<TI, 5>& o) {
+                     d[i] = fma_t(alpha, o.v[0], o.v[3]);
+                     const TI ri = fma_t(-alpha, o.v[1], o.v[4]);
+                     rr[i] = ri;
+                     const TI zi = o.v[2] * ri;
+                     srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+                     srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+                   });
+    trr = 0.0;
+    trz = 0.0;
+    for (int j = 0; j < lanes; ++j) {
+      trr += __shfl_sync(0xffffffffu, srr, j);
+      trz += __shfl_sync(0xffffffffu, srz, j);
+    }
   }
   if (lane == 0) {
     part[c] = trr;
@@ -357,22 +445,47 @@ __global__ void __launch_bounds__(32 * kWarps)
 
 // p = inv rr + beta p (the beta of a slot that finished this iteration is stale: its p is
 // never read again)
-template <class TI>
-__global__ void __launch_bounds__(32 * kWarps)
+template <class TI, bool BLOCK>
+__global__ void __launch_bounds__(256)
     k_b_p(const double* __restrict__ sc, const int* __restrict__ fl, const TI* __restrict__ inv,
           const TI* __restrict__ rr, TI* __restrict__ p, int64_t nchunks, const int* __restrict__ chunk_slot,
           const SlotDev* __restrict__ sd) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = slot_of_chunk(chunk_slot, c);
-  if (s < 0 || fl[s * NFL + F_DONE]) return;
-  const TI beta = static_cast<TI>(sc[s * NSC + S_BETA]);
-  const int64_t begin = c * kChunk;
-  const int64_t end = sd[s].off + sd[s].n;
-  const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
-  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<TI, 3>{{p[i], inv[i], rr[i]}}; },
-               [&](int64_t i, const Ops<TI, 3>& o) { p[i] = fma_t(beta, o.v[0], o.v[1] * o.v[2]); });
+  if constexpr (BLOCK) {
+    const int64_t c = blockIdx.x;
+    const int s = slot_of_chunk(chunk_slot, c);
+    if (s < 0 || fl[s * NFL + F_DONE]) return;
+    const TI beta = static_cast<TI>(sc[s * NSC + S_BETA]);
+    const int64_t begin = c * kChunk;
+    const int64_t end = sd[s].off + sd[s].n;
+    const int len = static_cast<int>((end - begin < kChunk) ? end - begin : kChunk);
+    TI vp[kChunkPer], vinv[kChunkPer], vrr[kChunkPer];
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        vp[k] = p[begin + j];
+        vinv[k] = inv[begin + j];
+        vrr[k] = rr[begin + j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) p[begin + j] = fma_t(beta, vp[k], vinv[k] * vrr[k]);
+    }
+  } else {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    if (c >= nchunks) return;
+    const int s = slot_of_chunk(chunk_slot, c);
+    if (s < 0 || fl[s * NFL + F_DONE]) return;
+    const TI beta = static_cast<TI>(sc[s * NSC + S_BETA]);
+    const int64_t begin = c * kChunk;
+    const int64_t end = sd[s].off + sd[s].n;
+    const int64_t len = (end - begin < kChunk) ? end - begin : kChunk;
+    lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<TI, 3>{{p[i], inv[i], rr[i]}}; },
+                 [&](int64_t i, const Ops<TI, 3>& o) { p[i] = fma_t(beta, o.v[0], o.v[1] * o.v[2]); });
+  }
 }
 
 // x += (double) d for slots that ran an inner solve this round; the round's counters
@@ -544,13 +657,22 @@ struct Engine {
 
   template <class TI>
   void inner_iteration_t(const unsigned char* inst, TI* p, TI* ap, const TI* iv, TI* d, TI* rr) {
-    const unsigned g = chunk_grid(high);
     box_batch_apply(sizeof(TI) == 4, inst, work.ptr, nwork, persistent ? queue.ptr : nullptr, cs);
-    k_b_pap<TI><<<g, 32 * kWarps, 0, cs>>>(p, ap, high, nchunks, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
-                                           part.ptr, sc.ptr, cnt.ptr);
-    k_b_update<TI><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p, ap, iv, d, rr, high, chunk_slot.ptr, sd_dev.ptr,
-                                              o.lanes, part.ptr, nchunks, cnt.ptr);
-    k_b_p<TI><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, p, high, chunk_slot.ptr, sd_dev.ptr);
+    if (high <= kBlockChunks) {  // a block per chunk
+      const unsigned gb = static_cast<unsigned>(high);
+      k_b_pap<TI, true><<<gb, kChunkBlock, 0, cs>>>(p, ap, high, nchunks, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
+                                                    part.ptr, sc.ptr, cnt.ptr);
+      k_b_update<TI, true><<<gb, kChunkBlock, 0, cs>>>(sc.ptr, fl.ptr, p, ap, iv, d, rr, high, chunk_slot.ptr,
+                                                       sd_dev.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
+      k_b_p<TI, true><<<gb, kChunkBlock, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, p, high, chunk_slot.ptr, sd_dev.ptr);
+    } else {  // a warp per chunk
+      const unsigned g = chunk_grid(high);
+      k_b_pap<TI, false><<<g, 32 * kWarps, 0, cs>>>(p, ap, high, nchunks, chunk_slot.ptr, sd_dev.ptr, fl.ptr, o.lanes,
+                                                    part.ptr, sc.ptr, cnt.ptr);
+      k_b_update<TI, false><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p, ap, iv, d, rr, high, chunk_slot.ptr,
+                                                       sd_dev.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
+      k_b_p<TI, false><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, p, high, chunk_slot.ptr, sd_dev.ptr);
+    }
     FX_LAUNCH_CHECK("batch_inner");
   }
   void inner_iteration() {

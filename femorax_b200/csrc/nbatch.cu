@@ -22,6 +22,7 @@ namespace fx {
 namespace {
 
 constexpr int kWarps = 8;
+static_assert(32 * kWarps == 256 && kChunkBlock == 256, "both forms of the CG kernels launch 256 threads");
 constexpr int64_t kMaxInstanceChunks = 2048;  // one level of chunk sums per instance
 
 // per-instance scalars and flags
@@ -222,28 +223,67 @@ __global__ void k_nb_cg_start(double* sc, int* fl, int count, double rtol, doubl
   f[G_CG_DONE] = f[G_CG_CONV] || max_it <= 0;
 }
 
+// The CG's vector kernels in two forms with the same arithmetic and sums: BLOCK, a block of
+// kChunkBlock threads per chunk (every entry's loads in flight at once, the chunk's sums by one warp
+// from shared memory), for combined meshes of at most kBlockChunks chunks; otherwise a warp per
+// chunk (8 per block, lane_loop). Both launch 256 threads per block.
+
 // A CG iteration's p.ap: chunk sums of the instances still solving (T accumulated in double, fused
 // multiply-adds, lane order), then in the warp that counts an instance's last chunk its second
 // level and ConjugateGradient's alpha step (p.ap <= 0: indefinite, the solve ends).
-template <class T>
-__global__ void __launch_bounds__(32 * kWarps)
+template <class T, bool BLOCK>
+__global__ void __launch_bounds__(256)
     k_nb_pap(const T* __restrict__ p, const T* __restrict__ ap, int64_t nchunks, const int* __restrict__ owner,
              const Range* __restrict__ rg, int* __restrict__ fl, int lanes, double* __restrict__ part,
              double* __restrict__ sc, unsigned* __restrict__ cnt) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = owner[c];
-  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
-  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  double acc = 0.0;
-  if (lane < lanes)
-    lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{p[i], ap[i]}}; },
-                 [&](int64_t, const Ops<T, 2>& o) {
-                   acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
-                 });
-  double total = 0.0;
-  for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  int lane;
+  int64_t c;
+  int s;
+  double total;
+  if constexpr (BLOCK) {
+    __shared__ T sa[kChunk], sb[kChunk];
+    c = blockIdx.x;
+    s = owner[c];
+    if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+    const int64_t begin = c * kChunk;
+    const int len = static_cast<int>(chunk_len(rg[s], begin));
+    T va[kChunkPer], vb[kChunkPer];
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        va[k] = p[begin + j];
+        vb[k] = ap[begin + j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        sa[j] = va[k];
+        sb[j] = vb[k];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    lane = threadIdx.x;
+    total = chunk_fma_sum(sa, sb, len, lanes, lane);
+  } else {
+    lane = threadIdx.x & 31;
+    c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    if (c >= nchunks) return;
+    s = owner[c];
+    if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+    const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+    double acc = 0.0;
+    if (lane < lanes)
+      lane_loop<8>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 2>{{p[i], ap[i]}}; },
+                   [&](int64_t, const Ops<T, 2>& o) {
+                     acc = fma(static_cast<double>(o.v[0]), static_cast<double>(o.v[1]), acc);
+                   });
+    total = 0.0;
+    for (int j = 0; j < lanes; ++j) total += __shfl_sync(0xffffffffu, acc, j);
+  }
   if (lane == 0) part[c] = total;
   if (!instance_last(cnt + s, rg[s].nc, lane)) return;
   const double pap = instance_level(part, nchunks, 0, rg[s], lanes, lane);
@@ -263,34 +303,80 @@ __global__ void __launch_bounds__(32 * kWarps)
 // du += alpha p; rr -= alpha ap; chunk sums of rr.rr and rr.z (vectors of type T, sums in double);
 // then in the warp that counts an instance's last chunk the two second levels and the iteration's
 // end (ConjugateGradient's test on ||rr||, the iteration limit, beta)
-template <class T>
-__global__ void __launch_bounds__(32 * kWarps)
+template <class T, bool BLOCK>
+__global__ void __launch_bounds__(256)
     k_nb_update(double* __restrict__ sc, int* __restrict__ fl, const T* __restrict__ p,
                 const T* __restrict__ ap, const T* __restrict__ inv, T* __restrict__ du, T* __restrict__ rr,
                 int64_t nchunks, const int* __restrict__ owner, const Range* __restrict__ rg, int lanes,
                 double* __restrict__ part, int64_t ld, unsigned* __restrict__ cnt) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = owner[c];
-  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
-  const T alpha = static_cast<T>(sc[s * NNS + N_ALPHA]);
-  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  double srr = 0.0, srz = 0.0;
-  if (lane < lanes)
-    lane_loop<4>(begin, len, lane, lanes, [&](int64_t i) { return Ops<T, 5>{{p[i], ap[i], inv[i], du[i], rr[i]}}; },
-                 [&](int64_t i, const Ops<T, 5>& o) {
-                   du[i] = fma(alpha, o.v[0], o.v[3]);
-                   const T ri = fma(-alpha, o.v[1], o.v[4]);
-                   rr[i] = ri;
-                   const T zi = o.v[2] * ri;
-                   srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
-                   srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
-                 });
-  double trr = 0.0, trz = 0.0;
-  for (int j = 0; j < lanes; ++j) {
-    trr += __shfl_sync(0xffffffffu, srr, j);
-    trz += __shfl_sync(0xffffffffu, srz, j);
+  int lane;
+  int64_t c;
+  int s;
+  double trr, trz;
+  if constexpr (BLOCK) {
+    __shared__ T sr[kChunk], sz[kChunk];
+    c = blockIdx.x;
+    s = owner[c];
+    if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+    const T alpha = static_cast<T>(sc[s * NNS + N_ALPHA]);
+    const int64_t begin = c * kChunk;
+    const int len = static_cast<int>(chunk_len(rg[s], begin));
+    T vp[kChunkPer], vap[kChunkPer], vinv[kChunkPer], vdu[kChunkPer], vrr[kChunkPer];
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        const int64_t i = begin + j;
+        vp[k] = p[i];
+        vap[k] = ap[i];
+        vinv[k] = inv[i];
+        vdu[k] = du[i];
+        vrr[k] = rr[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        const int64_t i = begin + j;
+        du[i] = fma(alpha, vp[k], vdu[k]);
+        const T ri = fma(-alpha, vap[k], vrr[k]);
+        rr[i] = ri;
+        sr[j] = ri;
+        sz[j] = vinv[k] * ri;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    lane = threadIdx.x;
+    trr = chunk_fma_sum(sr, sr, len, lanes, lane);
+    trz = chunk_fma_sum(sr, sz, len, lanes, lane);
+  } else {
+    lane = threadIdx.x & 31;
+    c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    if (c >= nchunks) return;
+    s = owner[c];
+    if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+    const T alpha = static_cast<T>(sc[s * NNS + N_ALPHA]);
+    const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+    double srr = 0.0, srz = 0.0;
+    if (lane < lanes)
+      lane_loop<4>(begin, len, lane, lanes,
+                   [&](int64_t i) { return Ops<T, 5>{{p[i], ap[i], inv[i], du[i], rr[i]}}; },
+                   [&](int64_t i, const Ops<T, 5>& o) {
+                     du[i] = fma(alpha, o.v[0], o.v[3]);
+                     const T ri = fma(-alpha, o.v[1], o.v[4]);
+                     rr[i] = ri;
+                     const T zi = o.v[2] * ri;
+                     srr = fma(static_cast<double>(ri), static_cast<double>(ri), srr);
+                     srz = fma(static_cast<double>(ri), static_cast<double>(zi), srz);
+                   });
+    trr = 0.0;
+    trz = 0.0;
+    for (int j = 0; j < lanes; ++j) {
+      trr += __shfl_sync(0xffffffffu, srr, j);
+      trz += __shfl_sync(0xffffffffu, srz, j);
+    }
   }
   if (lane == 0) {
     part[c] = trr;
@@ -321,20 +407,44 @@ __global__ void __launch_bounds__(32 * kWarps)
 }
 
 // p = inv rr + beta p
-template <class T>
-__global__ void __launch_bounds__(32 * kWarps)
+template <class T, bool BLOCK>
+__global__ void __launch_bounds__(256)
     k_nb_p(const double* __restrict__ sc, const int* __restrict__ fl, const T* __restrict__ inv,
            const T* __restrict__ rr, T* __restrict__ p, int64_t nchunks, const int* __restrict__ owner,
            const Range* __restrict__ rg) {
-  const int lane = threadIdx.x & 31;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
-  if (c >= nchunks) return;
-  const int s = owner[c];
-  if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
-  const T beta = static_cast<T>(sc[s * NNS + N_BETA]);
-  const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
-  lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<T, 3>{{p[i], inv[i], rr[i]}}; },
-               [&](int64_t i, const Ops<T, 3>& o) { p[i] = fma(beta, o.v[0], o.v[1] * o.v[2]); });
+  if constexpr (BLOCK) {
+    const int64_t c = blockIdx.x;
+    const int s = owner[c];
+    if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+    const T beta = static_cast<T>(sc[s * NNS + N_BETA]);
+    const int64_t begin = c * kChunk;
+    const int len = static_cast<int>(chunk_len(rg[s], begin));
+    T vp[kChunkPer], vinv[kChunkPer], vrr[kChunkPer];
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) {
+        vp[k] = p[begin + j];
+        vinv[k] = inv[begin + j];
+        vrr[k] = rr[begin + j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunkPer; ++k) {
+      const int j = threadIdx.x + k * kChunkBlock;
+      if (j < len) p[begin + j] = fma(beta, vp[k], vinv[k] * vrr[k]);
+    }
+  } else {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+    if (c >= nchunks) return;
+    const int s = owner[c];
+    if (s < 0 || fl[s * NNF + G_CG_DONE]) return;
+    const T beta = static_cast<T>(sc[s * NNS + N_BETA]);
+    const int64_t begin = c * kChunk, len = chunk_len(rg[s], begin);
+    lane_loop<8>(begin, len, lane, 32, [&](int64_t i) { return Ops<T, 3>{{p[i], inv[i], rr[i]}}; },
+                 [&](int64_t i, const Ops<T, 3>& o) { p[i] = fma(beta, o.v[0], o.v[1] * o.v[2]); });
+  }
 }
 
 // u += du for instances that solved this iteration; their counters
@@ -555,29 +665,38 @@ struct NBatch {
     FX_LAUNCH_CHECK("nbatch_level");
   }
 
+  // the vector kernels of one CG iteration (in vectors of type T), in the form for this many chunks
+  template <class T>
+  void cg_vectors(T* pv, T* apv, const T* iv, T* dv, T* rv) {
+    if (nchunks <= kBlockChunks) {  // a block per chunk
+      const unsigned gb = static_cast<unsigned>(nchunks);
+      k_nb_pap<T, true><<<gb, kChunkBlock, 0, cs>>>(pv, apv, nchunks, owner.ptr, rg.ptr, fl.ptr, o.lanes, part.ptr,
+                                                    sc.ptr, cnt.ptr);
+      k_nb_update<T, true><<<gb, kChunkBlock, 0, cs>>>(sc.ptr, fl.ptr, pv, apv, iv, dv, rv, nchunks, owner.ptr,
+                                                       rg.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
+      k_nb_p<T, true><<<gb, kChunkBlock, 0, cs>>>(sc.ptr, fl.ptr, iv, rv, pv, nchunks, owner.ptr, rg.ptr);
+    } else {  // a warp per chunk
+      const unsigned g = chunk_grid(nchunks);
+      k_nb_pap<T, false><<<g, 32 * kWarps, 0, cs>>>(pv, apv, nchunks, owner.ptr, rg.ptr, fl.ptr, o.lanes, part.ptr,
+                                                    sc.ptr, cnt.ptr);
+      k_nb_update<T, false><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, pv, apv, iv, dv, rv, nchunks, owner.ptr,
+                                                       rg.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
+      k_nb_p<T, false><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, iv, rv, pv, nchunks, owner.ptr, rg.ptr);
+    }
+  }
+
   void cg_iteration() {
     const double k[3] = {1.0, 0.0, 0.0};
-    const unsigned g = chunk_grid(nchunks);
     general_apply(force->s, k, p.ptr, ap.ptr, cs);
-    k_nb_pap<double><<<g, 32 * kWarps, 0, cs>>>(p.ptr, ap.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, o.lanes, part.ptr,
-                                                sc.ptr, cnt.ptr);
-    k_nb_update<double><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p.ptr, ap.ptr, inv.ptr, du.ptr, rr.ptr, nchunks,
-                                                   owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
-    k_nb_p<double><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv.ptr, rr.ptr, p.ptr, nchunks, owner.ptr, rg.ptr);
+    cg_vectors<double>(p.ptr, ap.ptr, inv.ptr, du.ptr, rr.ptr);
     FX_LAUNCH_CHECK("nbatch_cg");
   }
 
   // one iteration of the inner FP32 CG (the FP32 operator on the stored point tangents)
   void cg_iteration32() {
     const double k[3] = {1.0, 0.0, 0.0};
-    const unsigned g = chunk_grid(nchunks);
     general_apply_f32(force->s, k, p32.ptr, ap32.ptr, cs);
-    k_nb_pap<float><<<g, 32 * kWarps, 0, cs>>>(p32.ptr, ap32.ptr, nchunks, owner.ptr, rg.ptr, fl.ptr, o.lanes,
-                                               part.ptr, sc.ptr, cnt.ptr);
-    k_nb_update<float><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr,
-                                                  nchunks, owner.ptr, rg.ptr, o.lanes, part.ptr, nchunks, cnt.ptr);
-    k_nb_p<float><<<g, 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, inv32.ptr, rr32.ptr, p32.ptr, nchunks, owner.ptr,
-                                             rg.ptr);
+    cg_vectors<float>(p32.ptr, ap32.ptr, inv32.ptr, d32.ptr, rr32.ptr);
     FX_LAUNCH_CHECK("nbatch_cg32");
   }
 

@@ -217,6 +217,105 @@ __global__ void __launch_bounds__(32 * kWarps) k_cg_update(double* __restrict__ 
   }
 }
 
+// k_cg_pap and k_cg_update with a block per chunk (kChunkBlock threads; the grid is the chunks):
+// every entry's loads in flight at once, the chunk's sums by one warp from shared memory in the
+// same order, so the same bits; used for vectors of at most kBlockChunks chunks.
+template <class T>
+__global__ void __launch_bounds__(kChunkBlock) k_cg_pap_b(const T* __restrict__ p, const T* __restrict__ ap, int64_t n,
+                                                          int lanes, int64_t nchunks, double* __restrict__ out,
+                                                          double* __restrict__ out2, unsigned* __restrict__ counter,
+                                                          double* __restrict__ sc, int* __restrict__ fl) {
+  if (fl[F_DONE]) return;  // (the same for every block: the counter stays untouched)
+  __shared__ T sa[kChunk], sb[kChunk];
+  const int64_t c = blockIdx.x;
+  const int64_t begin = c * kChunk;
+  const int len = static_cast<int>((n - begin < kChunk) ? n - begin : kChunk);
+  T va[kChunkPer], vb[kChunkPer];
+#pragma unroll
+  for (int k = 0; k < kChunkPer; ++k) {
+    const int j = threadIdx.x + k * kChunkBlock;
+    if (j < len) {
+      va[k] = p[begin + j];
+      vb[k] = ap[begin + j];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kChunkPer; ++k) {
+    const int j = threadIdx.x + k * kChunkBlock;
+    if (j < len) {
+      sa[j] = va[k];
+      sb[j] = vb[k];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const double total = chunk_fma_sum(sa, sb, len, lanes, static_cast<int>(threadIdx.x));
+    if (threadIdx.x == 0) out[c] = total;
+  }
+  if (!last_block(counter)) return;
+  block_levels(out, out2, nchunks, 1, lanes, sc + S_PAP);
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    cg_alpha_step(sc, fl);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kChunkBlock) k_cg_update_b(double* __restrict__ sc, int* __restrict__ fl,
+                                                             const T* __restrict__ p, const T* __restrict__ ap,
+                                                             const T* __restrict__ inv, T* __restrict__ x,
+                                                             T* __restrict__ r, int64_t n, int lanes, int64_t nchunks,
+                                                             double* __restrict__ out, double* __restrict__ out2,
+                                                             unsigned* __restrict__ counter, int max_it) {
+  if (fl[F_DONE]) return;  // (the same for every block: the counter stays untouched)
+  __shared__ T sr[kChunk], sz[kChunk];
+  const T alpha = static_cast<T>(sc[S_ALPHA]);
+  const int64_t c = blockIdx.x;
+  const int64_t begin = c * kChunk;
+  const int len = static_cast<int>((n - begin < kChunk) ? n - begin : kChunk);
+  T vp[kChunkPer], vap[kChunkPer], vinv[kChunkPer], vx[kChunkPer], vr[kChunkPer];
+#pragma unroll
+  for (int k = 0; k < kChunkPer; ++k) {
+    const int j = threadIdx.x + k * kChunkBlock;
+    if (j < len) {
+      const int64_t i = begin + j;
+      vp[k] = p[i];
+      vap[k] = ap[i];
+      vinv[k] = inv[i];
+      vx[k] = x[i];
+      vr[k] = r[i];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kChunkPer; ++k) {
+    const int j = threadIdx.x + k * kChunkBlock;
+    if (j < len) {
+      const int64_t i = begin + j;
+      x[i] = fma(alpha, vp[k], vx[k]);
+      const T ri = fma(-alpha, vap[k], vr[k]);
+      r[i] = ri;
+      sr[j] = ri;
+      sz[j] = vinv[k] * ri;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = static_cast<int>(threadIdx.x);
+    const double trr = chunk_fma_sum(sr, sr, len, lanes, lane);
+    const double trz = chunk_fma_sum(sr, sz, len, lanes, lane);
+    if (lane == 0) {
+      out[c] = trr;
+      out[nchunks + c] = trz;
+    }
+  }
+  if (!last_block(counter)) return;
+  block_levels(out, out2, nchunks, 2, lanes, sc + S_RR);
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    cg_beta_step(sc, fl, max_it);
+  }
+}
+
 template <class T>
 __global__ void k_cg_p(const double* __restrict__ sc, const int* __restrict__ fl, const T* __restrict__ inv,
                        const T* __restrict__ r, T* __restrict__ p, int64_t n) {
@@ -435,10 +534,18 @@ struct Solver {
       apply(pp, aa, fl.ptr + F_DONE);
       // p.Ap and alpha, then the update, r.r, r.z and beta (each with its levels in the kernel's
       // last block), then p
-      k_cg_pap<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(pp, aa, n, lanes, nc, w.level[0].ptr, w.level[1].ptr,
-                                                         counter.ptr, sc.ptr, fl.ptr);
-      k_cg_update<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, pp, aa, iv, x, rr, n, lanes, nc,
-                                                            w.level[0].ptr, w.level[1].ptr, counter.ptr, max_it);
+      if (nc <= kBlockChunks) {
+        k_cg_pap_b<T><<<static_cast<unsigned>(nc), kChunkBlock, 0, cs>>>(pp, aa, n, lanes, nc, w.level[0].ptr,
+                                                                         w.level[1].ptr, counter.ptr, sc.ptr, fl.ptr);
+        k_cg_update_b<T><<<static_cast<unsigned>(nc), kChunkBlock, 0, cs>>>(sc.ptr, fl.ptr, pp, aa, iv, x, rr, n,
+                                                                            lanes, nc, w.level[0].ptr, w.level[1].ptr,
+                                                                            counter.ptr, max_it);
+      } else {
+        k_cg_pap<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(pp, aa, n, lanes, nc, w.level[0].ptr, w.level[1].ptr,
+                                                           counter.ptr, sc.ptr, fl.ptr);
+        k_cg_update<T><<<chunk_grid(nc), 32 * kWarps, 0, cs>>>(sc.ptr, fl.ptr, pp, aa, iv, x, rr, n, lanes, nc,
+                                                              w.level[0].ptr, w.level[1].ptr, counter.ptr, max_it);
+      }
       k_cg_p<T><<<ew(n), 256, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, pp, n);
       FX_LAUNCH_CHECK("cg_iteration");
     };
