@@ -748,6 +748,37 @@ def batched_j2_comparison(device, count=32, steps=8, seed=1):
             "converged": bool(b.converged and all(r.converged for r in single)), "bit_identical": bool(same)}
 
 
+def batched_j2_path(device, count=32, steps=8, seed=1):
+    """The batched arm of batched_j2_comparison alone (profiling): the same `count` seeded J2
+    instances on one cyclic cycle of `steps` load steps, Newton to ||r|| <= 1e-6 N, Jacobi-PCG to
+    1e-12; seconds by wall clock, Newton solves and CG iterations per instance and step."""
+    import torch
+    import femorax_b200 as fx
+    from femorax_b200 import serving, stages
+    inst = stages.j2_instances(count, seed=seed, sizes=(1, 2, 4, 8), nz_range=(20, 40))
+    meshes, fs = [], []
+    for spec, total in inst:
+        comp = fx.Model(spec).compile()
+        f, _ = stages.top_shear(spec, serving.equation_map(comp), total)
+        meshes.append(comp.mesh())
+        fs.append(f)
+    b = fx.BatchedNewton(meshes, fx.SolveOptions(relative_tolerance=1e-12, max_iterations=20000), device)
+    dev = torch.device("cuda", device)
+    F = torch.as_tensor(b.combine(fs), device=dev)
+    u = torch.zeros(b.total, dtype=torch.float64, device=dev)
+    newton, cg = [], []
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for lam in stages.cyclic_factors(1, steps):
+        it, res = b.step(F * float(lam), u, tol=1e-6, max_newton=25)
+        b.commit_state()
+        newton.append([int(v) for v in it])
+        cg.append([int(r.iterations) for r in res])
+    torch.cuda.synchronize(dev)
+    return {"instances": count, "load_steps": steps, "seconds": time.perf_counter() - t0, "newton": newton,
+            "cg_iterations": cg}
+
+
 def served_streams(device, count=1000, rates=((10.0, 40), (100.0, 400), (500.0, 400), (2000.0, 1000)), seed=3,
                    models=32, j2_models=12):
     """The served configuration at its sizes, on resident models (serving.pooled_stream: `models`
@@ -1055,6 +1086,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the explicit-stepping and served-versus-plain solve comparisons")
     ap.add_argument("--launch", default="", help="pin the box launch shape 'variant,kz' (profiling)")
+    ap.add_argument("--batched-j2", action="store_true",
+                    help="only the batched J2 path (32 instances, one cycle of 8 load steps; profiling)")
     ap.add_argument("--pimy-box", type=int, default=0,
                     help="only the PressureIndependMultiYield plastic box section, n^3 elements (profiling)")
     ap.add_argument("--served", type=int, default=0,
@@ -1075,6 +1108,9 @@ def main():
         return 0
     if args.pdmy_box:
         print(json.dumps(pdmy_force_box(int(os.environ.get("LOCAL_RANK", "0")), n=args.pdmy_box, evals=args.steps)))
+        return 0
+    if args.batched_j2:
+        print(json.dumps(batched_j2_path(int(os.environ.get("LOCAL_RANK", "0")))))
         return 0
     if args.pimy_box:
         print(json.dumps(pimy_explicit(int(os.environ.get("LOCAL_RANK", "0")), n=args.pimy_box, warm=args.warmup,
