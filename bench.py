@@ -77,13 +77,17 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
-    """DRAM bytes per apply from the committed ncu summary of this kernel and workload."""
+def load_traffic(variant, kz):
+    """DRAM bytes per apply from the committed ncu summary of this kernel and workload, when the
+    summary's launch shape (variant, kz) is the one timed; else None. Returns (bytes, source)."""
     p = os.path.join(ROOT, "profiles", "box_apply_layered128.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get("dram_bytes_per_launch")
-    return None
+    if not os.path.exists(p):
+        return None, "no ncu summary"
+    d = json.load(open(p))
+    shape = d.get("launch")
+    if shape is not None and (int(shape[0]), int(shape[1])) != (int(variant), int(kz)):
+        return None, f"ncu summary of launch {shape[0]},{shape[1]}; timed {variant},{kz}: not the same kernel"
+    return d.get("dram_bytes_per_launch"), "ncu summary profiles/box_apply_layered128.json (" + d.get("source", "") + ")"
 
 
 class ClockSampler:
@@ -1007,7 +1011,7 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     alg = algorithmic_bytes(neq, n_el, n_nodes)
     achieved = alg / (total_ms / args.steps * 1e-3) / 1e9
-    traffic = load_traffic()
+    traffic, traffic_source = load_traffic(launch[0], launch[1])
     alg32 = alg - 8 * neq  # x read and y written as 4-byte values
     ach32 = alg32 / (float(np.mean(f32_ms)) * 1e-3) / 1e9
     f32 = {"ms_per_apply": float(np.mean(f32_ms)), "gdof_per_s": neq / (float(np.mean(f32_ms)) * 1e-3) / 1e9,
@@ -1045,7 +1049,7 @@ def run_ours(args):
                        "chosen_by": "option" if args.launch else "autotuner", "all": tuned},
             "parity": parity,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": traffic, "traffic_source": traffic_source, "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg},
             "fp32_apply": f32,
             "gather_floor": floor,
