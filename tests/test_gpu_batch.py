@@ -6,7 +6,8 @@
   its rounds (continuous batching);
 - every solution meets the 1e-8 relative FP64 residual, checked here with the FP64 operator, and
   agrees with the plain FP64 CG solution to 1e-6 relative;
-- admission refuses when no slot or no range of chunks is free, and a retire makes room again.
+- admission refuses when no slot or no range of chunks is free, and a retire makes room again;
+- the block-per-chunk and warp-per-chunk forms of the CG vector kernels give the same bits.
 """
 import numpy as np
 import pytest
@@ -38,9 +39,9 @@ def engine(capacity=1 << 20, slots=8):
     return fx.BatchEngine(capacity, slots, options=fx.SolveOptions(relative_tolerance=RTOL))
 
 
-def run_to_end(e, slots):
+def run_to_end(e, slots, ticks=200):
     out = {}
-    for _ in range(200):
+    for _ in range(ticks):
         e.round()
         for s in list(slots):
             if e.finished(s):
@@ -72,6 +73,36 @@ def test_slot_equals_single_mixed_solve(prepared, alone):
         assert np.array_equal(xe, x.cpu().numpy()), rid
         assert (re.iterations, re.refinements) == (r.iterations, r.refinements)
         assert re.final_residual == r.final_residual
+
+
+def single_ir(force, b, n):
+    op = fx.MatrixFreeOperator(force, fx.OperatorCoefficients())
+    ir = fx.MixedPrecisionSolver(fx.SolveOptions(relative_tolerance=RTOL), inner_tolerance=1e-4)
+    ir.setup(op)
+    x = torch.zeros(n, dtype=torch.float64, device=DEV)
+    r = ir.solve(torch.as_tensor(b, device=DEV), x)
+    return x.cpu().numpy(), r
+
+
+def test_block_and_warp_forms_same_bits(prepared):
+    """The CG vector kernels take a block per chunk for vectors of at most 1,024 chunks and a warp
+    per chunk beyond; both sum in the same order. A small mesh batched beside one of more than 1,024
+    chunks runs the engine's warp form, its single solve the block form: the same bits, iterations
+    and rounds; the large mesh matches its own single solve too."""
+    big = serving.Request(9, 100, 100, 70)
+    fb, bb, nb = serving.prepare(big)
+    assert nb > 1024 * 2048
+    f0, b0, n0 = prepared[0]
+    e = engine(capacity=3 << 20)
+    s_big = e.admit(fb, bb)
+    s0 = e.admit(f0, b0)
+    out = run_to_end(e, {s_big: 9, s0: 0}, ticks=4000)
+    for rid, (force, b, n) in ((9, (fb, bb, nb)), (0, (f0, b0, n0))):
+        x, r = single_ir(force, b, n)
+        xe, re = out[rid]
+        assert r.converged and re.converged, rid
+        assert np.array_equal(xe, x), rid
+        assert (re.iterations, re.refinements) == (r.iterations, r.refinements), rid
 
 
 def test_alone_and_in_mix_are_the_same(prepared, alone):
