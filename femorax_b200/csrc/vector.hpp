@@ -46,7 +46,7 @@ __device__ __forceinline__ void lane_loop(int64_t begin, int64_t len, int lane, 
 constexpr int kChunkBlock = 256;
 constexpr int kChunkPer = static_cast<int>(kChunk) / kChunkBlock;
 // Vectors of at most this many chunks use the block-per-chunk forms; longer ones keep a warp per
-// chunk (enough warps in flight already; measured on a B200: the block forms 1.4x faster at 45 and
+// chunk (enough warps in flight already; measured on a B200: the block forms 1.4x faster at 64 and
 // 51 chunks, equal at 1,495, 4-7 % slower at the served engine's thousands of chunks).
 constexpr int64_t kBlockChunks = 1024;
 
