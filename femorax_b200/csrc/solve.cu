@@ -369,6 +369,10 @@ __device__ void cg_beta_step(double* sc, int* fl, int max_it) {
   sc[S_RZ] = sc[S_RZNEW];
 }
 
+// CG iterations per pass of the loop graph: fewer condition kernels and body relaunches against
+// at most kCgPass - 1 empty iterations after the solve ends.
+constexpr int kCgPass = 4;
+
 // The condition of the CG loop graph: another pass while the solve is not done, at most `cap`
 // passes (a bound the solve's own max_it already keeps below).
 __global__ void k_cg_cond(cudaGraphConditionalHandle h, const int* __restrict__ fl, int* __restrict__ passes, int cap) {
@@ -549,7 +553,7 @@ struct Solver {
       k_cg_p<T><<<ew(n), 256, 0, cs>>>(sc.ptr, fl.ptr, iv, rr, pp, n);
       FX_LAUNCH_CHECK("cg_iteration");
     };
-    // The iterations run as one graph: a while node whose body is two iterations and the
+    // The iterations run as one graph: a while node whose body is kCgPass iterations and the
     // condition kernel, so the device loops until the solve is done with no host round trip.
     // The begin above ran eagerly (its apply builds lazy state and this solver's coefficient
     // tables); a new graph is captured when the vectors differ from the last solve's.
@@ -575,11 +579,10 @@ struct Solver {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         FX_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         try {
-          // two iterations per pass (every kernel of an iteration skips once the solve is done, so
-          // a pass that ends the solve in its first iteration leaves the second one empty)
-          iteration();
-          iteration();
-          k_cg_cond<<<1, 1, 0, cs>>>(h, fl.ptr, passes.ptr, (max_it + 1) / 2 + 2);
+          // kCgPass iterations per pass (every kernel of an iteration skips once the solve is
+          // done, so the iterations of a pass after the one that ends the solve are empty)
+          for (int i = 0; i < kCgPass; ++i) iteration();
+          k_cg_cond<<<1, 1, 0, cs>>>(h, fl.ptr, passes.ptr, (max_it + kCgPass - 1) / kCgPass + 2);
           FX_LAUNCH_CHECK("cg_condition");
         } catch (...) {
           cudaStreamEndCapture(cs, &body);
