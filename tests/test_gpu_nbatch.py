@@ -2,7 +2,8 @@
 hardening and loads on one cyclic load path in one batch. Each instance's displacement history
 and Newton solve counts must be bit for bit those of the single-instance path (fx_solver_newton
 with the same options) on that mesh alone: the combined mesh keeps every instance's gather order,
-and every instance's reductions run over its own range in the documented order.
+and every instance's reductions run over its own range in the documented order, in the
+block-per-chunk form of the CG kernels (few chunks) and the warp-per-chunk form (more than 1,024).
 """
 import numpy as np
 import pytest
@@ -75,3 +76,28 @@ def test_mixed_batched_newton_equals_single_mixed_paths():
         assert np.array_equal(mixed.newton[:, i], single.newton), i
         peak = np.max(np.abs(plain.monitor[:, i]))
         assert np.max(np.abs(mixed.monitor[:, i] - plain.monitor[:, i])) <= 1e-6 * peak, i
+
+
+def test_many_instances_warp_form_equals_single_paths():
+    """More than 1,024 instances: the combined mesh spans more than 1,024 chunks (each instance's
+    range padded to whole chunks), so the batch's CG vector kernels take the warp-per-chunk form,
+    while each instance alone (one chunk) takes the block-per-chunk form: the same bits."""
+    inst = instances()
+    count = 1030
+    meshes, loads, mons = [], [], []
+    for i in range(count):
+        mesh, F, mon = inst[i % len(inst)]
+        meshes.append(mesh)
+        loads.append(F * (0.6 + 0.4 * (i % 7) / 6.0))
+        mons.append(mon)
+    b = fx.BatchedNewton(meshes)
+    assert b.offsets[-1] // 2048 > 1024
+    factors = stages.cyclic_factors(1, 8)[:2]
+    batched = stages.batched_load_path(meshes, loads, factors, mons, tol=1e-6)
+    for i in (0, 5, 517, count - 1):
+        single = stages.load_path(fx.InternalForce(meshes[i]), torch.as_tensor(loads[i], device=DEV), factors,
+                                  mons[i], tol=1e-6)
+        assert np.array_equal(batched.monitor[:, i], single.monitor), i
+        assert np.array_equal(batched.newton[:, i], single.newton), i
+        assert single.converged, i
+    assert batched.converged
